@@ -1,0 +1,86 @@
+"""Generate the golden fixtures under tests/golden/ from the reference's own
+test data.  Run once where the reference checkout is available:
+
+    python tests/golden/make_golden.py /path/to/chronusq_public
+
+Sources (paths within xsligroup/chronusq_public):
+* tests/func/reference/contract.hdf5 -- direct J/K of random X on water /
+  cc-pVTZ (tests/func/input/contract_ref.inp), checked by
+  tests/func/contract.cxx:97-190 at max|dAX| < 1e-9.  The 8 cases and their
+  (HER, contraction type) arguments follow contract.cxx:195-316, including the
+  two quirks (NONHER/REAL/K runs COULOMB, NONHER/COMPLEX/K runs HERMITIAN
+  EXCHANGE).
+* tests/scf/reference/water_cc-pVDZ_RHF_RHFGuess_READDEN_scratch.bin.ref --
+  one direct RHF build from a read density (tests/scf/rhf.cxx:74-110); the
+  basis is the inline uncontracted cc-pVDZ of
+  tests/scf/serial/rhf/water_cc-pVDZ_RHF_READDEN.inp.
+* tests/scf/reference/water_cc-pVDZ_DC-HF_RHFGuess_READDEN.bin.ref -- one 4C
+  Dirac-Coulomb build (tests/scf/fourcomphf.cxx:143-150).
+
+HDF5 datasets written from column-major buffers read back transposed; the
+fixtures store them in natural (row = first index) orientation.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from h5lite import H5File  # noqa: E402
+
+# (dataset group, HER flag, contraction type: 0 COULOMB / 1 EXCHANGE)
+CONTRACT_CASES = [
+    ("HER/REAL/J", 1, 0), ("NONHER/REAL/J", 0, 0),
+    ("HER/REAL/K", 1, 1), ("NONHER/REAL/K", 0, 0),
+    ("HER/COMPLEX/J", 1, 0), ("NONHER/COMPLEX/J", 0, 0),
+    ("HER/COMPLEX/K", 1, 1), ("NONHER/COMPLEX/K", 1, 1),
+]
+
+
+def _inline_basis(inp_path):
+    txt = open(inp_path).read()
+    return txt.split("BasisDef:")[1].split("[MISC]")[0]
+
+
+def main(ref_root):
+    f = H5File(os.path.join(ref_root, "tests/func/reference/contract.hdf5"))
+    out = {}
+    for g, her, ty in CONTRACT_CASES:
+        key = g.replace("/", "_")
+        out[key + "_X"] = f.read("/CONTRACTION/%s/X" % g).T.copy()
+        out[key + "_AX"] = f.read("/CONTRACTION/%s/AX" % g).T.copy()
+        out[key + "_her"] = np.int32(her)
+        out[key + "_type"] = np.int32(ty)
+    np.savez_compressed(os.path.join(HERE, "contract.npz"), **out)
+
+    rd = os.path.join(ref_root, "tests/scf/reference")
+    f = H5File(os.path.join(
+        rd, "water_cc-pVDZ_RHF_RHFGuess_READDEN_scratch.bin.ref"))
+    rhf = {k: f.read(p).T.copy() for k, p in [
+        ("D", "/SCF/1PDM_SCALAR"), ("F", "/SCF/FOCK_SCALAR"),
+        ("H", "/INTS/CORE_HAMILTONIAN_SCALAR"), ("S", "/INTS/OVERLAP"),
+        ("T", "/INTS/KINETIC")]}
+    rhf["E_total"] = f.read("/SCF/TOTAL_ENERGY")
+    rhf["E_many_body"] = f.read("/SCF/MANY_BODY_ENERGY")
+    rhf["basisdef"] = np.array(_inline_basis(os.path.join(
+        ref_root, "tests/scf/serial/rhf/water_cc-pVDZ_RHF_READDEN.inp")))
+    np.savez_compressed(os.path.join(HERE, "readden_rhf.npz"), **rhf)
+
+    f = H5File(os.path.join(rd, "water_cc-pVDZ_DC-HF_RHFGuess_READDEN.bin.ref"))
+    dc = {}
+    for comp in ("SCALAR", "MX", "MY", "MZ"):
+        dc["D_" + comp] = f.read("/SCF/1PDM_" + comp).T.copy()
+        dc["F_" + comp] = f.read("/SCF/FOCK_" + comp).T.copy()
+        dc["H_" + comp] = f.read("/INTS/CORE_HAMILTONIAN_" + comp).T.copy()
+    dc["S"] = f.read("/INTS/OVERLAP").T.copy()
+    dc["T"] = f.read("/INTS/KINETIC").T.copy()
+    dc["E_total"] = f.read("/SCF/TOTAL_ENERGY")
+    dc["E_many_body"] = f.read("/SCF/MANY_BODY_ENERGY")
+    dc["basisdef"] = np.array(_inline_basis(os.path.join(
+        ref_root, "tests/scf/serial/fourcomp/water_cc-pVDZ_DC-HF_READDEN.inp")))
+    np.savez_compressed(os.path.join(HERE, "readden_dc.npz"), **dc)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,60 @@
+"""Pins the CPU oracle to the reference's own golden data (no GPU)."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import (CONTRACT_CASES, contract_basis, golden,
+                     readden_rhf_basis)
+
+
+@pytest.fixture(scope="module")
+def contract_oracle():
+    return O.OracleBasis(contract_basis())
+
+
+@pytest.mark.parametrize("case", CONTRACT_CASES)
+def test_contract_hdf5(contract_oracle, case):
+    """tests/func/contract.cxx:97-190: max|AX - AX_ref| < 1e-9."""
+    g = golden("contract.npz")
+    AX, = contract_oracle.contract([g[case + "_X"]], [int(g[case + "_her"])],
+                                   [int(g[case + "_type"])])
+    assert np.abs(AX - g[case + "_AX"]).max() < 1e-9
+
+
+def test_readden_rhf_fock():
+    """One direct RHF build: FOCK - CORE_H = 2 J[D] - K[D]."""
+    g = golden("readden_rhf.npz")
+    ob = O.OracleBasis(readden_rhf_basis(g))
+    S, T = ob.overlap_kinetic()
+    assert np.abs(S - g["S"]).max() < 1e-12
+    assert np.abs(T - g["T"]).max() < 1e-9
+    J, K = ob.contract([g["D"], g["D"]], [1, 1], [0, 1])
+    G = 2 * J - K
+    assert np.abs(G - (g["F"] - g["H"])).max() < 1e-9
+    # two-electron energy 1/4 Tr[G D] (singleslater/quantum.hpp:147-205)
+    e2 = 0.25 * np.sum(G * g["D"].T) * 1.0
+    assert abs(e2 - float(g["E_many_body"][0])) < 1e-8
+
+
+def test_normalisation_agrees(contract_oracle):
+    b = contract_basis()
+    assert np.allclose(contract_oracle.coefs(), b.flat()["coef"],
+                       rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("m,T", [(0, 0.0), (0, 1e-8), (3, 0.37), (8, 12.3),
+                                 (12, 35.9), (12, 36.1), (16, 80.0),
+                                 (4, 200.0)])
+def test_boys_against_series(m, T):
+    # independent reference: F_m(T) = int_0^1 t^2m exp(-T t^2) dt by
+    # composite Gauss-Legendre on [0,1]
+    x, w = np.polynomial.legendre.leggauss(200)
+    segs = 40
+    tot = 0.0
+    for s in range(segs):
+        a, b = s / segs, (s + 1) / segs
+        t = 0.5 * (b - a) * x + 0.5 * (a + b)
+        tot += 0.5 * (b - a) * np.sum(w * t ** (2 * m) * np.exp(-T * t * t))
+    assert abs(O.boys(m, T) - tot) <= 1e-14 * max(tot, 1e-300) + 1e-300
