@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Fock builds/s of the direct J/K build on one B200 (replicas per GPU).
+
+Workload (default): seeded (H2O)_16 cluster, def2-SVP (N = 384), one
+closed-shell build G = 2 J[D] - K[D] per step with D = C C^T, C 384 x 40
+seeded and S-orthonormalised.  A step is one Fock build (J and K of one
+density in one ``twoBodyContract`` call).
+
+value   = builds/s of the mixed-precision build (FP32 for quartets whose
+          Schwarz x density bound is below --cutoff, FP64 otherwise), inputs
+          resident in HBM (device pointers), timed per step with CUDA events
+          on the build stream; L2 is flushed (256 MiB write) between steps,
+          outside the events.
+e2e     = the same build through the public Python API with host (numpy)
+          buffers: H2D of D, D2H of J and K inside the timed region.
+fp64    = the same, all quartets in FP64 (the reference precision).
+Errors  = max |G - G_oracle| and |E2 - E2_oracle| against the CPU oracle
+          (FP64), computed once outside the timed region.
+
+--impl reference times the reference's algorithm on the host cores: the
+C++/OpenMP restatement of directScaffoldNew in oracle/ (the reference
+itself needs libint2/libcint and cannot be built here).
+
+Multi-GPU: the north-star path runs on one GPU; with --gpus N each rank runs
+an independent replica of the same build (replicas only, no collective) and
+value sums the builds of all ranks over the slowest rank's time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("Fock builds/s (mixed vs FP64, same B200) at <=1e-6 Eh Fock err; "
+          "p50/p99 latency")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="h2o16_def2svp")
+    ap.add_argument("--cutoff", type=float, default=1e-8)
+    ap.add_argument("--no-oracle", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return ws, rank, local, pg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def fma_peaks():
+    from chronusq_public_b200.build import PEAK_LIB
+    L = ctypes.CDLL(PEAK_LIB)
+    L.cqf_fma_peak_tflops.restype = ctypes.c_double
+    L.cqf_fma_peak_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+    return L.cqf_fma_peak_tflops(1, 4096), L.cqf_fma_peak_tflops(0, 16384)
+
+
+def cpu_baseline(basis, D, budget_s=25.0):
+    """Times the oracle (C++/OpenMP restatement of directScaffoldNew) on all
+    host cores: one warm-up build then as many builds as fit the budget."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ob = O.OracleBasis(basis)
+    ob.schwarz()
+    t0 = time.perf_counter()
+    J, K = ob.contract([D, D], [1, 1], [0, 1])
+    first = time.perf_counter() - t0
+    times = [first]
+    while sum(times) < budget_s and len(times) < 5:
+        t0 = time.perf_counter()
+        ob.contract([D, D], [1, 1], [0, 1])
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times[1:] if len(times) > 1 else times)
+    return dict(builds_per_s=1.0 / med, s_per_build=med, n=len(times),
+                cores=os.cpu_count(), G=2 * J - K)
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    import numpy as np
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    mol, bname, nocc, seed = workloads.config(args.workload)
+    basis = BasisSet.build(mol, bname)
+    ob = O.OracleBasis(basis)
+    S, _ = ob.overlap_kinetic()
+    D = workloads.occupied_density(S, nocc, seed)
+    ob.schwarz()
+    for _ in range(max(1, min(args.warmup, 1))):
+        ob.contract([D, D], [1, 1], [0, 1])
+    times = []
+    budget = 150.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ob.contract([D, D], [1, 1], [0, 1])
+        times.append(time.perf_counter() - t0)
+        if sum(times) > budget:
+            break
+    tot = sum(times)
+    v = len(times) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": v,
+            "unit": "builds/s", "n_gpus": ws, "steps": len(times),
+            "warmup": 1, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "nbasis": basis.nbasis,
+                       "l2": "inputs smaller than L2; host CPU arm"},
+            "cpu_baseline": {"value": v, "unit": "builds/s",
+                             "cores": os.cpu_count(), "kind": "port",
+                             "sample": "%d full builds of %s (C++/OpenMP "
+                                       "restatement of directScaffoldNew; "
+                                       "libint2/libcint unavailable)"
+                                       % (len(times), args.workload)},
+            "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local, pg = dist_init(args)
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+
+    from chronusq_public_b200 import flops as FL
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.contraction import (COULOMB, EXCHANGE, DirectTPI,
+                                                  GTODirectTPIContraction,
+                                                  TwoBodyContraction)
+    from chronusq_public_b200.fockbuilder import FockBuilder, two_electron_energy
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mol, bname, nocc, seed = workloads.config(args.workload)
+    basis = BasisSet.build(mol, bname)
+    tpi = DirectTPI(basis, device=local)
+    S, _ = tpi.one_electron()
+    D = workloads.occupied_density(S, nocc, seed)
+    N = basis.nbasis
+
+    def colmajor(a):
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).to(dev).t()
+
+    Dd = colmajor(D)
+    Jd = torch.zeros((N, N), dtype=torch.float64, device=dev).t().contiguous().t()
+    Kd = torch.zeros_like(Jd).t().contiguous().t()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    con = GTODirectTPIContraction(tpi)
+    stream = torch.cuda.current_stream(dev)
+
+    def run(precision, cut, steps, warmup, collect=False):
+        for _ in range(warmup):
+            Jd.zero_(); Kd.zero_()
+            con.twoBodyContract([TwoBodyContraction(Dd, Jd, True, COULOMB),
+                                 TwoBodyContraction(Dd, Kd, True, EXCHANGE)],
+                                precision=precision, fp32_cutoff=cut,
+                                stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        ms = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            Jd.zero_(); Kd.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            con.twoBodyContract([TwoBodyContraction(Dd, Jd, True, COULOMB),
+                                 TwoBodyContraction(Dd, Kd, True, EXCHANGE)],
+                                precision=precision, fp32_cutoff=cut,
+                                stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        G = (2 * Jd - Kd).t().contiguous().t().cpu().numpy()
+        return ms, G, dict(con.last_stats)
+
+    ms64, G64, st64 = run("fp64", 0.0, args.steps, args.warmup)
+    with ClockSampler(local) as clk:
+        msmx, Gmx, stmx = run("mixed", args.cutoff, args.steps, args.warmup)
+    clocks = clk.summary()
+
+    # end-to-end through the public API with host buffers
+    fb = FockBuilder(tpi)
+    for _ in range(args.warmup):
+        fb.formRawGD(D, precision="mixed", fp32_cutoff=args.cutoff)
+    torch.cuda.synchronize()
+    te = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fb.formRawGD(D, precision="mixed", fp32_cutoff=args.cutoff)
+        te.append(time.perf_counter() - t0)
+
+    def agg(x):
+        t = torch.tensor([sum(x)], dtype=torch.float64, device=dev)
+        if pg:
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    t64, tmx, te2e = agg(ms64) / 1e3, agg(msmx) / 1e3, agg(te)
+    K = args.steps
+    v64 = ws * K / t64
+    vmx = ws * K / tmx
+    ve2e = ws * K / te2e
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    # roofline: algorithmic FLOPs of one build (count model) over the
+    # measured FMA peaks
+    Q = tpi.schwarz()
+    fl = FL.build_flops(basis, Q, [D], nmat_digest=2, fp32_cut=args.cutoff)
+    p64, p32 = fma_peaks()
+    t_build = tmx / K
+    achieved = (fl["f64"] + fl["f32"]) / t_build / 1e12
+    frac = (fl["f64"] / (p64 * 1e12) + fl["f32"] / (p32 * 1e12)) / t_build
+    fl64 = FL.build_flops(basis, Q, [D], nmat_digest=2)
+    frac64 = (fl64["f64"] / (p64 * 1e12)) / (t64 / K)
+
+    cpu = None
+    err = {}
+    if not args.no_oracle:
+        cpu = cpu_baseline(basis, D)
+        Go = cpu["G"]
+        err = {"fock_maxabs_fp64": float(np.abs(G64 - Go).max()),
+               "fock_maxabs_mixed": float(np.abs(Gmx - Go).max()),
+               "energy_err_mixed": abs(two_electron_energy(Gmx, D)
+                                       - two_electron_energy(Go, D)),
+               "energy_err_fp64": abs(two_electron_energy(G64, D)
+                                      - two_electron_energy(Go, D))}
+    launches_per_step = 5 + 21  # norms/sym/max/to_cart x2, memset, 21 class launches, back x2
+    line = {
+        "metric": METRIC, "value": vmx, "unit": "builds/s", "n_gpus": ws,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+f32 (mixed)", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "nbasis": N,
+                   "nshell": basis.nshell, "npair": tpi.npair,
+                   "fp32_cutoff": args.cutoff, "parallelism": "replicas",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "fp64": {"value": v64, "unit": "builds/s", "ms_per_step": 1e3 * t64 / K,
+                 "roofline_frac": frac64},
+        "mixed_over_fp64": vmx / v64,
+        "latency_ms": {"p50": float(np.percentile(msmx, 50)),
+                       "p99": float(np.percentile(msmx, 99))},
+        "errors_vs_oracle": err,
+        "quartets": {"computed_fp32": stmx["fp32"], "computed_fp64": stmx["fp64"],
+                     "screened": stmx["screened"], "total": stmx["total"]},
+        "roofline": {"bound": "fp64+fp32 FMA (CUDA cores)", "achieved": achieved,
+                     "peak": {"fp64_tflops": p64, "fp32_tflops": p32,
+                              "source": "measured in this run (FMA microbenchmark)"},
+                     "unit": "TFLOP/s", "frac": frac,
+                     "gflop_per_build": {"f64": fl["f64"] / 1e9, "f32": fl["f32"] / 1e9},
+                     "traffic": None},
+        "e2e": {"value": ve2e, "unit": "builds/s",
+                "h2d_bytes_per_step": 8 * N * N,
+                "d2h_bytes_per_step": 2 * 8 * N * N},
+        "gpu_launches": launches_per_step * K,
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["builds_per_s"], "unit": "builds/s",
+                                "cores": cpu["cores"], "kind": "port",
+                                "sample": "%d full builds (1 warm-up) of %s, "
+                                          "C++/OpenMP restatement of "
+                                          "directScaffoldNew" % (cpu["n"], args.workload)}
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,99 @@
+"""ctypes binding of libcqfock.so (declarations in include/cqfock.h).
+
+The library is the only compute path: if it is missing or fails to load this
+module raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libcqfock.so")
+
+CQF_OK, CQF_EINVAL, CQF_ENOMEM, CQF_ECUDA, CQF_ENOTSUP, CQF_ETIMEDOUT, \
+    CQF_ENODEV = range(7)
+CQF_COULOMB, CQF_EXCHANGE = 0, 1
+CQF_FP64, CQF_MIXED = 0, 1
+
+# every entry point declared in include/cqfock.h
+EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
+           "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
+           "cqf_two_body_contract",
+           "cqf_last_error")
+
+
+class CqfShell(C.Structure):
+    _fields_ = [("l", C.c_int), ("pure", C.c_int), ("nprim", C.c_int),
+                ("alpha", C.POINTER(C.c_double)),
+                ("coeff", C.POINTER(C.c_double)),
+                ("origin", C.c_double * 3)]
+
+
+class CqfContraction(C.Structure):
+    _fields_ = [("X", C.c_void_p), ("AX", C.c_void_p),
+                ("hermitian", C.c_int), ("type", C.c_int)]
+
+
+class CqfOpts(C.Structure):
+    _fields_ = [("is_complex", C.c_int), ("screen", C.c_int),
+                ("device_pointers", C.c_int), ("precision", C.c_int),
+                ("fp32_cutoff", C.c_double), ("stream", C.c_void_p)]
+
+
+class CqfStats(C.Structure):
+    _fields_ = [("quartets_total", C.c_longlong),
+                ("quartets_screened", C.c_longlong),
+                ("quartets_fp32", C.c_longlong),
+                ("quartets_fp64", C.c_longlong),
+                ("device_ms", C.c_double)]
+
+
+class CqfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("cqfock error %d: %s" % (status, msg))
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load libcqfock.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "libcqfock.so not built (%s); run python -m "
+            "chronusq_public_b200.build" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    L.cqf_opts_default.argtypes = [C.POINTER(CqfOpts)]
+    L.cqf_opts_default.restype = None
+    L.cqf_basis_create.argtypes = [C.POINTER(CqfShell), C.c_int, C.c_double,
+                                   C.c_int, C.POINTER(C.c_void_p)]
+    L.cqf_basis_create.restype = C.c_int
+    L.cqf_basis_destroy.argtypes = [C.c_void_p]
+    L.cqf_basis_destroy.restype = C.c_int
+    L.cqf_basis_info.argtypes = [C.c_void_p, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.cqf_basis_info.restype = C.c_int
+    L.cqf_basis_schwarz.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.cqf_basis_schwarz.restype = C.c_int
+    L.cqf_basis_one_electron.argtypes = [C.c_void_p, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+    L.cqf_basis_one_electron.restype = C.c_int
+    L.cqf_two_body_contract.argtypes = [C.c_void_p, C.POINTER(CqfContraction),
+                                        C.c_int, C.POINTER(CqfOpts),
+                                        C.POINTER(CqfStats)]
+    L.cqf_two_body_contract.restype = C.c_int
+    L.cqf_last_error.argtypes = []
+    L.cqf_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != CQF_OK:
+        raise CqfError(status, lib().cqf_last_error().decode())
+    return status

@@ -1,0 +1,174 @@
+"""Host-side mirror of ChronusQ's direct two-body contraction interface.
+
+``TwoBodyContraction`` and ``GTODirectTPIContraction.twoBodyContract`` keep
+the names, argument meaning and accumulate semantics of
+``include/particleintegrals/twopints.hpp:59-75`` and
+``include/particleintegrals/twopints/gtodirecttpi.hpp:143-228``; the work is
+done by libcqfock.so on the GPU through the C ABI of include/cqfock.h.
+
+Matrices: N x N, column-major semantics (index [i, j] is row i, column j);
+numpy arrays (host, any order) or CUDA torch tensors (device pointers, must
+be Fortran-contiguous i.e. ``t.T.contiguous().T`` or symmetric use).  AX is
+accumulated (AX += G[X]), as on the reference's multi-threaded path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import _cabi
+from ._cabi import CQF_COULOMB, CQF_EXCHANGE  # noqa: F401
+from .basis import BasisSet
+
+COULOMB, EXCHANGE = CQF_COULOMB, CQF_EXCHANGE
+
+
+@dataclass
+class TwoBodyContraction:
+    """``TwoBodyContraction<T>``: AX += G[X] of type contType."""
+    X: object
+    AX: object
+    HER: bool = True
+    contType: int = COULOMB
+
+
+class DirectTPI:
+    """Device-resident shell pairs and Schwarz bounds of one basis
+    (``DirectTPI``, gtodirecttpi.hpp:30-141; threshSchwarz default 1e-12)."""
+
+    def __init__(self, basis: BasisSet, threshSchwarz: float = 1e-12,
+                 device: int = 0):
+        L = _cabi.lib()
+        self.basis = basis
+        self.threshSchwarz = threshSchwarz
+        self.device = device
+        f = basis.flat()
+        self._keep = f
+        sh = (_cabi.CqfShell * basis.nshell)()
+        off = 0
+        self._alpha = np.ascontiguousarray(f["alpha"], dtype=np.float64)
+        self._coef = np.ascontiguousarray(f["coef"], dtype=np.float64)
+        dp = C.POINTER(C.c_double)
+        for s in range(basis.nshell):
+            n = int(f["nprim"][s])
+            sh[s].l = int(f["l"][s])
+            sh[s].pure = int(f["pure"][s])
+            sh[s].nprim = n
+            sh[s].alpha = C.cast(self._alpha.ctypes.data + 8 * off, dp)
+            sh[s].coeff = C.cast(self._coef.ctypes.data + 8 * off, dp)
+            for x in range(3):
+                sh[s].origin[x] = float(f["origin"][s, x])
+            off += n
+        h = C.c_void_p()
+        _cabi.check(L.cqf_basis_create(sh, basis.nshell, threshSchwarz, device,
+                                       C.byref(h)))
+        self.handle = h
+        nb, ns, npair = C.c_int(), C.c_int(), C.c_int()
+        _cabi.check(L.cqf_basis_info(h, C.byref(nb), C.byref(ns),
+                                     C.byref(npair)))
+        self.nbasis, self.nshell, self.npair = nb.value, ns.value, npair.value
+
+    def schwarz(self) -> np.ndarray:
+        Q = np.zeros((self.nshell, self.nshell), order="F")
+        _cabi.check(_cabi.lib().cqf_basis_schwarz(
+            self.handle, Q.ctypes.data_as(C.POINTER(C.c_double))))
+        return Q
+
+    def one_electron(self):
+        """(S, T): overlap and kinetic matrices, computed on the device."""
+        N = self.nbasis
+        S = np.zeros((N, N), order="F")
+        T = np.zeros((N, N), order="F")
+        dp = C.POINTER(C.c_double)
+        _cabi.check(_cabi.lib().cqf_basis_one_electron(
+            self.handle, S.ctypes.data_as(dp), T.ctypes.data_as(dp)))
+        return S, T
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _cabi.lib().cqf_basis_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+class GTODirectTPIContraction:
+    """``GTODirectTPIContraction<MatsT,double>`` on the GPU."""
+
+    def __init__(self, tpi: DirectTPI):
+        self.tpi = tpi
+        self.last_stats: Optional[dict] = None
+
+    def twoBodyContract(self, matList: List[TwoBodyContraction],
+                        screen: bool = True, precision: str = "fp64",
+                        fp32_cutoff: float = 0.0, stream=None) -> None:
+        """AX += G[X] for every entry (directScaffoldNew semantics)."""
+        if not matList:
+            return
+        N = self.tpi.nbasis
+        dev = _is_torch(matList[0].X)
+        is_c = any((x.X.is_complex() if _is_torch(x.X) else np.iscomplexobj(x.X))
+                   for x in matList)
+        n = len(matList)
+        arr = (_cabi.CqfContraction * n)()
+        keep = []
+        writeback = []
+        for i, c in enumerate(matList):
+            if dev:
+                for t in (c.X, c.AX):
+                    if tuple(t.shape) != (N, N):
+                        raise ValueError("matrix shape must be (N, N)")
+                    if not t.is_cuda:
+                        raise ValueError("mixing host and device matrices")
+                    if t.stride() != (1, N):
+                        raise ValueError("device matrices must be column-major"
+                                         " (stride (1, N))")
+                arr[i].X = C.c_void_p(c.X.data_ptr())
+                arr[i].AX = C.c_void_p(c.AX.data_ptr())
+            else:
+                dt = np.complex128 if is_c else np.float64
+                X = np.asfortranarray(c.X, dtype=dt)
+                if X.shape != (N, N):
+                    raise ValueError("matrix shape must be (N, N)")
+                if not (isinstance(c.AX, np.ndarray) and c.AX.dtype == dt
+                        and c.AX.flags.f_contiguous and c.AX.shape == (N, N)):
+                    AX = np.asfortranarray(c.AX, dtype=dt)
+                    writeback.append((c, AX))
+                else:
+                    AX = c.AX
+                keep += [X, AX]
+                arr[i].X = C.c_void_p(X.ctypes.data)
+                arr[i].AX = C.c_void_p(AX.ctypes.data)
+            arr[i].hermitian = 1 if c.HER else 0
+            arr[i].type = int(c.contType)
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.is_complex = 1 if is_c else 0
+        opts.screen = 1 if screen else 0
+        opts.device_pointers = 1 if dev else 0
+        opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
+        opts.fp32_cutoff = float(fp32_cutoff)
+        opts.stream = C.c_void_p(stream) if stream else None
+        st = _cabi.CqfStats()
+        _cabi.check(_cabi.lib().cqf_two_body_contract(
+            self.tpi.handle, arr, n, C.byref(opts), C.byref(st)))
+        for c, AX in writeback:
+            if isinstance(c.AX, np.ndarray):
+                c.AX[...] = AX
+            else:
+                c.AX = AX
+        self.last_stats = dict(total=st.quartets_total,
+                               screened=st.quartets_screened,
+                               fp32=st.quartets_fp32, fp64=st.quartets_fp64,
+                               device_ms=st.device_ms)

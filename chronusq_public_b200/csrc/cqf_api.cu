@@ -1,0 +1,837 @@
+// C ABI of the direct J/K build: basis set-up on the device and the
+// contraction driver (GTODirectTPIContraction::twoBodyContract replacement).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cqf_internal.hpp"
+#include "cqf_jk_kernels.cuh"
+
+using namespace cqf;
+
+namespace {
+
+thread_local std::string g_err;
+
+cqf_status fail(cqf_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CQF_CUDA(call)                                                                 \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? CQF_ENOMEM : CQF_ECUDA,            \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+  } while (0)
+
+#define CQF_TRY(expr)              \
+  do {                             \
+    cqf_status s_ = (expr);        \
+    if (s_ != CQF_OK) return s_;   \
+  } while (0)
+
+// ------------------------------------------------------------ host tables
+// Boys table F_m(j*DT), m = 0..BOYS_MMAX, by the convergent series in long
+// double followed by downward recursion (the table scheme of
+// RealGTOIntEngine::generateFmTTable, src/particleintegrals/aointegrals/
+// aointegrals_onee_inhouse.cxx:79-116, with a tighter series tolerance).
+void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
+  const int M = BOYS_MMAX;
+  t64.assign((size_t)BOYS_NPTS * (M + 1), 0.0);
+  t32.assign((size_t)BOYS_NPTS * (M + 1), 0.0f);
+  for (int j = 0; j < BOYS_NPTS; j++) {
+    long double T = (long double)j * BOYS_DT;
+    long double term = 1.0L / (2 * M + 1), sum = term;
+    for (int k = 1; k < 10000; k++) {
+      term *= 2.0L * T / (2 * M + 2 * k + 1);
+      sum += term;
+      if (term < sum * 1e-21L) break;
+    }
+    long double eT = expl(-T), F = eT * sum;
+    std::vector<long double> col(M + 1);
+    col[M] = F;
+    for (int m = M - 1; m >= 0; m--) col[m] = (2.0L * T * col[m + 1] + eT) / (2 * m + 1);
+    for (int m = 0; m <= M; m++) {
+      t64[(size_t)j * (M + 1) + m] = (double)col[m];
+      t32[(size_t)j * (M + 1) + m] = (float)col[m];
+    }
+  }
+}
+
+double fact(int n) {
+  double r = 1;
+  for (int i = 2; i <= n; i++) r *= i;
+  return r;
+}
+double binom(int n, int k) {
+  if (k < 0 || k > n) return 0.0;
+  double r = 1;
+  for (int i = 1; i <= k; i++) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Real solid harmonics over Cartesian components (Helgaker, Jorgensen &
+// Olsen eq. 6.4.47-6.4.50), m = -l..l; T[ic * (2l+1) + (m+l)].
+std::vector<double> solid_harmonics(int l) {
+  int nc = ncart(l), ns = 2 * l + 1;
+  std::vector<double> T(nc * ns, 0.0);
+  for (int m = -l; m <= l; m++) {
+    int am = std::abs(m), vm2 = (m >= 0) ? 0 : 1;
+    double N = 1.0 / (std::pow(2.0, am) * fact(l)) *
+               std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
+    for (int t = 0; t <= (l - am) / 2; t++)
+      for (int u = 0; u <= t; u++) {
+        int vmax2 = 2 * (int)std::floor(am / 2.0 - vm2 / 2.0) + vm2;
+        for (int v2 = vm2; v2 <= vmax2; v2 += 2) {
+          int sg = t + (v2 - vm2) / 2;
+          double C = ((sg % 2) ? -1.0 : 1.0) * std::pow(0.25, t) * binom(l, t) *
+                     binom(l - t, am + t) * binom(t, u) * binom(am, v2);
+          int ex = 2 * t + am - (2 * u + v2), ey = 2 * u + v2, ez = l - 2 * t - am;
+          for (int i = 0; i < nc; i++)
+            if (cart_lx(l, i) == ex && cart_ly(l, i) == ey && cart_lz(l, i) == ez)
+              T[i * ns + (m + l)] += N * C;
+        }
+      }
+  }
+  return T;
+}
+
+// ------------------------------------------------------------ set-up kernels
+// Cartesian overlap and kinetic blocks of two contracted shells from the 1D
+// Hermite coefficients E^{ij}_0 (McMurchie-Davidson); kinetic by
+// T_ij = -2b^2 S_{i,j+2} + b(2j+1) S_{ij} - j(j-1)/2 S_{i,j-2} per axis.
+__device__ void shell_pair_1e(const ShellDev& A, const ShellDev& B, const double* __restrict__ prim,
+                              int nprimTot, double (*S)[ncart(LMAX)], double (*T)[ncart(LMAX)]) {
+  double AB2 = 0.0;
+  for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+  const int na = ncart(A.l), nb = ncart(B.l);
+  for (int i = 0; i < na; i++)
+    for (int j = 0; j < nb; j++) {
+      S[i][j] = 0.0;
+      if (T) T[i][j] = 0.0;
+    }
+  const int lb2 = B.l + 2;
+  for (int ia = 0; ia < A.nprim; ia++)
+    for (int jb = 0; jb < B.nprim; jb++) {
+      const double a = prim[A.prim_off + ia], b = prim[B.prim_off + jb];
+      const double ca = prim[nprimTot + A.prim_off + ia], cb = prim[nprimTot + B.prim_off + jb];
+      const double p = a + b, mu = a * b / p;
+      const double K = ca * cb * exp(-mu * AB2) * pow(M_PI / p, 1.5);
+      double s1d[3][LMAX + 1][LMAX + 3];
+      for (int x = 0; x < 3; x++) {
+        const double P = (a * A.O[x] + b * B.O[x]) / p;
+        const double PA = P - A.O[x], PB = P - B.O[x], o2p = 0.5 / p;
+        double E[LMAX + 1][LMAX + 3][2 * LMAX + 3];
+        for (int i = 0; i <= A.l; i++)
+          for (int j = 0; j <= lb2; j++)
+            for (int t = 0; t <= i + j; t++) E[i][j][t] = 0.0;
+        E[0][0][0] = 1.0;
+        for (int i = 0; i <= A.l; i++)
+          for (int j = 0; j <= lb2; j++) {
+            if (i == 0 && j == 0) continue;
+            const bool up = (j == 0);
+            const int pi = up ? i - 1 : i, pj = up ? j : j - 1, top = pi + pj;
+            const double X = up ? PA : PB;
+            for (int t = 0; t <= i + j; t++) {
+              double v = (t <= top) ? X * E[pi][pj][t] : 0.0;
+              if (t > 0) v += o2p * E[pi][pj][t - 1];
+              if (t + 1 <= top) v += (t + 1) * E[pi][pj][t + 1];
+              E[i][j][t] = v;
+            }
+          }
+        for (int i = 0; i <= A.l; i++)
+          for (int j = 0; j <= lb2; j++) s1d[x][i][j] = E[i][j][0];
+      }
+      for (int u = 0; u < na; u++)
+        for (int v = 0; v < nb; v++) {
+          const int ia3[3] = {cart_lx(A.l, u), cart_ly(A.l, u), cart_lz(A.l, u)};
+          const int jb3[3] = {cart_lx(B.l, v), cart_ly(B.l, v), cart_lz(B.l, v)};
+          double s[3], t[3];
+          for (int x = 0; x < 3; x++) {
+            const int i = ia3[x], j = jb3[x];
+            s[x] = s1d[x][i][j];
+            t[x] = -2.0 * b * b * s1d[x][i][j + 2] + b * (2 * j + 1) * s1d[x][i][j] -
+                   (j >= 2 ? 0.5 * j * (j - 1) * s1d[x][i][j - 2] : 0.0);
+          }
+          S[u][v] += K * s[0] * s[1] * s[2];
+          if (T) T[u][v] += K * (t[0] * s[1] * s[2] + s[0] * t[1] * s[2] + s[0] * s[1] * t[2]);
+        }
+    }
+}
+
+// Spherical (where pure) element (mu, nu) of a Cartesian block.
+__device__ double sph_elem(const ShellDev& A, const ShellDev& B, const double* __restrict__ sph,
+                           const int* __restrict__ sphOff, double (*M)[ncart(LMAX)], int mu,
+                           int nu) {
+  const int na = ncart(A.l), nb = ncart(B.l);
+  const double* TA = sph + sphOff[A.l];
+  const double* TB = sph + sphOff[B.l];
+  double s = 0.0;
+  for (int u = 0; u < na; u++) {
+    const double ta = A.pure ? TA[u * nsph(A.l) + mu] : (u == mu);
+    if (ta == 0.0) continue;
+    for (int v = 0; v < nb; v++) {
+      const double tb = B.pure ? TB[v * nsph(B.l) + nu] : (v == nu);
+      s += ta * tb * M[u][v];
+    }
+  }
+  return s;
+}
+
+// Significant shell pairs: same centre (1e-5 Bohr per coordinate), or the
+// 2-norm of the overlap block >= 1e-12 (basisset.cxx:146-156, :652-706).
+__global__ void sig_pairs_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
+                                 const double* __restrict__ sph, const int* __restrict__ sphOff,
+                                 int nshell, int nprimTot, unsigned char* flags) {
+  long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long npair = (long long)nshell * (nshell + 1) / 2;
+  if (k >= npair) return;
+  int s1 = (int)((sqrt(8.0 * k + 1.0) - 1.0) / 2.0);
+  while ((long long)s1 * (s1 + 1) / 2 > k) s1--;
+  while ((long long)(s1 + 1) * (s1 + 2) / 2 <= k) s1++;
+  int s2 = (int)(k - (long long)s1 * (s1 + 1) / 2);
+  const ShellDev A = sh[s1], B = sh[s2];
+  bool same = fabs(A.O[0] - B.O[0]) < 1e-5 && fabs(A.O[1] - B.O[1]) < 1e-5 &&
+              fabs(A.O[2] - B.O[2]) < 1e-5;
+  if (same) { flags[k] = 1; return; }
+  double S[ncart(LMAX)][ncart(LMAX)];
+  shell_pair_1e(A, B, prim, nprimTot, S, nullptr);
+  const int ma = A.pure ? nsph(A.l) : ncart(A.l), mb = B.pure ? nsph(B.l) : ncart(B.l);
+  double n2 = 0.0;
+  for (int mu = 0; mu < ma; mu++)
+    for (int nu = 0; nu < mb; nu++) {
+      const double s = sph_elem(A, B, sph, sphOff, S, mu, nu);
+      n2 += s * s;
+    }
+  flags[k] = sqrt(n2) >= 1e-12 ? 1 : 0;
+}
+
+// Full overlap and kinetic matrices (column-major N x N), one thread per
+// shell pair block.
+__global__ void one_electron_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
+                                    const double* __restrict__ sph, const int* __restrict__ sphOff,
+                                    int nshell, int nprimTot, int N, double* Smat, double* Tmat) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nshell * nshell) return;
+  const int s1 = k % nshell, s2 = k / nshell;
+  const ShellDev A = sh[s1], B = sh[s2];
+  double S[ncart(LMAX)][ncart(LMAX)], T[ncart(LMAX)][ncart(LMAX)];
+  shell_pair_1e(A, B, prim, nprimTot, S, T);
+  const int ma = A.pure ? nsph(A.l) : ncart(A.l), mb = B.pure ? nsph(B.l) : ncart(B.l);
+  for (int mu = 0; mu < ma; mu++)
+    for (int nu = 0; nu < mb; nu++) {
+      const size_t e = (size_t)(A.sph_off + mu) + (size_t)(B.sph_off + nu) * N;
+      Smat[e] = sph_elem(A, B, sph, sphOff, S, mu, nu);
+      Tmat[e] = sph_elem(A, B, sph, sphOff, T, mu, nu);
+    }
+}
+
+__global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
+                                  int nprimTot, const PairDev* __restrict__ pairs, int npair,
+                                  PrimPairDev* pp) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npair) return;
+  const PairDev P = pairs[k];
+  const ShellDev A = sh[P.shA], B = sh[P.shB];
+  double AB2 = 0.0;
+  for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+  int idx = P.pp_off;
+  for (int ia = 0; ia < A.nprim; ia++)
+    for (int jb = 0; jb < B.nprim; jb++, idx++) {
+      double a = prim[A.prim_off + ia], b = prim[B.prim_off + jb];
+      double ca = prim[nprimTot + A.prim_off + ia], cb = prim[nprimTot + B.prim_off + jb];
+      PrimPairDev r;
+      r.p = a + b;
+      r.K = ca * cb * exp(-a * b / r.p * AB2);
+      for (int x = 0; x < 3; x++) {
+        r.P[x] = (a * A.O[x] + b * B.O[x]) / r.p;
+        r.PA[x] = r.P[x] - A.O[x];
+        r.PB[x] = r.P[x] - B.O[x];
+      }
+      r.pad = 0.0;
+      pp[idx] = r;
+    }
+}
+
+__global__ void sort_keys_kernel(const PairDev* pairs, int n, unsigned long long* keys, int* vals) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  unsigned long long qb = (unsigned long long)__double_as_longlong(pairs[k].Q);  // Q >= 0
+  keys[k] = ((unsigned long long)pairs[k].cls << 56) | ((~qb >> 8) & ((1ull << 56) - 1));
+  vals[k] = k;
+}
+
+__global__ void gather_pairs_kernel(const PairDev* in, const int* idx, int n, PairDev* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = in[idx[k]];
+}
+
+// ------------------------------------------------------------ build kernels
+// Shell-block infinity norms (ShellBlockNorm, direct.hpp:73-90): one thread
+// per (s1, s2) block, max over rows of the absolute row sums.
+__global__ void block_norms_kernel(const double* __restrict__ X, int cplx, int N,
+                                   const ShellDev* __restrict__ sh, int ns, double* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns * ns) return;
+  int s1 = k % ns, s2 = k / ns;
+  const ShellDev A = sh[s1], B = sh[s2];
+  int n1 = A.pure ? nsph(A.l) : ncart(A.l), n2 = B.pure ? nsph(B.l) : ncart(B.l);
+  double mx = 0.0;
+  for (int i = 0; i < n1; i++) {
+    double r = 0.0;
+    for (int j = 0; j < n2; j++) {
+      size_t e = (size_t)(A.sph_off + i) + (size_t)(B.sph_off + j) * N;
+      r += cplx ? hypot(X[2 * e], X[2 * e + 1]) : fabs(X[e]);
+    }
+    mx = fmax(mx, r);
+  }
+  out[k] = mx;
+}
+
+// symmetrise the norms of non-Hermitian matrices (direct.hpp:1533-1542)
+__global__ void sym_norms_kernel(double* nm, int ns) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns * ns) return;
+  int a = k % ns, b = k / ns;
+  if (a <= b) return;
+  double m = fmax(nm[a + (size_t)b * ns], nm[b + (size_t)a * ns]);
+  nm[a + (size_t)b * ns] = m;
+  nm[b + (size_t)a * ns] = m;
+}
+
+__global__ void max_norms_kernel(const double* __restrict__ nm, int nMat, size_t ns2,
+                                 double* out, unsigned long long* gmax) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (k < ns2) {
+    for (int i = 0; i < nMat; i++) m = fmax(m, nm[i * ns2 + k]);
+    out[k] = m;
+  }
+  // block max, then one atomic (non-negative doubles order as their bits)
+  __shared__ double red[256];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    atomicMax(gmax, (unsigned long long)__double_as_longlong(red[0]));
+}
+
+// Xc = T X T^T per matrix (T: block-diagonal Cartesian -> AO transform).
+__global__ void to_cart_kernel(const double* __restrict__ X, int cplx, int N, int nc,
+                               const ShellDev* __restrict__ sh, const int* __restrict__ c2s,
+                               const double* __restrict__ sph, const int* __restrict__ sphOff,
+                               double* Xc) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)nc * nc) return;
+  int ci = (int)(k % nc), cj = (int)(k / nc);
+  const ShellDev A = sh[c2s[ci]], B = sh[c2s[cj]];
+  int a = ci - A.cart_off, b = cj - B.cart_off;
+  int na = A.pure ? nsph(A.l) : ncart(A.l), nb = B.pure ? nsph(B.l) : ncart(B.l);
+  const double* TA = sph + sphOff[A.l];
+  const double* TB = sph + sphOff[B.l];
+  double re = 0.0, im = 0.0;
+  for (int mu = 0; mu < na; mu++) {
+    double ta = A.pure ? TA[a * nsph(A.l) + mu] : (a == mu);
+    if (ta == 0.0) continue;
+    for (int nu = 0; nu < nb; nu++) {
+      double tb = B.pure ? TB[b * nsph(B.l) + nu] : (b == nu);
+      if (tb == 0.0) continue;
+      size_t e = (size_t)(A.sph_off + mu) + (size_t)(B.sph_off + nu) * N;
+      if (cplx) {
+        re += ta * tb * X[2 * e];
+        im += ta * tb * X[2 * e + 1];
+      } else {
+        re += ta * tb * X[e];
+      }
+    }
+  }
+  if (cplx) {
+    Xc[2 * k] = re;
+    Xc[2 * k + 1] = im;
+  } else {
+    Xc[k] = re;
+  }
+}
+
+// AX += 1/2 (B + B^H) (Hermitian) or AX += 1/2 B, B = T^T Ac T
+// (direct.hpp:2036-2066).
+__global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int her, int N, int nc,
+                                 const ShellDev* __restrict__ sh, const int* __restrict__ ao2s,
+                                 const double* __restrict__ sph, const int* __restrict__ sphOff,
+                                 double* AX) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)N * N) return;
+  int i = (int)(k % N), j = (int)(k / N);
+  auto bval = [&](int r, int c, double& bre, double& bim) {
+    const ShellDev A = sh[ao2s[r]], B = sh[ao2s[c]];
+    int mu = r - A.sph_off, nu = c - B.sph_off;
+    int na = ncart(A.l), nb = ncart(B.l);
+    const double* TA = sph + sphOff[A.l];
+    const double* TB = sph + sphOff[B.l];
+    bre = 0.0;
+    bim = 0.0;
+    for (int a = 0; a < na; a++) {
+      double ta = A.pure ? TA[a * nsph(A.l) + mu] : (a == mu);
+      if (ta == 0.0) continue;
+      for (int b = 0; b < nb; b++) {
+        double tb = B.pure ? TB[b * nsph(B.l) + nu] : (b == nu);
+        if (tb == 0.0) continue;
+        size_t e = (size_t)(A.cart_off + a) + (size_t)(B.cart_off + b) * nc;
+        if (cplx) {
+          bre += ta * tb * Ac[2 * e];
+          bim += ta * tb * Ac[2 * e + 1];
+        } else {
+          bre += ta * tb * Ac[e];
+        }
+      }
+    }
+  };
+  double r1, i1;
+  bval(i, j, r1, i1);
+  double outr, outi;
+  if (her) {
+    double r2, i2;
+    bval(j, i, r2, i2);
+    outr = 0.5 * (r1 + r2);
+    outi = 0.5 * (i1 - i2);
+  } else {
+    outr = 0.5 * r1;
+    outi = 0.5 * i1;
+  }
+  if (cplx) {
+    AX[2 * k] += outr;
+    AX[2 * k + 1] += outi;
+  } else {
+    AX[k] += outr;
+  }
+}
+
+unsigned grid1(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+cqf_status ensure_ws(cqf_basis* B, size_t bytes) {
+  if (bytes <= B->ws_bytes) return CQF_OK;
+  if (B->d_ws) CQF_CUDA(cudaFree(B->d_ws));
+  B->d_ws = nullptr;
+  B->ws_bytes = 0;
+  CQF_CUDA(cudaMalloc(&B->d_ws, bytes));
+  B->ws_bytes = bytes;
+  return CQF_OK;
+}
+
+void free_basis(cqf_basis* B) {
+  if (!B) return;
+  cudaSetDevice(B->device);
+  cudaFree(B->d_shells);
+  cudaFree(B->d_prim);
+  cudaFree(B->d_pairs);
+  cudaFree(B->d_pp);
+  cudaFree(B->d_boys64);
+  cudaFree(B->d_boys32);
+  cudaFree(B->d_schwarz);
+  cudaFree(B->d_sph);
+  cudaFree(B->d_sphOff);
+  cudaFree(B->d_ao2shell);
+  cudaFree(B->d_cart2shell);
+  cudaFree(B->d_ws);
+  cudaFree(B->d_counters);
+  cudaFree(B->d_flags);
+  if (B->ev0) cudaEventDestroy(B->ev0);
+  if (B->ev1) cudaEventDestroy(B->ev1);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
+}
+
+template <typename T>
+cqf_status upload(T** dst, const std::vector<T>& src) {
+  CQF_CUDA(cudaMalloc((void**)dst, std::max<size_t>(1, src.size()) * sizeof(T)));
+  if (!src.empty())
+    CQF_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return CQF_OK;
+}
+
+cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int device,
+                        cqf_basis* B) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(CQF_ENODEV, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(CQF_EINVAL, "bad device ordinal");
+  B->device = device;
+  CQF_CUDA(cudaSetDevice(device));
+  CQF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+  CQF_CUDA(cudaEventCreate(&B->ev0));
+  CQF_CUDA(cudaEventCreate(&B->ev1));
+  B->thresh = thresh;
+  B->nshell = nshell;
+
+  // shells, primitive data
+  std::vector<double> alpha, coef;
+  int sphOff = 0, cartOff = 0;
+  for (int s = 0; s < nshell; s++) {
+    const cqf_shell& c = shells[s];
+    if (c.l < 0 || c.l > LMAX) return fail(CQF_EINVAL, "shell angular momentum above LMAX");
+    if (c.nprim <= 0 || !c.alpha || !c.coeff) return fail(CQF_EINVAL, "empty shell");
+    ShellDev d{};
+    d.l = c.l;
+    d.pure = c.pure ? 1 : 0;
+    d.nprim = c.nprim;
+    d.prim_off = (int)alpha.size();
+    d.cart_off = cartOff;
+    d.sph_off = sphOff;
+    for (int x = 0; x < 3; x++) d.O[x] = c.origin[x];
+    for (int i = 0; i < c.nprim; i++) {
+      alpha.push_back(c.alpha[i]);
+      coef.push_back(c.coeff[i]);
+    }
+    sphOff += d.pure ? nsph(d.l) : ncart(d.l);
+    cartOff += ncart(d.l);
+    B->maxL = std::max(B->maxL, d.l);
+    B->maxPrim = std::max(B->maxPrim, d.nprim);
+    B->h_shells.push_back(d);
+  }
+  B->nbasis = sphOff;
+  B->ncart = cartOff;
+  const int nprimTot = (int)alpha.size();
+  std::vector<double> prim(alpha);
+  prim.insert(prim.end(), coef.begin(), coef.end());
+  CQF_TRY(upload(&B->d_shells, B->h_shells));
+  CQF_TRY(upload(&B->d_prim, prim));
+
+  std::vector<int> ao2s, c2s;
+  for (int s = 0; s < nshell; s++) {
+    const ShellDev& d = B->h_shells[s];
+    for (int i = 0; i < (d.pure ? nsph(d.l) : ncart(d.l)); i++) ao2s.push_back(s);
+    for (int i = 0; i < ncart(d.l); i++) c2s.push_back(s);
+  }
+  CQF_TRY(upload(&B->d_ao2shell, ao2s));
+  CQF_TRY(upload(&B->d_cart2shell, c2s));
+
+  std::vector<double> sph;
+  std::vector<int> sphO;
+  for (int l = 0; l <= LMAX; l++) {
+    sphO.push_back((int)sph.size());
+    auto T = solid_harmonics(l);
+    sph.insert(sph.end(), T.begin(), T.end());
+  }
+  CQF_TRY(upload(&B->d_sph, sph));
+  CQF_TRY(upload(&B->d_sphOff, sphO));
+
+  std::vector<double> b64;
+  std::vector<float> b32;
+  make_boys_table(b64, b32);
+  CQF_TRY(upload(&B->d_boys64, b64));
+  CQF_TRY(upload(&B->d_boys32, b32));
+
+  // significant pairs on the device
+  long long nlt = (long long)nshell * (nshell + 1) / 2;
+  unsigned char* d_flags8 = nullptr;
+  CQF_CUDA(cudaMalloc(&d_flags8, std::max<long long>(1, nlt)));
+  sig_pairs_kernel<<<grid1(nlt, 128), 128, 0, B->stream>>>(B->d_shells, B->d_prim, B->d_sph,
+                                                           B->d_sphOff, nshell, nprimTot, d_flags8);
+  std::vector<unsigned char> f8(nlt);
+  CQF_CUDA(cudaMemcpyAsync(f8.data(), d_flags8, nlt, cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  cudaFree(d_flags8);
+
+  // pair list in the reference loop order, then grouped by class (stable)
+  std::vector<PairDev> lexPairs;
+  for (int s1 = 0, k = 0; s1 < nshell; s1++)
+    for (int s2 = 0; s2 <= s1; s2++, k++) {
+      if (!f8[k]) continue;
+      PairDev p{};
+      p.s1 = s1;
+      p.s2 = s2;
+      const ShellDev &A = B->h_shells[s1], &Bs = B->h_shells[s2];
+      if (A.l >= Bs.l) { p.shA = s1; p.shB = s2; }
+      else { p.shA = s2; p.shB = s1; }
+      p.cA = B->h_shells[p.shA].cart_off;
+      p.cB = B->h_shells[p.shB].cart_off;
+      p.lex = (int)lexPairs.size();
+      p.cls = class_id(B->h_shells[p.shA].l, B->h_shells[p.shB].l);
+      p.npp = B->h_shells[p.shA].nprim * B->h_shells[p.shB].nprim;
+      lexPairs.push_back(p);
+    }
+  std::vector<PairDev> pairs;
+  for (int c = 0; c < NCLS; c++) {
+    B->cls_beg[c] = (int)pairs.size();
+    for (auto& p : lexPairs)
+      if (p.cls == c) pairs.push_back(p);
+    B->cls_cnt[c] = (int)pairs.size() - B->cls_beg[c];
+  }
+  long long ppoff = 0;
+  for (auto& p : pairs) {
+    p.pp_off = (int)ppoff;
+    ppoff += p.npp;
+  }
+  B->npair = (int)pairs.size();
+  B->nprimpair = ppoff;
+  PairDev* d_tmp = nullptr;
+  CQF_TRY(upload(&d_tmp, pairs));
+  CQF_CUDA(cudaMalloc(&B->d_pp, std::max<long long>(1, ppoff) * sizeof(PrimPairDev)));
+  prim_pairs_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_shells, B->d_prim, nprimTot,
+                                                                 d_tmp, B->npair, B->d_pp);
+  CQF_CUDA(cudaMalloc(&B->d_schwarz, (size_t)nshell * nshell * sizeof(double)));
+  CQF_CUDA(cudaMemsetAsync(B->d_schwarz, 0, (size_t)nshell * nshell * sizeof(double), B->stream));
+  for (int c = 0; c < NCLS; c++)
+    if (B->cls_cnt[c] > 0)
+      schwarz_kernel<<<grid1(B->cls_cnt[c], 64), 64, 0, B->stream>>>(
+          d_tmp, B->d_pp, B->d_boys64, B->d_sph, B->d_sphOff, B->d_shells, B->cls_beg[c],
+          B->cls_cnt[c], nshell, B->d_schwarz, d_tmp);
+  CQF_CUDA(cudaGetLastError());
+
+  // sort each class by Schwarz bound, descending (stable: ties stay in
+  // reference loop order)
+  unsigned long long *kin = nullptr, *kout = nullptr;
+  int *vin = nullptr, *vout = nullptr;
+  int n = std::max(1, B->npair);
+  CQF_CUDA(cudaMalloc(&kin, n * sizeof(unsigned long long)));
+  CQF_CUDA(cudaMalloc(&kout, n * sizeof(unsigned long long)));
+  CQF_CUDA(cudaMalloc(&vin, n * sizeof(int)));
+  CQF_CUDA(cudaMalloc(&vout, n * sizeof(int)));
+  sort_keys_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(d_tmp, B->npair, kin, vin);
+  size_t tmpBytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, kin, kout, vin, vout, B->npair, 0, 64,
+                                  B->stream);
+  void* d_cub = nullptr;
+  CQF_CUDA(cudaMalloc(&d_cub, std::max<size_t>(1, tmpBytes)));
+  CQF_CUDA(cub::DeviceRadixSort::SortPairs(d_cub, tmpBytes, kin, kout, vin, vout, B->npair, 0,
+                                           64, B->stream));
+  CQF_CUDA(cudaMalloc(&B->d_pairs, n * sizeof(PairDev)));
+  gather_pairs_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(d_tmp, vout, B->npair,
+                                                                   B->d_pairs);
+  CQF_CUDA(cudaGetLastError());
+  B->h_pairs.resize(B->npair);
+  CQF_CUDA(cudaMemcpyAsync(B->h_pairs.data(), B->d_pairs, B->npair * sizeof(PairDev),
+                           cudaMemcpyDeviceToHost, B->stream));
+  B->h_schwarz.resize((size_t)nshell * nshell);
+  CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
+                           (size_t)nshell * nshell * sizeof(double), cudaMemcpyDeviceToHost,
+                           B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  cudaFree(kin);
+  cudaFree(kout);
+  cudaFree(vin);
+  cudaFree(vout);
+  cudaFree(d_cub);
+  cudaFree(d_tmp);
+  CQF_CUDA(cudaMalloc(&B->d_counters, 8 * sizeof(unsigned long long)));
+  CQF_CUDA(cudaMalloc(&B->d_flags, MAXMAT * sizeof(int)));
+  return CQF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cqf_opts_default(cqf_opts* o) {
+  if (!o) return;
+  o->is_complex = 0;
+  o->screen = 1;
+  o->device_pointers = 0;
+  o->precision = CQF_FP64;
+  o->fp32_cutoff = 0.0;
+  o->stream = nullptr;
+}
+
+const char* cqf_last_error(void) { return g_err.c_str(); }
+
+cqf_status cqf_basis_create(const cqf_shell* shells, int nshell, double thresh_schwarz,
+                            int device, cqf_basis** out) {
+  g_err.clear();
+  if (!out || !shells || nshell <= 0) return fail(CQF_EINVAL, "cqf_basis_create: bad argument");
+  *out = nullptr;
+  auto* B = new cqf_basis();
+  cqf_status s = basis_create(shells, nshell, thresh_schwarz, device, B);
+  if (s != CQF_OK) {
+    std::string keep = g_err;
+    free_basis(B);
+    g_err = keep;
+    return s;
+  }
+  *out = B;
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_destroy(cqf_basis* basis) {
+  free_basis(basis);
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_info(const cqf_basis* B, int* nbasis, int* nshell, int* npair) {
+  if (!B) return fail(CQF_EINVAL, "null basis");
+  if (nbasis) *nbasis = B->nbasis;
+  if (nshell) *nshell = B->nshell;
+  if (npair) *npair = B->npair;
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_schwarz(const cqf_basis* B, double* Q) {
+  if (!B || !Q) return fail(CQF_EINVAL, "null argument");
+  std::copy(B->h_schwarz.begin(), B->h_schwarz.end(), Q);
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_one_electron(cqf_basis* B, double* S, double* T) {
+  g_err.clear();
+  if (!B || !S || !T) return fail(CQF_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  CQF_TRY(ensure_ws(B, 2 * NN * sizeof(double)));
+  double* d = static_cast<double*>(B->d_ws);
+  int nprimTot = 0;
+  for (auto& sh : B->h_shells) nprimTot += sh.nprim;
+  one_electron_kernel<<<grid1((size_t)B->nshell * B->nshell, 64), 64, 0, B->stream>>>(
+      B->d_shells, B->d_prim, B->d_sph, B->d_sphOff, B->nshell, nprimTot, B->nbasis, d, d + NN);
+  CQF_CUDA(cudaGetLastError());
+  CQF_CUDA(cudaMemcpyAsync(S, d, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaMemcpyAsync(T, d + NN, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  return CQF_OK;
+}
+
+cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int nMat,
+                                 const cqf_opts* optsIn, cqf_stats* stats) {
+  g_err.clear();
+  if (!B || !list || nMat <= 0) return fail(CQF_EINVAL, "cqf_two_body_contract: bad argument");
+  if (nMat > MAXMAT) return fail(CQF_EINVAL, "too many contractions in one call");
+  cqf_opts opts;
+  cqf_opts_default(&opts);
+  if (optsIn) opts = *optsIn;
+  for (int m = 0; m < nMat; m++) {
+    if (!list[m].X || !list[m].AX) return fail(CQF_EINVAL, "null X or AX");
+    if (list[m].type != CQF_COULOMB && list[m].type != CQF_EXCHANGE)
+      return fail(CQF_EINVAL, "unknown contraction type");
+  }
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
+
+  const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
+  const int cw = opts.is_complex ? 2 : 1;
+  const size_t matN = (size_t)N * N * cw, matC = (size_t)nc * nc * cw;
+  const size_t ns2 = (size_t)ns * ns;
+  // workspace: [X copies | AX copies] (host path) | Xc | Ac | norms | normsMat | gmax
+  size_t off = 0;
+  auto take = [&](size_t doubles) {
+    size_t o = off;
+    off += (doubles + 31) / 32 * 32;
+    return o;
+  };
+  const bool host = !opts.device_pointers;
+  size_t oX = host ? take(matN * nMat) : 0, oAX = host ? take(matN * nMat) : 0;
+  size_t oXc = take(matC * nMat), oAc = take(matC * nMat);
+  size_t oNm = take(ns2), oNmM = take(ns2 * nMat), oG = take(4);
+  CQF_TRY(ensure_ws(B, off * sizeof(double)));
+  double* ws = static_cast<double*>(B->d_ws);
+
+  CQF_CUDA(cudaEventRecord(B->ev0, st));
+  std::vector<const double*> Xd(nMat);
+  std::vector<double*> AXd(nMat);
+  for (int m = 0; m < nMat; m++) {
+    if (host) {
+      Xd[m] = ws + oX + m * matN;
+      AXd[m] = ws + oAX + m * matN;
+      CQF_CUDA(cudaMemcpyAsync((void*)Xd[m], list[m].X, matN * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+      CQF_CUDA(cudaMemcpyAsync(AXd[m], list[m].AX, matN * sizeof(double), cudaMemcpyHostToDevice,
+                               st));
+    } else {
+      Xd[m] = static_cast<const double*>(list[m].X);
+      AXd[m] = static_cast<double*>(list[m].AX);
+    }
+  }
+  std::vector<int> flags(nMat);
+  for (int m = 0; m < nMat; m++)
+    flags[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
+  CQF_CUDA(cudaMemcpyAsync(B->d_flags, flags.data(), nMat * sizeof(int), cudaMemcpyHostToDevice,
+                           st));
+  CQF_CUDA(cudaMemsetAsync(B->d_counters, 0, 8 * sizeof(unsigned long long), st));
+  CQF_CUDA(cudaMemsetAsync(ws + oG, 0, 4 * sizeof(double), st));
+
+  // shell-block norms (per matrix, symmetrised when non-Hermitian), max
+  for (int m = 0; m < nMat; m++) {
+    double* nm = ws + oNmM + m * ns2;
+    block_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(Xd[m], opts.is_complex, N, B->d_shells, ns,
+                                                        nm);
+    if (!list[m].hermitian) sym_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(nm, ns);
+  }
+  max_norms_kernel<<<grid1(ns2, 256), 256, 0, st>>>(ws + oNmM, nMat, ns2, ws + oNm,
+                                                    reinterpret_cast<unsigned long long*>(ws + oG));
+  // densities to the Cartesian AO basis, zero accumulators
+  for (int m = 0; m < nMat; m++)
+    to_cart_kernel<<<grid1((size_t)nc * nc, 256), 256, 0, st>>>(
+        Xd[m], opts.is_complex, N, nc, B->d_shells, B->d_cart2shell, B->d_sph, B->d_sphOff,
+        ws + oXc + m * matC);
+  CQF_CUDA(cudaMemsetAsync(ws + oAc, 0, matC * nMat * sizeof(double), st));
+  CQF_CUDA(cudaGetLastError());
+
+  JKLaunch a{};
+  a.pairs = B->d_pairs;
+  a.pp = B->d_pp;
+  a.boys64 = B->d_boys64;
+  a.boys32 = B->d_boys32;
+  a.screen = opts.screen;
+  a.thresh = B->thresh;
+  a.norms = ws + oNm;
+  a.normsMat = ws + oNmM;
+  a.maxNorm = ws + oG;
+  a.nShell = ns;
+  a.nMat = nMat;
+  a.cplx = opts.is_complex;
+  a.ncart = nc;
+  a.flags = B->d_flags;
+  a.Xc = ws + oXc;
+  a.Ac = ws + oAc;
+  a.precision = opts.precision;
+  a.fp32_cut = opts.fp32_cutoff;
+  a.counters = B->d_counters;
+  for (int cb = 0; cb < NCLS; cb++)
+    for (int ck = 0; ck <= cb; ck++) {
+      if (!B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
+      int la, lb, lc, ld;
+      class_ls(cb, la, lb);
+      class_ls(ck, lc, ld);
+      a.braBeg = B->cls_beg[cb];
+      a.nBra = B->cls_cnt[cb];
+      a.ketBeg = B->cls_beg[ck];
+      a.nKet = B->cls_cnt[ck];
+      a.same = (cb == ck);
+      launch_jk_generic(a, la, lb, lc, ld, st);
+    }
+  CQF_CUDA(cudaGetLastError());
+  for (int m = 0; m < nMat; m++)
+    from_cart_kernel<<<grid1((size_t)N * N, 256), 256, 0, st>>>(
+        ws + oAc + m * matC, opts.is_complex, list[m].hermitian, N, nc, B->d_shells,
+        B->d_ao2shell, B->d_sph, B->d_sphOff, AXd[m]);
+  CQF_CUDA(cudaGetLastError());
+  if (host)
+    for (int m = 0; m < nMat; m++)
+      CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXd[m], matN * sizeof(double), cudaMemcpyDeviceToHost,
+                               st));
+  CQF_CUDA(cudaEventRecord(B->ev1, st));
+  unsigned long long cnt[4] = {0, 0, 0, 0};
+  CQF_CUDA(cudaMemcpyAsync(cnt, B->d_counters, 4 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+  CQF_CUDA(cudaStreamSynchronize(st));
+  if (stats) {
+    stats->quartets_total = (long long)cnt[0];
+    stats->quartets_screened = (long long)cnt[1];
+    stats->quartets_fp32 = (long long)cnt[2];
+    stats->quartets_fp64 = (long long)cnt[3];
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+    stats->device_ms = ms;
+  }
+  return CQF_OK;
+}
+
+}  // extern "C"

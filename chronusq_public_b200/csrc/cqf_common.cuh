@@ -1,0 +1,219 @@
+// Shared device-side definitions of the direct J/K build (sm_100a).
+//
+// Data layout in HBM (one cqf_basis):
+//   ShellDev[nshell]       shell metadata (l, pure, primitive/AO offsets, centre)
+//   PairDev[npair]         significant shell pairs (ShellPairData semantics,
+//                          src/basisset/basisset.cxx:652-706), grouped into
+//                          angular-momentum classes (lA >= lB) and sorted by
+//                          Schwarz bound (descending) inside each class
+//   PrimPairDev[nprimpair] primitive-pair data (p, K, P, PA, PB), 96 B each,
+//                          contiguous per shell pair so one pair's primitives
+//                          are one coalesced run
+//   boys table             F_m(T_j), T_j = j*0.05, m = 0..BOYS_MMAX (FP64 and
+//                          an FP32 copy), 186 KB, L2 resident
+//   Cartesian-AO densities / accumulators, nMat x ncart x ncart
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cqf {
+
+constexpr int LMAX = 3;            // highest shell angular momentum (f)
+constexpr int BOYS_MMAX = 32;      // tabulated Boys orders
+constexpr double BOYS_DT = 0.05;   // grid spacing of the Taylor table
+constexpr double BOYS_TMAX = 36.0; // above: F0 = sqrt(pi/T)/2 + upward recursion
+constexpr int BOYS_NPTS = 724;     // grid points 0 .. TMAX/DT (+ margin)
+constexpr int BOYS_K64 = 8;        // Taylor terms k = 0..8 (FP64, |dT| <= 0.025)
+constexpr int BOYS_K32 = 4;        // Taylor terms k = 0..4 (FP32)
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int nsph(int l) { return 2 * l + 1; }
+// number of Hermite functions with t+u+v <= L
+__host__ __device__ constexpr int nherm(int L) {
+  return L < 0 ? 0 : (L + 1) * (L + 2) * (L + 3) / 6;
+}
+// compact Hermite index: blocks of equal t+u+v, inside a block t descending,
+// then u descending (v ascending)
+__host__ __device__ constexpr int hidx(int t, int u, int v) {
+  return nherm(t + u + v - 1) + (u + v) * (u + v + 1) / 2 + v;
+}
+// Cartesian exponents of component i of an l shell (libint / CCA order)
+__host__ __device__ constexpr int cart_lx(int l, int i) {
+  int k = 0;
+  for (int a = 0; a <= l; a++)
+    for (int b = 0; b <= a; b++) {
+      if (k == i) return l - a;
+      k++;
+    }
+  return 0;
+}
+__host__ __device__ constexpr int cart_ly(int l, int i) {
+  int k = 0;
+  for (int a = 0; a <= l; a++)
+    for (int b = 0; b <= a; b++) {
+      if (k == i) return a - b;
+      k++;
+    }
+  return 0;
+}
+__host__ __device__ constexpr int cart_lz(int l, int i) {
+  return l - cart_lx(l, i) - cart_ly(l, i);
+}
+
+struct ShellDev {
+  int l, pure, nprim, prim_off;
+  int cart_off, sph_off, pad0, pad1;
+  double O[3];
+};
+
+// One significant shell pair.  (shA, shB) is the order the ERI kernels use
+// (l(shA) >= l(shB)); (s1, s2) is the reference loop order (s1 >= s2).
+struct PairDev {
+  int shA, shB, s1, s2;
+  int cA, cB;        // Cartesian AO offsets of shA / shB
+  int lex;           // rank of (s1, s2) in the reference loop order
+  int pp_off;        // first primitive pair
+  int npp;           // number of primitive pairs
+  int cls;           // class id (lA, lB)
+  double Q;          // Schwarz bound sqrt(||(ab|ab) diag||_inf)
+};
+
+struct PrimPairDev {
+  double p, K;       // exponent sum; c_a c_b exp(-mu |AB|^2)
+  double P[3], PA[3], PB[3];
+  double pad;
+};
+
+// ----------------------------------------------------------------- Boys
+// F_0..F_L at T.  Taylor expansion of F_L about the nearest grid point
+// (F_m' = -F_{m+1}), downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1);
+// for T >= TMAX, F_0 = sqrt(pi/T)/2 and upward recursion keeping e^-T.
+template <int L>
+__device__ __forceinline__ void boys_f64(double T, double* F,
+                                         const double* __restrict__ tab) {
+  if (T < BOYS_TMAX) {
+    int j = __double2int_rn(T * (1.0 / BOYS_DT));
+    double dT = j * BOYS_DT - T;
+    const double* row = tab + j * (BOYS_MMAX + 1) + L;
+    double s = __ldg(row + BOYS_K64);
+#pragma unroll
+    for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0 / (k + 1));
+    F[L] = s;
+    if (L > 0) {
+      double e = exp(-T), t2 = 2.0 * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    double rT = rsqrt(T);
+    F[0] = 0.88622692545275801365 * rT;  // sqrt(pi)/2
+    if (L > 0) {
+      double e = exp(-T), h = 0.5 * rT * rT;
+#pragma unroll
+      for (int m = 0; m < L; m++) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void boys_f32(float T, float* F, const float* __restrict__ tab) {
+  if (T < (float)BOYS_TMAX) {
+    int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
+    float dT = j * (float)BOYS_DT - T;
+    const float* row = tab + j * (BOYS_MMAX + 1) + L;
+    float s = __ldg(row + BOYS_K32);
+#pragma unroll
+    for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));
+    F[L] = s;
+    if (L > 0) {
+      float e = __expf(-T), t2 = 2.0f * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
+    }
+  } else {
+    float rT = rsqrtf(T);
+    F[0] = 0.886226925f * rT;
+    if (L > 0) {
+      float e = __expf(-T), h = 0.5f * rT * rT;
+#pragma unroll
+      for (int m = 0; m < L; m++) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+  }
+}
+
+// -------------------------------------------------- Hermite coefficients
+// E^{ij}_t for one axis (McMurchie-Davidson; Helgaker eq. 9.5.6) without the
+// Gaussian-product factor.  E[i][j][t], t <= i + j.
+template <typename R, int LA, int LB>
+__device__ __forceinline__ void hermite_E(R o2p, R PA, R PB, R (&E)[LA + 1][LB + 1][LA + LB + 1]) {
+#pragma unroll
+  for (int i = 0; i <= LA; i++)
+#pragma unroll
+    for (int j = 0; j <= LB; j++)
+#pragma unroll
+      for (int t = 0; t <= LA + LB; t++) E[i][j][t] = R(0);
+  E[0][0][0] = R(1);
+#pragma unroll
+  for (int i = 1; i <= LA; i++)
+#pragma unroll
+    for (int t = 0; t <= i; t++) {
+      R v = PA * (t <= i - 1 ? E[i - 1][0][t] : R(0));
+      if (t >= 1) v += o2p * E[i - 1][0][t - 1];
+      if (t + 1 <= i - 1) v += R(t + 1) * E[i - 1][0][t + 1];
+      E[i][0][t] = v;
+    }
+#pragma unroll
+  for (int i = 0; i <= LA; i++)
+#pragma unroll
+    for (int j = 1; j <= LB; j++)
+#pragma unroll
+      for (int t = 0; t <= i + j; t++) {
+        R v = PB * (t <= i + j - 1 ? E[i][j - 1][t] : R(0));
+        if (t >= 1) v += o2p * E[i][j - 1][t - 1];
+        if (t + 1 <= i + j - 1) v += R(t + 1) * E[i][j - 1][t + 1];
+        E[i][j][t] = v;
+      }
+}
+
+// -------------------------------------------------- Hermite integrals R_tuv
+// In-place downward sweep over the auxiliary index n (see hidx ordering):
+// R^{(n)}_{t+1,u,v} = t R^{(n+1)}_{t-1,u,v} + X_PQ R^{(n+1)}_{t,u,v}, etc.
+// On entry F[0..L] holds the Boys values; on exit R[hidx(t,u,v)] = R^{(0)}_tuv.
+template <typename R, int L>
+__device__ __forceinline__ void hermite_R(R alpha, R X, R Y, R Z, const R* F, R* Rv) {
+  R m2a = R(-2) * alpha;
+  R f[L + 1];
+  f[0] = R(1);
+#pragma unroll
+  for (int n = 1; n <= L; n++) f[n] = f[n - 1] * m2a;
+  Rv[0] = f[L] * F[L];
+#pragma unroll
+  for (int n = L - 1; n >= 0; n--) {
+#pragma unroll
+    for (int tot = L - n; tot >= 1; tot--) {
+#pragma unroll
+      for (int t = tot; t >= 0; t--) {
+#pragma unroll
+        for (int u = tot - t; u >= 0; u--) {
+          const int v = tot - t - u;
+          R val;
+          if (t > 0) {
+            val = X * Rv[hidx(t - 1, u, v)];
+            if (t > 1) val += R(t - 1) * Rv[hidx(t - 2, u, v)];
+          } else if (u > 0) {
+            val = Y * Rv[hidx(0, u - 1, v)];
+            if (u > 1) val += R(u - 1) * Rv[hidx(0, u - 2, v)];
+          } else {
+            val = Z * Rv[hidx(0, 0, v - 1)];
+            if (v > 1) val += R(v - 1) * Rv[hidx(0, 0, v - 2)];
+          }
+          Rv[hidx(t, u, v)] = val;
+        }
+      }
+    }
+    Rv[0] = f[n] * F[n];
+  }
+}
+
+}  // namespace cqf

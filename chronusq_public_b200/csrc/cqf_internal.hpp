@@ -1,0 +1,79 @@
+// Host-side internals shared by the translation units of libcqfock.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cqfock.h"
+#include "cqf_common.cuh"
+
+namespace cqf {
+
+constexpr int NCLS = (LMAX + 1) * (LMAX + 2) / 2;  // pair classes (lA >= lB)
+inline int class_id(int la, int lb) { return la * (la + 1) / 2 + lb; }
+inline void class_ls(int c, int& la, int& lb) {
+  la = 0;
+  while ((la + 1) * (la + 2) / 2 <= c) la++;
+  lb = c - la * (la + 1) / 2;
+}
+
+// Per-matrix flags packed for the kernels: bit0 HER, bit1 EXCHANGE.
+constexpr int MAXMAT = 512;
+
+// Arguments of one class-quartet J/K launch.
+struct JKLaunch {
+  const PairDev* pairs;
+  const PrimPairDev* pp;
+  const double* boys64;
+  const float* boys32;
+  int braBeg, nBra, ketBeg, nKet, same;
+  int screen;
+  double thresh;
+  const double* norms;      // max over matrices, nshell x nshell (col-major)
+  const double* normsMat;   // nMat x nshell x nshell (only read when nMat > 1)
+  const double* maxNorm;    // device scalar: max of norms (tile-level screen)
+  int nShell;
+  int nMat, cplx, ncart;
+  const int* flags;         // nMat flags (device)
+  const double* Xc;         // nMat x ncart x ncart (complex: interleaved)
+  double* Ac;               // same shape, accumulated
+  int precision;            // 0 FP64, 1 mixed
+  double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
+  unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
+};
+
+}  // namespace cqf
+
+struct cqf_basis {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nshell = 0, nbasis = 0, ncart = 0, npair = 0, maxL = 0, maxPrim = 0;
+  long long nprimpair = 0;
+  double thresh = 1e-12;
+  std::vector<cqf::ShellDev> h_shells;
+  std::vector<cqf::PairDev> h_pairs;     // final (class, Q-sorted) order
+  int cls_beg[cqf::NCLS] = {0}, cls_cnt[cqf::NCLS] = {0};
+  std::vector<double> h_schwarz;         // nshell^2
+  // device-resident basis data
+  cqf::ShellDev* d_shells = nullptr;
+  double* d_prim = nullptr;              // alpha | coeff
+  cqf::PairDev* d_pairs = nullptr;
+  cqf::PrimPairDev* d_pp = nullptr;
+  double* d_boys64 = nullptr;
+  float* d_boys32 = nullptr;
+  double* d_schwarz = nullptr;
+  double* d_sph = nullptr;               // solid-harmonic matrices, all l
+  int* d_sphOff = nullptr;               // offset of l's matrix in d_sph
+  int* d_ao2shell = nullptr;             // AO (spherical) -> shell
+  int* d_cart2shell = nullptr;           // Cartesian AO -> shell
+  // per-call workspace (grown on demand)
+  size_t ws_bytes = 0;
+  void* d_ws = nullptr;
+  unsigned long long* d_counters = nullptr;
+  int* d_flags = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::mutex mu;
+};

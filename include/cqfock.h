@@ -1,0 +1,123 @@
+/*
+ * cqfock.h -- C ABI of the B200 direct two-electron (J/K) Fock build.
+ *
+ * This is the drop-in boundary for ChronusQ's direct contraction path.  A thin
+ * C++ shim (chronusq_public_b200/shim/cqf_chronusq_shim.hpp) keeps ChronusQ's
+ * class signatures and calls these functions; integer status codes cross the
+ * boundary, never exceptions.
+ *
+ * Reference interfaces replaced (paths within xsligroup/chronusq_public):
+ *   cqf_basis_create      BasisSet::update + ShellPairData::computeShellPairs
+ *                         (src/basisset/basisset.cxx:98-191, :652-706) and
+ *                         DirectTPI::computeSchwarz
+ *                         (src/particleintegrals/aointegrals/aointegrals_utilities.cxx:53-162),
+ *                         cached per geometry as DirectTPI does
+ *                         (include/particleintegrals/twopints/gtodirecttpi.hpp:30-141)
+ *   cqf_two_body_contract GTODirectTPIContraction<MatsT,double>::twoBodyContract
+ *                         (include/particleintegrals/twopints/gtodirecttpi.hpp:199-206)
+ *                         -> directScaffoldNew
+ *                         (include/particleintegrals/contract/direct.hpp:1412-2123)
+ *   cqf_contraction       TwoBodyContraction<T> {X, AX, HER, contType}
+ *                         (include/particleintegrals/twopints.hpp:59-75)
+ *   CQF_COULOMB/EXCHANGE  TWOBODY_CONTRACTION_TYPE (twopints.hpp:31-41)
+ *
+ * Matrices are column-major N x N with leading dimension N (direct.hpp:1868),
+ * N = number of AO functions; complex matrices are interleaved (re, im)
+ * doubles, i.e. std::complex<double>.  AX is accumulated (+=) as on the
+ * reference's multi-threaded path (direct.hpp:2047-2058); callers zero it
+ * first, as FockBuilder::formRawGDInBatches does (fockbuilder/impl.hpp:131-137).
+ */
+#ifndef CQFOCK_H
+#define CQFOCK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CQF_OK = 0,
+  CQF_EINVAL = 1,     /* bad argument (null pointer, size, unsupported l) */
+  CQF_ENOMEM = 2,     /* device allocation failed */
+  CQF_ECUDA = 3,      /* CUDA runtime error */
+  CQF_ENOTSUP = 4,    /* feature not supported for these inputs */
+  CQF_ETIMEDOUT = 5,  /* a bounded device/host wait ran out */
+  CQF_ENODEV = 6      /* no CUDA device */
+} cqf_status;
+
+typedef enum { CQF_COULOMB = 0, CQF_EXCHANGE = 1 } cqf_contraction_type;
+
+typedef enum { CQF_FP64 = 0, CQF_MIXED = 1 } cqf_precision;
+
+/* One contracted shell, as libint2::Shell stores it in ChronusQ:
+ * coeff are the libint-normalised contraction coefficients (contr[0].coeff),
+ * pure = 1 for spherical (m = -l..l), 0 for Cartesian (x^l first). */
+typedef struct {
+  int l;
+  int pure;
+  int nprim;
+  const double* alpha;
+  const double* coeff;
+  double origin[3]; /* Bohr */
+} cqf_shell;
+
+typedef struct cqf_basis cqf_basis;
+
+/* One contraction: AX += G[X] (TwoBodyContraction<T>). */
+typedef struct {
+  const void* X;
+  void* AX;
+  int hermitian; /* TwoBodyContraction::HER */
+  int type;      /* cqf_contraction_type */
+} cqf_contraction;
+
+typedef struct {
+  int is_complex;       /* X/AX are std::complex<double> */
+  int screen;           /* 1: Schwarz x density screen (reference default) */
+  int device_pointers;  /* 1: X/AX are device pointers, 0: host pointers */
+  int precision;        /* cqf_precision */
+  double fp32_cutoff;   /* mixed: quartets with bound < cutoff run in FP32 */
+  void* stream;         /* cudaStream_t to run on; NULL = the basis' stream */
+} cqf_opts;
+
+typedef struct {
+  long long quartets_total;     /* unique quartets visited (8-fold) */
+  long long quartets_screened;  /* dropped by the Schwarz x density screen */
+  long long quartets_fp32;      /* computed on the FP32 path */
+  long long quartets_fp64;      /* computed on the FP64 path */
+  double device_ms;             /* device time of the contraction */
+} cqf_stats;
+
+/* Fill opts with the reference defaults (screen on, FP64, host pointers). */
+void cqf_opts_default(cqf_opts* opts);
+
+/* Upload shells, build significant shell pairs, primitive-pair data, class
+ * buckets and Schwarz bounds on `device`.  thresh_schwarz is
+ * DirectTPI::threshSchwarz_ (1e-12 in ChronusQ). */
+cqf_status cqf_basis_create(const cqf_shell* shells, int nshell, double thresh_schwarz,
+                            int device, cqf_basis** out);
+cqf_status cqf_basis_destroy(cqf_basis* basis);
+
+/* nbasis (AO functions), nshell, npair (significant shell pairs). */
+cqf_status cqf_basis_info(const cqf_basis* basis, int* nbasis, int* nshell, int* npair);
+
+/* Schwarz table, nshell x nshell column-major (host memory). */
+cqf_status cqf_basis_schwarz(const cqf_basis* basis, double* Q);
+
+/* Overlap S and kinetic T matrices (N x N column-major, host memory) of the
+ * basis, computed on the device.  Replaces the one-electron overlap / kinetic
+ * integrals ChronusQ takes from libint (used here to orthonormalise densities
+ * and for the four-component metric). */
+cqf_status cqf_basis_one_electron(cqf_basis* basis, double* S, double* T);
+
+/* GTODirectTPIContraction::twoBodyContract: for each entry, AX += G[X]. */
+cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
+                                 const cqf_opts* opts, cqf_stats* stats);
+
+/* Text of the last error on this thread ("" if none). */
+const char* cqf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CQFOCK_H */
