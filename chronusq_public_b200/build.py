@@ -34,6 +34,7 @@ def _sources():
 
 def _deps():
     return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) +
+                  glob.glob(os.path.join(CSRC, "gen", "*.cuh")) +
                   glob.glob(os.path.join(CSRC, "*.hpp")) +
                   glob.glob(os.path.join(ROOT, "include", "*.h")))
 
@@ -51,7 +52,19 @@ def _compile(src, verbose):
     return obj
 
 
+def generate(verbose: bool = False):
+    """Runs the kernel generators (csrc/gen_*.py -> csrc/gen/*.cuh)."""
+    for gen in sorted(glob.glob(os.path.join(CSRC, "gen_*.py"))):
+        out = os.path.join(CSRC, "gen", "cqf_" + os.path.basename(gen)[4:-3] + ".cuh")
+        if (not os.path.exists(out)
+                or os.path.getmtime(out) < os.path.getmtime(gen)):
+            if verbose:
+                print("generate", out, flush=True)
+            subprocess.check_call([sys.executable, gen, out])
+
+
 def build(verbose: bool = False) -> str:
+    generate(verbose)
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     srcs = _sources()

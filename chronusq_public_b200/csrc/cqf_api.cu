@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "cqf_internal.hpp"
+#include "cqf_jk_fast.cuh"
 #include "cqf_jk_kernels.cuh"
 
 using namespace cqf;
@@ -698,28 +699,22 @@ cqf_status cqf_basis_one_electron(cqf_basis* B, double* S, double* T) {
   return CQF_OK;
 }
 
-cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int nMat,
-                                 const cqf_opts* optsIn, cqf_stats* stats) {
-  g_err.clear();
-  if (!B || !list || nMat <= 0) return fail(CQF_EINVAL, "cqf_two_body_contract: bad argument");
-  if (nMat > MAXMAT) return fail(CQF_EINVAL, "too many contractions in one call");
-  cqf_opts opts;
-  cqf_opts_default(&opts);
-  if (optsIn) opts = *optsIn;
-  for (int m = 0; m < nMat; m++) {
-    if (!list[m].X || !list[m].AX) return fail(CQF_EINVAL, "null X or AX");
-    if (list[m].type != CQF_COULOMB && list[m].type != CQF_EXCHANGE)
-      return fail(CQF_EINVAL, "unknown contraction type");
-  }
-  std::lock_guard<std::mutex> lk(B->mu);
-  CQF_CUDA(cudaSetDevice(B->device));
-  cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
+}  // extern "C"
 
-  const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
+namespace cqf {
+
+// Workspace layout of one contraction (in doubles, each part 256-B aligned):
+// [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
+struct WsLayout {
+  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, total;
+};
+
+WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   const int cw = opts.is_complex ? 2 : 1;
-  const size_t matN = (size_t)N * N * cw, matC = (size_t)nc * nc * cw;
-  const size_t ns2 = (size_t)ns * ns;
-  // workspace: [X copies | AX copies] (host path) | Xc | Ac | norms | normsMat | gmax
+  const size_t matN = (size_t)B->nbasis * B->nbasis * cw;
+  const size_t matC = (size_t)B->ncart * B->ncart * cw;
+  const size_t ns2 = (size_t)B->nshell * B->nshell;
+  WsLayout L{};
   size_t off = 0;
   auto take = [&](size_t doubles) {
     size_t o = off;
@@ -727,12 +722,42 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int 
     return o;
   };
   const bool host = !opts.device_pointers;
-  size_t oX = host ? take(matN * nMat) : 0, oAX = host ? take(matN * nMat) : 0;
-  size_t oXc = take(matC * nMat), oAc = take(matC * nMat);
-  size_t oNm = take(ns2), oNmM = take(ns2 * nMat), oG = take(4);
-  CQF_TRY(ensure_ws(B, off * sizeof(double)));
-  double* ws = static_cast<double*>(B->d_ws);
+  L.oX = host ? take(matN * nMat) : 0;
+  L.oAX = host ? take(matN * nMat) : 0;
+  L.oXc = take(matC * nMat);
+  L.oAc = take(matC * nMat);
+  L.oNm = take(ns2);
+  L.oNmM = take(ns2 * nMat);
+  L.oG = take(4);
+  L.total = off;
+  return L;
+}
 
+cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat) {
+  if (!B || !list || nMat <= 0) return fail(CQF_EINVAL, "cqf_two_body_contract: bad argument");
+  if (nMat > MAXMAT) return fail(CQF_EINVAL, "too many contractions in one call");
+  for (int m = 0; m < nMat; m++) {
+    if (!list[m].X || !list[m].AX) return fail(CQF_EINVAL, "null X or AX");
+    if (list[m].type != CQF_COULOMB && list[m].type != CQF_EXCHANGE)
+      return fail(CQF_EINVAL, "unknown contraction type");
+  }
+  return CQF_OK;
+}
+
+// The contraction pipeline on a caller-provided workspace `ws` of at least
+// ws_layout(...).total doubles (device memory).  Caller holds B->mu and has
+// made B's device current.
+cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
+                         const cqf_opts& opts, cqf_stats* stats, double* ws) {
+  cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
+  const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
+  const int cw = opts.is_complex ? 2 : 1;
+  const size_t matN = (size_t)N * N * cw, matC = (size_t)nc * nc * cw;
+  const size_t ns2 = (size_t)ns * ns;
+  const WsLayout Lw = ws_layout(B, nMat, opts);
+  const bool host = !opts.device_pointers;
+  const size_t oX = Lw.oX, oAX = Lw.oAX, oXc = Lw.oXc, oAc = Lw.oAc, oNm = Lw.oNm,
+               oNmM = Lw.oNmM, oG = Lw.oG;
   CQF_CUDA(cudaEventRecord(B->ev0, st));
   std::vector<const double*> Xd(nMat);
   std::vector<double*> AXd(nMat);
@@ -794,6 +819,9 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int 
   a.precision = opts.precision;
   a.fp32_cut = opts.fp32_cutoff;
   a.counters = B->d_counters;
+  // closed-shell fast path: real matrices flagged Hermitian (symmetric)
+  bool fastOK = !opts.is_complex;
+  for (int m = 0; m < nMat; m++) fastOK = fastOK && list[m].hermitian;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck <= cb; ck++) {
       if (!B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
@@ -805,7 +833,9 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int 
       a.ketBeg = B->cls_beg[ck];
       a.nKet = B->cls_cnt[ck];
       a.same = (cb == ck);
-      launch_jk_generic(a, la, lb, lc, ld, st);
+      const int lm = std::max(std::max(la, lb), std::max(lc, ld));
+      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, st)))
+        launch_jk_generic(a, la, lb, lc, ld, st);
     }
   CQF_CUDA(cudaGetLastError());
   for (int m = 0; m < nMat; m++)
@@ -832,6 +862,24 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int 
     stats->device_ms = ms;
   }
   return CQF_OK;
+}
+
+
+}  // namespace cqf
+
+extern "C" {
+
+cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int nMat,
+                                 const cqf_opts* optsIn, cqf_stats* stats) {
+  g_err.clear();
+  CQF_TRY(check_contract_args(B, list, nMat));
+  cqf_opts opts;
+  cqf_opts_default(&opts);
+  if (optsIn) opts = *optsIn;
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
+  return contract_core(B, list, nMat, opts, stats, static_cast<double*>(B->d_ws));
 }
 
 }  // extern "C"

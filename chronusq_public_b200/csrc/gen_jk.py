@@ -1,0 +1,399 @@
+"""Generates cqf_gen_jk.cuh: straight-line McMurchie-Davidson kernels for the
+closed-shell (real, symmetric density) J/K build, one per shell-quartet class.
+
+Run by chronusq_public_b200/build.py before nvcc; the output goes to
+csrc/gen/ (not tracked).  For each class the generator
+
+* picks the orientation (which pair class is the block's bra) that keeps the
+  Hermite intermediate G[cd][tuv] smallest,
+* splits the ket Cartesian components c into chunks so that the live set
+  (integral block + G + R) stays inside the register file,
+* emits E coefficients, Boys/R recursion, the G and integral contractions as
+  scalar code with Hermite coefficients constant-folded (E^{00}_0 = 1,
+  E^{ij}_t = 0 for t > i + j),
+* emits the digestion of each density: J_ab (warp-reduced over the block's
+  kets, which share the bra pair), J_cd, and the four exchange blocks placed
+  in the bra rows (K_ac, K_bd, K_ad, K_bc); with a symmetric density and the
+  final 1/2 (A + A^T) these equal the reference's updates
+  (include/particleintegrals/contract/direct.hpp:1858-1918).
+"""
+import itertools
+import os
+import sys
+
+LMAX_FAST = 2  # classes with every l <= 2 get generated kernels
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def carts(l):
+    out = []
+    for i in range(l + 1):
+        for j in range(i + 1):
+            out.append((l - i, i - j, j))
+    return out
+
+
+def nherm(L):
+    return (L + 1) * (L + 2) * (L + 3) // 6
+
+
+def herm_list(L):
+    return [(t, u, v) for n in range(L + 1) for t in range(n, -1, -1)
+            for u in range(n - t, -1, -1) for v in [n - t - u]]
+
+
+class E1D:
+    """Symbolic 1D Hermite coefficients E^{ij}_t of one pair (axis x)."""
+
+    def __init__(self, w, li, lj, tag, o2p, PA, PB):
+        self.w = w
+        self.val = {}
+        self.val[(0, 0, 0)] = "1"
+        for i in range(li + 1):
+            for j in range(lj + 1):
+                if i == 0 and j == 0:
+                    continue
+                up = (j == 0)
+                pi, pj = (i - 1, j) if up else (i, j - 1)
+                X = PA if up else PB
+                for t in range(i + j + 1):
+                    terms = []
+                    a = self.get(pi, pj, t)
+                    if a is not None:
+                        terms.append(a if X is None else self._mul(X, a))
+                    b = self.get(pi, pj, t - 1)
+                    if b is not None:
+                        terms.append(self._mul(o2p, b))
+                    c = self.get(pi, pj, t + 1)
+                    if c is not None:
+                        terms.append(self._mul("T(%d)" % (t + 1), c) if t + 1 != 1 else c)
+                    if not terms:
+                        continue
+                    name = "%s_%d_%d_%d" % (tag, i, j, t)
+                    w.line("const T %s = %s;" % (name, " + ".join(terms)))
+                    self.val[(i, j, t)] = name
+
+    @staticmethod
+    def _mul(a, b):
+        if a == "1":
+            return b
+        if b == "1":
+            return a
+        return "%s * %s" % (a, b)
+
+    def get(self, i, j, t):
+        if t < 0 or t > i + j or i < 0 or j < 0:
+            return None
+        return self.val.get((i, j, t))
+
+
+class W:
+    def __init__(self):
+        self.lines = []
+        self.ind = 0
+
+    def line(self, s):
+        self.lines.append("  " * self.ind + s)
+
+    def open(self, s):
+        self.line(s)
+        self.ind += 1
+
+    def close(self, s="}"):
+        self.ind -= 1
+        self.line(s)
+
+
+def orientation(c1, c2):
+    """(bra, ket) pair classes minimising NCD * H(lab)."""
+    (a1, b1), (a2, b2) = c1, c2
+    g12 = ncart(a2) * ncart(b2) * nherm(a1 + b1)
+    g21 = ncart(a1) * ncart(b1) * nherm(a2 + b2)
+    return (c1, c2) if g12 <= g21 else (c2, c1)
+
+
+def chunk_size(la, lb, lc, ld):
+    """c components per chunk so NAB*CC*ND + CC*ND*HAB + H(L) stays small."""
+    nab = ncart(la) * ncart(lb)
+    nd = ncart(ld)
+    hab = nherm(la + lb)
+    hl = nherm(la + lb + lc + ld)
+    best = 1
+    for cc in range(1, ncart(lc) + 1):
+        if ncart(lc) % cc:
+            continue
+        live = nab * cc * nd + cc * nd * hab + hl
+        if live <= 110:
+            best = cc
+    return best
+
+
+def gen_class(la, lb, lc, ld):
+    """Device function computing the chunk [c0, c0+CC) of the contracted
+    Cartesian block into I_* scalars, then digesting it."""
+    w = W()
+    A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
+    NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
+    lab, lcd = la + lb, lc + ld
+    L = lab + lcd
+    CC = chunk_size(la, lb, lc, ld)
+    nchunk = NC // CC
+    hab = herm_list(lab)
+    hall = herm_list(L)
+    name = "%d%d%d%d" % (la, lb, lc, ld)
+    w.line("// (%s%s|%s%s): NAB=%d NCD=%d L=%d, %d chunk(s) of %d c-components"
+           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], NA * NB, NC * ND,
+              L, nchunk, CC))
+    w.open("struct GenJK_%s {" % name)
+    w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
+    w.line("static constexpr int NCHUNK = %d;" % nchunk)
+    w.line("static constexpr int NI = %d;  // integrals per chunk" % (NA * NB * CC * ND))
+    # ---- integral chunk
+    w.line("template <typename T>")
+    w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
+           "const PrimPairDev* __restrict__ pp, const T* __restrict__ boys, const int ch, "
+           "double (&I)[%d]) {" % (NA * NB * CC * ND))
+    w.open("#pragma unroll")
+    w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NA * NB * CC * ND))
+    w.ind -= 1
+    w.line("const T PI52x2 = T(34.986836655249725693);")
+    w.line("#pragma unroll 1")
+    w.open("for (int ip = 0; ip < P.npp; ip++) {")
+    w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
+    w.line("const T p = T(pa.p), Kab = T(pa.K), o2p = T(0.5) / p;")
+    w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
+    axes = "xyz"
+    if lab > 0:
+        for x in range(3):
+            w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
+    # G accumulators per chunk-local cd and bra Hermite tuv
+    cds = [(ci, di) for ci in range(CC) for di in range(ND)]
+    for (ci, di) in cds:
+        for (t, u, v) in hab:
+            w.line("T g_%d_%d_%d_%d_%d = T(0);" % (ci, di, t, u, v))
+    w.line("#pragma unroll 1")
+    w.open("for (int iq = 0; iq < Q.npp; iq++) {")
+    w.line("const PrimPairDev& pb = pp[Q.pp_off + iq];")
+    w.line("const T q = T(pb.p), Kcd = T(pb.K), o2q = T(0.5) / q;")
+    w.line("const T X = Px - T(pb.P[0]), Y = Py - T(pb.P[1]), Z = Pz - T(pb.P[2]);")
+    w.line("const T pq = p + q, alpha = p * q / pq;")
+    w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
+    w.line("T F[%d];" % (L + 1))
+    w.open("if constexpr (sizeof(T) == 8) {")
+    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));" % L)
+    w.close("} else {")
+    w.ind += 1
+    w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
+    w.close()
+    w.line("const T pref = PI52x2 / (p * q * sqrt(pq)) * Kab * Kcd;")
+    # ket E
+    if lcd > 0:
+        for x in range(3):
+            w.line("const T QC%s = T(pb.PA[%d]), QD%s = T(pb.PB[%d]);" % (axes[x], x, axes[x], x))
+    ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
+          for x in range(3)] if lcd > 0 else None
+    # R recursion (SSA over levels)
+    R = {}
+    w.line("const T m2a = T(-2) * alpha;")
+    pw = ["T(1)"]
+    for n in range(1, L + 1):
+        w.line("const T a%d = %s;" % (n, "m2a" if n == 1 else "a%d * m2a" % (n - 1)))
+        pw.append("a%d" % n)
+    for n in range(L, -1, -1):
+        w.line("const T r%d_0_0_0 = %s;" % (n, "F[0]" if n == 0 else "%s * F[%d]" % (pw[n], n)))
+        R[(n, 0, 0, 0)] = "r%d_0_0_0" % n
+    for tot in range(1, L + 1):
+        for n in range(L - tot, -1, -1):
+            for (t, u, v) in [h for h in hall if sum(h) == tot]:
+                if t > 0:
+                    e = "X * %s" % R[(n + 1, t - 1, u, v)]
+                    if t > 1:
+                        e += " + T(%d) * %s" % (t - 1, R[(n + 1, t - 2, u, v)])
+                elif u > 0:
+                    e = "Y * %s" % R[(n + 1, t, u - 1, v)]
+                    if u > 1:
+                        e += " + T(%d) * %s" % (u - 1, R[(n + 1, t, u - 2, v)])
+                else:
+                    e = "Z * %s" % R[(n + 1, t, u, v - 1)]
+                    if v > 1:
+                        e += " + T(%d) * %s" % (v - 1, R[(n + 1, t, u, v - 2)])
+                nm = "r%d_%d_%d_%d" % (n, t, u, v)
+                w.line("const T %s = %s;" % (nm, e))
+                R[(n, t, u, v)] = nm
+    # G: per chunk component (c = c0 + ci), runtime chunk index resolved by switch
+    w.open("switch (ch) {")
+    for chv in range(nchunk):
+        w.open("case %d: {" % chv)
+        for (ci, di) in cds:
+            c = chv * CC + ci
+            cx, cy, cz = Cc[c]
+            dx, dy, dz = Dd[di]
+            # ket weights for this (c,d): sign * Ex Ey Ez
+            terms = []
+            for ta in range(cx + dx + 1):
+                for nu in range(cy + dy + 1):
+                    for ph in range(cz + dz + 1):
+                        if lcd > 0:
+                            ex = ek[0].get(cx, dx, ta)
+                            ey = ek[1].get(cy, dy, nu)
+                            ez = ek[2].get(cz, dz, ph)
+                            if ex is None or ey is None or ez is None:
+                                continue
+                            fac = [f for f in (ex, ey, ez) if f != "1"]
+                        else:
+                            fac = []
+                        sgn = -1 if (ta + nu + ph) & 1 else 1
+                        terms.append((ta, nu, ph, sgn, fac))
+            wn = []
+            for (ta, nu, ph, sgn, fac) in terms:
+                nm = "w_%d_%d_%d_%d_%d" % (ci, di, ta, nu, ph)
+                expr = " * ".join(["pref"] + fac)
+                w.line("const T %s = %s%s;" % (nm, "-" if sgn < 0 else "", expr))
+                wn.append((ta, nu, ph, nm))
+            for (t, u, v) in hab:
+                s = " + ".join("%s * %s" % (nm, R[(0, t + ta, u + nu, v + ph)])
+                               for (ta, nu, ph, nm) in wn)
+                w.line("g_%d_%d_%d_%d_%d += %s;" % (ci, di, t, u, v, s))
+        w.line("break;")
+        w.close("}")
+    w.close("}")
+    w.close("}")  # iq loop
+    # bra E and I accumulation
+    eb = [E1D(w, la, lb, "ea" + axes[x], "o2p", "PA" + axes[x], "PB" + axes[x])
+          for x in range(3)] if lab > 0 else None
+    for ia, (ax, ay, az) in enumerate(A):
+        for ib, (bx, by, bz) in enumerate(B):
+            wterms = []
+            for t in range(ax + bx + 1):
+                for u in range(ay + by + 1):
+                    for v in range(az + bz + 1):
+                        if lab > 0:
+                            fx, fy, fz = eb[0].get(ax, bx, t), eb[1].get(ay, by, u), eb[2].get(az, bz, v)
+                            if fx is None or fy is None or fz is None:
+                                continue
+                            fac = [f for f in (fx, fy, fz) if f != "1"]
+                        else:
+                            fac = []
+                        wterms.append((t, u, v, fac))
+            names = []
+            for (t, u, v, fac) in wterms:
+                if fac:
+                    nm = "v_%d_%d_%d_%d_%d" % (ia, ib, t, u, v)
+                    w.line("const T %s = %s;" % (nm, " * ".join(fac)))
+                    names.append((t, u, v, nm))
+                else:
+                    names.append((t, u, v, None))
+            for (ci, di) in cds:
+                s = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d_%d" % (ci, di, t, u, v)
+                               for (t, u, v, nm) in names)
+                idx = (ia * NB + ib) * (CC * ND) + ci * ND + di
+                w.line("I[%d] += double(%s);" % (idx, s))
+    w.close("}")  # ip loop
+    w.close("}")  # eri
+    # ---- digestion of one chunk for one density
+    w.line("// digest chunk ch of I into J/K of one density (symmetric X)")
+    w.open("static __device__ __forceinline__ void digest(const double (&I)[%d], const int ch, "
+           "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
+           "int cC, int cD, double sJ, double sK, bool doJ, bool doK, double (&jab)[%d]) {"
+           % (NA * NB * CC * ND, NA * NB))
+    w.line("const int c0 = ch * %d;" % CC)
+    w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
+    w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
+
+    def Iv(a, b, ci, d):
+        return "I[%d]" % ((a * NB + b) * (CC * ND) + ci * ND + d)
+    w.open("if (doJ) {")
+    # J_ab += sum_cd I D[d,c]  (register, reduced by the caller)
+    for ci in range(CC):
+        for d in range(ND):
+            w.line("const double dcd_%d_%d = ld(cD + %d, cC + c0 + %d);" % (ci, d, d, ci))
+    for a in range(NA):
+        for b in range(NB):
+            s = " + ".join("%s * dcd_%d_%d" % (Iv(a, b, ci, d), ci, d)
+                           for ci in range(CC) for d in range(ND))
+            w.line("jab[%d] += %s;" % (a * NB + b, s))
+    # J_cd += sum_ab I D[a,b]
+    for a in range(NA):
+        for b in range(NB):
+            w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a, b, a, b))
+    for ci in range(CC):
+        for d in range(ND):
+            s = " + ".join("%s * dab_%d_%d" % (Iv(a, b, ci, d), a, b)
+                           for a in range(NA) for b in range(NB))
+            w.line("add(cC + c0 + %d, cD + %d, sJ * (%s));" % (ci, d, s))
+    w.close()
+    w.open("if (doK) {")
+    # K_ac += sum_bd I D[d,b]
+    for b in range(NB):
+        for d in range(ND):
+            w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b, d, b))
+    for a in range(NA):
+        for ci in range(CC):
+            s = " + ".join("%s * ddb_%d_%d" % (Iv(a, b, ci, d), d, b)
+                           for b in range(NB) for d in range(ND))
+            w.line("add(cA + %d, cC + c0 + %d, sK * (%s));" % (a, ci, s))
+    # K_bd += sum_ac I D[a,c]
+    for a in range(NA):
+        for ci in range(CC):
+            w.line("const double dac_%d_%d = ld(cA + %d, cC + c0 + %d);" % (a, ci, a, ci))
+    for b in range(NB):
+        for d in range(ND):
+            s = " + ".join("%s * dac_%d_%d" % (Iv(a, b, ci, d), a, ci)
+                           for a in range(NA) for ci in range(CC))
+            w.line("add(cB + %d, cD + %d, sK * (%s));" % (b, d, s))
+    # K_ad += sum_bc I D[b,c]
+    for b in range(NB):
+        for ci in range(CC):
+            w.line("const double dbc_%d_%d = ld(cB + %d, cC + c0 + %d);" % (b, ci, b, ci))
+    for a in range(NA):
+        for d in range(ND):
+            s = " + ".join("%s * dbc_%d_%d" % (Iv(a, b, ci, d), b, ci)
+                           for b in range(NB) for ci in range(CC))
+            w.line("add(cA + %d, cD + %d, sK * (%s));" % (a, d, s))
+    # K_bc += sum_ad I D[a,d]
+    for a in range(NA):
+        for d in range(ND):
+            w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a, d, a, d))
+    for b in range(NB):
+        for ci in range(CC):
+            s = " + ".join("%s * dad_%d_%d" % (Iv(a, b, ci, d), a, d)
+                           for a in range(NA) for d in range(ND))
+            w.line("add(cB + %d, cC + c0 + %d, sK * (%s));" % (b, ci, s))
+    w.close()
+    w.close("}")  # digest
+    w.close("};")
+    return "\n".join(w.lines), name
+
+
+def main(out_path):
+    pclasses = [(a, b) for a in range(LMAX_FAST + 1) for b in range(a + 1)]
+    chunks = ["// Generated by gen_jk.py -- do not edit.",
+              "#pragma once", '#include "../cqf_common.cuh"', "namespace cqf {", ""]
+    table = []
+    for i, c1 in enumerate(pclasses):
+        for c2 in pclasses[:i + 1]:
+            bra, ket = orientation(c1, c2)
+            code, name = gen_class(bra[0], bra[1], ket[0], ket[1])
+            chunks.append(code)
+            chunks.append("")
+            table.append((bra, ket, name))
+    # dispatcher over (bra class, ket class) as stored in the basis buckets
+    chunks.append("// (bra la, lb, ket lc, ld) of each generated class")
+    chunks.append("#define CQF_GEN_JK_CLASSES(X) \\")
+    chunks.append(" \\\n".join("  X(%d, %d, %d, %d, GenJK_%s)" % (b[0], b[1], k[0], k[1], n)
+                              for (b, k, n) in table))
+    chunks.append("")
+    chunks.append("}  // namespace cqf")
+    txt = "\n".join(chunks) + "\n"
+    os.makedirs(os.path.dirname(out_path), exist_ok=True)
+    if not os.path.exists(out_path) or open(out_path).read() != txt:
+        with open(out_path, "w") as f:
+            f.write(txt)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(
+        os.path.dirname(os.path.abspath(__file__)), "gen", "cqf_gen_jk.cuh"))
