@@ -19,8 +19,9 @@ CQF_FP64, CQF_MIXED = 0, 1
 # every entry point declared in include/cqfock.h
 EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
-           "cqf_two_body_contract",
+           "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
            "cqf_last_error")
+NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 
 class CqfShell(C.Structure):
@@ -87,6 +88,8 @@ def lib():
                                         C.c_int, C.POINTER(CqfOpts),
                                         C.POINTER(CqfStats)]
     L.cqf_two_body_contract.restype = C.c_int
+    L.cqf_two_body_contract_noalloc.argtypes = L.cqf_two_body_contract.argtypes
+    L.cqf_two_body_contract_noalloc.restype = C.c_int
     L.cqf_last_error.argtypes = []
     L.cqf_last_error.restype = C.c_char_p
     _lib = L

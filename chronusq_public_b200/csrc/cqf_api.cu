@@ -18,10 +18,16 @@ namespace {
 
 thread_local std::string g_err;
 
+}  // namespace
+
+namespace cqf {
 cqf_status fail(cqf_status s, const std::string& msg) {
   g_err = msg;
   return s;
 }
+}  // namespace cqf
+
+namespace {
 
 #define CQF_CUDA(call)                                                                 \
   do {                                                                                 \
@@ -702,12 +708,6 @@ cqf_status cqf_basis_one_electron(cqf_basis* B, double* S, double* T) {
 }  // extern "C"
 
 namespace cqf {
-
-// Workspace layout of one contraction (in doubles, each part 256-B aligned):
-// [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
-struct WsLayout {
-  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, total;
-};
 
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   const int cw = opts.is_complex ? 2 : 1;

@@ -45,6 +45,21 @@ struct JKLaunch {
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
 };
 
+// Sets the thread's last-error text and returns s (cqf_api.cu).
+cqf_status fail(cqf_status s, const std::string& msg);
+
+// Workspace layout of one contraction (in doubles, each part 256-B aligned):
+// [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
+struct WsLayout {
+  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, total;
+};
+WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
+cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat);
+// The contraction on a caller-provided device workspace of ws_layout().total
+// doubles; the caller holds B->mu and has made B's device current.
+cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
+                         const cqf_opts& opts, cqf_stats* stats, double* ws);
+
 }  // namespace cqf
 
 struct cqf_basis {

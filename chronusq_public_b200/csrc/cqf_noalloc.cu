@@ -1,0 +1,84 @@
+// cqf_two_body_contract_noalloc: the direct J/K contraction for callers that
+// must not allocate device memory during the call.
+//
+// Who cannot allocate: code running while a CUDA stream is being captured
+// into a graph (cudaMalloc/cudaFree are not allowed there), host code that
+// runs inside a framework that owns the whole device memory pool and forbids
+// side allocations (e.g. a serving engine that has reserved HBM up front), and
+// latency-critical loops that cannot afford the implicit device
+// synchronisation of cudaFree.  cqf_two_body_contract grows a per-basis
+// workspace with cudaMalloc on first use; this entry point instead uses one
+// fixed array compiled into the library.
+//
+// The scratch is a file-scope __device__ array of CQF_NOALLOC_SCRATCH_BYTES
+// (32 MiB).  Every GPU that loads the library holds it until the process
+// exits.  Calls whose workspace (Cartesian densities and accumulators, shell
+// block norms, and for host pointers the device copies of X and AX) exceeds
+// it are rejected with CQF_EINVAL.  All calls share the one array and it keeps
+// the last call's contents; everything that must start at zero is cleared by
+// the call itself.  Two calls that overlap on the GPU (different streams or
+// host threads with different bases) race on the array: serialise them.
+#include <cstdio>
+#include <mutex>
+
+#include "cqf_internal.hpp"
+
+namespace {
+
+constexpr size_t kScratchDoubles = CQF_NOALLOC_SCRATCH_BYTES / sizeof(double);
+
+// The scratch array.  In host code its name is a host-side stand-in, not a
+// device address: its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_addr_mu;
+double* g_addr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on `device`, resolved once per device
+// with that device current (the caller has made it current).
+cqf_status scratch_address(int device, double** out) {
+  if (device < 0 || device >= kMaxDevices)
+    return cqf::fail(CQF_EINVAL, "cqf_two_body_contract_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_addr_mu);
+  if (!g_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return cqf::fail(CQF_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") +
+                                      cudaGetErrorString(e));
+    g_addr[device] = static_cast<double*>(p);
+  }
+  *out = g_addr[device];
+  return CQF_OK;
+}
+
+}  // namespace
+
+extern "C" cqf_status cqf_two_body_contract_noalloc(cqf_basis* B, const cqf_contraction* list,
+                                                    int nMat, const cqf_opts* optsIn,
+                                                    cqf_stats* stats) {
+  cqf::fail(CQF_OK, "");
+  cqf_status s = cqf::check_contract_args(B, list, nMat);
+  if (s != CQF_OK) return s;
+  cqf_opts opts;
+  cqf_opts_default(&opts);
+  if (optsIn) opts = *optsIn;
+  const size_t need = cqf::ws_layout(B, nMat, opts).total;
+  if (need > kScratchDoubles) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg,
+                  "cqf_two_body_contract_noalloc: this call needs %zu bytes of scratch, the "
+                  "fixed scratch array holds %zu bytes (use cqf_two_body_contract)",
+                  need * sizeof(double), (size_t)CQF_NOALLOC_SCRATCH_BYTES);
+    return cqf::fail(CQF_EINVAL, msg);
+  }
+  std::lock_guard<std::mutex> lk(B->mu);
+  cudaError_t e = cudaSetDevice(B->device);
+  if (e != cudaSuccess)
+    return cqf::fail(CQF_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  double* ws = nullptr;
+  s = scratch_address(B->device, &ws);
+  if (s != CQF_OK) return s;
+  return cqf::contract_core(B, list, nMat, opts, stats, ws);
+}

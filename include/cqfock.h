@@ -113,6 +113,24 @@ cqf_status cqf_basis_one_electron(cqf_basis* basis, double* S, double* T);
 cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
                                  const cqf_opts* opts, cqf_stats* stats);
 
+/* Size of the fixed scratch array of cqf_two_body_contract_noalloc. */
+#define CQF_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* Same contraction as cqf_two_body_contract, but it allocates no device
+ * memory: its scratch is one fixed CQF_NOALLOC_SCRATCH_BYTES array compiled
+ * into the library (held by every GPU that loads the library until exit).
+ * No counterpart in the reference (ChronusQ takes scratch from its memory
+ * manager); it is for callers that cannot call cudaMalloc during the call,
+ * e.g. while capturing a CUDA graph or inside a framework that owns all
+ * device memory.  The basis must already exist (cqf_basis_create allocates).
+ * Calls needing more scratch than the array holds return CQF_EINVAL.  The
+ * first call on a device resolves the array's device address; make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents (each call clears what must start at zero);
+ * calls that overlap on the GPU race on it and must be serialised. */
+cqf_status cqf_two_body_contract_noalloc(cqf_basis* basis, const cqf_contraction* list, int n,
+                                         const cqf_opts* opts, cqf_stats* stats);
+
 /* Text of the last error on this thread ("" if none). */
 const char* cqf_last_error(void);
 
