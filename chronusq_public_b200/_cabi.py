@@ -20,6 +20,7 @@ CQF_FP64, CQF_MIXED = 0, 1
 EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
            "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
+           "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
            "cqf_last_error")
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
@@ -90,6 +91,13 @@ def lib():
     L.cqf_two_body_contract.restype = C.c_int
     L.cqf_two_body_contract_noalloc.argtypes = L.cqf_two_body_contract.argtypes
     L.cqf_two_body_contract_noalloc.restype = C.c_int
+    L.cqf_graph_create.argtypes = [C.c_void_p, C.POINTER(CqfContraction), C.c_int,
+                                   C.POINTER(CqfOpts), C.POINTER(C.c_void_p)]
+    L.cqf_graph_create.restype = C.c_int
+    L.cqf_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+    L.cqf_graph_launch.restype = C.c_int
+    L.cqf_graph_destroy.argtypes = [C.c_void_p]
+    L.cqf_graph_destroy.restype = C.c_int
     L.cqf_last_error.argtypes = []
     L.cqf_last_error.restype = C.c_char_p
     _lib = L

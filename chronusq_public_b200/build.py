@@ -55,7 +55,7 @@ def _compile(src, verbose):
 def generate(verbose: bool = False):
     """Runs the kernel generators (csrc/gen_*.py -> csrc/gen/*.cuh)."""
     for gen in sorted(glob.glob(os.path.join(CSRC, "gen_*.py"))):
-        out = os.path.join(CSRC, "gen", "cqf_" + os.path.basename(gen)[4:-3] + ".cuh")
+        out = os.path.join(CSRC, "gen", "cqf_" + os.path.basename(gen)[:-3] + ".cuh")
         if (not os.path.exists(out)
                 or os.path.getmtime(out) < os.path.getmtime(gen)):
             if verbose:

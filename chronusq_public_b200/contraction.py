@@ -103,6 +103,57 @@ def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
+class ContractionGraph:
+    """A contraction captured as a CUDA graph (``cqf_graph_create``): X and AX
+    (CUDA tensors, column-major) are bound at capture; every ``launch`` adds
+    G[X] into AX on ``stream`` without synchronising."""
+
+    def __init__(self, tpi: DirectTPI, matList, precision="fp64",
+                 fp32_cutoff=0.0, screen=True):
+        self.tpi = tpi
+        n = len(matList)
+        arr = (_cabi.CqfContraction * n)()
+        is_c = matList[0].X.is_complex()
+        N = tpi.nbasis
+        for i, c in enumerate(matList):
+            for t in (c.X, c.AX):
+                if not (_is_torch(t) and t.is_cuda and tuple(t.shape) == (N, N)
+                        and t.stride() == (1, N)):
+                    raise ValueError("graph matrices must be column-major CUDA "
+                                     "tensors of shape (N, N)")
+            arr[i].X = C.c_void_p(c.X.data_ptr())
+            arr[i].AX = C.c_void_p(c.AX.data_ptr())
+            arr[i].hermitian = 1 if c.HER else 0
+            arr[i].type = int(c.contType)
+        self._keep = list(matList)
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.is_complex = 1 if is_c else 0
+        opts.screen = 1 if screen else 0
+        opts.device_pointers = 1
+        opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
+        opts.fp32_cutoff = float(fp32_cutoff)
+        h = C.c_void_p()
+        _cabi.check(_cabi.lib().cqf_graph_create(tpi.handle, arr, n, C.byref(opts),
+                                                 C.byref(h)))
+        self.handle = h
+
+    def launch(self, stream=None):
+        _cabi.check(_cabi.lib().cqf_graph_launch(
+            self.handle, C.c_void_p(stream) if stream else None))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _cabi.lib().cqf_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GTODirectTPIContraction:
     """``GTODirectTPIContraction<MatsT,double>`` on the GPU."""
 

@@ -50,8 +50,8 @@ namespace {
 // aointegrals_onee_inhouse.cxx:79-116, with a tighter series tolerance).
 void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
   const int M = BOYS_MMAX;
-  t64.assign((size_t)BOYS_NPTS * (M + 1), 0.0);
-  t32.assign((size_t)BOYS_NPTS * (M + 1), 0.0f);
+  t64.assign((size_t)BOYS_NPTS * BOYS_ROW, 0.0);
+  t32.assign((size_t)BOYS_NPTS * BOYS_ROW, 0.0f);
   for (int j = 0; j < BOYS_NPTS; j++) {
     long double T = (long double)j * BOYS_DT;
     long double term = 1.0L / (2 * M + 1), sum = term;
@@ -65,9 +65,11 @@ void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
     col[M] = F;
     for (int m = M - 1; m >= 0; m--) col[m] = (2.0L * T * col[m + 1] + eT) / (2 * m + 1);
     for (int m = 0; m <= M; m++) {
-      t64[(size_t)j * (M + 1) + m] = (double)col[m];
-      t32[(size_t)j * (M + 1) + m] = (float)col[m];
+      t64[(size_t)j * BOYS_ROW + m] = (double)col[m];
+      t32[(size_t)j * BOYS_ROW + m] = (float)col[m];
     }
+    t64[(size_t)j * BOYS_ROW + M + 1] = (double)eT;
+    t32[(size_t)j * BOYS_ROW + M + 1] = (float)eT;
   }
 }
 
@@ -255,13 +257,13 @@ __global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double*
       double ca = prim[nprimTot + A.prim_off + ia], cb = prim[nprimTot + B.prim_off + jb];
       PrimPairDev r;
       r.p = a + b;
-      r.K = ca * cb * exp(-a * b / r.p * AB2);
+      r.Kp = ca * cb * exp(-a * b / r.p * AB2) / r.p;
       for (int x = 0; x < 3; x++) {
         r.P[x] = (a * A.O[x] + b * B.O[x]) / r.p;
         r.PA[x] = r.P[x] - A.O[x];
         r.PB[x] = r.P[x] - B.O[x];
       }
-      r.pad = 0.0;
+      r.o2p = 0.5 / r.p;
       pp[idx] = r;
     }
 }
@@ -451,6 +453,7 @@ void free_basis(cqf_basis* B) {
   cudaFree(B->d_ws);
   cudaFree(B->d_counters);
   cudaFree(B->d_flags);
+  if (B->h_flags) cudaFreeHost(B->h_flags);
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -587,11 +590,19 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
                                                                  d_tmp, B->npair, B->d_pp);
   CQF_CUDA(cudaMalloc(&B->d_schwarz, (size_t)nshell * nshell * sizeof(double)));
   CQF_CUDA(cudaMemsetAsync(B->d_schwarz, 0, (size_t)nshell * nshell * sizeof(double), B->stream));
-  for (int c = 0; c < NCLS; c++)
-    if (B->cls_cnt[c] > 0)
+  double* d_diag = nullptr;
+  CQF_CUDA(cudaMalloc(&d_diag, std::max(1, B->npair) * 36 * sizeof(double)));
+  for (int c = 0; c < NCLS; c++) {
+    if (B->cls_cnt[c] <= 0) continue;
+    int la, lb;
+    class_ls(c, la, lb);
+    if (!launch_schwarz_fast(la, lb, d_tmp, B->d_pp, B->d_boys64, B->d_sph, B->d_sphOff,
+                             B->d_shells, B->cls_beg[c], B->cls_cnt[c], nshell, B->d_schwarz,
+                             d_tmp, d_diag + (size_t)B->cls_beg[c] * 36, B->stream))
       schwarz_kernel<<<grid1(B->cls_cnt[c], 64), 64, 0, B->stream>>>(
           d_tmp, B->d_pp, B->d_boys64, B->d_sph, B->d_sphOff, B->d_shells, B->cls_beg[c],
           B->cls_cnt[c], nshell, B->d_schwarz, d_tmp);
+  }
   CQF_CUDA(cudaGetLastError());
 
   // sort each class by Schwarz bound, descending (stable: ties stay in
@@ -629,8 +640,10 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   cudaFree(vout);
   cudaFree(d_cub);
   cudaFree(d_tmp);
+  cudaFree(d_diag);
   CQF_CUDA(cudaMalloc(&B->d_counters, 8 * sizeof(unsigned long long)));
   CQF_CUDA(cudaMalloc(&B->d_flags, MAXMAT * sizeof(int)));
+  CQF_CUDA(cudaMallocHost(&B->h_flags, MAXMAT * sizeof(int)));
   return CQF_OK;
 }
 
@@ -748,7 +761,8 @@ cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, 
 // ws_layout(...).total doubles (device memory).  Caller holds B->mu and has
 // made B's device current.
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
-                         const cqf_opts& opts, cqf_stats* stats, double* ws) {
+                         const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
+                         const int* d_flags_pre) {
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const int cw = opts.is_complex ? 2 : 1;
@@ -758,7 +772,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   const bool host = !opts.device_pointers;
   const size_t oX = Lw.oX, oAX = Lw.oAX, oXc = Lw.oXc, oAc = Lw.oAc, oNm = Lw.oNm,
                oNmM = Lw.oNmM, oG = Lw.oG;
-  CQF_CUDA(cudaEventRecord(B->ev0, st));
+  if (!capture) CQF_CUDA(cudaEventRecord(B->ev0, st));
   std::vector<const double*> Xd(nMat);
   std::vector<double*> AXd(nMat);
   for (int m = 0; m < nMat; m++) {
@@ -774,11 +788,16 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       AXd[m] = static_cast<double*>(list[m].AX);
     }
   }
-  std::vector<int> flags(nMat);
-  for (int m = 0; m < nMat; m++)
-    flags[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
-  CQF_CUDA(cudaMemcpyAsync(B->d_flags, flags.data(), nMat * sizeof(int), cudaMemcpyHostToDevice,
-                           st));
+  // per-matrix flags: uploaded here through pinned staging (every earlier
+  // call on this basis has synchronised), or already on the device (graphs)
+  const int* d_flags = d_flags_pre;
+  if (!d_flags) {
+    for (int m = 0; m < nMat; m++)
+      B->h_flags[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
+    CQF_CUDA(cudaMemcpyAsync(B->d_flags, B->h_flags, nMat * sizeof(int), cudaMemcpyHostToDevice,
+                             st));
+    d_flags = B->d_flags;
+  }
   CQF_CUDA(cudaMemsetAsync(B->d_counters, 0, 8 * sizeof(unsigned long long), st));
   CQF_CUDA(cudaMemsetAsync(ws + oG, 0, 4 * sizeof(double), st));
 
@@ -813,7 +832,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.nMat = nMat;
   a.cplx = opts.is_complex;
   a.ncart = nc;
-  a.flags = B->d_flags;
+  a.flags = d_flags;
   a.Xc = ws + oXc;
   a.Ac = ws + oAc;
   a.precision = opts.precision;
@@ -847,6 +866,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
     for (int m = 0; m < nMat; m++)
       CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXd[m], matN * sizeof(double), cudaMemcpyDeviceToHost,
                                st));
+  if (capture) return CQF_OK;
   CQF_CUDA(cudaEventRecord(B->ev1, st));
   unsigned long long cnt[4] = {0, 0, 0, 0};
   CQF_CUDA(cudaMemcpyAsync(cnt, B->d_counters, 4 * sizeof(unsigned long long),
@@ -879,7 +899,8 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int 
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_CUDA(cudaSetDevice(B->device));
   CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
-  return contract_core(B, list, nMat, opts, stats, static_cast<double*>(B->d_ws));
+  return contract_core(B, list, nMat, opts, stats, static_cast<double*>(B->d_ws), false,
+                       nullptr);
 }
 
 }  // extern "C"

@@ -9,8 +9,8 @@
 //   PrimPairDev[nprimpair] primitive-pair data (p, K, P, PA, PB), 96 B each,
 //                          contiguous per shell pair so one pair's primitives
 //                          are one coalesced run
-//   boys table             F_m(T_j), T_j = j*0.05, m = 0..BOYS_MMAX (FP64 and
-//                          an FP32 copy), 186 KB, L2 resident
+//   boys table             F_m(T_j), T_j = j*0.05, m = 0..BOYS_MMAX, and
+//                          exp(-T_j) (FP64 and an FP32 copy), 197 KB, L2 resident
 //   Cartesian-AO densities / accumulators, nMat x ncart x ncart
 #pragma once
 
@@ -24,6 +24,7 @@ constexpr int BOYS_MMAX = 32;      // tabulated Boys orders
 constexpr double BOYS_DT = 0.05;   // grid spacing of the Taylor table
 constexpr double BOYS_TMAX = 36.0; // above: F0 = sqrt(pi/T)/2 + upward recursion
 constexpr int BOYS_NPTS = 724;     // grid points 0 .. TMAX/DT (+ margin)
+constexpr int BOYS_ROW = BOYS_MMAX + 2;  // F_0..F_MMAX, then exp(-T_j)
 constexpr int BOYS_K64 = 8;        // Taylor terms k = 0..8 (FP64, |dT| <= 0.025)
 constexpr int BOYS_K32 = 4;        // Taylor terms k = 0..4 (FP32)
 
@@ -80,9 +81,9 @@ struct PairDev {
 };
 
 struct PrimPairDev {
-  double p, K;       // exponent sum; c_a c_b exp(-mu |AB|^2)
+  double p, Kp;      // exponent sum; c_a c_b exp(-mu |AB|^2) / p
   double P[3], PA[3], PB[3];
-  double pad;
+  double o2p;        // 1 / (2p)
 };
 
 // ----------------------------------------------------------------- Boys
@@ -95,13 +96,18 @@ __device__ __forceinline__ void boys_f64(double T, double* F,
   if (T < BOYS_TMAX) {
     int j = __double2int_rn(T * (1.0 / BOYS_DT));
     double dT = j * BOYS_DT - T;
-    const double* row = tab + j * (BOYS_MMAX + 1) + L;
-    double s = __ldg(row + BOYS_K64);
+    const double* row = tab + j * BOYS_ROW;
+    double s = __ldg(row + L + BOYS_K64);
 #pragma unroll
-    for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0 / (k + 1));
+    for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + L + k) + s * dT * (1.0 / (k + 1));
     F[L] = s;
     if (L > 0) {
-      double e = exp(-T), t2 = 2.0 * T;
+      // exp(-T) = exp(-T_j) exp(dT), |dT| <= DT/2, Taylor to dT^8
+      double e = 1.0 + dT * (1.0 / 8);
+#pragma unroll
+      for (int k = 7; k >= 1; k--) e = 1.0 + dT * e * (1.0 / k);
+      e *= __ldg(row + BOYS_MMAX + 1);
+      const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
     }
@@ -121,7 +127,7 @@ __device__ __forceinline__ void boys_f32(float T, float* F, const float* __restr
   if (T < (float)BOYS_TMAX) {
     int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
     float dT = j * (float)BOYS_DT - T;
-    const float* row = tab + j * (BOYS_MMAX + 1) + L;
+    const float* row = tab + j * BOYS_ROW + L;
     float s = __ldg(row + BOYS_K32);
 #pragma unroll
     for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));

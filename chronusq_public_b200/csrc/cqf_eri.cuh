@@ -91,7 +91,7 @@ __device__ __forceinline__ void boys_rt<double>(int L, double T, double* F, cons
   if (T < BOYS_TMAX) {
     int j = __double2int_rn(T * (1.0 / BOYS_DT));
     double dT = j * BOYS_DT - T;
-    const double* row = tab + j * (BOYS_MMAX + 1) + L;
+    const double* row = tab + j * BOYS_ROW + L;
     double s = __ldg(row + BOYS_K64);
 #pragma unroll
     for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0 / (k + 1));
@@ -113,7 +113,7 @@ __device__ __forceinline__ void boys_rt<float>(int L, float T, float* F, const f
   if (T < (float)BOYS_TMAX) {
     int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
     float dT = j * (float)BOYS_DT - T;
-    const float* row = tab + j * (BOYS_MMAX + 1) + L;
+    const float* row = tab + j * BOYS_ROW + L;
     float s = __ldg(row + BOYS_K32);
 #pragma unroll
     for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));
@@ -178,7 +178,7 @@ __device__ void eri_column_rt(int la, int lb, int lc, int ld, int c, int d, cons
       const T X = T(A.P[0]) - T(B.P[0]), Y = T(A.P[1]) - T(B.P[1]), Z = T(A.P[2]) - T(B.P[2]);
       const T pq = p + q, alpha = p * q / pq;
       const T Targ = alpha * (X * X + Y * Y + Z * Z);
-      const T pref = PI52x2 / (p * q * sqrt(pq)) * T(A.K) * T(B.K);
+      const T pref = PI52x2 / sqrt(pq) * T(A.Kp) * T(B.Kp);
       boys_rt<T>(L, Targ, F, boys);
       hermite_R_rt<T>(L, alpha, X, Y, Z, F, Rv);
       const T* ex = Ec[0] + (cx * (ld + 1) + dx) * Lcd1;

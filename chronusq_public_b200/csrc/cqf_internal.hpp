@@ -57,8 +57,11 @@ WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
 cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat);
 // The contraction on a caller-provided device workspace of ws_layout().total
 // doubles; the caller holds B->mu and has made B's device current.
+// With capture = true nothing synchronises or reads back (stream capture);
+// d_flags_pre: per-matrix flags already on the device (else uploaded here).
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
-                         const cqf_opts& opts, cqf_stats* stats, double* ws);
+                         const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
+                         const int* d_flags_pre);
 
 }  // namespace cqf
 
@@ -88,7 +91,8 @@ struct cqf_basis {
   size_t ws_bytes = 0;
   void* d_ws = nullptr;
   unsigned long long* d_counters = nullptr;
-  int* d_flags = nullptr;
+  int* d_flags = nullptr;                // MAXMAT per-matrix flags
+  int* h_flags = nullptr;                // pinned staging of the flags
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::mutex mu;
 };

@@ -25,14 +25,19 @@ __device__ __forceinline__ void warp_sum(double (&v)[N]) {
 
 // FP64 launch: quartets with bound >= cut (all when cut <= 0); FP32 launch:
 // quartets with thresh <= bound < cut.  The FP64 launch also counts the
-// visited / screened quartets.
+// visited / screened quartets.  blockIdx.y = chunk * ketTiles + tile: every
+// thread of a block runs the same chunk (one code path per block), and the
+// chunks of one quartet run in parallel in different blocks.
 template <class GC, typename T>
 __global__ void __launch_bounds__(JK_THREADS)
     jk_fast_kernel(const JKLaunch a) {
   constexpr int NA = ncart(GC::LA), NB = ncart(GC::LB);
+  constexpr int NCH = GC::NCHUNK;
   constexpr bool IS64 = sizeof(T) == 8;
   const int ib = blockIdx.x;
-  const int jk = blockIdx.y * JK_THREADS + threadIdx.x;
+  const int ketTiles = (a.nKet + JK_THREADS - 1) / JK_THREADS;
+  const int ch = blockIdx.y / ketTiles, tile = blockIdx.y % ketTiles;
+  const int jk = tile * JK_THREADS + threadIdx.x;
   const PairDev P = a.pairs[a.braBeg + ib];
   const int ns = a.nShell;
   const double cut = (a.precision == 1) ? a.fp32_cut : 0.0;
@@ -43,11 +48,11 @@ __global__ void __launch_bounds__(JK_THREADS)
     Q = a.pairs[a.ketBeg + jk];
     visited = !(a.same && Q.lex > P.lex);
   }
-  const double tileMax =
-      __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + blockIdx.y * JK_THREADS].Q;
+  const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * JK_THREADS].Q;
   const bool tileDead = a.screen && tileMax < a.thresh;
+  const bool counter = IS64 && ch == 0;  // one count per quartet
   if (tileDead || (!IS64 && cut <= 0.0)) {
-    if (IS64) count_block(a.counters, visited, visited, false, false);
+    if (IS64) count_block(a.counters, counter && visited, counter && visited, false, false);
     return;
   }
   int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
@@ -65,9 +70,9 @@ __global__ void __launch_bounds__(JK_THREADS)
     work = !screened && (IS64 ? !lo : lo);
   }
   if (IS64)
-    count_block(a.counters, visited, screened, false, work);
+    count_block(a.counters, counter && visited, counter && screened, false, counter && work);
   else
-    count_block(a.counters, false, false, work, false);
+    count_block(a.counters, false, false, ch == 0 && work, false);
   if (!__syncthreads_or(work)) return;
 
   const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
@@ -77,64 +82,169 @@ __global__ void __launch_bounds__(JK_THREADS)
   const size_t matStride = (size_t)a.ncart * a.ncart;
   const T* boys = IS64 ? reinterpret_cast<const T*>(a.boys64)
                        : reinterpret_cast<const T*>(a.boys32);
+  double I[GC::NI];
+  if (work) {
+    GC::template eri<T>(P, Q, a.pp, boys, ch, I);
+  } else {
+#pragma unroll
+    for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
+  }
 #pragma unroll 1
-  for (int ch = 0; ch < GC::NCHUNK; ch++) {
-    double I[GC::NI];
-    if (work) {
-      GC::template eri<T>(P, Q, a.pp, boys, ch, I);
-    } else {
+  for (int m = 0; m < a.nMat; m++) {
+    const int fl = __ldg(a.flags + m);
+    const bool doJ = !(fl & 2), doK = (fl & 2);
+    double jab[NA * NB];
 #pragma unroll
-      for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
-    }
-#pragma unroll 1
-    for (int m = 0; m < a.nMat; m++) {
-      const int fl = __ldg(a.flags + m);
-      const bool doJ = !(fl & 2), doK = (fl & 2);
-      double jab[NA * NB];
+    for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
+    const double* X = a.Xc + m * matStride;
+    double* A = a.Ac + m * matStride;
+    GC::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work, doK && work, jab);
+    if (doJ) {
+      // every lane of the warp shares the bra pair: reduce, one atomic each
 #pragma unroll
-      for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
-      const double* X = a.Xc + m * matStride;
-      double* A = a.Ac + m * matStride;
-      GC::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work, doK && work, jab);
-      if (doJ) {
-        // every lane of the warp shares the bra pair: reduce, one atomic each
+      for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
+      warp_sum(jab);
+      if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
-        warp_sum(jab);
-        if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-          for (int i = 0; i < NA * NB; i++)
-            if (jab[i] != 0.0)
-              atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
-        }
+        for (int i = 0; i < NA * NB; i++)
+          if (jab[i] != 0.0)
+            atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
       }
     }
   }
 }
 
-// Launches the generated kernel of the class (bra bucket cb, ket bucket ck);
-// returns false when the class has no generated kernel.
+template <class GC>
+inline dim3 fast_grid(const JKLaunch& b) {
+  const int ketTiles = (b.nKet + JK_THREADS - 1) / JK_THREADS;
+  return dim3(b.nBra, (unsigned)(ketTiles * GC::NCHUNK));
+}
+
+// Launches the generated kernels of the class (la lb | lc ld) (either
+// orientation); returns false when the class has no generated kernel.
 inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, cudaStream_t st) {
   if (a.nBra == 0 || a.nKet == 0) return true;
   bool done = false;
-  auto go = [&](auto tag, bool swap) {
-    using GC = decltype(tag);
+  auto go = [&](auto tag64, auto tag32, bool swap) {
+    using G64 = decltype(tag64);
+    using G32 = decltype(tag32);
     JKLaunch b = a;
     if (swap) {
       b.braBeg = a.ketBeg; b.nBra = a.nKet;
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
     }
-    dim3 grid(b.nBra, (b.nKet + JK_THREADS - 1) / JK_THREADS);
-    jk_fast_kernel<GC, double><<<grid, JK_THREADS, 0, st>>>(b);
+    jk_fast_kernel<G64, double><<<fast_grid<G64>(b), JK_THREADS, 0, st>>>(b);
     if (b.precision == 1 && b.fp32_cut > 0.0)
-      jk_fast_kernel<GC, float><<<grid, JK_THREADS, 0, st>>>(b);
+      jk_fast_kernel<G32, float><<<fast_grid<G32>(b), JK_THREADS, 0, st>>>(b);
     done = true;
   };
-#define CQF_TRY_CLASS(A_, B_, C_, D_, NAME)                                   \
-  if (!done && la == A_ && lb == B_ && lc == C_ && ld == D_) go(NAME{}, false); \
-  if (!done && la == C_ && lb == D_ && lc == A_ && ld == B_) go(NAME{}, true);
+#define CQF_TRY_CLASS(A_, B_, C_, D_, N64, N32)                                          \
+  if (!done && la == A_ && lb == B_ && lc == C_ && ld == D_) go(N64{}, N32{}, false);    \
+  if (!done && la == C_ && lb == D_ && lc == A_ && ld == B_) go(N64{}, N32{}, true);
   CQF_GEN_JK_CLASSES(CQF_TRY_CLASS)
 #undef CQF_TRY_CLASS
+  return done;
+}
+
+// ----------------------------------------------------------- Schwarz (fast)
+// Diagonal (mu nu|mu nu) of the pairs of one class (LA, LB) with LA, LB <= 2
+// from the generated (ab|ab) code, one thread per (pair, chunk); the chunk's
+// share of each spherical diagonal element is added into diag[pair][mu][nu].
+template <class GC>
+__global__ void __launch_bounds__(JK_THREADS)
+    schwarz_diag_kernel(const PairDev* __restrict__ pairs, const PrimPairDev* __restrict__ pp,
+                        const double* __restrict__ boys, const double* __restrict__ sph,
+                        const int* __restrict__ sphOff, const ShellDev* __restrict__ shells,
+                        int beg, int n, double* diag) {
+  constexpr int NA = ncart(GC::LA), NB = ncart(GC::LB), NCH = GC::NCHUNK;
+  constexpr int CS = GC::NI / (NA * NB);
+  const long long item = (long long)blockIdx.x * JK_THREADS + threadIdx.x;
+  if (item >= (long long)n * NCH) return;
+  const int k = (int)(item / NCH), ch = (int)(item % NCH);
+  const PairDev P = pairs[beg + k];
+  const ShellDev A = shells[P.shA], B = shells[P.shB];
+  const int na = A.pure ? nsph(GC::LA) : NA, nb = B.pure ? nsph(GC::LB) : NB;
+  const double* TA = sph + sphOff[GC::LA];
+  const double* TB = sph + sphOff[GC::LB];
+  auto ta = [&](int c, int mu) { return A.pure ? TA[c * nsph(GC::LA) + mu] : (c == mu ? 1.0 : 0.0); };
+  auto tb = [&](int c, int nu) { return B.pure ? TB[c * nsph(GC::LB) + nu] : (c == nu ? 1.0 : 0.0); };
+  double I[GC::NI];
+  GC::template eri<double>(P, P, pp, boys, ch, I);
+  for (int mu = 0; mu < na; mu++)
+    for (int nu = 0; nu < nb; nu++) {
+      double s = 0.0;
+      for (int kk = 0; kk < CS; kk++) {
+        const int cd = ch * CS + kk;
+        if (cd >= NA * NB) break;
+        const double tcd = ta(cd / NB, mu) * tb(cd % NB, nu);
+        if (tcd == 0.0) continue;
+        double sab = 0.0;
+        for (int a = 0; a < NA; a++) {
+          const double t1 = ta(a, mu);
+          if (t1 == 0.0) continue;
+          for (int b = 0; b < NB; b++) sab += t1 * tb(b, nu) * I[(a * NB + b) * CS + kk];
+        }
+        s += tcd * sab;
+      }
+      if (s != 0.0) atomicAdd(diag + (size_t)k * 36 + mu * 6 + nu, s);
+    }
+}
+
+// Q = sqrt(max row sum |diag|) with rows the functions of s1
+// (aointegrals_utilities.cxx:78-104); writes the pair and the table.
+__global__ void schwarz_finish_kernel(const PairDev* __restrict__ pairs,
+                                      const ShellDev* __restrict__ shells, int beg, int n,
+                                      int nshell, const double* __restrict__ diag, double* Qtab,
+                                      PairDev* pairsOut) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const PairDev P = pairs[beg + k];
+  const ShellDev A = shells[P.shA], B = shells[P.shB];
+  const int na = A.pure ? nsph(A.l) : ncart(A.l), nb = B.pure ? nsph(B.l) : ncart(B.l);
+  const double* d = diag + (size_t)k * 36;
+  const bool swp = P.shA != P.s1;
+  double mx = 0.0;
+  if (!swp) {
+    for (int i = 0; i < na; i++) {
+      double r = 0.0;
+      for (int j = 0; j < nb; j++) r += fabs(d[i * 6 + j]);
+      mx = fmax(mx, r);
+    }
+  } else {
+    for (int j = 0; j < nb; j++) {
+      double r = 0.0;
+      for (int i = 0; i < na; i++) r += fabs(d[i * 6 + j]);
+      mx = fmax(mx, r);
+    }
+  }
+  const double q = sqrt(mx);
+  pairsOut[beg + k].Q = q;
+  Qtab[P.s1 + (size_t)P.s2 * nshell] = q;
+  Qtab[P.s2 + (size_t)P.s1 * nshell] = q;
+}
+
+// Schwarz bounds of one class with the generated code; false if the class
+// has none.  diag: n x 36 doubles (6 x 6 per pair), zeroed here.
+inline bool launch_schwarz_fast(int la, int lb, const PairDev* pairs, const PrimPairDev* pp,
+                                const double* boys, const double* sph, const int* sphOff,
+                                const ShellDev* shells, int beg, int n, int nshell, double* Qtab,
+                                PairDev* pairsOut, double* diag, cudaStream_t st) {
+  if (n <= 0) return true;
+  bool done = false;
+  auto go = [&](auto tag64) {
+    using G = decltype(tag64);
+    cudaMemsetAsync(diag, 0, (size_t)n * 36 * sizeof(double), st);
+    const long long items = (long long)n * G::NCHUNK;
+    schwarz_diag_kernel<G><<<(unsigned)((items + JK_THREADS - 1) / JK_THREADS), JK_THREADS, 0,
+                             st>>>(pairs, pp, boys, sph, sphOff, shells, beg, n, diag);
+    schwarz_finish_kernel<<<(n + 127) / 128, 128, 0, st>>>(pairs, shells, beg, n, nshell, diag,
+                                                          Qtab, pairsOut);
+    done = true;
+  };
+#define CQF_TRY_SCHWARZ(A_, B_, C_, D_, N64, N32) \
+  if (!done && A_ == la && B_ == lb && C_ == la && D_ == lb) go(N64{});
+  CQF_GEN_JK_CLASSES(CQF_TRY_SCHWARZ)
+#undef CQF_TRY_SCHWARZ
   return done;
 }
 

@@ -80,5 +80,5 @@ extern "C" cqf_status cqf_two_body_contract_noalloc(cqf_basis* B, const cqf_cont
   double* ws = nullptr;
   s = scratch_address(B->device, &ws);
   if (s != CQF_OK) return s;
-  return cqf::contract_core(B, list, nMat, opts, stats, ws);
+  return cqf::contract_core(B, list, nMat, opts, stats, ws, false, nullptr);
 }

@@ -115,71 +115,72 @@ def orientation(c1, c2):
     return (c1, c2) if g12 <= g21 else (c2, c1)
 
 
-def chunk_size(la, lb, lc, ld):
-    """c components per chunk so NAB*CC*ND + CC*ND*HAB + H(L) stays small."""
+def chunk_size(la, lb, lc, ld, prec):
+    """ket component pairs (flattened cd index) per chunk, so that the live
+    set (integral chunk + G chunk + R, in 4-byte register units) stays under
+    the budget of the precision; the integral chunk is always FP64."""
     nab = ncart(la) * ncart(lb)
-    nd = ncart(ld)
+    ncd = ncart(lc) * ncart(ld)
     hab = nherm(la + lb)
     hl = nherm(la + lb + lc + ld)
+    w = 2 if prec == 64 else 1
     best = 1
-    for cc in range(1, ncart(lc) + 1):
-        if ncart(lc) % cc:
-            continue
-        live = nab * cc * nd + cc * nd * hab + hl
-        if live <= 110:
-            best = cc
+    for cs in range(1, ncd + 1):
+        live = 2 * nab * cs + w * (cs * hab + hl)
+        if live <= 176:
+            best = cs
     return best
 
 
-def gen_class(la, lb, lc, ld):
-    """Device function computing the chunk [c0, c0+CC) of the contracted
-    Cartesian block into I_* scalars, then digesting it."""
+def gen_class(la, lb, lc, ld, prec):
+    """Struct GenJK<prec>_<class>: eri<T>() computes chunk ch (a contiguous
+    range of the flattened ket component index cd) of the contracted Cartesian
+    block; digest() adds that chunk's J/K contributions of one density."""
     w = W()
     A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
     NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
+    NAB, NCD = NA * NB, NC * ND
     lab, lcd = la + lb, lc + ld
     L = lab + lcd
-    CC = chunk_size(la, lb, lc, ld)
-    nchunk = NC // CC
+    CS = chunk_size(la, lb, lc, ld, prec)
+    nchunk = (NCD + CS - 1) // CS
+    chunks = [list(range(k * CS, min(NCD, (k + 1) * CS))) for k in range(nchunk)]
     hab = herm_list(lab)
     hall = herm_list(L)
-    name = "%d%d%d%d" % (la, lb, lc, ld)
-    w.line("// (%s%s|%s%s): NAB=%d NCD=%d L=%d, %d chunk(s) of %d c-components"
-           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], NA * NB, NC * ND,
-              L, nchunk, CC))
-    w.open("struct GenJK_%s {" % name)
+    name = "%d_%d%d%d%d" % (prec, la, lb, lc, ld)
+    w.line("// (%s%s|%s%s), FP%d build: NAB=%d NCD=%d L=%d, %d chunk(s) of <= %d cd pairs"
+           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], prec, NAB, NCD, L, nchunk, CS))
+    w.open("struct GenJK%s {" % name)
     w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
     w.line("static constexpr int NCHUNK = %d;" % nchunk)
-    w.line("static constexpr int NI = %d;  // integrals per chunk" % (NA * NB * CC * ND))
-    # ---- integral chunk
+    w.line("static constexpr int NI = %d;  // integrals per chunk" % (NAB * CS))
     w.line("template <typename T>")
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
            "const PrimPairDev* __restrict__ pp, const T* __restrict__ boys, const int ch, "
-           "double (&I)[%d]) {" % (NA * NB * CC * ND))
-    w.open("#pragma unroll")
-    w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NA * NB * CC * ND))
-    w.ind -= 1
+           "double (&I)[%d]) {" % (NAB * CS))
+    w.line("#pragma unroll")
+    w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NAB * CS))
     w.line("const T PI52x2 = T(34.986836655249725693);")
     w.line("#pragma unroll 1")
     w.open("for (int ip = 0; ip < P.npp; ip++) {")
     w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
-    w.line("const T p = T(pa.p), Kab = T(pa.K), o2p = T(0.5) / p;")
+    w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
     w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
     axes = "xyz"
     if lab > 0:
         for x in range(3):
             w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
-    # G accumulators per chunk-local cd and bra Hermite tuv
-    cds = [(ci, di) for ci in range(CC) for di in range(ND)]
-    for (ci, di) in cds:
+    for k in range(CS):
         for (t, u, v) in hab:
-            w.line("T g_%d_%d_%d_%d_%d = T(0);" % (ci, di, t, u, v))
+            w.line("T g_%d_%d_%d_%d = T(0);" % (k, t, u, v))
     w.line("#pragma unroll 1")
     w.open("for (int iq = 0; iq < Q.npp; iq++) {")
     w.line("const PrimPairDev& pb = pp[Q.pp_off + iq];")
-    w.line("const T q = T(pb.p), Kcd = T(pb.K), o2q = T(0.5) / q;")
+    w.line("const T q = T(pb.p), Kcd = T(pb.Kp), o2q = T(pb.o2p);")
     w.line("const T X = Px - T(pb.P[0]), Y = Py - T(pb.P[1]), Z = Pz - T(pb.P[2]);")
-    w.line("const T pq = p + q, alpha = p * q / pq;")
+    w.line("const T pq = p + q;")
+    w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
+    w.line("const T alpha = p * q * (rpq * rpq);")
     w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
     w.line("T F[%d];" % (L + 1))
     w.open("if constexpr (sizeof(T) == 8) {")
@@ -188,14 +189,12 @@ def gen_class(la, lb, lc, ld):
     w.ind += 1
     w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
     w.close()
-    w.line("const T pref = PI52x2 / (p * q * sqrt(pq)) * Kab * Kcd;")
-    # ket E
+    w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
     if lcd > 0:
         for x in range(3):
             w.line("const T QC%s = T(pb.PA[%d]), QD%s = T(pb.PB[%d]);" % (axes[x], x, axes[x], x))
     ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
           for x in range(3)] if lcd > 0 else None
-    # R recursion (SSA over levels)
     R = {}
     w.line("const T m2a = T(-2) * alpha;")
     pw = ["T(1)"]
@@ -223,16 +222,16 @@ def gen_class(la, lb, lc, ld):
                 nm = "r%d_%d_%d_%d" % (n, t, u, v)
                 w.line("const T %s = %s;" % (nm, e))
                 R[(n, t, u, v)] = nm
-    # G: per chunk component (c = c0 + ci), runtime chunk index resolved by switch
-    w.open("switch (ch) {")
-    for chv in range(nchunk):
-        w.open("case %d: {" % chv)
-        for (ci, di) in cds:
-            c = chv * CC + ci
+    if nchunk > 1:
+        w.open("switch (ch) {")
+    for chv, cdl in enumerate(chunks):
+        if nchunk > 1:
+            w.open("case %d: {" % chv)
+        for k, cd in enumerate(cdl):
+            c, di = divmod(cd, ND)
             cx, cy, cz = Cc[c]
             dx, dy, dz = Dd[di]
-            # ket weights for this (c,d): sign * Ex Ey Ez
-            terms = []
+            wn = []
             for ta in range(cx + dx + 1):
                 for nu in range(cy + dy + 1):
                     for ph in range(cz + dz + 1):
@@ -246,27 +245,25 @@ def gen_class(la, lb, lc, ld):
                         else:
                             fac = []
                         sgn = -1 if (ta + nu + ph) & 1 else 1
-                        terms.append((ta, nu, ph, sgn, fac))
-            wn = []
-            for (ta, nu, ph, sgn, fac) in terms:
-                nm = "w_%d_%d_%d_%d_%d" % (ci, di, ta, nu, ph)
-                expr = " * ".join(["pref"] + fac)
-                w.line("const T %s = %s%s;" % (nm, "-" if sgn < 0 else "", expr))
-                wn.append((ta, nu, ph, nm))
+                        nm = "w_%d_%d_%d_%d" % (k, ta, nu, ph)
+                        w.line("const T %s = %s%s;" % (nm, "-" if sgn < 0 else "",
+                                                        " * ".join(["pref"] + fac)))
+                        wn.append((ta, nu, ph, nm))
             for (t, u, v) in hab:
-                s = " + ".join("%s * %s" % (nm, R[(0, t + ta, u + nu, v + ph)])
-                               for (ta, nu, ph, nm) in wn)
-                w.line("g_%d_%d_%d_%d_%d += %s;" % (ci, di, t, u, v, s))
-        w.line("break;")
+                sm = " + ".join("%s * %s" % (nm, R[(0, t + ta, u + nu, v + ph)])
+                                for (ta, nu, ph, nm) in wn)
+                w.line("g_%d_%d_%d_%d += %s;" % (k, t, u, v, sm))
+        if nchunk > 1:
+            w.line("break;")
+            w.close("}")
+    if nchunk > 1:
         w.close("}")
-    w.close("}")
-    w.close("}")  # iq loop
-    # bra E and I accumulation
+    w.close("}")  # iq
     eb = [E1D(w, la, lb, "ea" + axes[x], "o2p", "PA" + axes[x], "PB" + axes[x])
           for x in range(3)] if lab > 0 else None
     for ia, (ax, ay, az) in enumerate(A):
         for ib, (bx, by, bz) in enumerate(B):
-            wterms = []
+            names = []
             for t in range(ax + bx + 1):
                 for u in range(ay + by + 1):
                     for v in range(az + bz + 1):
@@ -277,92 +274,95 @@ def gen_class(la, lb, lc, ld):
                             fac = [f for f in (fx, fy, fz) if f != "1"]
                         else:
                             fac = []
-                        wterms.append((t, u, v, fac))
-            names = []
-            for (t, u, v, fac) in wterms:
-                if fac:
-                    nm = "v_%d_%d_%d_%d_%d" % (ia, ib, t, u, v)
-                    w.line("const T %s = %s;" % (nm, " * ".join(fac)))
-                    names.append((t, u, v, nm))
-                else:
-                    names.append((t, u, v, None))
-            for (ci, di) in cds:
-                s = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d_%d" % (ci, di, t, u, v)
-                               for (t, u, v, nm) in names)
-                idx = (ia * NB + ib) * (CC * ND) + ci * ND + di
-                w.line("I[%d] += double(%s);" % (idx, s))
-    w.close("}")  # ip loop
+                        if fac:
+                            nm = "v_%d_%d_%d_%d_%d" % (ia, ib, t, u, v)
+                            w.line("const T %s = %s;" % (nm, " * ".join(fac)))
+                            names.append((t, u, v, nm))
+                        else:
+                            names.append((t, u, v, None))
+            for k in range(CS):
+                sm = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d" % (k, t, u, v)
+                                for (t, u, v, nm) in names)
+                w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+    w.close("}")  # ip
     w.close("}")  # eri
-    # ---- digestion of one chunk for one density
-    w.line("// digest chunk ch of I into J/K of one density (symmetric X)")
+    # ---- digestion
+    w.line("// J/K contributions of chunk ch for one density (symmetric X)")
     w.open("static __device__ __forceinline__ void digest(const double (&I)[%d], const int ch, "
            "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
            "int cC, int cD, double sJ, double sK, bool doJ, bool doK, double (&jab)[%d]) {"
-           % (NA * NB * CC * ND, NA * NB))
-    w.line("const int c0 = ch * %d;" % CC)
+           % (NAB * CS, NAB))
     w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
     w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
+    if nchunk > 1:
+        w.open("switch (ch) {")
+    for chv, cdl in enumerate(chunks):
+        if nchunk > 1:
+            w.open("case %d: {" % chv)
+        els = [(k,) + divmod(cd, ND) for k, cd in enumerate(cdl)]  # (k, c, d)
+        cs_ = sorted(set(c for (_, c, _) in els))
+        ds_ = sorted(set(d for (_, _, d) in els))
 
-    def Iv(a, b, ci, d):
-        return "I[%d]" % ((a * NB + b) * (CC * ND) + ci * ND + d)
-    w.open("if (doJ) {")
-    # J_ab += sum_cd I D[d,c]  (register, reduced by the caller)
-    for ci in range(CC):
-        for d in range(ND):
-            w.line("const double dcd_%d_%d = ld(cD + %d, cC + c0 + %d);" % (ci, d, d, ci))
-    for a in range(NA):
-        for b in range(NB):
-            s = " + ".join("%s * dcd_%d_%d" % (Iv(a, b, ci, d), ci, d)
-                           for ci in range(CC) for d in range(ND))
-            w.line("jab[%d] += %s;" % (a * NB + b, s))
-    # J_cd += sum_ab I D[a,b]
-    for a in range(NA):
-        for b in range(NB):
-            w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a, b, a, b))
-    for ci in range(CC):
-        for d in range(ND):
-            s = " + ".join("%s * dab_%d_%d" % (Iv(a, b, ci, d), a, b)
-                           for a in range(NA) for b in range(NB))
-            w.line("add(cC + c0 + %d, cD + %d, sJ * (%s));" % (ci, d, s))
-    w.close()
-    w.open("if (doK) {")
-    # K_ac += sum_bd I D[d,b]
-    for b in range(NB):
-        for d in range(ND):
-            w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b, d, b))
-    for a in range(NA):
-        for ci in range(CC):
-            s = " + ".join("%s * ddb_%d_%d" % (Iv(a, b, ci, d), d, b)
-                           for b in range(NB) for d in range(ND))
-            w.line("add(cA + %d, cC + c0 + %d, sK * (%s));" % (a, ci, s))
-    # K_bd += sum_ac I D[a,c]
-    for a in range(NA):
-        for ci in range(CC):
-            w.line("const double dac_%d_%d = ld(cA + %d, cC + c0 + %d);" % (a, ci, a, ci))
-    for b in range(NB):
-        for d in range(ND):
-            s = " + ".join("%s * dac_%d_%d" % (Iv(a, b, ci, d), a, ci)
-                           for a in range(NA) for ci in range(CC))
-            w.line("add(cB + %d, cD + %d, sK * (%s));" % (b, d, s))
-    # K_ad += sum_bc I D[b,c]
-    for b in range(NB):
-        for ci in range(CC):
-            w.line("const double dbc_%d_%d = ld(cB + %d, cC + c0 + %d);" % (b, ci, b, ci))
-    for a in range(NA):
-        for d in range(ND):
-            s = " + ".join("%s * dbc_%d_%d" % (Iv(a, b, ci, d), b, ci)
-                           for b in range(NB) for ci in range(CC))
-            w.line("add(cA + %d, cD + %d, sK * (%s));" % (a, d, s))
-    # K_bc += sum_ad I D[a,d]
-    for a in range(NA):
-        for d in range(ND):
-            w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a, d, a, d))
-    for b in range(NB):
-        for ci in range(CC):
-            s = " + ".join("%s * dad_%d_%d" % (Iv(a, b, ci, d), a, d)
-                           for a in range(NA) for d in range(ND))
-            w.line("add(cB + %d, cC + c0 + %d, sK * (%s));" % (b, ci, s))
-    w.close()
+        def Iv(a, b, k):
+            return "I[%d]" % ((a * NB + b) * CS + k)
+        w.open("if (doJ) {")
+        for (k, c, d) in els:
+            w.line("const double dcd_%d = ld(cD + %d, cC + %d);" % (k, d, c))
+        for a_ in range(NA):
+            for b_ in range(NB):
+                sm = " + ".join("%s * dcd_%d" % (Iv(a_, b_, k), k) for (k, c, d) in els)
+                w.line("jab[%d] += %s;" % (a_ * NB + b_, sm))
+        for a_ in range(NA):
+            for b_ in range(NB):
+                w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a_, b_, a_, b_))
+        for (k, c, d) in els:
+            sm = " + ".join("%s * dab_%d_%d" % (Iv(a_, b_, k), a_, b_)
+                            for a_ in range(NA) for b_ in range(NB))
+            w.line("add(cC + %d, cD + %d, sJ * (%s));" % (c, d, sm))
+        w.close()
+        w.open("if (doK) {")
+        # K_ac += sum_bd I D[d,b]
+        for b_ in range(NB):
+            for d in ds_:
+                w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b_, d, b_))
+        for a_ in range(NA):
+            for c in cs_:
+                sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
+                                for b_ in range(NB) for (k, cc, d) in els if cc == c)
+                w.line("add(cA + %d, cC + %d, sK * (%s));" % (a_, c, sm))
+        # K_bd += sum_ac I D[a,c]
+        for a_ in range(NA):
+            for c in cs_:
+                w.line("const double dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
+        for b_ in range(NB):
+            for d in ds_:
+                sm = " + ".join("%s * dac_%d_%d" % (Iv(a_, b_, k), a_, c)
+                                for a_ in range(NA) for (k, c, dd) in els if dd == d)
+                w.line("add(cB + %d, cD + %d, sK * (%s));" % (b_, d, sm))
+        # K_ad += sum_bc I D[b,c]
+        for b_ in range(NB):
+            for c in cs_:
+                w.line("const double dbc_%d_%d = ld(cB + %d, cC + %d);" % (b_, c, b_, c))
+        for a_ in range(NA):
+            for d in ds_:
+                sm = " + ".join("%s * dbc_%d_%d" % (Iv(a_, b_, k), b_, c)
+                                for b_ in range(NB) for (k, c, dd) in els if dd == d)
+                w.line("add(cA + %d, cD + %d, sK * (%s));" % (a_, d, sm))
+        # K_bc += sum_ad I D[a,d]
+        for a_ in range(NA):
+            for d in ds_:
+                w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a_, d, a_, d))
+        for b_ in range(NB):
+            for c in cs_:
+                sm = " + ".join("%s * dad_%d_%d" % (Iv(a_, b_, k), a_, d)
+                                for a_ in range(NA) for (k, cc, d) in els if cc == c)
+                w.line("add(cB + %d, cC + %d, sK * (%s));" % (b_, c, sm))
+        w.close()
+        if nchunk > 1:
+            w.line("break;")
+            w.close("}")
+    if nchunk > 1:
+        w.close("}")
     w.close("}")  # digest
     w.close("};")
     return "\n".join(w.lines), name
@@ -370,24 +370,26 @@ def gen_class(la, lb, lc, ld):
 
 def main(out_path):
     pclasses = [(a, b) for a in range(LMAX_FAST + 1) for b in range(a + 1)]
-    chunks = ["// Generated by gen_jk.py -- do not edit.",
-              "#pragma once", '#include "../cqf_common.cuh"', "namespace cqf {", ""]
+    parts = ["// Generated by gen_jk.py -- do not edit.",
+             "#pragma once", '#include "../cqf_common.cuh"', "namespace cqf {", ""]
     table = []
     for i, c1 in enumerate(pclasses):
         for c2 in pclasses[:i + 1]:
             bra, ket = orientation(c1, c2)
-            code, name = gen_class(bra[0], bra[1], ket[0], ket[1])
-            chunks.append(code)
-            chunks.append("")
-            table.append((bra, ket, name))
-    # dispatcher over (bra class, ket class) as stored in the basis buckets
-    chunks.append("// (bra la, lb, ket lc, ld) of each generated class")
-    chunks.append("#define CQF_GEN_JK_CLASSES(X) \\")
-    chunks.append(" \\\n".join("  X(%d, %d, %d, %d, GenJK_%s)" % (b[0], b[1], k[0], k[1], n)
-                              for (b, k, n) in table))
-    chunks.append("")
-    chunks.append("}  // namespace cqf")
-    txt = "\n".join(chunks) + "\n"
+            names = []
+            for prec in (64, 32):
+                code, name = gen_class(bra[0], bra[1], ket[0], ket[1], prec)
+                parts.append(code)
+                parts.append("")
+                names.append(name)
+            table.append((bra, ket, names))
+    parts.append("// (bra la, lb, ket lc, ld) of each generated class, FP64 / FP32 structs")
+    parts.append("#define CQF_GEN_JK_CLASSES(X) \\")
+    parts.append(" \\\n".join("  X(%d, %d, %d, %d, GenJK%s, GenJK%s)"
+                             % (b[0], b[1], k[0], k[1], n[0], n[1]) for (b, k, n) in table))
+    parts.append("")
+    parts.append("}  // namespace cqf")
+    txt = "\n".join(parts) + "\n"
     os.makedirs(os.path.dirname(out_path), exist_ok=True)
     if not os.path.exists(out_path) or open(out_path).read() != txt:
         with open(out_path, "w") as f:

@@ -113,6 +113,20 @@ cqf_status cqf_basis_one_electron(cqf_basis* basis, double* S, double* T);
 cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
                                  const cqf_opts* opts, cqf_stats* stats);
 
+/* CUDA-graph form of cqf_two_body_contract for builds repeated on the same
+ * device buffers (many densities per launch, RT-TDDFT steps, response
+ * right-hand sides).  cqf_graph_create captures the whole contraction once
+ * (device pointers only; X and AX are bound at creation, AX += G[X] on every
+ * launch); cqf_graph_launch replays it on `stream` (NULL = the basis' stream)
+ * without synchronising.  Batched form of FockBuilder::formRawGDInBatches'
+ * many-density call (include/fockbuilder/impl.hpp:109-244), as used by
+ * MOIntsTransformer (include/mointstransformer/tpi_ssfock.hpp:378-379). */
+typedef struct cqf_graph cqf_graph;
+cqf_status cqf_graph_create(cqf_basis* basis, const cqf_contraction* list, int n,
+                            const cqf_opts* opts, cqf_graph** out);
+cqf_status cqf_graph_launch(cqf_graph* graph, void* stream);
+cqf_status cqf_graph_destroy(cqf_graph* graph);
+
 /* Size of the fixed scratch array of cqf_two_body_contract_noalloc. */
 #define CQF_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 
