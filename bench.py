@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--workload", default="h2o16_def2svp")
     ap.add_argument("--cutoff", type=float, default=1e-8)
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--batched", type=int, default=1,
+                    help="also time the 64-density dD build as a CUDA graph")
+    ap.add_argument("--serving-requests", type=int, default=300,
+                    help="requests of the Poisson serving stream (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=10.0)
     return ap.parse_args()
 
 
@@ -153,6 +158,95 @@ def cpu_baseline(basis, D, budget_s=25.0):
                 cores=os.cpu_count(), G=2 * J - K)
 
 
+def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64):
+    """(H2O)8 / cc-pVDZ (N = 192): 64 symmetric perturbations
+    dD_k = 1e-3 (X_k + X_k^T) contracted (J and K) against one pass of
+    screened ERIs, incremental (AX += G[dD]), captured once as a CUDA graph
+    and replayed.  Unit: builds/s = densities per second."""
+    import numpy as np
+    import torch
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.contraction import (COULOMB, EXCHANGE, ContractionGraph,
+                                                  DirectTPI, TwoBodyContraction)
+    mol, bname, nocc, seed = workloads.config("h2o8_ccpvdz")
+    basis = BasisSet.build(mol, bname)
+    tpi = DirectTPI(basis, device=dev.index or 0)
+    N = basis.nbasis
+    dDs = workloads.delta_densities(N, ndens, eps=1e-3, seed_base=400)
+    X = [torch.from_numpy(np.ascontiguousarray(d.T)).to(dev).t() for d in dDs]
+    out = [torch.zeros((N, N), dtype=torch.float64, device=dev).t() for _ in range(2 * ndens)]
+    cont = []
+    for k in range(ndens):
+        cont.append(TwoBodyContraction(X[k], out[2 * k], True, COULOMB))
+        cont.append(TwoBodyContraction(X[k], out[2 * k + 1], True, EXCHANGE))
+    g = ContractionGraph(tpi, cont, precision=precision, fp32_cutoff=cutoff)
+    stream = torch.cuda.Stream(dev)
+    for _ in range(warmup):
+        g.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.launch(stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    g.close()
+    t = float(np.median(ms)) / 1e3
+    return {"workload": "h2o8_ccpvdz x 64 dD (J+K), CUDA graph", "nbasis": N,
+            "densities_per_launch": ndens, "ms_per_launch": t * 1e3,
+            "builds_per_s": ndens / t, "precision": precision, "fp32_cutoff": cutoff}
+
+
+def run_serving(dev, nreq, rate, cutoff):
+    """The serving stream: nreq requests with Poisson arrivals at `rate` Hz,
+    each a seeded (H2O)_n, n ~ U{1..32}, cc-pVDZ or def2-SVP (50/50), its own
+    seeded density, mixed precision; continuous batching with memory
+    admission.  Latency = completion - arrival."""
+    import numpy as np
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet
+    from chronusq_public_b200.contraction import DirectTPI
+    from chronusq_public_b200.serving import FockRequest, FockServer, poisson_stream
+    reqs = poisson_stream(nreq, rate, seed=5)
+    prepared = []
+    for r in reqs:
+        mol = workloads.water_cluster(r["nwater"], seed=r["geom_seed"],
+                                      box=max(6.0, 10.0 * (r["nwater"] / 16.0) ** (1 / 3)))
+        basis = BasisSet.build(mol, r["basis"])
+        # seeded S-orthonormalised occupied-orbital density (5 per water);
+        # S from the device, before the timed stream starts
+        tpi = DirectTPI(basis, device=dev.index or 0)
+        S, _ = tpi.one_electron()
+        tpi.close()
+        D = workloads.occupied_density(S, 5 * r["nwater"], r["dens_seed"])
+        prepared.append((r, mol, D))
+    srv = FockServer(device=dev.index or 0, slots=8, mem_budget=16 << 30)
+    futs = []
+    t0 = time.perf_counter()
+    for (r, mol, D) in prepared:
+        now = time.perf_counter() - t0
+        if r["t"] > now:
+            time.sleep(r["t"] - now)
+        futs.append(srv.submit(FockRequest(mol, r["basis"], D, precision="mixed",
+                                           fp32_cutoff=cutoff, rid=r["rid"],
+                                           arrival=t0 + r["t"])))
+    for f in futs:
+        f.result(timeout=600)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    return {"requests": nreq, "arrival_rate_hz": rate, "wall_s": wall,
+            "builds_per_s": nreq / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "fp32_cutoff": cutoff,
+            "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
+
+
 def reference_arm(args, ws, rank):
     if rank != 0:
         return
@@ -235,9 +329,10 @@ def main():
     Kd = torch.zeros_like(Jd).t().contiguous().t()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     con = GTODirectTPIContraction(tpi)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)   # the build and its events on one stream
 
     def run(precision, cut, steps, warmup, collect=False):
+        torch.cuda.set_stream(stream)
         for _ in range(warmup):
             Jd.zero_(); Kd.zero_()
             con.twoBodyContract([TwoBodyContraction(Dd, Jd, True, COULOMB),
@@ -311,6 +406,14 @@ def main():
     fl64 = FL.build_flops(basis, Q, [D], nmat_digest=2)
     frac64 = (fl64["f64"] / (p64 * 1e12)) / (t64 / K)
 
+    batched = None
+    if args.batched:
+        batched = {"fp64": run_batched(dev, args.steps, args.warmup),
+                   "mixed": run_batched(dev, args.steps, args.warmup, "mixed", args.cutoff)}
+    serving = None
+    if args.serving_requests > 0:
+        serving = run_serving(dev, args.serving_requests, args.serving_rate, args.cutoff)
+
     cpu = None
     err = {}
     if not args.no_oracle:
@@ -352,6 +455,10 @@ def main():
         "gpu_launches": launches_per_step * K,
         "clocks": clocks,
     }
+    if batched:
+        line["batched_dD_graph"] = batched
+    if serving:
+        line["serving"] = serving
     if cpu:
         line["cpu_baseline"] = {"value": cpu["builds_per_s"], "unit": "builds/s",
                                 "cores": cpu["cores"], "kind": "port",

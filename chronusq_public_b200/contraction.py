@@ -103,6 +103,15 @@ def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
+def _stream_arg(stream):
+    """CUDA stream handle for the C ABI.  None -> the basis' own stream;
+    0 (torch's legacy default stream) -> cudaStreamLegacy, so that work is
+    ordered with the caller's stream as the caller expects."""
+    if stream is None:
+        return None
+    return C.c_void_p(1 if int(stream) == 0 else int(stream))
+
+
 class ContractionGraph:
     """A contraction captured as a CUDA graph (``cqf_graph_create``): X and AX
     (CUDA tensors, column-major) are bound at capture; every ``launch`` adds
@@ -139,8 +148,7 @@ class ContractionGraph:
         self.handle = h
 
     def launch(self, stream=None):
-        _cabi.check(_cabi.lib().cqf_graph_launch(
-            self.handle, C.c_void_p(stream) if stream else None))
+        _cabi.check(_cabi.lib().cqf_graph_launch(self.handle, _stream_arg(stream)))
 
     def close(self):
         if getattr(self, "handle", None):
@@ -210,7 +218,7 @@ class GTODirectTPIContraction:
         opts.device_pointers = 1 if dev else 0
         opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
         opts.fp32_cutoff = float(fp32_cutoff)
-        opts.stream = C.c_void_p(stream) if stream else None
+        opts.stream = _stream_arg(stream)
         st = _cabi.CqfStats()
         _cabi.check(_cabi.lib().cqf_two_body_contract(
             self.tpi.handle, arr, n, C.byref(opts), C.byref(st)))

@@ -50,8 +50,9 @@ namespace {
 // aointegrals_onee_inhouse.cxx:79-116, with a tighter series tolerance).
 void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
   const int M = BOYS_MMAX;
-  t64.assign((size_t)BOYS_NPTS * BOYS_ROW, 0.0);
-  t32.assign((size_t)BOYS_NPTS * BOYS_ROW, 0.0f);
+  t64.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW, 0.0);
+  t32.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW, 0.0f);
+  std::vector<long double> col(M + 1);
   for (int j = 0; j < BOYS_NPTS; j++) {
     long double T = (long double)j * BOYS_DT;
     long double term = 1.0L / (2 * M + 1), sum = term;
@@ -60,16 +61,17 @@ void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
       sum += term;
       if (term < sum * 1e-21L) break;
     }
-    long double eT = expl(-T), F = eT * sum;
-    std::vector<long double> col(M + 1);
-    col[M] = F;
+    long double eT = expl(-T);
+    col[M] = eT * sum;
     for (int m = M - 1; m >= 0; m--) col[m] = (2.0L * T * col[m + 1] + eT) / (2 * m + 1);
-    for (int m = 0; m <= M; m++) {
-      t64[(size_t)j * BOYS_ROW + m] = (double)col[m];
-      t32[(size_t)j * BOYS_ROW + m] = (float)col[m];
+    for (int L = 0; L <= BOYS_LTAB; L++) {
+      double* r64 = &t64[((size_t)L * BOYS_NPTS + j) * BOYS_ROW];
+      float* r32 = &t32[((size_t)L * BOYS_NPTS + j) * BOYS_ROW];
+      for (int k = 0; k <= BOYS_K64; k++) r64[k] = (double)col[L + k];
+      r64[BOYS_ROW - 1] = (double)eT;
+      for (int k = 0; k <= BOYS_K32; k++) r32[k] = (float)col[L + k];
+      r32[BOYS_K32 + 1] = (float)eT;
     }
-    t64[(size_t)j * BOYS_ROW + M + 1] = (double)eT;
-    t32[(size_t)j * BOYS_ROW + M + 1] = (float)eT;
   }
 }
 
@@ -629,6 +631,26 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   B->h_pairs.resize(B->npair);
   CQF_CUDA(cudaMemcpyAsync(B->h_pairs.data(), B->d_pairs, B->npair * sizeof(PairDev),
                            cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  // primitive pairs in the same order as the sorted pairs: the primitives of
+  // consecutive kets of a tile are one contiguous run
+  {
+    std::vector<long long> src(B->npair);
+    long long off2 = 0;
+    for (int i = 0; i < B->npair; i++) {
+      src[i] = B->h_pairs[i].pp_off;
+      B->h_pairs[i].pp_off = (int)off2;
+      off2 += B->h_pairs[i].npp;
+    }
+    std::vector<PrimPairDev> hpp(ppoff), hpp2(ppoff);
+    CQF_CUDA(cudaMemcpy(hpp.data(), B->d_pp, ppoff * sizeof(PrimPairDev), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < B->npair; i++)
+      std::copy(hpp.begin() + src[i], hpp.begin() + src[i] + B->h_pairs[i].npp,
+                hpp2.begin() + B->h_pairs[i].pp_off);
+    CQF_CUDA(cudaMemcpy(B->d_pp, hpp2.data(), ppoff * sizeof(PrimPairDev), cudaMemcpyHostToDevice));
+    CQF_CUDA(cudaMemcpy(B->d_pairs, B->h_pairs.data(), B->npair * sizeof(PairDev),
+                        cudaMemcpyHostToDevice));
+  }
   B->h_schwarz.resize((size_t)nshell * nshell);
   CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
                            (size_t)nshell * nshell * sizeof(double), cudaMemcpyDeviceToHost,

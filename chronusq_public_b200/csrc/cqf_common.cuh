@@ -9,8 +9,11 @@
 //   PrimPairDev[nprimpair] primitive-pair data (p, K, P, PA, PB), 96 B each,
 //                          contiguous per shell pair so one pair's primitives
 //                          are one coalesced run
-//   boys table             F_m(T_j), T_j = j*0.05, m = 0..BOYS_MMAX, and
-//                          exp(-T_j) (FP64 and an FP32 copy), 197 KB, L2 resident
+//   boys tables            per angular sum L and grid point T_j = j*0.05 one
+//                          row {F_L..F_{L+6}(T_j), exp(-T_j)}: 64 B, 16-B
+//                          aligned, read with four 128-bit loads (FP64); FP32
+//                          rows {F_L..F_{L+4}, exp(-T_j), 0, 0}: 32 B
+//                          (1.1 MB + 0.6 MB for L <= 24, L2 resident)
 //   Cartesian-AO densities / accumulators, nMat x ncart x ncart
 #pragma once
 
@@ -24,9 +27,12 @@ constexpr int BOYS_MMAX = 32;      // tabulated Boys orders
 constexpr double BOYS_DT = 0.05;   // grid spacing of the Taylor table
 constexpr double BOYS_TMAX = 36.0; // above: F0 = sqrt(pi/T)/2 + upward recursion
 constexpr int BOYS_NPTS = 724;     // grid points 0 .. TMAX/DT (+ margin)
-constexpr int BOYS_ROW = BOYS_MMAX + 2;  // F_0..F_MMAX, then exp(-T_j)
-constexpr int BOYS_K64 = 8;        // Taylor terms k = 0..8 (FP64, |dT| <= 0.025)
-constexpr int BOYS_K32 = 4;        // Taylor terms k = 0..4 (FP32)
+constexpr int BOYS_LTAB = 24;      // per-L rows exist for L = 0..BOYS_LTAB
+constexpr int BOYS_ROW = 8;        // per-L row: F_L..F_{L+6}, exp(-T_j) (FP64);
+                                   // F_L..F_{L+4}, exp(-T_j), 0, 0 (FP32)
+constexpr int BOYS_K64 = 6;        // Taylor terms k = 0..6 (FP64, |dT| <= 0.025:
+                                   // remainder <= 0.025^7/7! = 1.2e-15 relative)
+constexpr int BOYS_K32 = 4;        // Taylor terms k = 0..4 (FP32, 4e-11 relative)
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int nsph(int l) { return 2 * l + 1; }
@@ -62,7 +68,7 @@ __host__ __device__ constexpr int cart_lz(int l, int i) {
   return l - cart_lx(l, i) - cart_ly(l, i);
 }
 
-struct ShellDev {
+struct __align__(16) ShellDev {
   int l, pure, nprim, prim_off;
   int cart_off, sph_off, pad0, pad1;
   double O[3];
@@ -70,7 +76,7 @@ struct ShellDev {
 
 // One significant shell pair.  (shA, shB) is the order the ERI kernels use
 // (l(shA) >= l(shB)); (s1, s2) is the reference loop order (s1 >= s2).
-struct PairDev {
+struct __align__(16) PairDev {
   int shA, shB, s1, s2;
   int cA, cB;        // Cartesian AO offsets of shA / shB
   int lex;           // rank of (s1, s2) in the reference loop order
@@ -80,7 +86,7 @@ struct PairDev {
   double Q;          // Schwarz bound sqrt(||(ab|ab) diag||_inf)
 };
 
-struct PrimPairDev {
+struct __align__(16) PrimPairDev {
   double p, Kp;      // exponent sum; c_a c_b exp(-mu |AB|^2) / p
   double P[3], PA[3], PB[3];
   double o2p;        // 1 / (2p)
@@ -94,19 +100,25 @@ template <int L>
 __device__ __forceinline__ void boys_f64(double T, double* F,
                                          const double* __restrict__ tab) {
   if (T < BOYS_TMAX) {
-    int j = __double2int_rn(T * (1.0 / BOYS_DT));
-    double dT = j * BOYS_DT - T;
-    const double* row = tab + j * BOYS_ROW;
-    double s = __ldg(row + L + BOYS_K64);
-#pragma unroll
-    for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + L + k) + s * dT * (1.0 / (k + 1));
+    const int j = __double2int_rn(T * (1.0 / BOYS_DT));
+    const double dT = j * BOYS_DT - T;
+    const double2* row = reinterpret_cast<const double2*>(tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW);
+    const double2 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2), r3 = __ldg(row + 3);
+    // Taylor of F_L about T_j (F_m' = -F_{m+1}), terms k = 0..6
+    double s = r3.x;
+    s = r2.y + s * dT * (1.0 / 6);
+    s = r2.x + s * dT * (1.0 / 5);
+    s = r1.y + s * dT * (1.0 / 4);
+    s = r1.x + s * dT * (1.0 / 3);
+    s = r0.y + s * dT * (1.0 / 2);
+    s = r0.x + s * dT;
     F[L] = s;
     if (L > 0) {
-      // exp(-T) = exp(-T_j) exp(dT), |dT| <= DT/2, Taylor to dT^8
-      double e = 1.0 + dT * (1.0 / 8);
+      // exp(-T) = exp(-T_j) exp(dT), |dT| <= DT/2, Taylor to dT^7
+      double e = 1.0 + dT * (1.0 / 7);
 #pragma unroll
-      for (int k = 7; k >= 1; k--) e = 1.0 + dT * e * (1.0 / k);
-      e *= __ldg(row + BOYS_MMAX + 1);
+      for (int k = 6; k >= 1; k--) e = 1.0 + dT * e * (1.0 / k);
+      e *= r3.y;
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
@@ -125,15 +137,19 @@ __device__ __forceinline__ void boys_f64(double T, double* F,
 template <int L>
 __device__ __forceinline__ void boys_f32(float T, float* F, const float* __restrict__ tab) {
   if (T < (float)BOYS_TMAX) {
-    int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
-    float dT = j * (float)BOYS_DT - T;
-    const float* row = tab + j * BOYS_ROW + L;
-    float s = __ldg(row + BOYS_K32);
-#pragma unroll
-    for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));
+    const int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
+    const float dT = j * (float)BOYS_DT - T;
+    const float4* row = reinterpret_cast<const float4*>(tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW);
+    const float4 r0 = __ldg(row), r1 = __ldg(row + 1);
+    float s = r1.x;
+    s = r0.w + s * dT * (1.0f / 4);
+    s = r0.z + s * dT * (1.0f / 3);
+    s = r0.y + s * dT * (1.0f / 2);
+    s = r0.x + s * dT;
     F[L] = s;
     if (L > 0) {
-      float e = __expf(-T), t2 = 2.0f * T;
+      const float e = r1.y * (1.0f + dT * (1.0f + dT * (0.5f + dT * (1.0f / 6))));
+      const float t2 = 2.0f * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
     }

@@ -42,11 +42,17 @@ __global__ void __launch_bounds__(JK_THREADS)
   const int ns = a.nShell;
   const double cut = (a.precision == 1) ? a.fp32_cut : 0.0;
 
+  // same class: each unordered pair {P, Q} once, as ket position <= bra
+  // position (no idle upper triangle; roles still follow the lex order)
+  if (a.same && tile * JK_THREADS > ib) {
+    if (IS64 && ch == 0) count_block(a.counters, false, false, false, false);
+    return;
+  }
   bool visited = false, screened = false, work = false;
   PairDev Q;
-  if (jk < a.nKet) {
+  if (jk < a.nKet && !(a.same && jk > ib)) {
     Q = a.pairs[a.ketBeg + jk];
-    visited = !(a.same && Q.lex > P.lex);
+    visited = true;
   }
   const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * JK_THREADS].Q;
   const bool tileDead = a.screen && tileMax < a.thresh;

@@ -155,9 +155,13 @@ __global__ void __launch_bounds__(JK_THREADS)
   double bound = 0.0;
   bool pRef = true;
   PairDev Q;
-  if (jk < a.nKet) {
+  if (a.same && blockIdx.y * JK_THREADS > ib) {  // tile wholly above the diagonal
+    count_block(a.counters, false, false, false, false);
+    return;
+  }
+  if (jk < a.nKet && !(a.same && jk > ib)) {  // each unordered pair once
     Q = a.pairs[a.ketBeg + jk];
-    visited = !(a.same && Q.lex > P.lex);
+    visited = true;
   }
   // tile-level screen: kets are sorted by Q (descending) inside the class
   const bool tileDead = a.screen &&

@@ -1,0 +1,55 @@
+// C++ caller of the library through include/cqfock.hpp: reads a basis and a
+// matrix from raw files, runs one twoBodyContract, writes AX.
+//   contract_cpp <dir> <her> <type> <complex>
+// <dir>/shells.txt: nshell, then per shell "l pure nprim x y z" + alpha + coeff
+// <dir>/X.bin: N*N doubles (x2 if complex), column-major; writes <dir>/AX.bin
+#include <complex>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <vector>
+
+#include "cqfock.hpp"
+
+template <typename T>
+int run(const std::string& dir, const std::vector<cqfock::Shell>& sh, bool her, int type) {
+  auto tpi = std::make_shared<cqfock::DirectTPI>(sh);
+  const size_t N = tpi->nBasis();
+  std::vector<T> X(N * N), AX(N * N, T(0));
+  std::ifstream fx(dir + "/X.bin", std::ios::binary);
+  fx.read(reinterpret_cast<char*>(X.data()), X.size() * sizeof(T));
+  cqfock::GTODirectTPIContraction<T> con(tpi);
+  std::vector<cqfock::TwoBodyContraction<T>> list = {
+      {X.data(), AX.data(), her, type ? cqfock::EXCHANGE : cqfock::COULOMB}};
+  con.twoBodyContract(true, list);
+  std::ofstream fo(dir + "/AX.bin", std::ios::binary);
+  fo.write(reinterpret_cast<const char*>(AX.data()), AX.size() * sizeof(T));
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 5) return 2;
+  std::string dir = argv[1];
+  bool her = std::atoi(argv[2]) != 0, cplx = std::atoi(argv[4]) != 0;
+  int type = std::atoi(argv[3]);
+  std::ifstream fs(dir + "/shells.txt");
+  int ns;
+  fs >> ns;
+  std::vector<cqfock::Shell> sh(ns);
+  for (auto& s : sh) {
+    int pure, np;
+    fs >> s.l >> pure >> np >> s.O[0] >> s.O[1] >> s.O[2];
+    s.pure = pure != 0;
+    s.alpha.resize(np);
+    s.coeff.resize(np);
+    for (auto& a : s.alpha) fs >> a;
+    for (auto& c : s.coeff) fs >> c;
+  }
+  try {
+    return cplx ? run<std::complex<double>>(dir, sh, her, type) : run<double>(dir, sh, her, type);
+  } catch (const std::exception& e) {
+    std::cerr << e.what() << "\n";
+    return 1;
+  }
+}
