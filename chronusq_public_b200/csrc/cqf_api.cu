@@ -50,8 +50,8 @@ namespace {
 // aointegrals_onee_inhouse.cxx:79-116, with a tighter series tolerance).
 void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
   const int M = BOYS_MMAX;
-  t64.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW, 0.0);
-  t32.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW, 0.0f);
+  t64.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW64, 0.0);
+  t32.assign((size_t)(BOYS_LTAB + 1) * BOYS_NPTS * BOYS_ROW32, 0.0f);
   std::vector<long double> col(M + 1);
   for (int j = 0; j < BOYS_NPTS; j++) {
     long double T = (long double)j * BOYS_DT;
@@ -65,10 +65,10 @@ void make_boys_table(std::vector<double>& t64, std::vector<float>& t32) {
     col[M] = eT * sum;
     for (int m = M - 1; m >= 0; m--) col[m] = (2.0L * T * col[m + 1] + eT) / (2 * m + 1);
     for (int L = 0; L <= BOYS_LTAB; L++) {
-      double* r64 = &t64[((size_t)L * BOYS_NPTS + j) * BOYS_ROW];
-      float* r32 = &t32[((size_t)L * BOYS_NPTS + j) * BOYS_ROW];
+      double* r64 = &t64[((size_t)L * BOYS_NPTS + j) * BOYS_ROW64];
+      float* r32 = &t32[((size_t)L * BOYS_NPTS + j) * BOYS_ROW32];
       for (int k = 0; k <= BOYS_K64; k++) r64[k] = (double)col[L + k];
-      r64[BOYS_ROW - 1] = (double)eT;
+      r64[BOYS_K64 + 1] = (double)eT;
       for (int k = 0; k <= BOYS_K32; k++) r32[k] = (float)col[L + k];
       r32[BOYS_K32 + 1] = (float)eT;
     }
@@ -478,6 +478,7 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   if (device < 0 || device >= ndev) return fail(CQF_EINVAL, "bad device ordinal");
   B->device = device;
   CQF_CUDA(cudaSetDevice(device));
+  CQF_CUDA(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
   CQF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
   CQF_CUDA(cudaEventCreate(&B->ev0));
   CQF_CUDA(cudaEventCreate(&B->ev1));
@@ -764,6 +765,7 @@ WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   L.oNm = take(ns2);
   L.oNmM = take(ns2 * nMat);
   L.oG = take(4);
+  L.oWork = take((NWORK + 1) / 2);
   L.total = off;
   return L;
 }
@@ -794,6 +796,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   const bool host = !opts.device_pointers;
   const size_t oX = Lw.oX, oAX = Lw.oAX, oXc = Lw.oXc, oAc = Lw.oAc, oNm = Lw.oNm,
                oNmM = Lw.oNmM, oG = Lw.oG;
+  unsigned int* work = reinterpret_cast<unsigned int*>(ws + Lw.oWork);
   if (!capture) CQF_CUDA(cudaEventRecord(B->ev0, st));
   std::vector<const double*> Xd(nMat);
   std::vector<double*> AXd(nMat);
@@ -822,6 +825,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   }
   CQF_CUDA(cudaMemsetAsync(B->d_counters, 0, 8 * sizeof(unsigned long long), st));
   CQF_CUDA(cudaMemsetAsync(ws + oG, 0, 4 * sizeof(double), st));
+  CQF_CUDA(cudaMemsetAsync(work, 0, NWORK * sizeof(unsigned int), st));
 
   // shell-block norms (per matrix, symmetrised when non-Hermitian), max
   for (int m = 0; m < nMat; m++) {
@@ -875,7 +879,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.nKet = B->cls_cnt[ck];
       a.same = (cb == ck);
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
-      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, st)))
+      unsigned int* w = work + 2 * (cb * NCLS + ck);
+      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, st)))
         launch_jk_generic(a, la, lb, lc, ld, st);
     }
   CQF_CUDA(cudaGetLastError());

@@ -9,11 +9,12 @@
 //   PrimPairDev[nprimpair] primitive-pair data (p, K, P, PA, PB), 96 B each,
 //                          contiguous per shell pair so one pair's primitives
 //                          are one coalesced run
-//   boys tables            per angular sum L and grid point T_j = j*0.05 one
-//                          row {F_L..F_{L+6}(T_j), exp(-T_j)}: 64 B, 16-B
-//                          aligned, read with four 128-bit loads (FP64); FP32
-//                          rows {F_L..F_{L+4}, exp(-T_j), 0, 0}: 32 B
-//                          (1.1 MB + 0.6 MB for L <= 24, L2 resident)
+//   boys tables            per angular sum L and grid point T_j = j*0.1 one
+//                          row {F_L..F_{L+8}(T_j), exp(-T_j)}: 80 B, 16-B
+//                          aligned, read with five 128-bit loads (FP64); FP32
+//                          rows {F_L..F_{L+5}, exp(-T_j), 0}: 32 B.  The
+//                          29 KB (FP64) / 11.6 KB (FP32) of one L are staged
+//                          in shared memory by the class kernels.
 //   Cartesian-AO densities / accumulators, nMat x ncart x ncart
 #pragma once
 
@@ -23,16 +24,19 @@
 namespace cqf {
 
 constexpr int LMAX = 3;            // highest shell angular momentum (f)
-constexpr int BOYS_MMAX = 32;      // tabulated Boys orders
-constexpr double BOYS_DT = 0.05;   // grid spacing of the Taylor table
+constexpr int BOYS_MMAX = 40;      // orders of the host-side generation
+constexpr double BOYS_DT = 0.1;    // grid spacing of the Taylor tables
 constexpr double BOYS_TMAX = 36.0; // above: F0 = sqrt(pi/T)/2 + upward recursion
-constexpr int BOYS_NPTS = 724;     // grid points 0 .. TMAX/DT (+ margin)
+constexpr int BOYS_NPTS = 362;     // grid points 0 .. TMAX/DT (+ margin)
 constexpr int BOYS_LTAB = 24;      // per-L rows exist for L = 0..BOYS_LTAB
-constexpr int BOYS_ROW = 8;        // per-L row: F_L..F_{L+6}, exp(-T_j) (FP64);
-                                   // F_L..F_{L+4}, exp(-T_j), 0, 0 (FP32)
-constexpr int BOYS_K64 = 6;        // Taylor terms k = 0..6 (FP64, |dT| <= 0.025:
-                                   // remainder <= 0.025^7/7! = 1.2e-15 relative)
-constexpr int BOYS_K32 = 4;        // Taylor terms k = 0..4 (FP32, 4e-11 relative)
+constexpr int BOYS_K64 = 8;        // FP64 Taylor terms k = 0..8, |dT| <= 0.05:
+                                   // remainder <= 0.05^9/9! = 5e-18 relative
+constexpr int BOYS_K32 = 5;        // FP32 Taylor terms k = 0..5 (2e-11 relative)
+constexpr int BOYS_ROW64 = 10;     // FP64 row: F_L..F_{L+8}, exp(-T_j)  (80 B)
+constexpr int BOYS_ROW32 = 8;      // FP32 row: F_L..F_{L+5}, exp(-T_j), 0 (32 B)
+// bytes of the rows of one L (what a block stages in shared memory)
+constexpr int BOYS_LBYTES64 = BOYS_NPTS * BOYS_ROW64 * 8;
+constexpr int BOYS_LBYTES32 = BOYS_NPTS * BOYS_ROW32 * 4;
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int nsph(int l) { return 2 * l + 1; }
@@ -96,16 +100,18 @@ struct __align__(16) PrimPairDev {
 // F_0..F_L at T.  Taylor expansion of F_L about the nearest grid point
 // (F_m' = -F_{m+1}), downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1);
 // for T >= TMAX, F_0 = sqrt(pi/T)/2 and upward recursion keeping e^-T.
+// `rows` points at the rows of this L (global or shared memory).
 template <int L>
-__device__ __forceinline__ void boys_f64(double T, double* F,
-                                         const double* __restrict__ tab) {
+__device__ __forceinline__ void boys_f64(double T, double* F, const double* __restrict__ rows) {
   if (T < BOYS_TMAX) {
     const int j = __double2int_rn(T * (1.0 / BOYS_DT));
     const double dT = j * BOYS_DT - T;
-    const double2* row = reinterpret_cast<const double2*>(tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW);
-    const double2 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2), r3 = __ldg(row + 3);
-    // Taylor of F_L about T_j (F_m' = -F_{m+1}), terms k = 0..6
-    double s = r3.x;
+    const double2* row = reinterpret_cast<const double2*>(rows + j * BOYS_ROW64);
+    const double2 r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3], r4 = row[4];
+    // Taylor of F_L about T_j (F_m' = -F_{m+1}), terms k = 0..8
+    double s = r4.x;
+    s = r3.y + s * dT * (1.0 / 8);
+    s = r3.x + s * dT * (1.0 / 7);
     s = r2.y + s * dT * (1.0 / 6);
     s = r2.x + s * dT * (1.0 / 5);
     s = r1.y + s * dT * (1.0 / 4);
@@ -114,11 +120,11 @@ __device__ __forceinline__ void boys_f64(double T, double* F,
     s = r0.x + s * dT;
     F[L] = s;
     if (L > 0) {
-      // exp(-T) = exp(-T_j) exp(dT), |dT| <= DT/2, Taylor to dT^7
-      double e = 1.0 + dT * (1.0 / 7);
+      // exp(-T) = exp(-T_j) exp(dT), |dT| <= DT/2, Taylor to dT^9
+      double e = 1.0 + dT * (1.0 / 9);
 #pragma unroll
-      for (int k = 6; k >= 1; k--) e = 1.0 + dT * e * (1.0 / k);
-      e *= r3.y;
+      for (int k = 8; k >= 1; k--) e = 1.0 + dT * e * (1.0 / k);
+      e *= r4.y;
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
@@ -135,20 +141,22 @@ __device__ __forceinline__ void boys_f64(double T, double* F,
 }
 
 template <int L>
-__device__ __forceinline__ void boys_f32(float T, float* F, const float* __restrict__ tab) {
+__device__ __forceinline__ void boys_f32(float T, float* F, const float* __restrict__ rows) {
   if (T < (float)BOYS_TMAX) {
     const int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
     const float dT = j * (float)BOYS_DT - T;
-    const float4* row = reinterpret_cast<const float4*>(tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW);
-    const float4 r0 = __ldg(row), r1 = __ldg(row + 1);
-    float s = r1.x;
+    const float4* row = reinterpret_cast<const float4*>(rows + j * BOYS_ROW32);
+    const float4 r0 = row[0], r1 = row[1];
+    float s = r1.y;
+    s = r1.x + s * dT * (1.0f / 5);
     s = r0.w + s * dT * (1.0f / 4);
     s = r0.z + s * dT * (1.0f / 3);
     s = r0.y + s * dT * (1.0f / 2);
     s = r0.x + s * dT;
     F[L] = s;
     if (L > 0) {
-      const float e = r1.y * (1.0f + dT * (1.0f + dT * (0.5f + dT * (1.0f / 6))));
+      const float e =
+          r1.z * (1.0f + dT * (1.0f + dT * (0.5f + dT * ((1.0f / 6) + dT * (1.0f / 24)))));
       const float t2 = 2.0f * T;
 #pragma unroll
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));

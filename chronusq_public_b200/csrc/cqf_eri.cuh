@@ -91,7 +91,7 @@ __device__ __forceinline__ void boys_rt<double>(int L, double T, double* F, cons
   if (T < BOYS_TMAX) {
     int j = __double2int_rn(T * (1.0 / BOYS_DT));
     double dT = j * BOYS_DT - T;
-    const double* row = tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW;
+    const double* row = tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW64;
     double s = __ldg(row + BOYS_K64);
 #pragma unroll
     for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0 / (k + 1));
@@ -113,7 +113,7 @@ __device__ __forceinline__ void boys_rt<float>(int L, float T, float* F, const f
   if (T < (float)BOYS_TMAX) {
     int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
     float dT = j * (float)BOYS_DT - T;
-    const float* row = tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW;
+    const float* row = tab + ((size_t)L * BOYS_NPTS + j) * BOYS_ROW32;
     float s = __ldg(row + BOYS_K32);
 #pragma unroll
     for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));

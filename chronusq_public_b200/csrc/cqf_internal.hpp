@@ -51,8 +51,9 @@ cqf_status fail(cqf_status s, const std::string& msg);
 // Workspace layout of one contraction (in doubles, each part 256-B aligned):
 // [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
 struct WsLayout {
-  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, total;
+  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oWork, total;
 };
+constexpr int NWORK = 2 * NCLS * NCLS;  // persistent-kernel work counters per call
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
 cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat);
 // The contraction on a caller-provided device workspace of ws_layout().total
@@ -67,6 +68,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
 
 struct cqf_basis {
   int device = 0;
+  int nsm = 148;
   cudaStream_t stream = nullptr;
   int nshell = 0, nbasis = 0, ncart = 0, npair = 0, maxL = 0, maxPrim = 0;
   long long nprimpair = 0;

@@ -12,6 +12,8 @@
 #include "cqf_jk_kernels.cuh"
 #include "gen/cqf_gen_jk.cuh"
 
+#include <algorithm>
+
 namespace cqf {
 
 template <int N>
@@ -23,112 +25,136 @@ __device__ __forceinline__ void warp_sum(double (&v)[N]) {
   }
 }
 
-// FP64 launch: quartets with bound >= cut (all when cut <= 0); FP32 launch:
-// quartets with thresh <= bound < cut.  The FP64 launch also counts the
-// visited / screened quartets.  blockIdx.y = chunk * ketTiles + tile: every
-// thread of a block runs the same chunk (one code path per block), and the
-// chunks of one quartet run in parallel in different blocks.
+// Rows of the Boys tables for angular sum L (global memory).
+template <typename T>
+__device__ __forceinline__ const T* boys_rows(const JKLaunch& a, int L);
+template <>
+__device__ __forceinline__ const double* boys_rows<double>(const JKLaunch& a, int L) {
+  return a.boys64 + (size_t)L * BOYS_NPTS * BOYS_ROW64;
+}
+template <>
+__device__ __forceinline__ const float* boys_rows<float>(const JKLaunch& a, int L) {
+  return a.boys32 + (size_t)L * BOYS_NPTS * BOYS_ROW32;
+}
+
+// Persistent class kernel.  Each block stages the Boys rows of this class's
+// angular sum in shared memory once, then takes work items
+// (bra pair, chunk, ket tile of 128) from a device counter until none are
+// left.  FP64 launch: quartets with bound >= cut (all when cut <= 0); FP32
+// launch: quartets with thresh <= bound < cut.  The FP64 launch also counts
+// the visited / screened quartets.
 template <class GC, typename T>
-__global__ void __launch_bounds__(JK_THREADS)
-    jk_fast_kernel(const JKLaunch a) {
+__global__ void __launch_bounds__(JK_THREADS, GC::MINB)
+    jk_fast_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
   constexpr int NA = ncart(GC::LA), NB = ncart(GC::LB);
   constexpr int NCH = GC::NCHUNK;
+  constexpr int LSUM = GC::LA + GC::LB + GC::LC + GC::LD;
   constexpr bool IS64 = sizeof(T) == 8;
-  const int ib = blockIdx.x;
-  const int ketTiles = (a.nKet + JK_THREADS - 1) / JK_THREADS;
-  const int ch = blockIdx.y / ketTiles, tile = blockIdx.y % ketTiles;
-  const int jk = tile * JK_THREADS + threadIdx.x;
-  const PairDev P = a.pairs[a.braBeg + ib];
+  constexpr int TBYTES = IS64 ? BOYS_LBYTES64 : BOYS_LBYTES32;
+  extern __shared__ float4 s_boys4[];
+  {
+    const float4* g = reinterpret_cast<const float4*>(boys_rows<T>(a, LSUM));
+    for (int i = threadIdx.x; i < TBYTES / 16; i += JK_THREADS) s_boys4[i] = __ldg(g + i);
+  }
+  const T* boys = reinterpret_cast<const T*>(s_boys4);
+  __shared__ long long s_item;
   const int ns = a.nShell;
   const double cut = (a.precision == 1) ? a.fp32_cut : 0.0;
-
-  // same class: each unordered pair {P, Q} once, as ket position <= bra
-  // position (no idle upper triangle; roles still follow the lex order)
-  if (a.same && tile * JK_THREADS > ib) {
-    if (IS64 && ch == 0) count_block(a.counters, false, false, false, false);
-    return;
-  }
-  bool visited = false, screened = false, work = false;
-  PairDev Q;
-  if (jk < a.nKet && !(a.same && jk > ib)) {
-    Q = a.pairs[a.ketBeg + jk];
-    visited = true;
-  }
-  const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * JK_THREADS].Q;
-  const bool tileDead = a.screen && tileMax < a.thresh;
-  const bool counter = IS64 && ch == 0;  // one count per quartet
-  if (tileDead || (!IS64 && cut <= 0.0)) {
-    if (IS64) count_block(a.counters, counter && visited, counter && visited, false, false);
-    return;
-  }
-  int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
-  if (visited) {
-    const bool pRef = P.lex >= Q.lex;
-    const PairDev& R12 = pRef ? P : Q;
-    const PairDev& R34 = pRef ? Q : P;
-    s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
-    double bound = 1e300;
-    if (a.screen) {
-      bound = sh_max(a.norms, s1, s2, s3, s4, ns) * P.Q * Q.Q;
-      screened = bound < a.thresh;
-    }
-    const bool lo = bound < cut;
-    work = !screened && (IS64 ? !lo : lo);
-  }
-  if (IS64)
-    count_block(a.counters, counter && visited, counter && screened, false, counter && work);
-  else
-    count_block(a.counters, false, false, ch == 0 && work, false);
-  if (!__syncthreads_or(work)) return;
-
-  const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
-                     ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
-  const double sJ = work ? 0.5 * deg : 0.0, sK = work ? 0.25 * deg : 0.0;
+  const int ketTiles = (a.nKet + JK_THREADS - 1) / JK_THREADS;
+  const long long perBra = (long long)ketTiles * NCH;
+  const long long total = (long long)a.nBra * perBra;
   const size_t nc = a.ncart;
   const size_t matStride = (size_t)a.ncart * a.ncart;
-  const T* boys = IS64 ? reinterpret_cast<const T*>(a.boys64)
-                       : reinterpret_cast<const T*>(a.boys32);
-  double I[GC::NI];
-  if (work) {
-    GC::template eri<T>(P, Q, a.pp, boys, ch, I);
-  } else {
+  if (!IS64 && cut <= 0.0) return;  // uniform: nothing below the cut
+
+  for (;;) {
+    __syncthreads();  // table staged / previous item's s_item consumed
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(work, 1u);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    const int ib = (int)(item / perBra);
+    const int rem = (int)(item % perBra);
+    const int ch = rem / ketTiles, tile = rem % ketTiles;
+    // same class: each unordered pair {P, Q} once, as ket position <= bra
+    // position (roles still follow the lex order)
+    if (a.same && tile * JK_THREADS > ib) continue;
+    const int jk = tile * JK_THREADS + threadIdx.x;
+    const PairDev P = a.pairs[a.braBeg + ib];
+    bool visited = false, screened = false, work_ = false;
+    PairDev Q;
+    if (jk < a.nKet && !(a.same && jk > ib)) {
+      Q = a.pairs[a.ketBeg + jk];
+      visited = true;
+    }
+    const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * JK_THREADS].Q;
+    const bool counter = IS64 && ch == 0;  // one count per quartet
+    if (a.screen && tileMax < a.thresh) {
+      if (IS64) count_block(a.counters, counter && visited, counter && visited, false, false);
+      continue;
+    }
+    int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+    if (visited) {
+      const bool pRef = P.lex >= Q.lex;
+      const PairDev& R12 = pRef ? P : Q;
+      const PairDev& R34 = pRef ? Q : P;
+      s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
+      double bound = 1e300;
+      if (a.screen) {
+        bound = sh_max(a.norms, s1, s2, s3, s4, ns) * P.Q * Q.Q;
+        screened = bound < a.thresh;
+      }
+      const bool lo = bound < cut;
+      work_ = !screened && (IS64 ? !lo : lo);
+    }
+    if (IS64)
+      count_block(a.counters, counter && visited, counter && screened, false, counter && work_);
+    else
+      count_block(a.counters, false, false, ch == 0 && work_, false);
+    if (!__syncthreads_or(work_)) continue;
+
+    const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
+                       ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
+    const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
+    double I[GC::NI];
+    if (work_) {
+      GC::template eri<T>(P, Q, a.pp, boys, ch, I);
+    } else {
 #pragma unroll
-    for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
-  }
+      for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
+    }
 #pragma unroll 1
-  for (int m = 0; m < a.nMat; m++) {
-    const int fl = __ldg(a.flags + m);
-    const bool doJ = !(fl & 2), doK = (fl & 2);
-    double jab[NA * NB];
+    for (int m = 0; m < a.nMat; m++) {
+      const int fl = __ldg(a.flags + m);
+      const bool doJ = !(fl & 2), doK = (fl & 2);
+      double jab[NA * NB];
 #pragma unroll
-    for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
-    const double* X = a.Xc + m * matStride;
-    double* A = a.Ac + m * matStride;
-    GC::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work, doK && work, jab);
-    if (doJ) {
-      // every lane of the warp shares the bra pair: reduce, one atomic each
+      for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
+      const double* X = a.Xc + m * matStride;
+      double* A = a.Ac + m * matStride;
+      GC::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
+                 jab);
+      if (doJ) {
+        // every lane of the warp shares the bra pair: reduce, one atomic each
 #pragma unroll
-      for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
-      warp_sum(jab);
-      if ((threadIdx.x & 31) == 0) {
+        for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
+        warp_sum(jab);
+        if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int i = 0; i < NA * NB; i++)
-          if (jab[i] != 0.0)
-            atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
+          for (int i = 0; i < NA * NB; i++)
+            if (jab[i] != 0.0)
+              atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
+        }
       }
     }
   }
 }
 
-template <class GC>
-inline dim3 fast_grid(const JKLaunch& b) {
-  const int ketTiles = (b.nKet + JK_THREADS - 1) / JK_THREADS;
-  return dim3(b.nBra, (unsigned)(ketTiles * GC::NCHUNK));
-}
-
 // Launches the generated kernels of the class (la lb | lc ld) (either
 // orientation); returns false when the class has no generated kernel.
-inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, cudaStream_t st) {
+// work: two zeroed device counters for this class (FP64, FP32 launch).
+inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned int* work,
+                           int nsm, cudaStream_t st) {
   if (a.nBra == 0 || a.nKet == 0) return true;
   bool done = false;
   auto go = [&](auto tag64, auto tag32, bool swap) {
@@ -139,9 +165,16 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, cudaStrea
       b.braBeg = a.ketBeg; b.nBra = a.nKet;
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
     }
-    jk_fast_kernel<G64, double><<<fast_grid<G64>(b), JK_THREADS, 0, st>>>(b);
+    const long long tiles = (long long)((b.nKet + JK_THREADS - 1) / JK_THREADS);
+    const long long items64 = (long long)b.nBra * tiles * G64::NCHUNK;
+    const long long items32 = (long long)b.nBra * tiles * G32::NCHUNK;
+    // persistent blocks: enough for full residency on every SM (extra blocks
+    // queue and find the counter exhausted)
+    const unsigned g64 = (unsigned)std::min<long long>(items64, (long long)nsm * 8);
+    const unsigned g32 = (unsigned)std::min<long long>(items32, (long long)nsm * 8);
+    jk_fast_kernel<G64, double><<<g64, JK_THREADS, BOYS_LBYTES64, st>>>(b, work);
     if (b.precision == 1 && b.fp32_cut > 0.0)
-      jk_fast_kernel<G32, float><<<fast_grid<G32>(b), JK_THREADS, 0, st>>>(b);
+      jk_fast_kernel<G32, float><<<g32, JK_THREADS, BOYS_LBYTES32, st>>>(b, work + 1);
     done = true;
   };
 #define CQF_TRY_CLASS(A_, B_, C_, D_, N64, N32)                                          \
@@ -175,7 +208,8 @@ __global__ void __launch_bounds__(JK_THREADS)
   auto ta = [&](int c, int mu) { return A.pure ? TA[c * nsph(GC::LA) + mu] : (c == mu ? 1.0 : 0.0); };
   auto tb = [&](int c, int nu) { return B.pure ? TB[c * nsph(GC::LB) + nu] : (c == nu ? 1.0 : 0.0); };
   double I[GC::NI];
-  GC::template eri<double>(P, P, pp, boys, ch, I);
+  GC::template eri<double>(P, P, pp,
+                           boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I);
   for (int mu = 0; mu < na; mu++)
     for (int nu = 0; nu < nb; nu++) {
       double s = 0.0;

@@ -154,6 +154,10 @@ def gen_class(la, lb, lc, ld, prec):
     w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
     w.line("static constexpr int NCHUNK = %d;" % nchunk)
     w.line("static constexpr int NI = %d;  // integrals per chunk" % (NAB * CS))
+    # resident blocks per SM the register allocator should target: small
+    # low-L classes are latency bound and gain from occupancy
+    minb = 6 if L <= 1 else (4 if (L == 2 and NAB * CS <= 9) else 1)
+    w.line("static constexpr int MINB = %d;" % minb)
     w.line("template <typename T>")
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
            "const PrimPairDev* __restrict__ pp, const T* __restrict__ boys, const int ch, "
@@ -184,7 +188,7 @@ def gen_class(la, lb, lc, ld, prec):
     w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
     w.line("T F[%d];" % (L + 1))
     w.open("if constexpr (sizeof(T) == 8) {")
-    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));" % L)
+    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
     w.close("} else {")
     w.ind += 1
     w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
