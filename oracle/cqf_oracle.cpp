@@ -36,6 +36,7 @@
 // Build: see oracle/Makefile (g++ -O3 -march=native -fopenmp -shared).
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -967,6 +968,617 @@ void orc_flops(void* b, int nMat, const double* const* X, double thresh, double 
         }
       }
   out[0] = f64; out[1] = f32; out[2] = nk; out[3] = n32;
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Four-component Dirac-Coulomb (test infrastructure, same rules as above).
+//
+// Restates GTODirectRelERIContraction::directScaffoldLibcint
+// (include/particleintegrals/contract/direct4C_libcint.hpp):
+//   * Schwarz tables (:341-481): Q^LL = sqrt(max |(ab|ab)|) over the whole
+//     block, Q^SS = C2 sqrt(max |(dA dB ab|dA dB ab)|) over the 81 components;
+//   * BARE_COULOMB (LL|LL) (:514-790), LLSS (:810-1441), SSSS (:1841-2832):
+//     loop order, screens, degeneracy factors, update sites and conditions;
+//   * and FourCompFock::formGDDirect (include/fockbuilder/fourcompfock/
+//     impl.hpp:3752-4636): LL/SS/LS blocks, the 2C2 / -C2 / 2C4 / -C4
+//     weights, LS -> SL, G = twoeH - xHFX K.
+// The component formulas of the reference are products of spin operators:
+// a differentiated pair (m, n) acts as P_mn = dm.dn + i sigma.(dm x dn) on
+// the electron's spin; exchange updates are -P D P' (SSSS) or -D P (LS),
+// Coulomb updates P Re Tr[P' D]/2.  They are evaluated here through that
+// algebra (own formulation; the reference writes each component out).
+// Derivative ERIs (libcint int2e_ipvip1 / int2e_ipvip1ipvip2 in the
+// reference, v5.1.2, not present) are computed by McMurchie-Davidson over
+// the raised/lowered Cartesian functions: d/dx x^a e^{-a x^2} =
+// a x^{a-1} e - 2 alpha x^{a+1} e.
+// ======================================================================
+namespace {
+
+// Primitive-contracted Cartesian ERIs over all exponent tuples with total
+// <= lmax of each centre (dense table), then derivative blocks from it.
+struct RaisedTable {
+  int lm[4];
+  std::vector<std::array<int, 3>> tup[4];  // tuples per centre
+  std::vector<int> idx[4];                 // (ax,ay,az) -> position
+  std::vector<double> v;                   // [a][b][c][d]
+  int n[4];
+  int pos(int c, int x, int y, int z) const {
+    int L = lm[c] + 1;
+    if (x < 0 || y < 0 || z < 0 || x + y + z > lm[c]) return -1;
+    return idx[c][(x * L + y) * L + z];
+  }
+};
+
+void build_tuples(RaisedTable& T, int c, int lmax) {
+  T.lm[c] = lmax;
+  int L = lmax + 1;
+  T.idx[c].assign(L * L * L, -1);
+  T.tup[c].clear();
+  for (int l = 0; l <= lmax; l++)
+    for (int i = 0; i <= l; i++)
+      for (int j = 0; j <= i; j++) {
+        std::array<int, 3> t = {l - i, i - j, j};
+        T.idx[c][(t[0] * L + t[1]) * L + t[2]] = (int)T.tup[c].size();
+        T.tup[c].push_back(t);
+      }
+  T.n[c] = (int)T.tup[c].size();
+}
+
+// Uncontracted primitive table for exponents (a,b,c,d) on centres (A..D).
+void prim_table(double a, const double* A, double b, const double* B, double c, const double* C,
+                double d, const double* D, RaisedTable& T) {
+  int l1 = T.lm[0], l2 = T.lm[1], l3 = T.lm[2], l4 = T.lm[3];
+  int lab = l1 + l2, lcd = l3 + l4, L = lab + lcd;
+  double p = a + b, q = c + d, alpha = p * q / (p + q);
+  double P[3], Q[3], PQ[3];
+  for (int x = 0; x < 3; x++) {
+    P[x] = (a * A[x] + b * B[x]) / p;
+    Q[x] = (c * C[x] + d * D[x]) / q;
+    PQ[x] = P[x] - Q[x];
+  }
+  double AB2 = 0, CD2 = 0;
+  for (int x = 0; x < 3; x++) {
+    AB2 += (A[x] - B[x]) * (A[x] - B[x]);
+    CD2 += (C[x] - D[x]) * (C[x] - D[x]);
+  }
+  double Kab = std::exp(-a * b / p * AB2), Kcd = std::exp(-c * d / q * CD2);
+  double pref = 2.0 * std::pow(M_PI, 2.5) / (p * q * std::sqrt(p + q)) * Kab * Kcd;
+  std::vector<double> Eb[3], Ek[3];
+  for (int x = 0; x < 3; x++) {
+    hermite_E(l1, l2, p, P[x] - A[x], P[x] - B[x], Eb[x]);
+    hermite_E(l3, l4, q, Q[x] - C[x], Q[x] - D[x], Ek[x]);
+  }
+  int L1 = L + 1;
+  std::vector<double> R((size_t)(L + 1) * L1 * L1 * L1, 0.0);
+  auto Ridx = [&](int nn, int t, int u, int v) -> size_t {
+    return (((size_t)nn * L1 + t) * L1 + u) * L1 + v;
+  };
+  double F[96];
+  boys().eval(L, alpha * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]), F);
+  double f = 1.0;
+  for (int nn = 0; nn <= L; nn++) { R[Ridx(nn, 0, 0, 0)] = f * F[nn]; f *= -2.0 * alpha; }
+  for (int nn = L - 1; nn >= 0; nn--)
+    for (int t = 0; t <= L - nn; t++)
+      for (int u = 0; u <= L - nn - t; u++)
+        for (int v = 0; v <= L - nn - t - u; v++) {
+          if (t + u + v == 0) continue;
+          double val;
+          if (t > 0) {
+            val = PQ[0] * R[Ridx(nn + 1, t - 1, u, v)];
+            if (t > 1) val += (t - 1) * R[Ridx(nn + 1, t - 2, u, v)];
+          } else if (u > 0) {
+            val = PQ[1] * R[Ridx(nn + 1, t, u - 1, v)];
+            if (u > 1) val += (u - 1) * R[Ridx(nn + 1, t, u - 2, v)];
+          } else {
+            val = PQ[2] * R[Ridx(nn + 1, t, u, v - 1)];
+            if (v > 1) val += (v - 1) * R[Ridx(nn + 1, t, u, v - 2)];
+          }
+          R[Ridx(nn, t, u, v)] = val;
+        }
+  const int Lb1 = lab + 1, Lk1 = lcd + 1;
+  // G[cd][tuv]
+  int ncd = T.n[2] * T.n[3];
+  std::vector<double> G((size_t)ncd * Lb1 * Lb1 * Lb1, 0.0);
+  for (int ci = 0; ci < T.n[2]; ci++)
+    for (int di = 0; di < T.n[3]; di++) {
+      const auto &tc = T.tup[2][ci], &td = T.tup[3][di];
+      double* g = &G[((size_t)ci * T.n[3] + di) * Lb1 * Lb1 * Lb1];
+      const double* ex = &Ek[0][((size_t)tc[0] * (l4 + 1) + td[0]) * Lk1];
+      const double* ey = &Ek[1][((size_t)tc[1] * (l4 + 1) + td[1]) * Lk1];
+      const double* ez = &Ek[2][((size_t)tc[2] * (l4 + 1) + td[2]) * Lk1];
+      for (int t = 0; t <= lab; t++)
+        for (int u = 0; u <= lab - t; u++)
+          for (int v = 0; v <= lab - t - u; v++) {
+            double s = 0.0;
+            for (int ta = 0; ta <= tc[0] + td[0]; ta++)
+              for (int nu = 0; nu <= tc[1] + td[1]; nu++)
+                for (int ph = 0; ph <= tc[2] + td[2]; ph++) {
+                  double e = ex[ta] * ey[nu] * ez[ph];
+                  if ((ta + nu + ph) & 1) e = -e;
+                  s += e * R[Ridx(0, t + ta, u + nu, v + ph)];
+                }
+            g[(t * Lb1 + u) * Lb1 + v] = pref * s;
+          }
+    }
+  T.v.assign((size_t)T.n[0] * T.n[1] * ncd, 0.0);
+  for (int ai = 0; ai < T.n[0]; ai++)
+    for (int bi = 0; bi < T.n[1]; bi++) {
+      const auto &ta = T.tup[0][ai], &tb = T.tup[1][bi];
+      const double* ex = &Eb[0][((size_t)ta[0] * (l2 + 1) + tb[0]) * Lb1];
+      const double* ey = &Eb[1][((size_t)ta[1] * (l2 + 1) + tb[1]) * Lb1];
+      const double* ez = &Eb[2][((size_t)ta[2] * (l2 + 1) + tb[2]) * Lb1];
+      for (int cd = 0; cd < ncd; cd++) {
+        const double* g = &G[(size_t)cd * Lb1 * Lb1 * Lb1];
+        double s = 0.0;
+        for (int t = 0; t <= ta[0] + tb[0]; t++)
+          for (int u = 0; u <= ta[1] + tb[1]; u++)
+            for (int v = 0; v <= ta[2] + tb[2]; v++)
+              s += ex[t] * ey[u] * ez[v] * g[(t * Lb1 + u) * Lb1 + v];
+        T.v[((size_t)ai * T.n[1] + bi) * ncd + cd] = s;
+      }
+    }
+}
+
+// Derivative ERIs of a contracted quartet: comp-major blocks
+// out[comp][i][j][k][l] over the AO functions of s1..s4 (spherical where
+// pure), with derivatives (d/dr of the orbital) on the centres in dmask
+// (bit 0..3 = s1..s4); comp = sum over differentiated centres, in order,
+// of 3-digit indices (x, y, z), the last centre varying fastest.
+void eri_deriv_quartet(const Basis& bs, int s1, int s2, int s3, int s4, int dmask,
+                       std::vector<double>& out) {
+  const int sh[4] = {s1, s2, s3, s4};
+  const Shell* S[4] = {&bs.shells[s1], &bs.shells[s2], &bs.shells[s3], &bs.shells[s4]};
+  int nd = 0;
+  for (int c = 0; c < 4; c++) nd += (dmask >> c) & 1;
+  int ncomp = 1;
+  for (int k = 0; k < nd; k++) ncomp *= 3;
+  int nc[4];
+  for (int c = 0; c < 4; c++) nc[c] = ncart(S[c]->l);
+  const size_t ncart4 = (size_t)nc[0] * nc[1] * nc[2] * nc[3];
+  std::vector<double> cart((size_t)ncomp * ncart4, 0.0);
+  RaisedTable T;
+  for (int c = 0; c < 4; c++) build_tuples(T, c, S[c]->l + ((dmask >> c) & 1));
+  for (size_t i = 0; i < S[0]->alpha.size(); i++)
+    for (size_t j = 0; j < S[1]->alpha.size(); j++)
+      for (size_t k = 0; k < S[2]->alpha.size(); k++)
+        for (size_t l = 0; l < S[3]->alpha.size(); l++) {
+          const double ex[4] = {S[0]->alpha[i], S[1]->alpha[j], S[2]->alpha[k], S[3]->alpha[l]};
+          const double cf = S[0]->coef[i] * S[1]->coef[j] * S[2]->coef[k] * S[3]->coef[l];
+          prim_table(ex[0], S[0]->O, ex[1], S[1]->O, ex[2], S[2]->O, ex[3], S[3]->O, T);
+          const int nT2 = T.n[2] * T.n[3], nT1 = T.n[1];
+          for (int a = 0; a < nc[0]; a++)
+            for (int b = 0; b < nc[1]; b++)
+              for (int c = 0; c < nc[2]; c++)
+                for (int d = 0; d < nc[3]; d++) {
+                  int base[4][3];
+                  const int comps[4] = {a, b, c, d};
+                  for (int q = 0; q < 4; q++) {
+                    base[q][0] = bs.cx[S[q]->l][comps[q]];
+                    base[q][1] = bs.cy[S[q]->l][comps[q]];
+                    base[q][2] = bs.cz[S[q]->l][comps[q]];
+                  }
+                  const size_t cidx = (((size_t)a * nc[1] + b) * nc[2] + c) * nc[3] + d;
+                  for (int comp = 0; comp < ncomp; comp++) {
+                    // direction of each differentiated centre
+                    int dir[4] = {-1, -1, -1, -1};
+                    int rem = comp;
+                    for (int q = 3; q >= 0; q--)
+                      if ((dmask >> q) & 1) { dir[q] = rem % 3; rem /= 3; }
+                    // sum over lowered (-) / raised (+) choices
+                    double val = 0.0;
+                    for (int sel = 0; sel < (1 << 4); sel++) {
+                      bool ok = true;
+                      double w = 1.0;
+                      int tp[4][3];
+                      for (int q = 0; q < 4 && ok; q++) {
+                        for (int x = 0; x < 3; x++) tp[q][x] = base[q][x];
+                        if (dir[q] < 0) {
+                          if ((sel >> q) & 1) ok = false;
+                          continue;
+                        }
+                        if ((sel >> q) & 1) {  // raised: -2 alpha
+                          tp[q][dir[q]] += 1;
+                          w *= -2.0 * ex[q];
+                        } else {  // lowered: a_i
+                          int ai = base[q][dir[q]];
+                          if (ai == 0) { ok = false; continue; }
+                          tp[q][dir[q]] -= 1;
+                          w *= ai;
+                        }
+                      }
+                      if (!ok) continue;
+                      int p0 = T.pos(0, tp[0][0], tp[0][1], tp[0][2]);
+                      int p1 = T.pos(1, tp[1][0], tp[1][1], tp[1][2]);
+                      int p2 = T.pos(2, tp[2][0], tp[2][1], tp[2][2]);
+                      int p3 = T.pos(3, tp[3][0], tp[3][1], tp[3][2]);
+                      val += w * T.v[((size_t)p0 * nT1 + p1) * nT2 + (size_t)p2 * T.n[3] + p3];
+                    }
+                    cart[(size_t)comp * ncart4 + cidx] += cf * val;
+                  }
+                }
+        }
+  // spherical transform of every component block
+  size_t nsph4 = 1;
+  for (int c = 0; c < 4; c++) nsph4 *= S[c]->size();
+  out.assign((size_t)ncomp * nsph4, 0.0);
+  std::vector<double> blk;
+  for (int comp = 0; comp < ncomp; comp++) {
+    blk.assign(cart.begin() + comp * ncart4, cart.begin() + (comp + 1) * ncart4);
+    cart_to_sph_block(bs, S, 4, blk);
+    std::copy(blk.begin(), blk.end(), out.begin() + comp * nsph4);
+  }
+  (void)sh;
+}
+
+}  // namespace
+
+namespace {
+
+using cdbl = std::complex<double>;
+const cdbl I1(0.0, 1.0);
+
+// s + v.sigma (2x2 spin matrix in Pauli components)
+struct Q4 {
+  cdbl s, v[3];
+};
+Q4 qmul(const Q4& p, const Q4& q) {
+  Q4 r;
+  r.s = p.s * q.s + p.v[0] * q.v[0] + p.v[1] * q.v[1] + p.v[2] * q.v[2];
+  for (int x = 0; x < 3; x++) {
+    int y = (x + 1) % 3, z = (x + 2) % 3;
+    r.v[x] = p.s * q.v[x] + q.s * p.v[x] + I1 * (p.v[y] * q.v[z] - p.v[z] * q.v[y]);
+  }
+  return r;
+}
+Q4 sigma(int a) {  // a = 0 (identity), 1..3 (x, y, z)
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  if (a == 0) r.s = 1.0;
+  else r.v[a - 1] = 1.0;
+  return r;
+}
+
+// Index of the 17 (X, AX) pairs of a 4C contraction list
+// (DIRAC_PAULI_SPINOR_COMP, direct4C_libcint.hpp:279-310).
+enum { CLLMS, XLLMS, XLLMX, XLLMY, XLLMZ, CSSMS, CSSMX, CSSMY, CSSMZ, XSSMS, XSSMX, XSSMY,
+       XSSMZ, XLSMS, XLSMX, XLSMY, XLSMZ, NREL };
+
+// (i, j, sign) patterns of the dot (a = 0) and cross (a = 1..3) products of
+// two derivative directions.
+struct Pat { int i, j; double s; };
+const std::vector<Pat>& pat(int a) {
+  static const std::vector<Pat> P[4] = {
+      {{0, 0, 1}, {1, 1, 1}, {2, 2, 1}},
+      {{1, 2, 1}, {2, 1, -1}},
+      {{2, 0, 1}, {0, 2, -1}},
+      {{0, 1, 1}, {1, 0, -1}}};
+  return P[a];
+}
+
+// Shell-block norms of one complex N x N matrix (direct.hpp:73-90).
+void norms_c(const Basis& bs, const cdbl* X, std::vector<double>& out) {
+  int ns = (int)bs.shells.size(), N = bs.nbasis;
+  out.assign((size_t)ns * ns, 0.0);
+  shell_block_norm(bs, X, N, out.data());
+}
+
+struct Schwarz4C {
+  std::vector<double> LL, SS;  // nshell^2
+};
+
+// direct4C_libcint.hpp:341-481
+void schwarz_4c(const Basis& bs, bool needLL, bool needSS, Schwarz4C& Q) {
+  const int ns = (int)bs.shells.size();
+  const double C2 = 1.0 / (4.0 * 137.035999074 * 137.035999074);
+  if (needLL) Q.LL.assign((size_t)ns * ns, 0.0);
+  if (needSS) Q.SS.assign((size_t)ns * ns, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int s1 = 0; s1 < ns; s1++) {
+    std::vector<double> buf, scr;
+    for (int s2 = 0; s2 <= s1; s2++) {
+      if (needLL) {
+        eri_quartet(bs, s1, s2, s1, s2, buf, scr);
+        double mx = 0;
+        for (double v : buf) mx = std::max(mx, std::abs(v));
+        Q.LL[s1 + (size_t)s2 * ns] = Q.LL[s2 + (size_t)s1 * ns] = std::sqrt(mx);
+      }
+      if (needSS) {
+        eri_deriv_quartet(bs, s1, s2, s1, s2, 15, buf);
+        double mx = 0;
+        for (double v : buf) mx = std::max(mx, std::abs(v));
+        Q.SS[s1 + (size_t)s2 * ns] = Q.SS[s2 + (size_t)s1 * ns] = C2 * std::sqrt(mx);
+      }
+    }
+  }
+}
+
+inline Q4 dens(const cdbl* const* X, int base, size_t e) {
+  return Q4{X[base][e], {X[base + 1][e], X[base + 2][e], X[base + 3][e]}};
+}
+
+// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS) of
+// directScaffoldLibcint; AX (17 N x N complex) is zeroed first (:313-314).
+void direct_4c(const Basis& bs, int type, const cdbl* const* X, cdbl* const* AX, double thresh,
+               const Schwarz4C& Qs, bool exchange) {
+  const int ns = (int)bs.shells.size(), N = bs.nbasis;
+  const size_t NN = (size_t)N * N;
+  for (int m = 0; m < NREL; m++) std::fill(AX[m], AX[m] + NN, cdbl(0.0));
+  // max shell-block norms over the matrices each type screens with
+  std::vector<int> mats;
+  if (type == 0) mats = {CLLMS, XLLMS, XLLMX, XLLMY, XLLMZ};
+  else if (type == 1) mats = {CLLMS, CSSMS, CSSMX, CSSMY, CSSMZ, XLSMS, XLSMX, XLSMY, XLSMZ};
+  else mats = {CSSMS, CSSMX, CSSMY, CSSMZ};
+  std::vector<double> nrm((size_t)ns * ns, 0.0), tmp;
+  for (int m : mats) {
+    norms_c(bs, X[m], tmp);
+    for (size_t i = 0; i < nrm.size(); i++) nrm[i] = std::max(nrm[i], std::abs(tmp[i]));
+  }
+  auto B = [&](int a, int b) { return nrm[a + (size_t)b * ns]; };
+  const double* Q12 = (type == 0) ? Qs.LL.data() : Qs.SS.data();
+  const double* Q34 = (type == 2) ? Qs.SS.data() : Qs.LL.data();
+  const int nth = omp_get_max_threads();
+  std::vector<cdbl> loc((size_t)nth * NREL * NN, cdbl(0.0));
+#pragma omp parallel
+  {
+    const int tid = omp_get_thread_num();
+    cdbl* A[NREL];
+    for (int m = 0; m < NREL; m++) A[m] = &loc[((size_t)tid * NREL + m) * NN];
+    auto ix = [N](int r, int c) { return (size_t)r + (size_t)c * N; };
+    std::vector<double> buf, scr;
+    size_t s1234 = 0;
+    for (int s1 = 0; s1 < ns; s1++)
+      for (int s2 = 0; s2 <= s1; s2++) {
+        const double shMax12 = B(s1, s2);
+        const int s3max = (type == 1) ? ns - 1 : s1;
+        for (int s3 = 0; s3 <= s3max; s3++) {
+          const double shMax123 = std::max(std::max(B(s1, s3), B(s2, s3)), shMax12);
+          const int s4max = (type == 1) ? s3 : ((s1 == s3) ? s2 : s3);
+          for (int s4 = 0; s4 <= s4max; s4++, s1234++) {
+            if (s1234 % nth != (size_t)tid) continue;
+            double shMax = std::max(B(s1, s4), std::max(B(s2, s4), B(s3, s4)));
+            shMax = std::max(shMax, shMax123);
+            if (shMax * Q12[s1 + (size_t)s2 * ns] * Q34[s3 + (size_t)s4 * ns] < thresh) continue;
+            const int n1 = bs.shells[s1].size(), n2 = bs.shells[s2].size();
+            const int n3 = bs.shells[s3].size(), n4 = bs.shells[s4].size();
+            const int o1 = bs.off[s1], o2 = bs.off[s2], o3 = bs.off[s3], o4 = bs.off[s4];
+            const double s12d = (s1 == s2) ? 1.0 : 2.0, s34d = (s3 == s4) ? 1.0 : 2.0;
+            const size_t nq = (size_t)n1 * n2 * n3 * n4;
+            if (type == 0) {
+              eri_quartet(bs, s1, s2, s3, s4, buf, scr);
+              const double deg = s12d * s34d * ((s1 == s3) ? (s2 == s4 ? 1.0 : 2.0) : 2.0);
+              for (int i = 0; i < n1; i++)
+                for (int j = 0; j < n2; j++)
+                  for (int k = 0; k < n3; k++)
+                    for (int l = 0; l < n4; l++) {
+                      const int b1 = o1 + i, b2 = o2 + j, b3 = o3 + k, b4 = o4 + l;
+                      double v = buf[(((size_t)i * n2 + j) * n3 + k) * n4 + l] * 0.5 * deg;
+                      A[CLLMS][ix(b1, b2)] += v * X[CLLMS][ix(b4, b3)].real();
+                      A[CLLMS][ix(b3, b4)] += v * X[CLLMS][ix(b2, b1)].real();
+                      v *= 0.5;
+                      for (int c = 0; c < 4; c++) {
+                        A[XLLMS + c][ix(b1, b4)] += v * X[XLLMS + c][ix(b2, b3)];
+                        A[XLLMS + c][ix(b1, b3)] += v * X[XLLMS + c][ix(b2, b4)];
+                        A[XLLMS + c][ix(b2, b4)] += v * X[XLLMS + c][ix(b1, b3)];
+                        A[XLLMS + c][ix(b2, b3)] += v * X[XLLMS + c][ix(b1, b4)];
+                      }
+                    }
+              continue;
+            }
+            // derivative integrals: LLSS on (s1 s2), SSSS on all four
+            eri_deriv_quartet(bs, s1, s2, s3, s4, type == 1 ? 3 : 15, buf);
+            for (int i = 0; i < n1; i++)
+              for (int j = 0; j < n2; j++)
+                for (int k = 0; k < n3; k++)
+                  for (int l = 0; l < n4; l++) {
+                    const int b1 = o1 + i, b2 = o2 + j, b3 = o3 + k, b4 = o4 + l;
+                    const size_t q = (((size_t)i * n2 + j) * n3 + k) * n4 + l;
+                    if (type == 1) {
+                      // operator components of the (1 2) pair
+                      double M[4];
+                      for (int a = 0; a < 4; a++) {
+                        M[a] = 0.0;
+                        for (const auto& p : pat(a)) M[a] += p.s * buf[(size_t)(3 * p.i + p.j) * nq + q];
+                      }
+                      // Coulomb: LL(3,4) from the SS density, SS(1,2) from LL
+                      if (b3 >= b4) {
+                        const Q4 d = dens(X, CSSMS, ix(b2, b1));
+                        double r = M[0] * d.s.real();
+                        for (int x = 0; x < 3; x++) r -= M[x + 1] * d.v[x].imag();
+                        A[CLLMS][ix(b3, b4)] += s12d * r;
+                      }
+                      if (b1 >= b2) {
+                        const double rho = X[CLLMS][ix(b4, b3)].real();
+                        for (int a = 0; a < 4; a++) A[CSSMS + a][ix(b1, b2)] += s34d * M[a] * rho;
+                      }
+                      if (!exchange) continue;
+                      // exchange LS blocks: -D P (P12 or P21)
+                      auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
+                        const Q4 d = dens(X, XLSMS, ix(d1, d2));
+                        Q4 r{0.0, {0.0, 0.0, 0.0}};
+                        for (int a = 0; a < 4; a++) {
+                          const cdbl c = (a == 0) ? cdbl(M[0]) : I1 * (flip * M[a]);
+                          const Q4 t = qmul(d, sigma(a));
+                          r.s += c * t.s;
+                          for (int x = 0; x < 3; x++) r.v[x] += c * t.v[x];
+                        }
+                        A[XLSMS][ix(t1, t2)] -= r.s;
+                        for (int x = 0; x < 3; x++) A[XLSMX + x][ix(t1, t2)] -= r.v[x];
+                      };
+                      ls(b3, b2, b4, b1, 1.0);
+                      if (s1 != s2) ls(b3, b1, b4, b2, -1.0);
+                      if (s3 != s4) {
+                        ls(b4, b2, b3, b1, 1.0);
+                        if (s1 != s2) ls(b4, b1, b3, b2, -1.0);
+                      }
+                    } else {
+                      // combined operator components M[a][b] of (12)(34)
+                      double M[4][4];
+                      for (int a = 0; a < 4; a++)
+                        for (int b = 0; b < 4; b++) {
+                          double s = 0.0;
+                          for (const auto& p : pat(a))
+                            for (const auto& r : pat(b))
+                              s += p.s * r.s * buf[(size_t)(27 * p.i + 9 * p.j + 3 * r.i + r.j) * nq + q];
+                          M[a][b] = s;
+                        }
+                      // Coulomb: SS(t) = P_t rho, rho = Re Tr[P_o D(o2,o1)]/2
+                      auto coul = [&](int t1, int t2, int d1, int d2, bool swap, double sd) {
+                        const Q4 d = dens(X, CSSMS, ix(d1, d2));
+                        const double rv[4] = {d.s.real(), -d.v[0].imag(), -d.v[1].imag(),
+                                              -d.v[2].imag()};
+                        for (int a = 0; a < 4; a++) {
+                          double s = 0.0;
+                          for (int b = 0; b < 4; b++) s += (swap ? M[b][a] : M[a][b]) * rv[b];
+                          A[CSSMS + a][ix(t1, t2)] += sd * s;
+                        }
+                      };
+                      if (b1 >= b2) coul(b1, b2, b4, b3, false, s34d);
+                      if ((s1 != s3 || s2 != s4) && b3 >= b4) coul(b3, b4, b2, b1, true, s12d);
+                      if (!exchange) continue;
+                      // exchange SS: -P_first D P_second (fl: orientation signs)
+                      auto ex = [&](int t1, int t2, int d1, int d2, bool swap, double f1, double f2) {
+                        const Q4 d = dens(X, XSSMS, ix(d1, d2));
+                        Q4 r{0.0, {0.0, 0.0, 0.0}};
+                        for (int a = 0; a < 4; a++)
+                          for (int b = 0; b < 4; b++) {
+                            const double m = swap ? M[b][a] : M[a][b];
+                            if (m == 0.0) continue;
+                            cdbl c = m;
+                            if (a > 0) c *= I1 * f1;
+                            if (b > 0) c *= I1 * f2;
+                            const Q4 t = qmul(qmul(sigma(a), d), sigma(b));
+                            r.s += c * t.s;
+                            for (int x = 0; x < 3; x++) r.v[x] += c * t.v[x];
+                          }
+                        A[XSSMS][ix(t1, t2)] -= r.s;
+                        for (int x = 0; x < 3; x++) A[XSSMX + x][ix(t1, t2)] -= r.v[x];
+                      };
+                      if (b1 >= b4) ex(b1, b4, b2, b3, false, 1, 1);
+                      if (s3 != s4 && b1 >= b3) ex(b1, b3, b2, b4, false, 1, -1);
+                      if (s1 != s2) {
+                        if (b2 >= b4) ex(b2, b4, b1, b3, false, -1, 1);
+                        if (s3 != s4 && b2 >= b3) ex(b2, b3, b1, b4, false, -1, -1);
+                      }
+                      if (s1 != s3 || s2 != s4) {
+                        if (b3 >= b2) ex(b3, b2, b4, b1, true, 1, 1);
+                        if (s1 != s2 && b3 >= b1) ex(b3, b1, b4, b2, true, 1, -1);
+                        if (s3 != s4 && b4 >= b2) {
+                          ex(b4, b2, b3, b1, true, -1, 1);
+                          if (s1 != s2 && b4 >= b1) ex(b4, b1, b3, b2, true, -1, -1);
+                        }
+                      }
+                    }
+                  }
+          }
+        }
+      }
+  }
+  // thread reduction and the per-type epilogues
+  std::vector<cdbl> red((size_t)NREL * NN, cdbl(0.0));
+  for (int t = 0; t < nth; t++)
+    for (size_t e = 0; e < (size_t)NREL * NN; e++) red[e] += loc[(size_t)t * NREL * NN + e];
+  auto R = [&](int m) { return &red[(size_t)m * NN]; };
+  if (type == 0) {
+    for (int m = CLLMS; m <= XLLMZ; m++)
+      for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++)
+          AX[m][i + (size_t)j * N] += 0.5 * R(m)[i + (size_t)j * N] + 0.5 * std::conj(R(m)[j + (size_t)i * N]);
+    return;
+  }
+  std::vector<int> her;
+  for (int m = 0; m < NREL; m++) {
+    cdbl f = (m == CSSMX || m == CSSMY || m == CSSMZ) ? I1 : cdbl(1.0);
+    for (size_t e = 0; e < NN; e++) AX[m][e] += f * R(m)[e];
+  }
+  if (type == 1) her = {CLLMS, CSSMS, CSSMX, CSSMY, CSSMZ};
+  else her = {CSSMS, CSSMX, CSSMY, CSSMZ, XSSMS, XSSMX, XSSMY, XSSMZ};
+  for (int m : her)
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < i; j++) AX[m][j + (size_t)i * N] = std::conj(AX[m][i + (size_t)j * N]);
+}
+
+}  // namespace
+
+extern "C" {
+
+// FourCompFock::formGDDirect (fourcompfock/impl.hpp:3752-4636) with
+// BareCoulomb / DiracCoulomb / DiracCoulombSSSS switches.  D and G: 4 Pauli
+// components (S, X, Y, Z) of 2N x 2N complex column-major matrices; G gets
+// twoeH - xHFX * K.
+// libcint selects the reference's bare-Coulomb branch: with libcint the
+// 17-entry BARE_COULOMB contraction and twoeH_LL = 2 CLLMS
+// (fourcompfock/impl.hpp:3901-3933), without it the 1C J/K contraction and
+// twoeH_LL = J (:3934-3969).
+int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare, int dc,
+                      int ssss, double xHFX, double thresh, int libcint) {
+  auto* bs = static_cast<Basis*>(b);
+  const int N = bs->nbasis, N2 = 2 * N;
+  const cdbl* const* D = reinterpret_cast<const cdbl* const*>(Dv);
+  cdbl* const* G = reinterpret_cast<cdbl* const*>(Gv);
+  const double c = 137.035999074, C2 = 1.0 / (4 * c * c), C4 = 1.0 / (16 * c * c * c * c);
+  const bool exch = std::abs(xHFX) >= 1e-12;
+  const size_t NN = (size_t)N * N, NN2 = (size_t)N2 * N2;
+  // blocks LL, SS, LS of each Pauli component
+  std::vector<cdbl> blk[3][4];
+  for (int cmp = 0; cmp < 4; cmp++)
+    for (int k = 0; k < 3; k++) {
+      blk[k][cmp].assign(NN, 0.0);
+      const int ro = (k == 1) ? N : 0, co = (k == 0) ? 0 : N;  // LL (0,0) SS (N,N) LS (0,N)
+      for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++)
+          blk[k][cmp][i + (size_t)j * N] = D[cmp][(ro + i) + (size_t)(co + j) * N2];
+    }
+  std::vector<cdbl> ax((size_t)NREL * NN);
+  const cdbl* X[NREL];
+  cdbl* AX[NREL];
+  for (int m = 0; m < NREL; m++) AX[m] = &ax[(size_t)m * NN];
+  X[CLLMS] = blk[0][0].data();
+  for (int c4 = 0; c4 < 4; c4++) {
+    X[XLLMS + c4] = blk[0][c4].data();
+    X[CSSMS + c4] = blk[1][c4].data();
+    X[XSSMS + c4] = blk[1][c4].data();
+    X[XLSMS + c4] = blk[2][c4].data();
+  }
+  std::vector<cdbl> twoeH[4], K[4];
+  for (int c4 = 0; c4 < 4; c4++) {
+    twoeH[c4].assign(NN2, 0.0);
+    K[c4].assign(NN2, 0.0);
+  }
+  auto add = [&](std::vector<cdbl>& dst, int ro, int co, const cdbl* src, cdbl f) {
+    for (int j = 0; j < N; j++)
+      for (int i = 0; i < N; i++) dst[(ro + i) + (size_t)(co + j) * N2] += f * src[i + (size_t)j * N];
+  };
+  Schwarz4C Qs;
+  schwarz_4c(*bs, bare || dc, dc || ssss, Qs);
+  if (bare) {
+    direct_4c(*bs, 0, X, AX, thresh, Qs, exch);
+    add(twoeH[0], 0, 0, AX[CLLMS], libcint ? 2.0 : 1.0);
+    if (exch)
+      for (int c4 = 0; c4 < 4; c4++) add(K[c4], 0, 0, AX[XLLMS + c4], 1.0);
+  }
+  if (dc) {
+    direct_4c(*bs, 1, X, AX, thresh, Qs, exch);
+    add(twoeH[0], 0, 0, AX[CLLMS], 2.0 * C2);
+    for (int c4 = 0; c4 < 4; c4++) add(twoeH[c4], N, N, AX[CSSMS + c4], 2.0 * C2);
+    if (exch)
+      for (int c4 = 0; c4 < 4; c4++) add(K[c4], 0, N, AX[XLSMS + c4], -C2);
+  }
+  if (ssss) {
+    direct_4c(*bs, 2, X, AX, thresh, Qs, exch);
+    for (int c4 = 0; c4 < 4; c4++) add(twoeH[c4], N, N, AX[CSSMS + c4], 2.0 * C4);
+    if (exch)
+      for (int c4 = 0; c4 < 4; c4++) add(K[c4], N, N, AX[XSSMS + c4], -C4);
+  }
+  // LS -> SL as the conjugate transpose, then G = twoeH - xHFX K
+  for (int c4 = 0; c4 < 4; c4++) {
+    for (auto* M : {&twoeH[c4], &K[c4]})
+      for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++)
+          (*M)[(N + j) + (size_t)i * N2] = std::conj((*M)[i + (size_t)(N + j) * N2]);
+    for (size_t e = 0; e < NN2; e++) G[c4][e] = twoeH[c4][e] - (exch ? xHFX * K[c4][e] : 0.0);
+  }
+  return 0;
 }
 
 }  // extern "C"

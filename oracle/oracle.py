@@ -56,6 +56,10 @@ def lib():
                                    C.c_int, C.POINTER(C.c_longlong)]
         L.orc_flops.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                 C.c_double, C.c_double, dp]
+        L.orc_dirac_coulomb.argtypes = [C.c_void_p, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p), C.c_int, C.c_int,
+                                        C.c_int, C.c_double, C.c_double, C.c_int]
+        L.orc_dirac_coulomb.restype = C.c_int
         _lib = L
     return _lib
 
@@ -148,6 +152,18 @@ class OracleBasis:
                            thresh, nthreads, 1 if screen else 0, st)
         self.last_stats = dict(total=st[0], screened=st[1], computed=st[2])
         return AX
+
+    def dirac_coulomb(self, D, bare=True, dc=True, ssss=True, xHFX=1.0,
+                      thresh=1e-12, libcint=True):
+        """FourCompFock::formGDDirect: D = [S, X, Y, Z] Pauli components of
+        the 2N x 2N density; returns G = twoeH - xHFX K (same layout)."""
+        Ds = [np.asfortranarray(d, dtype=np.complex128) for d in D]
+        Gs = [np.zeros_like(d, order="F") for d in Ds]
+        dp_ = (C.c_void_p * 4)(*[d.ctypes.data for d in Ds])
+        gp_ = (C.c_void_p * 4)(*[g.ctypes.data for g in Gs])
+        lib().orc_dirac_coulomb(self.h, dp_, gp_, int(bare), int(dc), int(ssss),
+                                xHFX, thresh, int(libcint))
+        return Gs
 
     def flops(self, mats, thresh=1e-12, fp32_cut=0.0):
         Xs = [np.asfortranarray(np.abs(m), dtype=np.float64) for m in mats]

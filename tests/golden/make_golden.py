@@ -81,6 +81,31 @@ def main(ref_root):
         ref_root, "tests/scf/serial/fourcomp/water_cc-pVDZ_DC-HF_READDEN.inp")))
     np.savez_compressed(os.path.join(HERE, "readden_dc.npz"), **dc)
 
+    # 4C build from a full 4C density (DC-HF guess, libcint, bare Coulomb
+    # only -- the stored FOCK has zero SS / LS two-electron blocks): the LL
+    # blocks of D and of G = FOCK - CORE_H, all four Pauli components.
+    f = H5File(os.path.join(rd, "water_cc-pVDZ_DC-HF_DCHFGuess_READDEN_scratch.bin.ref"))
+    N = 40
+    out = {}
+    for comp in ("SCALAR", "MX", "MY", "MZ"):
+        D = f.read("/SCF/1PDM_" + comp).T
+        G = f.read("/SCF/FOCK_" + comp).T - f.read("/INTS/CORE_HAMILTONIAN_" + comp).T
+        out["D_" + comp] = np.where(np.abs(D) < 1e-200, 0, D)[:N, :N].copy()
+        out["G_" + comp] = np.where(np.abs(G) < 1e-200, 0, G)[:N, :N].copy()
+    np.savez_compressed(os.path.join(HERE, "readden_dchf_ll.npz"), **out)
+
+    # converged complex 4C-HF water / 6-31G(d) with Dirac-Coulomb (LLSS) on,
+    # SSSS off, non-libcint bare Coulomb
+    # (tests/scf/serial/qn/water_6-31Gd_4chf_bfgs.inp): D and G = F - H.
+    f = H5File(os.path.join(rd, "water_6-31Gd_qn_4chf.bin.ref"))
+    out = {}
+    for comp in ("SCALAR", "MX", "MY", "MZ"):
+        D = f.read("/SCF/1PDM_" + comp).T
+        G = f.read("/SCF/FOCK_" + comp).T - f.read("/INTS/CORE_HAMILTONIAN_" + comp).T
+        out["D_" + comp] = np.where(np.abs(D) < 1e-200, 0, D).copy()
+        out["G_" + comp] = np.where(np.abs(G) < 1e-200, 0, G).copy()
+    np.savez_compressed(os.path.join(HERE, "qn_4chf_dc.npz"), **out)
+
 
 if __name__ == "__main__":
     main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

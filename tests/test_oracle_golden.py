@@ -5,8 +5,9 @@ import numpy as np
 import pytest
 
 import oracle as O
+from chronusq_public_b200.basis import BasisSet, parse_gbs
 from helpers import (CONTRACT_CASES, contract_basis, golden,
-                     readden_rhf_basis)
+                     readden_rhf_basis, water_ref)
 
 
 @pytest.fixture(scope="module")
@@ -58,3 +59,52 @@ def test_boys_against_series(m, T):
         t = 0.5 * (b - a) * x + 0.5 * (a + b)
         tot += 0.5 * (b - a) * np.sum(w * t ** (2 * m) * np.exp(-T * t * t))
     assert abs(O.boys(m, T) - tot) <= 1e-14 * max(tot, 1e-300) + 1e-300
+
+
+def _readden_dc_basis():
+    return BasisSet.build(water_ref(), parse_gbs(str(golden("readden_dc.npz")["basisdef"])))
+
+
+PAULI = ("SCALAR", "MX", "MY", "MZ")
+
+
+def test_dirac_coulomb_bare_libcint():
+    """4C bare Coulomb (libcint branch, twoeH_LL = 2 CLLMS,
+    fourcompfock/impl.hpp:3901-3933) against the DC-HF-guess READDEN build,
+    whose stored FOCK carries only the LL two-electron block."""
+    g = golden("readden_dchf_ll.npz")
+    ob = O.OracleBasis(_readden_dc_basis())
+    N = ob.nbasis
+    D = []
+    for c in PAULI:
+        d = np.zeros((2 * N, 2 * N), dtype=np.complex128)
+        d[:N, :N] = g["D_" + c]
+        D.append(d)
+    G = ob.dirac_coulomb(D, bare=True, dc=False, ssss=False, libcint=True)
+    for k, c in enumerate(PAULI):
+        assert np.abs(G[k][:N, :N] - g["G_" + c]).max() < 1e-9, c
+        assert np.abs(G[k][N:, :]).max() == 0 and np.abs(G[k][:, N:]).max() == 0
+
+
+def test_dirac_coulomb_rhf_guess():
+    """Same build from the RHF-guess READDEN density (spin components zero)."""
+    g = golden("readden_dc.npz")
+    ob = O.OracleBasis(_readden_dc_basis())
+    D = [np.where(np.abs(g["D_" + c]) < 1e-200, 0, g["D_" + c]) for c in PAULI]
+    G = ob.dirac_coulomb(D, bare=True, dc=False, ssss=False, libcint=True)
+    for k, c in enumerate(PAULI):
+        ref = g["F_" + c] - g["H_" + c]
+        ref = np.where(np.abs(ref) < 1e-200, 0, ref)
+        assert np.abs(G[k] - ref).max() < 1e-9, c
+
+
+def test_dirac_coulomb_llss():
+    """Converged complex 4C-HF water / 6-31G(d) with the Dirac-Coulomb LLSS
+    terms (SS and LS blocks from the derivative ERIs, impl.hpp:4003-4147) and
+    the non-libcint bare Coulomb (twoeH_LL = J, impl.hpp:3934-3969)."""
+    g = golden("qn_4chf_dc.npz")
+    ob = O.OracleBasis(BasisSet.build(water_ref(), "6-31gd"))
+    D = [g["D_" + c] for c in PAULI]
+    G = ob.dirac_coulomb(D, bare=True, dc=True, ssss=False, libcint=False)
+    for k, c in enumerate(PAULI):
+        assert np.abs(G[k] - g["G_" + c]).max() < 1e-9, c
