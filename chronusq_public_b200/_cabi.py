@@ -21,7 +21,13 @@ EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
            "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
            "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
-           "cqf_last_error")
+           "cqf_rel_two_body_contract", "cqf_dc_opts_default",
+           "cqf_four_comp_gd", "cqf_last_error")
+# cqf_rel_comp / cqf_rel_type (DIRAC_PAULI_SPINOR_COMP order)
+(CQF_CLLMS, CQF_XLLMS, CQF_XLLMX, CQF_XLLMY, CQF_XLLMZ, CQF_CSSMS, CQF_CSSMX,
+ CQF_CSSMY, CQF_CSSMZ, CQF_XSSMS, CQF_XSSMX, CQF_XSSMY, CQF_XSSMZ, CQF_XLSMS,
+ CQF_XLSMX, CQF_XLSMY, CQF_XLSMZ, CQF_REL_NMAT) = range(18)
+CQF_REL_BARE_COULOMB, CQF_REL_LLSS, CQF_REL_SSSS = range(3)
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 
@@ -49,6 +55,12 @@ class CqfStats(C.Structure):
                 ("quartets_fp32", C.c_longlong),
                 ("quartets_fp64", C.c_longlong),
                 ("device_ms", C.c_double)]
+
+
+class CqfDcOpts(C.Structure):
+    _fields_ = [("bare_coulomb", C.c_int), ("dirac_coulomb", C.c_int),
+                ("dirac_coulomb_ssss", C.c_int), ("libcint", C.c_int),
+                ("xHFX", C.c_double)]
 
 
 class CqfError(RuntimeError):
@@ -98,6 +110,16 @@ def lib():
     L.cqf_graph_launch.restype = C.c_int
     L.cqf_graph_destroy.argtypes = [C.c_void_p]
     L.cqf_graph_destroy.restype = C.c_int
+    L.cqf_rel_two_body_contract.argtypes = [
+        C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int,
+        C.c_int, C.POINTER(CqfOpts), C.POINTER(CqfStats)]
+    L.cqf_rel_two_body_contract.restype = C.c_int
+    L.cqf_dc_opts_default.argtypes = [C.POINTER(CqfDcOpts)]
+    L.cqf_dc_opts_default.restype = None
+    L.cqf_four_comp_gd.argtypes = [
+        C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+        C.POINTER(CqfDcOpts), C.POINTER(CqfOpts), C.POINTER(CqfStats)]
+    L.cqf_four_comp_gd.restype = C.c_int
     L.cqf_last_error.argtypes = []
     L.cqf_last_error.restype = C.c_char_p
     _lib = L

@@ -231,3 +231,79 @@ class GTODirectTPIContraction:
                                screened=st.quartets_screened,
                                fp32=st.quartets_fp32, fp64=st.quartets_fp64,
                                device_ms=st.device_ms)
+
+
+# ---------------------------------------------------------------- 4C
+BARE_COULOMB, LLSS, SSSS = (_cabi.CQF_REL_BARE_COULOMB, _cabi.CQF_REL_LLSS,
+                            _cabi.CQF_REL_SSSS)
+# DIRAC_PAULI_SPINOR_COMP order of the 17 (X, AX) entries
+# (include/particleintegrals/contract/direct4C_libcint.hpp:279-310)
+REL_COMPS = ("CLLMS", "XLLMS", "XLLMX", "XLLMY", "XLLMZ", "CSSMS", "CSSMX",
+             "CSSMY", "CSSMZ", "XSSMS", "XSSMX", "XSSMY", "XSSMZ", "XLSMS",
+             "XLSMX", "XLSMY", "XLSMZ")
+
+
+def _stats(st):
+    return dict(total=st.quartets_total, screened=st.quartets_screened,
+                fp32=st.quartets_fp32, fp64=st.quartets_fp64,
+                device_ms=st.device_ms)
+
+
+class GTODirectRelERIContraction:
+    """``GTODirectRelERIContraction<dcomplex,double>`` on the GPU
+    (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94)."""
+
+    def __init__(self, tpi: DirectTPI):
+        self.tpi = tpi
+        self.last_stats: Optional[dict] = None
+
+    def twoBodyContract(self, matList: List[TwoBodyContraction],
+                        contType: int, computeExchange: bool = True,
+                        screen: bool = True, stream=None) -> None:
+        """17 entries in REL_COMPS order (None for entries the type does not
+        use).  Every given AX is overwritten (the reference zeroes AX on
+        entry); X and AX are N x N complex (numpy, or column-major CUDA
+        complex128 tensors)."""
+        if len(matList) != _cabi.CQF_REL_NMAT:
+            raise ValueError("a 4C contraction list has 17 entries")
+        N = self.tpi.nbasis
+        present = [c for c in matList if c is not None]
+        dev = bool(present) and _is_torch(present[0].X)
+        n = _cabi.CQF_REL_NMAT
+        xs = (C.c_void_p * n)()
+        axs = (C.c_void_p * n)()
+        keep, writeback = [], []
+        for i, c in enumerate(matList):
+            if c is None:
+                continue
+            if dev:
+                for t in (c.X, c.AX):
+                    if tuple(t.shape) != (N, N) or not t.is_cuda or t.stride() != (1, N):
+                        raise ValueError("device matrices must be (N, N) column-major")
+                xs[i] = c.X.data_ptr()
+                axs[i] = c.AX.data_ptr()
+            else:
+                X = np.asfortranarray(c.X, dtype=np.complex128)
+                if X.shape != (N, N):
+                    raise ValueError("matrix shape must be (N, N)")
+                AX = np.zeros((N, N), dtype=np.complex128, order="F")
+                keep += [X, AX]
+                writeback.append((c, AX))
+                xs[i] = X.ctypes.data
+                axs[i] = AX.ctypes.data
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.is_complex = 1
+        opts.screen = 1 if screen else 0
+        opts.device_pointers = 1 if dev else 0
+        opts.stream = _stream_arg(stream)
+        st = _cabi.CqfStats()
+        _cabi.check(_cabi.lib().cqf_rel_two_body_contract(
+            self.tpi.handle, xs, axs, int(contType), 1 if computeExchange else 0,
+            C.byref(opts), C.byref(st)))
+        for c, AX in writeback:
+            if isinstance(c.AX, np.ndarray) and c.AX.shape == (N, N):
+                c.AX[...] = AX
+            else:
+                c.AX = AX
+        self.last_stats = _stats(st)

@@ -455,6 +455,9 @@ void free_basis(cqf_basis* B) {
   cudaFree(B->d_ws);
   cudaFree(B->d_counters);
   cudaFree(B->d_flags);
+  cudaFree(B->d_qLL);
+  cudaFree(B->d_qSS);
+  cudaFree(B->d_relws);
   if (B->h_flags) cudaFreeHost(B->h_flags);
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
@@ -744,6 +747,26 @@ cqf_status cqf_basis_one_electron(cqf_basis* B, double* S, double* T) {
 }  // extern "C"
 
 namespace cqf {
+
+void launch_block_norms(const cqf_basis* B, const double* X, int cplx, double* out,
+                        cudaStream_t st) {
+  const size_t ns2 = (size_t)B->nshell * B->nshell;
+  block_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(X, cplx, B->nbasis, B->d_shells, B->nshell,
+                                                      out);
+}
+
+void launch_max_norms(const double* nm, int nMat, size_t ns2, double* out,
+                      unsigned long long* gmax, cudaStream_t st) {
+  max_norms_kernel<<<grid1(ns2, 256), 256, 0, st>>>(nm, nMat, ns2, out, gmax);
+}
+
+void launch_to_cart(const cqf_basis* B, const double* X, int cplx, double* Xc, cudaStream_t st) {
+  const size_t nc2 = (size_t)B->ncart * B->ncart;
+  to_cart_kernel<<<grid1(nc2, 256), 256, 0, st>>>(X, cplx, B->nbasis, B->ncart, B->d_shells,
+                                                  B->d_cart2shell, B->d_sph, B->d_sphOff, Xc);
+}
+
+cqf_status basis_workspace(cqf_basis* B, size_t bytes) { return ensure_ws(B, bytes); }
 
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   const int cw = opts.is_complex ? 2 : 1;

@@ -64,6 +64,18 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
                          const int* d_flags_pre);
 
+// Launch helpers shared with the four-component path (cqf_api.cu).
+// Shell-block infinity norms of one N x N matrix (complex: |z|).
+void launch_block_norms(const cqf_basis* B, const double* X, int cplx, double* out,
+                        cudaStream_t st);
+// out = elementwise max over nMat norm tables; *gmax = max of out (bits).
+void launch_max_norms(const double* nm, int nMat, size_t ns2, double* out,
+                      unsigned long long* gmax, cudaStream_t st);
+// Xc = T X T^T (spherical -> Cartesian AO), real or complex interleaved.
+void launch_to_cart(const cqf_basis* B, const double* X, int cplx, double* Xc, cudaStream_t st);
+// Grows the basis' contraction workspace (B->d_ws) to at least `bytes`.
+cqf_status basis_workspace(cqf_basis* B, size_t bytes);
+
 }  // namespace cqf
 
 struct cqf_basis {
@@ -96,5 +108,13 @@ struct cqf_basis {
   int* d_flags = nullptr;                // MAXMAT per-matrix flags
   int* h_flags = nullptr;                // pinned staging of the flags
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // four-component path: Schwarz tables (computed on first use, nshell^2
+  // each, zero for pairs outside the significant-pair list) and workspace
+  double* d_qLL = nullptr;
+  double* d_qSS = nullptr;
+  bool rel_qLL = false, rel_qSS = false;
+  std::vector<double> h_qLL, h_qSS;
+  void* d_relws = nullptr;
+  size_t relws_bytes = 0;
   std::mutex mu;
 };

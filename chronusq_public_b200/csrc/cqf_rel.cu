@@ -1,0 +1,1198 @@
+// Four-component Dirac-Coulomb direct contraction on the device.
+//
+// Replaces GTODirectRelERIContraction::twoBodyContract -> directScaffoldLibcint
+// (include/particleintegrals/contract/direct4C_libcint.hpp:138-2832) and the
+// FourCompFock::formGDDirect assembly (include/fockbuilder/fourcompfock/
+// impl.hpp:3752-4636).
+//
+// Small-component functions are the large-component ones differentiated
+// (restricted kinetic balance), so the LLSS and SSSS terms need derivative
+// ERIs.  A differentiated pair (m, n) acts on the electron's spin as the
+// operator P_mn = dm.dn + i sigma.(dm x dn): four real operator components
+// (dot, cross x, y, z) per integral.  The reference takes the 9 / 81 raw
+// derivative components from libcint and writes each spin product out; here
+// the components come from McMurchie-Davidson over the pair's Hermite tables
+// raised by one on each centre,
+//     d/dx [x^i e^{-a x^2}] = i x^{i-1} e^{-a x^2} - 2a x^{i+1} e^{-a x^2},
+// and the digestion is the Pauli algebra of P:
+//   Coulomb   J^a(12) += P^a(12|34) rho(43), rho = (Re D^S, -Im D^x, -Im D^y, -Im D^z)
+//   LS exchange  K(3,2) -= D(4,1) P_12                          (LLSS)
+//   SS exchange  K(1,4) -= P_12 D(2,3) P_34                     (SSSS)
+// with the reference's quartet sets, screens and degeneracy factors.
+//
+// Layout: densities and accumulators live in the Cartesian AO basis (exact
+// transforms before and after, as on the 1C path); Coulomb accumulators are
+// real, exchange accumulators complex.  One thread per unique shell quartet
+// loops over the ket's Cartesian components; for each it sums the primitive
+// quartets into the operator components of every bra component pair and
+// digests them with FP64 atomics.  Hermitian outputs are completed from the
+// accumulated half at the back transform (the reference's "upper =
+// conj(lower)" after Hermitian digestion).
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "cqf_eri.cuh"
+#include "cqf_internal.hpp"
+
+namespace cqf {
+namespace {
+
+#define CQF_RCUDA(call)                                                                    \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(e_ == cudaErrorMemoryAllocation ? CQF_ENOMEM : CQF_ECUDA,                \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+  } while (0)
+
+#define CQF_RTRY(expr)           \
+  do {                           \
+    cqf_status s_ = (expr);      \
+    if (s_ != CQF_OK) return s_; \
+  } while (0)
+
+// speed of light in atomic units (include/physcon.hpp:40)
+constexpr double SPEED_OF_LIGHT = 137.035999074;
+
+unsigned rgrid(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// max of the six shell-block norms of a quartet in the reference's roles
+// (direct4C_libcint.hpp:602-620, :940-948)
+__device__ __forceinline__ double sh_max(const double* __restrict__ n, int s1, int s2, int s3,
+                                         int s4, int ns) {
+  auto B = [&](int a, int b) { return __ldg(n + a + (size_t)b * ns); };
+  return fmax(fmax(fmax(B(s1, s2), B(s1, s3)), fmax(B(s2, s3), B(s1, s4))),
+              fmax(B(s2, s4), B(s3, s4)));
+}
+
+// ------------------------------------------------------------ spin algebra
+struct __align__(16) Q4 {  // s + v . sigma, complex components
+  double2 s, x, y, z;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 ctimes_i(double2 a) { return make_double2(-a.y, a.x); }
+
+// (p.s + p.v sigma)(q.s + q.v sigma) = p.s q.s + p.v.q.v
+//   + (p.s q.v + q.s p.v + i p.v x q.v) . sigma
+__device__ __forceinline__ Q4 qmul(const Q4& p, const Q4& q) {
+  Q4 r;
+  r.s = cadd(cadd(cmul(p.s, q.s), cmul(p.x, q.x)), cadd(cmul(p.y, q.y), cmul(p.z, q.z)));
+  r.x = cadd(cadd(cmul(p.s, q.x), cmul(q.s, p.x)),
+             ctimes_i(csub(cmul(p.y, q.z), cmul(p.z, q.y))));
+  r.y = cadd(cadd(cmul(p.s, q.y), cmul(q.s, p.y)),
+             ctimes_i(csub(cmul(p.z, q.x), cmul(p.x, q.z))));
+  r.z = cadd(cadd(cmul(p.s, q.z), cmul(q.s, p.z)),
+             ctimes_i(csub(cmul(p.x, q.y), cmul(p.y, q.x))));
+  return r;
+}
+
+__device__ __forceinline__ double2 ldz(const double* X, size_t e) {
+  return __ldg(reinterpret_cast<const double2*>(X) + e);
+}
+__device__ __forceinline__ void addz(double* A, size_t e, double2 v, double w) {
+  atomicAdd(A + 2 * e, v.x * w);
+  atomicAdd(A + 2 * e + 1, v.y * w);
+}
+
+// ------------------------------------------------------- derivative ERIs
+// One Cartesian axis of a primitive pair as a Hermite expansion, with d/dx
+// on the first centre (type bit 0) and / or the second (bit 1).  E is the
+// pair's table raised by one on both centres when a derivative is taken:
+// E[(i * (l2r + 1) + j) * Lr + t].  Returns the length (t = 0 .. n-1).
+__device__ __forceinline__ int axis_factor(const double* E, int l2r, int Lr, int i, int j,
+                                           int type, double a2, double b2, double* f) {
+  const int dA = type & 1, dB = (type >> 1) & 1;
+  const int n = i + j + dA + dB + 1;
+  auto e = [&](int ii, int jj, int t) -> double {
+    return (ii < 0 || jj < 0 || t > ii + jj) ? 0.0 : E[(ii * (l2r + 1) + jj) * Lr + t];
+  };
+#pragma unroll 1
+  for (int t = 0; t < n; t++) {
+    double v;
+    if (type == 0) v = e(i, j, t);
+    else if (type == 1) v = i * e(i - 1, j, t) - a2 * e(i + 1, j, t);
+    else if (type == 2) v = j * e(i, j - 1, t) - b2 * e(i, j + 1, t);
+    else
+      v = (i * j) * e(i - 1, j - 1, t) - b2 * i * e(i - 1, j + 1, t) -
+          a2 * j * e(i + 1, j - 1, t) + a2 * b2 * e(i + 1, j + 1, t);
+    f[t] = v;
+  }
+  return n;
+}
+
+// G[tuv] += s * sum f_x[tau] f_y[nu] f_z[phi] R_{t+tau,u+nu,v+phi} for
+// t+u+v <= Lb; the ket factors carry the (-1)^(tau+nu+phi) sign already.
+__device__ __forceinline__ void ket_add(double* G, double s, const double* fx, int nx,
+                                        const double* fy, int ny, const double* fz, int nz,
+                                        int Lb, const double* Rv) {
+#pragma unroll 1
+  for (int t = 0; t <= Lb; t++)
+#pragma unroll 1
+    for (int u = 0; u <= Lb - t; u++)
+#pragma unroll 1
+      for (int v = 0; v <= Lb - t - u; v++) {
+        double acc = 0.0;
+#pragma unroll 1
+        for (int a = 0; a < nx; a++) {
+          const double fa = fx[a];
+          if (fa == 0.0) continue;
+#pragma unroll 1
+          for (int b = 0; b < ny; b++) {
+            const double fab = fa * fy[b];
+            if (fab == 0.0) continue;
+#pragma unroll 1
+            for (int c = 0; c < nz; c++) acc += fab * fz[c] * Rv[hidx(t + a, u + b, v + c)];
+          }
+        }
+        G[hidx(t, u, v)] += s * acc;
+      }
+}
+
+__device__ __forceinline__ double bra_dot(const double* gx, int nx, const double* gy, int ny,
+                                          const double* gz, int nz, const double* G) {
+  double s = 0.0;
+#pragma unroll 1
+  for (int t = 0; t < nx; t++) {
+    if (gx[t] == 0.0) continue;
+#pragma unroll 1
+    for (int u = 0; u < ny; u++) {
+      const double gxy = gx[t] * gy[u];
+      if (gxy == 0.0) continue;
+#pragma unroll 1
+      for (int v = 0; v < nz; v++) s += gxy * gz[v] * G[hidx(t, u, v)];
+    }
+  }
+  return s;
+}
+
+// operator component of the derivative pair (mu on the first centre, nu on
+// the second): dot (0) or cross x / y / z (1..3), with its sign
+__device__ __forceinline__ void op_of(int mu, int nu, int& op, double& sg) {
+  if (mu == nu) {
+    op = 0;
+    sg = 1.0;
+  } else {
+    op = 3 - mu - nu + 1;
+    sg = (nu == (mu + 1) % 3) ? 1.0 : -1.0;
+  }
+}
+
+// exponents of primitive pair ip of pair P (prim_pairs_kernel order: first
+// shell's primitive outer)
+__device__ __forceinline__ void pair_exps(const ShellDev& SA, const ShellDev& SB,
+                                          const double* __restrict__ prim, int ip, double& ea,
+                                          double& eb) {
+  ea = __ldg(prim + SA.prim_off + ip / SB.nprim);
+  eb = __ldg(prim + SB.prim_off + ip % SB.nprim);
+}
+
+constexpr double PI52X2 = 34.986836655249725693;  // 2 pi^(5/2)
+
+struct RelLaunch {
+  const PairDev* pairs;
+  const PrimPairDev* pp;
+  const ShellDev* shells;
+  const double* prim;
+  const double* boys;
+  int braBeg, nBra, ketBeg, nKet, same;
+  int screen;
+  double thresh;
+  const double* norms;  // max shell-block norms of the screening matrices
+  const double* qLL;
+  const double* qSS;
+  int nShell, ncart, exchange;
+  const double* Xll;     // Cartesian complex X[CLLMS]
+  const double* Xss[4];  // Cartesian complex X[CSSM*]
+  const double* Xk[4];   // exchange densities: X[XLSM*] (LLSS) / X[XSSM*] (SSSS)
+  double* Jll;           // real
+  double* Jss[4];        // real
+  double* K[4];          // complex
+  unsigned long long* counters;
+};
+
+constexpr int REL_THREADS = 64;
+
+// TYPE 1: LLSS (bra = SS pair, differentiated; ket = LL pair), all
+// (bra, ket) combinations (direct4C_libcint.hpp:907-929).
+// TYPE 2: SSSS, unique quartets of pairs (:2018-2047).
+template <int LM, int TYPE>
+__global__ void __launch_bounds__(REL_THREADS)
+    rel_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+  const int ib = blockIdx.x;
+  const int jk = blockIdx.y * REL_THREADS + threadIdx.x;
+  const int ns = a.nShell;
+  const bool visited = jk < a.nKet && !(TYPE == 2 && a.same && jk > ib);
+  const PairDev P = a.pairs[a.braBeg + ib];
+  PairDev Q = P;
+  bool work = false;
+  if (visited) {
+    Q = a.pairs[a.ketBeg + jk];
+    int s1, s2, s3, s4;
+    double q12, q34;
+    if (TYPE == 1) {
+      s1 = P.s1; s2 = P.s2; s3 = Q.s1; s4 = Q.s2;
+      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+      q34 = __ldg(a.qLL + s3 + (size_t)s4 * ns);
+    } else {
+      const bool pRef = P.lex >= Q.lex;
+      const PairDev& R12 = pRef ? P : Q;
+      const PairDev& R34 = pRef ? Q : P;
+      s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
+      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+      q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
+    }
+    // shMax * Q12 * Q34 < thresh (:947-948, :2059-2061)
+    work = !a.screen || sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34 >= a.thresh;
+  }
+  {
+    const unsigned mask = __activemask();
+    const unsigned bv = __ballot_sync(mask, visited), bw = __ballot_sync(mask, work);
+    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
+      if (bv) atomicAdd(a.counters + 0, (unsigned long long)__popc(bv));
+      if (bv & ~bw) atomicAdd(a.counters + 1, (unsigned long long)__popc(bv & ~bw));
+      if (bw) atomicAdd(a.counters + 3, (unsigned long long)__popc(bw));
+    }
+  }
+  if (!work) return;
+
+  constexpr int NB = (TYPE == 2) ? 4 : 1;  // ket operator components
+  constexpr int NC = 4 * NB;               // operator components per integral
+  constexpr int NCL = ncart(LM);
+  constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
+  constexpr int HB = nherm(2 * LM + 2);
+  constexpr int HL = nherm(4 * LM + 2 + 2 * (TYPE == 2));
+  constexpr int FL = 2 * LM + 3;
+  const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int dK = (TYPE == 2) ? 1 : 0;
+  const int Lb = la + lb + 2, Lk = lc + ld + 2 * dK, L = Lb + Lk;
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+  const bool dAB = P.shA == P.shB, dCD = Q.shA == Q.shB, samePQ = P.lex == Q.lex;
+  const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
+  // the back transform adds the transpose (Hermitian completion): a
+  // contribution on a pair's own diagonal block is counted twice there
+  const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
+  const size_t nc = a.ncart;
+  auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
+
+  double Ea[3][E1], Ec[3][E1];
+  double G[NB][HB];
+  double Rv[HL];
+  double F[4 * LM + 5];
+  double acc[NCL * NCL * NC];
+  double fa[3][4][FL], fc[3][4][FL];
+  int nfa[3][4], nfc[3][4];
+
+#pragma unroll 1
+  for (int c = 0; c < ncc; c++)
+#pragma unroll 1
+    for (int d = 0; d < nd; d++) {
+      const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
+      const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+#pragma unroll 1
+      for (int k = 0; k < na * nb * NC; k++) acc[k] = 0.0;
+#pragma unroll 1
+      for (int ip = 0; ip < P.npp; ip++) {
+        const PrimPairDev& A = a.pp[P.pp_off + ip];
+        double ea, eb;
+        pair_exps(SA, SB, a.prim, ip, ea, eb);
+        const double p = A.p;
+#pragma unroll 1
+        for (int x = 0; x < 3; x++) hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
+#pragma unroll 1
+        for (int b = 0; b < NB; b++)
+#pragma unroll 1
+          for (int h = 0; h < nherm(Lb); h++) G[b][h] = 0.0;
+#pragma unroll 1
+        for (int iq = 0; iq < Q.npp; iq++) {
+          const PrimPairDev& B = a.pp[Q.pp_off + iq];
+          double ec, ed;
+          pair_exps(SC, SD, a.prim, iq, ec, ed);
+          const double q = B.p;
+#pragma unroll 1
+          for (int x = 0; x < 3; x++)
+            hermite_E_rt<double, LM + 1>(lc + dK, ld + dK, B.o2p, B.PA[x], B.PB[x], Ec[x]);
+          const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
+          const double pq = p + q, alpha = p * q / pq;
+          const double Targ = alpha * (X * X + Y * Y + Z * Z);
+          const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+          boys_rt<double>(L, Targ, F, a.boys);
+          hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
+          const int ntk = (TYPE == 2) ? 4 : 1;
+#pragma unroll 1
+          for (int x = 0; x < 3; x++)
+#pragma unroll 1
+            for (int ty = 0; ty < ntk; ty++) {
+              nfc[x][ty] = axis_factor(Ec[x], ld + dK, lc + ld + 2 * dK + 1, ci[x], di[x], ty,
+                                       2.0 * ec, 2.0 * ed, fc[x][ty]);
+#pragma unroll 1
+              for (int t = 1; t < nfc[x][ty]; t += 2) fc[x][ty][t] = -fc[x][ty][t];
+            }
+          if (TYPE == 1) {
+            ket_add(G[0], pref, fc[0][0], nfc[0][0], fc[1][0], nfc[1][0], fc[2][0], nfc[2][0],
+                    Lb, Rv);
+          } else {
+#pragma unroll 1
+            for (int kk = 0; kk < 3; kk++)
+#pragma unroll 1
+              for (int ll = 0; ll < 3; ll++) {
+                int op;
+                double sg;
+                op_of(kk, ll, op, sg);
+                const int tx = (kk == 0) | ((ll == 0) << 1), ty = (kk == 1) | ((ll == 1) << 1),
+                          tz = (kk == 2) | ((ll == 2) << 1);
+                ket_add(G[op < NB ? op : 0], sg * pref, fc[0][tx], nfc[0][tx], fc[1][ty],
+                        nfc[1][ty], fc[2][tz], nfc[2][tz], Lb, Rv);
+              }
+          }
+        }
+        // bra: the 9 derivative pairs of every component pair (a, b)
+#pragma unroll 1
+        for (int ai = 0; ai < na; ai++)
+#pragma unroll 1
+          for (int bi = 0; bi < nb; bi++) {
+            const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+            const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+#pragma unroll 1
+            for (int x = 0; x < 3; x++)
+#pragma unroll 1
+              for (int ty = 0; ty < 4; ty++)
+                nfa[x][ty] = axis_factor(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty, 2.0 * ea,
+                                         2.0 * eb, fa[x][ty]);
+            double* m = acc + (ai * nb + bi) * NC;
+#pragma unroll 1
+            for (int mu = 0; mu < 3; mu++)
+#pragma unroll 1
+              for (int nu = 0; nu < 3; nu++) {
+                int op;
+                double sg;
+                op_of(mu, nu, op, sg);
+                const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
+                          tz = (mu == 2) | ((nu == 2) << 1);
+#pragma unroll 1
+                for (int b = 0; b < NB; b++)
+                  m[op * NB + b] += sg * bra_dot(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty],
+                                                 fa[2][tz], nfa[2][tz], G[b]);
+              }
+          }
+      }
+
+      // ---- digestion of ket component pair (c, d)
+      const int gC = Q.cA + c, gD = Q.cB + d;
+      if (TYPE == 1) {
+        const double rhoLL = __ldg(a.Xll + 2 * ix(gD, gC));
+        double jll = 0.0;
+#pragma unroll 1
+        for (int ai = 0; ai < na; ai++)
+#pragma unroll 1
+          for (int bi = 0; bi < nb; bi++) {
+            const int gA = P.cA + ai, gB = P.cB + bi;
+            const double* m = acc + (ai * nb + bi) * NC;
+            // Coulomb SS(1,2) from the LL density (:1145-1190)
+            const double wj = w12 * s34d * rhoLL;
+            if (wj != 0.0)
+#pragma unroll
+              for (int op = 0; op < 4; op++) atomicAdd(a.Jss[op] + ix(gA, gB), wj * m[op]);
+            // Coulomb LL(3,4) from the SS density
+            const size_t eBA = ix(gB, gA);
+            jll += m[0] * __ldg(a.Xss[0] + 2 * eBA) - m[1] * __ldg(a.Xss[1] + 2 * eBA + 1) -
+                   m[2] * __ldg(a.Xss[2] + 2 * eBA + 1) - m[3] * __ldg(a.Xss[3] + 2 * eBA + 1);
+            if (!a.exchange) continue;
+            // exchange LS: K(t1, t2) -= D(d1, d2) P (:1200-1299)
+            auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
+              const size_t e = ix(d1, d2);
+              Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+              Q4 C{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
+                   make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
+              const Q4 r = qmul(dq, C);
+              const size_t t = ix(t1, t2);
+              addz(a.K[0], t, r.s, -1.0);
+              addz(a.K[1], t, r.x, -1.0);
+              addz(a.K[2], t, r.y, -1.0);
+              addz(a.K[3], t, r.z, -1.0);
+            };
+            ls(gC, gB, gD, gA, 1.0);
+            if (!dAB) ls(gC, gA, gD, gB, -1.0);
+            if (!dCD) {
+              ls(gD, gB, gC, gA, 1.0);
+              if (!dAB) ls(gD, gA, gC, gB, -1.0);
+            }
+          }
+        if (jll != 0.0) atomicAdd(a.Jll + ix(gC, gD), w34 * s12d * jll);
+      } else {
+        const size_t eDC = ix(gD, gC);
+        const double rvDC[4] = {__ldg(a.Xss[0] + 2 * eDC), -__ldg(a.Xss[1] + 2 * eDC + 1),
+                                -__ldg(a.Xss[2] + 2 * eDC + 1), -__ldg(a.Xss[3] + 2 * eDC + 1)};
+        double jcd[4] = {0.0, 0.0, 0.0, 0.0};
+        const double wx = samePQ ? 0.5 : 1.0;
+#pragma unroll 1
+        for (int ai = 0; ai < na; ai++)
+#pragma unroll 1
+          for (int bi = 0; bi < nb; bi++) {
+            const int gA = P.cA + ai, gB = P.cB + bi;
+            const double* m = acc + (ai * nb + bi) * NC;  // m[a * 4 + b]
+            // Coulomb SS(1,2) from D(4,3), and SS(3,4) from D(2,1) when the
+            // bra and ket pairs differ (:2342-2380)
+#pragma unroll
+            for (int op = 0; op < 4; op++) {
+              const double v = m[op * 4 + 0] * rvDC[0] + m[op * 4 + 1] * rvDC[1] +
+                               m[op * 4 + 2] * rvDC[2] + m[op * 4 + 3] * rvDC[3];
+              if (v != 0.0) atomicAdd(a.Jss[op] + ix(gA, gB), w12 * s34d * v);
+            }
+            if (!samePQ) {
+              const size_t eBA = ix(gB, gA);
+              const double rvBA[4] = {__ldg(a.Xss[0] + 2 * eBA), -__ldg(a.Xss[1] + 2 * eBA + 1),
+                                      -__ldg(a.Xss[2] + 2 * eBA + 1),
+                                      -__ldg(a.Xss[3] + 2 * eBA + 1)};
+#pragma unroll
+              for (int b = 0; b < 4; b++)
+                jcd[b] += m[0 * 4 + b] * rvBA[0] + m[1 * 4 + b] * rvBA[1] +
+                          m[2 * 4 + b] * rvBA[2] + m[3 * 4 + b] * rvBA[3];
+            }
+            if (!a.exchange) continue;
+            // exchange SS: K(t1, t2) -= P_12 D(d1, d2) P_34 with the bra / ket
+            // orientation signs f1, f2 (:2381-2445); the Hermitian-conjugate
+            // images come from the completion in the back transform
+            auto ex = [&](int t1, int t2, int d1, int d2, double f1, double f2) {
+              const size_t e = ix(d1, d2);
+              const Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+              Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+#pragma unroll 1
+              for (int b = 0; b < 4; b++) {
+                // left operator sum_a c_ab sigma_a, c_ab = m_ab (i f1)^[a>0] (i f2)^[b>0]
+                double2 cs = make_double2(m[0 * 4 + b], 0.0);
+                double2 cx = make_double2(0.0, f1 * m[1 * 4 + b]);
+                double2 cy = make_double2(0.0, f1 * m[2 * 4 + b]);
+                double2 cz = make_double2(0.0, f1 * m[3 * 4 + b]);
+                if (b > 0) {
+                  cs = make_double2(-f2 * cs.y, f2 * cs.x);
+                  cx = make_double2(-f2 * cx.y, f2 * cx.x);
+                  cy = make_double2(-f2 * cy.y, f2 * cy.x);
+                  cz = make_double2(-f2 * cz.y, f2 * cz.x);
+                }
+                const Q4 Lq{cs, cx, cy, cz};
+                Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+                      make_double2(0, 0)};
+                if (b == 0) sb.s = make_double2(1, 0);
+                else if (b == 1) sb.x = make_double2(1, 0);
+                else if (b == 2) sb.y = make_double2(1, 0);
+                else sb.z = make_double2(1, 0);
+                const Q4 t = qmul(qmul(Lq, dq), sb);
+                r.s = cadd(r.s, t.s);
+                r.x = cadd(r.x, t.x);
+                r.y = cadd(r.y, t.y);
+                r.z = cadd(r.z, t.z);
+              }
+              const size_t t = ix(t1, t2);
+              addz(a.K[0], t, r.s, -wx);
+              addz(a.K[1], t, r.x, -wx);
+              addz(a.K[2], t, r.y, -wx);
+              addz(a.K[3], t, r.z, -wx);
+            };
+            ex(gA, gD, gB, gC, 1.0, 1.0);
+            if (!dCD) ex(gA, gC, gB, gD, 1.0, -1.0);
+            if (!dAB) {
+              ex(gB, gD, gA, gC, -1.0, 1.0);
+              if (!dCD) ex(gB, gC, gA, gD, -1.0, -1.0);
+            }
+          }
+        if (!samePQ)
+#pragma unroll
+          for (int b = 0; b < 4; b++)
+            if (jcd[b] != 0.0) atomicAdd(a.Jss[b] + ix(gC, gD), w34 * s12d * jcd[b]);
+      }
+    }
+}
+
+template <int TYPE>
+void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
+  if (a.nBra == 0 || a.nKet == 0) return;
+  dim3 grid(a.nBra, (a.nKet + REL_THREADS - 1) / REL_THREADS);
+  const int lm = std::max(std::max(la, lb), std::max(lc, ld));
+  if (lm <= 1) rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
+  else if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
+  else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
+}
+
+// ------------------------------------------------------------ 4C Schwarz
+// Q^LL(a,b) = sqrt(max |(ab|ab)|) and Q^SS(a,b) = C2 sqrt(max over the 81
+// components of |(dA dB ab|dA dB ab)|), both over every element of the
+// spherical quartet block (direct4C_libcint.hpp:341-481).  One block per
+// pair: each component's Cartesian quartet block is built in shared memory
+// one ket column per thread, transformed to the spherical basis index by
+// index, and reduced.
+
+// Cartesian column out[(a*nb + b) * stride] = (d ab | d cd) of the ket
+// component pair (c, d) with derivative directions dir[0..3] (-1: none).
+template <int LM>
+__device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const int* dir,
+                             const PairDev& P, const PairDev& Q, const PrimPairDev* pp,
+                             const ShellDev* shells, const double* prim, const double* boys,
+                             double* out, int stride) {
+  constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
+  constexpr int HB = nherm(2 * LM + 2);
+  constexpr int HL = nherm(4 * LM + 4);
+  constexpr int FL = 2 * LM + 3;
+  const int na = ncart(la), nb = ncart(lb);
+  const int rb = (dir[0] >= 0 || dir[1] >= 0) ? 1 : 0, rk = (dir[2] >= 0 || dir[3] >= 0) ? 1 : 0;
+  const int Lb = la + lb + (dir[0] >= 0) + (dir[1] >= 0);
+  const int Lk = lc + ld + (dir[2] >= 0) + (dir[3] >= 0);
+  const int L = Lb + Lk;
+  const ShellDev SA = shells[P.shA], SB = shells[P.shB], SC = shells[Q.shA], SD = shells[Q.shB];
+  const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
+  const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+  double Ea[3][E1], Ec[3][E1], G[HB], Rv[HL], F[4 * LM + 5], f[3][FL], g[3][FL];
+  int nf[3], ng[3];
+  for (int k = 0; k < na * nb; k++) out[k * stride] = 0.0;
+  for (int ip = 0; ip < P.npp; ip++) {
+    const PrimPairDev& A = pp[P.pp_off + ip];
+    double ea, eb;
+    pair_exps(SA, SB, prim, ip, ea, eb);
+    for (int x = 0; x < 3; x++)
+      hermite_E_rt<double, LM + 1>(la + rb, lb + rb, A.o2p, A.PA[x], A.PB[x], Ea[x]);
+    for (int h = 0; h < nherm(Lb); h++) G[h] = 0.0;
+    for (int iq = 0; iq < Q.npp; iq++) {
+      const PrimPairDev& B = pp[Q.pp_off + iq];
+      double ec, ed;
+      pair_exps(SC, SD, prim, iq, ec, ed);
+      for (int x = 0; x < 3; x++)
+        hermite_E_rt<double, LM + 1>(lc + rk, ld + rk, B.o2p, B.PA[x], B.PB[x], Ec[x]);
+      const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
+      const double pq = A.p + B.p, alpha = A.p * B.p / pq;
+      const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+      boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), F, boys);
+      hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
+      for (int x = 0; x < 3; x++) {
+        const int ty = (dir[2] == x) | ((dir[3] == x) << 1);
+        nf[x] = axis_factor(Ec[x], ld + rk, lc + ld + 2 * rk + 1, ci[x], di[x], ty, 2.0 * ec,
+                            2.0 * ed, f[x]);
+        for (int t = 1; t < nf[x]; t += 2) f[x][t] = -f[x][t];
+      }
+      ket_add(G, pref, f[0], nf[0], f[1], nf[1], f[2], nf[2], Lb, Rv);
+    }
+    for (int ai = 0; ai < na; ai++)
+      for (int bi = 0; bi < nb; bi++) {
+        const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+        const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+        for (int x = 0; x < 3; x++) {
+          const int ty = (dir[0] == x) | ((dir[1] == x) << 1);
+          ng[x] = axis_factor(Ea[x], lb + rb, la + lb + 2 * rb + 1, ax[x], bx[x], ty, 2.0 * ea,
+                              2.0 * eb, g[x]);
+        }
+        out[(ai * nb + bi) * stride] += bra_dot(g[0], ng[0], g[1], ng[1], g[2], ng[2], G);
+      }
+  }
+}
+
+// one index of a 4-index block (row-major, index 3 fastest) from Cartesian
+// to spherical: out[.. mu ..] = sum_c T[c][mu] in[.. c ..]
+__device__ void sph_index(const double* in, double* out, int* dims, int k, const double* T,
+                          int nsk) {
+  int od[4] = {dims[0], dims[1], dims[2], dims[3]};
+  od[k] = nsk;
+  const int tot = od[0] * od[1] * od[2] * od[3];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    int i[4], r = e;
+    for (int q = 3; q >= 0; q--) {
+      i[q] = r % od[q];
+      r /= od[q];
+    }
+    const int mu = i[k];
+    double s = 0.0;
+    for (int c = 0; c < dims[k]; c++) {
+      const double t = T[c * nsk + mu];
+      if (t == 0.0) continue;
+      i[k] = c;
+      s += t * in[((i[0] * dims[1] + i[1]) * dims[2] + i[2]) * dims[3] + i[3]];
+    }
+    out[e] = s;
+  }
+  dims[k] = nsk;
+}
+
+__device__ double block_absmax(const double* buf, int n) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) m = fmax(m, fabs(buf[e]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = (threadIdx.x < (blockDim.x + 31) / 32) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) red[0] = m;
+  }
+  __syncthreads();
+  m = red[0];
+  __syncthreads();
+  return m;
+}
+
+constexpr int SCH_THREADS = 128;
+
+template <int LM>
+__global__ void __launch_bounds__(SCH_THREADS)
+    rel_schwarz_kernel(const PairDev* __restrict__ pairs, const PrimPairDev* __restrict__ pp,
+                       const ShellDev* __restrict__ shells, const double* __restrict__ prim,
+                       const double* __restrict__ boys, const double* __restrict__ sph,
+                       const int* __restrict__ sphOff, int beg, int la, int lb, int needLL,
+                       int needSS, int nshell, double* qLL, double* qSS) {
+  extern __shared__ double sm[];
+  const PairDev P = pairs[beg + blockIdx.x];
+  const ShellDev SA = shells[P.shA], SB = shells[P.shB];
+  const int na = ncart(la), nb = ncart(lb);
+  const int n4 = na * nb * na * nb;
+  double mxLL = 0.0, mxSS = 0.0;
+  for (int comp = needLL ? -1 : 0; comp < (needSS ? 81 : 0); comp++) {
+    int dir[4] = {-1, -1, -1, -1};
+    if (comp >= 0) {
+      dir[0] = comp / 27;
+      dir[1] = (comp / 9) % 3;
+      dir[2] = (comp / 3) % 3;
+      dir[3] = comp % 3;
+    }
+    double* cur = sm;
+    double* nxt = sm + n4;
+    for (int col = threadIdx.x; col < na * nb; col += blockDim.x)
+      deriv_column<LM>(la, lb, la, lb, col / nb, col % nb, dir, P, P, pp, shells, prim, boys,
+                       cur + col, na * nb);
+    __syncthreads();
+    int dims[4] = {na, nb, na, nb};
+    const ShellDev* S4[4] = {&SA, &SB, &SA, &SB};
+    for (int k = 0; k < 4; k++) {
+      const ShellDev& S = *S4[k];
+      if (!S.pure) continue;
+      sph_index(cur, nxt, dims, k, sph + sphOff[S.l], nsph(S.l));
+      __syncthreads();
+      double* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+    const double m = block_absmax(cur, dims[0] * dims[1] * dims[2] * dims[3]);
+    if (comp < 0) mxLL = m;
+    else mxSS = fmax(mxSS, m);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const size_t e1 = P.s1 + (size_t)P.s2 * nshell, e2 = P.s2 + (size_t)P.s1 * nshell;
+    if (needLL) qLL[e1] = qLL[e2] = sqrt(mxLL);
+    if (needSS) {
+      const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
+      qSS[e1] = qSS[e2] = C2 * sqrt(mxSS);
+    }
+  }
+}
+
+cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream_t st) {
+  needLL = needLL && !B->rel_qLL;
+  needSS = needSS && !B->rel_qSS;
+  if (!needLL && !needSS) return CQF_OK;
+  const size_t ns2 = (size_t)B->nshell * B->nshell;
+  if (!B->d_qLL) {
+    CQF_RCUDA(cudaMalloc(&B->d_qLL, ns2 * sizeof(double)));
+    CQF_RCUDA(cudaMemsetAsync(B->d_qLL, 0, ns2 * sizeof(double), st));
+  }
+  if (!B->d_qSS) {
+    CQF_RCUDA(cudaMalloc(&B->d_qSS, ns2 * sizeof(double)));
+    CQF_RCUDA(cudaMemsetAsync(B->d_qSS, 0, ns2 * sizeof(double), st));
+  }
+  for (int c = 0; c < NCLS; c++) {
+    if (B->cls_cnt[c] <= 0) continue;
+    int la, lb;
+    class_ls(c, la, lb);
+    const int n4 = ncart(la) * ncart(lb) * ncart(la) * ncart(lb);
+    const size_t smem = 2 * (size_t)n4 * sizeof(double);
+    const int lm = std::max(la, 1);
+#define CQF_SCH(LMV)                                                                         \
+  if (lm == LMV) {                                                                           \
+    CQF_RCUDA(cudaFuncSetAttribute(rel_schwarz_kernel<LMV>,                                  \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    rel_schwarz_kernel<LMV><<<B->cls_cnt[c], SCH_THREADS, smem, st>>>(                       \
+        B->d_pairs, B->d_pp, B->d_shells, B->d_prim, B->d_boys64, B->d_sph, B->d_sphOff,     \
+        B->cls_beg[c], la, lb, needLL, needSS, B->nshell, B->d_qLL, B->d_qSS);               \
+  }
+    CQF_SCH(1)
+    CQF_SCH(2)
+    CQF_SCH(3)
+#undef CQF_SCH
+    CQF_RCUDA(cudaGetLastError());
+  }
+  if (needLL) {
+    B->h_qLL.resize(ns2);
+    CQF_RCUDA(cudaMemcpyAsync(B->h_qLL.data(), B->d_qLL, ns2 * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+  }
+  if (needSS) {
+    B->h_qSS.resize(ns2);
+    CQF_RCUDA(cudaMemcpyAsync(B->h_qSS.data(), B->d_qSS, ns2 * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+  }
+  CQF_RCUDA(cudaStreamSynchronize(st));
+  B->rel_qLL = B->rel_qLL || needLL;
+  B->rel_qSS = B->rel_qSS || needSS;
+  return CQF_OK;
+}
+
+// ---------------------------------------------------------- back transform
+// AX (complex N x N, assigned) from a Cartesian accumulator, B = T^T Ac T:
+//   mode 0: B (complex)             mode 1: B + B^T (real Ac)
+//   mode 2: i (B - B^T) (real Ac)   mode 3: B + B^H (complex)
+__global__ void rel_from_cart_kernel(const double* __restrict__ Ac, int mode, int N, int nc,
+                                     const ShellDev* __restrict__ sh,
+                                     const int* __restrict__ ao2s,
+                                     const double* __restrict__ sph,
+                                     const int* __restrict__ sphOff, double* AX) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)N * N) return;
+  const int i = (int)(k % N), j = (int)(k / N);
+  const bool cplx = (mode == 0 || mode == 3);
+  auto bval = [&](int r, int c, double& bre, double& bim) {
+    const ShellDev A = sh[ao2s[r]], B = sh[ao2s[c]];
+    const int mu = r - A.sph_off, nu = c - B.sph_off;
+    const double* TA = sph + sphOff[A.l];
+    const double* TB = sph + sphOff[B.l];
+    bre = 0.0;
+    bim = 0.0;
+    for (int a = 0; a < ncart(A.l); a++) {
+      const double ta = A.pure ? TA[a * nsph(A.l) + mu] : (a == mu);
+      if (ta == 0.0) continue;
+      for (int b = 0; b < ncart(B.l); b++) {
+        const double tb = B.pure ? TB[b * nsph(B.l) + nu] : (b == nu);
+        if (tb == 0.0) continue;
+        const size_t e = (size_t)(A.cart_off + a) + (size_t)(B.cart_off + b) * nc;
+        if (cplx) {
+          bre += ta * tb * Ac[2 * e];
+          bim += ta * tb * Ac[2 * e + 1];
+        } else {
+          bre += ta * tb * Ac[e];
+        }
+      }
+    }
+  };
+  double r1, i1, r2 = 0.0, i2 = 0.0;
+  bval(i, j, r1, i1);
+  if (mode != 0) bval(j, i, r2, i2);
+  double outr, outi;
+  if (mode == 0) { outr = r1; outi = i1; }
+  else if (mode == 1) { outr = r1 + r2; outi = 0.0; }
+  else if (mode == 2) { outr = 0.0; outi = r1 - r2; }
+  else { outr = r1 + r2; outi = i1 - i2; }
+  AX[2 * k] = outr;
+  AX[2 * k + 1] = outi;
+}
+
+// imaginary part set to zero (the Coulomb density of the bare term)
+__global__ void real_part_kernel(const double* __restrict__ X, size_t n, double* Y) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  Y[2 * k] = X[2 * k];
+  Y[2 * k + 1] = 0.0;
+}
+
+// ------------------------------------------------------ 4C assembly kernels
+// blk(i, j) = D(ro + i, co + j), N x N out of 2N x 2N
+__global__ void get_block_kernel(const double* __restrict__ D, int N, int ro, int co,
+                                 double* blk) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)N * N) return;
+  const int i = (int)(k % N), j = (int)(k / N);
+  const size_t e = (size_t)(ro + i) + (size_t)(co + j) * 2 * N;
+  blk[2 * k] = D[2 * e];
+  blk[2 * k + 1] = D[2 * e + 1];
+}
+
+// M(ro + i, co + j) += f * src(i, j)
+__global__ void add_block_kernel(double* M, int N, int ro, int co, const double* __restrict__ src,
+                                 double f) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)N * N) return;
+  const int i = (int)(k % N), j = (int)(k / N);
+  const size_t e = (size_t)(ro + i) + (size_t)(co + j) * 2 * N;
+  M[2 * e] += f * src[2 * k];
+  M[2 * e + 1] += f * src[2 * k + 1];
+}
+
+// SL = LS^H (impl.hpp:4560-4575), then G = twoeH - xHFX K
+__global__ void finish_gd_kernel(double* twoeH, double* K, int N, double xHFX, int exch,
+                                 double* G) {
+  const int N2 = 2 * N;
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)N2 * N2) return;
+  const int r = (int)(k % N2), c = (int)(k / N2);
+  size_t src = k;
+  bool conj = false;
+  if (r >= N && c < N) {  // SL block element (N + j, i) = conj(LS(i, N + j))
+    src = (size_t)c + (size_t)r * N2;
+    conj = true;
+  }
+  double hr = twoeH[2 * src], hi = twoeH[2 * src + 1];
+  double kr = K[2 * src], ki = K[2 * src + 1];
+  if (conj) {
+    hi = -hi;
+    ki = -ki;
+  }
+  G[2 * k] = hr - (exch ? xHFX * kr : 0.0);
+  G[2 * k + 1] = hi - (exch ? xHFX * ki : 0.0);
+}
+
+// ------------------------------------------------------------ host driver
+cqf_status ensure_relws(cqf_basis* B, size_t bytes) {
+  if (bytes <= B->relws_bytes) return CQF_OK;
+  if (B->d_relws) CQF_RCUDA(cudaFree(B->d_relws));
+  B->d_relws = nullptr;
+  B->relws_bytes = 0;
+  CQF_RCUDA(cudaMalloc(&B->d_relws, bytes));
+  B->relws_bytes = bytes;
+  return CQF_OK;
+}
+
+size_t align32(size_t n) { return (n + 31) / 32 * 32; }
+
+// One contraction type on device pointers (X, AX: 17 entries, N x N complex).
+// ws: device scratch of rel_ws_doubles() doubles.
+size_t rel_ws_doubles(const cqf_basis* B) {
+  const size_t nc2 = (size_t)B->ncart * B->ncart, ns2 = (size_t)B->nshell * B->nshell;
+  return align32(9 * 2 * nc2) + align32(13 * nc2) + align32(10 * ns2) + 64;
+}
+
+cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int type,
+                            int exch, int screen, cudaStream_t st, double* ws,
+                            unsigned long long* cnt) {
+  const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
+  const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
+  for (int m = 0; m < CQF_REL_NMAT; m++)
+    if (AX[m]) CQF_RCUDA(cudaMemsetAsync(AX[m], 0, 2 * NN * sizeof(double), st));
+
+  if (type == CQF_REL_BARE_COULOMB) {
+    // (LL|LL): the 1C engine on J[Re X] and K[X] (the same quartets, screen
+    // and digestion as the reference's BARE_COULOMB branch, :514-790)
+    if (!X[CQF_CLLMS] || !AX[CQF_CLLMS]) return fail(CQF_EINVAL, "BARE_COULOMB needs CLLMS");
+    double* reX = ws;  // N x N complex
+    real_part_kernel<<<rgrid(NN, 256), 256, 0, st>>>(X[CQF_CLLMS], NN, reX);
+    CQF_RCUDA(cudaGetLastError());
+    std::vector<cqf_contraction> list;
+    list.push_back({reX, AX[CQF_CLLMS], 1, CQF_COULOMB});
+    if (exch)
+      for (int c = 0; c < 4; c++) {
+        if (!X[CQF_XLLMS + c] || !AX[CQF_XLLMS + c])
+          return fail(CQF_EINVAL, "BARE_COULOMB exchange needs XLLM*");
+        list.push_back({X[CQF_XLLMS + c], AX[CQF_XLLMS + c], 1, CQF_EXCHANGE});
+      }
+    cqf_opts o;
+    cqf_opts_default(&o);
+    o.is_complex = 1;
+    o.device_pointers = 1;
+    o.screen = screen;
+    o.stream = st;
+    CQF_RTRY(basis_workspace(B, ws_layout(B, (int)list.size(), o).total * sizeof(double)));
+    cqf_stats s1{};
+    CQF_RTRY(contract_core(B, list.data(), (int)list.size(), o, &s1,
+                           static_cast<double*>(B->d_ws), false, nullptr));
+    cnt[0] += s1.quartets_total;
+    cnt[1] += s1.quartets_screened;
+    cnt[3] += s1.quartets_fp64;
+    return CQF_OK;
+  }
+
+  const bool llss = (type == CQF_REL_LLSS);
+  CQF_RTRY(ensure_rel_schwarz(B, llss, true, st));
+  // required entries
+  std::vector<int> need = {CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ};
+  if (llss) need.push_back(CQF_CLLMS);
+  if (exch)
+    for (int c = 0; c < 4; c++) need.push_back((llss ? CQF_XLSMS : CQF_XSSMS) + c);
+  for (int m : need)
+    if (!X[m]) return fail(CQF_EINVAL, "missing X entry for this contraction type");
+  std::vector<int> outs = {CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ};
+  if (llss) outs.push_back(CQF_CLLMS);
+  if (exch)
+    for (int c = 0; c < 4; c++) outs.push_back((llss ? CQF_XLSMS : CQF_XSSMS) + c);
+  for (int m : outs)
+    if (!AX[m]) return fail(CQF_EINVAL, "missing AX entry for this contraction type");
+
+  // workspace: 9 Cartesian complex densities | 13 real accumulators (Jll,
+  // Jss x4, K x4 complex) | norms
+  double* xc = ws;
+  double* accb = ws + align32(9 * 2 * nc2);
+  double* nrm = accb + align32(13 * nc2);
+  double* Jll = accb;
+  double* Jss[4] = {accb + nc2, accb + 2 * nc2, accb + 3 * nc2, accb + 4 * nc2};
+  double* Kc[4] = {accb + 5 * nc2, accb + 7 * nc2, accb + 9 * nc2, accb + 11 * nc2};
+  auto XC = [&](int slot) { return xc + (size_t)slot * 2 * nc2; };
+  // slots: 0 CLLMS, 1..4 CSSM*, 5..8 exchange densities
+  if (llss) launch_to_cart(B, X[CQF_CLLMS], 1, XC(0), st);
+  for (int c = 0; c < 4; c++) launch_to_cart(B, X[CQF_CSSMS + c], 1, XC(1 + c), st);
+  if (exch)
+    for (int c = 0; c < 4; c++)
+      launch_to_cart(B, X[(llss ? CQF_XLSMS : CQF_XSSMS) + c], 1, XC(5 + c), st);
+  // screening norms: max over CLLMS, CSSM*, XLSM* (LLSS) or CSSM* (SSSS)
+  std::vector<int> smats = {CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ};
+  if (llss) {
+    smats.insert(smats.begin(), CQF_CLLMS);
+    for (int c = 0; c < 4; c++)
+      if (X[CQF_XLSMS + c]) smats.push_back(CQF_XLSMS + c);
+  }
+  double* nmAll = nrm + ns2;
+  for (size_t i = 0; i < smats.size(); i++)
+    launch_block_norms(B, X[smats[i]], 1, nmAll + i * ns2, st);
+  launch_max_norms(nmAll, (int)smats.size(), ns2, nrm,
+                   reinterpret_cast<unsigned long long*>(nmAll + 9 * ns2), st);
+  CQF_RCUDA(cudaMemsetAsync(accb, 0, 13 * nc2 * sizeof(double), st));
+  unsigned long long* dcnt = B->d_counters;
+  CQF_RCUDA(cudaMemsetAsync(dcnt, 0, 4 * sizeof(unsigned long long), st));
+  CQF_RCUDA(cudaGetLastError());
+
+  RelLaunch a{};
+  a.pairs = B->d_pairs;
+  a.pp = B->d_pp;
+  a.shells = B->d_shells;
+  a.prim = B->d_prim;
+  a.boys = B->d_boys64;
+  a.screen = screen;
+  a.thresh = B->thresh;
+  a.norms = nrm;
+  a.qLL = B->d_qLL;
+  a.qSS = B->d_qSS;
+  a.nShell = ns;
+  a.ncart = nc;
+  a.exchange = exch;
+  a.Xll = XC(0);
+  for (int c = 0; c < 4; c++) {
+    a.Xss[c] = XC(1 + c);
+    a.Xk[c] = XC(5 + c);
+    a.Jss[c] = Jss[c];
+    a.K[c] = Kc[c];
+  }
+  a.Jll = Jll;
+  a.counters = dcnt;
+  for (int cb = 0; cb < NCLS; cb++)
+    for (int ck = 0; ck < NCLS; ck++) {
+      if (!llss && ck > cb) continue;
+      if (!B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
+      int la, lb, lc, ld;
+      class_ls(cb, la, lb);
+      class_ls(ck, lc, ld);
+      a.braBeg = B->cls_beg[cb];
+      a.nBra = B->cls_cnt[cb];
+      a.ketBeg = B->cls_beg[ck];
+      a.nKet = B->cls_cnt[ck];
+      a.same = (cb == ck);
+      if (llss) launch_rel<1>(a, la, lb, lc, ld, st);
+      else launch_rel<2>(a, la, lb, lc, ld, st);
+    }
+  CQF_RCUDA(cudaGetLastError());
+  auto back = [&](const double* src, int mode, double* dst) {
+    rel_from_cart_kernel<<<rgrid(NN, 256), 256, 0, st>>>(src, mode, N, nc, B->d_shells,
+                                                         B->d_ao2shell, B->d_sph, B->d_sphOff,
+                                                         dst);
+  };
+  if (llss) back(Jll, 1, AX[CQF_CLLMS]);
+  back(Jss[0], 1, AX[CQF_CSSMS]);
+  for (int c = 1; c < 4; c++) back(Jss[c], 2, AX[CQF_CSSMS + c]);
+  if (exch)
+    for (int c = 0; c < 4; c++)
+      back(Kc[c], llss ? 0 : 3, AX[(llss ? CQF_XLSMS : CQF_XSSMS) + c]);
+  CQF_RCUDA(cudaGetLastError());
+  unsigned long long h[4];
+  CQF_RCUDA(cudaMemcpyAsync(h, dcnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CQF_RCUDA(cudaStreamSynchronize(st));
+  cnt[0] += h[0];
+  cnt[1] += h[1];
+  cnt[3] += h[3];
+  return CQF_OK;
+}
+
+}  // namespace
+}  // namespace cqf
+
+using namespace cqf;
+
+extern "C" {
+
+cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* const* AX,
+                                     int type, int compute_exchange, const cqf_opts* optsIn,
+                                     cqf_stats* stats) {
+  if (!B || !X || !AX) return fail(CQF_EINVAL, "cqf_rel_two_body_contract: null argument");
+  if (type < CQF_REL_BARE_COULOMB || type > CQF_REL_SSSS)
+    return fail(CQF_EINVAL, "cqf_rel_two_body_contract: unknown contraction type");
+  cqf_opts o;
+  cqf_opts_default(&o);
+  if (optsIn) o = *optsIn;
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_RCUDA(cudaSetDevice(B->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : B->stream;
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  const size_t wsd = rel_ws_doubles(B);
+  const size_t hostd = o.device_pointers ? 0 : align32(2 * NN) * 2 * CQF_REL_NMAT;
+  CQF_RTRY(ensure_relws(B, (wsd + hostd) * sizeof(double)));
+  double* ws = static_cast<double*>(B->d_relws);
+  double* hbuf = ws + wsd;
+  const double* Xd[CQF_REL_NMAT];
+  double* AXd[CQF_REL_NMAT];
+  for (int m = 0; m < CQF_REL_NMAT; m++) {
+    if (o.device_pointers) {
+      Xd[m] = static_cast<const double*>(X[m]);
+      AXd[m] = static_cast<double*>(AX[m]);
+    } else {
+      double* xd = hbuf + (size_t)m * align32(2 * NN);
+      double* ad = hbuf + (size_t)(CQF_REL_NMAT + m) * align32(2 * NN);
+      Xd[m] = X[m] ? xd : nullptr;
+      AXd[m] = AX[m] ? ad : nullptr;
+      if (X[m])
+        CQF_RCUDA(cudaMemcpyAsync(xd, X[m], 2 * NN * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+  }
+  CQF_RCUDA(cudaEventRecord(B->ev0, st));
+  unsigned long long cnt[4] = {0, 0, 0, 0};
+  CQF_RTRY(rel_contract_dev(B, Xd, AXd, type, compute_exchange, o.screen, st, ws, cnt));
+  CQF_RCUDA(cudaEventRecord(B->ev1, st));
+  if (!o.device_pointers)
+    for (int m = 0; m < CQF_REL_NMAT; m++)
+      if (AX[m])
+        CQF_RCUDA(cudaMemcpyAsync(AX[m], AXd[m], 2 * NN * sizeof(double), cudaMemcpyDeviceToHost,
+                                  st));
+  CQF_RCUDA(cudaStreamSynchronize(st));
+  if (stats) {
+    stats->quartets_total = (long long)cnt[0];
+    stats->quartets_screened = (long long)cnt[1];
+    stats->quartets_fp32 = 0;
+    stats->quartets_fp64 = (long long)cnt[3];
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+    stats->device_ms = ms;
+  }
+  return CQF_OK;
+}
+
+void cqf_dc_opts_default(cqf_dc_opts* o) {
+  if (!o) return;
+  o->bare_coulomb = 1;
+  o->dirac_coulomb = 1;
+  o->dirac_coulomb_ssss = 1;
+  o->libcint = 1;
+  o->xHFX = 1.0;
+}
+
+cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
+                            const cqf_dc_opts* dcIn, const cqf_opts* optsIn, cqf_stats* stats) {
+  if (!B || !D || !G) return fail(CQF_EINVAL, "cqf_four_comp_gd: null argument");
+  for (int c = 0; c < 4; c++)
+    if (!D[c] || !G[c]) return fail(CQF_EINVAL, "cqf_four_comp_gd: null D or G component");
+  cqf_dc_opts dc;
+  cqf_dc_opts_default(&dc);
+  if (dcIn) dc = *dcIn;
+  cqf_opts o;
+  cqf_opts_default(&o);
+  if (optsIn) o = *optsIn;
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_RCUDA(cudaSetDevice(B->device));
+  cudaStream_t st = o.stream ? (cudaStream_t)o.stream : B->stream;
+  const int N = B->nbasis;
+  const size_t NN = (size_t)N * N, NN2 = 4 * NN;
+  const double c2 = SPEED_OF_LIGHT * SPEED_OF_LIGHT;
+  const double C2 = 1.0 / (4.0 * c2), C4 = 1.0 / (16.0 * c2 * c2);
+  const bool exch = std::fabs(dc.xHFX) >= 1e-12;
+  // workspace: rel scratch | blocks 12 x N^2 | AX 17 x N^2 | twoeH 4 x 4N^2 |
+  // K 4 x 4N^2 | D/G staging (host pointers) 8 x 4N^2, all complex
+  const size_t wsd = rel_ws_doubles(B);
+  const size_t blkd = align32(2 * NN), bigd = align32(2 * NN2);
+  const size_t total = wsd + 12 * blkd + CQF_REL_NMAT * blkd + 8 * bigd +
+                       (o.device_pointers ? 0 : 8 * bigd);
+  CQF_RTRY(ensure_relws(B, total * sizeof(double)));
+  double* ws = static_cast<double*>(B->d_relws);
+  double* blk = ws + wsd;
+  double* axb = blk + 12 * blkd;
+  double* twoeH = axb + CQF_REL_NMAT * blkd;
+  double* Kb = twoeH + 4 * bigd;
+  double* stage = Kb + 4 * bigd;
+  const double* Dd[4];
+  double* Gd[4];
+  for (int c = 0; c < 4; c++) {
+    if (o.device_pointers) {
+      Dd[c] = static_cast<const double*>(D[c]);
+      Gd[c] = static_cast<double*>(G[c]);
+    } else {
+      double* dd = stage + c * bigd;
+      Dd[c] = dd;
+      Gd[c] = stage + (4 + c) * bigd;
+      CQF_RCUDA(cudaMemcpyAsync(dd, D[c], 2 * NN2 * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+  }
+  CQF_RCUDA(cudaEventRecord(B->ev0, st));
+  // LL / SS / LS blocks of each Pauli component (impl.hpp:3847-3857)
+  auto B3 = [&](int k, int c) { return blk + (size_t)(k * 4 + c) * blkd; };
+  const int ro[3] = {0, N, 0}, co[3] = {0, N, N};
+  for (int k = 0; k < 3; k++)
+    for (int c = 0; c < 4; c++)
+      get_block_kernel<<<rgrid(NN, 256), 256, 0, st>>>(Dd[c], N, ro[k], co[k], B3(k, c));
+  CQF_RCUDA(cudaMemsetAsync(twoeH, 0, 8 * bigd * sizeof(double), st));
+  CQF_RCUDA(cudaGetLastError());
+  const double* X[CQF_REL_NMAT];
+  double* AX[CQF_REL_NMAT];
+  X[CQF_CLLMS] = B3(0, 0);
+  for (int c = 0; c < 4; c++) {
+    X[CQF_XLLMS + c] = B3(0, c);
+    X[CQF_CSSMS + c] = B3(1, c);
+    X[CQF_XSSMS + c] = B3(1, c);
+    X[CQF_XLSMS + c] = B3(2, c);
+  }
+  for (int m = 0; m < CQF_REL_NMAT; m++) AX[m] = axb + (size_t)m * blkd;
+  auto H = [&](int c) { return twoeH + (size_t)c * bigd; };
+  auto Kk = [&](int c) { return Kb + (size_t)c * bigd; };
+  auto add = [&](double* M, int r0, int c0, const double* src, double f) {
+    add_block_kernel<<<rgrid(NN, 256), 256, 0, st>>>(M, N, r0, c0, src, f);
+  };
+  unsigned long long cnt[4] = {0, 0, 0, 0};
+  if (dc.bare_coulomb) {  // impl.hpp:3895-3969
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_BARE_COULOMB, exch, o.screen, st, ws, cnt));
+    add(H(0), 0, 0, AX[CQF_CLLMS], dc.libcint ? 2.0 : 1.0);
+    if (exch)
+      for (int c = 0; c < 4; c++) add(Kk(c), 0, 0, AX[CQF_XLLMS + c], 1.0);
+  }
+  if (dc.dirac_coulomb) {  // impl.hpp:4003-4147
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_LLSS, exch, o.screen, st, ws, cnt));
+    add(H(0), 0, 0, AX[CQF_CLLMS], 2.0 * C2);
+    for (int c = 0; c < 4; c++) add(H(c), N, N, AX[CQF_CSSMS + c], 2.0 * C2);
+    if (exch)
+      for (int c = 0; c < 4; c++) add(Kk(c), 0, N, AX[CQF_XLSMS + c], -C2);
+  }
+  if (dc.dirac_coulomb_ssss) {  // impl.hpp:4149-4233
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_SSSS, exch, o.screen, st, ws, cnt));
+    for (int c = 0; c < 4; c++) add(H(c), N, N, AX[CQF_CSSMS + c], 2.0 * C4);
+    if (exch)
+      for (int c = 0; c < 4; c++) add(Kk(c), N, N, AX[CQF_XSSMS + c], -C4);
+  }
+  for (int c = 0; c < 4; c++)
+    finish_gd_kernel<<<rgrid(NN2, 256), 256, 0, st>>>(H(c), Kk(c), N, dc.xHFX, exch ? 1 : 0,
+                                                      Gd[c]);
+  CQF_RCUDA(cudaGetLastError());
+  CQF_RCUDA(cudaEventRecord(B->ev1, st));
+  if (!o.device_pointers)
+    for (int c = 0; c < 4; c++)
+      CQF_RCUDA(cudaMemcpyAsync(G[c], Gd[c], 2 * NN2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                st));
+  CQF_RCUDA(cudaStreamSynchronize(st));
+  if (stats) {
+    stats->quartets_total = (long long)cnt[0];
+    stats->quartets_screened = (long long)cnt[1];
+    stats->quartets_fp32 = 0;
+    stats->quartets_fp64 = (long long)cnt[3];
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+    stats->device_ms = ms;
+  }
+  return CQF_OK;
+}
+
+}  // extern "C"

@@ -63,3 +63,75 @@ def two_electron_energy(G, D) -> float:
     """1/4 Tr[G D] (the many-body term of singleslater/quantum.hpp:147-205
     for the scalar component)."""
     return 0.25 * float(np.sum(np.asarray(G) * np.asarray(D).T))
+
+
+class FourCompFock:
+    """``FourCompFock<dcomplex,double>::formGDDirect``
+    (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) on the GPU.
+
+    Hamiltonian switches as the reference's HamiltonianOptions (BareCoulomb,
+    DiracCoulomb, DiracCoulombSSSS, Libcint); the density is the four Pauli
+    components (scalar, MX, MY, MZ) of the 2N x 2N complex 4C one-particle
+    density (LL block first).  ``formGD`` returns the same four components of
+    G = twoeH - xHFX K.
+    """
+
+    def __init__(self, tpi: DirectTPI, BareCoulomb: bool = True,
+                 DiracCoulomb: bool = True, DiracCoulombSSSS: bool = True,
+                 Libcint: bool = True):
+        self.tpi = tpi
+        self.BareCoulomb = BareCoulomb
+        self.DiracCoulomb = DiracCoulomb
+        self.DiracCoulombSSSS = DiracCoulombSSSS
+        self.Libcint = Libcint
+        self.last_stats = None
+
+    def formGD(self, D: List, xHFX: float = 1.0, screen: bool = True,
+               stream=None) -> List:
+        import ctypes as C
+
+        from . import _cabi
+        from .contraction import _is_torch, _stats, _stream_arg
+        if len(D) != 4:
+            raise ValueError("D is the list of 4 Pauli components")
+        N2 = 2 * self.tpi.nbasis
+        dev = _is_torch(D[0])
+        dp = (C.c_void_p * 4)()
+        gp = (C.c_void_p * 4)()
+        keep = []
+        if dev:
+            import torch
+            G = [torch.zeros((N2, N2), dtype=torch.complex128, device=D[0].device).T
+                 for _ in range(4)]
+            for c in range(4):
+                if tuple(D[c].shape) != (N2, N2) or D[c].stride() != (1, N2):
+                    raise ValueError("device densities must be (2N, 2N) column-major")
+                dp[c] = D[c].data_ptr()
+                gp[c] = G[c].data_ptr()
+        else:
+            G = [np.zeros((N2, N2), dtype=np.complex128, order="F") for _ in range(4)]
+            for c in range(4):
+                Dc = np.asfortranarray(D[c], dtype=np.complex128)
+                if Dc.shape != (N2, N2):
+                    raise ValueError("density components must be (2N, 2N)")
+                keep.append(Dc)
+                dp[c] = Dc.ctypes.data
+                gp[c] = G[c].ctypes.data
+        dco = _cabi.CqfDcOpts()
+        _cabi.lib().cqf_dc_opts_default(C.byref(dco))
+        dco.bare_coulomb = int(self.BareCoulomb)
+        dco.dirac_coulomb = int(self.DiracCoulomb)
+        dco.dirac_coulomb_ssss = int(self.DiracCoulombSSSS)
+        dco.libcint = int(self.Libcint)
+        dco.xHFX = float(xHFX)
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.is_complex = 1
+        opts.screen = 1 if screen else 0
+        opts.device_pointers = 1 if dev else 0
+        opts.stream = _stream_arg(stream)
+        st = _cabi.CqfStats()
+        _cabi.check(_cabi.lib().cqf_four_comp_gd(
+            self.tpi.handle, dp, gp, C.byref(dco), C.byref(opts), C.byref(st)))
+        self.last_stats = _stats(st)
+        return G

@@ -12,6 +12,11 @@ Every workload is deterministic in its seed (numpy ``default_rng``):
                      closed shell is 2 C C^T; the configs use C C^T as
                      written).
 * ``delta_densities`` dD_k = eps (X_k + X_k^T), X_k ~ N(0,1), seeds base+k.
+* ``ag4_cluster``    Ag4 tetrahedron, edge 2.7 Angstrom, every vertex
+                     coordinate jittered by U(-0.05, 0.05) Angstrom.
+* ``spinor_density_4c`` complex Gaussian occupied 4C spinors orthonormalised
+                     in the metric diag(S, S, T/2c^2, T/2c^2), D = C C^H as
+                     the four Pauli components of the 2N x 2N matrix.
 
 S comes from the device one-electron integrals of libcqfock.so.
 """
@@ -82,6 +87,40 @@ def delta_densities(N: int, count: int, eps: float = 1e-3,
     return out
 
 
+def ag4_cluster(seed: int = 3, edge: float = 2.7, jitter: float = 0.05) -> Molecule:
+    rng = np.random.default_rng(seed)
+    a = edge / np.sqrt(2.0)  # tetrahedron from alternate cube corners
+    v = 0.5 * a * np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], float)
+    v = v + rng.uniform(-jitter, jitter, size=v.shape)
+    return Molecule.from_angstrom([("Ag", *map(float, x)) for x in v])
+
+
+SPEED_OF_LIGHT = 137.035999074  # atomic units (ChronusQ include/physcon.hpp)
+
+
+def spinor_density_4c(S: np.ndarray, T: np.ndarray, nocc: int, seed: int):
+    """Pauli components [scalar, MX, MY, MZ] (each 2N x 2N, LL block first)
+    of D = C C^H, C (4N x nocc) complex Gaussian with rows (L alpha, L beta,
+    S alpha, S beta), orthonormalised in the 4C metric."""
+    rng = np.random.default_rng(seed)
+    N = S.shape[0]
+    C = rng.normal(size=(4 * N, nocc)) + 1j * rng.normal(size=(4 * N, nocc))
+    Ms = T / (2.0 * SPEED_OF_LIGHT ** 2)
+    Z = np.zeros_like(S)
+    M = np.block([[S, Z, Z, Z], [Z, S, Z, Z], [Z, Z, Ms, Z], [Z, Z, Z, Ms]])
+    w, V = np.linalg.eigh(C.conj().T @ M @ C)
+    C = C @ (V @ np.diag(w ** -0.5) @ V.conj().T)
+    Dfull = C @ C.conj().T
+    idx_a = np.r_[0:N, 2 * N:3 * N]       # (L alpha, S alpha)
+    idx_b = np.r_[N:2 * N, 3 * N:4 * N]   # (L beta, S beta)
+    aa = Dfull[np.ix_(idx_a, idx_a)]
+    bb = Dfull[np.ix_(idx_b, idx_b)]
+    ab = Dfull[np.ix_(idx_a, idx_b)]
+    ba = Dfull[np.ix_(idx_b, idx_a)]
+    return [np.asfortranarray(aa + bb), np.asfortranarray(ab + ba),
+            np.asfortranarray(1j * (ab - ba)), np.asfortranarray(aa - bb)]
+
+
 # workload names -> (molecule factory, basis, occupied orbitals, seed)
 def config(name: str):
     if name == "h2o_ccpvdz":
@@ -90,7 +129,18 @@ def config(name: str):
         return water_cluster(16, seed=2), "def2-svp", 40, 2
     if name == "h2o8_ccpvdz":
         return water_cluster(8, seed=4), "cc-pvdz", 40, 4
+    if name == "ag4_dc":  # uncontracted basis, 188 occupied spinors
+        return ag4_cluster(3), "sapporo-dkh3-dzp-2012_no", 188, 3
     raise KeyError(name)
+
+
+def build_ag4_dc(tpi_factory, seed: int = 3):
+    """(basis, DirectTPI, D[4]) of the Ag4 four-component workload."""
+    mol, bname, nocc, _ = config("ag4_dc")
+    basis = BasisSet.build(mol, bname, uncontract=True)
+    tpi = tpi_factory(basis)
+    S, T = tpi.one_electron()
+    return basis, tpi, spinor_density_4c(S, T, nocc, seed)
 
 
 def build_config(name: str, tpi_factory):

@@ -135,8 +135,7 @@ cqf_status cqf_graph_destroy(cqf_graph* graph);
  * into the library (held by every GPU that loads the library until exit).
  * No counterpart in the reference (ChronusQ takes scratch from its memory
  * manager); it is for callers that cannot call cudaMalloc during the call,
- * e.g. while capturing a CUDA graph or inside a framework that owns all
- * device memory.  The basis must already exist (cqf_basis_create allocates).
+ * e.g. inside a framework that owns all device memory.  The basis must already exist (cqf_basis_create allocates).
  * Calls needing more scratch than the array holds return CQF_EINVAL.  The
  * first call on a device resolves the array's device address; make that
  * first call before any stream capture.  All calls share the array and it
@@ -144,6 +143,61 @@ cqf_status cqf_graph_destroy(cqf_graph* graph);
  * calls that overlap on the GPU race on it and must be serialised. */
 cqf_status cqf_two_body_contract_noalloc(cqf_basis* basis, const cqf_contraction* list, int n,
                                          const cqf_opts* opts, cqf_stats* stats);
+
+/* ---------------------------------------------------------------------
+ * Four-component Dirac-Coulomb contraction.
+ *
+ * The 17 (X, AX) entries of one relativistic contraction, in the order of
+ * DIRAC_PAULI_SPINOR_COMP (include/particleintegrals/contract/
+ * direct4C_libcint.hpp:279-310): Coulomb LL (MS), exchange LL (MS, MX, MY,
+ * MZ), Coulomb SS (4), exchange SS (4), exchange LS (4).  Every X and AX is
+ * an N x N complex (interleaved re, im) column-major matrix, N = nbasis.
+ * --------------------------------------------------------------------- */
+typedef enum {
+  CQF_CLLMS = 0, CQF_XLLMS, CQF_XLLMX, CQF_XLLMY, CQF_XLLMZ,
+  CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ,
+  CQF_XSSMS, CQF_XSSMX, CQF_XSSMY, CQF_XSSMZ,
+  CQF_XLSMS, CQF_XLSMX, CQF_XLSMY, CQF_XLSMZ,
+  CQF_REL_NMAT
+} cqf_rel_comp;
+
+/* TYPE of the 4C contraction (entry 0's contType in the reference). */
+typedef enum { CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2 } cqf_rel_type;
+
+/* GTODirectRelERIContraction::twoBodyContract (include/particleintegrals/
+ * twopints/gtodirectreleri.hpp:75-94) -> directScaffoldLibcint
+ * (direct4C_libcint.hpp:138-2832) for one contraction type: every non-NULL
+ * AX is zeroed (:313-314), then
+ *   BARE_COULOMB: AX[CLLMS] = J[Re X[CLLMS]], AX[XLLM*] = K[X[XLLM*]] (:514-790)
+ *   LLSS: AX[CLLMS], AX[CSSM*] (Coulomb, order c^-2) and, with
+ *         compute_exchange, AX[XLSM*] (:810-1441)
+ *   SSSS: AX[CSSM*] and, with compute_exchange, AX[XSSM*] (:1841-2832).
+ * Entries a type does not read or write may be NULL.  The densities must be
+ * Hermitian, as the reference requires (:144-145).  opts->is_complex and
+ * opts->precision are ignored (complex, FP64); opts->device_pointers and
+ * opts->stream apply. */
+cqf_status cqf_rel_two_body_contract(cqf_basis* basis, const void* const* X, void* const* AX,
+                                     int type, int compute_exchange, const cqf_opts* opts,
+                                     cqf_stats* stats);
+
+/* Hamiltonian switches of the 4C two-electron build (the reference's
+ * HamiltonianOptions: BareCoulomb, DiracCoulomb, DiracCoulombSSSS, Libcint)
+ * and the exchange scaling xHFX. */
+typedef struct {
+  int bare_coulomb, dirac_coulomb, dirac_coulomb_ssss, libcint;
+  double xHFX;
+} cqf_dc_opts;
+/* Defaults of the reference: all three on, libcint on, xHFX = 1. */
+void cqf_dc_opts_default(cqf_dc_opts* o);
+
+/* FourCompFock::formGDDirect (include/fockbuilder/fourcompfock/impl.hpp:
+ * 3752-4636): D[4] = Pauli components (scalar, MX, MY, MZ) of the
+ * 2N x 2N complex 4C density (column-major, LL block first); G[4] receives
+ * twoeH - xHFX K with the 2C^2 / -C^2 / 2C^4 / -C^4 weights of the LLSS and
+ * SSSS terms, twoeH_LL = 2 J (libcint) or J, and the SL blocks set to the
+ * conjugate transpose of the LS blocks. */
+cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const* G,
+                            const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 
 /* Text of the last error on this thread ("" if none). */
 const char* cqf_last_error(void);

@@ -1581,4 +1581,19 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
   return 0;
 }
 
+// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS) of
+// GTODirectRelERIContraction::twoBodyContract on the 17 N x N complex
+// (X, AX) entries in DIRAC_PAULI_SPINOR_COMP order; AX is zeroed first
+// (direct4C_libcint.hpp:313-314).
+int orc_rel_contract(void* b, int type, const void* const* Xv, void* const* AXv, double thresh,
+                     int exchange) {
+  auto* bs = static_cast<Basis*>(b);
+  const cdbl* const* X = reinterpret_cast<const cdbl* const*>(Xv);
+  cdbl* const* AX = reinterpret_cast<cdbl* const*>(AXv);
+  Schwarz4C Qs;
+  schwarz_4c(*bs, type <= 1, type >= 1, Qs);
+  direct_4c(*bs, type, X, AX, thresh, Qs, exchange != 0);
+  return 0;
+}
+
 }  // extern "C"

@@ -60,6 +60,9 @@ def lib():
                                         C.POINTER(C.c_void_p), C.c_int, C.c_int,
                                         C.c_int, C.c_double, C.c_double, C.c_int]
         L.orc_dirac_coulomb.restype = C.c_int
+        L.orc_rel_contract.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
+                                       C.POINTER(C.c_void_p), C.c_double, C.c_int]
+        L.orc_rel_contract.restype = C.c_int
         _lib = L
     return _lib
 
@@ -164,6 +167,17 @@ class OracleBasis:
         lib().orc_dirac_coulomb(self.h, dp_, gp_, int(bare), int(dc), int(ssss),
                                 xHFX, thresh, int(libcint))
         return Gs
+
+    def rel_contract(self, X, contType, exchange=True, thresh=1e-12):
+        """GTODirectRelERIContraction::twoBodyContract: X = the 17 N x N
+        complex matrices (DIRAC_PAULI_SPINOR_COMP order); returns the 17 AX."""
+        Xs = [np.asfortranarray(x, dtype=np.complex128) for x in X]
+        AX = [np.zeros_like(x, order="F") for x in Xs]
+        xp = (C.c_void_p * 17)(*[x.ctypes.data for x in Xs])
+        ap = (C.c_void_p * 17)(*[a.ctypes.data for a in AX])
+        lib().orc_rel_contract(self.h, int(contType), xp, ap, thresh,
+                               1 if exchange else 0)
+        return AX
 
     def flops(self, mats, thresh=1e-12, fp32_cut=0.0):
         Xs = [np.asfortranarray(np.abs(m), dtype=np.float64) for m in mats]
