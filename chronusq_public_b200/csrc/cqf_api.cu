@@ -445,6 +445,8 @@ void free_basis(cqf_basis* B) {
   cudaFree(B->d_prim);
   cudaFree(B->d_pairs);
   cudaFree(B->d_pp);
+  cudaFree(B->d_ketT);
+  cudaFree(B->d_tileOff);
   cudaFree(B->d_boys64);
   cudaFree(B->d_boys32);
   cudaFree(B->d_schwarz);
@@ -654,6 +656,37 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     CQF_CUDA(cudaMemcpy(B->d_pp, hpp2.data(), ppoff * sizeof(PrimPairDev), cudaMemcpyHostToDevice));
     CQF_CUDA(cudaMemcpy(B->d_pairs, B->h_pairs.data(), B->npair * sizeof(PairDev),
                         cudaMemcpyHostToDevice));
+    // the same data tile-interleaved for the class kernels' kets: per ket
+    // tile (KETT_TILE consecutive pairs of a class), field-major runs of
+    // KETT_TILE values for each primitive (zero past a pair's npp)
+    std::vector<long long> toff;
+    std::vector<double> kt;
+    for (int c = 0; c < NCLS; c++) {
+      B->cls_tile_beg[c] = (int)toff.size();
+      const int cnt = B->cls_cnt[c];
+      for (int t0 = 0; t0 < cnt; t0 += KETT_TILE) {
+        int mx = 0;
+        for (int l = 0; l < KETT_TILE && t0 + l < cnt; l++)
+          mx = std::max(mx, B->h_pairs[B->cls_beg[c] + t0 + l].npp);
+        const size_t base = kt.size();
+        toff.push_back((long long)base);
+        kt.resize(base + (size_t)mx * KETT_NF * KETT_TILE, 0.0);
+        for (int l = 0; l < KETT_TILE && t0 + l < cnt; l++) {
+          const PairDev& Pp = B->h_pairs[B->cls_beg[c] + t0 + l];
+          for (int iq = 0; iq < Pp.npp; iq++) {
+            const PrimPairDev& r = hpp2[Pp.pp_off + iq];
+            const double f[KETT_NF] = {r.p,     r.Kp,    r.o2p,   r.P[0],  r.P[1],  r.P[2],
+                                       r.PA[0], r.PA[1], r.PA[2], r.PB[0], r.PB[1], r.PB[2]};
+            for (int k = 0; k < KETT_NF; k++)
+              kt[base + ((size_t)iq * KETT_NF + k) * KETT_TILE + l] = f[k];
+          }
+        }
+      }
+    }
+    toff.push_back((long long)kt.size());
+    kt.push_back(0.0);
+    CQF_TRY(upload(&B->d_ketT, kt));
+    CQF_TRY(upload(&B->d_tileOff, toff));
   }
   B->h_schwarz.resize((size_t)nshell * nshell);
   CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
@@ -887,6 +920,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.precision = opts.precision;
   a.fp32_cut = opts.fp32_cutoff;
   a.counters = B->d_counters;
+  a.ketT = B->d_ketT;
+  a.tileOff = B->d_tileOff;
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;
   for (int m = 0; m < nMat; m++) fastOK = fastOK && list[m].hermitian;
@@ -901,6 +936,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.ketBeg = B->cls_beg[ck];
       a.nKet = B->cls_cnt[ck];
       a.same = (cb == ck);
+      a.braTileBeg = B->cls_tile_beg[cb];
+      a.ketTileBeg = B->cls_tile_beg[ck];
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
       unsigned int* w = work + 2 * (cb * NCLS + ck);
       if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, st)))

@@ -23,6 +23,11 @@ inline void class_ls(int c, int& la, int& lb) {
 // Per-matrix flags packed for the kernels: bit0 HER, bit1 EXCHANGE.
 constexpr int MAXMAT = 512;
 
+// Tile-interleaved ket primitive data: fields p, Kp, o2p, P[3], PA[3], PB[3]
+// of KETT_TILE consecutive kets of a class (one persistent-kernel ket tile).
+constexpr int KETT_NF = 12;
+constexpr int KETT_TILE = 128;
+
 // Arguments of one class-quartet J/K launch.
 struct JKLaunch {
   const PairDev* pairs;
@@ -40,6 +45,12 @@ struct JKLaunch {
   const int* flags;         // nMat flags (device)
   const double* Xc;         // nMat x ncart x ncart (complex: interleaved)
   double* Ac;               // same shape, accumulated
+  // ket primitive pairs, tile-interleaved (structure of arrays): field f of
+  // primitive iq of the ket at tile position l is
+  // ketT[tileOff[ketTileBeg + tile] + (iq * KETT_NF + f) * KETT_TILE + l]
+  const double* ketT;
+  const long long* tileOff;
+  int braTileBeg, ketTileBeg;
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
@@ -88,12 +99,15 @@ struct cqf_basis {
   std::vector<cqf::ShellDev> h_shells;
   std::vector<cqf::PairDev> h_pairs;     // final (class, Q-sorted) order
   int cls_beg[cqf::NCLS] = {0}, cls_cnt[cqf::NCLS] = {0};
+  int cls_tile_beg[cqf::NCLS] = {0};    // first ket tile of each class
   std::vector<double> h_schwarz;         // nshell^2
   // device-resident basis data
   cqf::ShellDev* d_shells = nullptr;
   double* d_prim = nullptr;              // alpha | coeff
   cqf::PairDev* d_pairs = nullptr;
   cqf::PrimPairDev* d_pp = nullptr;
+  double* d_ketT = nullptr;              // tile-interleaved ket primitive data
+  long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
   double* d_boys64 = nullptr;
   float* d_boys32 = nullptr;
   double* d_schwarz = nullptr;

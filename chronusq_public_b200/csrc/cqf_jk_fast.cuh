@@ -16,6 +16,8 @@
 
 namespace cqf {
 
+static_assert(JK_THREADS == KETT_TILE, "a ket tile is one block of kets");
+
 template <int N>
 __device__ __forceinline__ void warp_sum(double (&v)[N]) {
 #pragma unroll
@@ -24,6 +26,32 @@ __device__ __forceinline__ void warp_sum(double (&v)[N]) {
     for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
   }
 }
+
+// Ket primitive-pair data of one quartet for the generated eri():
+// KetAoS reads the PrimPairDev records of the pair (any pair order);
+// KetSoA reads the tile-interleaved copy, where the 128 kets of a tile have
+// each field of primitive iq contiguous (a warp's load is one coalesced run).
+struct KetAoS {
+  const PrimPairDev* b;
+  __device__ __forceinline__ double p(int iq) const { return b[iq].p; }
+  __device__ __forceinline__ double Kp(int iq) const { return b[iq].Kp; }
+  __device__ __forceinline__ double o2p(int iq) const { return b[iq].o2p; }
+  __device__ __forceinline__ double P(int iq, int x) const { return b[iq].P[x]; }
+  __device__ __forceinline__ double PA(int iq, int x) const { return b[iq].PA[x]; }
+  __device__ __forceinline__ double PB(int iq, int x) const { return b[iq].PB[x]; }
+};
+struct KetSoA {
+  const double* q;  // tile base + lane
+  __device__ __forceinline__ double f(int iq, int k) const {
+    return __ldg(q + (iq * KETT_NF + k) * KETT_TILE);
+  }
+  __device__ __forceinline__ double p(int iq) const { return f(iq, 0); }
+  __device__ __forceinline__ double Kp(int iq) const { return f(iq, 1); }
+  __device__ __forceinline__ double o2p(int iq) const { return f(iq, 2); }
+  __device__ __forceinline__ double P(int iq, int x) const { return f(iq, 3 + x); }
+  __device__ __forceinline__ double PA(int iq, int x) const { return f(iq, 6 + x); }
+  __device__ __forceinline__ double PB(int iq, int x) const { return f(iq, 9 + x); }
+};
 
 // Rows of the Boys tables for angular sum L (global memory).
 template <typename T>
@@ -118,7 +146,8 @@ __global__ void __launch_bounds__(JK_THREADS, GC::MINB)
     const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
     double I[GC::NI];
     if (work_) {
-      GC::template eri<T>(P, Q, a.pp, boys, ch, I);
+      const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + tile) + threadIdx.x};
+      GC::template eri<T>(P, Q, a.pp, kq, boys, ch, I);
     } else {
 #pragma unroll
       for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
@@ -164,6 +193,7 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
     if (swap) {
       b.braBeg = a.ketBeg; b.nBra = a.nKet;
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
+      b.braTileBeg = a.ketTileBeg; b.ketTileBeg = a.braTileBeg;
     }
     const long long tiles = (long long)((b.nKet + JK_THREADS - 1) / JK_THREADS);
     const long long items64 = (long long)b.nBra * tiles * G64::NCHUNK;
@@ -208,7 +238,7 @@ __global__ void __launch_bounds__(JK_THREADS)
   auto ta = [&](int c, int mu) { return A.pure ? TA[c * nsph(GC::LA) + mu] : (c == mu ? 1.0 : 0.0); };
   auto tb = [&](int c, int nu) { return B.pure ? TB[c * nsph(GC::LB) + nu] : (c == nu ? 1.0 : 0.0); };
   double I[GC::NI];
-  GC::template eri<double>(P, P, pp,
+  GC::template eri<double>(P, P, pp, KetAoS{pp + P.pp_off},
                            boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I);
   for (int mu = 0; mu < na; mu++)
     for (int nu = 0; nu < nb; nu++) {

@@ -158,10 +158,11 @@ def gen_class(la, lb, lc, ld, prec):
     # low-L classes are latency bound and gain from occupancy
     minb = 6 if L <= 1 else (4 if (L == 2 and NAB * CS <= 9) else 1)
     w.line("static constexpr int MINB = %d;" % minb)
-    w.line("template <typename T>")
+    # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
+    w.line("template <typename T, class KA>")
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
-           "const PrimPairDev* __restrict__ pp, const T* __restrict__ boys, const int ch, "
-           "double (&I)[%d]) {" % (NAB * CS))
+           "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
+           "const int ch, double (&I)[%d]) {" % (NAB * CS))
     w.line("#pragma unroll")
     w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NAB * CS))
     w.line("const T PI52x2 = T(34.986836655249725693);")
@@ -179,9 +180,8 @@ def gen_class(la, lb, lc, ld, prec):
             w.line("T g_%d_%d_%d_%d = T(0);" % (k, t, u, v))
     w.line("#pragma unroll 1")
     w.open("for (int iq = 0; iq < Q.npp; iq++) {")
-    w.line("const PrimPairDev& pb = pp[Q.pp_off + iq];")
-    w.line("const T q = T(pb.p), Kcd = T(pb.Kp), o2q = T(pb.o2p);")
-    w.line("const T X = Px - T(pb.P[0]), Y = Py - T(pb.P[1]), Z = Pz - T(pb.P[2]);")
+    w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
+    w.line("const T X = Px - T(kq.P(iq, 0)), Y = Py - T(kq.P(iq, 1)), Z = Pz - T(kq.P(iq, 2));")
     w.line("const T pq = p + q;")
     w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
     w.line("const T alpha = p * q * (rpq * rpq);")
@@ -196,7 +196,8 @@ def gen_class(la, lb, lc, ld, prec):
     w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
     if lcd > 0:
         for x in range(3):
-            w.line("const T QC%s = T(pb.PA[%d]), QD%s = T(pb.PB[%d]);" % (axes[x], x, axes[x], x))
+            w.line("const T QC%s = T(kq.PA(iq, %d)), QD%s = T(kq.PB(iq, %d));"
+                   % (axes[x], x, axes[x], x))
     ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
           for x in range(3)] if lcd > 0 else None
     R = {}
