@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="h2o16_def2svp")
-    ap.add_argument("--cutoff", type=float, default=1e-8)
+    ap.add_argument("--cutoff", type=float, default=1e-2)
     ap.add_argument("--no-oracle", action="store_true")
     ap.add_argument("--batched", type=int, default=1,
                     help="also time the 64-density dD build as a CUDA graph")

@@ -336,6 +336,22 @@ __global__ void max_norms_kernel(const double* __restrict__ nm, int nMat, size_t
     atomicMax(gmax, (unsigned long long)__double_as_longlong(red[0]));
 }
 
+// transpose of the max-norm table and the norm of each pair's own block
+__global__ void norms_aux_kernel(const double* __restrict__ nm, int ns,
+                                 const PairDev* __restrict__ pairs, int npair, double* nmT,
+                                 double* pn) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t ns2 = (size_t)ns * ns;
+  if (k < ns2) {
+    const int r = (int)(k % ns), c = (int)(k / ns);
+    nmT[k] = nm[c + (size_t)r * ns];
+  }
+  if (k < (size_t)npair) {
+    const PairDev P = pairs[k];
+    pn[k] = nm[P.s1 + (size_t)P.s2 * ns];
+  }
+}
+
 // Xc = T X T^T per matrix (T: block-diagonal Cartesian -> AO transform).
 __global__ void to_cart_kernel(const double* __restrict__ X, int cplx, int N, int nc,
                                const ShellDev* __restrict__ sh, const int* __restrict__ c2s,
@@ -428,12 +444,17 @@ __global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int he
 
 unsigned grid1(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// Basis-owned device memory is stream-ordered on the basis' stream
+// (cudaMallocAsync / cudaFreeAsync): creating, growing or destroying one
+// basis never waits for the work of other bases (no device-wide sync).  The
+// stream is synchronised before a new buffer is used from another stream.
 cqf_status ensure_ws(cqf_basis* B, size_t bytes) {
   if (bytes <= B->ws_bytes) return CQF_OK;
-  if (B->d_ws) CQF_CUDA(cudaFree(B->d_ws));
+  if (B->d_ws) CQF_CUDA(cudaFreeAsync(B->d_ws, B->stream));
   B->d_ws = nullptr;
   B->ws_bytes = 0;
-  CQF_CUDA(cudaMalloc(&B->d_ws, bytes));
+  CQF_CUDA(cudaMallocAsync(&B->d_ws, bytes, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
   B->ws_bytes = bytes;
   return CQF_OK;
 }
@@ -441,26 +462,16 @@ cqf_status ensure_ws(cqf_basis* B, size_t bytes) {
 void free_basis(cqf_basis* B) {
   if (!B) return;
   cudaSetDevice(B->device);
-  cudaFree(B->d_shells);
-  cudaFree(B->d_prim);
-  cudaFree(B->d_pairs);
-  cudaFree(B->d_pp);
-  cudaFree(B->d_ketT);
-  cudaFree(B->d_tileOff);
-  cudaFree(B->d_boys64);
-  cudaFree(B->d_boys32);
-  cudaFree(B->d_schwarz);
-  cudaFree(B->d_sph);
-  cudaFree(B->d_sphOff);
-  cudaFree(B->d_ao2shell);
-  cudaFree(B->d_cart2shell);
-  cudaFree(B->d_ws);
-  cudaFree(B->d_counters);
-  cudaFree(B->d_flags);
-  cudaFree(B->d_qLL);
-  cudaFree(B->d_qSS);
-  cudaFree(B->d_relws);
-  if (B->h_flags) cudaFreeHost(B->h_flags);
+  if (B->stream) {
+    cudaStream_t st = B->stream;
+    for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
+                    (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_schwarz,
+                    (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
+                    (void*)B->d_cart2shell, (void*)B->d_ws, (void*)B->d_counters,
+                    (void*)B->d_flags, (void*)B->d_qLL, (void*)B->d_qSS, (void*)B->d_relws})
+      if (p) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+  }
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -468,10 +479,44 @@ void free_basis(cqf_basis* B) {
 }
 
 template <typename T>
-cqf_status upload(T** dst, const std::vector<T>& src) {
-  CQF_CUDA(cudaMalloc((void**)dst, std::max<size_t>(1, src.size()) * sizeof(T)));
+cqf_status upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
+  CQF_CUDA(cudaMallocAsync((void**)dst, std::max<size_t>(1, src.size()) * sizeof(T), st));
+  // pageable source: the copy is staged before the call returns
   if (!src.empty())
-    CQF_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    CQF_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
+                             st));
+  return CQF_OK;
+}
+
+// Boys tables: computed once per process, one device copy per device (held
+// until exit, shared by every basis on the device).
+cqf_status boys_tables(int device, cudaStream_t st, double** d64, float** d32) {
+  static std::mutex mu;
+  static std::vector<double> h64;
+  static std::vector<float> h32;
+  static std::vector<double*> dev64;
+  static std::vector<float*> dev32;
+  std::lock_guard<std::mutex> lk(mu);
+  if (h64.empty()) make_boys_table(h64, h32);
+  if ((int)dev64.size() <= device) {
+    dev64.resize(device + 1, nullptr);
+    dev32.resize(device + 1, nullptr);
+  }
+  if (!dev64[device]) {
+    double* p64 = nullptr;
+    float* p32 = nullptr;
+    CQF_CUDA(cudaMalloc(&p64, h64.size() * sizeof(double)));
+    CQF_CUDA(cudaMalloc(&p32, h32.size() * sizeof(float)));
+    CQF_CUDA(cudaMemcpyAsync(p64, h64.data(), h64.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, st));
+    CQF_CUDA(cudaMemcpyAsync(p32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice,
+                             st));
+    CQF_CUDA(cudaStreamSynchronize(st));
+    dev64[device] = p64;
+    dev32[device] = p32;
+  }
+  *d64 = dev64[device];
+  *d32 = dev32[device];
   return CQF_OK;
 }
 
@@ -520,8 +565,8 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   const int nprimTot = (int)alpha.size();
   std::vector<double> prim(alpha);
   prim.insert(prim.end(), coef.begin(), coef.end());
-  CQF_TRY(upload(&B->d_shells, B->h_shells));
-  CQF_TRY(upload(&B->d_prim, prim));
+  CQF_TRY(upload(&B->d_shells, B->h_shells, B->stream));
+  CQF_TRY(upload(&B->d_prim, prim, B->stream));
 
   std::vector<int> ao2s, c2s;
   for (int s = 0; s < nshell; s++) {
@@ -529,8 +574,8 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     for (int i = 0; i < (d.pure ? nsph(d.l) : ncart(d.l)); i++) ao2s.push_back(s);
     for (int i = 0; i < ncart(d.l); i++) c2s.push_back(s);
   }
-  CQF_TRY(upload(&B->d_ao2shell, ao2s));
-  CQF_TRY(upload(&B->d_cart2shell, c2s));
+  CQF_TRY(upload(&B->d_ao2shell, ao2s, B->stream));
+  CQF_TRY(upload(&B->d_cart2shell, c2s, B->stream));
 
   std::vector<double> sph;
   std::vector<int> sphO;
@@ -539,25 +584,21 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     auto T = solid_harmonics(l);
     sph.insert(sph.end(), T.begin(), T.end());
   }
-  CQF_TRY(upload(&B->d_sph, sph));
-  CQF_TRY(upload(&B->d_sphOff, sphO));
+  CQF_TRY(upload(&B->d_sph, sph, B->stream));
+  CQF_TRY(upload(&B->d_sphOff, sphO, B->stream));
 
-  std::vector<double> b64;
-  std::vector<float> b32;
-  make_boys_table(b64, b32);
-  CQF_TRY(upload(&B->d_boys64, b64));
-  CQF_TRY(upload(&B->d_boys32, b32));
+  CQF_TRY(boys_tables(device, B->stream, &B->d_boys64, &B->d_boys32));
 
   // significant pairs on the device
   long long nlt = (long long)nshell * (nshell + 1) / 2;
   unsigned char* d_flags8 = nullptr;
-  CQF_CUDA(cudaMalloc(&d_flags8, std::max<long long>(1, nlt)));
+  CQF_CUDA(cudaMallocAsync(&d_flags8, std::max<long long>(1, nlt), B->stream));
   sig_pairs_kernel<<<grid1(nlt, 128), 128, 0, B->stream>>>(B->d_shells, B->d_prim, B->d_sph,
                                                            B->d_sphOff, nshell, nprimTot, d_flags8);
   std::vector<unsigned char> f8(nlt);
   CQF_CUDA(cudaMemcpyAsync(f8.data(), d_flags8, nlt, cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
-  cudaFree(d_flags8);
+  cudaFreeAsync(d_flags8, B->stream);
 
   // pair list in the reference loop order, then grouped by class (stable)
   std::vector<PairDev> lexPairs;
@@ -592,14 +633,14 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   B->npair = (int)pairs.size();
   B->nprimpair = ppoff;
   PairDev* d_tmp = nullptr;
-  CQF_TRY(upload(&d_tmp, pairs));
-  CQF_CUDA(cudaMalloc(&B->d_pp, std::max<long long>(1, ppoff) * sizeof(PrimPairDev)));
+  CQF_TRY(upload(&d_tmp, pairs, B->stream));
+  CQF_CUDA(cudaMallocAsync(&B->d_pp, std::max<long long>(1, ppoff) * sizeof(PrimPairDev), B->stream));
   prim_pairs_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_shells, B->d_prim, nprimTot,
                                                                  d_tmp, B->npair, B->d_pp);
-  CQF_CUDA(cudaMalloc(&B->d_schwarz, (size_t)nshell * nshell * sizeof(double)));
+  CQF_CUDA(cudaMallocAsync(&B->d_schwarz, (size_t)nshell * nshell * sizeof(double), B->stream));
   CQF_CUDA(cudaMemsetAsync(B->d_schwarz, 0, (size_t)nshell * nshell * sizeof(double), B->stream));
   double* d_diag = nullptr;
-  CQF_CUDA(cudaMalloc(&d_diag, std::max(1, B->npair) * 36 * sizeof(double)));
+  CQF_CUDA(cudaMallocAsync(&d_diag, std::max(1, B->npair) * 36 * sizeof(double), B->stream));
   for (int c = 0; c < NCLS; c++) {
     if (B->cls_cnt[c] <= 0) continue;
     int la, lb;
@@ -618,19 +659,19 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   unsigned long long *kin = nullptr, *kout = nullptr;
   int *vin = nullptr, *vout = nullptr;
   int n = std::max(1, B->npair);
-  CQF_CUDA(cudaMalloc(&kin, n * sizeof(unsigned long long)));
-  CQF_CUDA(cudaMalloc(&kout, n * sizeof(unsigned long long)));
-  CQF_CUDA(cudaMalloc(&vin, n * sizeof(int)));
-  CQF_CUDA(cudaMalloc(&vout, n * sizeof(int)));
+  CQF_CUDA(cudaMallocAsync(&kin, n * sizeof(unsigned long long), B->stream));
+  CQF_CUDA(cudaMallocAsync(&kout, n * sizeof(unsigned long long), B->stream));
+  CQF_CUDA(cudaMallocAsync(&vin, n * sizeof(int), B->stream));
+  CQF_CUDA(cudaMallocAsync(&vout, n * sizeof(int), B->stream));
   sort_keys_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(d_tmp, B->npair, kin, vin);
   size_t tmpBytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, kin, kout, vin, vout, B->npair, 0, 64,
                                   B->stream);
   void* d_cub = nullptr;
-  CQF_CUDA(cudaMalloc(&d_cub, std::max<size_t>(1, tmpBytes)));
+  CQF_CUDA(cudaMallocAsync(&d_cub, std::max<size_t>(1, tmpBytes), B->stream));
   CQF_CUDA(cub::DeviceRadixSort::SortPairs(d_cub, tmpBytes, kin, kout, vin, vout, B->npair, 0,
                                            64, B->stream));
-  CQF_CUDA(cudaMalloc(&B->d_pairs, n * sizeof(PairDev)));
+  CQF_CUDA(cudaMallocAsync(&B->d_pairs, n * sizeof(PairDev), B->stream));
   gather_pairs_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(d_tmp, vout, B->npair,
                                                                    B->d_pairs);
   CQF_CUDA(cudaGetLastError());
@@ -649,13 +690,16 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
       off2 += B->h_pairs[i].npp;
     }
     std::vector<PrimPairDev> hpp(ppoff), hpp2(ppoff);
-    CQF_CUDA(cudaMemcpy(hpp.data(), B->d_pp, ppoff * sizeof(PrimPairDev), cudaMemcpyDeviceToHost));
+    CQF_CUDA(cudaMemcpyAsync(hpp.data(), B->d_pp, ppoff * sizeof(PrimPairDev),
+                             cudaMemcpyDeviceToHost, B->stream));
+    CQF_CUDA(cudaStreamSynchronize(B->stream));
     for (int i = 0; i < B->npair; i++)
       std::copy(hpp.begin() + src[i], hpp.begin() + src[i] + B->h_pairs[i].npp,
                 hpp2.begin() + B->h_pairs[i].pp_off);
-    CQF_CUDA(cudaMemcpy(B->d_pp, hpp2.data(), ppoff * sizeof(PrimPairDev), cudaMemcpyHostToDevice));
-    CQF_CUDA(cudaMemcpy(B->d_pairs, B->h_pairs.data(), B->npair * sizeof(PairDev),
-                        cudaMemcpyHostToDevice));
+    CQF_CUDA(cudaMemcpyAsync(B->d_pp, hpp2.data(), ppoff * sizeof(PrimPairDev),
+                             cudaMemcpyHostToDevice, B->stream));
+    CQF_CUDA(cudaMemcpyAsync(B->d_pairs, B->h_pairs.data(), B->npair * sizeof(PairDev),
+                             cudaMemcpyHostToDevice, B->stream));
     // the same data tile-interleaved for the class kernels' kets: per ket
     // tile (KETT_TILE consecutive pairs of a class), field-major runs of
     // KETT_TILE values for each primitive (zero past a pair's npp)
@@ -685,24 +729,25 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     }
     toff.push_back((long long)kt.size());
     kt.push_back(0.0);
-    CQF_TRY(upload(&B->d_ketT, kt));
-    CQF_TRY(upload(&B->d_tileOff, toff));
+    CQF_TRY(upload(&B->d_ketT, kt, B->stream));
+    CQF_TRY(upload(&B->d_tileOff, toff, B->stream));
   }
   B->h_schwarz.resize((size_t)nshell * nshell);
   CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
                            (size_t)nshell * nshell * sizeof(double), cudaMemcpyDeviceToHost,
                            B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
-  cudaFree(kin);
-  cudaFree(kout);
-  cudaFree(vin);
-  cudaFree(vout);
-  cudaFree(d_cub);
-  cudaFree(d_tmp);
-  cudaFree(d_diag);
-  CQF_CUDA(cudaMalloc(&B->d_counters, 8 * sizeof(unsigned long long)));
-  CQF_CUDA(cudaMalloc(&B->d_flags, MAXMAT * sizeof(int)));
-  CQF_CUDA(cudaMallocHost(&B->h_flags, MAXMAT * sizeof(int)));
+  cudaFreeAsync(kin, B->stream);
+  cudaFreeAsync(kout, B->stream);
+  cudaFreeAsync(vin, B->stream);
+  cudaFreeAsync(vout, B->stream);
+  cudaFreeAsync(d_cub, B->stream);
+  cudaFreeAsync(d_tmp, B->stream);
+  cudaFreeAsync(d_diag, B->stream);
+  CQF_CUDA(cudaMallocAsync(&B->d_counters, 8 * sizeof(unsigned long long), B->stream));
+  CQF_CUDA(cudaMallocAsync(&B->d_flags, MAXMAT * sizeof(int), B->stream));
+  B->h_flags.assign(MAXMAT, 0);
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
   return CQF_OK;
 }
 
@@ -822,6 +867,8 @@ WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   L.oNmM = take(ns2 * nMat);
   L.oG = take(4);
   L.oWork = take((NWORK + 1) / 2);
+  L.oNmT = take(ns2);
+  L.oPN = take((size_t)std::max(1, B->npair));
   L.total = off;
   return L;
 }
@@ -875,7 +922,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   if (!d_flags) {
     for (int m = 0; m < nMat; m++)
       B->h_flags[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
-    CQF_CUDA(cudaMemcpyAsync(B->d_flags, B->h_flags, nMat * sizeof(int), cudaMemcpyHostToDevice,
+    CQF_CUDA(cudaMemcpyAsync(B->d_flags, B->h_flags.data(), nMat * sizeof(int), cudaMemcpyHostToDevice,
                              st));
     d_flags = B->d_flags;
   }
@@ -892,6 +939,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   }
   max_norms_kernel<<<grid1(ns2, 256), 256, 0, st>>>(ws + oNmM, nMat, ns2, ws + oNm,
                                                     reinterpret_cast<unsigned long long*>(ws + oG));
+  norms_aux_kernel<<<grid1(std::max(ns2, (size_t)B->npair), 256), 256, 0, st>>>(
+      ws + oNm, ns, B->d_pairs, B->npair, ws + Lw.oNmT, ws + Lw.oPN);
   // densities to the Cartesian AO basis, zero accumulators
   for (int m = 0; m < nMat; m++)
     to_cart_kernel<<<grid1((size_t)nc * nc, 256), 256, 0, st>>>(
@@ -910,6 +959,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.norms = ws + oNm;
   a.normsMat = ws + oNmM;
   a.maxNorm = ws + oG;
+  a.normsT = ws + Lw.oNmT;
+  a.pairNorm = ws + Lw.oPN;
   a.nShell = ns;
   a.nMat = nMat;
   a.cplx = opts.is_complex;

@@ -40,6 +40,8 @@ struct JKLaunch {
   const double* norms;      // max over matrices, nshell x nshell (col-major)
   const double* normsMat;   // nMat x nshell x nshell (only read when nMat > 1)
   const double* maxNorm;    // device scalar: max of norms (tile-level screen)
+  const double* normsT;     // transpose of norms
+  const double* pairNorm;   // per pair (pair order): norms(s1, s2)
   int nShell;
   int nMat, cplx, ncart;
   const int* flags;         // nMat flags (device)
@@ -62,7 +64,7 @@ cqf_status fail(cqf_status s, const std::string& msg);
 // Workspace layout of one contraction (in doubles, each part 256-B aligned):
 // [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
 struct WsLayout {
-  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oWork, total;
+  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oWork, oNmT, oPN, total;
 };
 constexpr int NWORK = 2 * NCLS * NCLS;  // persistent-kernel work counters per call
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
@@ -120,7 +122,7 @@ struct cqf_basis {
   void* d_ws = nullptr;
   unsigned long long* d_counters = nullptr;
   int* d_flags = nullptr;                // MAXMAT per-matrix flags
-  int* h_flags = nullptr;                // pinned staging of the flags
+  std::vector<int> h_flags;              // host staging of the flags
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // four-component path: Schwarz tables (computed on first use, nshell^2
   // each, zero for pairs outside the significant-pair list) and workspace

@@ -66,59 +66,95 @@ __device__ __forceinline__ const float* boys_rows<float>(const JKLaunch& a, int 
 }
 
 // Persistent class kernel.  Each block stages the Boys rows of this class's
-// angular sum in shared memory once, then takes work items
-// (bra pair, chunk, ket tile of 128) from a device counter until none are
-// left.  FP64 launch: quartets with bound >= cut (all when cut <= 0); FP32
-// launch: quartets with thresh <= bound < cut.  The FP64 launch also counts
-// the visited / screened quartets.
-template <class GC, typename T>
-__global__ void __launch_bounds__(JK_THREADS, GC::MINB)
-    jk_fast_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
-  constexpr int NA = ncart(GC::LA), NB = ncart(GC::LB);
-  constexpr int NCH = GC::NCHUNK;
-  constexpr int LSUM = GC::LA + GC::LB + GC::LC + GC::LD;
-  constexpr bool IS64 = sizeof(T) == 8;
-  constexpr int TBYTES = IS64 ? BOYS_LBYTES64 : BOYS_LBYTES32;
-  extern __shared__ float4 s_boys4[];
-  {
-    const float4* g = reinterpret_cast<const float4*>(boys_rows<T>(a, LSUM));
-    for (int i = threadIdx.x; i < TBYTES / 16; i += JK_THREADS) s_boys4[i] = __ldg(g + i);
-  }
-  const T* boys = reinterpret_cast<const T*>(s_boys4);
-  __shared__ long long s_item;
+// angular sum in shared memory once (FP64 rows, plus the FP32 rows on the
+// mixed path); then every warp independently takes work items (bra pair,
+// chunk, ket tile of 32) from a device counter until none are left -- no
+// block barriers after the staging.  On the mixed path a warp computes its
+// quartets in FP32 when every surviving quartet's bound is below the cut
+// and in FP64 otherwise (kets are sorted by Schwarz bound, so the warps of
+// a bra row switch from FP64 to FP32 once), in one traversal.
+constexpr int WTILE = 32;  // kets per work item (one warp)
+
+// Shell-block norm maximum of a quartet in the reference's roles
+// (direct.hpp:1693-1736), with the warp-uniform bra pair P: the pair norms
+// come from the per-pair array, and the four cross terms are read from the
+// column of a bra shell (normsT holds the transpose), so a warp's lanes read
+// one column instead of 32 scattered ones.
+__device__ __forceinline__ double sh_max_bra(const JKLaunch& a, const PairDev& P,
+                                             const PairDev& Q, double nP, double nQ,
+                                             bool pRef) {
   const int ns = a.nShell;
-  const double cut = (a.precision == 1) ? a.fp32_cut : 0.0;
-  const int ketTiles = (a.nKet + JK_THREADS - 1) / JK_THREADS;
+  double m;
+  if (pRef) {  // rows from P (uniform): B(r, c) = normsT[c + r ns]
+    const double* c1 = a.normsT + (size_t)P.s1 * ns;
+    const double* c2 = a.normsT + (size_t)P.s2 * ns;
+    m = fmax(fmax(__ldg(c1 + Q.s1), __ldg(c2 + Q.s1)), fmax(__ldg(c1 + Q.s2), __ldg(c2 + Q.s2)));
+  } else {     // rows from Q, columns from P (uniform): B(r, c) = norms[r + c ns]
+    const double* c1 = a.norms + (size_t)P.s1 * ns;
+    const double* c2 = a.norms + (size_t)P.s2 * ns;
+    m = fmax(fmax(__ldg(c1 + Q.s1), __ldg(c1 + Q.s2)), fmax(__ldg(c2 + Q.s1), __ldg(c2 + Q.s2)));
+  }
+  return fmax(m, fmax(nP, nQ));
+}
+
+template <class G64, class G32, bool MIXED>
+__global__ void __launch_bounds__(JK_THREADS, G64::MINB)
+    jk_fast_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
+  static_assert(G64::NCHUNK == G32::NCHUNK && G64::NI == G32::NI, "shared chunking");
+  constexpr int NA = ncart(G64::LA), NB = ncart(G64::LB);
+  constexpr int NCH = G64::NCHUNK;
+  constexpr int LSUM = G64::LA + G64::LB + G64::LC + G64::LD;
+  extern __shared__ float4 s_boys4[];
+  const double cut = MIXED ? a.fp32_cut : 0.0;
+  constexpr bool mixed = MIXED;
+  {
+    const float4* g = reinterpret_cast<const float4*>(boys_rows<double>(a, LSUM));
+    for (int i = threadIdx.x; i < BOYS_LBYTES64 / 16; i += JK_THREADS) s_boys4[i] = __ldg(g + i);
+    if (mixed) {
+      const float4* g32 = reinterpret_cast<const float4*>(boys_rows<float>(a, LSUM));
+      for (int i = threadIdx.x; i < BOYS_LBYTES32 / 16; i += JK_THREADS)
+        s_boys4[BOYS_LBYTES64 / 16 + i] = __ldg(g32 + i);
+    }
+  }
+  __syncthreads();
+  const double* boys64 = reinterpret_cast<const double*>(s_boys4);
+  const float* boys32 = reinterpret_cast<const float*>(s_boys4 + BOYS_LBYTES64 / 16);
+  const int lane = threadIdx.x & 31;
+  const int ketTiles = (a.nKet + WTILE - 1) / WTILE;
   const long long perBra = (long long)ketTiles * NCH;
   const long long total = (long long)a.nBra * perBra;
   const size_t nc = a.ncart;
   const size_t matStride = (size_t)a.ncart * a.ncart;
-  if (!IS64 && cut <= 0.0) return;  // uniform: nothing below the cut
+  // quartet counts of this warp, flushed once at exit
+  unsigned long long cVis = 0, cScr = 0, c32 = 0, c64 = 0;
 
   for (;;) {
-    __syncthreads();  // table staged / previous item's s_item consumed
-    if (threadIdx.x == 0) s_item = (long long)atomicAdd(work, 1u);
-    __syncthreads();
-    const long long item = s_item;
+    unsigned int itemU = 0;
+    if (lane == 0) itemU = atomicAdd(work, 1u);
+    const long long item = (long long)__shfl_sync(0xffffffffu, itemU, 0);
     if (item >= total) break;
     const int ib = (int)(item / perBra);
     const int rem = (int)(item % perBra);
     const int ch = rem / ketTiles, tile = rem % ketTiles;
     // same class: each unordered pair {P, Q} once, as ket position <= bra
     // position (roles still follow the lex order)
-    if (a.same && tile * JK_THREADS > ib) continue;
-    const int jk = tile * JK_THREADS + threadIdx.x;
+    if (a.same && tile * WTILE > ib) continue;
+    const int jk = tile * WTILE + lane;
     const PairDev P = a.pairs[a.braBeg + ib];
-    bool visited = false, screened = false, work_ = false;
+    bool visited = false, screened = false, w64 = false, w32 = false;
     PairDev Q;
     if (jk < a.nKet && !(a.same && jk > ib)) {
       Q = a.pairs[a.ketBeg + jk];
       visited = true;
     }
-    const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * JK_THREADS].Q;
-    const bool counter = IS64 && ch == 0;  // one count per quartet
+    const bool counter = ch == 0;  // one count per quartet
+    const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * WTILE].Q;
     if (a.screen && tileMax < a.thresh) {
-      if (IS64) count_block(a.counters, counter && visited, counter && visited, false, false);
+      if (counter) {
+        const unsigned bv = __ballot_sync(0xffffffffu, visited);
+        cVis += __popc(bv);
+        cScr += __popc(bv);
+      }
       continue;
     }
     int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
@@ -129,28 +165,43 @@ __global__ void __launch_bounds__(JK_THREADS, GC::MINB)
       s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
       double bound = 1e300;
       if (a.screen) {
-        bound = sh_max(a.norms, s1, s2, s3, s4, ns) * P.Q * Q.Q;
+        bound = sh_max_bra(a, P, Q, __ldg(a.pairNorm + a.braBeg + ib),
+                           __ldg(a.pairNorm + a.ketBeg + jk), pRef) * P.Q * Q.Q;
         screened = bound < a.thresh;
       }
-      const bool lo = bound < cut;
-      work_ = !screened && (IS64 ? !lo : lo);
+      w64 = !screened;
+      w32 = w64 && mixed && bound < cut;
     }
-    if (IS64)
-      count_block(a.counters, counter && visited, counter && screened, false, counter && work_);
-    else
-      count_block(a.counters, false, false, ch == 0 && work_, false);
-    if (!__syncthreads_or(work_)) continue;
+    // one precision per warp: FP32 only when every surviving quartet of the
+    // warp is below the cut (no divergent FP64 / FP32 code in a warp)
+    if (__any_sync(0xffffffffu, w64 && !w32)) {
+      w32 = false;
+    } else {
+      w64 = w64 && !w32;
+    }
+    const unsigned b64 = __ballot_sync(0xffffffffu, w64);
+    const unsigned b32 = __ballot_sync(0xffffffffu, w32);
+    if (counter) {
+      cVis += __popc(__ballot_sync(0xffffffffu, visited));
+      cScr += __popc(__ballot_sync(0xffffffffu, screened));
+      c64 += __popc(b64);
+      c32 += __popc(b32);
+    }
+    if (!(b64 | b32)) continue;
+    const bool work_ = w64 || w32;
 
     const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
                        ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
     const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
-    double I[GC::NI];
-    if (work_) {
-      const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + tile) + threadIdx.x};
-      GC::template eri<T>(P, Q, a.pp, kq, boys, ch, I);
+    double I[G64::NI];
+    const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
+    if (w64) {
+      G64::template eri<double>(P, Q, a.pp, kq, boys64, ch, I);
+    } else if (MIXED && w32) {
+      G32::template eri<float>(P, Q, a.pp, kq, boys32, ch, I);
     } else {
 #pragma unroll
-      for (int i = 0; i < GC::NI; i++) I[i] = 0.0;
+      for (int i = 0; i < G64::NI; i++) I[i] = 0.0;
     }
 #pragma unroll 1
     for (int m = 0; m < a.nMat; m++) {
@@ -161,14 +212,14 @@ __global__ void __launch_bounds__(JK_THREADS, GC::MINB)
       for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
       const double* X = a.Xc + m * matStride;
       double* A = a.Ac + m * matStride;
-      GC::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
-                 jab);
+      G64::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
+                  jab);
       if (doJ) {
         // every lane of the warp shares the bra pair: reduce, one atomic each
 #pragma unroll
         for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
         warp_sum(jab);
-        if ((threadIdx.x & 31) == 0) {
+        if (lane == 0) {
 #pragma unroll
           for (int i = 0; i < NA * NB; i++)
             if (jab[i] != 0.0)
@@ -176,6 +227,12 @@ __global__ void __launch_bounds__(JK_THREADS, GC::MINB)
         }
       }
     }
+  }
+  if (lane == 0) {
+    if (cVis) atomicAdd(a.counters + 0, cVis);
+    if (cScr) atomicAdd(a.counters + 1, cScr);
+    if (c32) atomicAdd(a.counters + 2, c32);
+    if (c64) atomicAdd(a.counters + 3, c64);
   }
 }
 
@@ -195,16 +252,19 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
       b.braTileBeg = a.ketTileBeg; b.ketTileBeg = a.braTileBeg;
     }
-    const long long tiles = (long long)((b.nKet + JK_THREADS - 1) / JK_THREADS);
-    const long long items64 = (long long)b.nBra * tiles * G64::NCHUNK;
-    const long long items32 = (long long)b.nBra * tiles * G32::NCHUNK;
+    const long long tiles = (long long)((b.nKet + WTILE - 1) / WTILE);
+    const long long items = (long long)b.nBra * tiles * G64::NCHUNK;
     // persistent blocks: enough for full residency on every SM (extra blocks
-    // queue and find the counter exhausted)
-    const unsigned g64 = (unsigned)std::min<long long>(items64, (long long)nsm * 8);
-    const unsigned g32 = (unsigned)std::min<long long>(items32, (long long)nsm * 8);
-    jk_fast_kernel<G64, double><<<g64, JK_THREADS, BOYS_LBYTES64, st>>>(b, work);
-    if (b.precision == 1 && b.fp32_cut > 0.0)
-      jk_fast_kernel<G32, float><<<g32, JK_THREADS, BOYS_LBYTES32, st>>>(b, work + 1);
+    // queue and find the counter exhausted); one work item per warp at a time
+    constexpr int WPB = JK_THREADS / 32;
+    const unsigned g = (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * 8);
+    const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
+    const size_t smem = BOYS_LBYTES64 + (mixed ? BOYS_LBYTES32 : 0);
+    static_assert(BOYS_LBYTES64 + BOYS_LBYTES32 <= 48 * 1024, "default shared memory limit");
+    if (mixed)
+      jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, smem, st>>>(b, work);
+    else
+      jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, smem, st>>>(b, work);
     done = true;
   };
 #define CQF_TRY_CLASS(A_, B_, C_, D_, N64, N32)                                          \

@@ -699,14 +699,16 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream
   needSS = needSS && !B->rel_qSS;
   if (!needLL && !needSS) return CQF_OK;
   const size_t ns2 = (size_t)B->nshell * B->nshell;
+  // basis-owned, stream-ordered on the basis' stream (freed by free_basis)
   if (!B->d_qLL) {
-    CQF_RCUDA(cudaMalloc(&B->d_qLL, ns2 * sizeof(double)));
-    CQF_RCUDA(cudaMemsetAsync(B->d_qLL, 0, ns2 * sizeof(double), st));
+    CQF_RCUDA(cudaMallocAsync(&B->d_qLL, ns2 * sizeof(double), B->stream));
+    CQF_RCUDA(cudaMemsetAsync(B->d_qLL, 0, ns2 * sizeof(double), B->stream));
   }
   if (!B->d_qSS) {
-    CQF_RCUDA(cudaMalloc(&B->d_qSS, ns2 * sizeof(double)));
-    CQF_RCUDA(cudaMemsetAsync(B->d_qSS, 0, ns2 * sizeof(double), st));
+    CQF_RCUDA(cudaMallocAsync(&B->d_qSS, ns2 * sizeof(double), B->stream));
+    CQF_RCUDA(cudaMemsetAsync(B->d_qSS, 0, ns2 * sizeof(double), B->stream));
   }
+  CQF_RCUDA(cudaStreamSynchronize(B->stream));
   for (int c = 0; c < NCLS; c++) {
     if (B->cls_cnt[c] <= 0) continue;
     int la, lb;
@@ -849,10 +851,11 @@ __global__ void finish_gd_kernel(double* twoeH, double* K, int N, double xHFX, i
 // ------------------------------------------------------------ host driver
 cqf_status ensure_relws(cqf_basis* B, size_t bytes) {
   if (bytes <= B->relws_bytes) return CQF_OK;
-  if (B->d_relws) CQF_RCUDA(cudaFree(B->d_relws));
+  if (B->d_relws) CQF_RCUDA(cudaFreeAsync(B->d_relws, B->stream));
   B->d_relws = nullptr;
   B->relws_bytes = 0;
-  CQF_RCUDA(cudaMalloc(&B->d_relws, bytes));
+  CQF_RCUDA(cudaMallocAsync(&B->d_relws, bytes, B->stream));
+  CQF_RCUDA(cudaStreamSynchronize(B->stream));
   B->relws_bytes = bytes;
   return CQF_OK;
 }

@@ -142,7 +142,9 @@ def gen_class(la, lb, lc, ld, prec):
     NAB, NCD = NA * NB, NC * ND
     lab, lcd = la + lb, lc + ld
     L = lab + lcd
-    CS = chunk_size(la, lb, lc, ld, prec)
+    # both precisions use the FP64 chunking: one launch computes FP64 and
+    # FP32 quartets side by side with the same chunk index and digestion
+    CS = chunk_size(la, lb, lc, ld, 64)
     nchunk = (NCD + CS - 1) // CS
     chunks = [list(range(k * CS, min(NCD, (k + 1) * CS))) for k in range(nchunk)]
     hab = herm_list(lab)
