@@ -1,12 +1,10 @@
 // cqf_two_body_contract_noalloc: the direct J/K contraction for callers that
 // must not allocate device memory during the call.
 //
-// Who cannot allocate: code running while a CUDA stream is being captured
-// into a graph (cudaMalloc/cudaFree are not allowed there), host code that
-// runs inside a framework that owns the whole device memory pool and forbids
-// side allocations (e.g. a serving engine that has reserved HBM up front), and
-// latency-critical loops that cannot afford the implicit device
-// synchronisation of cudaFree.  cqf_two_body_contract grows a per-basis
+// Who cannot allocate: host code that runs inside a framework that owns the
+// whole device memory pool and forbids side allocations (e.g. a serving
+// engine that has reserved HBM up front), and latency-critical loops that
+// cannot afford the implicit device synchronisation of cudaFree.  cqf_two_body_contract grows a per-basis
 // workspace with cudaMalloc on first use; this entry point instead uses one
 // fixed array compiled into the library.
 //

@@ -1,9 +1,8 @@
 """cqf_two_body_contract_noalloc against cqf_two_body_contract.
 
 Some callers of the J/K contraction cannot allocate device memory during the
-call: code that runs while a CUDA stream is being captured into a graph (where
-cudaMalloc is not allowed), or a host program whose framework owns all of the
-GPU's memory.  For them the library has an entry point that takes its
+call: a host program whose framework owns all of the GPU's memory, or a
+latency-critical loop that cannot afford cudaFree's device synchronisation.  For them the library has an entry point that takes its
 scratch from one fixed array compiled into libcqfock.so instead of growing a
 workspace with cudaMalloc.  This file checks, through the C ABI, that two
 calls in a row of that entry point give the regular entry point's J and K on
