@@ -226,11 +226,15 @@ constexpr int REL_THREADS = 64;
 // TYPE 1: LLSS (bra = SS pair, differentiated; ket = LL pair), all
 // (bra, ket) combinations (direct4C_libcint.hpp:907-929).
 // TYPE 2: SSSS, unique quartets of pairs (:2018-2047).
+// The ket's Cartesian component pairs (c, d) of a quartet are split over
+// nsplit threads (grid y = ket tiles x nsplit): the heavy classes with few
+// quartets (f shells) still fill the GPU.
 template <int LM, int TYPE>
 __global__ void __launch_bounds__(REL_THREADS)
-    rel_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+    rel_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int nsplit) {
   const int ib = blockIdx.x;
-  const int jk = blockIdx.y * REL_THREADS + threadIdx.x;
+  const int split = blockIdx.y % nsplit;
+  const int jk = (blockIdx.y / nsplit) * REL_THREADS + threadIdx.x;
   const int ns = a.nShell;
   const bool visited = jk < a.nKet && !(TYPE == 2 && a.same && jk > ib);
   const PairDev P = a.pairs[a.braBeg + ib];
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(REL_THREADS)
     // shMax * Q12 * Q34 < thresh (:947-948, :2059-2061)
     work = !a.screen || sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34 >= a.thresh;
   }
-  {
+  if (split == 0) {
     const unsigned mask = __activemask();
     const unsigned bv = __ballot_sync(mask, visited), bw = __ballot_sync(mask, work);
     if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
@@ -264,7 +268,6 @@ __global__ void __launch_bounds__(REL_THREADS)
       if (bw) atomicAdd(a.counters + 3, (unsigned long long)__popc(bw));
     }
   }
-  if (!work) return;
 
   constexpr int NB = (TYPE == 2) ? 4 : 1;  // ket operator components
   constexpr int NC = 4 * NB;               // operator components per integral
@@ -274,15 +277,19 @@ __global__ void __launch_bounds__(REL_THREADS)
   constexpr int HL = nherm(4 * LM + 2 + 2 * (TYPE == 2));
   constexpr int FL = 2 * LM + 3;
   const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb;
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  if (!work) return;
+
   const int dK = (TYPE == 2) ? 1 : 0;
   const int Lb = la + lb + 2, Lk = lc + ld + 2 * dK, L = Lb + Lk;
-  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
   const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
   const bool dAB = P.shA == P.shB, dCD = Q.shA == Q.shB, samePQ = P.lex == Q.lex;
   const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
   // the back transform adds the transpose (Hermitian completion): a
   // contribution on a pair's own diagonal block is counted twice there
   const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
+  const bool single = P.npp == 1 && Q.npp == 1;  // digest without accumulating
   const size_t nc = a.ncart;
   auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
 
@@ -295,21 +302,140 @@ __global__ void __launch_bounds__(REL_THREADS)
   int nfa[3][4], nfc[3][4];
 
 #pragma unroll 1
-  for (int c = 0; c < ncc; c++)
-#pragma unroll 1
-    for (int d = 0; d < nd; d++) {
+  for (int cd = split; cd < ncc * nd; cd += nsplit) {
+    {
+      const int c = cd / nd, d = cd % nd;
       const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
       const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+      const int gC = Q.cA + c, gD = Q.cB + d;
+      // per-column Coulomb accumulators (LLSS: J_LL(C,D); SSSS: J_SS(C,D))
+      double jcol[4] = {0.0, 0.0, 0.0, 0.0};
+      double rhoLL = 0.0;
+      double rvDC[4] = {0.0, 0.0, 0.0, 0.0};
+      if (TYPE == 1) {
+        rhoLL = __ldg(a.Xll + 2 * ix(gD, gC));
+      } else {
+        const size_t eDC = ix(gD, gC);
+        rvDC[0] = __ldg(a.Xss[0] + 2 * eDC);
+        rvDC[1] = -__ldg(a.Xss[1] + 2 * eDC + 1);
+        rvDC[2] = -__ldg(a.Xss[2] + 2 * eDC + 1);
+        rvDC[3] = -__ldg(a.Xss[3] + 2 * eDC + 1);
+      }
+      const double wx = samePQ ? 0.5 : 1.0;
+
+      // ---- digestion of one bra component pair's operator components m
+      auto digest = [&](int ai, int bi, const double* m) {
+        const int gA = P.cA + ai, gB = P.cB + bi;
+        if (TYPE == 1) {
+          // Coulomb SS(1,2) from the LL density (:1145-1190)
+          const double wj = w12 * s34d * rhoLL;
+          if (wj != 0.0)
+#pragma unroll
+            for (int op = 0; op < 4; op++) atomicAdd(a.Jss[op] + ix(gA, gB), wj * m[op]);
+          // Coulomb LL(3,4) from the SS density
+          const size_t eBA = ix(gB, gA);
+          jcol[0] += m[0] * __ldg(a.Xss[0] + 2 * eBA) - m[1] * __ldg(a.Xss[1] + 2 * eBA + 1) -
+                     m[2] * __ldg(a.Xss[2] + 2 * eBA + 1) - m[3] * __ldg(a.Xss[3] + 2 * eBA + 1);
+          if (!a.exchange) return;
+          // exchange LS: K(t1, t2) -= D(d1, d2) P (:1200-1299)
+          auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
+            const size_t e = ix(d1, d2);
+            Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+            Q4 Cq{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
+                  make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
+            const Q4 r = qmul(dq, Cq);
+            const size_t t = ix(t1, t2);
+            addz(a.K[0], t, r.s, -1.0);
+            addz(a.K[1], t, r.x, -1.0);
+            addz(a.K[2], t, r.y, -1.0);
+            addz(a.K[3], t, r.z, -1.0);
+          };
+          ls(gC, gB, gD, gA, 1.0);
+          if (!dAB) ls(gC, gA, gD, gB, -1.0);
+          if (!dCD) {
+            ls(gD, gB, gC, gA, 1.0);
+            if (!dAB) ls(gD, gA, gC, gB, -1.0);
+          }
+        } else {
+          // m[a * 4 + b]; Coulomb SS(1,2) from D(4,3), and SS(3,4) from
+          // D(2,1) when the bra and ket pairs differ (:2342-2380)
+#pragma unroll
+          for (int op = 0; op < 4; op++) {
+            const double v = m[op * 4 + 0] * rvDC[0] + m[op * 4 + 1] * rvDC[1] +
+                             m[op * 4 + 2] * rvDC[2] + m[op * 4 + 3] * rvDC[3];
+            if (v != 0.0) atomicAdd(a.Jss[op] + ix(gA, gB), w12 * s34d * v);
+          }
+          if (!samePQ) {
+            const size_t eBA = ix(gB, gA);
+            const double rvBA[4] = {__ldg(a.Xss[0] + 2 * eBA), -__ldg(a.Xss[1] + 2 * eBA + 1),
+                                    -__ldg(a.Xss[2] + 2 * eBA + 1),
+                                    -__ldg(a.Xss[3] + 2 * eBA + 1)};
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+              jcol[b] += m[0 * 4 + b] * rvBA[0] + m[1 * 4 + b] * rvBA[1] +
+                         m[2 * 4 + b] * rvBA[2] + m[3 * 4 + b] * rvBA[3];
+          }
+          if (!a.exchange) return;
+          // exchange SS: K(t1, t2) -= P_12 D(d1, d2) P_34 with the bra / ket
+          // orientation signs f1, f2 (:2381-2445); the Hermitian-conjugate
+          // images come from the completion in the back transform
+          auto ex = [&](int t1, int t2, int d1, int d2, double f1, double f2) {
+            const size_t e = ix(d1, d2);
+            const Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+            Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
 #pragma unroll 1
-      for (int k = 0; k < na * nb * NC; k++) acc[k] = 0.0;
+            for (int b = 0; b < 4; b++) {
+              // left operator sum_a c_ab sigma_a, c_ab = m_ab (i f1)^[a>0] (i f2)^[b>0]
+              double2 cs = make_double2(m[0 * 4 + b], 0.0);
+              double2 cx = make_double2(0.0, f1 * m[1 * 4 + b]);
+              double2 cy = make_double2(0.0, f1 * m[2 * 4 + b]);
+              double2 cz = make_double2(0.0, f1 * m[3 * 4 + b]);
+              if (b > 0) {
+                cs = make_double2(-f2 * cs.y, f2 * cs.x);
+                cx = make_double2(-f2 * cx.y, f2 * cx.x);
+                cy = make_double2(-f2 * cy.y, f2 * cy.x);
+                cz = make_double2(-f2 * cz.y, f2 * cz.x);
+              }
+              const Q4 Lq{cs, cx, cy, cz};
+              Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+                    make_double2(0, 0)};
+              if (b == 0) sb.s = make_double2(1, 0);
+              else if (b == 1) sb.x = make_double2(1, 0);
+              else if (b == 2) sb.y = make_double2(1, 0);
+              else sb.z = make_double2(1, 0);
+              const Q4 t = qmul(qmul(Lq, dq), sb);
+              r.s = cadd(r.s, t.s);
+              r.x = cadd(r.x, t.x);
+              r.y = cadd(r.y, t.y);
+              r.z = cadd(r.z, t.z);
+            }
+            const size_t t = ix(t1, t2);
+            addz(a.K[0], t, r.s, -wx);
+            addz(a.K[1], t, r.x, -wx);
+            addz(a.K[2], t, r.y, -wx);
+            addz(a.K[3], t, r.z, -wx);
+          };
+          ex(gA, gD, gB, gC, 1.0, 1.0);
+          if (!dCD) ex(gA, gC, gB, gD, 1.0, -1.0);
+          if (!dAB) {
+            ex(gB, gD, gA, gC, -1.0, 1.0);
+            if (!dCD) ex(gB, gC, gA, gD, -1.0, -1.0);
+          }
+        }
+      };
+
+      if (!single)
+#pragma unroll 1
+        for (int k = 0; k < nab * NC; k++) acc[k] = 0.0;
 #pragma unroll 1
       for (int ip = 0; ip < P.npp; ip++) {
         const PrimPairDev& A = a.pp[P.pp_off + ip];
         double ea, eb;
         pair_exps(SA, SB, a.prim, ip, ea, eb);
-        const double p = A.p;
 #pragma unroll 1
-        for (int x = 0; x < 3; x++) hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
+        for (int x = 0; x < 3; x++)
+          hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
+        const double p = A.p;
 #pragma unroll 1
         for (int b = 0; b < NB; b++)
 #pragma unroll 1
@@ -362,6 +488,7 @@ __global__ void __launch_bounds__(REL_THREADS)
         for (int ai = 0; ai < na; ai++)
 #pragma unroll 1
           for (int bi = 0; bi < nb; bi++) {
+            const int ab = ai * nb + bi;
             const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
             const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
 #pragma unroll 1
@@ -370,7 +497,11 @@ __global__ void __launch_bounds__(REL_THREADS)
               for (int ty = 0; ty < 4; ty++)
                 nfa[x][ty] = axis_factor(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty, 2.0 * ea,
                                          2.0 * eb, fa[x][ty]);
-            double* m = acc + (ai * nb + bi) * NC;
+            double mloc[NC];
+            double* m = single ? mloc : acc + ab * NC;
+            if (single)
+#pragma unroll
+              for (int k = 0; k < NC; k++) mloc[k] = 0.0;
 #pragma unroll 1
             for (int mu = 0; mu < 3; mu++)
 #pragma unroll 1
@@ -385,144 +516,40 @@ __global__ void __launch_bounds__(REL_THREADS)
                   m[op * NB + b] += sg * bra_dot(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty],
                                                  fa[2][tz], nfa[2][tz], G[b]);
               }
+            if (single) digest(ai, bi, mloc);
           }
       }
+      if (!single)
+#pragma unroll 1
+        for (int ab = 0; ab < nab; ab++) digest(ab / nb, ab % nb, acc + ab * NC);
 
-      // ---- digestion of ket component pair (c, d)
-      const int gC = Q.cA + c, gD = Q.cB + d;
+      // per-column Coulomb flush
       if (TYPE == 1) {
-        const double rhoLL = __ldg(a.Xll + 2 * ix(gD, gC));
-        double jll = 0.0;
-#pragma unroll 1
-        for (int ai = 0; ai < na; ai++)
-#pragma unroll 1
-          for (int bi = 0; bi < nb; bi++) {
-            const int gA = P.cA + ai, gB = P.cB + bi;
-            const double* m = acc + (ai * nb + bi) * NC;
-            // Coulomb SS(1,2) from the LL density (:1145-1190)
-            const double wj = w12 * s34d * rhoLL;
-            if (wj != 0.0)
+        if (jcol[0] != 0.0) atomicAdd(a.Jll + ix(gC, gD), w34 * s12d * jcol[0]);
+      } else if (!samePQ) {
 #pragma unroll
-              for (int op = 0; op < 4; op++) atomicAdd(a.Jss[op] + ix(gA, gB), wj * m[op]);
-            // Coulomb LL(3,4) from the SS density
-            const size_t eBA = ix(gB, gA);
-            jll += m[0] * __ldg(a.Xss[0] + 2 * eBA) - m[1] * __ldg(a.Xss[1] + 2 * eBA + 1) -
-                   m[2] * __ldg(a.Xss[2] + 2 * eBA + 1) - m[3] * __ldg(a.Xss[3] + 2 * eBA + 1);
-            if (!a.exchange) continue;
-            // exchange LS: K(t1, t2) -= D(d1, d2) P (:1200-1299)
-            auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
-              const size_t e = ix(d1, d2);
-              Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
-              Q4 C{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
-                   make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
-              const Q4 r = qmul(dq, C);
-              const size_t t = ix(t1, t2);
-              addz(a.K[0], t, r.s, -1.0);
-              addz(a.K[1], t, r.x, -1.0);
-              addz(a.K[2], t, r.y, -1.0);
-              addz(a.K[3], t, r.z, -1.0);
-            };
-            ls(gC, gB, gD, gA, 1.0);
-            if (!dAB) ls(gC, gA, gD, gB, -1.0);
-            if (!dCD) {
-              ls(gD, gB, gC, gA, 1.0);
-              if (!dAB) ls(gD, gA, gC, gB, -1.0);
-            }
-          }
-        if (jll != 0.0) atomicAdd(a.Jll + ix(gC, gD), w34 * s12d * jll);
-      } else {
-        const size_t eDC = ix(gD, gC);
-        const double rvDC[4] = {__ldg(a.Xss[0] + 2 * eDC), -__ldg(a.Xss[1] + 2 * eDC + 1),
-                                -__ldg(a.Xss[2] + 2 * eDC + 1), -__ldg(a.Xss[3] + 2 * eDC + 1)};
-        double jcd[4] = {0.0, 0.0, 0.0, 0.0};
-        const double wx = samePQ ? 0.5 : 1.0;
-#pragma unroll 1
-        for (int ai = 0; ai < na; ai++)
-#pragma unroll 1
-          for (int bi = 0; bi < nb; bi++) {
-            const int gA = P.cA + ai, gB = P.cB + bi;
-            const double* m = acc + (ai * nb + bi) * NC;  // m[a * 4 + b]
-            // Coulomb SS(1,2) from D(4,3), and SS(3,4) from D(2,1) when the
-            // bra and ket pairs differ (:2342-2380)
-#pragma unroll
-            for (int op = 0; op < 4; op++) {
-              const double v = m[op * 4 + 0] * rvDC[0] + m[op * 4 + 1] * rvDC[1] +
-                               m[op * 4 + 2] * rvDC[2] + m[op * 4 + 3] * rvDC[3];
-              if (v != 0.0) atomicAdd(a.Jss[op] + ix(gA, gB), w12 * s34d * v);
-            }
-            if (!samePQ) {
-              const size_t eBA = ix(gB, gA);
-              const double rvBA[4] = {__ldg(a.Xss[0] + 2 * eBA), -__ldg(a.Xss[1] + 2 * eBA + 1),
-                                      -__ldg(a.Xss[2] + 2 * eBA + 1),
-                                      -__ldg(a.Xss[3] + 2 * eBA + 1)};
-#pragma unroll
-              for (int b = 0; b < 4; b++)
-                jcd[b] += m[0 * 4 + b] * rvBA[0] + m[1 * 4 + b] * rvBA[1] +
-                          m[2 * 4 + b] * rvBA[2] + m[3 * 4 + b] * rvBA[3];
-            }
-            if (!a.exchange) continue;
-            // exchange SS: K(t1, t2) -= P_12 D(d1, d2) P_34 with the bra / ket
-            // orientation signs f1, f2 (:2381-2445); the Hermitian-conjugate
-            // images come from the completion in the back transform
-            auto ex = [&](int t1, int t2, int d1, int d2, double f1, double f2) {
-              const size_t e = ix(d1, d2);
-              const Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
-              Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-#pragma unroll 1
-              for (int b = 0; b < 4; b++) {
-                // left operator sum_a c_ab sigma_a, c_ab = m_ab (i f1)^[a>0] (i f2)^[b>0]
-                double2 cs = make_double2(m[0 * 4 + b], 0.0);
-                double2 cx = make_double2(0.0, f1 * m[1 * 4 + b]);
-                double2 cy = make_double2(0.0, f1 * m[2 * 4 + b]);
-                double2 cz = make_double2(0.0, f1 * m[3 * 4 + b]);
-                if (b > 0) {
-                  cs = make_double2(-f2 * cs.y, f2 * cs.x);
-                  cx = make_double2(-f2 * cx.y, f2 * cx.x);
-                  cy = make_double2(-f2 * cy.y, f2 * cy.x);
-                  cz = make_double2(-f2 * cz.y, f2 * cz.x);
-                }
-                const Q4 Lq{cs, cx, cy, cz};
-                Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
-                      make_double2(0, 0)};
-                if (b == 0) sb.s = make_double2(1, 0);
-                else if (b == 1) sb.x = make_double2(1, 0);
-                else if (b == 2) sb.y = make_double2(1, 0);
-                else sb.z = make_double2(1, 0);
-                const Q4 t = qmul(qmul(Lq, dq), sb);
-                r.s = cadd(r.s, t.s);
-                r.x = cadd(r.x, t.x);
-                r.y = cadd(r.y, t.y);
-                r.z = cadd(r.z, t.z);
-              }
-              const size_t t = ix(t1, t2);
-              addz(a.K[0], t, r.s, -wx);
-              addz(a.K[1], t, r.x, -wx);
-              addz(a.K[2], t, r.y, -wx);
-              addz(a.K[3], t, r.z, -wx);
-            };
-            ex(gA, gD, gB, gC, 1.0, 1.0);
-            if (!dCD) ex(gA, gC, gB, gD, 1.0, -1.0);
-            if (!dAB) {
-              ex(gB, gD, gA, gC, -1.0, 1.0);
-              if (!dCD) ex(gB, gC, gA, gD, -1.0, -1.0);
-            }
-          }
-        if (!samePQ)
-#pragma unroll
-          for (int b = 0; b < 4; b++)
-            if (jcd[b] != 0.0) atomicAdd(a.Jss[b] + ix(gC, gD), w34 * s12d * jcd[b]);
+        for (int b = 0; b < 4; b++)
+          if (jcol[b] != 0.0) atomicAdd(a.Jss[b] + ix(gC, gD), w34 * s12d * jcol[b]);
       }
     }
+  }
 }
 
 template <int TYPE>
 void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
   if (a.nBra == 0 || a.nKet == 0) return;
-  dim3 grid(a.nBra, (a.nKet + REL_THREADS - 1) / REL_THREADS);
+  const int tiles = (a.nKet + REL_THREADS - 1) / REL_THREADS;
+  // split each quartet's ket components over enough threads to fill the GPU
+  // (~256k threads per launch), at most one component pair per thread
+  const long long quartets = (long long)a.nBra * a.nKet;
+  const int ncd = ncart(lc) * ncart(ld);
+  int nsplit = (int)std::min<long long>(ncd, std::max<long long>(1, (1 << 18) / quartets));
+  nsplit = std::max(1, std::min(nsplit, 65535 / tiles));
+  dim3 grid(a.nBra, tiles * nsplit);
   const int lm = std::max(std::max(la, lb), std::max(lc, ld));
-  if (lm <= 1) rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
-  else if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
-  else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld);
+  if (lm <= 1) rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+  else if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+  else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
 }
 
 // ------------------------------------------------------------ 4C Schwarz
