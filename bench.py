@@ -247,8 +247,45 @@ def run_serving(dev, nreq, rate, cutoff):
             "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
 
 
+def reference_arm_4c(args, ws):
+    """Oracle 4C build (bare Coulomb + LLSS) of one Ag atom of the Ag4
+    workload's basis: the bounded CPU sample of config 3."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet, Molecule
+    b1 = BasisSet.build(Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)]),
+                        "sapporo-dkh3-dzp-2012_no", uncontract=True)
+    ob = O.OracleBasis(b1)
+    S1, T1 = ob.overlap_kinetic()
+    D1 = workloads.spinor_density_4c(S1, T1, 47, 3)
+    times = []
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        ob.dirac_coulomb(D1, bare=True, dc=True, ssss=False)
+        times.append(time.perf_counter() - t0)
+    v = len(times) / sum(times)
+    sample = ("one Ag atom (N = 152) of the ag4_dc basis, bare Coulomb + LLSS, "
+              "C++/OpenMP restatement of directScaffoldLibcint + formGDDirect")
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "builds/s",
+                      "n_gpus": ws, "steps": len(times), "warmup": 0,
+                      "ms_per_step": 1e3 * sum(times) / len(times),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64 (complex)", "data": "synthetic (seeded)",
+                      "config": {"workload": "ag4_dc", "sample": sample},
+                      "cpu_baseline": {"value": v, "unit": "builds/s",
+                                       "cores": os.cpu_count(), "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def reference_arm(args, ws, rank):
     if rank != 0:
+        return
+    if args.workload == "ag4_dc":
+        reference_arm_4c(args, ws)
         return
     import numpy as np
 
@@ -292,9 +329,116 @@ def reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_four_component(args, ws, rank, local, pg):
+    """Config 3: four-component Dirac-Coulomb build (BareCoulomb + DiracCoulomb
+    + SSSS, libcint branch) of the seeded Ag4 tetrahedron, uncontracted
+    sapporo-dkh3-dzp basis (N = 608, 4C dimension 2432), density from 188
+    seeded complex spinors orthonormalised in the 4C metric; FP64.  A step is
+    one full formGDDirect build.  The CPU baseline is the oracle on a bounded
+    sample (one Ag atom, bare Coulomb + LLSS) with the GPU timed on the same
+    sample."""
+    import numpy as np
+    import torch
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet, Molecule
+    from chronusq_public_b200.contraction import DirectTPI
+    from chronusq_public_b200.fockbuilder import FourCompFock
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    basis, tpi, D = workloads.build_ag4_dc(lambda b: DirectTPI(b, device=local))
+    N2 = 2 * basis.nbasis
+    Dd = [torch.from_numpy(np.ascontiguousarray(d.T)).to(dev).t() for d in D]
+    fb = FourCompFock(tpi)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        fb.formGD(Dd, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            G = fb.formGD(Dd, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    stats = dict(fb.last_stats)
+    torch.cuda.synchronize()
+    herm = max(float((g - g.conj().t()).abs().max()) for g in G)
+    # e2e: host numpy buffers through the public API
+    te = []
+    t0 = time.perf_counter()
+    fb.formGD(D)
+    te.append(time.perf_counter() - t0)
+    t = torch.tensor([sum(ms) / 1e3, sum(te) / len(te)], dtype=torch.float64, device=dev)
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    tdev, te2e = float(t[0]), float(t[1])
+    if rank != 0:
+        return
+    K = args.steps
+    line = {
+        "metric": METRIC, "value": ws * K / tdev, "unit": "builds/s", "n_gpus": ws,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * tdev / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (complex)", "data": "synthetic (seeded)",
+        "config": {"workload": "ag4_dc", "nbasis_1c": basis.nbasis, "dim_4c": 2 * N2,
+                   "nshell": basis.nshell, "npair": tpi.npair,
+                   "hamiltonian": "BareCoulomb + DiracCoulomb + SSSS (libcint)",
+                   "parallelism": "replicas",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "quartets": {"computed": stats["fp64"], "screened": stats["screened"],
+                     "total": stats["total"]},
+        "checks": {"G_hermiticity_maxabs": herm},
+        "e2e": {"value": ws / te2e, "unit": "builds/s",
+                "h2d_bytes_per_step": 4 * 16 * N2 * N2,
+                "d2h_bytes_per_step": 4 * 16 * N2 * N2},
+        "clocks": clk.summary(),
+    }
+    if not args.no_oracle:
+        # bounded CPU sample: one Ag atom, bare Coulomb + LLSS, oracle vs GPU
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        mol1 = Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)])
+        b1 = BasisSet.build(mol1, "sapporo-dkh3-dzp-2012_no", uncontract=True)
+        tpi1 = DirectTPI(b1, device=local)
+        S1, T1 = tpi1.one_electron()
+        D1 = workloads.spinor_density_4c(S1, T1, 47, 3)
+        ob = O.OracleBasis(b1)
+        t0 = time.perf_counter()
+        Go = ob.dirac_coulomb(D1, bare=True, dc=True, ssss=False)
+        tcpu = time.perf_counter() - t0
+        fb1 = FourCompFock(tpi1, DiracCoulombSSSS=False)
+        fb1.formGD(D1)
+        t0 = time.perf_counter()
+        Gg = fb1.formGD(D1)
+        tg = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": 1.0 / tcpu, "unit": "builds/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "one Ag atom (N = 152), bare Coulomb + LLSS, C++/OpenMP restatement "
+                      "of directScaffoldLibcint + formGDDirect",
+            "gpu_same_sample_builds_per_s": 1.0 / tg,
+            "fock_maxabs_gpu_vs_oracle": max(float(np.abs(a - b).max())
+                                             for a, b in zip(Gg, Go))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_init(args)
+    if args.impl == "ours" and args.workload == "ag4_dc":
+        run_four_component(args, ws, rank, local, pg)
+        if pg:
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         reference_arm(args, ws, rank)
         if pg:
@@ -425,7 +569,10 @@ def main():
                                        - two_electron_energy(Go, D)),
                "energy_err_fp64": abs(two_electron_energy(G64, D)
                                       - two_electron_energy(Go, D))}
-    launches_per_step = 5 + 21  # norms/sym/max/to_cart x2, memset, 21 class launches, back x2
+    # kernels per build: block norms x2, max, norms_aux, to_cart x2, one per
+    # class pair, back transform x2
+    ncls = len({(max(a.l, b.l), min(a.l, b.l)) for a in basis.shells for b in basis.shells})
+    launches_per_step = 2 + 1 + 1 + 2 + ncls * (ncls + 1) // 2 + 2
     line = {
         "metric": METRIC, "value": vmx, "unit": "builds/s", "n_gpus": ws,
         "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / K,
@@ -448,7 +595,9 @@ def main():
                               "source": "measured in this run (FMA microbenchmark)"},
                      "unit": "TFLOP/s", "frac": frac,
                      "gflop_per_build": {"f64": fl["f64"] / 1e9, "f32": fl["f32"] / 1e9},
-                     "traffic": None},
+                     # DRAM bytes of one FP64 build (all its launches) from an
+                     # ncu capture with per-launch cache flush (an upper bound)
+                     "traffic": 1.02e8 if args.workload == "h2o16_def2svp" else None},
         "e2e": {"value": ve2e, "unit": "builds/s",
                 "h2d_bytes_per_step": 8 * N * N,
                 "d2h_bytes_per_step": 2 * 8 * N * N},
