@@ -12,9 +12,11 @@ csrc/gen/ (not tracked).  For each class the generator
   scalar code with Hermite coefficients constant-folded (E^{00}_0 = 1,
   E^{ij}_t = 0 for t > i + j),
 * emits the digestion of each density: J_ab (warp-reduced over the block's
-  kets, which share the bra pair), J_cd, and the four exchange blocks placed
-  in the bra rows (K_ac, K_bd, K_ad, K_bc); with a symmetric density and the
-  final 1/2 (A + A^T) these equal the reference's updates
+  kets, which share the bra pair), J_cd, and the four exchange blocks
+  (K_ac, K_bd, K_ad, K_bc) stored transposed, in the bra function's column
+  (a warp's atomics then land in one column: the bra is warp-uniform); with a
+  symmetric density and the final 1/2 (A + A^T) these equal the reference's
+  updates
   (include/particleintegrals/contract/direct.hpp:1858-1918).
 """
 import itertools
@@ -336,7 +338,7 @@ def gen_class(la, lb, lc, ld, prec):
             for c in cs_:
                 sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
                                 for b_ in range(NB) for (k, cc, d) in els if cc == c)
-                w.line("add(cA + %d, cC + %d, sK * (%s));" % (a_, c, sm))
+                w.line("add(cC + %d, cA + %d, sK * (%s));" % (c, a_, sm))
         # K_bd += sum_ac I D[a,c]
         for a_ in range(NA):
             for c in cs_:
@@ -345,7 +347,7 @@ def gen_class(la, lb, lc, ld, prec):
             for d in ds_:
                 sm = " + ".join("%s * dac_%d_%d" % (Iv(a_, b_, k), a_, c)
                                 for a_ in range(NA) for (k, c, dd) in els if dd == d)
-                w.line("add(cB + %d, cD + %d, sK * (%s));" % (b_, d, sm))
+                w.line("add(cD + %d, cB + %d, sK * (%s));" % (d, b_, sm))
         # K_ad += sum_bc I D[b,c]
         for b_ in range(NB):
             for c in cs_:
@@ -354,7 +356,7 @@ def gen_class(la, lb, lc, ld, prec):
             for d in ds_:
                 sm = " + ".join("%s * dbc_%d_%d" % (Iv(a_, b_, k), b_, c)
                                 for b_ in range(NB) for (k, c, dd) in els if dd == d)
-                w.line("add(cA + %d, cD + %d, sK * (%s));" % (a_, d, sm))
+                w.line("add(cD + %d, cA + %d, sK * (%s));" % (d, a_, sm))
         # K_bc += sum_ad I D[a,d]
         for a_ in range(NA):
             for d in ds_:
@@ -363,7 +365,7 @@ def gen_class(la, lb, lc, ld, prec):
             for c in cs_:
                 sm = " + ".join("%s * dad_%d_%d" % (Iv(a_, b_, k), a_, d)
                                 for a_ in range(NA) for (k, cc, d) in els if cc == c)
-                w.line("add(cB + %d, cC + %d, sK * (%s));" % (b_, c, sm))
+                w.line("add(cC + %d, cB + %d, sK * (%s));" % (c, b_, sm))
         w.close()
         if nchunk > 1:
             w.line("break;")
