@@ -65,11 +65,11 @@ __device__ __forceinline__ const float* boys_rows<float>(const JKLaunch& a, int 
   return a.boys32 + (size_t)L * BOYS_NPTS * BOYS_ROW32;
 }
 
-// Persistent class kernel.  Each block stages the Boys rows of this class's
-// angular sum in shared memory once (FP64 rows, plus the FP32 rows on the
-// mixed path); then every warp independently takes work items (bra pair,
-// chunk, ket tile of 32) from a device counter until none are left -- no
-// block barriers after the staging.  On the mixed path a warp computes its
+// Persistent class kernel.  Every warp independently takes work items (bra
+// pair, chunk, ket tile of 32) from a device counter until none are left --
+// no block barriers.  The Boys rows of the class's angular sum (29 KB FP64,
+// 12 KB FP32) are read from global memory through L1: staging them in shared
+// memory capped residency at 6 blocks per SM and measured slower.  On the mixed path a warp computes its
 // quartets in FP32 when every surviving quartet's bound is below the cut
 // and in FP64 otherwise (kets are sorted by Schwarz bound, so the warps of
 // a bra row switch from FP64 to FP32 once), in one traversal.
@@ -104,21 +104,10 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
   constexpr int NA = ncart(G64::LA), NB = ncart(G64::LB);
   constexpr int NCH = G64::NCHUNK;
   constexpr int LSUM = G64::LA + G64::LB + G64::LC + G64::LD;
-  extern __shared__ float4 s_boys4[];
   const double cut = MIXED ? a.fp32_cut : 0.0;
   constexpr bool mixed = MIXED;
-  {
-    const float4* g = reinterpret_cast<const float4*>(boys_rows<double>(a, LSUM));
-    for (int i = threadIdx.x; i < BOYS_LBYTES64 / 16; i += JK_THREADS) s_boys4[i] = __ldg(g + i);
-    if (mixed) {
-      const float4* g32 = reinterpret_cast<const float4*>(boys_rows<float>(a, LSUM));
-      for (int i = threadIdx.x; i < BOYS_LBYTES32 / 16; i += JK_THREADS)
-        s_boys4[BOYS_LBYTES64 / 16 + i] = __ldg(g32 + i);
-    }
-  }
-  __syncthreads();
-  const double* boys64 = reinterpret_cast<const double*>(s_boys4);
-  const float* boys32 = reinterpret_cast<const float*>(s_boys4 + BOYS_LBYTES64 / 16);
+  const double* boys64 = boys_rows<double>(a, LSUM);
+  const float* boys32 = boys_rows<float>(a, LSUM);
   const int lane = threadIdx.x & 31;
   const int ketTiles = (a.nKet + WTILE - 1) / WTILE;
   const long long perBra = (long long)ketTiles * NCH;
@@ -259,12 +248,10 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
     constexpr int WPB = JK_THREADS / 32;
     const unsigned g = (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * 8);
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
-    const size_t smem = BOYS_LBYTES64 + (mixed ? BOYS_LBYTES32 : 0);
-    static_assert(BOYS_LBYTES64 + BOYS_LBYTES32 <= 48 * 1024, "default shared memory limit");
     if (mixed)
-      jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, smem, st>>>(b, work);
+      jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
     else
-      jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, smem, st>>>(b, work);
+      jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
     done = true;
   };
 #define CQF_TRY_CLASS(A_, B_, C_, D_, N64, N32)                                          \
