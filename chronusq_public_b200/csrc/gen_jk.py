@@ -134,76 +134,21 @@ def chunk_size(la, lb, lc, ld, prec):
     return best
 
 
-def gen_class(la, lb, lc, ld, prec):
-    """Struct GenJK<prec>_<class>: eri<T>() computes chunk ch (a contiguous
-    range of the flattened ket component index cd) of the contracted Cartesian
-    block; digest() adds that chunk's J/K contributions of one density."""
-    w = W()
-    A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
-    NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
-    NAB, NCD = NA * NB, NC * ND
-    lab, lcd = la + lb, lc + ld
-    L = lab + lcd
-    # both precisions use the FP64 chunking: one launch computes FP64 and
-    # FP32 quartets side by side with the same chunk index and digestion
-    CS = chunk_size(la, lb, lc, ld, 64)
-    nchunk = (NCD + CS - 1) // CS
-    chunks = [list(range(k * CS, min(NCD, (k + 1) * CS))) for k in range(nchunk)]
-    hab = herm_list(lab)
-    hall = herm_list(L)
-    name = "%d_%d%d%d%d" % (prec, la, lb, lc, ld)
-    w.line("// (%s%s|%s%s), FP%d build: NAB=%d NCD=%d L=%d, %d chunk(s) of <= %d cd pairs"
-           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], prec, NAB, NCD, L, nchunk, CS))
-    w.open("struct GenJK%s {" % name)
-    w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
-    w.line("static constexpr int NCHUNK = %d;" % nchunk)
-    w.line("static constexpr int NI = %d;  // integrals per chunk" % (NAB * CS))
-    # resident blocks per SM the register allocator should target: small
-    # low-L classes are latency bound and gain from occupancy
-    minb = 6 if L <= 1 else (4 if (L == 2 and NAB * CS <= 9) else 1)
-    w.line("static constexpr int MINB = %d;" % minb)
-    # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
-    w.line("template <typename T, class KA>")
-    w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
-           "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
-           "const int ch, double (&I)[%d]) {" % (NAB * CS))
-    w.line("#pragma unroll")
-    w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NAB * CS))
-    w.line("const T PI52x2 = T(34.986836655249725693);")
-    w.line("#pragma unroll 1")
-    w.open("for (int ip = 0; ip < P.npp; ip++) {")
-    w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
-    w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
-    w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
-    axes = "xyz"
-    if lab > 0:
-        for x in range(3):
-            w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
-    for k in range(CS):
-        for (t, u, v) in hab:
-            w.line("T g_%d_%d_%d_%d = T(0);" % (k, t, u, v))
-    w.line("#pragma unroll 1")
-    w.open("for (int iq = 0; iq < Q.npp; iq++) {")
-    w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
-    w.line("const T X = Px - T(kq.P(iq, 0)), Y = Py - T(kq.P(iq, 1)), Z = Pz - T(kq.P(iq, 2));")
-    w.line("const T pq = p + q;")
-    w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
-    w.line("const T alpha = p * q * (rpq * rpq);")
-    w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
-    w.line("T F[%d];" % (L + 1))
-    w.open("if constexpr (sizeof(T) == 8) {")
-    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
-    w.close("} else {")
-    w.ind += 1
-    w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
-    w.close()
-    w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
-    if lcd > 0:
-        for x in range(3):
-            w.line("const T QC%s = T(kq.PA(iq, %d)), QD%s = T(kq.PB(iq, %d));"
-                   % (axes[x], x, axes[x], x))
-    ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
-          for x in range(3)] if lcd > 0 else None
+def use_mirror(la, lb, lc, ld, nchunk):
+    """Ket-outer primitive loops (emit_eri_mirror) for single-chunk classes
+    whose live set -- integral block, bra-side Hermite accumulators
+    G'[ab][tau nu phi] and R, in 4-byte register units -- fits the budget."""
+    if nchunk != 1:
+        return False
+    nab = ncart(la) * ncart(lb)
+    ncd = ncart(lc) * ncart(ld)
+    live = 2 * nab * ncd + 2 * (nab * nherm(lc + ld) + nherm(la + lb + lc + ld))
+    return live <= 176
+
+
+def emit_R(w, L, hall):
+    """R^{(n)}_tuv recursion for total order L as straight-line code; returns
+    the name of each R^{(n)}_tuv."""
     R = {}
     w.line("const T m2a = T(-2) * alpha;")
     pw = ["T(1)"]
@@ -231,43 +176,63 @@ def gen_class(la, lb, lc, ld, prec):
                 nm = "r%d_%d_%d_%d" % (n, t, u, v)
                 w.line("const T %s = %s;" % (nm, e))
                 R[(n, t, u, v)] = nm
-    if nchunk > 1:
-        w.open("switch (ch) {")
-    for chv, cdl in enumerate(chunks):
-        if nchunk > 1:
-            w.open("case %d: {" % chv)
-        for k, cd in enumerate(cdl):
-            c, di = divmod(cd, ND)
-            cx, cy, cz = Cc[c]
-            dx, dy, dz = Dd[di]
-            wn = []
-            for ta in range(cx + dx + 1):
-                for nu in range(cy + dy + 1):
-                    for ph in range(cz + dz + 1):
-                        if lcd > 0:
-                            ex = ek[0].get(cx, dx, ta)
-                            ey = ek[1].get(cy, dy, nu)
-                            ez = ek[2].get(cz, dz, ph)
-                            if ex is None or ey is None or ez is None:
-                                continue
-                            fac = [f for f in (ex, ey, ez) if f != "1"]
-                        else:
-                            fac = []
-                        sgn = -1 if (ta + nu + ph) & 1 else 1
-                        nm = "w_%d_%d_%d_%d" % (k, ta, nu, ph)
-                        w.line("const T %s = %s%s;" % (nm, "-" if sgn < 0 else "",
-                                                        " * ".join(["pref"] + fac)))
-                        wn.append((ta, nu, ph, nm))
-            for (t, u, v) in hab:
-                sm = " + ".join("%s * %s" % (nm, R[(0, t + ta, u + nu, v + ph)])
-                                for (ta, nu, ph, nm) in wn)
-                w.line("g_%d_%d_%d_%d += %s;" % (k, t, u, v, sm))
-        if nchunk > 1:
-            w.line("break;")
-            w.close("}")
-    if nchunk > 1:
-        w.close("}")
-    w.close("}")  # iq
+    return R
+
+
+def emit_eri_mirror(w, la, lb, lc, ld, CS):
+    """eri() body with the ket primitives (per lane) in the outer loop and the
+    bra primitives (shared by the warp) in the inner one:
+        G'[ab][tnp] = sum_ip pref sum_tuv E^ab_tuv R_{t+tau,u+nu,v+phi}
+        I[ab][cd]  += sum_tnp (-1)^(tau+nu+phi) E^cd_tnp G'[ab][tnp]
+    (the same integrals as the bra-outer order; each lane loads its ket
+    primitive data and builds its ket E coefficients once per ket primitive
+    instead of once per primitive pair)."""
+    A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
+    NA, NB, ND = len(A), len(B), len(Dd)
+    NCD = len(Cc) * ND
+    lab, lcd = la + lb, lc + ld
+    L = lab + lcd
+    hcd = herm_list(lcd)
+    hall = herm_list(L)
+    axes = "xyz"
+    w.line("#pragma unroll")
+    w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NA * NB * CS))
+    w.line("const T PI52x2 = T(34.986836655249725693);")
+    w.line("#pragma unroll 1")
+    w.open("for (int iq = 0; iq < Q.npp; iq++) {")
+    w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
+    w.line("const T Qx = T(kq.P(iq, 0)), Qy = T(kq.P(iq, 1)), Qz = T(kq.P(iq, 2));")
+    if lcd > 0:
+        for x in range(3):
+            w.line("const T QC%s = T(kq.PA(iq, %d)), QD%s = T(kq.PB(iq, %d));"
+                   % (axes[x], x, axes[x], x))
+    ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
+          for x in range(3)] if lcd > 0 else None
+    for ia in range(NA):
+        for ib in range(NB):
+            for (t, u, v) in hcd:
+                w.line("T h_%d_%d_%d_%d_%d = T(0);" % (ia, ib, t, u, v))
+    w.line("#pragma unroll 1")
+    w.open("for (int ip = 0; ip < P.npp; ip++) {")
+    w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
+    w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
+    w.line("const T X = T(pa.P[0]) - Qx, Y = T(pa.P[1]) - Qy, Z = T(pa.P[2]) - Qz;")
+    if lab > 0:
+        for x in range(3):
+            w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
+    w.line("const T pq = p + q;")
+    w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
+    w.line("const T alpha = p * q * (rpq * rpq);")
+    w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
+    w.line("T F[%d];" % (L + 1))
+    w.open("if constexpr (sizeof(T) == 8) {")
+    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
+    w.close("} else {")
+    w.ind += 1
+    w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
+    w.close()
+    w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
+    R = emit_R(w, L, hall)
     eb = [E1D(w, la, lb, "ea" + axes[x], "o2p", "PA" + axes[x], "PB" + axes[x])
           for x in range(3)] if lab > 0 else None
     for ia, (ax, ay, az) in enumerate(A):
@@ -289,12 +254,201 @@ def gen_class(la, lb, lc, ld, prec):
                             names.append((t, u, v, nm))
                         else:
                             names.append((t, u, v, None))
-            for k in range(CS):
-                sm = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d" % (k, t, u, v)
+            for (tk, uk, vk) in hcd:
+                sm = " + ".join(("%s * " % nm if nm else "") + R[(0, t + tk, u + uk, v + vk)]
                                 for (t, u, v, nm) in names)
-                w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+                w.line("h_%d_%d_%d_%d_%d += pref * (%s);" % (ia, ib, tk, uk, vk, sm))
     w.close("}")  # ip
+    for k in range(NCD):
+        c, di = divmod(k, ND)
+        cx, cy, cz = Cc[c]
+        dx, dy, dz = Dd[di]
+        terms = []
+        for ta in range(cx + dx + 1):
+            for nu in range(cy + dy + 1):
+                for ph in range(cz + dz + 1):
+                    if lcd > 0:
+                        ex, ey, ez = ek[0].get(cx, dx, ta), ek[1].get(cy, dy, nu), ek[2].get(cz, dz, ph)
+                        if ex is None or ey is None or ez is None:
+                            continue
+                        fac = [f for f in (ex, ey, ez) if f != "1"]
+                    else:
+                        fac = []
+                    terms.append((ta, nu, ph, fac, (ta + nu + ph) & 1))
+        for ia in range(NA):
+            for ib in range(NB):
+                sm = " + ".join(("-" if sg else "") + " * ".join(fac + ["h_%d_%d_%d_%d_%d" % (ia, ib, ta, nu, ph)])
+                                for (ta, nu, ph, fac, sg) in terms)
+                w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+    w.close("}")  # iq
     w.close("}")  # eri
+
+
+def gen_class(la, lb, lc, ld, prec):
+    """Struct GenJK<prec>_<class>: eri<T>() computes chunk ch (a contiguous
+    range of the flattened ket component index cd) of the contracted Cartesian
+    block; digest() adds that chunk's J/K contributions of one density."""
+    w = W()
+    A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
+    NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
+    NAB, NCD = NA * NB, NC * ND
+    lab, lcd = la + lb, lc + ld
+    L = lab + lcd
+    # both precisions use the FP64 chunking: one launch computes FP64 and
+    # FP32 quartets side by side with the same chunk index and digestion
+    CS = chunk_size(la, lb, lc, ld, 64)
+    nchunk = (NCD + CS - 1) // CS
+    mirror = use_mirror(la, lb, lc, ld, nchunk)
+    chunks = [list(range(k * CS, min(NCD, (k + 1) * CS))) for k in range(nchunk)]
+    hab = herm_list(lab)
+    hall = herm_list(L)
+    name = "%d_%d%d%d%d" % (prec, la, lb, lc, ld)
+    w.line("// (%s%s|%s%s), FP%d build: NAB=%d NCD=%d L=%d, %d chunk(s) of <= %d cd pairs"
+           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], prec, NAB, NCD, L, nchunk, CS))
+    w.open("struct GenJK%s {" % name)
+    w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
+    w.line("static constexpr int NCHUNK = %d;" % nchunk)
+    w.line("static constexpr int NI = %d;  // integrals per chunk" % (NAB * CS))
+    # resident blocks per SM the register allocator should target: small
+    # low-L classes are latency bound and gain from occupancy
+    minb = 6 if L <= 1 else (4 if (L == 2 and NAB * CS <= 9) else 1)
+    w.line("static constexpr int MINB = %d;" % minb)
+    # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
+    w.line("template <typename T, class KA>")
+    w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
+           "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
+           "const int ch, double (&I)[%d]) {" % (NAB * CS))
+    if mirror:
+        emit_eri_mirror(w, la, lb, lc, ld, CS)
+    else:
+        w.line("#pragma unroll")
+        w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NAB * CS))
+        w.line("const T PI52x2 = T(34.986836655249725693);")
+        w.line("#pragma unroll 1")
+        w.open("for (int ip = 0; ip < P.npp; ip++) {")
+        w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
+        w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
+        w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
+        axes = "xyz"
+        if lab > 0:
+            for x in range(3):
+                w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
+        for k in range(CS):
+            for (t, u, v) in hab:
+                w.line("T g_%d_%d_%d_%d = T(0);" % (k, t, u, v))
+        w.line("#pragma unroll 1")
+        w.open("for (int iq = 0; iq < Q.npp; iq++) {")
+        w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
+        w.line("const T X = Px - T(kq.P(iq, 0)), Y = Py - T(kq.P(iq, 1)), Z = Pz - T(kq.P(iq, 2));")
+        w.line("const T pq = p + q;")
+        w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
+        w.line("const T alpha = p * q * (rpq * rpq);")
+        w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
+        w.line("T F[%d];" % (L + 1))
+        w.open("if constexpr (sizeof(T) == 8) {")
+        w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
+        w.close("} else {")
+        w.ind += 1
+        w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
+        w.close()
+        w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
+        if lcd > 0:
+            for x in range(3):
+                w.line("const T QC%s = T(kq.PA(iq, %d)), QD%s = T(kq.PB(iq, %d));"
+                       % (axes[x], x, axes[x], x))
+        ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
+              for x in range(3)] if lcd > 0 else None
+        R = {}
+        w.line("const T m2a = T(-2) * alpha;")
+        pw = ["T(1)"]
+        for n in range(1, L + 1):
+            w.line("const T a%d = %s;" % (n, "m2a" if n == 1 else "a%d * m2a" % (n - 1)))
+            pw.append("a%d" % n)
+        for n in range(L, -1, -1):
+            w.line("const T r%d_0_0_0 = %s;" % (n, "F[0]" if n == 0 else "%s * F[%d]" % (pw[n], n)))
+            R[(n, 0, 0, 0)] = "r%d_0_0_0" % n
+        for tot in range(1, L + 1):
+            for n in range(L - tot, -1, -1):
+                for (t, u, v) in [h for h in hall if sum(h) == tot]:
+                    if t > 0:
+                        e = "X * %s" % R[(n + 1, t - 1, u, v)]
+                        if t > 1:
+                            e += " + T(%d) * %s" % (t - 1, R[(n + 1, t - 2, u, v)])
+                    elif u > 0:
+                        e = "Y * %s" % R[(n + 1, t, u - 1, v)]
+                        if u > 1:
+                            e += " + T(%d) * %s" % (u - 1, R[(n + 1, t, u - 2, v)])
+                    else:
+                        e = "Z * %s" % R[(n + 1, t, u, v - 1)]
+                        if v > 1:
+                            e += " + T(%d) * %s" % (v - 1, R[(n + 1, t, u, v - 2)])
+                    nm = "r%d_%d_%d_%d" % (n, t, u, v)
+                    w.line("const T %s = %s;" % (nm, e))
+                    R[(n, t, u, v)] = nm
+        if nchunk > 1:
+            w.open("switch (ch) {")
+        for chv, cdl in enumerate(chunks):
+            if nchunk > 1:
+                w.open("case %d: {" % chv)
+            for k, cd in enumerate(cdl):
+                c, di = divmod(cd, ND)
+                cx, cy, cz = Cc[c]
+                dx, dy, dz = Dd[di]
+                wn = []
+                for ta in range(cx + dx + 1):
+                    for nu in range(cy + dy + 1):
+                        for ph in range(cz + dz + 1):
+                            if lcd > 0:
+                                ex = ek[0].get(cx, dx, ta)
+                                ey = ek[1].get(cy, dy, nu)
+                                ez = ek[2].get(cz, dz, ph)
+                                if ex is None or ey is None or ez is None:
+                                    continue
+                                fac = [f for f in (ex, ey, ez) if f != "1"]
+                            else:
+                                fac = []
+                            sgn = -1 if (ta + nu + ph) & 1 else 1
+                            nm = "w_%d_%d_%d_%d" % (k, ta, nu, ph)
+                            w.line("const T %s = %s%s;" % (nm, "-" if sgn < 0 else "",
+                                                            " * ".join(["pref"] + fac)))
+                            wn.append((ta, nu, ph, nm))
+                for (t, u, v) in hab:
+                    sm = " + ".join("%s * %s" % (nm, R[(0, t + ta, u + nu, v + ph)])
+                                    for (ta, nu, ph, nm) in wn)
+                    w.line("g_%d_%d_%d_%d += %s;" % (k, t, u, v, sm))
+            if nchunk > 1:
+                w.line("break;")
+                w.close("}")
+        if nchunk > 1:
+            w.close("}")
+        w.close("}")  # iq
+        eb = [E1D(w, la, lb, "ea" + axes[x], "o2p", "PA" + axes[x], "PB" + axes[x])
+              for x in range(3)] if lab > 0 else None
+        for ia, (ax, ay, az) in enumerate(A):
+            for ib, (bx, by, bz) in enumerate(B):
+                names = []
+                for t in range(ax + bx + 1):
+                    for u in range(ay + by + 1):
+                        for v in range(az + bz + 1):
+                            if lab > 0:
+                                fx, fy, fz = eb[0].get(ax, bx, t), eb[1].get(ay, by, u), eb[2].get(az, bz, v)
+                                if fx is None or fy is None or fz is None:
+                                    continue
+                                fac = [f for f in (fx, fy, fz) if f != "1"]
+                            else:
+                                fac = []
+                            if fac:
+                                nm = "v_%d_%d_%d_%d_%d" % (ia, ib, t, u, v)
+                                w.line("const T %s = %s;" % (nm, " * ".join(fac)))
+                                names.append((t, u, v, nm))
+                            else:
+                                names.append((t, u, v, None))
+                for k in range(CS):
+                    sm = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d" % (k, t, u, v)
+                                    for (t, u, v, nm) in names)
+                    w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+        w.close("}")  # ip
+        w.close("}")  # eri
     # ---- digestion
     w.line("// J/K contributions of chunk ch for one density (symmetric X)")
     w.open("static __device__ __forceinline__ void digest(const double (&I)[%d], const int ch, "
