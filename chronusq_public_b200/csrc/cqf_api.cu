@@ -465,7 +465,8 @@ void free_basis(cqf_basis* B) {
   if (B->stream) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
-                    (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_schwarz,
+                    (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_braPerm,
+                    (void*)B->d_groups, (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
                     (void*)B->d_cart2shell, (void*)B->d_ws, (void*)B->d_counters,
                     (void*)B->d_flags, (void*)B->d_qLL, (void*)B->d_qSS, (void*)B->d_relws})
@@ -731,6 +732,45 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     kt.push_back(0.0);
     CQF_TRY(upload(&B->d_ketT, kt, B->stream));
     CQF_TRY(upload(&B->d_tileOff, toff, B->stream));
+    // bra groups: per class, pairs ordered by first shell (stable: Schwarz
+    // order inside a shell), runs of one shell cut into groups of at most
+    // BRA_GROUP_MAX
+    std::vector<int> perm(std::max(1, B->npair));
+    std::vector<int2> grp;
+    for (int c = 0; c < NCLS; c++) {
+      const int beg = B->cls_beg[c], cnt = B->cls_cnt[c];
+      std::vector<int> ord(cnt);
+      for (int i = 0; i < cnt; i++) ord[i] = i;
+      std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+        return B->h_pairs[beg + x].shA < B->h_pairs[beg + y].shA;
+      });
+      for (int i = 0; i < cnt; i++) perm[beg + i] = ord[i];
+      B->cls_group_beg[c] = (int)grp.size();
+      // a group's primitive pairs are capped (one warp runs its members in
+      // sequence: heavily contracted pairs stay alone), and the groups are
+      // queued heaviest first so the work counter hands them out early
+      std::vector<std::pair<int, int2>> cg;
+      for (int i = 0; i < cnt;) {
+        int j = i, work = 0;
+        const int sh = B->h_pairs[beg + ord[i]].shA;
+        while (j < cnt && j - i < BRA_GROUP_MAX && B->h_pairs[beg + ord[j]].shA == sh &&
+               (j == i || work + B->h_pairs[beg + ord[j]].npp <= BRA_GROUP_NPP)) {
+          work += B->h_pairs[beg + ord[j]].npp;
+          j++;
+        }
+        cg.push_back({work, make_int2(i, j - i)});
+        i = j;
+      }
+      std::stable_sort(cg.begin(), cg.end(),
+                       [](const std::pair<int, int2>& x, const std::pair<int, int2>& y) {
+                         return x.first > y.first;
+                       });
+      for (auto& e : cg) grp.push_back(e.second);
+      B->cls_group_cnt[c] = (int)grp.size() - B->cls_group_beg[c];
+    }
+    if (grp.empty()) grp.push_back(make_int2(0, 0));
+    CQF_TRY(upload(&B->d_braPerm, perm, B->stream));
+    CQF_TRY(upload(&B->d_groups, grp, B->stream));
   }
   B->h_schwarz.resize((size_t)nshell * nshell);
   CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
@@ -973,6 +1013,15 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.counters = B->d_counters;
   a.ketT = B->d_ketT;
   a.tileOff = B->d_tileOff;
+  a.braPerm = B->d_braPerm;
+  a.groups = B->d_groups;
+  // one J and one K matrix: the grouped kernels sum their per-lane J_cd,
+  // K_ac, K_ad over a bra group before flushing
+  a.jmat = a.kmat = -1;
+  if (nMat == 2 && list[0].type != list[1].type) {
+    a.jmat = list[0].type == CQF_COULOMB ? 0 : 1;
+    a.kmat = 1 - a.jmat;
+  }
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;
   for (int m = 0; m < nMat; m++) fastOK = fastOK && list[m].hermitian;
@@ -989,6 +1038,10 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.same = (cb == ck);
       a.braTileBeg = B->cls_tile_beg[cb];
       a.ketTileBeg = B->cls_tile_beg[ck];
+      a.braGroupBeg = B->cls_group_beg[cb];
+      a.braNGroups = B->cls_group_cnt[cb];
+      a.ketGroupBeg = B->cls_group_beg[ck];
+      a.ketNGroups = B->cls_group_cnt[ck];
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
       unsigned int* w = work + 2 * (cb * NCLS + ck);
       if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, st)))

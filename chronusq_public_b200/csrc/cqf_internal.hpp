@@ -27,6 +27,8 @@ constexpr int MAXMAT = 512;
 // of KETT_TILE consecutive kets of a class (one persistent-kernel ket tile).
 constexpr int KETT_NF = 12;
 constexpr int KETT_TILE = 128;
+constexpr int BRA_GROUP_MAX = 8;  // bra pairs per group (same first shell)
+constexpr int BRA_GROUP_NPP = 32; // primitive pairs per group (a single pair may exceed)
 
 // Arguments of one class-quartet J/K launch.
 struct JKLaunch {
@@ -53,6 +55,13 @@ struct JKLaunch {
   const double* ketT;
   const long long* tileOff;
   int braTileBeg, ketTileBeg;
+  // bra groups (grouped light classes): bra pairs of a class reordered so
+  // that pairs with the same first shell are adjacent (braPerm: position in
+  // the class list), cut into groups {first index into braPerm, count}
+  const int* braPerm;
+  const int2* groups;
+  int braGroupBeg, braNGroups, ketGroupBeg, ketNGroups;
+  int jmat, kmat;           // the J and the K matrix when nMat == 2 (else -1)
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
@@ -102,6 +111,7 @@ struct cqf_basis {
   std::vector<cqf::PairDev> h_pairs;     // final (class, Q-sorted) order
   int cls_beg[cqf::NCLS] = {0}, cls_cnt[cqf::NCLS] = {0};
   int cls_tile_beg[cqf::NCLS] = {0};    // first ket tile of each class
+  int cls_group_beg[cqf::NCLS] = {0}, cls_group_cnt[cqf::NCLS] = {0};
   std::vector<double> h_schwarz;         // nshell^2
   // device-resident basis data
   cqf::ShellDev* d_shells = nullptr;
@@ -110,6 +120,8 @@ struct cqf_basis {
   cqf::PrimPairDev* d_pp = nullptr;
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
+  int* d_braPerm = nullptr;              // npair: class-relative bra order
+  int2* d_groups = nullptr;              // bra groups of all classes
   double* d_boys64 = nullptr;
   float* d_boys32 = nullptr;
   double* d_schwarz = nullptr;

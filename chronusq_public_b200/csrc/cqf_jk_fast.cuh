@@ -225,6 +225,177 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
   }
 }
 
+// Grouped variant for the light single-chunk classes (G64::GROUPED): a work
+// item is (bra group, ket tile of 32); the group's bra pairs share their
+// first shell A, so each lane's updates J_cd, K_ac and K_ad (targets fixed by
+// its ket pair and by A) are summed in registers over the whole group and
+// flushed once -- fewer atomics than one flush per quartet.  With other than
+// one J and one K matrix the sums are flushed after every quartet and matrix.
+// Quartet set, screens, roles, degeneracy and precision choice are those of
+// jk_fast_kernel.
+template <class G64, class G32, bool MIXED>
+__global__ void __launch_bounds__(JK_THREADS, G64::MINB)
+    jk_group_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
+  static_assert(G64::NCHUNK == 1 && G32::NCHUNK == 1, "single-chunk classes");
+  constexpr int NA = ncart(G64::LA), NB = ncart(G64::LB);
+  constexpr int NC = ncart(G64::LC), ND = ncart(G64::LD);
+  constexpr int LSUM = G64::LA + G64::LB + G64::LC + G64::LD;
+  const double cut = MIXED ? a.fp32_cut : 0.0;
+  const double* boys64 = boys_rows<double>(a, LSUM);
+  const float* boys32 = boys_rows<float>(a, LSUM);
+  const int lane = threadIdx.x & 31;
+  const int ketTiles = (a.nKet + WTILE - 1) / WTILE;
+  const long long total = (long long)a.braNGroups * ketTiles;
+  const size_t nc = a.ncart;
+  const size_t matStride = (size_t)a.ncart * a.ncart;
+  const bool grouped = a.jmat >= 0;
+  unsigned long long cVis = 0, cScr = 0, c32 = 0, c64 = 0;
+
+  for (;;) {
+    unsigned int itemU = 0;
+    if (lane == 0) itemU = atomicAdd(work, 1u);
+    const long long item = (long long)__shfl_sync(0xffffffffu, itemU, 0);
+    if (item >= total) break;
+    const int g = (int)(item / ketTiles), tile = (int)(item % ketTiles);
+    const int2 gr = __ldg(a.groups + a.braGroupBeg + g);
+    const int jk = tile * WTILE + lane;
+    const bool qvalid = jk < a.nKet;
+    PairDev Q;
+    if (qvalid) Q = a.pairs[a.ketBeg + jk];
+    const double tileQ = a.pairs[a.ketBeg + tile * WTILE].Q;
+    double jcd[G64::NJCD], kac[G64::NKAC], kad[G64::NKAD];
+#pragma unroll
+    for (int i = 0; i < G64::NJCD; i++) jcd[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < G64::NKAC; i++) kac[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < G64::NKAD; i++) kad[i] = 0.0;
+    int cAgrp = 0;
+    bool any = false;
+
+#pragma unroll 1
+    for (int mm = 0; mm < gr.y; mm++) {
+      const int ib = __ldg(a.braPerm + a.braBeg + gr.x + mm);  // position in the class
+      if (a.same && tile * WTILE > ib) continue;  // warp-uniform
+      const PairDev P = a.pairs[a.braBeg + ib];
+      const bool visited = qvalid && !(a.same && jk > ib);
+      if (a.screen && __ldg(a.maxNorm) * P.Q * tileQ < a.thresh) {
+        const unsigned bv = __ballot_sync(0xffffffffu, visited);
+        cVis += __popc(bv);
+        cScr += __popc(bv);
+        continue;
+      }
+      bool screened = false, w64 = false, w32 = false;
+      int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+      if (visited) {
+        const bool pRef = P.lex >= Q.lex;
+        const PairDev& R12 = pRef ? P : Q;
+        const PairDev& R34 = pRef ? Q : P;
+        s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
+        double bound = 1e300;
+        if (a.screen) {
+          bound = sh_max_bra(a, P, Q, __ldg(a.pairNorm + a.braBeg + ib),
+                             __ldg(a.pairNorm + a.ketBeg + jk), pRef) * P.Q * Q.Q;
+          screened = bound < a.thresh;
+        }
+        w64 = !screened;
+        w32 = w64 && MIXED && bound < cut;
+      }
+      if (__any_sync(0xffffffffu, w64 && !w32)) w32 = false;
+      else w64 = w64 && !w32;
+      const unsigned b64 = __ballot_sync(0xffffffffu, w64);
+      const unsigned b32 = __ballot_sync(0xffffffffu, w32);
+      cVis += __popc(__ballot_sync(0xffffffffu, visited));
+      cScr += __popc(__ballot_sync(0xffffffffu, screened));
+      c64 += __popc(b64);
+      c32 += __popc(b32);
+      if (!(b64 | b32)) continue;
+      const bool work_ = w64 || w32;
+      cAgrp = P.cA;
+      any = any || work_;
+      const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
+                         ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
+      const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
+      double I[G64::NI];
+      if (w64) {
+        const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
+        G64::template eri<double>(P, Q, a.pp, kq, boys64, 0, I);
+      } else if (MIXED && w32) {
+        const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
+        G32::template eri<float>(P, Q, a.pp, kq, boys32, 0, I);
+      } else {
+#pragma unroll
+        for (int i = 0; i < G64::NI; i++) I[i] = 0.0;
+      }
+#pragma unroll 1
+      for (int m = 0; m < a.nMat; m++) {
+        const int fl = __ldg(a.flags + m);
+        const bool doJ = !(fl & 2), doK = (fl & 2);
+        double jab[NA * NB];
+#pragma unroll
+        for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
+        const double* X = a.Xc + m * matStride;
+        double* A = a.Ac + m * matStride;
+        G64::digest_g(I, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
+                      jab, jcd, kac, kad);
+        if (!grouped && work_) {  // flush this matrix's sums now
+#pragma unroll
+          for (int k = 0; k < G64::NJCD; k++) {
+            if (jcd[k] != 0.0)
+              atomicAdd(A + (size_t)(Q.cA + k / ND) + (size_t)(Q.cB + k % ND) * nc, jcd[k]);
+            jcd[k] = 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < G64::NKAC; k++) {
+            if (kac[k] != 0.0)
+              atomicAdd(A + (size_t)(Q.cA + k % NC) + (size_t)(P.cA + k / NC) * nc, kac[k]);
+            kac[k] = 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < G64::NKAD; k++) {
+            if (kad[k] != 0.0)
+              atomicAdd(A + (size_t)(Q.cB + k % ND) + (size_t)(P.cA + k / ND) * nc, kad[k]);
+            kad[k] = 0.0;
+          }
+        }
+        if (doJ) {
+#pragma unroll
+          for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
+          warp_sum(jab);
+          if (lane == 0) {
+#pragma unroll
+            for (int i = 0; i < NA * NB; i++)
+              if (jab[i] != 0.0)
+                atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
+          }
+        }
+      }
+    }
+    if (grouped && any) {
+      double* AJ = a.Ac + a.jmat * matStride;
+      double* AK = a.Ac + a.kmat * matStride;
+#pragma unroll
+      for (int k = 0; k < G64::NJCD; k++)
+        if (jcd[k] != 0.0)
+          atomicAdd(AJ + (size_t)(Q.cA + k / ND) + (size_t)(Q.cB + k % ND) * nc, jcd[k]);
+#pragma unroll
+      for (int k = 0; k < G64::NKAC; k++)
+        if (kac[k] != 0.0)
+          atomicAdd(AK + (size_t)(Q.cA + k % NC) + (size_t)(cAgrp + k / NC) * nc, kac[k]);
+#pragma unroll
+      for (int k = 0; k < G64::NKAD; k++)
+        if (kad[k] != 0.0)
+          atomicAdd(AK + (size_t)(Q.cB + k % ND) + (size_t)(cAgrp + k / ND) * nc, kad[k]);
+    }
+  }
+  if (lane == 0) {
+    if (cVis) atomicAdd(a.counters + 0, cVis);
+    if (cScr) atomicAdd(a.counters + 1, cScr);
+    if (c32) atomicAdd(a.counters + 2, c32);
+    if (c64) atomicAdd(a.counters + 3, c64);
+  }
+}
+
 // Launches the generated kernels of the class (la lb | lc ld) (either
 // orientation); returns false when the class has no generated kernel.
 // work: two zeroed device counters for this class (FP64, FP32 launch).
@@ -240,18 +411,28 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
       b.braBeg = a.ketBeg; b.nBra = a.nKet;
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
       b.braTileBeg = a.ketTileBeg; b.ketTileBeg = a.braTileBeg;
+      b.braGroupBeg = a.ketGroupBeg; b.braNGroups = a.ketNGroups;
+      b.ketGroupBeg = a.braGroupBeg; b.ketNGroups = a.braNGroups;
     }
     const long long tiles = (long long)((b.nKet + WTILE - 1) / WTILE);
-    const long long items = (long long)b.nBra * tiles * G64::NCHUNK;
+    const long long items = G64::GROUPED ? (long long)b.braNGroups * tiles
+                                         : (long long)b.nBra * tiles * G64::NCHUNK;
     // persistent blocks: enough for full residency on every SM (extra blocks
     // queue and find the counter exhausted); one work item per warp at a time
     constexpr int WPB = JK_THREADS / 32;
     const unsigned g = (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * 8);
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
-    if (mixed)
-      jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
-    else
-      jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+    if constexpr (G64::GROUPED) {
+      if (mixed)
+        jk_group_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
+      else
+        jk_group_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+    } else {
+      if (mixed)
+        jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
+      else
+        jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+    }
     done = true;
   };
 #define CQF_TRY_CLASS(A_, B_, C_, D_, N64, N32)                                          \

@@ -284,6 +284,79 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS):
     w.close("}")  # eri
 
 
+def emit_digest_g(w, A, B, Cc, Dd):
+    """digest_g(): the digestion of a single-chunk class with the updates
+    whose target is fixed by the ket and the bra's first shell -- J_cd, K_ac,
+    K_ad -- added into per-lane arrays (jcd, kac, kad), which the grouped
+    kernel sums over all bra pairs of a group that share that shell before
+    one flush; J_ab into jab (warp-reduced by the caller); K_bd, K_bc with
+    atomics as in digest()."""
+    NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
+    NAB, NCD = NA * NB, NC * ND
+    w.line("static constexpr int NJCD = %d, NKAC = %d, NKAD = %d;" % (NCD, NA * NC, NA * ND))
+    w.open("static __device__ __forceinline__ void digest_g(const double (&I)[%d], "
+           "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
+           "int cC, int cD, double sJ, double sK, bool doJ, bool doK, double (&jab)[%d], "
+           "double (&jcd)[%d], double (&kac)[%d], double (&kad)[%d]) {"
+           % (NAB * NCD, NAB, NCD, NA * NC, NA * ND))
+    w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
+    w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
+    els = [(k,) + divmod(k, ND) for k in range(NCD)]  # (k, c, d)
+
+    def Iv(a, b, k):
+        return "I[%d]" % ((a * NB + b) * NCD + k)
+    w.open("if (doJ) {")
+    for (k, c, d) in els:
+        w.line("const double dcd_%d = ld(cD + %d, cC + %d);" % (k, d, c))
+    for a_ in range(NA):
+        for b_ in range(NB):
+            sm = " + ".join("%s * dcd_%d" % (Iv(a_, b_, k), k) for (k, c, d) in els)
+            w.line("jab[%d] += %s;" % (a_ * NB + b_, sm))
+    for a_ in range(NA):
+        for b_ in range(NB):
+            w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a_, b_, a_, b_))
+    for (k, c, d) in els:
+        sm = " + ".join("%s * dab_%d_%d" % (Iv(a_, b_, k), a_, b_)
+                        for a_ in range(NA) for b_ in range(NB))
+        w.line("jcd[%d] += sJ * (%s);" % (k, sm))
+    w.close()
+    w.open("if (doK) {")
+    for b_ in range(NB):
+        for d in range(ND):
+            w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b_, d, b_))
+    for a_ in range(NA):
+        for c in range(NC):
+            sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
+                            for b_ in range(NB) for (k, cc, d) in els if cc == c)
+            w.line("kac[%d] += sK * (%s);" % (a_ * NC + c, sm))
+    for a_ in range(NA):
+        for c in range(NC):
+            w.line("const double dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
+    for b_ in range(NB):
+        for d in range(ND):
+            sm = " + ".join("%s * dac_%d_%d" % (Iv(a_, b_, k), a_, c)
+                            for a_ in range(NA) for (k, c, dd) in els if dd == d)
+            w.line("add(cD + %d, cB + %d, sK * (%s));" % (d, b_, sm))
+    for b_ in range(NB):
+        for c in range(NC):
+            w.line("const double dbc_%d_%d = ld(cB + %d, cC + %d);" % (b_, c, b_, c))
+    for a_ in range(NA):
+        for d in range(ND):
+            sm = " + ".join("%s * dbc_%d_%d" % (Iv(a_, b_, k), b_, c)
+                            for b_ in range(NB) for (k, c, dd) in els if dd == d)
+            w.line("kad[%d] += sK * (%s);" % (a_ * ND + d, sm))
+    for a_ in range(NA):
+        for d in range(ND):
+            w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a_, d, a_, d))
+    for b_ in range(NB):
+        for c in range(NC):
+            sm = " + ".join("%s * dad_%d_%d" % (Iv(a_, b_, k), a_, d)
+                            for a_ in range(NA) for (k, cc, d) in els if cc == c)
+            w.line("add(cC + %d, cB + %d, sK * (%s));" % (c, b_, sm))
+    w.close()
+    w.close("}")  # digest_g
+
+
 def gen_class(la, lb, lc, ld, prec):
     """Struct GenJK<prec>_<class>: eri<T>() computes chunk ch (a contiguous
     range of the flattened ket component index cd) of the contracted Cartesian
@@ -527,6 +600,13 @@ def gen_class(la, lb, lc, ld, prec):
     if nchunk > 1:
         w.close("}")
     w.close("}")  # digest
+    # bra groups for the light classes whose bra starts with an s shell: their
+    # per-lane sums (J_cd, K_ac, K_ad) stay small; for p/d first shells the
+    # extra registers spill and measured slower
+    grouped = mirror and la == 0
+    w.line("static constexpr bool GROUPED = %s;" % ("true" if grouped else "false"))
+    if grouped:
+        emit_digest_g(w, A, B, Cc, Dd)
     w.close("};")
     return "\n".join(w.lines), name
 
