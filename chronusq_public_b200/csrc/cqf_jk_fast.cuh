@@ -229,8 +229,9 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
 // item is (bra group, ket tile of 32); the group's bra pairs share their
 // first shell A, so each lane's updates J_cd, K_ac and K_ad (targets fixed by
 // its ket pair and by A) are summed in registers over the whole group and
-// flushed once -- fewer atomics than one flush per quartet.  With other than
-// one J and one K matrix the sums are flushed after every quartet and matrix.
+// flushed once -- fewer atomics than one flush per quartet.  Launched when
+// the call has one J and one K matrix (else jk_fast_kernel runs; the
+// per-matrix flush below keeps the kernel correct for any matrix list).
 // Quartet set, screens, roles, degeneracy and precision choice are those of
 // jk_fast_kernel.
 template <class G64, class G32, bool MIXED>
@@ -415,18 +416,28 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
       b.ketGroupBeg = a.braGroupBeg; b.ketNGroups = a.braNGroups;
     }
     const long long tiles = (long long)((b.nKet + WTILE - 1) / WTILE);
-    const long long items = G64::GROUPED ? (long long)b.braNGroups * tiles
-                                         : (long long)b.nBra * tiles * G64::NCHUNK;
+    // bra groups pay off when one J and one K matrix share the sums;
+    // many-density launches use the per-quartet kernel
+    const bool useGroups = G64::GROUPED && b.jmat >= 0;
+    const long long items = useGroups ? (long long)b.braNGroups * tiles
+                                      : (long long)b.nBra * tiles * G64::NCHUNK;
     // persistent blocks: enough for full residency on every SM (extra blocks
     // queue and find the counter exhausted); one work item per warp at a time
     constexpr int WPB = JK_THREADS / 32;
     const unsigned g = (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * 8);
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
     if constexpr (G64::GROUPED) {
-      if (mixed)
-        jk_group_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
-      else
-        jk_group_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+      if (useGroups) {
+        if (mixed)
+          jk_group_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
+        else
+          jk_group_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+      } else {
+        if (mixed)
+          jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
+        else
+          jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+      }
     } else {
       if (mixed)
         jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
