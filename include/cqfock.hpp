@@ -8,6 +8,8 @@
 //       include/particleintegrals/twopints/gtodirecttpi.hpp:30-141
 //   GTODirectTPIContraction<MatsT>::twoBodyContract(screen, list)
 //       include/particleintegrals/twopints/gtodirecttpi.hpp:199-206
+//   GTODirectRelERIContraction / FourCompFock (the four-component build)
+//       gtodirectreleri.hpp:75-94, fockbuilder/fourcompfock/impl.hpp:3752-4636
 // Errors become std::runtime_error, as ChronusQ's CErr does (include/cerr.hpp).
 #pragma once
 
@@ -22,7 +24,18 @@
 
 namespace cqfock {
 
-enum TWOBODY_CONTRACTION_TYPE { COULOMB = CQF_COULOMB, EXCHANGE = CQF_EXCHANGE };
+// include/particleintegrals/twopints.hpp:31-41 (same order and values)
+enum TWOBODY_CONTRACTION_TYPE {
+  COULOMB = CQF_COULOMB,
+  EXCHANGE = CQF_EXCHANGE,
+  PAIR,
+  BARE_COULOMB,
+  LLLL,
+  LLSS,
+  SSSS,
+  GAUNT,
+  GAUGE
+};
 
 template <typename T>
 struct TwoBodyContraction {
@@ -119,6 +132,80 @@ class GTODirectTPIContraction {
 
  private:
   std::shared_ptr<DirectTPI> tpi_;
+};
+
+// GTODirectRelERIContraction<dcomplex,double>::twoBodyContract
+// (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94): 17 entries
+// in DIRAC_PAULI_SPINOR_COMP order, contType of entry 0 = BARE_COULOMB, LLSS
+// or SSSS; every AX is overwritten (zeroed, then the contraction).
+class GTODirectRelERIContraction {
+ public:
+  explicit GTODirectRelERIContraction(std::shared_ptr<DirectTPI> tpi) : tpi_(std::move(tpi)) {}
+
+  void twoBodyContract(const bool screen,
+                       std::vector<TwoBodyContraction<std::complex<double>>>& list,
+                       const bool computeExchange = true, cqf_stats* stats = nullptr) const {
+    if (list.size() != CQF_REL_NMAT)
+      throw std::runtime_error("GTODirectRelERIContraction: the 4C list has 17 entries");
+    int type;
+    switch (list[0].contType) {
+      case BARE_COULOMB: type = CQF_REL_BARE_COULOMB; break;
+      case LLSS: type = CQF_REL_LLSS; break;
+      case SSSS: type = CQF_REL_SSSS; break;
+      default: throw std::runtime_error("GTODirectRelERIContraction: unsupported contraction type");
+    }
+    const void* X[CQF_REL_NMAT];
+    void* AX[CQF_REL_NMAT];
+    for (int m = 0; m < CQF_REL_NMAT; m++) {
+      X[m] = list[m].X;
+      AX[m] = list[m].AX;
+    }
+    cqf_opts o;
+    cqf_opts_default(&o);
+    o.is_complex = 1;
+    o.screen = screen ? 1 : 0;
+    check(cqf_rel_two_body_contract(tpi_->handle(), X, AX, type, computeExchange ? 1 : 0, &o,
+                                    stats),
+          "cqf_rel_two_body_contract");
+  }
+
+ private:
+  std::shared_ptr<DirectTPI> tpi_;
+};
+
+// FourCompFock<dcomplex,double>::formGDDirect
+// (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) with the
+// HamiltonianOptions switches BareCoulomb, DiracCoulomb, DiracCoulombSSSS and
+// Libcint.  D and G: the four Pauli components (scalar, MX, MY, MZ) of the
+// 2N x 2N complex 4C matrices, column-major, LL block first.
+class FourCompFock {
+ public:
+  explicit FourCompFock(std::shared_ptr<DirectTPI> tpi, bool BareCoulomb = true,
+                        bool DiracCoulomb = true, bool DiracCoulombSSSS = true,
+                        bool Libcint = true)
+      : tpi_(std::move(tpi)) {
+    cqf_dc_opts_default(&dc_);
+    dc_.bare_coulomb = BareCoulomb;
+    dc_.dirac_coulomb = DiracCoulomb;
+    dc_.dirac_coulomb_ssss = DiracCoulombSSSS;
+    dc_.libcint = Libcint;
+  }
+
+  void formGD(const std::complex<double>* const D[4], std::complex<double>* const G[4],
+              double xHFX = 1.0, cqf_stats* stats = nullptr) const {
+    cqf_dc_opts dc = dc_;
+    dc.xHFX = xHFX;
+    const void* d[4] = {D[0], D[1], D[2], D[3]};
+    void* g[4] = {G[0], G[1], G[2], G[3]};
+    cqf_opts o;
+    cqf_opts_default(&o);
+    o.is_complex = 1;
+    check(cqf_four_comp_gd(tpi_->handle(), d, g, &dc, &o, stats), "cqf_four_comp_gd");
+  }
+
+ private:
+  std::shared_ptr<DirectTPI> tpi_;
+  cqf_dc_opts dc_;
 };
 
 }  // namespace cqfock
