@@ -223,6 +223,126 @@ struct RelLaunch {
 
 constexpr int REL_THREADS = 64;
 
+// Digestion of the operator components m of one bra component pair (a, b)
+// against ket component pair (c, d) = (gC, gD) (Cartesian AO indices): the
+// update formulas of the reference with the Pauli algebra of P.  jcol gets
+// the caller's per-column Coulomb sum (J_LL(C,D) for LLSS, J_SS(C,D) for SSSS).
+struct RelCol {
+  int gC, gD;
+  bool dAB, dCD, samePQ;
+  double s34d, w12, wx;
+  double rhoLL;    // LLSS: Re X_CLL(D, C)
+  double rvDC[4];  // SSSS: (Re S, -Im X, -Im Y, -Im Z) of X_CSS(D, C)
+};
+
+template <int TYPE>
+__device__ __forceinline__ void rel_digest(const RelLaunch& a, const PairDev& P, const RelCol& col,
+                                           int ai, int bi, const double* m, double* jcol) {
+  const size_t nc = a.ncart;
+  auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
+  const int gC = col.gC, gD = col.gD;
+  const bool dAB = col.dAB, dCD = col.dCD, samePQ = col.samePQ;
+  const double s34d = col.s34d, w12 = col.w12, wx = col.wx, rhoLL = col.rhoLL;
+  const double* rvDC = col.rvDC;
+  const int gA = P.cA + ai, gB = P.cB + bi;
+  if (TYPE == 1) {
+    // Coulomb SS(1,2) from the LL density (:1145-1190)
+    const double wj = w12 * s34d * rhoLL;
+    if (wj != 0.0)
+#pragma unroll
+      for (int op = 0; op < 4; op++) atomicAdd(a.Jss[op] + ix(gA, gB), wj * m[op]);
+    // Coulomb LL(3,4) from the SS density
+    const size_t eBA = ix(gB, gA);
+    jcol[0] += m[0] * __ldg(a.Xss[0] + 2 * eBA) - m[1] * __ldg(a.Xss[1] + 2 * eBA + 1) -
+               m[2] * __ldg(a.Xss[2] + 2 * eBA + 1) - m[3] * __ldg(a.Xss[3] + 2 * eBA + 1);
+    if (!a.exchange) return;
+    // exchange LS: K(t1, t2) -= D(d1, d2) P (:1200-1299)
+    auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
+      const size_t e = ix(d1, d2);
+      Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+      Q4 Cq{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
+            make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
+      const Q4 r = qmul(dq, Cq);
+      const size_t t = ix(t1, t2);
+      addz(a.K[0], t, r.s, -1.0);
+      addz(a.K[1], t, r.x, -1.0);
+      addz(a.K[2], t, r.y, -1.0);
+      addz(a.K[3], t, r.z, -1.0);
+    };
+    ls(gC, gB, gD, gA, 1.0);
+    if (!dAB) ls(gC, gA, gD, gB, -1.0);
+    if (!dCD) {
+      ls(gD, gB, gC, gA, 1.0);
+      if (!dAB) ls(gD, gA, gC, gB, -1.0);
+    }
+  } else {
+    // m[a * 4 + b]; Coulomb SS(1,2) from D(4,3), and SS(3,4) from
+    // D(2,1) when the bra and ket pairs differ (:2342-2380)
+#pragma unroll
+    for (int op = 0; op < 4; op++) {
+      const double v = m[op * 4 + 0] * rvDC[0] + m[op * 4 + 1] * rvDC[1] +
+                       m[op * 4 + 2] * rvDC[2] + m[op * 4 + 3] * rvDC[3];
+      if (v != 0.0) atomicAdd(a.Jss[op] + ix(gA, gB), w12 * s34d * v);
+    }
+    if (!samePQ) {
+      const size_t eBA = ix(gB, gA);
+      const double rvBA[4] = {__ldg(a.Xss[0] + 2 * eBA), -__ldg(a.Xss[1] + 2 * eBA + 1),
+                              -__ldg(a.Xss[2] + 2 * eBA + 1),
+                              -__ldg(a.Xss[3] + 2 * eBA + 1)};
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+        jcol[b] += m[0 * 4 + b] * rvBA[0] + m[1 * 4 + b] * rvBA[1] +
+                   m[2 * 4 + b] * rvBA[2] + m[3 * 4 + b] * rvBA[3];
+    }
+    if (!a.exchange) return;
+    // exchange SS: K(t1, t2) -= P_12 D(d1, d2) P_34 with the bra / ket
+    // orientation signs f1, f2 (:2381-2445); the Hermitian-conjugate
+    // images come from the completion in the back transform
+    auto ex = [&](int t1, int t2, int d1, int d2, double f1, double f2) {
+      const size_t e = ix(d1, d2);
+      const Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
+      Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+#pragma unroll 1
+      for (int b = 0; b < 4; b++) {
+        // left operator sum_a c_ab sigma_a, c_ab = m_ab (i f1)^[a>0] (i f2)^[b>0]
+        double2 cs = make_double2(m[0 * 4 + b], 0.0);
+        double2 cx = make_double2(0.0, f1 * m[1 * 4 + b]);
+        double2 cy = make_double2(0.0, f1 * m[2 * 4 + b]);
+        double2 cz = make_double2(0.0, f1 * m[3 * 4 + b]);
+        if (b > 0) {
+          cs = make_double2(-f2 * cs.y, f2 * cs.x);
+          cx = make_double2(-f2 * cx.y, f2 * cx.x);
+          cy = make_double2(-f2 * cy.y, f2 * cy.x);
+          cz = make_double2(-f2 * cz.y, f2 * cz.x);
+        }
+        const Q4 Lq{cs, cx, cy, cz};
+        Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+              make_double2(0, 0)};
+        if (b == 0) sb.s = make_double2(1, 0);
+        else if (b == 1) sb.x = make_double2(1, 0);
+        else if (b == 2) sb.y = make_double2(1, 0);
+        else sb.z = make_double2(1, 0);
+        const Q4 t = qmul(qmul(Lq, dq), sb);
+        r.s = cadd(r.s, t.s);
+        r.x = cadd(r.x, t.x);
+        r.y = cadd(r.y, t.y);
+        r.z = cadd(r.z, t.z);
+      }
+      const size_t t = ix(t1, t2);
+      addz(a.K[0], t, r.s, -wx);
+      addz(a.K[1], t, r.x, -wx);
+      addz(a.K[2], t, r.y, -wx);
+      addz(a.K[3], t, r.z, -wx);
+    };
+    ex(gA, gD, gB, gC, 1.0, 1.0);
+    if (!dCD) ex(gA, gC, gB, gD, 1.0, -1.0);
+    if (!dAB) {
+      ex(gB, gD, gA, gC, -1.0, 1.0);
+      if (!dCD) ex(gB, gC, gA, gD, -1.0, -1.0);
+    }
+  }
+}
+
 // TYPE 1: LLSS (bra = SS pair, differentiated; ket = LL pair), all
 // (bra, ket) combinations (direct4C_libcint.hpp:907-929).
 // TYPE 2: SSSS, unique quartets of pairs (:2018-2047).
@@ -321,108 +441,9 @@ __global__ void __launch_bounds__(REL_THREADS)
         rvDC[2] = -__ldg(a.Xss[2] + 2 * eDC + 1);
         rvDC[3] = -__ldg(a.Xss[3] + 2 * eDC + 1);
       }
-      const double wx = samePQ ? 0.5 : 1.0;
 
-      // ---- digestion of one bra component pair's operator components m
-      auto digest = [&](int ai, int bi, const double* m) {
-        const int gA = P.cA + ai, gB = P.cB + bi;
-        if (TYPE == 1) {
-          // Coulomb SS(1,2) from the LL density (:1145-1190)
-          const double wj = w12 * s34d * rhoLL;
-          if (wj != 0.0)
-#pragma unroll
-            for (int op = 0; op < 4; op++) atomicAdd(a.Jss[op] + ix(gA, gB), wj * m[op]);
-          // Coulomb LL(3,4) from the SS density
-          const size_t eBA = ix(gB, gA);
-          jcol[0] += m[0] * __ldg(a.Xss[0] + 2 * eBA) - m[1] * __ldg(a.Xss[1] + 2 * eBA + 1) -
-                     m[2] * __ldg(a.Xss[2] + 2 * eBA + 1) - m[3] * __ldg(a.Xss[3] + 2 * eBA + 1);
-          if (!a.exchange) return;
-          // exchange LS: K(t1, t2) -= D(d1, d2) P (:1200-1299)
-          auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
-            const size_t e = ix(d1, d2);
-            Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
-            Q4 Cq{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
-                  make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
-            const Q4 r = qmul(dq, Cq);
-            const size_t t = ix(t1, t2);
-            addz(a.K[0], t, r.s, -1.0);
-            addz(a.K[1], t, r.x, -1.0);
-            addz(a.K[2], t, r.y, -1.0);
-            addz(a.K[3], t, r.z, -1.0);
-          };
-          ls(gC, gB, gD, gA, 1.0);
-          if (!dAB) ls(gC, gA, gD, gB, -1.0);
-          if (!dCD) {
-            ls(gD, gB, gC, gA, 1.0);
-            if (!dAB) ls(gD, gA, gC, gB, -1.0);
-          }
-        } else {
-          // m[a * 4 + b]; Coulomb SS(1,2) from D(4,3), and SS(3,4) from
-          // D(2,1) when the bra and ket pairs differ (:2342-2380)
-#pragma unroll
-          for (int op = 0; op < 4; op++) {
-            const double v = m[op * 4 + 0] * rvDC[0] + m[op * 4 + 1] * rvDC[1] +
-                             m[op * 4 + 2] * rvDC[2] + m[op * 4 + 3] * rvDC[3];
-            if (v != 0.0) atomicAdd(a.Jss[op] + ix(gA, gB), w12 * s34d * v);
-          }
-          if (!samePQ) {
-            const size_t eBA = ix(gB, gA);
-            const double rvBA[4] = {__ldg(a.Xss[0] + 2 * eBA), -__ldg(a.Xss[1] + 2 * eBA + 1),
-                                    -__ldg(a.Xss[2] + 2 * eBA + 1),
-                                    -__ldg(a.Xss[3] + 2 * eBA + 1)};
-#pragma unroll
-            for (int b = 0; b < 4; b++)
-              jcol[b] += m[0 * 4 + b] * rvBA[0] + m[1 * 4 + b] * rvBA[1] +
-                         m[2 * 4 + b] * rvBA[2] + m[3 * 4 + b] * rvBA[3];
-          }
-          if (!a.exchange) return;
-          // exchange SS: K(t1, t2) -= P_12 D(d1, d2) P_34 with the bra / ket
-          // orientation signs f1, f2 (:2381-2445); the Hermitian-conjugate
-          // images come from the completion in the back transform
-          auto ex = [&](int t1, int t2, int d1, int d2, double f1, double f2) {
-            const size_t e = ix(d1, d2);
-            const Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
-            Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-#pragma unroll 1
-            for (int b = 0; b < 4; b++) {
-              // left operator sum_a c_ab sigma_a, c_ab = m_ab (i f1)^[a>0] (i f2)^[b>0]
-              double2 cs = make_double2(m[0 * 4 + b], 0.0);
-              double2 cx = make_double2(0.0, f1 * m[1 * 4 + b]);
-              double2 cy = make_double2(0.0, f1 * m[2 * 4 + b]);
-              double2 cz = make_double2(0.0, f1 * m[3 * 4 + b]);
-              if (b > 0) {
-                cs = make_double2(-f2 * cs.y, f2 * cs.x);
-                cx = make_double2(-f2 * cx.y, f2 * cx.x);
-                cy = make_double2(-f2 * cy.y, f2 * cy.x);
-                cz = make_double2(-f2 * cz.y, f2 * cz.x);
-              }
-              const Q4 Lq{cs, cx, cy, cz};
-              Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
-                    make_double2(0, 0)};
-              if (b == 0) sb.s = make_double2(1, 0);
-              else if (b == 1) sb.x = make_double2(1, 0);
-              else if (b == 2) sb.y = make_double2(1, 0);
-              else sb.z = make_double2(1, 0);
-              const Q4 t = qmul(qmul(Lq, dq), sb);
-              r.s = cadd(r.s, t.s);
-              r.x = cadd(r.x, t.x);
-              r.y = cadd(r.y, t.y);
-              r.z = cadd(r.z, t.z);
-            }
-            const size_t t = ix(t1, t2);
-            addz(a.K[0], t, r.s, -wx);
-            addz(a.K[1], t, r.x, -wx);
-            addz(a.K[2], t, r.y, -wx);
-            addz(a.K[3], t, r.z, -wx);
-          };
-          ex(gA, gD, gB, gC, 1.0, 1.0);
-          if (!dCD) ex(gA, gC, gB, gD, 1.0, -1.0);
-          if (!dAB) {
-            ex(gB, gD, gA, gC, -1.0, 1.0);
-            if (!dCD) ex(gB, gC, gA, gD, -1.0, -1.0);
-          }
-        }
-      };
+      const RelCol col{gC, gD, dAB, dCD, samePQ, s34d, w12, samePQ ? 0.5 : 1.0, rhoLL,
+                       {rvDC[0], rvDC[1], rvDC[2], rvDC[3]}};
 
       if (!single)
 #pragma unroll 1
@@ -516,12 +537,12 @@ __global__ void __launch_bounds__(REL_THREADS)
                   m[op * NB + b] += sg * bra_dot(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty],
                                                  fa[2][tz], nfa[2][tz], G[b]);
               }
-            if (single) digest(ai, bi, mloc);
+            if (single) rel_digest<TYPE>(a, P, col, ai, bi, mloc, jcol);
           }
       }
       if (!single)
 #pragma unroll 1
-        for (int ab = 0; ab < nab; ab++) digest(ab / nb, ab % nb, acc + ab * NC);
+        for (int ab = 0; ab < nab; ab++) rel_digest<TYPE>(a, P, col, ab / nb, ab % nb, acc + ab * NC, jcol);
 
       // per-column Coulomb flush
       if (TYPE == 1) {
@@ -532,6 +553,309 @@ __global__ void __launch_bounds__(REL_THREADS)
           if (jcol[b] != 0.0) atomicAdd(a.Jss[b] + ix(gC, gD), w34 * s12d * jcol[b]);
       }
     }
+  }
+}
+
+// Hermite index (t, u, v) of compact index e (inverse of hidx).
+__device__ __forceinline__ void hinv(int e, int& t, int& u, int& v) {
+  int sdeg = 0;
+  while (nherm(sdeg) <= e) sdeg++;
+  int r = e - nherm(sdeg - 1), k = 0;
+  while ((k + 1) * (k + 2) / 2 <= r) k++;
+  v = r - k * (k + 1) / 2;
+  u = k - v;
+  t = sdeg - k;
+}
+
+constexpr int RB_THREADS = 128;
+
+// Shared-memory layout of rel_block_kernel (doubles), per launch.
+struct RelBlockLayout {
+  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, total;
+};
+__host__ __device__ inline RelBlockLayout rel_block_layout(int la, int lb, int lc, int ld,
+                                                           int type) {
+  const int dK = type == 2 ? 1 : 0;
+  const int Lb = la + lb + 2, L = Lb + lc + ld + 2 * dK;
+  const int NB = type == 2 ? 4 : 1;
+  const int nab = ncart(la) * ncart(lb);
+  const int FL = 2 * (la > lb ? la : lb) + 3;
+  const int FLk = 2 * (lc > ld ? lc : ld) + 3;
+  RelBlockLayout Lo;
+  int o = 0;
+  auto take = [&](int n) { int r = o; o += (n + 1) / 2 * 2; return r; };
+  Lo.oR0 = take(nherm(L));
+  Lo.oR1 = take(nherm(L));
+  Lo.oEb = take(3 * (la + 2) * (lb + 2) * (la + lb + 3));
+  Lo.oEk = take(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
+  Lo.oFa = take(nab * 12 * FL);
+  Lo.oFc = take(12 * FLk);
+  Lo.oG = take(NB * nherm(Lb));
+  Lo.oM = take(nab * 4 * NB);
+  Lo.oF = take(L + 1);
+  Lo.oJ = take(4);
+  Lo.total = o;
+  return Lo;
+}
+
+// Block-cooperative form of rel_kernel for the heavy classes (d and f
+// shells): one block per unique quartet, everything in shared memory.  Per
+// primitive quartet: E tables, R (level by level, ping-pong buffers, all
+// threads), the bra factors of every component pair; per ket component pair
+// (c, d): its ket factors, G[b][tuv] (one entry per thread), the operator
+// components of every bra component pair (one (ab, b) unit per thread) and
+// their digestion (one ab per thread), the per-column Coulomb sum reduced in
+// shared memory.  Same quartet set, screens and updates as rel_kernel.
+template <int TYPE>
+__global__ void __launch_bounds__(RB_THREADS)
+    rel_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+  extern __shared__ double sm[];
+  const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  int ib, jk;
+  if (TYPE == 2 && a.same) {  // SSSS, one class: unordered pairs jk <= ib
+    long long r = (long long)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
+    while (r * (r + 1) / 2 > q) r--;
+    while ((r + 1) * (r + 2) / 2 <= q) r++;
+    ib = (int)r;
+    jk = (int)(q - r * (r + 1) / 2);
+  } else {
+    ib = (int)(q / a.nKet);
+    jk = (int)(q % a.nKet);
+  }
+  if (ib >= a.nBra) return;
+  const int ns = a.nShell;
+  const PairDev P = a.pairs[a.braBeg + ib];
+  const PairDev Q = a.pairs[a.ketBeg + jk];
+  bool work;
+  {
+    int s1, s2, s3, s4;
+    double q12, q34;
+    if (TYPE == 1) {
+      s1 = P.s1; s2 = P.s2; s3 = Q.s1; s4 = Q.s2;
+      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+      q34 = __ldg(a.qLL + s3 + (size_t)s4 * ns);
+    } else {
+      const bool pRef = P.lex >= Q.lex;
+      const PairDev& R12 = pRef ? P : Q;
+      const PairDev& R34 = pRef ? Q : P;
+      s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
+      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+      q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
+    }
+    work = !a.screen || sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34 >= a.thresh;
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(a.counters + 0, 1ull);
+    atomicAdd(a.counters + (work ? 3 : 1), 1ull);
+  }
+  if (!work) return;  // block-uniform
+
+  constexpr int NB = (TYPE == 2) ? 4 : 1;
+  constexpr int NC = 4 * NB;
+  const int tid = threadIdx.x;
+  const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb;
+  const int dK = (TYPE == 2) ? 1 : 0;
+  const int Lb = la + lb + 2, L = Lb + lc + ld + 2 * dK;
+  const int FL = 2 * max(la, lb) + 3, FLk = 2 * max(lc, ld) + 3;
+  const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
+  double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
+  double* Eb = sm + Lo.oEb;
+  double* Ek = sm + Lo.oEk;
+  double* fa = sm + Lo.oFa;
+  double* fc = sm + Lo.oFc;
+  double* G = sm + Lo.oG;
+  double* Mc = sm + Lo.oM;
+  double* Fs = sm + Lo.oF;
+  double* Js = sm + Lo.oJ;
+  const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
+  const int E1k = (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK);
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+  const bool dAB = P.shA == P.shB, dCD = Q.shA == Q.shB, samePQ = P.lex == Q.lex;
+  const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
+  const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
+  const size_t nc = a.ncart;
+  const double* R = Rb[0];  // R^(0) after the recursion
+  double ec = 0.0, ed = 0.0, pref = 0.0;
+
+  // E tables, R and the bra factors of primitive quartet (ip, iq)
+  auto prep = [&](int ip, int iq) {
+    const PrimPairDev& A = a.pp[P.pp_off + ip];
+    const PrimPairDev& B = a.pp[Q.pp_off + iq];
+    double ea, eb;
+    pair_exps(SA, SB, a.prim, ip, ea, eb);
+    pair_exps(SC, SD, a.prim, iq, ec, ed);
+    if (tid < 3)
+      hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid], Eb + tid * E1b);
+    else if (tid < 6)
+      hermite_E_rt<double, LMAX + 1>(lc + dK, ld + dK, B.o2p, B.PA[tid - 3], B.PB[tid - 3],
+                                     Ek + (tid - 3) * E1k);
+    const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
+    const double pq = A.p + B.p, alpha = A.p * B.p / pq;
+    pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+    if (tid == 6) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+    __syncthreads();
+    // R^(n)_tuv, n = L .. 0, from R^(n+1); level n in Rb[n & 1]
+    const double m2a = -2.0 * alpha;
+    for (int n = L; n >= 0; n--) {
+      double* cur = Rb[n & 1];
+      const double* prv = Rb[(n + 1) & 1];
+      const int cnt = nherm(L - n);
+      for (int e = tid; e < cnt; e += RB_THREADS) {
+        int t, u, v;
+        hinv(e, t, u, v);
+        double val;
+        if (e == 0) {
+          double f = 1.0;
+          for (int k = 0; k < n; k++) f *= m2a;
+          val = f * Fs[n];
+        } else if (t > 0) {
+          val = X * prv[hidx(t - 1, u, v)];
+          if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+        } else if (u > 0) {
+          val = Y * prv[hidx(0, u - 1, v)];
+          if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+        } else {
+          val = Z * prv[hidx(0, 0, v - 1)];
+          if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+        }
+        cur[e] = val;
+      }
+      __syncthreads();
+    }
+    // bra factors of every component pair, axis and derivative type
+    for (int it = tid; it < nab * 12; it += RB_THREADS) {
+      const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
+      const int ai = ab / nb, bi = ab % nb;
+      const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
+      const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
+      axis_factor(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
+                  fa + (size_t)it * FL);
+    }
+    __syncthreads();
+  };
+
+  const bool single = P.npp == 1 && Q.npp == 1;
+  if (single) prep(0, 0);
+  if (tid < 4) Js[tid] = 0.0;
+#pragma unroll 1
+  for (int cd = 0; cd < ncc * nd; cd++) {
+    const int c = cd / nd, d = cd % nd;
+    const int gC = Q.cA + c, gD = Q.cB + d;
+    for (int e = tid; e < nab * NC; e += RB_THREADS) Mc[e] = 0.0;
+#pragma unroll 1
+    for (int ip = 0; ip < P.npp; ip++)
+#pragma unroll 1
+      for (int iq = 0; iq < Q.npp; iq++) {
+        if (!single) prep(ip, iq);  // ends with a barrier
+        // ket factors of this component pair (sign (-1)^t folded in)
+        const int ntk = (TYPE == 2) ? 4 : 1;
+        if (tid < 3 * ntk) {
+          const int x = tid / ntk, ty = tid % ntk;
+          const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
+          const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
+          double* f = fc + (x * 4 + ty) * FLk;
+          const int n = axis_factor(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
+                                    2.0 * ec, 2.0 * ed, f);
+          for (int t = 1; t < n; t += 2) f[t] = -f[t];
+        }
+        __syncthreads();
+        // G[b][tuv]
+        const int hb = nherm(Lb);
+        for (int e = tid; e < NB * hb; e += RB_THREADS) {
+          const int b = e / hb, h = e % hb;
+          int t, u, v;
+          hinv(h, t, u, v);
+          const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
+          const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+          double gsum = 0.0;
+          for (int kk = 0; kk < (TYPE == 2 ? 3 : 1); kk++)
+            for (int ll = 0; ll < (TYPE == 2 ? 3 : 1); ll++) {
+              int op = 0;
+              double sg = 1.0;
+              int tyx = 0, tyy = 0, tyz = 0;
+              if (TYPE == 2) {
+                op_of(kk, ll, op, sg);
+                if (op != b) continue;
+                tyx = (kk == 0) | ((ll == 0) << 1);
+                tyy = (kk == 1) | ((ll == 1) << 1);
+                tyz = (kk == 2) | ((ll == 2) << 1);
+              }
+              const double* fx = fc + (0 * 4 + tyx) * FLk;
+              const double* fy = fc + (1 * 4 + tyy) * FLk;
+              const double* fz = fc + (2 * 4 + tyz) * FLk;
+              const int nx = ci[0] + di[0] + (tyx & 1) + (tyx >> 1) + 1;
+              const int ny = ci[1] + di[1] + (tyy & 1) + (tyy >> 1) + 1;
+              const int nz = ci[2] + di[2] + (tyz & 1) + (tyz >> 1) + 1;
+              double acc = 0.0;
+              for (int i = 0; i < nx; i++) {
+                if (fx[i] == 0.0) continue;
+                for (int j = 0; j < ny; j++) {
+                  const double fxy = fx[i] * fy[j];
+                  if (fxy == 0.0) continue;
+                  for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+                }
+              }
+              gsum += sg * acc;
+            }
+          G[e] = pref * gsum;
+        }
+        __syncthreads();
+        // operator components of every bra component pair: unit (ab, b)
+        for (int e = tid; e < nab * NB; e += RB_THREADS) {
+          const int ab = e / NB, b = e % NB;
+          const int ai = ab / nb, bi = ab % nb;
+          const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+          const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+          double m4[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int mu = 0; mu < 3; mu++)
+            for (int nu = 0; nu < 3; nu++) {
+              int op;
+              double sg;
+              op_of(mu, nu, op, sg);
+              const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
+                        tz = (mu == 2) | ((nu == 2) << 1);
+              const double* gx = fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL;
+              const double* gy = fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL;
+              const double* gz = fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL;
+              m4[op] += sg * bra_dot(gx, ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1, gy,
+                                     ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1, gz,
+                                     ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + b * hb);
+            }
+          for (int op = 0; op < 4; op++) Mc[ab * NC + op * NB + b] += m4[op];
+        }
+        __syncthreads();
+      }
+    // digestion, one bra component pair per thread
+    RelCol col{gC, gD, dAB, dCD, samePQ, s34d, w12, samePQ ? 0.5 : 1.0, 0.0, {0, 0, 0, 0}};
+    if (TYPE == 1) {
+      col.rhoLL = __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc));
+    } else {
+      const size_t eDC = (size_t)gD + (size_t)gC * nc;
+      col.rvDC[0] = __ldg(a.Xss[0] + 2 * eDC);
+      col.rvDC[1] = -__ldg(a.Xss[1] + 2 * eDC + 1);
+      col.rvDC[2] = -__ldg(a.Xss[2] + 2 * eDC + 1);
+      col.rvDC[3] = -__ldg(a.Xss[3] + 2 * eDC + 1);
+    }
+    for (int ab = tid; ab < nab; ab += RB_THREADS) {
+      double jl[4] = {0.0, 0.0, 0.0, 0.0};
+      rel_digest<TYPE>(a, P, col, ab / nb, ab % nb, Mc + ab * NC, jl);
+      for (int b = 0; b < 4; b++)
+        if (jl[b] != 0.0) atomicAdd(Js + b, jl[b]);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const size_t eCD = (size_t)gC + (size_t)gD * nc;
+      if (TYPE == 1) {
+        if (Js[0] != 0.0) atomicAdd(a.Jll + eCD, w34 * s12d * Js[0]);
+      } else if (!samePQ) {
+        for (int b = 0; b < 4; b++)
+          if (Js[b] != 0.0) atomicAdd(a.Jss[b] + eCD, w34 * s12d * Js[b]);
+      }
+      for (int b = 0; b < 4; b++) Js[b] = 0.0;
+    }
+    __syncthreads();
   }
 }
 
@@ -547,9 +871,26 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
   nsplit = std::max(1, std::min(nsplit, 65535 / tiles));
   dim3 grid(a.nBra, tiles * nsplit);
   const int lm = std::max(std::max(la, lb), std::max(lc, ld));
-  if (lm <= 1) rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
-  else if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
-  else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+  if (lm <= 1) {
+    rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    return;
+  }
+  if (TYPE == 1) {  // LLSS: 4x the quartets, 1/4 of the work each -- per thread
+    if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    return;
+  }
+  // SSSS d and f classes: one block per quartet, intermediates in shared memory
+  const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
+  const size_t smem = (size_t)Lo.total * sizeof(double);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(rel_block_kernel<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  const long long nq = (TYPE == 2 && a.same) ? (long long)a.nBra * (a.nBra + 1) / 2
+                                             : (long long)a.nBra * a.nKet;
+  const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
+  const unsigned gy = (unsigned)((nq + gx - 1) / gx);
+  rel_block_kernel<TYPE><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
 }
 
 // ------------------------------------------------------------ 4C Schwarz
