@@ -859,6 +859,214 @@ __global__ void __launch_bounds__(RB_THREADS)
   }
 }
 
+// Shared-memory layout of rel_llss_block_kernel (doubles).
+struct LlssBlockLayout {
+  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, total;
+};
+__host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int lc, int ld) {
+  const int Lb = la + lb + 2, L = Lb + lc + ld;
+  const int nab = ncart(la) * ncart(lb), ncd = ncart(lc) * ncart(ld);
+  const int FL = 2 * (la > lb ? la : lb) + 3, FLk = lc + ld + 1;
+  LlssBlockLayout Lo;
+  int o = 0;
+  auto take = [&](int n) { int r = o; o += (n + 1) / 2 * 2; return r; };
+  Lo.oR0 = take(nherm(L));
+  Lo.oR1 = take(nherm(L));
+  Lo.oEb = take(3 * (la + 2) * (lb + 2) * (la + lb + 3));
+  Lo.oEk = take(3 * (lc + 1) * (ld + 1) * (lc + ld + 1));
+  Lo.oFa = take(nab * 12 * FL);
+  Lo.oFc = take(ncd * 3 * FLk);
+  Lo.oG = take(ncd * nherm(Lb));
+  Lo.oM = take(nab * ncd * 4);
+  Lo.oF = take(L + 1);
+  Lo.oJ = take(ncd);
+  Lo.total = o;
+  return Lo;
+}
+
+// LLSS form of the block kernel: the ket pair is undifferentiated, so the
+// ket-contracted Hermite sums G[cd][tuv] of every ket component pair are
+// built at once, and the operator components of every (bra, ket) component
+// element are one work unit per thread (nab x ncd units); digestion per
+// element, the per-column Coulomb sums J_LL(C,D) reduced in shared memory.
+__global__ void __launch_bounds__(RB_THREADS)
+    rel_llss_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+  extern __shared__ double sm[];
+  const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  const int ib = (int)(q / a.nKet), jk = (int)(q % a.nKet);
+  if (ib >= a.nBra) return;
+  const int ns = a.nShell;
+  const PairDev P = a.pairs[a.braBeg + ib];
+  const PairDev Q = a.pairs[a.ketBeg + jk];
+  const bool work = !a.screen ||
+      sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) * __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
+              __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns) >= a.thresh;
+  if (threadIdx.x == 0) {
+    atomicAdd(a.counters + 0, 1ull);
+    atomicAdd(a.counters + (work ? 3 : 1), 1ull);
+  }
+  if (!work) return;  // block-uniform
+
+  const int tid = threadIdx.x;
+  const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb, ncd = ncc * nd;
+  const int Lb = la + lb + 2, L = Lb + lc + ld;
+  const int hb = nherm(Lb);
+  const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
+  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
+  double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
+  double* Eb = sm + Lo.oEb;
+  double* Ek = sm + Lo.oEk;
+  double* fa = sm + Lo.oFa;
+  double* fc = sm + Lo.oFc;
+  double* G = sm + Lo.oG;
+  double* Mc = sm + Lo.oM;
+  double* Fs = sm + Lo.oF;
+  double* Js = sm + Lo.oJ;
+  const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
+  const int E1k = (lc + 1) * (ld + 1) * (lc + ld + 1);
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+  const bool dAB = P.shA == P.shB, dCD = Q.shA == Q.shB;
+  const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
+  const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
+  const size_t nc = a.ncart;
+  const double* R = Rb[0];
+
+  for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
+  for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
+#pragma unroll 1
+  for (int ip = 0; ip < P.npp; ip++)
+#pragma unroll 1
+    for (int iq = 0; iq < Q.npp; iq++) {
+      const PrimPairDev& A = a.pp[P.pp_off + ip];
+      const PrimPairDev& B = a.pp[Q.pp_off + iq];
+      double ea, eb, ec, ed;
+      pair_exps(SA, SB, a.prim, ip, ea, eb);
+      pair_exps(SC, SD, a.prim, iq, ec, ed);
+      __syncthreads();  // the previous primitive quartet's readers are done
+      if (tid < 3)
+        hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid],
+                                       Eb + tid * E1b);
+      else if (tid < 6)
+        hermite_E_rt<double, LMAX + 1>(lc, ld, B.o2p, B.PA[tid - 3], B.PB[tid - 3],
+                                       Ek + (tid - 3) * E1k);
+      const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
+      const double pq = A.p + B.p, alpha = A.p * B.p / pq;
+      const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+      if (tid == 6) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+      __syncthreads();
+      const double m2a = -2.0 * alpha;
+      for (int n = L; n >= 0; n--) {
+        double* cur = Rb[n & 1];
+        const double* prv = Rb[(n + 1) & 1];
+        const int cnt = nherm(L - n);
+        for (int e = tid; e < cnt; e += RB_THREADS) {
+          int t, u, v;
+          hinv(e, t, u, v);
+          double val;
+          if (e == 0) {
+            double f = 1.0;
+            for (int k = 0; k < n; k++) f *= m2a;
+            val = f * Fs[n];
+          } else if (t > 0) {
+            val = X * prv[hidx(t - 1, u, v)];
+            if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+          } else if (u > 0) {
+            val = Y * prv[hidx(0, u - 1, v)];
+            if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+          } else {
+            val = Z * prv[hidx(0, 0, v - 1)];
+            if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+          }
+          cur[e] = val;
+        }
+        __syncthreads();
+      }
+      // bra factors (every pair, axis, derivative type); ket factors of every
+      // ket component pair (undifferentiated, sign (-1)^t folded in)
+      for (int it = tid; it < nab * 12; it += RB_THREADS) {
+        const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
+        const int ai = ab / nb, bi = ab % nb;
+        const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
+        const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
+        axis_factor(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
+                    fa + (size_t)it * FL);
+      }
+      for (int it = tid; it < ncd * 3; it += RB_THREADS) {
+        const int cd = it / 3, x = it % 3, c = cd / nd, d = cd % nd;
+        const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
+        const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
+        double* f = fc + (size_t)it * FLk;
+        const int n = axis_factor(Ek + x * E1k, ld, lc + ld + 1, ci, di, 0, 0.0, 0.0, f);
+        for (int t = 1; t < n; t += 2) f[t] = -f[t];
+      }
+      __syncthreads();
+      // G[cd][tuv] of every ket component pair
+      for (int e = tid; e < ncd * hb; e += RB_THREADS) {
+        const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
+        int t, u, v;
+        hinv(h, t, u, v);
+        const double* fx = fc + (size_t)(cd * 3 + 0) * FLk;
+        const double* fy = fc + (size_t)(cd * 3 + 1) * FLk;
+        const double* fz = fc + (size_t)(cd * 3 + 2) * FLk;
+        const int nx = cart_lx(lc, c) + cart_lx(ld, d) + 1;
+        const int ny = cart_ly(lc, c) + cart_ly(ld, d) + 1;
+        const int nz = cart_lz(lc, c) + cart_lz(ld, d) + 1;
+        double acc = 0.0;
+        for (int i = 0; i < nx; i++) {
+          if (fx[i] == 0.0) continue;
+          for (int j = 0; j < ny; j++) {
+            const double fxy = fx[i] * fy[j];
+            if (fxy == 0.0) continue;
+            for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+          }
+        }
+        G[e] = pref * acc;
+      }
+      __syncthreads();
+      // operator components of every (bra, ket) component element
+      for (int e = tid; e < nab * ncd; e += RB_THREADS) {
+        const int ab = e / ncd, cd = e % ncd;
+        const int ai = ab / nb, bi = ab % nb;
+        const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+        const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+        double m4[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int mu = 0; mu < 3; mu++)
+          for (int nu = 0; nu < 3; nu++) {
+            int op;
+            double sg;
+            op_of(mu, nu, op, sg);
+            const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
+                      tz = (mu == 2) | ((nu == 2) << 1);
+            m4[op] += sg * bra_dot(fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL,
+                                   ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1,
+                                   fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL,
+                                   ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1,
+                                   fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL,
+                                   ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + (size_t)cd * hb);
+          }
+        for (int op = 0; op < 4; op++) Mc[(size_t)e * 4 + op] += m4[op];
+      }
+    }
+  __syncthreads();
+  // digestion, one (bra, ket) component element per thread
+  for (int e = tid; e < nab * ncd; e += RB_THREADS) {
+    const int ab = e / ncd, cd = e % ncd;
+    const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
+    RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
+               __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc)), {0, 0, 0, 0}};
+    double jl[4] = {0.0, 0.0, 0.0, 0.0};
+    rel_digest<1>(a, P, col, ab / nb, ab % nb, Mc + (size_t)e * 4, jl);
+    if (jl[0] != 0.0) atomicAdd(Js + cd, jl[0]);
+  }
+  __syncthreads();
+  for (int cd = tid; cd < ncd; cd += RB_THREADS)
+    if (Js[cd] != 0.0)
+      atomicAdd(a.Jll + (size_t)(Q.cA + cd / nd) + (size_t)(Q.cB + cd % nd) * nc,
+                w34 * s12d * Js[cd]);
+}
+
 template <int TYPE>
 void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
   if (a.nBra == 0 || a.nKet == 0) return;
@@ -875,9 +1083,24 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
     rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     return;
   }
-  if (TYPE == 1) {  // LLSS: 4x the quartets, 1/4 of the work each -- per thread
-    if (lm == 2) rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
-    else rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+  if (TYPE == 1) {
+    // LLSS d/f classes: one block per quartet with every ket component at
+    // once, when it fits in shared memory; else per thread
+    const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
+    const size_t smem = (size_t)Lo.total * sizeof(double);
+    if (smem <= 160 * 1024) {
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(rel_llss_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+      const long long nq = (long long)a.nBra * a.nKet;
+      const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
+      const unsigned gy = (unsigned)((nq + gx - 1) / gx);
+      rel_llss_block_kernel<<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+    } else if (lm == 2) {
+      rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    } else {
+      rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    }
     return;
   }
   // SSSS d and f classes: one block per quartet, intermediates in shared memory
