@@ -6,15 +6,18 @@
 //                          src/basisset/basisset.cxx:652-706), grouped into
 //                          angular-momentum classes (lA >= lB) and sorted by
 //                          Schwarz bound (descending) inside each class
-//   PrimPairDev[nprimpair] primitive-pair data (p, K, P, PA, PB), 96 B each,
-//                          contiguous per shell pair so one pair's primitives
-//                          are one coalesced run
+//   PrimPairDev[nprimpair] primitive-pair data (p, K/p, 1/2p, P, PA, PB),
+//                          96 B each, contiguous per shell pair; the same
+//                          data tile-interleaved (field-major runs of 128
+//                          kets) for the class kernels' per-lane ket loads
+//   bra groups             per class a bra order by first shell, cut into
+//                          groups (grouped class kernels)
 //   boys tables            per angular sum L and grid point T_j = j*0.1 one
 //                          row {F_L..F_{L+8}(T_j), exp(-T_j)}: 80 B, 16-B
 //                          aligned, read with five 128-bit loads (FP64); FP32
 //                          rows {F_L..F_{L+5}, exp(-T_j), 0}: 32 B.  The
-//                          29 KB (FP64) / 11.6 KB (FP32) of one L are staged
-//                          in shared memory by the class kernels.
+//                          29 KB (FP64) / 11.6 KB (FP32) of one L are read
+//                          through L1; one copy per device for all bases.
 //   Cartesian-AO densities / accumulators, nMat x ncart x ncart
 #pragma once
 
