@@ -336,7 +336,9 @@ def run_four_component(args, ws, rank, local, pg):
     seeded complex spinors orthonormalised in the 4C metric; FP64.  A step is
     one full formGDDirect build.  The CPU baseline is the oracle on a bounded
     sample (one Ag atom, bare Coulomb + LLSS) with the GPU timed on the same
-    sample."""
+    sample.  The line's "mixed" object is one build with FP32 arithmetic on
+    the quartets whose screening bound is below --cutoff, timed the same way,
+    and its largest deviation from the FP64 build."""
     import numpy as np
     import torch
 
@@ -373,6 +375,20 @@ def run_four_component(args, ws, rank, local, pg):
     stats = dict(fb.last_stats)
     torch.cuda.synchronize()
     herm = max(float((g - g.conj().t()).abs().max()) for g in G)
+    # mixed precision (FP32 on quartets with bound < cutoff): one timed build
+    # after one warm-up, and its largest deviation from the FP64 build
+    fb.formGD(Dd, precision="mixed", fp32_cutoff=args.cutoff, stream=stream.cuda_stream)
+    flush.fill_(1.0)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    Gm = fb.formGD(Dd, precision="mixed", fp32_cutoff=args.cutoff, stream=stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms_mixed = e0.elapsed_time(e1)
+    smix = dict(fb.last_stats)
+    mixed_err = max(float((a - b).abs().max()) for a, b in zip(Gm, G))
+    del Gm
     # e2e: host numpy buffers through the public API
     te = []
     t0 = time.perf_counter()
@@ -398,6 +414,9 @@ def run_four_component(args, ws, rank, local, pg):
         "quartets": {"computed": stats["fp64"], "screened": stats["screened"],
                      "total": stats["total"]},
         "checks": {"G_hermiticity_maxabs": herm},
+        "mixed": {"builds_per_s": ws * 1e3 / ms_mixed, "fp32_cutoff": args.cutoff,
+                  "G_maxabs_vs_fp64": mixed_err, "quartets_fp32": smix["fp32"],
+                  "quartets_fp64": smix["fp64"], "speedup_vs_fp64": (tdev / K) / (ms_mixed / 1e3)},
         "e2e": {"value": ws / te2e, "unit": "builds/s",
                 "h2d_bytes_per_step": 4 * 16 * N2 * N2,
                 "d2h_bytes_per_step": 4 * 16 * N2 * N2},

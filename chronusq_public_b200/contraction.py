@@ -259,11 +259,14 @@ class GTODirectRelERIContraction:
 
     def twoBodyContract(self, matList: List[TwoBodyContraction],
                         contType: int, computeExchange: bool = True,
-                        screen: bool = True, stream=None) -> None:
+                        screen: bool = True, precision: str = "fp64",
+                        fp32_cutoff: float = 0.0, stream=None) -> None:
         """17 entries in REL_COMPS order (None for entries the type does not
         use).  Every given AX is overwritten (the reference zeroes AX on
         entry); X and AX are N x N complex (numpy, or column-major CUDA
-        complex128 tensors)."""
+        complex128 tensors).  precision="mixed" runs the quartets whose
+        screening bound is below fp32_cutoff in FP32 arithmetic (the
+        reference is FP64 throughout)."""
         if len(matList) != _cabi.CQF_REL_NMAT:
             raise ValueError("a 4C contraction list has 17 entries")
         N = self.tpi.nbasis
@@ -295,6 +298,8 @@ class GTODirectRelERIContraction:
         _cabi.lib().cqf_opts_default(C.byref(opts))
         opts.is_complex = 1
         opts.screen = 1 if screen else 0
+        opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
+        opts.fp32_cutoff = float(fp32_cutoff)
         opts.device_pointers = 1 if dev else 0
         opts.stream = _stream_arg(stream)
         st = _cabi.CqfStats()

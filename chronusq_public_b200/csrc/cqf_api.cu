@@ -465,7 +465,8 @@ void free_basis(cqf_basis* B) {
   if (B->stream) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
-                    (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_braPerm,
+                    (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_pairRange,
+                    (void*)B->d_braPerm,
                     (void*)B->d_groups, (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
                     (void*)B->d_cart2shell, (void*)B->d_ws, (void*)B->d_counters,
@@ -731,6 +732,20 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     toff.push_back((long long)kt.size());
     kt.push_back(0.0);
     CQF_TRY(upload(&B->d_ketT, kt, B->stream));
+    // FP32 range data per pair: log2 of 2 max p and of max |Kp| over its
+    // primitive pairs (fp32_range_ok)
+    std::vector<float2> rng(std::max(1, B->npair), make_float2(0.f, 0.f));
+    for (int i = 0; i < B->npair; i++) {
+      double pm = 0.0, km = 0.0;
+      for (int iq = 0; iq < B->h_pairs[i].npp; iq++) {
+        const PrimPairDev& r = hpp2[B->h_pairs[i].pp_off + iq];
+        pm = std::max(pm, r.p);
+        km = std::max(km, std::fabs(r.Kp));
+      }
+      rng[i] = make_float2((float)std::log2(std::max(2.0 * pm, 1e-30)),
+                           (float)std::log2(std::max(km, 1e-60)));
+    }
+    CQF_TRY(upload(&B->d_pairRange, rng, B->stream));
     CQF_TRY(upload(&B->d_tileOff, toff, B->stream));
     // bra groups: per class, pairs ordered by first shell (stable: Schwarz
     // order inside a shell), runs of one shell cut into groups of at most
@@ -1001,6 +1016,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.maxNorm = ws + oG;
   a.normsT = ws + Lw.oNmT;
   a.pairNorm = ws + Lw.oPN;
+  a.pairRange = B->d_pairRange;
   a.nShell = ns;
   a.nMat = nMat;
   a.cplx = opts.is_complex;

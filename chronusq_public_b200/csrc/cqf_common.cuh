@@ -99,6 +99,23 @@ struct __align__(16) PrimPairDev {
   double o2p;        // 1 / (2p)
 };
 
+// FP32 range guard of the mixed path.  The Hermite recursion starts from
+// R^(n)_000 = (-2 alpha)^n F_n(T), n <= L, so its intermediates reach
+// (2 alpha)^L; alpha = pq / (p + q) <= min(p, q).  Tight primitives (core
+// shells of heavy atoms, exponents 1e4 .. 1e8) push that past FP32's 2^128
+// at moderate L, and F_n underflows at the same time (inf * 0 = NaN), while
+// FP64's range holds.  A quartet may run in FP32 only when
+//   L log2(2 min(p, q))                                 <= 100, and
+//   that + log2 max|Kp| + log2 max|Kq| + 2 dP log2(2p) + 2 dQ log2(2q) <= 110
+// with p, q the pairs' largest primitive exponent sums and dP, dQ = 1 for a
+// pair carrying the two derivative factors of a small-component bra or ket
+// (each up to 2p).  r.x = log2(2 max p), r.y = log2(max |Kp|) per pair.
+__device__ __forceinline__ bool fp32_range_ok(float2 rP, float2 rQ, int L, int dP, int dQ) {
+  const float lr = (float)L * fmaxf(fminf(rP.x, rQ.x), 0.f);
+  const float ld = 2.f * ((float)dP * fmaxf(rP.x, 0.f) + (float)dQ * fmaxf(rQ.x, 0.f));
+  return lr <= 100.f && lr + rP.y + rQ.y + ld <= 110.f;
+}
+
 // ----------------------------------------------------------------- Boys
 // F_0..F_L at T.  Taylor expansion of F_L about the nearest grid point
 // (F_m' = -F_{m+1}), downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1);

@@ -44,6 +44,7 @@ struct JKLaunch {
   const double* maxNorm;    // device scalar: max of norms (tile-level screen)
   const double* normsT;     // transpose of norms
   const double* pairNorm;   // per pair (pair order): norms(s1, s2)
+  const float2* pairRange;  // per pair: FP32 range data (fp32_range_ok)
   int nShell;
   int nMat, cplx, ncart;
   const int* flags;         // nMat flags (device)
@@ -120,6 +121,7 @@ struct cqf_basis {
   cqf::PrimPairDev* d_pp = nullptr;
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
+  float2* d_pairRange = nullptr;         // per pair: FP32 range data
   int* d_braPerm = nullptr;              // npair: class-relative bra order
   int2* d_groups = nullptr;              // bra groups of all classes
   double* d_boys64 = nullptr;

@@ -159,7 +159,9 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
         screened = bound < a.thresh;
       }
       w64 = !screened;
-      w32 = w64 && mixed && bound < cut;
+      w32 = w64 && mixed && bound < cut &&
+            fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib), __ldg(a.pairRange + a.ketBeg + jk),
+                          LSUM, 0, 0);
     }
     // one precision per warp: FP32 only when every surviving quartet of the
     // warp is below the cut (no divergent FP64 / FP32 code in a warp)
@@ -300,7 +302,9 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
           screened = bound < a.thresh;
         }
         w64 = !screened;
-        w32 = w64 && MIXED && bound < cut;
+        w32 = w64 && MIXED && bound < cut &&
+              fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                            __ldg(a.pairRange + a.ketBeg + jk), LSUM, 0, 0);
       }
       if (__any_sync(0xffffffffu, w64 && !w32)) w32 = false;
       else w64 = w64 && !w32;

@@ -180,7 +180,9 @@ __global__ void __launch_bounds__(JK_THREADS)
       screened = bound < a.thresh;
     }
     work = !screened;
-    fp32 = work && a.precision == 1 && bound < a.fp32_cut;
+    fp32 = work && a.precision == 1 && bound < a.fp32_cut &&
+           fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib), __ldg(a.pairRange + a.ketBeg + jk),
+                         la + lb + lc + ld, 0, 0);
   }
   count_block(a.counters, visited, screened, fp32, work && !fp32);
   if (!work) return;

@@ -110,22 +110,23 @@ __device__ __forceinline__ void addz(double* A, size_t e, double2 v, double w) {
 // on the first centre (type bit 0) and / or the second (bit 1).  E is the
 // pair's table raised by one on both centres when a derivative is taken:
 // E[(i * (l2r + 1) + j) * Lr + t].  Returns the length (t = 0 .. n-1).
-__device__ __forceinline__ int axis_factor(const double* E, int l2r, int Lr, int i, int j,
-                                           int type, double a2, double b2, double* f) {
+template <typename T>
+__device__ __forceinline__ int axis_factor(const T* E, int l2r, int Lr, int i, int j, int type,
+                                           T a2, T b2, T* f) {
   const int dA = type & 1, dB = (type >> 1) & 1;
   const int n = i + j + dA + dB + 1;
-  auto e = [&](int ii, int jj, int t) -> double {
-    return (ii < 0 || jj < 0 || t > ii + jj) ? 0.0 : E[(ii * (l2r + 1) + jj) * Lr + t];
+  auto e = [&](int ii, int jj, int t) -> T {
+    return (ii < 0 || jj < 0 || t > ii + jj) ? T(0) : E[(ii * (l2r + 1) + jj) * Lr + t];
   };
 #pragma unroll 1
   for (int t = 0; t < n; t++) {
-    double v;
+    T v;
     if (type == 0) v = e(i, j, t);
-    else if (type == 1) v = i * e(i - 1, j, t) - a2 * e(i + 1, j, t);
-    else if (type == 2) v = j * e(i, j - 1, t) - b2 * e(i, j + 1, t);
+    else if (type == 1) v = T(i) * e(i - 1, j, t) - a2 * e(i + 1, j, t);
+    else if (type == 2) v = T(j) * e(i, j - 1, t) - b2 * e(i, j + 1, t);
     else
-      v = (i * j) * e(i - 1, j - 1, t) - b2 * i * e(i - 1, j + 1, t) -
-          a2 * j * e(i + 1, j - 1, t) + a2 * b2 * e(i + 1, j + 1, t);
+      v = T(i * j) * e(i - 1, j - 1, t) - b2 * T(i) * e(i - 1, j + 1, t) -
+          a2 * T(j) * e(i + 1, j - 1, t) + a2 * b2 * e(i + 1, j + 1, t);
     f[t] = v;
   }
   return n;
@@ -133,24 +134,24 @@ __device__ __forceinline__ int axis_factor(const double* E, int l2r, int Lr, int
 
 // G[tuv] += s * sum f_x[tau] f_y[nu] f_z[phi] R_{t+tau,u+nu,v+phi} for
 // t+u+v <= Lb; the ket factors carry the (-1)^(tau+nu+phi) sign already.
-__device__ __forceinline__ void ket_add(double* G, double s, const double* fx, int nx,
-                                        const double* fy, int ny, const double* fz, int nz,
-                                        int Lb, const double* Rv) {
+template <typename T>
+__device__ __forceinline__ void ket_add(T* G, T s, const T* fx, int nx, const T* fy, int ny,
+                                        const T* fz, int nz, int Lb, const T* Rv) {
 #pragma unroll 1
   for (int t = 0; t <= Lb; t++)
 #pragma unroll 1
     for (int u = 0; u <= Lb - t; u++)
 #pragma unroll 1
       for (int v = 0; v <= Lb - t - u; v++) {
-        double acc = 0.0;
+        T acc = T(0);
 #pragma unroll 1
         for (int a = 0; a < nx; a++) {
-          const double fa = fx[a];
-          if (fa == 0.0) continue;
+          const T fa = fx[a];
+          if (fa == T(0)) continue;
 #pragma unroll 1
           for (int b = 0; b < ny; b++) {
-            const double fab = fa * fy[b];
-            if (fab == 0.0) continue;
+            const T fab = fa * fy[b];
+            if (fab == T(0)) continue;
 #pragma unroll 1
             for (int c = 0; c < nz; c++) acc += fab * fz[c] * Rv[hidx(t + a, u + b, v + c)];
           }
@@ -159,16 +160,17 @@ __device__ __forceinline__ void ket_add(double* G, double s, const double* fx, i
       }
 }
 
-__device__ __forceinline__ double bra_dot(const double* gx, int nx, const double* gy, int ny,
-                                          const double* gz, int nz, const double* G) {
-  double s = 0.0;
+template <typename T>
+__device__ __forceinline__ T bra_dot(const T* gx, int nx, const T* gy, int ny, const T* gz,
+                                     int nz, const T* G) {
+  T s = T(0);
 #pragma unroll 1
   for (int t = 0; t < nx; t++) {
-    if (gx[t] == 0.0) continue;
+    if (gx[t] == T(0)) continue;
 #pragma unroll 1
     for (int u = 0; u < ny; u++) {
-      const double gxy = gx[t] * gy[u];
-      if (gxy == 0.0) continue;
+      const T gxy = gx[t] * gy[u];
+      if (gxy == T(0)) continue;
 #pragma unroll 1
       for (int v = 0; v < nz; v++) s += gxy * gz[v] * G[hidx(t, u, v)];
     }
@@ -205,6 +207,10 @@ struct RelLaunch {
   const ShellDev* shells;
   const double* prim;
   const double* boys;
+  const float* boys32;
+  const float2* pairRange;  // per pair: FP32 range data (fp32_range_ok)
+  int mixed;      // 1: quartets with bound < cut run in FP32 (second launch)
+  double cut;
   int braBeg, nBra, ketBeg, nKet, same;
   int screen;
   double thresh;
@@ -349,9 +355,12 @@ __device__ __forceinline__ void rel_digest(const RelLaunch& a, const PairDev& P,
 // The ket's Cartesian component pairs (c, d) of a quartet are split over
 // nsplit threads (grid y = ket tiles x nsplit): the heavy classes with few
 // quartets (f shells) still fill the GPU.
-template <int LM, int TYPE>
+// T: primitive arithmetic (double; float for the small-bound quartets of a
+// mixed launch); operator components, digestion and accumulation in FP64.
+template <int LM, int TYPE, typename T>
 __global__ void __launch_bounds__(REL_THREADS)
     rel_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int nsplit) {
+  constexpr bool IS32 = sizeof(T) == 4;
   const int ib = blockIdx.x;
   const int split = blockIdx.y % nsplit;
   const int jk = (blockIdx.y / nsplit) * REL_THREADS + threadIdx.x;
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(REL_THREADS)
   const bool visited = jk < a.nKet && !(TYPE == 2 && a.same && jk > ib);
   const PairDev P = a.pairs[a.braBeg + ib];
   PairDev Q = P;
-  bool work = false;
+  bool work = false, mine = false;
   if (visited) {
     Q = a.pairs[a.ketBeg + jk];
     int s1, s2, s3, s4;
@@ -377,15 +386,22 @@ __global__ void __launch_bounds__(REL_THREADS)
       q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
     }
     // shMax * Q12 * Q34 < thresh (:947-948, :2059-2061)
-    work = !a.screen || sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34 >= a.thresh;
+    const double bound = sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34;
+    work = !a.screen || bound >= a.thresh;
+    const bool lo = a.mixed && bound < a.cut &&
+                    fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                                  __ldg(a.pairRange + a.ketBeg + jk),
+                                  la + lb + lc + ld + 2 + 2 * (TYPE == 2), 1, TYPE == 2);
+    mine = work && (IS32 ? lo : !lo);
   }
   if (split == 0) {
     const unsigned mask = __activemask();
     const unsigned bv = __ballot_sync(mask, visited), bw = __ballot_sync(mask, work);
+    const unsigned bm = __ballot_sync(mask, mine);
     if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
-      if (bv) atomicAdd(a.counters + 0, (unsigned long long)__popc(bv));
-      if (bv & ~bw) atomicAdd(a.counters + 1, (unsigned long long)__popc(bv & ~bw));
-      if (bw) atomicAdd(a.counters + 3, (unsigned long long)__popc(bw));
+      if (!IS32 && bv) atomicAdd(a.counters + 0, (unsigned long long)__popc(bv));
+      if (!IS32 && (bv & ~bw)) atomicAdd(a.counters + 1, (unsigned long long)__popc(bv & ~bw));
+      if (bm) atomicAdd(a.counters + (IS32 ? 2 : 3), (unsigned long long)__popc(bm));
     }
   }
 
@@ -399,7 +415,8 @@ __global__ void __launch_bounds__(REL_THREADS)
   const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
   const int nab = na * nb;
   const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
-  if (!work) return;
+  if (!mine) return;
+  const T* boysT = reinterpret_cast<const T*>(IS32 ? (const void*)a.boys32 : (const void*)a.boys);
 
   const int dK = (TYPE == 2) ? 1 : 0;
   const int Lb = la + lb + 2, Lk = lc + ld + 2 * dK, L = Lb + Lk;
@@ -413,12 +430,12 @@ __global__ void __launch_bounds__(REL_THREADS)
   const size_t nc = a.ncart;
   auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
 
-  double Ea[3][E1], Ec[3][E1];
-  double G[NB][HB];
-  double Rv[HL];
-  double F[4 * LM + 5];
+  T Ea[3][E1], Ec[3][E1];
+  T G[NB][HB];
+  T Rv[HL];
+  T F[4 * LM + 5];
   double acc[NCL * NCL * NC];
-  double fa[3][4][FL], fc[3][4][FL];
+  T fa[3][4][FL], fc[3][4][FL];
   int nfa[3][4], nfc[3][4];
 
 #pragma unroll 1
@@ -455,40 +472,40 @@ __global__ void __launch_bounds__(REL_THREADS)
         pair_exps(SA, SB, a.prim, ip, ea, eb);
 #pragma unroll 1
         for (int x = 0; x < 3; x++)
-          hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
-        const double p = A.p;
+          hermite_E_rt<T, LM + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[x]), T(A.PB[x]), Ea[x]);
+        const T p = T(A.p);
 #pragma unroll 1
         for (int b = 0; b < NB; b++)
 #pragma unroll 1
-          for (int h = 0; h < nherm(Lb); h++) G[b][h] = 0.0;
+          for (int h = 0; h < nherm(Lb); h++) G[b][h] = T(0);
 #pragma unroll 1
         for (int iq = 0; iq < Q.npp; iq++) {
           const PrimPairDev& B = a.pp[Q.pp_off + iq];
           double ec, ed;
           pair_exps(SC, SD, a.prim, iq, ec, ed);
-          const double q = B.p;
+          const T q = T(B.p);
 #pragma unroll 1
           for (int x = 0; x < 3; x++)
-            hermite_E_rt<double, LM + 1>(lc + dK, ld + dK, B.o2p, B.PA[x], B.PB[x], Ec[x]);
-          const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
-          const double pq = p + q, alpha = p * q / pq;
-          const double Targ = alpha * (X * X + Y * Y + Z * Z);
-          const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
-          boys_rt<double>(L, Targ, F, a.boys);
-          hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
+            hermite_E_rt<T, LM + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[x]), T(B.PB[x]), Ec[x]);
+          const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
+          const T pq = p + q, alpha = p * q / pq;
+          const T Targ = alpha * (X * X + Y * Y + Z * Z);
+          const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
+          boys_rt<T>(L, Targ, F, boysT);
+          hermite_R_rt<T>(L, alpha, X, Y, Z, F, Rv);
           const int ntk = (TYPE == 2) ? 4 : 1;
 #pragma unroll 1
           for (int x = 0; x < 3; x++)
 #pragma unroll 1
             for (int ty = 0; ty < ntk; ty++) {
-              nfc[x][ty] = axis_factor(Ec[x], ld + dK, lc + ld + 2 * dK + 1, ci[x], di[x], ty,
-                                       2.0 * ec, 2.0 * ed, fc[x][ty]);
+              nfc[x][ty] = axis_factor<T>(Ec[x], ld + dK, lc + ld + 2 * dK + 1, ci[x], di[x], ty,
+                                          T(2.0 * ec), T(2.0 * ed), fc[x][ty]);
 #pragma unroll 1
               for (int t = 1; t < nfc[x][ty]; t += 2) fc[x][ty][t] = -fc[x][ty][t];
             }
           if (TYPE == 1) {
-            ket_add(G[0], pref, fc[0][0], nfc[0][0], fc[1][0], nfc[1][0], fc[2][0], nfc[2][0],
-                    Lb, Rv);
+            ket_add<T>(G[0], pref, fc[0][0], nfc[0][0], fc[1][0], nfc[1][0], fc[2][0], nfc[2][0],
+                       Lb, Rv);
           } else {
 #pragma unroll 1
             for (int kk = 0; kk < 3; kk++)
@@ -499,8 +516,8 @@ __global__ void __launch_bounds__(REL_THREADS)
                 op_of(kk, ll, op, sg);
                 const int tx = (kk == 0) | ((ll == 0) << 1), ty = (kk == 1) | ((ll == 1) << 1),
                           tz = (kk == 2) | ((ll == 2) << 1);
-                ket_add(G[op < NB ? op : 0], sg * pref, fc[0][tx], nfc[0][tx], fc[1][ty],
-                        nfc[1][ty], fc[2][tz], nfc[2][tz], Lb, Rv);
+                ket_add<T>(G[op < NB ? op : 0], T(sg) * pref, fc[0][tx], nfc[0][tx], fc[1][ty],
+                           nfc[1][ty], fc[2][tz], nfc[2][tz], Lb, Rv);
               }
           }
         }
@@ -516,8 +533,8 @@ __global__ void __launch_bounds__(REL_THREADS)
             for (int x = 0; x < 3; x++)
 #pragma unroll 1
               for (int ty = 0; ty < 4; ty++)
-                nfa[x][ty] = axis_factor(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty, 2.0 * ea,
-                                         2.0 * eb, fa[x][ty]);
+                nfa[x][ty] = axis_factor<T>(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty,
+                                            T(2.0 * ea), T(2.0 * eb), fa[x][ty]);
             double mloc[NC];
             double* m = single ? mloc : acc + ab * NC;
             if (single)
@@ -534,8 +551,8 @@ __global__ void __launch_bounds__(REL_THREADS)
                           tz = (mu == 2) | ((nu == 2) << 1);
 #pragma unroll 1
                 for (int b = 0; b < NB; b++)
-                  m[op * NB + b] += sg * bra_dot(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty],
-                                                 fa[2][tz], nfa[2][tz], G[b]);
+                  m[op * NB + b] += sg * double(bra_dot<T>(fa[0][tx], nfa[0][tx], fa[1][ty],
+                                                           nfa[1][ty], fa[2][tz], nfa[2][tz], G[b]));
               }
             if (single) rel_digest<TYPE>(a, P, col, ai, bi, mloc, jcol);
           }
@@ -606,9 +623,10 @@ __host__ __device__ inline RelBlockLayout rel_block_layout(int la, int lb, int l
 // components of every bra component pair (one (ab, b) unit per thread) and
 // their digestion (one ab per thread), the per-column Coulomb sum reduced in
 // shared memory.  Same quartet set, screens and updates as rel_kernel.
-template <int TYPE>
+template <int TYPE, typename T>
 __global__ void __launch_bounds__(RB_THREADS)
     rel_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+  constexpr bool IS32 = sizeof(T) == 4;
   extern __shared__ double sm[];
   const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   int ib, jk;
@@ -626,7 +644,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
-  bool work;
+  bool work, mine;
   {
     int s1, s2, s3, s4;
     double q12, q34;
@@ -642,13 +660,21 @@ __global__ void __launch_bounds__(RB_THREADS)
       q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
       q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
     }
-    work = !a.screen || sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34 >= a.thresh;
+    const double bound = sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34;
+    work = !a.screen || bound >= a.thresh;
+    const bool lo = a.mixed && bound < a.cut &&
+                    fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                                  __ldg(a.pairRange + a.ketBeg + jk),
+                                  la + lb + lc + ld + 2 + 2 * (TYPE == 2), 1, TYPE == 2);
+    mine = work && (IS32 ? lo : !lo);
   }
   if (threadIdx.x == 0) {
-    atomicAdd(a.counters + 0, 1ull);
-    atomicAdd(a.counters + (work ? 3 : 1), 1ull);
+    if (!IS32) atomicAdd(a.counters + 0, 1ull);
+    if (!IS32 && !work) atomicAdd(a.counters + 1, 1ull);
+    if (mine) atomicAdd(a.counters + (IS32 ? 2 : 3), 1ull);
   }
-  if (!work) return;  // block-uniform
+  if (!mine) return;  // block-uniform
+  const T* boysT = reinterpret_cast<const T*>(IS32 ? (const void*)a.boys32 : (const void*)a.boys);
 
   constexpr int NB = (TYPE == 2) ? 4 : 1;
   constexpr int NC = 4 * NB;
@@ -659,14 +685,14 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int Lb = la + lb + 2, L = Lb + lc + ld + 2 * dK;
   const int FL = 2 * max(la, lb) + 3, FLk = 2 * max(lc, ld) + 3;
   const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
-  double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
-  double* Eb = sm + Lo.oEb;
-  double* Ek = sm + Lo.oEk;
-  double* fa = sm + Lo.oFa;
-  double* fc = sm + Lo.oFc;
-  double* G = sm + Lo.oG;
+  T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
+  T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
+  T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
+  T* fa = reinterpret_cast<T*>(sm + Lo.oFa);
+  T* fc = reinterpret_cast<T*>(sm + Lo.oFc);
+  T* G = reinterpret_cast<T*>(sm + Lo.oG);
   double* Mc = sm + Lo.oM;
-  double* Fs = sm + Lo.oF;
+  T* Fs = reinterpret_cast<T*>(sm + Lo.oF);
   double* Js = sm + Lo.oJ;
   const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
   const int E1k = (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK);
@@ -676,8 +702,9 @@ __global__ void __launch_bounds__(RB_THREADS)
   const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
   const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
   const size_t nc = a.ncart;
-  const double* R = Rb[0];  // R^(0) after the recursion
-  double ec = 0.0, ed = 0.0, pref = 0.0;
+  const T* R = Rb[0];  // R^(0) after the recursion
+  double ec = 0.0, ed = 0.0;
+  T pref = T(0);
 
   // E tables, R and the bra factors of primitive quartet (ip, iq)
   auto prep = [&](int ip, int iq) {
@@ -687,38 +714,39 @@ __global__ void __launch_bounds__(RB_THREADS)
     pair_exps(SA, SB, a.prim, ip, ea, eb);
     pair_exps(SC, SD, a.prim, iq, ec, ed);
     if (tid < 3)
-      hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid], Eb + tid * E1b);
+      hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
+                                Eb + tid * E1b);
     else if (tid < 6)
-      hermite_E_rt<double, LMAX + 1>(lc + dK, ld + dK, B.o2p, B.PA[tid - 3], B.PB[tid - 3],
-                                     Ek + (tid - 3) * E1k);
-    const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
-    const double pq = A.p + B.p, alpha = A.p * B.p / pq;
-    pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
-    if (tid == 6) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+      hermite_E_rt<T, LMAX + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[tid - 3]), T(B.PB[tid - 3]),
+                                Ek + (tid - 3) * E1k);
+    const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
+    const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
+    pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
+    if (tid == 6) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
     __syncthreads();
     // R^(n)_tuv, n = L .. 0, from R^(n+1); level n in Rb[n & 1]
-    const double m2a = -2.0 * alpha;
+    const T m2a = T(-2) * alpha;
     for (int n = L; n >= 0; n--) {
-      double* cur = Rb[n & 1];
-      const double* prv = Rb[(n + 1) & 1];
+      T* cur = Rb[n & 1];
+      const T* prv = Rb[(n + 1) & 1];
       const int cnt = nherm(L - n);
       for (int e = tid; e < cnt; e += RB_THREADS) {
         int t, u, v;
         hinv(e, t, u, v);
-        double val;
+        T val;
         if (e == 0) {
-          double f = 1.0;
+          T f = T(1);
           for (int k = 0; k < n; k++) f *= m2a;
           val = f * Fs[n];
         } else if (t > 0) {
           val = X * prv[hidx(t - 1, u, v)];
-          if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+          if (t > 1) val += T(t - 1) * prv[hidx(t - 2, u, v)];
         } else if (u > 0) {
           val = Y * prv[hidx(0, u - 1, v)];
-          if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+          if (u > 1) val += T(u - 1) * prv[hidx(0, u - 2, v)];
         } else {
           val = Z * prv[hidx(0, 0, v - 1)];
-          if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+          if (v > 1) val += T(v - 1) * prv[hidx(0, 0, v - 2)];
         }
         cur[e] = val;
       }
@@ -730,8 +758,8 @@ __global__ void __launch_bounds__(RB_THREADS)
       const int ai = ab / nb, bi = ab % nb;
       const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
       const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
-      axis_factor(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
-                  fa + (size_t)it * FL);
+      axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
+                     fa + (size_t)it * FL);
     }
     __syncthreads();
   };
@@ -755,9 +783,9 @@ __global__ void __launch_bounds__(RB_THREADS)
           const int x = tid / ntk, ty = tid % ntk;
           const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
           const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
-          double* f = fc + (x * 4 + ty) * FLk;
-          const int n = axis_factor(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
-                                    2.0 * ec, 2.0 * ed, f);
+          T* f = fc + (x * 4 + ty) * FLk;
+          const int n = axis_factor<T>(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
+                                       T(2.0 * ec), T(2.0 * ed), f);
           for (int t = 1; t < n; t += 2) f[t] = -f[t];
         }
         __syncthreads();
@@ -769,7 +797,7 @@ __global__ void __launch_bounds__(RB_THREADS)
           hinv(h, t, u, v);
           const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
           const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
-          double gsum = 0.0;
+          T gsum = T(0);
           for (int kk = 0; kk < (TYPE == 2 ? 3 : 1); kk++)
             for (int ll = 0; ll < (TYPE == 2 ? 3 : 1); ll++) {
               int op = 0;
@@ -782,22 +810,22 @@ __global__ void __launch_bounds__(RB_THREADS)
                 tyy = (kk == 1) | ((ll == 1) << 1);
                 tyz = (kk == 2) | ((ll == 2) << 1);
               }
-              const double* fx = fc + (0 * 4 + tyx) * FLk;
-              const double* fy = fc + (1 * 4 + tyy) * FLk;
-              const double* fz = fc + (2 * 4 + tyz) * FLk;
+              const T* fx = fc + (0 * 4 + tyx) * FLk;
+              const T* fy = fc + (1 * 4 + tyy) * FLk;
+              const T* fz = fc + (2 * 4 + tyz) * FLk;
               const int nx = ci[0] + di[0] + (tyx & 1) + (tyx >> 1) + 1;
               const int ny = ci[1] + di[1] + (tyy & 1) + (tyy >> 1) + 1;
               const int nz = ci[2] + di[2] + (tyz & 1) + (tyz >> 1) + 1;
-              double acc = 0.0;
+              T acc = T(0);
               for (int i = 0; i < nx; i++) {
-                if (fx[i] == 0.0) continue;
+                if (fx[i] == T(0)) continue;
                 for (int j = 0; j < ny; j++) {
-                  const double fxy = fx[i] * fy[j];
-                  if (fxy == 0.0) continue;
+                  const T fxy = fx[i] * fy[j];
+                  if (fxy == T(0)) continue;
                   for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
                 }
               }
-              gsum += sg * acc;
+              gsum += T(sg) * acc;
             }
           G[e] = pref * gsum;
         }
@@ -816,10 +844,10 @@ __global__ void __launch_bounds__(RB_THREADS)
               op_of(mu, nu, op, sg);
               const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
                         tz = (mu == 2) | ((nu == 2) << 1);
-              const double* gx = fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL;
-              const double* gy = fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL;
-              const double* gz = fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL;
-              m4[op] += sg * bra_dot(gx, ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1, gy,
+              const T* gx = fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL;
+              const T* gy = fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL;
+              const T* gz = fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL;
+              m4[op] += sg * (double)bra_dot<T>(gx, ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1, gy,
                                      ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1, gz,
                                      ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + b * hb);
             }
@@ -889,8 +917,10 @@ __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int
 // built at once, and the operator components of every (bra, ket) component
 // element are one work unit per thread (nab x ncd units); digestion per
 // element, the per-column Coulomb sums J_LL(C,D) reduced in shared memory.
+template <typename T>
 __global__ void __launch_bounds__(RB_THREADS)
     rel_llss_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
+  constexpr bool IS32 = sizeof(T) == 4;
   extern __shared__ double sm[];
   const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   const int ib = (int)(q / a.nKet), jk = (int)(q % a.nKet);
@@ -898,14 +928,21 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
-  const bool work = !a.screen ||
-      sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) * __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
-              __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns) >= a.thresh;
+  const double bound = sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) *
+                       __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
+                       __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns);
+  const bool work = !a.screen || bound >= a.thresh;
+  const bool lo = a.mixed && bound < a.cut &&
+                  fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                                __ldg(a.pairRange + a.ketBeg + jk), la + lb + lc + ld + 2, 1, 0);
+  const bool mine = work && (IS32 ? lo : !lo);
   if (threadIdx.x == 0) {
-    atomicAdd(a.counters + 0, 1ull);
-    atomicAdd(a.counters + (work ? 3 : 1), 1ull);
+    if (!IS32) atomicAdd(a.counters + 0, 1ull);
+    if (!IS32 && !work) atomicAdd(a.counters + 1, 1ull);
+    if (mine) atomicAdd(a.counters + (IS32 ? 2 : 3), 1ull);
   }
-  if (!work) return;  // block-uniform
+  if (!mine) return;  // block-uniform
+  const T* boysT = reinterpret_cast<const T*>(IS32 ? (const void*)a.boys32 : (const void*)a.boys);
 
   const int tid = threadIdx.x;
   const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
@@ -914,14 +951,14 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int hb = nherm(Lb);
   const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
   const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
-  double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
-  double* Eb = sm + Lo.oEb;
-  double* Ek = sm + Lo.oEk;
-  double* fa = sm + Lo.oFa;
-  double* fc = sm + Lo.oFc;
-  double* G = sm + Lo.oG;
+  T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
+  T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
+  T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
+  T* fa = reinterpret_cast<T*>(sm + Lo.oFa);
+  T* fc = reinterpret_cast<T*>(sm + Lo.oFc);
+  T* G = reinterpret_cast<T*>(sm + Lo.oG);
   double* Mc = sm + Lo.oM;
-  double* Fs = sm + Lo.oF;
+  T* Fs = reinterpret_cast<T*>(sm + Lo.oF);
   double* Js = sm + Lo.oJ;
   const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
   const int E1k = (lc + 1) * (ld + 1) * (lc + ld + 1);
@@ -931,7 +968,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const double s12d = dAB ? 1.0 : 2.0, s34d = dCD ? 1.0 : 2.0;
   const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
   const size_t nc = a.ncart;
-  const double* R = Rb[0];
+  const T* R = Rb[0];
 
   for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
   for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
@@ -946,38 +983,38 @@ __global__ void __launch_bounds__(RB_THREADS)
       pair_exps(SC, SD, a.prim, iq, ec, ed);
       __syncthreads();  // the previous primitive quartet's readers are done
       if (tid < 3)
-        hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid],
-                                       Eb + tid * E1b);
+        hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
+                                  Eb + tid * E1b);
       else if (tid < 6)
-        hermite_E_rt<double, LMAX + 1>(lc, ld, B.o2p, B.PA[tid - 3], B.PB[tid - 3],
-                                       Ek + (tid - 3) * E1k);
-      const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
-      const double pq = A.p + B.p, alpha = A.p * B.p / pq;
-      const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
-      if (tid == 6) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+        hermite_E_rt<T, LMAX + 1>(lc, ld, T(B.o2p), T(B.PA[tid - 3]), T(B.PB[tid - 3]),
+                                  Ek + (tid - 3) * E1k);
+      const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
+      const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
+      const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
+      if (tid == 6) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
       __syncthreads();
-      const double m2a = -2.0 * alpha;
+      const T m2a = T(-2) * alpha;
       for (int n = L; n >= 0; n--) {
-        double* cur = Rb[n & 1];
-        const double* prv = Rb[(n + 1) & 1];
+        T* cur = Rb[n & 1];
+        const T* prv = Rb[(n + 1) & 1];
         const int cnt = nherm(L - n);
         for (int e = tid; e < cnt; e += RB_THREADS) {
           int t, u, v;
           hinv(e, t, u, v);
-          double val;
+          T val;
           if (e == 0) {
-            double f = 1.0;
+            T f = T(1);
             for (int k = 0; k < n; k++) f *= m2a;
             val = f * Fs[n];
           } else if (t > 0) {
             val = X * prv[hidx(t - 1, u, v)];
-            if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+            if (t > 1) val += T(t - 1) * prv[hidx(t - 2, u, v)];
           } else if (u > 0) {
             val = Y * prv[hidx(0, u - 1, v)];
-            if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+            if (u > 1) val += T(u - 1) * prv[hidx(0, u - 2, v)];
           } else {
             val = Z * prv[hidx(0, 0, v - 1)];
-            if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+            if (v > 1) val += T(v - 1) * prv[hidx(0, 0, v - 2)];
           }
           cur[e] = val;
         }
@@ -990,15 +1027,15 @@ __global__ void __launch_bounds__(RB_THREADS)
         const int ai = ab / nb, bi = ab % nb;
         const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
         const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
-        axis_factor(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
-                    fa + (size_t)it * FL);
+        axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
+                       fa + (size_t)it * FL);
       }
       for (int it = tid; it < ncd * 3; it += RB_THREADS) {
         const int cd = it / 3, x = it % 3, c = cd / nd, d = cd % nd;
         const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
         const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
-        double* f = fc + (size_t)it * FLk;
-        const int n = axis_factor(Ek + x * E1k, ld, lc + ld + 1, ci, di, 0, 0.0, 0.0, f);
+        T* f = fc + (size_t)it * FLk;
+        const int n = axis_factor<T>(Ek + x * E1k, ld, lc + ld + 1, ci, di, 0, T(0), T(0), f);
         for (int t = 1; t < n; t += 2) f[t] = -f[t];
       }
       __syncthreads();
@@ -1007,18 +1044,18 @@ __global__ void __launch_bounds__(RB_THREADS)
         const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
         int t, u, v;
         hinv(h, t, u, v);
-        const double* fx = fc + (size_t)(cd * 3 + 0) * FLk;
-        const double* fy = fc + (size_t)(cd * 3 + 1) * FLk;
-        const double* fz = fc + (size_t)(cd * 3 + 2) * FLk;
+        const T* fx = fc + (size_t)(cd * 3 + 0) * FLk;
+        const T* fy = fc + (size_t)(cd * 3 + 1) * FLk;
+        const T* fz = fc + (size_t)(cd * 3 + 2) * FLk;
         const int nx = cart_lx(lc, c) + cart_lx(ld, d) + 1;
         const int ny = cart_ly(lc, c) + cart_ly(ld, d) + 1;
         const int nz = cart_lz(lc, c) + cart_lz(ld, d) + 1;
-        double acc = 0.0;
+        T acc = T(0);
         for (int i = 0; i < nx; i++) {
-          if (fx[i] == 0.0) continue;
+          if (fx[i] == T(0)) continue;
           for (int j = 0; j < ny; j++) {
-            const double fxy = fx[i] * fy[j];
-            if (fxy == 0.0) continue;
+            const T fxy = fx[i] * fy[j];
+            if (fxy == T(0)) continue;
             for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
           }
         }
@@ -1039,7 +1076,7 @@ __global__ void __launch_bounds__(RB_THREADS)
             op_of(mu, nu, op, sg);
             const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
                       tz = (mu == 2) | ((nu == 2) << 1);
-            m4[op] += sg * bra_dot(fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL,
+            m4[op] += sg * (double)bra_dot<T>(fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL,
                                    ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1,
                                    fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL,
                                    ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1,
@@ -1067,9 +1104,11 @@ __global__ void __launch_bounds__(RB_THREADS)
                 w34 * s12d * Js[cd]);
 }
 
-template <int TYPE>
-void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
-  if (a.nBra == 0 || a.nKet == 0) return;
+// One class in one arithmetic precision: the instance in T computes the
+// quartets that precision owns (every surviving one for double without the
+// mixed mode; with it, double takes bound >= cut and float the rest).
+template <int TYPE, typename T>
+void launch_rel_prec(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
   const int tiles = (a.nKet + REL_THREADS - 1) / REL_THREADS;
   // split each quartet's ket components over enough threads to fill the GPU
   // (~256k threads per launch), at most one component pair per thread
@@ -1080,7 +1119,7 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
   dim3 grid(a.nBra, tiles * nsplit);
   const int lm = std::max(std::max(la, lb), std::max(lc, ld));
   if (lm <= 1) {
-    rel_kernel<1, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+    rel_kernel<1, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     return;
   }
   if (TYPE == 1) {
@@ -1090,16 +1129,16 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
     const size_t smem = (size_t)Lo.total * sizeof(double);
     if (smem <= 160 * 1024) {
       if (smem > 48 * 1024)
-        cudaFuncSetAttribute(rel_llss_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(rel_llss_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
       const long long nq = (long long)a.nBra * a.nKet;
       const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
       const unsigned gy = (unsigned)((nq + gx - 1) / gx);
-      rel_llss_block_kernel<<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+      rel_llss_block_kernel<T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
     } else if (lm == 2) {
-      rel_kernel<2, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+      rel_kernel<2, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     } else {
-      rel_kernel<3, TYPE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
+      rel_kernel<3, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     }
     return;
   }
@@ -1107,13 +1146,20 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
   const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
   const size_t smem = (size_t)Lo.total * sizeof(double);
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute(rel_block_kernel<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(rel_block_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
   const long long nq = (TYPE == 2 && a.same) ? (long long)a.nBra * (a.nBra + 1) / 2
                                              : (long long)a.nBra * a.nKet;
   const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
   const unsigned gy = (unsigned)((nq + gx - 1) / gx);
-  rel_block_kernel<TYPE><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+  rel_block_kernel<TYPE, T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+}
+
+template <int TYPE>
+void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
+  if (a.nBra == 0 || a.nKet == 0) return;
+  launch_rel_prec<TYPE, double>(a, la, lb, lc, ld, st);
+  if (a.mixed) launch_rel_prec<TYPE, float>(a, la, lb, lc, ld, st);
 }
 
 // ------------------------------------------------------------ 4C Schwarz
@@ -1454,15 +1500,20 @@ cqf_status ensure_relws(cqf_basis* B, size_t bytes) {
 size_t align32(size_t n) { return (n + 31) / 32 * 32; }
 
 // One contraction type on device pointers (X, AX: 17 entries, N x N complex).
-// ws: device scratch of rel_ws_doubles() doubles.
+// ws: device scratch of rel_ws_doubles() doubles.  From opts: screen, and
+// precision / fp32_cutoff (CQF_MIXED: quartets whose screening bound is below
+// the cutoff run in FP32 arithmetic, the rest in FP64).  cnt: total,
+// screened, FP32, FP64 quartet counts, added to.
 size_t rel_ws_doubles(const cqf_basis* B) {
   const size_t nc2 = (size_t)B->ncart * B->ncart, ns2 = (size_t)B->nshell * B->nshell;
   return align32(9 * 2 * nc2) + align32(13 * nc2) + align32(10 * ns2) + 64;
 }
 
 cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int type,
-                            int exch, int screen, cudaStream_t st, double* ws,
+                            int exch, const cqf_opts& opts, cudaStream_t st, double* ws,
                             unsigned long long* cnt) {
+  const int screen = opts.screen;
+  const bool mixed = opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
   for (int m = 0; m < CQF_REL_NMAT; m++)
@@ -1488,6 +1539,8 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
     o.is_complex = 1;
     o.device_pointers = 1;
     o.screen = screen;
+    o.precision = opts.precision;
+    o.fp32_cutoff = opts.fp32_cutoff;
     o.stream = st;
     CQF_RTRY(basis_workspace(B, ws_layout(B, (int)list.size(), o).total * sizeof(double)));
     cqf_stats s1{};
@@ -1495,6 +1548,7 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
                            static_cast<double*>(B->d_ws), false, nullptr));
     cnt[0] += s1.quartets_total;
     cnt[1] += s1.quartets_screened;
+    cnt[2] += s1.quartets_fp32;
     cnt[3] += s1.quartets_fp64;
     return CQF_OK;
   }
@@ -1553,6 +1607,10 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   a.shells = B->d_shells;
   a.prim = B->d_prim;
   a.boys = B->d_boys64;
+  a.boys32 = B->d_boys32;
+  a.pairRange = B->d_pairRange;
+  a.mixed = mixed ? 1 : 0;
+  a.cut = opts.fp32_cutoff;
   a.screen = screen;
   a.thresh = B->thresh;
   a.norms = nrm;
@@ -1603,6 +1661,7 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   CQF_RCUDA(cudaStreamSynchronize(st));
   cnt[0] += h[0];
   cnt[1] += h[1];
+  cnt[2] += h[2];
   cnt[3] += h[3];
   return CQF_OK;
 }
@@ -1649,7 +1708,7 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
   }
   CQF_RCUDA(cudaEventRecord(B->ev0, st));
   unsigned long long cnt[4] = {0, 0, 0, 0};
-  CQF_RTRY(rel_contract_dev(B, Xd, AXd, type, compute_exchange, o.screen, st, ws, cnt));
+  CQF_RTRY(rel_contract_dev(B, Xd, AXd, type, compute_exchange, o, st, ws, cnt));
   CQF_RCUDA(cudaEventRecord(B->ev1, st));
   if (!o.device_pointers)
     for (int m = 0; m < CQF_REL_NMAT; m++)
@@ -1660,7 +1719,7 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
   if (stats) {
     stats->quartets_total = (long long)cnt[0];
     stats->quartets_screened = (long long)cnt[1];
-    stats->quartets_fp32 = 0;
+    stats->quartets_fp32 = (long long)cnt[2];
     stats->quartets_fp64 = (long long)cnt[3];
     float ms = 0.f;
     cudaEventElapsedTime(&ms, B->ev0, B->ev1);
@@ -1749,20 +1808,20 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
   };
   unsigned long long cnt[4] = {0, 0, 0, 0};
   if (dc.bare_coulomb) {  // impl.hpp:3895-3969
-    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_BARE_COULOMB, exch, o.screen, st, ws, cnt));
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_BARE_COULOMB, exch, o, st, ws, cnt));
     add(H(0), 0, 0, AX[CQF_CLLMS], dc.libcint ? 2.0 : 1.0);
     if (exch)
       for (int c = 0; c < 4; c++) add(Kk(c), 0, 0, AX[CQF_XLLMS + c], 1.0);
   }
   if (dc.dirac_coulomb) {  // impl.hpp:4003-4147
-    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_LLSS, exch, o.screen, st, ws, cnt));
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_LLSS, exch, o, st, ws, cnt));
     add(H(0), 0, 0, AX[CQF_CLLMS], 2.0 * C2);
     for (int c = 0; c < 4; c++) add(H(c), N, N, AX[CQF_CSSMS + c], 2.0 * C2);
     if (exch)
       for (int c = 0; c < 4; c++) add(Kk(c), 0, N, AX[CQF_XLSMS + c], -C2);
   }
   if (dc.dirac_coulomb_ssss) {  // impl.hpp:4149-4233
-    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_SSSS, exch, o.screen, st, ws, cnt));
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_SSSS, exch, o, st, ws, cnt));
     for (int c = 0; c < 4; c++) add(H(c), N, N, AX[CQF_CSSMS + c], 2.0 * C4);
     if (exch)
       for (int c = 0; c < 4; c++) add(Kk(c), N, N, AX[CQF_XSSMS + c], -C4);
@@ -1780,7 +1839,7 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
   if (stats) {
     stats->quartets_total = (long long)cnt[0];
     stats->quartets_screened = (long long)cnt[1];
-    stats->quartets_fp32 = 0;
+    stats->quartets_fp32 = (long long)cnt[2];
     stats->quartets_fp64 = (long long)cnt[3];
     float ms = 0.f;
     cudaEventElapsedTime(&ms, B->ev0, B->ev1);

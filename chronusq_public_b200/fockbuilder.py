@@ -87,6 +87,7 @@ class FourCompFock:
         self.last_stats = None
 
     def formGD(self, D: List, xHFX: float = 1.0, screen: bool = True,
+               precision: str = "fp64", fp32_cutoff: float = 0.0,
                stream=None) -> List:
         import ctypes as C
 
@@ -128,6 +129,8 @@ class FourCompFock:
         _cabi.lib().cqf_opts_default(C.byref(opts))
         opts.is_complex = 1
         opts.screen = 1 if screen else 0
+        opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
+        opts.fp32_cutoff = float(fp32_cutoff)
         opts.device_pointers = 1 if dev else 0
         opts.stream = _stream_arg(stream)
         st = _cabi.CqfStats()

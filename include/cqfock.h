@@ -173,9 +173,11 @@ typedef enum { CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2 } cq
  *         compute_exchange, AX[XLSM*] (:810-1441)
  *   SSSS: AX[CSSM*] and, with compute_exchange, AX[XSSM*] (:1841-2832).
  * Entries a type does not read or write may be NULL.  The densities must be
- * Hermitian, as the reference requires (:144-145).  opts->is_complex and
- * opts->precision are ignored (complex, FP64); opts->device_pointers and
- * opts->stream apply. */
+ * Hermitian, as the reference requires (:144-145).  opts->is_complex is
+ * ignored (always complex); opts->device_pointers, opts->stream, opts->screen
+ * apply, and opts->precision = CQF_MIXED runs the quartets whose screening
+ * bound is below opts->fp32_cutoff in FP32 arithmetic (digestion and
+ * accumulation stay FP64; the reference is FP64 throughout). */
 cqf_status cqf_rel_two_body_contract(cqf_basis* basis, const void* const* X, void* const* AX,
                                      int type, int compute_exchange, const cqf_opts* opts,
                                      cqf_stats* stats);
@@ -195,7 +197,9 @@ void cqf_dc_opts_default(cqf_dc_opts* o);
  * 2N x 2N complex 4C density (column-major, LL block first); G[4] receives
  * twoeH - xHFX K with the 2C^2 / -C^2 / 2C^4 / -C^4 weights of the LLSS and
  * SSSS terms, twoeH_LL = 2 J (libcint) or J, and the SL blocks set to the
- * conjugate transpose of the LS blocks. */
+ * conjugate transpose of the LS blocks.  opts as for
+ * cqf_rel_two_body_contract (CQF_MIXED applies to every contraction type of
+ * the build, the bare-Coulomb one included). */
 cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const* G,
                             const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 

@@ -34,3 +34,45 @@ def readden_rhf_basis(g=None):
 CONTRACT_CASES = ["HER_REAL_J", "NONHER_REAL_J", "HER_REAL_K", "NONHER_REAL_K",
                   "HER_COMPLEX_J", "NONHER_COMPLEX_J", "HER_COMPLEX_K",
                   "NONHER_COMPLEX_K"]
+
+
+# Two centres with very tight d shells (exponent 1e5) beside ordinary ones:
+# in FP32 the Hermite recursion of the tight-tight quartets would overflow
+# ((2 alpha)^L past 2^128) while F_n(T) underflows, so the mixed path must
+# keep them in FP64 whatever their screening bound.
+TIGHT_D_BASIS = """
+****
+He 0
+S 2 1.00
+  4.0 0.4
+  0.9 0.7
+P 1 1.00
+  1.1 1.0
+D 1 1.00
+  1.0e5 1.0
+D 1 1.00
+  0.8 1.0
+****
+H 0
+S 1 1.00
+  0.5 1.0
+D 1 1.00
+  1.0e5 1.0
+****
+"""
+
+
+def tight_d_basis():
+    mol = Molecule.from_angstrom([("He", 0.0, 0.0, 0.0), ("H", 0.4, -0.3, 1.3)])
+    return BasisSet.build(mol, parse_gbs(TIGHT_D_BASIS))
+
+
+def tight_ao_scale(basis, damp=1e-5):
+    """Per-AO factor: `damp` on the AOs of shells with an exponent above
+    1e4, 1 elsewhere (a density scaled by it on rows and columns has tiny
+    blocks on the tight shells, so their quartets' bounds are small)."""
+    f = np.ones(basis.nbasis)
+    for s, sh in enumerate(basis.shells):
+        if sh.alpha.max() > 1e4:
+            f[basis.offsets[s]:basis.offsets[s] + sh.size] = damp
+    return f

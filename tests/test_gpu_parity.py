@@ -13,7 +13,7 @@ from chronusq_public_b200.contraction import (  # noqa: E402
 from chronusq_public_b200.fockbuilder import (FockBuilder,  # noqa: E402
                                               two_electron_energy)
 from helpers import (CONTRACT_CASES, contract_basis, golden,  # noqa: E402
-                     readden_rhf_basis)
+                     readden_rhf_basis, tight_ao_scale, tight_d_basis)
 
 FP64_TOL = 1e-9
 
@@ -115,6 +115,26 @@ def test_mixed_precision_within_1e6():
     assert s["fp32"] > 0
     assert np.abs(Gm - G64).max() <= 1e-6
     assert abs(two_electron_energy(Gm, D) - two_electron_energy(G64, D)) <= 1e-6
+
+
+def test_mixed_precision_tight_primitives():
+    """Quartets of very tight shells stay in FP64 on the mixed path even when
+    their bound is below the cut (FP32 would overflow there)."""
+    basis = tight_d_basis()
+    tpi = DirectTPI(basis)
+    ob = O.OracleBasis(basis)
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((basis.nbasis, basis.nbasis))
+    f = tight_ao_scale(basis)
+    D = 0.1 * (A + A.T) * f[:, None] * f[None, :]
+    Jo, Ko = ob.contract([D, D], [1, 1], [0, 1])
+    fb = FockBuilder(tpi)
+    G, J, K = fb.formRawGD(D, precision="mixed", fp32_cutoff=1e-2)
+    s = fb.contraction.last_stats
+    assert s["fp32"] > 0 and s["fp64"] > 0, s
+    assert np.isfinite(G).all()
+    assert np.abs(J - Jo).max() <= 1e-6
+    assert np.abs(K - Ko).max() <= 1e-6
 
 
 def _dev(a):

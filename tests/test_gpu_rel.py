@@ -10,7 +10,8 @@ from chronusq_public_b200.contraction import (BARE_COULOMB, LLSS, SSSS, DirectTP
                                               GTODirectRelERIContraction,
                                               TwoBodyContraction)
 from chronusq_public_b200.fockbuilder import FourCompFock
-from helpers import golden, water_ref
+from chronusq_public_b200.workloads import SPEED_OF_LIGHT
+from helpers import golden, tight_ao_scale, tight_d_basis, water_ref
 
 pytestmark = pytest.mark.gpu
 
@@ -183,3 +184,78 @@ def test_four_comp_gd_hermitian(fsys):
     G = FourCompFock(tpi).formGD(D, xHFX=0.7)
     for k in range(4):
         assert np.abs(G[k] - G[k].conj().T).max() < 1e-9 * max(1.0, np.abs(G[k]).max())
+
+
+# Mixed precision: quartets whose screening bound is below the cutoff run in
+# FP32 arithmetic; the build must stay within 1e-6 Eh of the FP64 oracle.
+MIXED_TOL = 1e-6
+MIXED_CUT = 1e-2
+# weight of each type's output in G (impl.hpp:3895-4636): 2 for the bare
+# Coulomb J (libcint), 2 C^2 for LLSS, 2 C^4 for SSSS (C^2 = 1 / 4c^2), so
+# the raw contraction's deviation times it is the deviation in Eh
+_C2 = 1.0 / (4.0 * SPEED_OF_LIGHT ** 2)
+FOCK_WEIGHT = {BARE_COULOMB: 2.0, LLSS: 2.0 * _C2, SSSS: 2.0 * _C2 * _C2}
+
+
+@pytest.mark.parametrize("sysname,ctype", [("w631", BARE_COULOMB), ("w631", LLSS),
+                                           ("w631", SSSS), ("fsys", LLSS), ("fsys", SSSS)])
+def test_rel_contract_mixed(request, sysname, ctype):
+    bs, tpi, ob = request.getfixturevalue(sysname)
+    N = bs.nbasis
+    _D, X = rel_inputs(N, 41 + ctype)
+    ref = ob.rel_contract(X, ctype, True)
+    c = GTODirectRelERIContraction(tpi)
+    split = False
+    # the small-component bounds carry c^-2 and c^-4 factors: sweep the
+    # cutoff so that some launch splits its quartets between both precisions
+    for cut in [MIXED_CUT * 10.0 ** -k for k in range(11)]:
+        lst = [TwoBodyContraction(X[m], np.zeros((N, N), complex)) for m in range(17)]
+        c.twoBodyContract(lst, ctype, precision="mixed", fp32_cutoff=cut)
+        st = c.last_stats
+        if cut == MIXED_CUT:
+            assert st["fp32"] > 0, st
+        split |= st["fp32"] > 0 and st["fp64"] > 0
+        assert st["fp32"] + st["fp64"] + st["screened"] == st["total"], st
+        for m in OUTS[ctype]:
+            err = FOCK_WEIGHT[ctype] * np.abs(lst[m].AX - ref[m]).max()
+            assert err < MIXED_TOL, (cut, m, err)
+    assert split
+
+
+def test_four_comp_gd_mixed(w631):
+    bs, tpi, ob = w631
+    D, _X = rel_inputs(bs.nbasis, 13)
+    ref = ob.dirac_coulomb(D, bare=True, dc=True, ssss=True, libcint=True)
+    fb = FourCompFock(tpi)
+    G = fb.formGD(D, precision="mixed", fp32_cutoff=MIXED_CUT)
+    smx = fb.last_stats
+    assert smx["fp32"] > 0
+    for k in range(4):
+        assert np.abs(G[k] - ref[k]).max() < MIXED_TOL, k
+    # FP64 and mixed builds visit and screen the same quartets
+    fb.formGD(D)
+    s64 = fb.last_stats
+    assert s64["fp32"] == 0
+    assert (s64["total"], s64["screened"]) == (smx["total"], smx["screened"])
+    assert s64["fp64"] == smx["fp64"] + smx["fp32"]
+
+
+@pytest.mark.parametrize("ctype", [BARE_COULOMB, LLSS, SSSS])
+def test_rel_contract_mixed_tight_primitives(ctype):
+    """Very tight d shells (exponent 1e5) with damped density blocks: their
+    quartets fall below the cut but must stay in FP64 (FP32 overflows)."""
+    bs = tight_d_basis()
+    tpi, ob = DirectTPI(bs), O.OracleBasis(bs)
+    N = bs.nbasis
+    f = tight_ao_scale(bs)
+    _D, X = rel_inputs(N, 51 + ctype)
+    X = [np.asfortranarray(x * f[:, None] * f[None, :]) for x in X]
+    ref = ob.rel_contract(X, ctype, True)
+    lst = [TwoBodyContraction(X[m], np.zeros((N, N), complex)) for m in range(17)]
+    c = GTODirectRelERIContraction(tpi)
+    c.twoBodyContract(lst, ctype, precision="mixed", fp32_cutoff=MIXED_CUT)
+    assert c.last_stats["fp32"] > 0, c.last_stats
+    for m in OUTS[ctype]:
+        assert np.isfinite(lst[m].AX).all(), m
+        err = FOCK_WEIGHT[ctype] * np.abs(lst[m].AX - ref[m]).max()
+        assert err < MIXED_TOL, (m, err)
