@@ -14,6 +14,11 @@ value   = builds/s of the mixed-precision build (FP32 for quartets whose
 e2e     = the same build through the public Python API with host (numpy)
           buffers: H2D of D, D2H of J and K inside the timed region.
 fp64    = the same, all quartets in FP64 (the reference precision).
+cutoff_sweep = the mixed build at the configuration's cutoffs 1e-6 .. 1e-10
+          (builds/s, FP32 quartets, Fock and energy error).
+batched_dD_graph = (H2O)8 / cc-pVDZ, 64 dD densities per CUDA-graph launch,
+          FP64 and mixed, beside the same work one density per call in FP64
+          (mixed_batched_over_fp64_single: the batched mixed rate over it).
 Errors  = max |G - G_oracle| and |E2 - E2_oracle| against the CPU oracle
           (FP64), computed once outside the timed region.
 
@@ -181,8 +186,31 @@ def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64):
     for k in range(ndens):
         cont.append(TwoBodyContraction(X[k], out[2 * k], True, COULOMB))
         cont.append(TwoBodyContraction(X[k], out[2 * k + 1], True, EXCHANGE))
-    g = ContractionGraph(tpi, cont, precision=precision, fp32_cutoff=cutoff)
     stream = torch.cuda.Stream(dev)
+    single = None
+    if precision == "fp64":
+        # the same work one density per call (J and K of dD_0, FP64, no
+        # graph): the FP64 GPU build the batched rate is compared with
+        from chronusq_public_b200.contraction import GTODirectTPIContraction
+        con = GTODirectTPIContraction(tpi)
+        one = [TwoBodyContraction(X[0], out[0], True, COULOMB),
+               TwoBodyContraction(X[0], out[1], True, EXCHANGE)]
+        for _ in range(warmup):
+            con.twoBodyContract(one, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        ms1 = []
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            con.twoBodyContract(one, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms1.append(e0.elapsed_time(e1))
+        t1 = float(np.median(ms1)) / 1e3
+        single = {"ms_per_build": t1 * 1e3, "builds_per_s": 1.0 / t1,
+                  "what": "one dD per call (J+K), FP64, no graph"}
+    g = ContractionGraph(tpi, cont, precision=precision, fp32_cutoff=cutoff)
     for _ in range(warmup):
         g.launch(stream.cuda_stream)
     torch.cuda.synchronize()
@@ -197,9 +225,12 @@ def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64):
         ms.append(e0.elapsed_time(e1))
     g.close()
     t = float(np.median(ms)) / 1e3
-    return {"workload": "h2o8_ccpvdz x 64 dD (J+K), CUDA graph", "nbasis": N,
-            "densities_per_launch": ndens, "ms_per_launch": t * 1e3,
-            "builds_per_s": ndens / t, "precision": precision, "fp32_cutoff": cutoff}
+    res = {"workload": "h2o8_ccpvdz x 64 dD (J+K), CUDA graph", "nbasis": N,
+           "densities_per_launch": ndens, "ms_per_launch": t * 1e3,
+           "builds_per_s": ndens / t, "precision": precision, "fp32_cutoff": cutoff}
+    if single:
+        res["fp64_single_density"] = single
+    return res
 
 
 def run_serving(dev, nreq, rate, cutoff):
@@ -244,6 +275,7 @@ def run_serving(dev, nreq, rate, cutoff):
     return {"requests": nreq, "arrival_rate_hz": rate, "wall_s": wall,
             "builds_per_s": nreq / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "mean_ms": st["mean_ms"], "fp32_cutoff": cutoff,
+            "phases_ms": {k: st[k] for k in ("queue_ms", "setup_ms", "build_ms") if k in st},
             "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
 
 
@@ -525,10 +557,17 @@ def main():
         G = (2 * Jd - Kd).t().contiguous().t().cpu().numpy()
         return ms, G, dict(con.last_stats)
 
-    ms64, G64, st64 = run("fp64", 0.0, args.steps, args.warmup)
     with ClockSampler(local) as clk:
+        ms64, G64, st64 = run("fp64", 0.0, args.steps, args.warmup)
         msmx, Gmx, stmx = run("mixed", args.cutoff, args.steps, args.warmup)
     clocks = clk.summary()
+    # the configuration's cutoff sweep (1e-6 .. 1e-10): builds/s and, below,
+    # the Fock and energy errors of each
+    sweep = []
+    for cut in (1e-6, 1e-7, 1e-8, 1e-9, 1e-10):
+        msc, Gc, stc = run("mixed", cut, max(3, args.steps // 2), 1)
+        sweep.append({"fp32_cutoff": cut, "builds_per_s": 1e3 * len(msc) / sum(msc),
+                      "quartets_fp32": stc["fp32"], "G": Gc})
 
     # end-to-end through the public API with host buffers
     fb = FockBuilder(tpi)
@@ -573,6 +612,9 @@ def main():
     if args.batched:
         batched = {"fp64": run_batched(dev, args.steps, args.warmup),
                    "mixed": run_batched(dev, args.steps, args.warmup, "mixed", args.cutoff)}
+        batched["mixed_batched_over_fp64_single"] = (
+            batched["mixed"]["builds_per_s"]
+            / batched["fp64"]["fp64_single_density"]["builds_per_s"])
     serving = None
     if args.serving_requests > 0:
         serving = run_serving(dev, args.serving_requests, args.serving_rate, args.cutoff)
@@ -588,6 +630,12 @@ def main():
                                        - two_electron_energy(Go, D)),
                "energy_err_fp64": abs(two_electron_energy(G64, D)
                                       - two_electron_energy(Go, D))}
+    Gref = cpu["G"] if cpu else G64
+    for sw in sweep:
+        Gc = sw.pop("G")
+        sw["fock_maxabs"] = float(np.abs(Gc - Gref).max())
+        sw["energy_err"] = abs(two_electron_energy(Gc, D) - two_electron_energy(Gref, D))
+        sw["errors_against"] = "oracle" if cpu else "FP64 GPU build"
     # kernels per build: block norms x2, max, norms_aux, to_cart x2, one per
     # class pair, back transform x2
     ncls = len({(max(a.l, b.l), min(a.l, b.l)) for a in basis.shells for b in basis.shells})
@@ -604,6 +652,7 @@ def main():
         "fp64": {"value": v64, "unit": "builds/s", "ms_per_step": 1e3 * t64 / K,
                  "roofline_frac": frac64},
         "mixed_over_fp64": vmx / v64,
+        "cutoff_sweep": sweep,
         "latency_ms": {"p50": float(np.percentile(msmx, 50)),
                        "p99": float(np.percentile(msmx, 99))},
         "errors_vs_oracle": err,

@@ -283,6 +283,68 @@ __global__ void gather_pairs_kernel(const PairDev* in, const int* idx, int n, Pa
   if (k < n) out[k] = in[idx[k]];
 }
 
+// Primitive pairs of pair i moved from src[i] to pairs[i].pp_off (the order
+// of the Schwarz-sorted pair list); one thread per pair.
+__global__ void reorder_pp_kernel(const PrimPairDev* __restrict__ in, const PairDev* pairs,
+                                  const long long* __restrict__ src, int n,
+                                  PrimPairDev* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const PairDev P = pairs[i];
+  for (int k = 0; k < P.npp; k++) out[P.pp_off + k] = in[src[i] + k];
+}
+
+// FP32 range data of each pair: log2 of 2 max p and of max |Kp| over its
+// primitive pairs (fp32_range_ok).
+__global__ void pair_range_kernel(const PrimPairDev* __restrict__ pp, const PairDev* pairs,
+                                  int n, float2* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const PairDev P = pairs[i];
+  double pm = 0.0, km = 0.0;
+  for (int k = 0; k < P.npp; k++) {
+    pm = fmax(pm, pp[P.pp_off + k].p);
+    km = fmax(km, fabs(pp[P.pp_off + k].Kp));
+  }
+  out[i] = make_float2((float)log2(fmax(2.0 * pm, 1e-30)), (float)log2(fmax(km, 1e-60)));
+}
+
+// Tile-interleaved ket data: one block per ket tile (KETT_TILE consecutive
+// pairs of a class starting at pair tileFirst[t], tileCnt[t] of them), lane
+// l = thread; field f of primitive iq of lane l at
+// out[tileOff[t] + (iq * KETT_NF + f) * KETT_TILE + l], zero past the pair's
+// primitives, for iq below the tile's largest primitive count.
+__global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp, const PairDev* pairs,
+                                 const int* __restrict__ tileFirst,
+                                 const int* __restrict__ tileCnt,
+                                 const long long* __restrict__ tileOff, double* out) {
+  const int t = blockIdx.x, l = threadIdx.x;
+  const long long base = tileOff[t];
+  const int mx = (int)((tileOff[t + 1] - base) / (KETT_NF * KETT_TILE));
+  const bool have = l < tileCnt[t];
+  int npp = 0, off = 0;
+  if (have) {
+    const PairDev P = pairs[tileFirst[t] + l];
+    npp = P.npp;
+    off = P.pp_off;
+  }
+  for (int iq = 0; iq < mx; iq++) {
+    double f[KETT_NF];
+    if (iq < npp) {
+      const PrimPairDev r = pp[off + iq];
+      f[0] = r.p; f[1] = r.Kp; f[2] = r.o2p;
+      for (int x = 0; x < 3; x++) {
+        f[3 + x] = r.P[x];
+        f[6 + x] = r.PA[x];
+        f[9 + x] = r.PB[x];
+      }
+    } else {
+      for (int k = 0; k < KETT_NF; k++) f[k] = 0.0;
+    }
+    for (int k = 0; k < KETT_NF; k++) out[base + ((long long)iq * KETT_NF + k) * KETT_TILE + l] = f[k];
+  }
+}
+
 // ------------------------------------------------------------ build kernels
 // Shell-block infinity norms (ShellBlockNorm, direct.hpp:73-90): one thread
 // per (s1, s2) block, max over rows of the absolute row sums.
@@ -505,6 +567,17 @@ cqf_status boys_tables(int device, cudaStream_t st, double** d64, float** d32) {
     dev32.resize(device + 1, nullptr);
   }
   if (!dev64[device]) {
+    // the basis and workspace buffers are stream-ordered allocations from
+    // the device's default pool; with its default release threshold (0) every
+    // stream synchronisation hands the freed memory back to the driver, and
+    // concurrent set-ups (a server) then serialise on re-mapping it.  Keep
+    // freed memory in the pool for reuse (a process-local setting of this
+    // process's pool, gone at exit).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     double* p64 = nullptr;
     float* p32 = nullptr;
     CQF_CUDA(cudaMalloc(&p64, h64.size() * sizeof(double)));
@@ -682,71 +755,66 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
                            cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
   // primitive pairs in the same order as the sorted pairs: the primitives of
-  // consecutive kets of a tile are one contiguous run
+  // consecutive kets of a tile are one contiguous run (moved on the device;
+  // only the per-pair offsets cross to the host and back)
   {
-    std::vector<long long> src(B->npair);
+    std::vector<long long> src(std::max(1, B->npair));
     long long off2 = 0;
     for (int i = 0; i < B->npair; i++) {
       src[i] = B->h_pairs[i].pp_off;
       B->h_pairs[i].pp_off = (int)off2;
       off2 += B->h_pairs[i].npp;
     }
-    std::vector<PrimPairDev> hpp(ppoff), hpp2(ppoff);
-    CQF_CUDA(cudaMemcpyAsync(hpp.data(), B->d_pp, ppoff * sizeof(PrimPairDev),
-                             cudaMemcpyDeviceToHost, B->stream));
-    CQF_CUDA(cudaStreamSynchronize(B->stream));
-    for (int i = 0; i < B->npair; i++)
-      std::copy(hpp.begin() + src[i], hpp.begin() + src[i] + B->h_pairs[i].npp,
-                hpp2.begin() + B->h_pairs[i].pp_off);
-    CQF_CUDA(cudaMemcpyAsync(B->d_pp, hpp2.data(), ppoff * sizeof(PrimPairDev),
-                             cudaMemcpyHostToDevice, B->stream));
     CQF_CUDA(cudaMemcpyAsync(B->d_pairs, B->h_pairs.data(), B->npair * sizeof(PairDev),
                              cudaMemcpyHostToDevice, B->stream));
+    long long* d_src = nullptr;
+    CQF_TRY(upload(&d_src, src, B->stream));
+    PrimPairDev* d_pp2 = nullptr;
+    CQF_CUDA(cudaMallocAsync(&d_pp2, std::max<long long>(1, ppoff) * sizeof(PrimPairDev),
+                             B->stream));
+    reorder_pp_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_pp, B->d_pairs, d_src,
+                                                                   B->npair, d_pp2);
+    cudaFreeAsync(B->d_pp, B->stream);
+    cudaFreeAsync(d_src, B->stream);
+    B->d_pp = d_pp2;
     // the same data tile-interleaved for the class kernels' kets: per ket
     // tile (KETT_TILE consecutive pairs of a class), field-major runs of
     // KETT_TILE values for each primitive (zero past a pair's npp)
     std::vector<long long> toff;
-    std::vector<double> kt;
+    std::vector<int> tfirst, tcnt;
+    long long ktn = 0;
     for (int c = 0; c < NCLS; c++) {
       B->cls_tile_beg[c] = (int)toff.size();
       const int cnt = B->cls_cnt[c];
       for (int t0 = 0; t0 < cnt; t0 += KETT_TILE) {
         int mx = 0;
-        for (int l = 0; l < KETT_TILE && t0 + l < cnt; l++)
-          mx = std::max(mx, B->h_pairs[B->cls_beg[c] + t0 + l].npp);
-        const size_t base = kt.size();
-        toff.push_back((long long)base);
-        kt.resize(base + (size_t)mx * KETT_NF * KETT_TILE, 0.0);
-        for (int l = 0; l < KETT_TILE && t0 + l < cnt; l++) {
-          const PairDev& Pp = B->h_pairs[B->cls_beg[c] + t0 + l];
-          for (int iq = 0; iq < Pp.npp; iq++) {
-            const PrimPairDev& r = hpp2[Pp.pp_off + iq];
-            const double f[KETT_NF] = {r.p,     r.Kp,    r.o2p,   r.P[0],  r.P[1],  r.P[2],
-                                       r.PA[0], r.PA[1], r.PA[2], r.PB[0], r.PB[1], r.PB[2]};
-            for (int k = 0; k < KETT_NF; k++)
-              kt[base + ((size_t)iq * KETT_NF + k) * KETT_TILE + l] = f[k];
-          }
-        }
+        const int n = std::min(KETT_TILE, cnt - t0);
+        for (int l = 0; l < n; l++) mx = std::max(mx, B->h_pairs[B->cls_beg[c] + t0 + l].npp);
+        toff.push_back(ktn);
+        tfirst.push_back(B->cls_beg[c] + t0);
+        tcnt.push_back(n);
+        ktn += (long long)mx * KETT_NF * KETT_TILE;
       }
     }
-    toff.push_back((long long)kt.size());
-    kt.push_back(0.0);
-    CQF_TRY(upload(&B->d_ketT, kt, B->stream));
-    // FP32 range data per pair: log2 of 2 max p and of max |Kp| over its
-    // primitive pairs (fp32_range_ok)
-    std::vector<float2> rng(std::max(1, B->npair), make_float2(0.f, 0.f));
-    for (int i = 0; i < B->npair; i++) {
-      double pm = 0.0, km = 0.0;
-      for (int iq = 0; iq < B->h_pairs[i].npp; iq++) {
-        const PrimPairDev& r = hpp2[B->h_pairs[i].pp_off + iq];
-        pm = std::max(pm, r.p);
-        km = std::max(km, std::fabs(r.Kp));
-      }
-      rng[i] = make_float2((float)std::log2(std::max(2.0 * pm, 1e-30)),
-                           (float)std::log2(std::max(km, 1e-60)));
-    }
-    CQF_TRY(upload(&B->d_pairRange, rng, B->stream));
+    const int ntile = (int)toff.size();
+    toff.push_back(ktn);
+    CQF_CUDA(cudaMallocAsync(&B->d_ketT, (size_t)(ktn + 1) * sizeof(double), B->stream));
+    CQF_CUDA(cudaMemsetAsync(B->d_ketT + ktn, 0, sizeof(double), B->stream));
     CQF_TRY(upload(&B->d_tileOff, toff, B->stream));
+    if (ntile > 0) {
+      int *d_tf = nullptr, *d_tc = nullptr;
+      CQF_TRY(upload(&d_tf, tfirst, B->stream));
+      CQF_TRY(upload(&d_tc, tcnt, B->stream));
+      ket_tiles_kernel<<<ntile, KETT_TILE, 0, B->stream>>>(B->d_pp, B->d_pairs, d_tf, d_tc,
+                                                           B->d_tileOff, B->d_ketT);
+      cudaFreeAsync(d_tf, B->stream);
+      cudaFreeAsync(d_tc, B->stream);
+    }
+    CQF_CUDA(cudaMallocAsync(&B->d_pairRange, std::max(1, B->npair) * sizeof(float2),
+                             B->stream));
+    pair_range_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_pp, B->d_pairs,
+                                                                   B->npair, B->d_pairRange);
+    CQF_CUDA(cudaGetLastError());
     // bra groups: per class, pairs ordered by first shell (stable: Schwarz
     // order inside a shell), runs of one shell cut into groups of at most
     // BRA_GROUP_MAX

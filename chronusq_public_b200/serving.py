@@ -79,6 +79,8 @@ class FockServer:
         self._cache_mem = 0
         self._stop = False
         self.latencies: Dict[int, float] = {}
+        # per request: (queue wait, device set-up, build) in seconds
+        self.phases: Dict[int, tuple] = {}
         self.completed = 0
         self._sched = threading.Thread(target=self._schedule, daemon=True)
         self._sched.start()
@@ -105,10 +107,17 @@ class FockServer:
         lat = np.array(list(self.latencies.values()))
         if len(lat) == 0:
             return {}
-        return {"completed": self.completed,
-                "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "mean_ms": float(lat.mean() * 1e3)}
+        out = {"completed": self.completed,
+               "p50_ms": float(np.percentile(lat, 50) * 1e3),
+               "p99_ms": float(np.percentile(lat, 99) * 1e3),
+               "mean_ms": float(lat.mean() * 1e3)}
+        if self.phases:
+            ph = np.array(list(self.phases.values())) * 1e3
+            for i, name in enumerate(("queue", "setup", "build")):
+                out[name + "_ms"] = {"p50": float(np.percentile(ph[:, i], 50)),
+                                     "p99": float(np.percentile(ph[:, i], 99)),
+                                     "mean": float(ph[:, i].mean())}
+        return out
 
     # ------------------------------------------------------------ internals
     def _schedule(self):
@@ -169,7 +178,9 @@ class FockServer:
 
     def _run(self, req: FockRequest, basis: BasisSet, need: int):
         try:
+            t_start = time.perf_counter()
             tpi, key = self._get_tpi(req, basis)
+            t_setup = time.perf_counter()
             try:
                 G, _J, _K = FockBuilder(tpi).formRawGD(
                     req.D, precision=req.precision, fp32_cutoff=req.fp32_cutoff)
@@ -178,6 +189,8 @@ class FockServer:
             done = time.perf_counter()
             with self._lock:
                 self.latencies[req.rid] = done - req.arrival
+                self.phases[req.rid] = (t_start - req.arrival, t_setup - t_start,
+                                        done - t_setup)
                 self.completed += 1
                 data_mem = footprint_bytes(basis) - 8 * 2 * 2 * basis.nbasis ** 2
                 self._cache[key] = (tpi, max(data_mem, 0))
