@@ -275,7 +275,8 @@ def run_serving(dev, nreq, rate, cutoff):
     return {"requests": nreq, "arrival_rate_hz": rate, "wall_s": wall,
             "builds_per_s": nreq / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "mean_ms": st["mean_ms"], "fp32_cutoff": cutoff,
-            "phases_ms": {k: st[k] for k in ("queue_ms", "setup_ms", "build_ms") if k in st},
+            "phases_ms": {k: st[k] for k in ("prep_ms", "queue_ms", "setup_ms", "build_ms")
+                          if k in st},
             "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
 
 

@@ -22,7 +22,9 @@ EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
            "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
            "cqf_rel_two_body_contract", "cqf_dc_opts_default",
-           "cqf_four_comp_gd", "cqf_last_error")
+           "cqf_four_comp_gd", "cqf_server_opts_default", "cqf_fock_footprint",
+           "cqf_server_create", "cqf_server_submit", "cqf_server_wait",
+           "cqf_server_get_stats", "cqf_server_destroy", "cqf_last_error")
 # cqf_rel_comp / cqf_rel_type (DIRAC_PAULI_SPINOR_COMP order)
 (CQF_CLLMS, CQF_XLLMS, CQF_XLLMX, CQF_XLLMY, CQF_XLLMZ, CQF_CSSMS, CQF_CSSMX,
  CQF_CSSMY, CQF_CSSMZ, CQF_XSSMS, CQF_XSSMX, CQF_XSSMY, CQF_XSSMZ, CQF_XLSMS,
@@ -61,6 +63,31 @@ class CqfDcOpts(C.Structure):
     _fields_ = [("bare_coulomb", C.c_int), ("dirac_coulomb", C.c_int),
                 ("dirac_coulomb_ssss", C.c_int), ("libcint", C.c_int),
                 ("xHFX", C.c_double)]
+
+
+class CqfServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int),
+                ("mem_budget", C.c_ulonglong), ("cache_entries", C.c_int)]
+
+
+class CqfFockRequest(C.Structure):
+    _fields_ = [("shells", C.POINTER(CqfShell)), ("nshell", C.c_int),
+                ("thresh_schwarz", C.c_double), ("D", C.POINTER(C.c_double)),
+                ("G", C.POINTER(C.c_double)), ("xHFX", C.c_double),
+                ("precision", C.c_int), ("fp32_cutoff", C.c_double)]
+
+
+class CqfRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("queue_ms", C.c_double),
+                ("setup_ms", C.c_double), ("build_ms", C.c_double),
+                ("latency_ms", C.c_double)]
+
+
+class CqfServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("failed", C.c_longlong), ("peak_inflight", C.c_int),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double)]
 
 
 class CqfError(RuntimeError):
@@ -120,6 +147,22 @@ def lib():
         C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
         C.POINTER(CqfDcOpts), C.POINTER(CqfOpts), C.POINTER(CqfStats)]
     L.cqf_four_comp_gd.restype = C.c_int
+    L.cqf_server_opts_default.argtypes = [C.POINTER(CqfServerOpts)]
+    L.cqf_server_opts_default.restype = None
+    L.cqf_fock_footprint.argtypes = [C.POINTER(CqfShell), C.c_int]
+    L.cqf_fock_footprint.restype = C.c_ulonglong
+    L.cqf_server_create.argtypes = [C.POINTER(CqfServerOpts), C.POINTER(C.c_void_p)]
+    L.cqf_server_create.restype = C.c_int
+    L.cqf_server_submit.argtypes = [C.c_void_p, C.POINTER(CqfFockRequest),
+                                    C.POINTER(C.c_longlong)]
+    L.cqf_server_submit.restype = C.c_int
+    L.cqf_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double,
+                                  C.POINTER(CqfRequestInfo)]
+    L.cqf_server_wait.restype = C.c_int
+    L.cqf_server_get_stats.argtypes = [C.c_void_p, C.POINTER(CqfServerStats)]
+    L.cqf_server_get_stats.restype = C.c_int
+    L.cqf_server_destroy.argtypes = [C.c_void_p]
+    L.cqf_server_destroy.restype = C.c_int
     L.cqf_last_error.argtypes = []
     L.cqf_last_error.restype = C.c_char_p
     _lib = L

@@ -35,6 +35,28 @@ class TwoBodyContraction:
     contType: int = COULOMB
 
 
+def shell_array(basis: BasisSet):
+    """(cqf_shell array, owner) of a basis: the ctypes shells point into
+    arrays held by `owner`, which must outlive every use of the shells."""
+    f = basis.flat()
+    alpha = np.ascontiguousarray(f["alpha"], dtype=np.float64)
+    coef = np.ascontiguousarray(f["coef"], dtype=np.float64)
+    sh = (_cabi.CqfShell * basis.nshell)()
+    dp = C.POINTER(C.c_double)
+    off = 0
+    for s in range(basis.nshell):
+        n = int(f["nprim"][s])
+        sh[s].l = int(f["l"][s])
+        sh[s].pure = int(f["pure"][s])
+        sh[s].nprim = n
+        sh[s].alpha = C.cast(alpha.ctypes.data + 8 * off, dp)
+        sh[s].coeff = C.cast(coef.ctypes.data + 8 * off, dp)
+        for x in range(3):
+            sh[s].origin[x] = float(f["origin"][s, x])
+        off += n
+    return sh, (f, alpha, coef)
+
+
 class DirectTPI:
     """Device-resident shell pairs and Schwarz bounds of one basis
     (``DirectTPI``, gtodirecttpi.hpp:30-141; threshSchwarz default 1e-12)."""
@@ -45,23 +67,7 @@ class DirectTPI:
         self.basis = basis
         self.threshSchwarz = threshSchwarz
         self.device = device
-        f = basis.flat()
-        self._keep = f
-        sh = (_cabi.CqfShell * basis.nshell)()
-        off = 0
-        self._alpha = np.ascontiguousarray(f["alpha"], dtype=np.float64)
-        self._coef = np.ascontiguousarray(f["coef"], dtype=np.float64)
-        dp = C.POINTER(C.c_double)
-        for s in range(basis.nshell):
-            n = int(f["nprim"][s])
-            sh[s].l = int(f["l"][s])
-            sh[s].pure = int(f["pure"][s])
-            sh[s].nprim = n
-            sh[s].alpha = C.cast(self._alpha.ctypes.data + 8 * off, dp)
-            sh[s].coeff = C.cast(self._coef.ctypes.data + 8 * off, dp)
-            for x in range(3):
-                sh[s].origin[x] = float(f["origin"][s, x])
-            off += n
+        sh, self._keep = shell_array(basis)
         h = C.c_void_p()
         _cabi.check(L.cqf_basis_create(sh, basis.nshell, threshSchwarz, device,
                                        C.byref(h)))

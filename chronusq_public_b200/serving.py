@@ -1,21 +1,26 @@
-"""Continuous-batching Fock-build server on one GPU.
+"""Continuous-batching Fock-build server on one GPU (Python face of the
+native server, ``cqf_server_*`` in include/cqfock.h).
 
-Requests (molecule, basis name, density) arrive at any time.  The server
+Requests (molecule, basis name, density) arrive at any time.  The native
+server (csrc/cqf_server.cu)
 
-* admits a request when an execution slot is free and its device-memory
-  footprint (shell-pair data + contraction workspace, estimated before any
-  allocation) fits in the budget that the requests already on the GPU leave;
-  requests that do not fit wait in FIFO order and are admitted as soon as
-  slots / memory free up (no batch boundaries: continuous batching);
-* runs every admitted request on its own worker thread and its own CUDA
-  stream (each device basis owns a stream), so the basis set-up and J/K
-  kernels of different requests overlap on the device; ctypes releases the
-  GIL for the duration of each C-ABI call;
-* keeps the device shell-pair data (``DirectTPI``) of recent geometries
-  resident in HBM (LRU, counted in the budget) so repeated geometries (SCF
-  iterations, RT steps) skip set-up;
-* records per-request latency (completion - arrival) and reports throughput
-  with p50 / p99 latency.
+* admits the oldest waiting request when an execution slot is free and its
+  device-memory footprint (shell-pair data + contraction workspace,
+  ``cqf_fock_footprint``, estimated before any allocation) fits in the budget
+  that the running requests and the cached bases leave; idle cached bases are
+  evicted (least recently used) to make room; no batch boundaries
+  (continuous batching);
+* runs every admitted request on its own worker thread and its basis' own
+  CUDA stream, so the basis set-up and J/K kernels of different requests
+  overlap on the device;
+* keeps the device shell-pair data of recent geometries resident in HBM
+  (LRU, counted in the budget), so repeated geometries (SCF iterations, RT
+  steps) skip set-up.
+
+This wrapper builds each request's basis from its molecule on a thread of
+its own, submits it, waits (the C call releases the GIL) and resolves the
+request's Future with G = 2 J[D] - K[D]; it records per-request latency
+(completion - arrival) and phase times and reports p50 / p99.
 
 Each request's result depends only on its own inputs: the kernels and the
 work split are the same alone and in a mix (the only difference is the order
@@ -23,18 +28,18 @@ of floating-point atomics), which ``tests/test_gpu_serving.py`` checks.
 """
 from __future__ import annotations
 
-import collections
+import ctypes as C
 import threading
 import time
 from concurrent.futures import Future
 from dataclasses import dataclass, field
-from typing import Dict, Optional
+from typing import Dict
 
 import numpy as np
 
+from . import _cabi
 from .basis import BasisSet, Molecule
-from .contraction import DirectTPI
-from .fockbuilder import FockBuilder
+from .contraction import shell_array
 
 
 @dataclass
@@ -49,162 +54,99 @@ class FockRequest:
     future: Future = field(default_factory=Future)
 
 
-def _geometry_key(mol: Molecule, basis: str):
-    return (basis, mol.Z.tobytes(), np.round(mol.xyz, 10).tobytes())
-
-
-def footprint_bytes(basis: BasisSet, nmat: int = 2) -> int:
-    """Device bytes a request needs: shell/pair/primitive-pair data (upper
-    bound: every pair significant) plus the per-call workspace."""
-    ns, N, nc = basis.nshell, basis.nbasis, basis.ncart
-    npair = ns * (ns + 1) // 2
-    kprim = basis.max_prim ** 2
-    pairs = npair * (64 + 96 * kprim) + ns * ns * 8 + 300_000
-    ws = 8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns)
-    return int(pairs + ws)
+def footprint_bytes(basis: BasisSet) -> int:
+    """Device bytes the server charges a request of this basis
+    (``cqf_fock_footprint``: shell-pair data, upper bound with every pair
+    significant, plus the workspace of one J and one K)."""
+    sh, _keep = shell_array(basis)
+    return int(_cabi.lib().cqf_fock_footprint(sh, basis.nshell))
 
 
 class FockServer:
     def __init__(self, device: int = 0, slots: int = 8,
                  mem_budget: int = 8 << 30, cache_entries: int = 16):
-        self.device = device
-        self.slots = slots
-        self.mem_budget = mem_budget
-        self.cache_entries = cache_entries
-        self._lock = threading.Condition()
-        self._queue: collections.deque = collections.deque()
-        self._inflight = 0
-        self._mem_in_use = 0
-        self._cache: "collections.OrderedDict" = collections.OrderedDict()
-        self._cache_mem = 0
-        self._stop = False
+        L = _cabi.lib()
+        o = _cabi.CqfServerOpts()
+        L.cqf_server_opts_default(C.byref(o))
+        o.device, o.slots = device, slots
+        o.mem_budget, o.cache_entries = int(mem_budget), cache_entries
+        h = C.c_void_p()
+        _cabi.check(L.cqf_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._lock = threading.Lock()
+        self._threads = []
         self.latencies: Dict[int, float] = {}
-        # per request: (queue wait, device set-up, build) in seconds
+        # per request: (prep, queue, set-up, build) in seconds; prep = basis
+        # construction on the host before submission
         self.phases: Dict[int, tuple] = {}
-        self.completed = 0
-        self._sched = threading.Thread(target=self._schedule, daemon=True)
-        self._sched.start()
 
     # ------------------------------------------------------------ public
     def submit(self, req: FockRequest) -> Future:
         if not req.arrival:
             req.arrival = time.perf_counter()
+        t = threading.Thread(target=self._serve, args=(req,), daemon=True)
         with self._lock:
-            self._queue.append(req)
-            self._lock.notify_all()
+            self._threads.append(t)
+        t.start()
         return req.future
 
     def close(self):
         with self._lock:
-            self._stop = True
-            self._lock.notify_all()
-        self._sched.join(timeout=60)
-        for _, (tpi, _m) in self._cache.items():
-            tpi.close()
-        self._cache.clear()
+            threads = list(self._threads)
+        for t in threads:
+            t.join()
+        if self._h:
+            _cabi.lib().cqf_server_destroy(self._h)
+            self._h = None
 
     def stats(self):
         lat = np.array(list(self.latencies.values()))
         if len(lat) == 0:
             return {}
-        out = {"completed": self.completed,
+        st = _cabi.CqfServerStats()
+        _cabi.check(_cabi.lib().cqf_server_get_stats(self._h, C.byref(st)))
+        out = {"completed": len(lat), "failed": int(st.failed),
+               "peak_inflight": int(st.peak_inflight),
                "p50_ms": float(np.percentile(lat, 50) * 1e3),
                "p99_ms": float(np.percentile(lat, 99) * 1e3),
                "mean_ms": float(lat.mean() * 1e3)}
-        if self.phases:
-            ph = np.array(list(self.phases.values())) * 1e3
-            for i, name in enumerate(("queue", "setup", "build")):
-                out[name + "_ms"] = {"p50": float(np.percentile(ph[:, i], 50)),
-                                     "p99": float(np.percentile(ph[:, i], 99)),
-                                     "mean": float(ph[:, i].mean())}
+        ph = np.array(list(self.phases.values())) * 1e3
+        for i, name in enumerate(("prep", "queue", "setup", "build")):
+            out[name + "_ms"] = {"p50": float(np.percentile(ph[:, i], 50)),
+                                 "p99": float(np.percentile(ph[:, i], 99)),
+                                 "mean": float(ph[:, i].mean())}
         return out
 
     # ------------------------------------------------------------ internals
-    def _schedule(self):
-        while True:
-            with self._lock:
-                while not self._stop and not self._admissible():
-                    self._lock.wait(timeout=0.5)
-                if self._stop and not self._queue:
-                    return
-                if not self._admissible():
-                    continue
-                req, basis, need = self._queue.popleft()
-                self._inflight += 1
-                self._mem_in_use += need
-            threading.Thread(target=self._run, args=(req, basis, need),
-                             daemon=True).start()
-
-    def _admissible(self) -> bool:
-        """Head of the queue fits a slot and the memory budget (FIFO)."""
-        if not self._queue or self._inflight >= self.slots:
-            return False
-        head = self._queue[0]
-        if isinstance(head, FockRequest):
-            basis = BasisSet.build(head.mol, head.basis)
-            self._queue[0] = (head, basis, footprint_bytes(basis))
-        req, basis, need = self._queue[0]
-        key = _geometry_key(req.mol, req.basis)
-        if key in self._cache:
-            need -= self._cache[key][1]
-        free = self.mem_budget - self._mem_in_use - self._cache_mem
-        while free < need and self._evict_one():
-            free = self.mem_budget - self._mem_in_use - self._cache_mem
-        if free >= need or self._inflight == 0:
-            self._queue[0] = (req, basis, max(need, 0))
-            return True
-        return False
-
-    def _evict_one(self) -> bool:
-        for key, (tpi, mem) in self._cache.items():
-            if getattr(tpi, "_busy", 0) == 0:
-                del self._cache[key]
-                self._cache_mem -= mem
-                tpi.close()
-                return True
-        return False
-
-    def _get_tpi(self, req: FockRequest, basis: BasisSet):
-        key = _geometry_key(req.mol, req.basis)
-        with self._lock:
-            hit = self._cache.pop(key, None)
-            if hit is not None:
-                self._cache_mem -= hit[1]
-                hit[0]._busy = getattr(hit[0], "_busy", 0) + 1
-                return hit[0], key
-        tpi = DirectTPI(basis, device=self.device)
-        tpi._busy = 1
-        return tpi, key
-
-    def _run(self, req: FockRequest, basis: BasisSet, need: int):
+    def _serve(self, req: FockRequest):
         try:
-            t_start = time.perf_counter()
-            tpi, key = self._get_tpi(req, basis)
-            t_setup = time.perf_counter()
-            try:
-                G, _J, _K = FockBuilder(tpi).formRawGD(
-                    req.D, precision=req.precision, fp32_cutoff=req.fp32_cutoff)
-            finally:
-                tpi._busy -= 1
+            L = _cabi.lib()
+            basis = BasisSet.build(req.mol, req.basis)
+            sh, keep = shell_array(basis)
+            N = basis.nbasis
+            D = np.asfortranarray(req.D, dtype=np.float64)
+            if D.shape != (N, N):
+                raise ValueError("density shape does not match the basis")
+            G = np.zeros((N, N), order="F")
+            dp = C.POINTER(C.c_double)
+            q = _cabi.CqfFockRequest(sh, basis.nshell, 1e-12, D.ctypes.data_as(dp),
+                                     G.ctypes.data_as(dp), 1.0,
+                                     _cabi.CQF_MIXED if req.precision == "mixed"
+                                     else _cabi.CQF_FP64, float(req.fp32_cutoff))
+            t_sub = time.perf_counter()
+            rid = C.c_longlong()
+            _cabi.check(L.cqf_server_submit(self._h, C.byref(q), C.byref(rid)))
+            info = _cabi.CqfRequestInfo()
+            _cabi.check(L.cqf_server_wait(self._h, rid.value, -1.0, C.byref(info)))
             done = time.perf_counter()
+            del keep
             with self._lock:
                 self.latencies[req.rid] = done - req.arrival
-                self.phases[req.rid] = (t_start - req.arrival, t_setup - t_start,
-                                        done - t_setup)
-                self.completed += 1
-                data_mem = footprint_bytes(basis) - 8 * 2 * 2 * basis.nbasis ** 2
-                self._cache[key] = (tpi, max(data_mem, 0))
-                self._cache_mem += max(data_mem, 0)
-                while len(self._cache) > self.cache_entries and self._evict_one():
-                    pass
+                self.phases[req.rid] = (t_sub - req.arrival, info.queue_ms / 1e3,
+                                        info.setup_ms / 1e3, info.build_ms / 1e3)
             req.future.set_result(G)
         except BaseException as e:  # report to the caller, keep serving
             req.future.set_exception(e)
-        finally:
-            with self._lock:
-                self._inflight -= 1
-                self._mem_in_use -= need
-                self._lock.notify_all()
 
 
 def poisson_stream(n: int, rate_hz: float, seed: int = 5, max_waters: int = 32):

@@ -203,6 +203,81 @@ void cqf_dc_opts_default(cqf_dc_opts* o);
 cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const* G,
                             const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 
+/* ---------------------------------------------------------------------
+ * Fock-build server: requests of any basis size arrive at any time and
+ * share one GPU (continuous batching).  No counterpart in the reference
+ * (ChronusQ runs one build at a time); each request is the closed-shell
+ * build FockBuilder::formRawGDInBatches performs for one density
+ * (include/fockbuilder/impl.hpp:109-244): G = 2 J[D] - xHFX K[D].
+ *
+ * The server admits the oldest waiting request (FIFO) when an execution
+ * slot is free and its device-memory footprint (cqf_fock_footprint) fits in
+ * the budget that the running requests and the cached bases leave, evicting
+ * idle cached bases (least recently used) to make room; a request alone on
+ * the GPU is always admitted.  Every admitted request runs on its own worker
+ * thread and its basis' own stream, so the set-up and kernels of different
+ * requests overlap on the device.  Bases of recent geometries stay resident
+ * (cache_entries), so a repeated geometry (SCF iterations, RT steps) skips
+ * set-up.  A request's result depends only on its own inputs: the kernels
+ * and work split are the same alone and in a mix (only the order of
+ * floating-point atomics differs).
+ * --------------------------------------------------------------------- */
+typedef struct cqf_server cqf_server;
+
+typedef struct {
+  int device;
+  int slots;                       /* requests on the GPU at once */
+  unsigned long long mem_budget;   /* bytes for running requests + cached bases */
+  int cache_entries;               /* bases kept resident after their request */
+} cqf_server_opts;
+/* device 0, 8 slots, 8 GiB, 16 cached bases. */
+void cqf_server_opts_default(cqf_server_opts* o);
+
+typedef struct {
+  const cqf_shell* shells;   /* copied at submission */
+  int nshell;
+  double thresh_schwarz;     /* 1e-12 in ChronusQ */
+  const double* D;           /* N x N real symmetric density, host, copied at submission */
+  double* G;                 /* out: N x N host buffer, written on completion */
+  double xHFX;               /* exchange scaling (1 for Hartree-Fock) */
+  int precision;             /* cqf_precision */
+  double fp32_cutoff;
+} cqf_fock_request;
+
+/* Per-request timing (milliseconds from submission) and outcome. */
+typedef struct {
+  cqf_status status;
+  double queue_ms;    /* submission -> admission */
+  double setup_ms;    /* basis set-up (0 when cached) */
+  double build_ms;    /* J/K build and G */
+  double latency_ms;  /* submission -> completion */
+} cqf_request_info;
+
+typedef struct {
+  long long submitted, completed, failed;
+  int peak_inflight;               /* most requests on the GPU at once */
+  double p50_ms, p99_ms, mean_ms;  /* latency over completed requests */
+} cqf_server_stats;
+
+/* Device bytes a request of this basis is charged for: shell-pair data
+ * (upper bound: every pair significant, every pair with the largest
+ * primitive count) plus the contraction workspace of one J and one K. */
+unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell);
+
+cqf_status cqf_server_create(const cqf_server_opts* opts, cqf_server** out);
+/* Queues a request; *id identifies it in cqf_server_wait.  Returns without
+ * waiting; G must stay valid until the request completes. */
+cqf_status cqf_server_submit(cqf_server* server, const cqf_fock_request* req, long long* id);
+/* Waits for request id (timeout_s < 0: no limit); fills info when it is
+ * done.  Returns the request's status (its error text becomes this thread's
+ * cqf_last_error), or CQF_ETIMEDOUT if it has not completed in time.  A
+ * completed request is forgotten once a wait has returned its outcome. */
+cqf_status cqf_server_wait(cqf_server* server, long long id, double timeout_s,
+                           cqf_request_info* info);
+cqf_status cqf_server_get_stats(cqf_server* server, cqf_server_stats* stats);
+/* Finishes every submitted request, then frees the server and its bases. */
+cqf_status cqf_server_destroy(cqf_server* server);
+
 /* Text of the last error on this thread ("" if none). */
 const char* cqf_last_error(void);
 

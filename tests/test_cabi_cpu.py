@@ -118,3 +118,78 @@ def test_flop_model_matches_oracle_count():
     assert mine["quartets"] == ref["quartets"]
     assert abs(mine["f64"] - ref["f64"]) <= 1e-9 * ref["f64"]
     assert abs(mine["f32"] - ref["f32"]) <= 1e-9 * max(ref["f32"], 1.0)
+
+
+def _footprint_model(basis, nmat=2):
+    """The server's footprint formula restated (cqf_fock_footprint)."""
+    ns, N, nc = basis.nshell, basis.nbasis, basis.ncart
+    npair = ns * (ns + 1) // 2
+    kprim = basis.max_prim ** 2
+    pairs = npair * (64 + 96 * kprim) + ns * ns * 8 + 300_000
+    ws = 8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns)
+    return pairs + ws
+
+
+def test_server_footprint_matches_model():
+    from chronusq_public_b200.serving import footprint_bytes
+    for nw, b in ((1, "cc-pvdz"), (3, "def2-svp")):
+        basis = BasisSet.build(workloads.water_cluster(nw, seed=3, box=6.0), b)
+        assert footprint_bytes(basis) == _footprint_model(basis)
+
+
+def test_server_rejects_bad_arguments():
+    L = _cabi.lib()
+    o = _cabi.CqfServerOpts()
+    L.cqf_server_opts_default(ctypes.byref(o))
+    assert (o.slots, o.cache_entries) == (8, 16)
+    o.slots = 0
+    h = ctypes.c_void_p()
+    assert L.cqf_server_create(ctypes.byref(o), ctypes.byref(h)) == _cabi.CQF_EINVAL
+    o.slots = 2
+    assert L.cqf_server_create(ctypes.byref(o), ctypes.byref(h)) == _cabi.CQF_OK
+    q = _cabi.CqfFockRequest()
+    rid = ctypes.c_longlong()
+    assert L.cqf_server_submit(h, ctypes.byref(q), ctypes.byref(rid)) == _cabi.CQF_EINVAL
+    assert L.cqf_server_wait(h, 12345, 0.0, None) == _cabi.CQF_EINVAL
+    assert b"unknown request" in L.cqf_last_error()
+    assert L.cqf_server_destroy(h) == _cabi.CQF_OK
+
+
+def test_server_reports_failed_requests_without_device():
+    """Without a GPU every request fails in basis set-up; the server reports
+    the status and its text to the waiter, counts the failures and shuts
+    down cleanly."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from chronusq_public_b200.contraction import shell_array
+    L = _cabi.lib()
+    basis = BasisSet.build(workloads.water_cluster(1, seed=3, box=6.0), "cc-pvdz")
+    sh, keep = shell_array(basis)
+    N = basis.nbasis
+    D = np.asfortranarray(np.eye(N))
+    G = np.zeros((N, N), order="F")
+    o = _cabi.CqfServerOpts()
+    L.cqf_server_opts_default(ctypes.byref(o))
+    o.slots = 2
+    h = ctypes.c_void_p()
+    assert L.cqf_server_create(ctypes.byref(o), ctypes.byref(h)) == _cabi.CQF_OK
+    dp = ctypes.POINTER(ctypes.c_double)
+    q = _cabi.CqfFockRequest(sh, basis.nshell, 1e-12, D.ctypes.data_as(dp),
+                             G.ctypes.data_as(dp), 1.0, _cabi.CQF_FP64, 0.0)
+    ids = []
+    for _ in range(3):
+        rid = ctypes.c_longlong()
+        assert L.cqf_server_submit(h, ctypes.byref(q), ctypes.byref(rid)) == _cabi.CQF_OK
+        ids.append(rid.value)
+    assert len(set(ids)) == 3
+    for rid in ids:
+        info = _cabi.CqfRequestInfo()
+        st = L.cqf_server_wait(h, rid, 30.0, ctypes.byref(info))
+        assert st == _cabi.CQF_ENODEV and info.status == _cabi.CQF_ENODEV
+        assert b"no CUDA device" in L.cqf_last_error()
+    s = _cabi.CqfServerStats()
+    assert L.cqf_server_get_stats(h, ctypes.byref(s)) == _cabi.CQF_OK
+    assert (s.submitted, s.completed, s.failed) == (3, 0, 3)
+    assert (G == 0).all()
+    assert L.cqf_server_destroy(h) == _cabi.CQF_OK

@@ -60,16 +60,11 @@ def test_memory_admission_limits_concurrency():
     reqs += [r for r in _requests(4, seed=11, nwater=3) if r[1] == "def2-svp"]
     need = max(footprint_bytes(r[3]) for r in reqs)
     assert min(footprint_bytes(r[3]) for r in reqs) * 2 > need * 1.5
-    srv = FockServer(slots=8, mem_budget=int(need * 1.5))
-    peak = [0]
-    orig = srv._run
-
-    def run(*a):
-        peak[0] = max(peak[0], srv._inflight)
-        return orig(*a)
-    srv._run = run
+    srv = FockServer(slots=8, mem_budget=int(need * 1.5), cache_entries=0)
     futs = [srv.submit(FockRequest(mol, b, D, rid=i)) for i, (mol, b, D, _) in enumerate(reqs)]
     for f in futs:
         f.result(timeout=120)
+    st = srv.stats()
     srv.close()
-    assert peak[0] == 1
+    assert st["completed"] == len(reqs)
+    assert st["peak_inflight"] == 1
