@@ -43,6 +43,24 @@ def atomic_number(sym: str) -> int:
     return Z_OF[sym.strip().upper()]
 
 
+# Mass number of each element's default isotope (the most abundant stable
+# one, as the reference's defaultIsotope map in include/atom.hpp), Z = 1..54
+# without Tc; used for the finite-nucleus charge radius.
+_MASS_NUMBER = dict(zip(range(1, 55), (
+    1, 4, 7, 9, 11, 12, 14, 16, 19, 20, 23, 24, 27, 28, 31, 32, 35, 40, 39, 40,
+    45, 48, 51, 52, 55, 56, 59, 58, 63, 64, 69, 74, 75, 80, 79, 84, 85, 88, 89,
+    90, 93, 98, None, 102, 103, 106, 107, 114, 115, 120, 121, 130, 127, 132)))
+
+
+def finite_nucleus_exponent(mass_number: int) -> float:
+    """Exponent zeta of the Gaussian nuclear charge Z (zeta/pi)^{3/2}
+    exp(-zeta r^2) with root-mean-square radius 0.836 A^{1/3} + 0.570 fm:
+    zeta = 3 / (2 r^2), r in Bohr (Molecule::computeCDist,
+    src/molecule/molecule.cxx:197-226)."""
+    r = (0.836 * mass_number ** (1.0 / 3.0) + 0.570) * 1e-5 / ANG_PER_BOHR
+    return 1.5 / (r * r)
+
+
 def n_cart(l: int) -> int:
     return (l + 1) * (l + 2) // 2
 
@@ -215,6 +233,21 @@ class Molecule:
     @property
     def natom(self) -> int:
         return len(self.Z)
+
+    def nuclei(self, finite: bool = False, mass_numbers=None) -> np.ndarray:
+        """(natom, 5) rows {Z, x, y, z (Bohr), zeta}: zeta = 0 for point
+        charges, else the Gaussian finite-nucleus exponent of each atom's
+        default isotope (or of ``mass_numbers``)."""
+        out = np.zeros((self.natom, 5))
+        out[:, 0] = self.Z
+        out[:, 1:4] = self.xyz
+        if finite:
+            for i, z in enumerate(self.Z):
+                A = mass_numbers[i] if mass_numbers is not None else _MASS_NUMBER.get(int(z))
+                if A is None:
+                    raise KeyError("no default isotope for Z = %d; pass mass_numbers" % z)
+                out[i, 4] = finite_nucleus_exponent(A)
+        return out
 
     def nuclear_repulsion(self) -> float:
         e = 0.0

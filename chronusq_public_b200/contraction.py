@@ -93,6 +93,18 @@ class DirectTPI:
             self.handle, S.ctypes.data_as(dp), T.ctypes.data_as(dp)))
         return S, T
 
+    def nuclear(self, nuclei) -> np.ndarray:
+        """V: nuclear-attraction matrix in the field of ``nuclei``
+        ((natom, 5) rows {Z, x, y, z, zeta}; ``Molecule.nuclei``), computed
+        on the device."""
+        N = self.nbasis
+        nuc = np.ascontiguousarray(nuclei, dtype=np.float64).reshape(-1, 5)
+        V = np.zeros((N, N), order="F")
+        dp = C.POINTER(C.c_double)
+        _cabi.check(_cabi.lib().cqf_basis_nuclear(
+            self.handle, len(nuc), nuc.ctypes.data_as(dp), V.ctypes.data_as(dp)))
+        return V
+
     def close(self):
         if getattr(self, "handle", None):
             _cabi.lib().cqf_basis_destroy(self.handle)

@@ -243,6 +243,71 @@ __global__ void one_electron_kernel(const ShellDev* __restrict__ sh, const doubl
     }
 }
 
+// Nuclear-attraction matrix (column-major N x N), one thread per shell-pair
+// block: V_ab = -sum_C Z_C (2 pi / p) f sum_tuv E^x_t E^y_u E^z_v R_tuv(a', P - C)
+// per primitive pair (McMurchie-Davidson); point nucleus a' = p, f = 1;
+// Gaussian charge of exponent zeta a' = p zeta / (p + zeta),
+// f = sqrt(zeta / (p + zeta)).  nuc[5 c ..] = {Z, x, y, z, zeta}.
+__global__ void nuclear_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
+                               const double* __restrict__ sph, const int* __restrict__ sphOff,
+                               int nshell, int nprimTot, int N, int natom,
+                               const double* __restrict__ nuc, const double* __restrict__ boys,
+                               double* Vmat) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nshell * nshell) return;
+  const int s1 = k % nshell, s2 = k / nshell;
+  const ShellDev A = sh[s1], B = sh[s2];
+  const int la = A.l, lb = B.l, L = la + lb, L1 = L + 1;
+  const int na = ncart(la), nb = ncart(lb);
+  constexpr int E1 = (LMAX + 1) * (LMAX + 1) * (2 * LMAX + 1);
+  double V[ncart(LMAX)][ncart(LMAX)];
+  for (int i = 0; i < na; i++)
+    for (int j = 0; j < nb; j++) V[i][j] = 0.0;
+  double AB2 = 0.0;
+  for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+  double E[3][E1], F[2 * LMAX + 1], R[nherm(2 * LMAX)];
+  for (int ia = 0; ia < A.nprim; ia++)
+    for (int jb = 0; jb < B.nprim; jb++) {
+      const double a = prim[A.prim_off + ia], b = prim[B.prim_off + jb];
+      const double ca = prim[nprimTot + A.prim_off + ia], cb = prim[nprimTot + B.prim_off + jb];
+      const double p = a + b, K = ca * cb * exp(-a * b / p * AB2);
+      double P[3];
+      for (int x = 0; x < 3; x++) {
+        P[x] = (a * A.O[x] + b * B.O[x]) / p;
+        hermite_E_rt<double, LMAX>(la, lb, 0.5 / p, P[x] - A.O[x], P[x] - B.O[x], E[x]);
+      }
+      for (int c = 0; c < natom; c++) {
+        const double Z = nuc[5 * c], zeta = nuc[5 * c + 4];
+        const double X = P[0] - nuc[5 * c + 1], Y = P[1] - nuc[5 * c + 2],
+                     W = P[2] - nuc[5 * c + 3];
+        const double al = zeta > 0.0 ? p * zeta / (p + zeta) : p;
+        const double f = zeta > 0.0 ? sqrt(zeta / (p + zeta)) : 1.0;
+        boys_rt<double>(L, al * (X * X + Y * Y + W * W), F, boys);
+        hermite_R_rt<double>(L, al, X, Y, W, F, R);
+        const double pref = -Z * K * 2.0 * M_PI / p * f;
+        for (int u = 0; u < na; u++) {
+          const int ax = cart_lx(la, u), ay = cart_ly(la, u), az = cart_lz(la, u);
+          for (int v = 0; v < nb; v++) {
+            const int bx = cart_lx(lb, v), by = cart_ly(lb, v), bz = cart_lz(lb, v);
+            const double* ex = E[0] + (ax * (lb + 1) + bx) * L1;
+            const double* ey = E[1] + (ay * (lb + 1) + by) * L1;
+            const double* ez = E[2] + (az * (lb + 1) + bz) * L1;
+            double sum = 0.0;
+            for (int t = 0; t <= ax + bx; t++)
+              for (int w = 0; w <= ay + by; w++)
+                for (int z = 0; z <= az + bz; z++) sum += ex[t] * ey[w] * ez[z] * R[hidx(t, w, z)];
+            V[u][v] += pref * sum;
+          }
+        }
+      }
+    }
+  const int ma = A.pure ? nsph(A.l) : ncart(A.l), mb = B.pure ? nsph(B.l) : ncart(B.l);
+  for (int mu = 0; mu < ma; mu++)
+    for (int nu = 0; nu < mb; nu++)
+      Vmat[(size_t)(A.sph_off + mu) + (size_t)(B.sph_off + nu) * N] =
+          sph_elem(A, B, sph, sphOff, V, mu, nu);
+}
+
 __global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
                                   int nprimTot, const PairDev* __restrict__ pairs, int npair,
                                   PrimPairDev* pp) {
@@ -941,6 +1006,30 @@ cqf_status cqf_basis_one_electron(cqf_basis* B, double* S, double* T) {
   CQF_CUDA(cudaGetLastError());
   CQF_CUDA(cudaMemcpyAsync(S, d, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaMemcpyAsync(T, d + NN, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_nuclear(cqf_basis* B, int natom, const double* nuclei, double* V) {
+  g_err.clear();
+  if (!B || !V || natom < 0 || (natom > 0 && !nuclei))
+    return fail(CQF_EINVAL, "cqf_basis_nuclear: bad argument");
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  CQF_TRY(ensure_ws(B, (NN + 5 * (size_t)std::max(1, natom)) * sizeof(double)));
+  double* d = static_cast<double*>(B->d_ws);
+  double* dn = d + NN;
+  if (natom > 0)
+    CQF_CUDA(cudaMemcpyAsync(dn, nuclei, 5 * (size_t)natom * sizeof(double),
+                             cudaMemcpyHostToDevice, B->stream));
+  int nprimTot = 0;
+  for (auto& sh : B->h_shells) nprimTot += sh.nprim;
+  nuclear_kernel<<<grid1((size_t)B->nshell * B->nshell, 64), 64, 0, B->stream>>>(
+      B->d_shells, B->d_prim, B->d_sph, B->d_sphOff, B->nshell, nprimTot, B->nbasis, natom, dn,
+      B->d_boys64, d);
+  CQF_CUDA(cudaGetLastError());
+  CQF_CUDA(cudaMemcpyAsync(V, d, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
   return CQF_OK;
 }

@@ -109,6 +109,17 @@ cqf_status cqf_basis_schwarz(const cqf_basis* basis, double* Q);
  * and for the four-component metric). */
 cqf_status cqf_basis_one_electron(cqf_basis* basis, double* S, double* T);
 
+/* Nuclear-attraction matrix V (N x N column-major, host memory) of the basis
+ * in the field of natom nuclei, nuclei[5 i .. 5 i + 4] = {Z, x, y, z (Bohr),
+ * zeta}: zeta = 0 is a point charge (the libint2::Operator::nuclear engine
+ * with charges -Z at the atoms, src/particleintegrals/aointegrals/
+ * aointegrals_onee_drivers.cxx:139-145); zeta > 0 a Gaussian charge
+ * Z (zeta/pi)^{3/2} exp(-zeta r^2) (finiteWidthNuc, the four-component
+ * default; Molecule::computeCDist, src/molecule/molecule.cxx:197-226).
+ * The reference's core Hamiltonian is T + V (stored as its scalar Pauli
+ * component, 2 (T + V)); for four components its LL block is V. */
+cqf_status cqf_basis_nuclear(cqf_basis* basis, int natom, const double* nuclei, double* V);
+
 /* GTODirectTPIContraction::twoBodyContract: for each entry, AX += G[X]. */
 cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
                                  const cqf_opts* opts, cqf_stats* stats);

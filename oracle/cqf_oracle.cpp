@@ -877,6 +877,97 @@ void orc_overlap_kinetic(void* b, double* S, double* Tk) {
     }
 }
 
+// Nuclear-attraction matrix V (column-major N x N): V_ab = -sum_C Z_C
+// (a| |r - C|^-1 |b) for point nuclei (the libint2::Operator::nuclear engine
+// with charges -Z at the atoms, src/particleintegrals/aointegrals/
+// aointegrals_onee_drivers.cxx:139-145), or the potential of a Gaussian
+// nuclear charge Z (zeta/pi)^{3/2} exp(-zeta |r - C|^2) (finiteWidthNuc;
+// Molecule::computeCDist, src/molecule/molecule.cxx:197-226).  McMurchie-
+// Davidson: for a primitive pair (p, P) and nucleus C,
+//   (2 pi / p) f sum_tuv E^x_t E^y_u E^z_v R_tuv(a', P - C),
+// point: a' = p, f = 1; Gaussian: a' = p zeta / (p + zeta),
+// f = sqrt(zeta / (p + zeta)).  nuc[5 i ..] = {Z, x, y, z, zeta (0: point)}.
+void orc_nuclear(void* b, int natom, const double* nuc, double* V) {
+  auto* bs = static_cast<Basis*>(b);
+  int ns = (int)bs->shells.size(), N = bs->nbasis;
+  for (int s1 = 0; s1 < ns; s1++)
+    for (int s2 = 0; s2 < ns; s2++) {
+      const Shell &A = bs->shells[s1], &B = bs->shells[s2];
+      const int la = A.l, lb = B.l, L = la + lb, L1 = L + 1;
+      const int na = ncart(la), nb = ncart(lb);
+      std::vector<double> Vb((size_t)na * nb, 0.0);
+      double AB2 = 0;
+      for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+      const auto &ax = bs->cx[la], &ay = bs->cy[la], &az = bs->cz[la];
+      const auto &bx = bs->cx[lb], &by = bs->cy[lb], &bz = bs->cz[lb];
+      std::vector<double> R((size_t)(L + 1) * L1 * L1 * L1);
+      auto Ridx = [&](int n, int t, int u, int v) -> size_t {
+        return (((size_t)n * L1 + t) * L1 + u) * L1 + v;
+      };
+      for (size_t i = 0; i < A.alpha.size(); i++)
+        for (size_t j = 0; j < B.alpha.size(); j++) {
+          const double a = A.alpha[i], bb = B.alpha[j], p = a + bb, mu = a * bb / p;
+          double P[3];
+          for (int x = 0; x < 3; x++) P[x] = (a * A.O[x] + bb * B.O[x]) / p;
+          const double K = A.coef[i] * B.coef[j] * std::exp(-mu * AB2);
+          std::vector<double> E[3];
+          for (int x = 0; x < 3; x++) hermite_E(la, lb, p, P[x] - A.O[x], P[x] - B.O[x], E[x]);
+          auto e = [&](int x, int ii, int jj, int t) {
+            return E[x][((size_t)ii * (lb + 1) + jj) * L1 + t];
+          };
+          for (int c = 0; c < natom; c++) {
+            const double Z = nuc[5 * c], zeta = nuc[5 * c + 4];
+            const double PC[3] = {P[0] - nuc[5 * c + 1], P[1] - nuc[5 * c + 2],
+                                  P[2] - nuc[5 * c + 3]};
+            const double al = zeta > 0.0 ? p * zeta / (p + zeta) : p;
+            const double f = zeta > 0.0 ? std::sqrt(zeta / (p + zeta)) : 1.0;
+            const double T = al * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+            double F[64];
+            boys().eval(L, T, F);
+            double m2a = -2.0 * al, fn = 1.0;
+            for (int n = 0; n <= L; n++) { R[Ridx(n, 0, 0, 0)] = fn * F[n]; fn *= m2a; }
+            for (int n = L - 1; n >= 0; n--) {
+              const int top = L - n;
+              for (int t = 0; t <= top; t++)
+                for (int u = 0; u <= top - t; u++)
+                  for (int v = 0; v <= top - t - u; v++) {
+                    if (t + u + v == 0) continue;
+                    double val;
+                    if (t > 0) {
+                      val = PC[0] * R[Ridx(n + 1, t - 1, u, v)];
+                      if (t > 1) val += (t - 1) * R[Ridx(n + 1, t - 2, u, v)];
+                    } else if (u > 0) {
+                      val = PC[1] * R[Ridx(n + 1, t, u - 1, v)];
+                      if (u > 1) val += (u - 1) * R[Ridx(n + 1, t, u - 2, v)];
+                    } else {
+                      val = PC[2] * R[Ridx(n + 1, t, u, v - 1)];
+                      if (v > 1) val += (v - 1) * R[Ridx(n + 1, t, u, v - 2)];
+                    }
+                    R[Ridx(n, t, u, v)] = val;
+                  }
+            }
+            const double pref = -Z * K * 2.0 * M_PI / p * f;
+            for (int u = 0; u < na; u++)
+              for (int v = 0; v < nb; v++) {
+                double sum = 0.0;
+                for (int t = 0; t <= ax[u] + bx[v]; t++)
+                  for (int w = 0; w <= ay[u] + by[v]; w++)
+                    for (int z = 0; z <= az[u] + bz[v]; z++)
+                      sum += e(0, ax[u], bx[v], t) * e(1, ay[u], by[v], w) *
+                             e(2, az[u], bz[v], z) * R[Ridx(0, t, w, z)];
+                Vb[u * nb + v] += pref * sum;
+              }
+          }
+        }
+      const Shell* sh[2] = {&A, &B};
+      cart_to_sph_block(*bs, sh, 2, Vb);
+      const int n1 = A.size(), n2 = B.size();
+      for (int i = 0; i < n1; i++)
+        for (int j = 0; j < n2; j++)
+          V[(bs->off[s1] + i) + (size_t)(bs->off[s2] + j) * N] = Vb[i * n2 + j];
+    }
+}
+
 // Contracted shell quartet in AO order (row-major i,j,k,l).
 int orc_eri_quartet(void* b, int s1, int s2, int s3, int s4, double* out) {
   auto* bs = static_cast<Basis*>(b);

@@ -44,6 +44,7 @@ def lib():
         L.orc_boys.argtypes = [C.c_int, C.c_double]
         L.orc_boys.restype = C.c_double
         L.orc_overlap_kinetic.argtypes = [C.c_void_p, dp, dp]
+        L.orc_nuclear.argtypes = [C.c_void_p, C.c_int, dp, dp]
         L.orc_eri_quartet.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                       C.c_int, dp]
         L.orc_eri_quartet.restype = C.c_int
@@ -115,6 +116,15 @@ class OracleBasis:
         T = np.zeros((N, N), order="F")
         lib().orc_overlap_kinetic(self.h, _dp(S), _dp(T))
         return S, T
+
+    def nuclear(self, nuclei):
+        """V (N x N): nuclei = (natom, 5) rows {Z, x, y, z, zeta}, zeta = 0
+        for a point charge (orc_nuclear)."""
+        N = self.nbasis
+        nuc = np.ascontiguousarray(nuclei, dtype=np.float64)
+        V = np.zeros((N, N), order="F")
+        lib().orc_nuclear(self.h, len(nuc), _dp(nuc), _dp(V))
+        return V
 
     def eri_quartet(self, s1, s2, s3, s4):
         n = [int(self.sizes[s]) for s in (s1, s2, s3, s4)]

@@ -108,3 +108,38 @@ def test_dirac_coulomb_llss():
     G = ob.dirac_coulomb(D, bare=True, dc=True, ssss=False, libcint=False)
     for k, c in enumerate(PAULI):
         assert np.abs(G[k] - g["G_" + c]).max() < 1e-9, c
+
+
+def test_nuclear_point_rhf_core_hamiltonian():
+    """Point nuclei: the reference stores the core Hamiltonian's scalar
+    Pauli component, 2 (T + V) (INTS/CORE_HAMILTONIAN_SCALAR)."""
+    g = golden("readden_rhf.npz")
+    ob = O.OracleBasis(readden_rhf_basis(g))
+    V = ob.nuclear(water_ref().nuclei())
+    assert np.abs(V - (g["H"] / 2 - g["T"])).max() < 1e-10
+
+
+def test_nuclear_finite_four_component_core_hamiltonian():
+    """Gaussian nuclei (the 4C default): the LL block of the DC core
+    Hamiltonian's scalar component is 2 V, its LS block 2 T; point nuclei
+    would miss it by far more than the tolerance."""
+    g = golden("readden_dc.npz")
+    mol = water_ref()
+    bs = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
+    ob = O.OracleBasis(bs)
+    N = bs.nbasis
+    H = g["H_SCALAR"]
+    Vf = ob.nuclear(mol.nuclei(finite=True))
+    assert np.abs(H[:N, :N].real - 2 * Vf).max() < 1e-10
+    assert np.abs(H[:N, :N].real - 2 * ob.nuclear(mol.nuclei())).max() > 1e-3
+    _S, T = ob.overlap_kinetic()
+    assert np.abs(H[:N, N:].real - 2 * T).max() < 1e-9
+
+
+def test_finite_nucleus_exponent():
+    from chronusq_public_b200.basis import finite_nucleus_exponent
+    # O-16: r = 0.836 * 16^(1/3) + 0.570 fm
+    r = (0.836 * 16 ** (1 / 3) + 0.570) * 1e-5 / 0.52917721092
+    assert math.isclose(finite_nucleus_exponent(16), 1.5 / r ** 2, rel_tol=1e-14)
+    nuc = water_ref().nuclei(finite=True)
+    assert nuc.shape == (3, 5) and (nuc[:, 4] > 1e8).all()
