@@ -19,7 +19,8 @@ CQF_FP64, CQF_MIXED = 0, 1
 # every entry point declared in include/cqfock.h
 EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
-           "cqf_basis_nuclear",
+           "cqf_basis_nuclear", "cqf_basis_nuclear_pvp",
+           "cqf_four_comp_core_hamiltonian",
            "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
            "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
            "cqf_rel_two_body_contract", "cqf_dc_opts_default",
@@ -128,6 +129,11 @@ def lib():
     L.cqf_basis_nuclear.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]
     L.cqf_basis_nuclear.restype = C.c_int
+    L.cqf_basis_nuclear_pvp.argtypes = L.cqf_basis_nuclear.argtypes
+    L.cqf_basis_nuclear_pvp.restype = C.c_int
+    L.cqf_four_comp_core_hamiltonian.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                                 C.POINTER(C.c_void_p)]
+    L.cqf_four_comp_core_hamiltonian.restype = C.c_int
     L.cqf_two_body_contract.argtypes = [C.c_void_p, C.POINTER(CqfContraction),
                                         C.c_int, C.POINTER(CqfOpts),
                                         C.POINTER(CqfStats)]

@@ -105,6 +105,30 @@ class DirectTPI:
             self.handle, len(nuc), nuc.ctypes.data_as(dp), V.ctypes.data_as(dp)))
         return V
 
+    def nuclear_pvp(self, nuclei) -> np.ndarray:
+        """(4, N, N): pV.p and the spin-orbit (pV x p)_x,y,z of the four-
+        component core Hamiltonian, computed on the device."""
+        N = self.nbasis
+        nuc = np.ascontiguousarray(nuclei, dtype=np.float64).reshape(-1, 5)
+        buf = np.zeros(4 * N * N)
+        dp = C.POINTER(C.c_double)
+        _cabi.check(_cabi.lib().cqf_basis_nuclear_pvp(
+            self.handle, len(nuc), nuc.ctypes.data_as(dp), buf.ctypes.data_as(dp)))
+        return np.stack([buf[k * N * N:(k + 1) * N * N].reshape(N, N, order="F")
+                         for k in range(4)])
+
+    def four_comp_core_hamiltonian(self, nuclei) -> list:
+        """``FourComponent::compute4CCH``: the four Pauli components
+        (scalar, MX, MY, MZ) of the 2N x 2N complex core Hamiltonian
+        [[V, T], [T, W / 4c^2 - T]] as the reference stores them."""
+        M = 2 * self.nbasis
+        nuc = np.ascontiguousarray(nuclei, dtype=np.float64).reshape(-1, 5)
+        H = [np.zeros((M, M), dtype=np.complex128, order="F") for _ in range(4)]
+        hp = (C.c_void_p * 4)(*[h.ctypes.data for h in H])
+        _cabi.check(_cabi.lib().cqf_four_comp_core_hamiltonian(
+            self.handle, len(nuc), nuc.ctypes.data_as(C.POINTER(C.c_double)), hp))
+        return H
+
     def close(self):
         if getattr(self, "handle", None):
             _cabi.lib().cqf_basis_destroy(self.handle)

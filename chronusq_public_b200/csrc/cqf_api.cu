@@ -308,6 +308,101 @@ __global__ void nuclear_kernel(const ShellDev* __restrict__ sh, const double* __
           sph_elem(A, B, sph, sphOff, V, mu, nu);
 }
 
+// Derivative nuclear-attraction matrices of the four-component core
+// Hamiltonian, one thread per shell-pair block: with D_{mu nu} = <d_mu a| V
+// |d_nu b> (electron-coordinate gradients; d_x x^i e = i x^{i-1} e -
+// 2 a x^{i+1} e, so each D is a sum of plain nuclear-attraction integrals of
+// l +- 1 on each side, from Hermite tables of (la + 1, lb + 1)),
+// W0 = pV.p = sum_mu D_{mu mu} and W_k = (pV x p)_k = D_{ij} - D_{ji}
+// ((i, j, k) cyclic); out: 4 consecutive N x N column-major matrices.
+__global__ void nuclear_pvp_kernel(const ShellDev* __restrict__ sh,
+                                   const double* __restrict__ prim,
+                                   const double* __restrict__ sph, const int* __restrict__ sphOff,
+                                   int nshell, int nprimTot, int N, int natom,
+                                   const double* __restrict__ nuc, const double* __restrict__ boys,
+                                   double* Wmat) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nshell * nshell) return;
+  const int s1 = k % nshell, s2 = k / nshell;
+  const ShellDev A = sh[s1], B = sh[s2];
+  const int la = A.l, lb = B.l, La = la + 1, Lb = lb + 1, L = La + Lb, L1 = L + 1;
+  const int na = ncart(la), nb = ncart(lb);
+  constexpr int E1 = (LMAX + 2) * (LMAX + 2) * (2 * LMAX + 3);
+  double W[4][ncart(LMAX)][ncart(LMAX)];
+  for (int q = 0; q < 4; q++)
+    for (int i = 0; i < na; i++)
+      for (int j = 0; j < nb; j++) W[q][i][j] = 0.0;
+  double AB2 = 0.0;
+  for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+  double E[3][E1], F[2 * LMAX + 3], R[nherm(2 * LMAX + 2)];
+  for (int ia = 0; ia < A.nprim; ia++)
+    for (int jb = 0; jb < B.nprim; jb++) {
+      const double a = prim[A.prim_off + ia], b = prim[B.prim_off + jb];
+      const double ca = prim[nprimTot + A.prim_off + ia], cb = prim[nprimTot + B.prim_off + jb];
+      const double p = a + b, K = ca * cb * exp(-a * b / p * AB2);
+      double P[3];
+      for (int x = 0; x < 3; x++) {
+        P[x] = (a * A.O[x] + b * B.O[x]) / p;
+        hermite_E_rt<double, LMAX + 1>(La, Lb, 0.5 / p, P[x] - A.O[x], P[x] - B.O[x], E[x]);
+      }
+      for (int c = 0; c < natom; c++) {
+        const double Z = nuc[5 * c], zeta = nuc[5 * c + 4];
+        const double X = P[0] - nuc[5 * c + 1], Y = P[1] - nuc[5 * c + 2],
+                     Wz = P[2] - nuc[5 * c + 3];
+        const double al = zeta > 0.0 ? p * zeta / (p + zeta) : p;
+        const double f = zeta > 0.0 ? sqrt(zeta / (p + zeta)) : 1.0;
+        boys_rt<double>(L, al * (X * X + Y * Y + Wz * Wz), F, boys);
+        hermite_R_rt<double>(L, al, X, Y, Wz, F, R);
+        const double pref = -Z * K * 2.0 * M_PI / p * f;
+        // plain integral of Cartesian exponents (i0, i1, i2 | j0, j1, j2)
+        auto vint = [&](int i0, int i1, int i2, int j0, int j1, int j2) {
+          if (i0 < 0 || i1 < 0 || i2 < 0 || j0 < 0 || j1 < 0 || j2 < 0) return 0.0;
+          const double* ex = E[0] + (i0 * (Lb + 1) + j0) * L1;
+          const double* ey = E[1] + (i1 * (Lb + 1) + j1) * L1;
+          const double* ez = E[2] + (i2 * (Lb + 1) + j2) * L1;
+          double sum = 0.0;
+          for (int t = 0; t <= i0 + j0; t++)
+            for (int w = 0; w <= i1 + j1; w++)
+              for (int z = 0; z <= i2 + j2; z++) sum += ex[t] * ey[w] * ez[z] * R[hidx(t, w, z)];
+          return sum;
+        };
+        for (int u = 0; u < na; u++) {
+          const int a0[3] = {cart_lx(la, u), cart_ly(la, u), cart_lz(la, u)};
+          for (int v = 0; v < nb; v++) {
+            const int b0[3] = {cart_lx(lb, v), cart_ly(lb, v), cart_lz(lb, v)};
+            double D[3][3];
+            for (int m = 0; m < 3; m++)
+              for (int n = 0; n < 3; n++) {
+                double d = 0.0;
+                for (int sa = -1; sa <= 1; sa += 2)
+                  for (int sb = -1; sb <= 1; sb += 2) {
+                    const double fa = sa < 0 ? (double)a0[m] : -2.0 * a;
+                    const double fb = sb < 0 ? (double)b0[n] : -2.0 * b;
+                    if (fa == 0.0 || fb == 0.0) continue;
+                    int ii[3] = {a0[0], a0[1], a0[2]}, jj[3] = {b0[0], b0[1], b0[2]};
+                    ii[m] += sa;
+                    jj[n] += sb;
+                    d += fa * fb * vint(ii[0], ii[1], ii[2], jj[0], jj[1], jj[2]);
+                  }
+                D[m][n] = pref * d;
+              }
+            W[0][u][v] += D[0][0] + D[1][1] + D[2][2];
+            W[1][u][v] += D[1][2] - D[2][1];
+            W[2][u][v] += D[2][0] - D[0][2];
+            W[3][u][v] += D[0][1] - D[1][0];
+          }
+        }
+      }
+    }
+  const int ma = A.pure ? nsph(A.l) : ncart(A.l), mb = B.pure ? nsph(B.l) : ncart(B.l);
+  const size_t NN = (size_t)N * N;
+  for (int q = 0; q < 4; q++)
+    for (int mu = 0; mu < ma; mu++)
+      for (int nu = 0; nu < mb; nu++)
+        Wmat[q * NN + (size_t)(A.sph_off + mu) + (size_t)(B.sph_off + nu) * N] =
+            sph_elem(A, B, sph, sphOff, W[q], mu, nu);
+}
+
 __global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double* __restrict__ prim,
                                   int nprimTot, const PairDev* __restrict__ pairs, int npair,
                                   PrimPairDev* pp) {
@@ -1031,6 +1126,58 @@ cqf_status cqf_basis_nuclear(cqf_basis* B, int natom, const double* nuclei, doub
   CQF_CUDA(cudaGetLastError());
   CQF_CUDA(cudaMemcpyAsync(V, d, NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
+  return CQF_OK;
+}
+
+cqf_status cqf_basis_nuclear_pvp(cqf_basis* B, int natom, const double* nuclei, double* W) {
+  g_err.clear();
+  if (!B || !W || natom < 0 || (natom > 0 && !nuclei))
+    return fail(CQF_EINVAL, "cqf_basis_nuclear_pvp: bad argument");
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  CQF_TRY(ensure_ws(B, (4 * NN + 5 * (size_t)std::max(1, natom)) * sizeof(double)));
+  double* d = static_cast<double*>(B->d_ws);
+  double* dn = d + 4 * NN;
+  if (natom > 0)
+    CQF_CUDA(cudaMemcpyAsync(dn, nuclei, 5 * (size_t)natom * sizeof(double),
+                             cudaMemcpyHostToDevice, B->stream));
+  int nprimTot = 0;
+  for (auto& sh : B->h_shells) nprimTot += sh.nprim;
+  nuclear_pvp_kernel<<<grid1((size_t)B->nshell * B->nshell, 64), 64, 0, B->stream>>>(
+      B->d_shells, B->d_prim, B->d_sph, B->d_sphOff, B->nshell, nprimTot, B->nbasis, natom, dn,
+      B->d_boys64, d);
+  CQF_CUDA(cudaGetLastError());
+  CQF_CUDA(cudaMemcpyAsync(W, d, 4 * NN * sizeof(double), cudaMemcpyDeviceToHost, B->stream));
+  CQF_CUDA(cudaStreamSynchronize(B->stream));
+  return CQF_OK;
+}
+
+cqf_status cqf_four_comp_core_hamiltonian(cqf_basis* B, int natom, const double* nuclei,
+                                          void* const* H) {
+  if (!B || !H) return fail(CQF_EINVAL, "cqf_four_comp_core_hamiltonian: null argument");
+  for (int c = 0; c < 4; c++)
+    if (!H[c]) return fail(CQF_EINVAL, "cqf_four_comp_core_hamiltonian: null component");
+  const int N = B->nbasis;
+  const size_t NN = (size_t)N * N;
+  std::vector<double> S(NN), T(NN), V(NN), W(4 * NN);
+  CQF_TRY(cqf_basis_one_electron(B, S.data(), T.data()));
+  CQF_TRY(cqf_basis_nuclear(B, natom, nuclei, V.data()));
+  CQF_TRY(cqf_basis_nuclear_pvp(B, natom, nuclei, W.data()));
+  const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
+  const size_t M = 2 * (size_t)N;  // 4C dimension
+  for (int c = 0; c < 4; c++) std::fill_n(static_cast<double*>(H[c]), 2 * M * M, 0.0);
+  // element (r, col) of component c: interleaved complex, column-major
+  auto at = [&](int c, size_t r, size_t col) { return static_cast<double*>(H[c]) + 2 * (r + col * M); };
+  for (int j = 0; j < N; j++)
+    for (int i = 0; i < N; i++) {
+      const size_t e = (size_t)i + (size_t)j * N;
+      at(0, i, j)[0] = 2.0 * V[e];
+      at(0, i, N + j)[0] = 2.0 * T[e];
+      at(0, N + i, j)[0] = 2.0 * T[e];
+      at(0, N + i, N + j)[0] = 2.0 * (C2 * W[e] - T[e]);
+      for (int k = 1; k < 4; k++) at(k, N + i, N + j)[1] = 2.0 * C2 * W[k * NN + e];
+    }
   return CQF_OK;
 }
 

@@ -27,6 +27,7 @@
 namespace cqf {
 
 constexpr int LMAX = 3;            // highest shell angular momentum (f)
+constexpr double SPEED_OF_LIGHT = 137.035999074;  // atomic units (include/physcon.hpp:40)
 constexpr int BOYS_MMAX = 40;      // orders of the host-side generation
 constexpr double BOYS_DT = 0.1;    // grid spacing of the Taylor tables
 constexpr double BOYS_TMAX = 36.0; // above: F0 = sqrt(pi/T)/2 + upward recursion

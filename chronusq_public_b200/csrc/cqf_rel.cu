@@ -53,9 +53,6 @@ namespace {
     if (s_ != CQF_OK) return s_; \
   } while (0)
 
-// speed of light in atomic units (include/physcon.hpp:40)
-constexpr double SPEED_OF_LIGHT = 137.035999074;
-
 unsigned rgrid(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // max of the six shell-block norms of a quartet in the reference's roles

@@ -120,6 +120,22 @@ cqf_status cqf_basis_one_electron(cqf_basis* basis, double* S, double* T);
  * component, 2 (T + V)); for four components its LL block is V. */
 cqf_status cqf_basis_nuclear(cqf_basis* basis, int natom, const double* nuclei, double* V);
 
+/* Derivative nuclear-attraction matrices of the four-component core
+ * Hamiltonian, nuclei as for cqf_basis_nuclear: W (4 consecutive N x N
+ * column-major host matrices) = pV.p, (pV x p)_x, (pV x p)_y, (pV x p)_z,
+ * with (pV x p)_k = <d_i a|V|d_j b> - <d_j a|V|d_i b>, (i, j, k) cyclic
+ * (the scalar / SOX / SOY / SOZ components of OnePRelInts,
+ * src/particleintegrals/spatialtospinor.cxx:205-230). */
+cqf_status cqf_basis_nuclear_pvp(cqf_basis* basis, int natom, const double* nuclei, double* W);
+
+/* FourComponent::compute4CCH (src/fourcomp/fourcomp.cxx:36-100): the
+ * four-component core Hamiltonian [[V, T], [T, W / (4c^2) - T]] as the four
+ * Pauli components (scalar, MX, MY, MZ) the reference stores, each a 2N x 2N
+ * complex column-major host matrix (LL block first): scalar = 2 x the
+ * spin-free blocks, MX/MY/MZ = 2i (pV x p)_k / (4c^2) in the SS block. */
+cqf_status cqf_four_comp_core_hamiltonian(cqf_basis* basis, int natom, const double* nuclei,
+                                          void* const* H);
+
 /* GTODirectTPIContraction::twoBodyContract: for each entry, AX += G[X]. */
 cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
                                  const cqf_opts* opts, cqf_stats* stats);

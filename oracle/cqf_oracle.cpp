@@ -968,6 +968,135 @@ void orc_nuclear(void* b, int natom, const double* nuc, double* V) {
     }
 }
 
+// Derivative nuclear-attraction matrices of the four-component core
+// Hamiltonian: D_{mu nu}(a, b) = <d_mu a| V |d_nu b> (d = gradient with
+// respect to the electron coordinate, V = -sum_C Z_C / |r - C| or its
+// Gaussian-nucleus form as in orc_nuclear), and
+//   W[0] = pV.p   = sum_mu D_{mu mu},
+//   W[1..3] = (pV x p)_k = D_{ij} - D_{ji}, (i, j, k) cyclic,
+// each N x N column-major (the OnePRelInts scalar / SOX / SOY / SOZ
+// components, include/particleintegrals/onepints/relativisticints.hpp;
+// src/particleintegrals/spatialtospinor.cxx:205-230).  d_x x^i e^{-a x^2} =
+// i x^{i-1} e^{..} - 2 a x^{i+1} e^{..}, so every D is a sum of plain
+// nuclear-attraction integrals with l raised or lowered by one on each side,
+// from Hermite tables of (la + 1, lb + 1).
+void orc_nuclear_pvp(void* b, int natom, const double* nuc, double* W) {
+  auto* bs = static_cast<Basis*>(b);
+  int ns = (int)bs->shells.size(), N = bs->nbasis;
+  for (int s1 = 0; s1 < ns; s1++)
+    for (int s2 = 0; s2 < ns; s2++) {
+      const Shell &A = bs->shells[s1], &B = bs->shells[s2];
+      const int la = A.l, lb = B.l, La = la + 1, Lb = lb + 1, L = La + Lb, L1 = L + 1;
+      const int na = ncart(la), nb = ncart(lb);
+      std::vector<double> Dm((size_t)9 * na * nb, 0.0);
+      double AB2 = 0;
+      for (int x = 0; x < 3; x++) AB2 += (A.O[x] - B.O[x]) * (A.O[x] - B.O[x]);
+      const auto &ax = bs->cx[la], &ay = bs->cy[la], &az = bs->cz[la];
+      const auto &bx = bs->cx[lb], &by = bs->cy[lb], &bz = bs->cz[lb];
+      std::vector<double> R((size_t)(L + 1) * L1 * L1 * L1);
+      auto Ridx = [&](int n, int t, int u, int v) -> size_t {
+        return (((size_t)n * L1 + t) * L1 + u) * L1 + v;
+      };
+      for (size_t i = 0; i < A.alpha.size(); i++)
+        for (size_t j = 0; j < B.alpha.size(); j++) {
+          const double a = A.alpha[i], bb = B.alpha[j], p = a + bb, mu = a * bb / p;
+          double P[3];
+          for (int x = 0; x < 3; x++) P[x] = (a * A.O[x] + bb * B.O[x]) / p;
+          const double K = A.coef[i] * B.coef[j] * std::exp(-mu * AB2);
+          std::vector<double> E[3];
+          for (int x = 0; x < 3; x++) hermite_E(La, Lb, p, P[x] - A.O[x], P[x] - B.O[x], E[x]);
+          auto e = [&](int x, int ii, int jj, int t) {
+            if (ii < 0 || jj < 0 || t > ii + jj) return 0.0;
+            return E[x][((size_t)ii * (Lb + 1) + jj) * L1 + t];
+          };
+          for (int c = 0; c < natom; c++) {
+            const double Z = nuc[5 * c], zeta = nuc[5 * c + 4];
+            const double PC[3] = {P[0] - nuc[5 * c + 1], P[1] - nuc[5 * c + 2],
+                                  P[2] - nuc[5 * c + 3]};
+            const double al = zeta > 0.0 ? p * zeta / (p + zeta) : p;
+            const double f = zeta > 0.0 ? std::sqrt(zeta / (p + zeta)) : 1.0;
+            const double T = al * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+            double F[64];
+            boys().eval(L, T, F);
+            double m2a = -2.0 * al, fn = 1.0;
+            for (int n = 0; n <= L; n++) { R[Ridx(n, 0, 0, 0)] = fn * F[n]; fn *= m2a; }
+            for (int n = L - 1; n >= 0; n--) {
+              const int top = L - n;
+              for (int t = 0; t <= top; t++)
+                for (int u = 0; u <= top - t; u++)
+                  for (int v = 0; v <= top - t - u; v++) {
+                    if (t + u + v == 0) continue;
+                    double val;
+                    if (t > 0) {
+                      val = PC[0] * R[Ridx(n + 1, t - 1, u, v)];
+                      if (t > 1) val += (t - 1) * R[Ridx(n + 1, t - 2, u, v)];
+                    } else if (u > 0) {
+                      val = PC[1] * R[Ridx(n + 1, t, u - 1, v)];
+                      if (u > 1) val += (u - 1) * R[Ridx(n + 1, t, u - 2, v)];
+                    } else {
+                      val = PC[2] * R[Ridx(n + 1, t, u, v - 1)];
+                      if (v > 1) val += (v - 1) * R[Ridx(n + 1, t, u, v - 2)];
+                    }
+                    R[Ridx(n, t, u, v)] = val;
+                  }
+            }
+            const double pref = -Z * K * 2.0 * M_PI / p * f;
+            // plain integral of Cartesian exponents ia[3], ib[3]
+            auto vint = [&](const int* ia, const int* ib) {
+              for (int x = 0; x < 3; x++)
+                if (ia[x] < 0 || ib[x] < 0) return 0.0;
+              double sum = 0.0;
+              for (int t = 0; t <= ia[0] + ib[0]; t++)
+                for (int w = 0; w <= ia[1] + ib[1]; w++)
+                  for (int z = 0; z <= ia[2] + ib[2]; z++)
+                    sum += e(0, ia[0], ib[0], t) * e(1, ia[1], ib[1], w) *
+                           e(2, ia[2], ib[2], z) * R[Ridx(0, t, w, z)];
+              return sum;
+            };
+            for (int u = 0; u < na; u++)
+              for (int v = 0; v < nb; v++) {
+                const int a0[3] = {ax[u], ay[u], az[u]}, b0[3] = {bx[v], by[v], bz[v]};
+                for (int m = 0; m < 3; m++)
+                  for (int nn = 0; nn < 3; nn++) {
+                    double d = 0.0;
+                    for (int sa = -1; sa <= 1; sa += 2)
+                      for (int sb = -1; sb <= 1; sb += 2) {
+                        const double fa = sa < 0 ? a0[m] : -2.0 * a;
+                        const double fb = sb < 0 ? b0[nn] : -2.0 * bb;
+                        if (fa == 0.0 || fb == 0.0) continue;
+                        int ia[3] = {a0[0], a0[1], a0[2]}, ib[3] = {b0[0], b0[1], b0[2]};
+                        ia[m] += sa;
+                        ib[nn] += sb;
+                        d += fa * fb * vint(ia, ib);
+                      }
+                    Dm[((size_t)(m * 3 + nn) * na + u) * nb + v] += pref * d;
+                  }
+              }
+          }
+        }
+      std::vector<double> Wb[4];
+      for (int k = 0; k < 4; k++) Wb[k].assign((size_t)na * nb, 0.0);
+      auto D = [&](int m, int nn, int u, int v) { return Dm[((size_t)(m * 3 + nn) * na + u) * nb + v]; };
+      for (int u = 0; u < na; u++)
+        for (int v = 0; v < nb; v++) {
+          const size_t q = (size_t)u * nb + v;
+          Wb[0][q] = D(0, 0, u, v) + D(1, 1, u, v) + D(2, 2, u, v);
+          Wb[1][q] = D(1, 2, u, v) - D(2, 1, u, v);
+          Wb[2][q] = D(2, 0, u, v) - D(0, 2, u, v);
+          Wb[3][q] = D(0, 1, u, v) - D(1, 0, u, v);
+        }
+      const Shell* sh[2] = {&A, &B};
+      const int n1 = A.size(), n2 = B.size();
+      for (int k = 0; k < 4; k++) {
+        cart_to_sph_block(*bs, sh, 2, Wb[k]);
+        for (int i = 0; i < n1; i++)
+          for (int j = 0; j < n2; j++)
+            W[(size_t)k * N * N + (bs->off[s1] + i) + (size_t)(bs->off[s2] + j) * N] =
+                Wb[k][i * n2 + j];
+      }
+    }
+}
+
 // Contracted shell quartet in AO order (row-major i,j,k,l).
 int orc_eri_quartet(void* b, int s1, int s2, int s3, int s4, double* out) {
   auto* bs = static_cast<Basis*>(b);

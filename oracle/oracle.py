@@ -45,6 +45,7 @@ def lib():
         L.orc_boys.restype = C.c_double
         L.orc_overlap_kinetic.argtypes = [C.c_void_p, dp, dp]
         L.orc_nuclear.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        L.orc_nuclear_pvp.argtypes = [C.c_void_p, C.c_int, dp, dp]
         L.orc_eri_quartet.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                       C.c_int, dp]
         L.orc_eri_quartet.restype = C.c_int
@@ -125,6 +126,17 @@ class OracleBasis:
         V = np.zeros((N, N), order="F")
         lib().orc_nuclear(self.h, len(nuc), _dp(nuc), _dp(V))
         return V
+
+    def nuclear_pvp(self, nuclei):
+        """[pV.p, (pVxp)_x, (pVxp)_y, (pVxp)_z], each N x N (orc_nuclear_pvp)."""
+        N = self.nbasis
+        nuc = np.ascontiguousarray(nuclei, dtype=np.float64)
+        W = np.zeros((4, N, N))
+        buf = np.zeros(4 * N * N)
+        lib().orc_nuclear_pvp(self.h, len(nuc), _dp(nuc), _dp(buf))
+        for k in range(4):
+            W[k] = buf[k * N * N:(k + 1) * N * N].reshape(N, N, order="F")
+        return W
 
     def eri_quartet(self, s1, s2, s3, s4):
         n = [int(self.sizes[s]) for s in (s1, s2, s3, s4)]

@@ -41,3 +41,30 @@ def test_nuclear_ag_f_shells_vs_oracle(finite):
     Vo = O.OracleBasis(bs).nuclear(nuc)
     assert np.abs(V - Vo).max() < 1e-10 * max(1.0, np.abs(Vo).max())
     assert np.abs(V - V.T).max() < 1e-10 * np.abs(Vo).max()
+
+
+def test_four_comp_core_hamiltonian_matches_reference():
+    """All four Pauli components, every block, against the reference's stored
+    4C core Hamiltonian (water, Gaussian nuclei)."""
+    g = golden("readden_dc.npz")
+    mol = water_ref()
+    bs = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
+    H = DirectTPI(bs).four_comp_core_hamiltonian(mol.nuclei(finite=True))
+    for k, comp in enumerate(("SCALAR", "MX", "MY", "MZ")):
+        ref = g["H_" + comp]
+        assert np.abs(H[k] - ref).max() < 1e-9 * max(1.0, np.abs(ref).max()), comp
+
+
+@pytest.mark.parametrize("finite", [False, True])
+def test_nuclear_pvp_ag_f_shells_vs_oracle(finite):
+    mol = Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0), ("Ag", 0.3, 0.5, 2.6)])
+    bs = BasisSet.build(mol, "sapporo-dkh3-dzp-2012_no", uncontract=True)
+    nuc = mol.nuclei(finite=finite)
+    W = DirectTPI(bs).nuclear_pvp(nuc)
+    Wo = O.OracleBasis(bs).nuclear_pvp(nuc)
+    for k in range(4):
+        assert np.abs(W[k] - Wo[k]).max() < 1e-10 * max(1.0, np.abs(Wo[k]).max()), k
+    # pV.p symmetric, the spin-orbit parts antisymmetric
+    assert np.abs(W[0] - W[0].T).max() < 1e-9 * np.abs(W[0]).max()
+    for k in (1, 2, 3):
+        assert np.abs(W[k] + W[k].T).max() < 1e-9 * np.abs(W[k]).max()

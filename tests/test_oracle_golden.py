@@ -143,3 +143,24 @@ def test_finite_nucleus_exponent():
     assert math.isclose(finite_nucleus_exponent(16), 1.5 / r ** 2, rel_tol=1e-14)
     nuc = water_ref().nuclei(finite=True)
     assert nuc.shape == (3, 5) and (nuc[:, 4] > 1e8).all()
+
+
+def test_four_component_core_hamiltonian_ss_block():
+    """SS block of the reference's 4C core Hamiltonian (compute4CCH,
+    src/fourcomp/fourcomp.cxx:36-100): scalar 2 (pV.p / 4c^2 - T), MX/MY/MZ
+    2i (pV x p)_k / 4c^2, with Gaussian nuclei."""
+    g = golden("readden_dc.npz")
+    mol = water_ref()
+    bs = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
+    ob = O.OracleBasis(bs)
+    N = bs.nbasis
+    W = ob.nuclear_pvp(mol.nuclei(finite=True))
+    _S, T = ob.overlap_kinetic()
+    C2 = 1.0 / (4.0 * 137.035999074 ** 2)
+    ss = g["H_SCALAR"][N:, N:]
+    assert np.abs(ss.real - 2 * (C2 * W[0] - T)).max() < 1e-9
+    assert np.abs(ss.imag).max() == 0
+    for k, comp in enumerate(("MX", "MY", "MZ")):
+        h = g["H_" + comp]
+        assert np.abs(h[N:, N:] - 2j * C2 * W[1 + k]).max() < 1e-12
+        assert np.abs(h[:N, :]).max() == 0 and np.abs(h[N:, :N]).max() == 0
