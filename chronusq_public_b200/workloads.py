@@ -152,3 +152,36 @@ def build_config(name: str, tpi_factory):
     S, _T = tpi.one_electron()
     D = occupied_density(S, nocc, seed)
     return mol, basis, tpi, D
+
+
+def main(argv=None):
+    """One FP64 build of a named workload on cuda:0, with its time:
+
+        python -m chronusq_public_b200.workloads ag4_dc
+
+    (a single, unwarmed build -- the command profiling captures use; timed
+    throughput comes from bench.py)."""
+    import argparse
+    import time
+
+    from .contraction import DirectTPI
+    from .fockbuilder import FockBuilder, FourCompFock
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload")
+    args = ap.parse_args(argv)
+    if args.workload == "ag4_dc":
+        _basis, tpi, D = build_ag4_dc(lambda b: DirectTPI(b))
+        fb = FourCompFock(tpi)
+        t0 = time.perf_counter()
+        fb.formGD(D)
+    else:
+        _mol, _basis, tpi, D = build_config(args.workload, lambda b: DirectTPI(b))
+        fb = FockBuilder(tpi)
+        t0 = time.perf_counter()
+        fb.formRawGD(D)
+    dt = time.perf_counter() - t0
+    print("%s: one build %.3f s" % (args.workload, dt), flush=True)
+
+
+if __name__ == "__main__":
+    main()
