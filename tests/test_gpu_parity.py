@@ -179,3 +179,51 @@ def test_many_densities_one_call_matches_oracle():
     for k, X in enumerate(dDs):
         Jo, Ko = ob.contract([X, X], [1, 1], [COULOMB, EXCHANGE])
         assert np.abs(Gs[k] - (2 * Jo - Ko)).max() < FP64_TOL
+
+
+def _jk_vs_oracle(basis, seed=5):
+    tpi = DirectTPI(basis)
+    ob = O.OracleBasis(basis)
+    N = basis.nbasis
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((N, N))
+    D = 0.5 * (A + A.T)
+    G, J, K = FockBuilder(tpi).formRawGD(D)
+    Jo, Ko = ob.contract([D, D], [1, 1], [0, 1])
+    assert np.abs(J - Jo).max() < FP64_TOL
+    assert np.abs(K - Ko).max() < FP64_TOL
+    return tpi
+
+
+def test_edge_single_s_function():
+    """N = 1: one H atom with one s shell (only the (ss|ss) class)."""
+    from chronusq_public_b200.basis import BasisSet, Molecule, parse_gbs
+    gbs = "****\nH 0\nS 1 1.00\n  0.8 1.0\n****\n"
+    basis = BasisSet.build(Molecule.from_angstrom([("H", 0.0, 0.0, 0.0)]), parse_gbs(gbs))
+    assert basis.nbasis == 1
+    _jk_vs_oracle(basis)
+
+
+def test_edge_distant_fragments_insignificant_pairs():
+    """Two waters 60 Angstrom apart: no significant pair links them, the
+    quartet list is two disconnected blocks."""
+    from chronusq_public_b200.basis import BasisSet, Molecule
+    w = workloads.water()
+    xyz = np.vstack([w.xyz, w.xyz + np.array([60.0 / 0.52917721092, 0.0, 0.0])])
+    mol = Molecule(np.concatenate([w.Z, w.Z]), xyz)
+    basis = BasisSet.build(mol, "cc-pvdz")
+    tpi = _jk_vs_oracle(basis)
+    assert tpi.npair < basis.nshell * (basis.nshell + 1) // 2
+
+
+def test_edge_empty_contraction_list():
+    basis = contract_basis()
+    tpi = DirectTPI(basis)
+    GTODirectTPIContraction(tpi).twoBodyContract([])  # a no-op, no error
+    import ctypes as C
+    from chronusq_public_b200 import _cabi
+    # the C ABI refuses an empty list with a status (the Python mirror, like
+    # the reference's loop, does nothing)
+    st = _cabi.CqfStats()
+    assert _cabi.lib().cqf_two_body_contract(tpi.handle, None, 0, None,
+                                             C.byref(st)) == _cabi.CQF_EINVAL
