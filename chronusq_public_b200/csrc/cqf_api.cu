@@ -698,6 +698,9 @@ void free_basis(cqf_basis* B) {
   }
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
+  if (B->evFork) cudaEventDestroy(B->evFork);
+  for (int i = 0; i < NAUX; i++)
+    if (B->evJoin[i]) cudaEventDestroy(B->evJoin[i]);
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
 }
@@ -709,6 +712,31 @@ cqf_status upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
   if (!src.empty())
     CQF_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice,
                              st));
+  return CQF_OK;
+}
+
+// Auxiliary streams of the class-quartet launches: a per-device pool created
+// once per process and lent round-robin to the bases (a server creates and
+// destroys a basis per request; creating streams each time costs set-up
+// latency).  Bases that share a pooled stream only order those launches.
+cqf_status aux_stream(int device, cudaStream_t* out) {
+  constexpr int POOL = 16;
+  static std::mutex mu;
+  static std::vector<std::vector<cudaStream_t>> pools;
+  static std::vector<unsigned> next;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)pools.size() <= device) {
+    pools.resize(device + 1);
+    next.resize(device + 1, 0u);
+  }
+  if (pools[device].empty()) {
+    for (int i = 0; i < POOL; i++) {
+      cudaStream_t s = nullptr;
+      CQF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      pools[device].push_back(s);
+    }
+  }
+  *out = pools[device][next[device]++ % POOL];
   return CQF_OK;
 }
 
@@ -767,6 +795,11 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   CQF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
   CQF_CUDA(cudaEventCreate(&B->ev0));
   CQF_CUDA(cudaEventCreate(&B->ev1));
+  CQF_CUDA(cudaEventCreateWithFlags(&B->evFork, cudaEventDisableTiming));
+  for (int i = 0; i < NAUX; i++) {
+    CQF_TRY(aux_stream(device, &B->aux[i]));
+    CQF_CUDA(cudaEventCreateWithFlags(&B->evJoin[i], cudaEventDisableTiming));
+  }
   B->thresh = thresh;
   B->nshell = nshell;
 
@@ -1345,6 +1378,15 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;
   for (int m = 0; m < nMat; m++) fastOK = fastOK && list[m].hermitian;
+  // the class kernels go round-robin onto st and the NAUX auxiliary streams
+  // (they only add into Ac and the counters: order-free), so each persistent
+  // launch's tail overlaps the next one's start; fork here, join after the
+  // loop
+  CQF_CUDA(cudaEventRecord(B->evFork, st));
+  for (int i = 0; i < NAUX; i++) CQF_CUDA(cudaStreamWaitEvent(B->aux[i], B->evFork, 0));
+  cudaStream_t lanes[NAUX + 1] = {st};
+  for (int i = 0; i < NAUX; i++) lanes[1 + i] = B->aux[i];
+  int nlaunch = 0;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck <= cb; ck++) {
       if (!B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
@@ -1364,9 +1406,14 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.ketNGroups = B->cls_group_cnt[ck];
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
       unsigned int* w = work + 2 * (cb * NCLS + ck);
-      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, st)))
-        launch_jk_generic(a, la, lb, lc, ld, st);
+      const cudaStream_t ls = lanes[nlaunch++ % (NAUX + 1)];
+      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, ls)))
+        launch_jk_generic(a, la, lb, lc, ld, ls);
     }
+  for (int i = 0; i < NAUX; i++) {
+    CQF_CUDA(cudaEventRecord(B->evJoin[i], B->aux[i]));
+    CQF_CUDA(cudaStreamWaitEvent(st, B->evJoin[i], 0));
+  }
   CQF_CUDA(cudaGetLastError());
   for (int m = 0; m < nMat; m++)
     from_cart_kernel<<<grid1((size_t)N * N, 256), 256, 0, st>>>(

@@ -25,6 +25,7 @@ constexpr int MAXMAT = 512;
 
 // Tile-interleaved ket primitive data: fields p, Kp, o2p, P[3], PA[3], PB[3]
 // of KETT_TILE consecutive kets of a class (one persistent-kernel ket tile).
+constexpr int NAUX = 2;           // auxiliary streams of the class-quartet launches
 constexpr int KETT_NF = 12;
 constexpr int KETT_TILE = 128;
 constexpr int BRA_GROUP_MAX = 8;  // bra pairs per group (same first shell)
@@ -138,6 +139,11 @@ struct cqf_basis {
   int* d_flags = nullptr;                // MAXMAT per-matrix flags
   std::vector<int> h_flags;              // host staging of the flags
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // class-quartet kernels are spread over the call's stream and these NAUX
+  // (fork / join by events) so that each persistent launch's tail overlaps
+  // the next one's start; the streams come from a per-device pool
+  cudaStream_t aux[cqf::NAUX] = {};
+  cudaEvent_t evFork = nullptr, evJoin[cqf::NAUX] = {};
   // four-component path: Schwarz tables (computed on first use, nshell^2
   // each, zero for pairs outside the significant-pair list) and workspace
   double* d_qLL = nullptr;
