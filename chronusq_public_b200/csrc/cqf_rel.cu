@@ -1101,6 +1101,10 @@ __global__ void __launch_bounds__(RB_THREADS)
                 w34 * s12d * Js[cd]);
 }
 
+// Dynamic shared-memory limit of the block kernels (the largest layout, SSSS
+// (ff|ff), is 129 KB; LLSS layouts above it run per thread).
+constexpr size_t REL_SMEM_MAX = 160 * 1024;
+
 // One class in one arithmetic precision: the instance in T computes the
 // quartets that precision owns (every surviving one for double without the
 // mixed mode; with it, double takes bound >= cut and float the rest).
@@ -1124,10 +1128,11 @@ void launch_rel_prec(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStr
     // once, when it fits in shared memory; else per thread
     const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
     const size_t smem = (size_t)Lo.total * sizeof(double);
-    if (smem <= 160 * 1024) {
-      if (smem > 48 * 1024)
-        cudaFuncSetAttribute(rel_llss_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+    if (smem <= REL_SMEM_MAX) {
+      // always the same limit (on the current device), never one below a
+      // launch still queued
+      cudaFuncSetAttribute(rel_llss_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)REL_SMEM_MAX);
       const long long nq = (long long)a.nBra * a.nKet;
       const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
       const unsigned gy = (unsigned)((nq + gx - 1) / gx);
@@ -1142,9 +1147,8 @@ void launch_rel_prec(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStr
   // SSSS d and f classes: one block per quartet, intermediates in shared memory
   const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
   const size_t smem = (size_t)Lo.total * sizeof(double);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(rel_block_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+  cudaFuncSetAttribute(rel_block_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)REL_SMEM_MAX);
   const long long nq = (TYPE == 2 && a.same) ? (long long)a.nBra * (a.nBra + 1) / 2
                                              : (long long)a.nBra * a.nKet;
   const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
