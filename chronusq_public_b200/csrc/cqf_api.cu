@@ -681,6 +681,8 @@ cqf_status ensure_ws(cqf_basis* B, size_t bytes) {
   return CQF_OK;
 }
 
+void aux_release(int device, cudaStream_t s);
+
 void free_basis(cqf_basis* B) {
   if (!B) return;
   cudaSetDevice(B->device);
@@ -699,8 +701,10 @@ void free_basis(cqf_basis* B) {
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->evFork) cudaEventDestroy(B->evFork);
-  for (int i = 0; i < NAUX; i++)
+  for (int i = 0; i < NAUX; i++) {
     if (B->evJoin[i]) cudaEventDestroy(B->evJoin[i]);
+    aux_release(B->device, B->aux[i]);
+  }
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
 }
@@ -715,29 +719,43 @@ cqf_status upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
   return CQF_OK;
 }
 
-// Auxiliary streams of the class-quartet launches: a per-device pool created
-// once per process and lent round-robin to the bases (a server creates and
-// destroys a basis per request; creating streams each time costs set-up
-// latency).  Bases that share a pooled stream only order those launches.
+// Auxiliary streams of the class-quartet launches: a per-device free list.
+// A basis takes NAUX streams when it is created and gives them back when it
+// is destroyed, so no two live bases share one (a stream being captured into
+// a graph for one basis is never used by another) and a server that creates
+// and destroys a basis per request reuses streams instead of creating them
+// (stream creation showed in the set-up latency).  Streams are kept until
+// the process exits.
+struct AuxPool {
+  std::mutex mu;
+  std::vector<std::vector<cudaStream_t>> free;
+};
+AuxPool& aux_pool() {
+  static AuxPool p;
+  return p;
+}
+
 cqf_status aux_stream(int device, cudaStream_t* out) {
-  constexpr int POOL = 16;
-  static std::mutex mu;
-  static std::vector<std::vector<cudaStream_t>> pools;
-  static std::vector<unsigned> next;
-  std::lock_guard<std::mutex> lk(mu);
-  if ((int)pools.size() <= device) {
-    pools.resize(device + 1);
-    next.resize(device + 1, 0u);
-  }
-  if (pools[device].empty()) {
-    for (int i = 0; i < POOL; i++) {
-      cudaStream_t s = nullptr;
-      CQF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-      pools[device].push_back(s);
+  AuxPool& P = aux_pool();
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    if ((int)P.free.size() <= device) P.free.resize(device + 1);
+    if (!P.free[device].empty()) {
+      *out = P.free[device].back();
+      P.free[device].pop_back();
+      return CQF_OK;
     }
   }
-  *out = pools[device][next[device]++ % POOL];
+  CQF_CUDA(cudaStreamCreateWithFlags(out, cudaStreamNonBlocking));
   return CQF_OK;
+}
+
+void aux_release(int device, cudaStream_t s) {
+  if (!s) return;
+  AuxPool& P = aux_pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  if ((int)P.free.size() <= device) P.free.resize(device + 1);
+  P.free[device].push_back(s);
 }
 
 // Boys tables: computed once per process, one device copy per device (held
