@@ -666,6 +666,20 @@ __global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int he
 
 unsigned grid1(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// X <- (X + X^T) / 2 in place (n x n, column-major); each unordered pair
+// (i < j) belongs to one thread.
+__global__ void symmetrize_kernel(double* X, int n) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= (size_t)n * n) return;
+  const int i = (int)(k % n), j = (int)(k / n);
+  if (i >= j) return;
+  double* a = X + i + (size_t)j * n;
+  double* b = X + j + (size_t)i * n;
+  const double v = 0.5 * (*a + *b);
+  *a = v;
+  *b = v;
+}
+
 // Basis-owned device memory is stream-ordered on the basis' stream
 // (cudaMallocAsync / cudaFreeAsync): creating, growing or destroying one
 // basis never waits for the work of other bases (no device-wide sync).  The
@@ -1330,8 +1344,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   // call on this basis has synchronised), or already on the device (graphs)
   const int* d_flags = d_flags_pre;
   if (!d_flags) {
-    for (int m = 0; m < nMat; m++)
-      B->h_flags[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
+    for (int m = 0; m < nMat; m++) B->h_flags[m] = contraction_flags(list[m], opts.is_complex != 0);
     CQF_CUDA(cudaMemcpyAsync(B->d_flags, B->h_flags.data(), nMat * sizeof(int), cudaMemcpyHostToDevice,
                              st));
     d_flags = B->d_flags;
@@ -1352,10 +1365,13 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   norms_aux_kernel<<<grid1(std::max(ns2, (size_t)B->npair), 256), 256, 0, st>>>(
       ws + oNm, ns, B->d_pairs, B->npair, ws + Lw.oNmT, ws + Lw.oPN);
   // densities to the Cartesian AO basis, zero accumulators
-  for (int m = 0; m < nMat; m++)
+  for (int m = 0; m < nMat; m++) {
     to_cart_kernel<<<grid1((size_t)nc * nc, 256), 256, 0, st>>>(
         Xd[m], opts.is_complex, N, nc, B->d_shells, B->d_cart2shell, B->d_sph, B->d_sphOff,
         ws + oXc + m * matC);
+    if (!list[m].hermitian && hermitian_eff(list[m], opts.is_complex != 0))
+      symmetrize_kernel<<<grid1((size_t)nc * nc, 256), 256, 0, st>>>(ws + oXc + m * matC, nc);
+  }
   CQF_CUDA(cudaMemsetAsync(ws + oAc, 0, matC * nMat * sizeof(double), st));
   CQF_CUDA(cudaGetLastError());
 
@@ -1395,7 +1411,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   }
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;
-  for (int m = 0; m < nMat; m++) fastOK = fastOK && list[m].hermitian;
+  for (int m = 0; m < nMat; m++) fastOK = fastOK && hermitian_eff(list[m], false);
   // the class kernels go round-robin onto st and the NAUX auxiliary streams
   // (they only add into Ac and the counters: order-free), so each persistent
   // launch's tail overlaps the next one's start; fork here, join after the
@@ -1435,7 +1451,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   CQF_CUDA(cudaGetLastError());
   for (int m = 0; m < nMat; m++)
     from_cart_kernel<<<grid1((size_t)N * N, 256), 256, 0, st>>>(
-        ws + oAc + m * matC, opts.is_complex, list[m].hermitian, N, nc, B->d_shells,
+        ws + oAc + m * matC, opts.is_complex, hermitian_eff(list[m], opts.is_complex != 0) ? 1 : 0,
+        N, nc, B->d_shells,
         B->d_ao2shell, B->d_sph, B->d_sphOff, AXd[m]);
   CQF_CUDA(cudaGetLastError());
   if (host)

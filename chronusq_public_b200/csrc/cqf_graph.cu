@@ -43,7 +43,7 @@ cqf_status create(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf
   CQF_GCUDA(cudaMalloc(&G->d_flags, nMat * sizeof(int)));
   std::vector<int> fl(nMat);
   for (int m = 0; m < nMat; m++)
-    fl[m] = (list[m].hermitian ? 1 : 0) | (list[m].type == CQF_EXCHANGE ? 2 : 0);
+    fl[m] = cqf::contraction_flags(list[m], opts.is_complex != 0);
   CQF_GCUDA(cudaMemcpy(G->d_flags, fl.data(), nMat * sizeof(int), cudaMemcpyHostToDevice));
   // warm-up into throw-away outputs, so every kernel of the graph is loaded
   // before capture starts

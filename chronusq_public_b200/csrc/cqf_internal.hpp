@@ -84,6 +84,19 @@ cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, 
 // doubles; the caller holds B->mu and has made B's device current.
 // With capture = true nothing synchronises or reads back (stream capture);
 // d_flags_pre: per-matrix flags already on the device (else uploaded here).
+// A real Coulomb contraction of a non-Hermitian X equals that of its
+// symmetric part (J[X] = J[(X + X^T)/2], as (ab|cd) = (ab|dc); the
+// reference's non-Hermitian J branch, direct.hpp:1920-1950, symmetrises the
+// same way), so it runs as a Hermitian one on the symmetrised Cartesian
+// density; the screen keeps the norms of X as given.
+inline bool hermitian_eff(const cqf_contraction& c, bool cplx) {
+  return c.hermitian || (!cplx && c.type == CQF_COULOMB);
+}
+// per-matrix kernel flags: bit 0 Hermitian (effective), bit 1 exchange
+inline int contraction_flags(const cqf_contraction& c, bool cplx) {
+  return (hermitian_eff(c, cplx) ? 1 : 0) | (c.type == CQF_EXCHANGE ? 2 : 0);
+}
+
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
                          const int* d_flags_pre);

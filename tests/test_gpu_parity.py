@@ -227,3 +227,19 @@ def test_edge_empty_contraction_list():
     st = _cabi.CqfStats()
     assert _cabi.lib().cqf_two_body_contract(tpi.handle, None, 0, None,
                                              C.byref(st)) == _cabi.CQF_EINVAL
+
+
+def test_nonhermitian_real_coulomb_fast_path():
+    """Real non-Hermitian J (MOIntsTransformer's pseudo-densities) runs on the
+    fast kernels through its symmetric part; it must match the oracle's
+    non-Hermitian branch, several densities in one call."""
+    basis, tpi, ob, D = _oracle_and_device("h2o8_ccpvdz")
+    rng = np.random.default_rng(17)
+    N = basis.nbasis
+    Xs = [np.asfortranarray(0.1 * rng.standard_normal((N, N))) for _ in range(3)]
+    outs = [np.zeros((N, N), order="F") for _ in Xs]
+    GTODirectTPIContraction(tpi).twoBodyContract(
+        [TwoBodyContraction(X, J, False, COULOMB) for X, J in zip(Xs, outs)])
+    refs = ob.contract(Xs, [0, 0, 0], [0, 0, 0])
+    for J, Jo in zip(outs, refs):
+        assert np.abs(J - Jo).max() < FP64_TOL
