@@ -647,7 +647,12 @@ __global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int he
   double r1, i1;
   bval(i, j, r1, i1);
   double outr, outi;
-  if (her) {
+  if (her == 2) {  // real antisymmetric density: exchange stored transposed
+    double r2, i2;
+    bval(j, i, r2, i2);
+    outr = 0.5 * (r2 - r1);
+    outi = 0.0;
+  } else if (her) {
     double r2, i2;
     bval(j, i, r2, i2);
     outr = 0.5 * (r1 + r2);
@@ -665,6 +670,24 @@ __global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int he
 }
 
 unsigned grid1(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// Real and imaginary parts of an interleaved complex matrix (n entries).
+__global__ void split_complex_kernel(const double* __restrict__ Xc, size_t n, double* re,
+                                     double* im) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  re[k] = Xc[2 * k];
+  if (im) im[k] = Xc[2 * k + 1];
+}
+
+// AXc += re + i im (interleaved complex; im may be null).
+__global__ void add_complex_kernel(double* AXc, size_t n, const double* __restrict__ re,
+                                   const double* __restrict__ im) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  AXc[2 * k] += re[k];
+  if (im) AXc[2 * k + 1] += im[k];
+}
 
 // X <- (X + X^T) / 2 in place (n x n, column-major); each unordered pair
 // (i < j) belongs to one thread.
@@ -1308,12 +1331,93 @@ cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, 
   return CQF_OK;
 }
 
+cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
+                         const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
+                         const int* d_flags_pre, const double* const* normSrc);
+
+// Complex Hermitian densities on the real fast kernels: with X = S + iA (S
+// real symmetric, A real antisymmetric), J[X] = J[S] and K[X] = K[S] + i K[A],
+// so one real contraction -- J on S, K on S and K on A (flagged
+// antisymmetric) -- gives every result; the screen uses the norms of the
+// complex X, as the reference's does.  Used when every class of the basis
+// runs on the fast kernels (l <= 2).  Caller holds B->mu, device current.
+cqf_status contract_complex_split(cqf_basis* B, const cqf_contraction* list, int nMat, int nReal,
+                                  const cqf_opts& opts, cqf_stats* stats) {
+  cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  const size_t blk = (NN + 31) / 32 * 32;
+  const bool host = !opts.device_pointers;
+  cqf_opts ro = opts;
+  ro.is_complex = 0;
+  ro.device_pointers = 1;
+  const size_t inner = ws_layout(B, nReal, ro).total;
+  // [inner workspace | complex X, AX staging (host pointers) | real X | real AX]
+  const size_t total = inner + (host ? 4 * blk * nMat : 0) + 2 * blk * nReal;
+  CQF_TRY(ensure_ws(B, total * sizeof(double)));
+  double* ws = static_cast<double*>(B->d_ws);
+  double* stage = ws + inner;
+  double* rX = stage + (host ? 4 * blk * nMat : 0);
+  double* rA = rX + blk * nReal;
+  std::vector<const double*> Xc(nMat);
+  std::vector<double*> AXc(nMat);
+  for (int m = 0; m < nMat; m++) {
+    if (host) {
+      double* x = stage + 4 * blk * m;
+      double* ax = x + 2 * blk;
+      CQF_CUDA(cudaMemcpyAsync(x, list[m].X, 2 * NN * sizeof(double), cudaMemcpyHostToDevice,
+                               st));
+      CQF_CUDA(cudaMemcpyAsync(ax, list[m].AX, 2 * NN * sizeof(double), cudaMemcpyHostToDevice,
+                               st));
+      Xc[m] = x;
+      AXc[m] = ax;
+    } else {
+      Xc[m] = static_cast<const double*>(list[m].X);
+      AXc[m] = static_cast<double*>(list[m].AX);
+    }
+  }
+  std::vector<cqf_contraction> rl;
+  std::vector<const double*> src;
+  std::vector<int> owner;  // real entry -> (matrix, part: 0 real, 1 imaginary)
+  for (int m = 0; m < nMat; m++) {
+    const bool k = list[m].type == CQF_EXCHANGE;
+    double* re = rX + blk * rl.size();
+    double* im = k ? re + blk : nullptr;
+    split_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(Xc[m], NN, re, im);
+    rl.push_back({re, rA + blk * rl.size(), 1, list[m].type});
+    src.push_back(Xc[m]);
+    owner.push_back(2 * m);
+    if (k) {
+      rl.push_back({im, rA + blk * rl.size(), -1, CQF_EXCHANGE});
+      src.push_back(Xc[m]);
+      owner.push_back(2 * m + 1);
+    }
+  }
+  CQF_CUDA(cudaMemsetAsync(rA, 0, blk * nReal * sizeof(double), st));
+  CQF_CUDA(cudaGetLastError());
+  CQF_TRY(contract_core(B, rl.data(), nReal, ro, stats, ws, false, nullptr, src.data()));
+  for (int r = 0; r < nReal; r++) {
+    if (owner[r] & 1) continue;  // added with its real part
+    const int m = owner[r] >> 1;
+    const bool k = list[m].type == CQF_EXCHANGE;
+    add_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(
+        AXc[m], NN, static_cast<const double*>(rl[r].AX),
+        k ? static_cast<const double*>(rl[r + 1].AX) : nullptr);
+  }
+  CQF_CUDA(cudaGetLastError());
+  if (host)
+    for (int m = 0; m < nMat; m++)
+      CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXc[m], 2 * NN * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+  CQF_CUDA(cudaStreamSynchronize(st));
+  return CQF_OK;
+}
+
 // The contraction pipeline on a caller-provided workspace `ws` of at least
 // ws_layout(...).total doubles (device memory).  Caller holds B->mu and has
 // made B's device current.
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
-                         const int* d_flags_pre) {
+                         const int* d_flags_pre, const double* const* normSrc) {
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const int cw = opts.is_complex ? 2 : 1;
@@ -1356,8 +1460,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   // shell-block norms (per matrix, symmetrised when non-Hermitian), max
   for (int m = 0; m < nMat; m++) {
     double* nm = ws + oNmM + m * ns2;
-    block_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(Xd[m], opts.is_complex, N, B->d_shells, ns,
-                                                        nm);
+    block_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(
+        normSrc ? normSrc[m] : Xd[m], normSrc ? 1 : opts.is_complex, N, B->d_shells, ns, nm);
     if (!list[m].hermitian) sym_norms_kernel<<<grid1(ns2, 128), 128, 0, st>>>(nm, ns);
   }
   max_norms_kernel<<<grid1(ns2, 256), 256, 0, st>>>(ws + oNmM, nMat, ns2, ws + oNm,
@@ -1451,7 +1555,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   CQF_CUDA(cudaGetLastError());
   for (int m = 0; m < nMat; m++)
     from_cart_kernel<<<grid1((size_t)N * N, 256), 256, 0, st>>>(
-        ws + oAc + m * matC, opts.is_complex, hermitian_eff(list[m], opts.is_complex != 0) ? 1 : 0,
+        ws + oAc + m * matC, opts.is_complex,
+        list[m].hermitian < 0 ? 2 : (hermitian_eff(list[m], opts.is_complex != 0) ? 1 : 0),
         N, nc, B->d_shells,
         B->d_ao2shell, B->d_sph, B->d_sphOff, AXd[m]);
   CQF_CUDA(cudaGetLastError());
@@ -1482,17 +1587,28 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
 
 extern "C" {
 
-cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* list, int nMat,
+cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* listIn, int nMat,
                                  const cqf_opts* optsIn, cqf_stats* stats) {
   g_err.clear();
-  CQF_TRY(check_contract_args(B, list, nMat));
+  CQF_TRY(check_contract_args(B, listIn, nMat));
   cqf_opts opts;
   cqf_opts_default(&opts);
   if (optsIn) opts = *optsIn;
+  // TwoBodyContraction::HER is a bool: any nonzero value is Hermitian
+  std::vector<cqf_contraction> list(listIn, listIn + nMat);
+  bool allHer = true;
+  for (auto& c : list) {
+    c.hermitian = c.hermitian ? 1 : 0;
+    allHer = allHer && c.hermitian;
+  }
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_CUDA(cudaSetDevice(B->device));
+  int nReal = 0;
+  for (auto& c : list) nReal += c.type == CQF_EXCHANGE ? 2 : 1;
+  if (opts.is_complex && allHer && B->maxL <= 2 && nReal <= MAXMAT)
+    return contract_complex_split(B, list.data(), nMat, nReal, opts, stats);
   CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
-  return contract_core(B, list, nMat, opts, stats, static_cast<double*>(B->d_ws), false,
+  return contract_core(B, list.data(), nMat, opts, stats, static_cast<double*>(B->d_ws), false,
                        nullptr);
 }
 

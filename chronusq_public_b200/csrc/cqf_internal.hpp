@@ -92,14 +92,20 @@ cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, 
 inline bool hermitian_eff(const cqf_contraction& c, bool cplx) {
   return c.hermitian || (!cplx && c.type == CQF_COULOMB);
 }
-// per-matrix kernel flags: bit 0 Hermitian (effective), bit 1 exchange
+// per-matrix kernel flags: bit 0 Hermitian (effective), bit 1 exchange,
+// bit 2 real antisymmetric (hermitian = -1: only the library's own split of
+// a complex Hermitian density makes such entries)
 inline int contraction_flags(const cqf_contraction& c, bool cplx) {
-  return (hermitian_eff(c, cplx) ? 1 : 0) | (c.type == CQF_EXCHANGE ? 2 : 0);
+  return (hermitian_eff(c, cplx) ? 1 : 0) | (c.type == CQF_EXCHANGE ? 2 : 0) |
+         (c.hermitian < 0 ? 4 : 0);
 }
 
+// normSrc (optional, device pointers): per entry, the complex matrix whose
+// shell-block norms screen it in place of its own X (the split of a complex
+// Hermitian density keeps the reference's complex screen).
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
-                         const int* d_flags_pre);
+                         const int* d_flags_pre, const double* const* normSrc = nullptr);
 
 // Launch helpers shared with the four-component path (cqf_api.cu).
 // Shell-block infinity norms of one N x N matrix (complex: |z|).

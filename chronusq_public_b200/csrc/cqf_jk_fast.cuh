@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
       for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
       const double* X = a.Xc + m * matStride;
       double* A = a.Ac + m * matStride;
-      G64::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
+      G64::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, (fl & 4) ? -sK : sK,
+                  doJ && work_, doK && work_,
                   jab);
       if (doJ) {
         // every lane of the warp shares the bra pair: reduce, one atomic each
@@ -341,7 +342,8 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
         for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
         const double* X = a.Xc + m * matStride;
         double* A = a.Ac + m * matStride;
-        G64::digest_g(I, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, doJ && work_, doK && work_,
+        G64::digest_g(I, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, (fl & 4) ? -sK : sK,
+                      doJ && work_, doK && work_,
                       jab, jcd, kac, kad);
         if (!grouped && work_) {  // flush this matrix's sums now
 #pragma unroll

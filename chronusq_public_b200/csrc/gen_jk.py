@@ -296,7 +296,7 @@ def emit_digest_g(w, A, B, Cc, Dd):
     w.line("static constexpr int NJCD = %d, NKAC = %d, NKAD = %d;" % (NCD, NA * NC, NA * ND))
     w.open("static __device__ __forceinline__ void digest_g(const double (&I)[%d], "
            "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
-           "int cC, int cD, double sJ, double sK, bool doJ, bool doK, double (&jab)[%d], "
+           "int cC, int cD, double sJ, double sK, double sKac, bool doJ, bool doK, double (&jab)[%d], "
            "double (&jcd)[%d], double (&kac)[%d], double (&kad)[%d]) {"
            % (NAB * NCD, NAB, NCD, NA * NC, NA * ND))
     w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
@@ -328,7 +328,7 @@ def emit_digest_g(w, A, B, Cc, Dd):
         for c in range(NC):
             sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
                             for b_ in range(NB) for (k, cc, d) in els if cc == c)
-            w.line("kac[%d] += sK * (%s);" % (a_ * NC + c, sm))
+            w.line("kac[%d] += sKac * (%s);" % (a_ * NC + c, sm))
     for a_ in range(NA):
         for c in range(NC):
             w.line("const double dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
@@ -523,10 +523,12 @@ def gen_class(la, lb, lc, ld, prec):
         w.close("}")  # ip
         w.close("}")  # eri
     # ---- digestion
-    w.line("// J/K contributions of chunk ch for one density (symmetric X)")
+    w.line("// J/K contributions of chunk ch for one density (symmetric X).  The")
+    w.line("// K_ac update reads X(d, b) (the other three read X in bra-row order): sKac")
+    w.line("// = sK for a symmetric X, -sK for an antisymmetric one")
     w.open("static __device__ __forceinline__ void digest(const double (&I)[%d], const int ch, "
            "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
-           "int cC, int cD, double sJ, double sK, bool doJ, bool doK, double (&jab)[%d]) {"
+           "int cC, int cD, double sJ, double sK, double sKac, bool doJ, bool doK, double (&jab)[%d]) {"
            % (NAB * CS, NAB))
     w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
     w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
@@ -565,7 +567,7 @@ def gen_class(la, lb, lc, ld, prec):
             for c in cs_:
                 sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
                                 for b_ in range(NB) for (k, cc, d) in els if cc == c)
-                w.line("add(cC + %d, cA + %d, sK * (%s));" % (c, a_, sm))
+                w.line("add(cC + %d, cA + %d, sKac * (%s));" % (c, a_, sm))
         # K_bd += sum_ac I D[a,c]
         for a_ in range(NA):
             for c in cs_:

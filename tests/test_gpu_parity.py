@@ -243,3 +243,60 @@ def test_nonhermitian_real_coulomb_fast_path():
     refs = ob.contract(Xs, [0, 0, 0], [0, 0, 0])
     for J, Jo in zip(outs, refs):
         assert np.abs(J - Jo).max() < FP64_TOL
+
+
+def _herm_complex(N, seed, scale=0.1):
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+    return np.asfortranarray(scale * 0.5 * (A + A.conj().T))
+
+
+@pytest.mark.parametrize("name", ["h2o_ccpvdz", "h2o8_ccpvdz"])
+def test_complex_hermitian_fast_split(name):
+    """Complex Hermitian J and K (s..d basis) through the real fast kernels
+    -- J[S], K[S] + i K[A] for X = S + iA -- against the oracle's complex
+    Hermitian branch; AX accumulates into what it held."""
+    basis, tpi, ob, _D = _oracle_and_device(name)
+    N = basis.nbasis
+    X1, X2 = _herm_complex(N, 31), _herm_complex(N, 32)
+    J = np.asfortranarray(np.full((N, N), 0.25 + 0.5j))
+    K1 = np.zeros((N, N), complex, order="F")
+    K2 = np.zeros((N, N), complex, order="F")
+    GTODirectTPIContraction(tpi).twoBodyContract(
+        [TwoBodyContraction(X1, J, True, COULOMB), TwoBodyContraction(X1, K1, True, EXCHANGE),
+         TwoBodyContraction(X2, K2, True, EXCHANGE)])
+    Jo, K1o, K2o = ob.contract([X1, X1, X2], [1, 1, 1], [0, 1, 1])
+    assert np.abs(J - (Jo + (0.25 + 0.5j))).max() < FP64_TOL
+    assert np.abs(K1 - K1o).max() < FP64_TOL
+    assert np.abs(K2 - K2o).max() < FP64_TOL
+    assert np.abs(K1.imag).max() > 1e-3  # the antisymmetric part is exercised
+
+
+def test_complex_hermitian_fast_split_device_pointers():
+    import torch
+    basis, tpi, ob, _D = _oracle_and_device("h2o_ccpvdz")
+    N = basis.nbasis
+    X = _herm_complex(N, 33)
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).cuda().t()
+    Jd = torch.zeros((N, N), dtype=torch.complex128, device="cuda").t()
+    Kd = torch.zeros((N, N), dtype=torch.complex128, device="cuda").t()
+    GTODirectTPIContraction(tpi).twoBodyContract(
+        [TwoBodyContraction(Xd, Jd, True, COULOMB), TwoBodyContraction(Xd, Kd, True, EXCHANGE)])
+    torch.cuda.synchronize()
+    Jo, Ko = ob.contract([X, X], [1, 1], [0, 1])
+    assert np.abs(Jd.cpu().numpy() - Jo).max() < FP64_TOL
+    assert np.abs(Kd.cpu().numpy() - Ko).max() < FP64_TOL
+
+
+def test_complex_hermitian_f_shells_generic():
+    """With f shells the complex Hermitian build stays on the generic kernel."""
+    basis = contract_basis()
+    assert basis.max_l == 3
+    tpi = DirectTPI(basis)
+    ob = O.OracleBasis(basis)
+    X = _herm_complex(basis.nbasis, 34, 0.05)
+    N = basis.nbasis
+    K = np.zeros((N, N), complex, order="F")
+    GTODirectTPIContraction(tpi).twoBodyContract([TwoBodyContraction(X, K, True, EXCHANGE)])
+    Ko, = ob.contract([X], [1], [1])
+    assert np.abs(K - Ko).max() < FP64_TOL
