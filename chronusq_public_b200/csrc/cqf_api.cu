@@ -1340,73 +1340,119 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
 // so one real contraction -- J on S, K on S and K on A (flagged
 // antisymmetric) -- gives every result; the screen uses the norms of the
 // complex X, as the reference's does.  Used when every class of the basis
-// runs on the fast kernels (l <= 2).  Caller holds B->mu, device current.
-cqf_status contract_complex_split(cqf_basis* B, const cqf_contraction* list, int nMat, int nReal,
+// runs on the fast kernels (l <= 2; split_eligible).
+
+bool split_eligible(const cqf_basis* B, const cqf_contraction* list, int nMat,
+                    const cqf_opts& opts) {
+  if (!opts.is_complex || B->maxL > 2) return false;
+  int nReal = 0;
+  for (int m = 0; m < nMat; m++) {
+    if (!list[m].hermitian) return false;
+    nReal += list[m].type == CQF_EXCHANGE ? 2 : 1;
+  }
+  return nReal <= MAXMAT;
+}
+
+// The real contraction list of a split, in order: per complex entry its real
+// part, and for exchange its imaginary part (hermitian = -1) after it.
+int split_real_count(const cqf_contraction* list, int nMat) {
+  int n = 0;
+  for (int m = 0; m < nMat; m++) n += list[m].type == CQF_EXCHANGE ? 2 : 1;
+  return n;
+}
+void split_flags(const cqf_contraction* list, int nMat, int* fl) {
+  int r = 0;
+  for (int m = 0; m < nMat; m++) {
+    cqf_contraction c{nullptr, nullptr, 1, list[m].type};
+    fl[r++] = contraction_flags(c, false);
+    if (list[m].type == CQF_EXCHANGE) {
+      c.hermitian = -1;
+      fl[r++] = contraction_flags(c, false);
+    }
+  }
+}
+
+// Workspace (doubles) of split_core: the real contraction's | real X | real AX.
+size_t split_ws_doubles(const cqf_basis* B, int nReal, const cqf_opts& opts) {
+  cqf_opts ro = opts;
+  ro.is_complex = 0;
+  ro.device_pointers = 1;
+  const size_t blk = ((size_t)B->nbasis * B->nbasis + 31) / 32 * 32;
+  return ws_layout(B, nReal, ro).total + 2 * blk * nReal;
+}
+
+// The split on device pointers and a caller-provided workspace; with
+// `capture` it only enqueues (stream capture), like contract_core.
+cqf_status split_core(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf_opts& opts,
+                      cqf_stats* stats, double* ws, bool capture, const int* d_flags_pre) {
+  cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  const size_t blk = (NN + 31) / 32 * 32;
+  const int nReal = split_real_count(list, nMat);
+  cqf_opts ro = opts;
+  ro.is_complex = 0;
+  ro.device_pointers = 1;
+  double* rX = ws + ws_layout(B, nReal, ro).total;
+  double* rA = rX + blk * nReal;
+  std::vector<cqf_contraction> rl;
+  std::vector<const double*> src;
+  for (int m = 0; m < nMat; m++) {
+    const bool k = list[m].type == CQF_EXCHANGE;
+    const double* X = static_cast<const double*>(list[m].X);
+    double* re = rX + blk * rl.size();
+    split_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(X, NN, re, k ? re + blk : nullptr);
+    rl.push_back({re, rA + blk * rl.size(), 1, list[m].type});
+    src.push_back(X);
+    if (k) {
+      rl.push_back({re + blk, rA + blk * rl.size(), -1, CQF_EXCHANGE});
+      src.push_back(X);
+    }
+  }
+  CQF_CUDA(cudaMemsetAsync(rA, 0, blk * nReal * sizeof(double), st));
+  CQF_CUDA(cudaGetLastError());
+  CQF_TRY(contract_core(B, rl.data(), nReal, ro, stats, ws, capture, d_flags_pre, src.data()));
+  for (int m = 0, r = 0; m < nMat; m++) {
+    const bool k = list[m].type == CQF_EXCHANGE;
+    add_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(
+        static_cast<double*>(list[m].AX), NN, static_cast<const double*>(rl[r].AX),
+        k ? static_cast<const double*>(rl[r + 1].AX) : nullptr);
+    r += k ? 2 : 1;
+  }
+  CQF_CUDA(cudaGetLastError());
+  return CQF_OK;
+}
+
+// cqf_two_body_contract's split: host pointers are staged on the device.
+// Caller holds B->mu, device current.
+cqf_status contract_complex_split(cqf_basis* B, const cqf_contraction* list, int nMat,
                                   const cqf_opts& opts, cqf_stats* stats) {
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const size_t NN = (size_t)B->nbasis * B->nbasis;
   const size_t blk = (NN + 31) / 32 * 32;
   const bool host = !opts.device_pointers;
-  cqf_opts ro = opts;
-  ro.is_complex = 0;
-  ro.device_pointers = 1;
-  const size_t inner = ws_layout(B, nReal, ro).total;
-  // [inner workspace | complex X, AX staging (host pointers) | real X | real AX]
-  const size_t total = inner + (host ? 4 * blk * nMat : 0) + 2 * blk * nReal;
-  CQF_TRY(ensure_ws(B, total * sizeof(double)));
+  const size_t inner = split_ws_doubles(B, split_real_count(list, nMat), opts);
+  // [split workspace | complex X, AX staging (host pointers)]
+  CQF_TRY(ensure_ws(B, (inner + (host ? 4 * blk * nMat : 0)) * sizeof(double)));
   double* ws = static_cast<double*>(B->d_ws);
-  double* stage = ws + inner;
-  double* rX = stage + (host ? 4 * blk * nMat : 0);
-  double* rA = rX + blk * nReal;
-  std::vector<const double*> Xc(nMat);
-  std::vector<double*> AXc(nMat);
-  for (int m = 0; m < nMat; m++) {
-    if (host) {
-      double* x = stage + 4 * blk * m;
+  std::vector<cqf_contraction> dl(list, list + nMat);
+  if (host) {
+    for (int m = 0; m < nMat; m++) {
+      double* x = ws + inner + 4 * blk * m;
       double* ax = x + 2 * blk;
       CQF_CUDA(cudaMemcpyAsync(x, list[m].X, 2 * NN * sizeof(double), cudaMemcpyHostToDevice,
                                st));
       CQF_CUDA(cudaMemcpyAsync(ax, list[m].AX, 2 * NN * sizeof(double), cudaMemcpyHostToDevice,
                                st));
-      Xc[m] = x;
-      AXc[m] = ax;
-    } else {
-      Xc[m] = static_cast<const double*>(list[m].X);
-      AXc[m] = static_cast<double*>(list[m].AX);
+      dl[m].X = x;
+      dl[m].AX = ax;
     }
   }
-  std::vector<cqf_contraction> rl;
-  std::vector<const double*> src;
-  std::vector<int> owner;  // real entry -> (matrix, part: 0 real, 1 imaginary)
-  for (int m = 0; m < nMat; m++) {
-    const bool k = list[m].type == CQF_EXCHANGE;
-    double* re = rX + blk * rl.size();
-    double* im = k ? re + blk : nullptr;
-    split_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(Xc[m], NN, re, im);
-    rl.push_back({re, rA + blk * rl.size(), 1, list[m].type});
-    src.push_back(Xc[m]);
-    owner.push_back(2 * m);
-    if (k) {
-      rl.push_back({im, rA + blk * rl.size(), -1, CQF_EXCHANGE});
-      src.push_back(Xc[m]);
-      owner.push_back(2 * m + 1);
-    }
-  }
-  CQF_CUDA(cudaMemsetAsync(rA, 0, blk * nReal * sizeof(double), st));
-  CQF_CUDA(cudaGetLastError());
-  CQF_TRY(contract_core(B, rl.data(), nReal, ro, stats, ws, false, nullptr, src.data()));
-  for (int r = 0; r < nReal; r++) {
-    if (owner[r] & 1) continue;  // added with its real part
-    const int m = owner[r] >> 1;
-    const bool k = list[m].type == CQF_EXCHANGE;
-    add_complex_kernel<<<grid1(NN, 256), 256, 0, st>>>(
-        AXc[m], NN, static_cast<const double*>(rl[r].AX),
-        k ? static_cast<const double*>(rl[r + 1].AX) : nullptr);
-  }
-  CQF_CUDA(cudaGetLastError());
+  cqf_opts dopts = opts;
+  dopts.device_pointers = 1;
+  CQF_TRY(split_core(B, dl.data(), nMat, dopts, stats, ws, false, nullptr));
   if (host)
     for (int m = 0; m < nMat; m++)
-      CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXc[m], 2 * NN * sizeof(double),
+      CQF_CUDA(cudaMemcpyAsync(list[m].AX, dl[m].AX, 2 * NN * sizeof(double),
                                cudaMemcpyDeviceToHost, st));
   CQF_CUDA(cudaStreamSynchronize(st));
   return CQF_OK;
@@ -1603,10 +1649,8 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* listIn, in
   }
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_CUDA(cudaSetDevice(B->device));
-  int nReal = 0;
-  for (auto& c : list) nReal += c.type == CQF_EXCHANGE ? 2 : 1;
-  if (opts.is_complex && allHer && B->maxL <= 2 && nReal <= MAXMAT)
-    return contract_complex_split(B, list.data(), nMat, nReal, opts, stats);
+  if (allHer && split_eligible(B, list.data(), nMat, opts))
+    return contract_complex_split(B, list.data(), nMat, opts, stats);
   CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
   return contract_core(B, list.data(), nMat, opts, stats, static_cast<double*>(B->d_ws), false,
                        nullptr);

@@ -38,13 +38,23 @@ void release(cqf_graph* G) {
 cqf_status create(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf_opts& opts,
                   cqf_graph* G) {
   G->B = B;
-  const size_t wsd = cqf::ws_layout(B, nMat, opts).total;
+  // complex Hermitian densities on an s..d basis: the real split
+  const bool split = cqf::split_eligible(B, list, nMat, opts);
+  const int nFlags = split ? cqf::split_real_count(list, nMat) : nMat;
+  const size_t wsd = split ? cqf::split_ws_doubles(B, nFlags, opts)
+                           : cqf::ws_layout(B, nMat, opts).total;
   CQF_GCUDA(cudaMalloc(&G->ws, wsd * sizeof(double)));
-  CQF_GCUDA(cudaMalloc(&G->d_flags, nMat * sizeof(int)));
-  std::vector<int> fl(nMat);
-  for (int m = 0; m < nMat; m++)
-    fl[m] = cqf::contraction_flags(list[m], opts.is_complex != 0);
-  CQF_GCUDA(cudaMemcpy(G->d_flags, fl.data(), nMat * sizeof(int), cudaMemcpyHostToDevice));
+  CQF_GCUDA(cudaMalloc(&G->d_flags, nFlags * sizeof(int)));
+  std::vector<int> fl(nFlags);
+  if (split)
+    cqf::split_flags(list, nMat, fl.data());
+  else
+    for (int m = 0; m < nMat; m++) fl[m] = cqf::contraction_flags(list[m], opts.is_complex != 0);
+  CQF_GCUDA(cudaMemcpy(G->d_flags, fl.data(), nFlags * sizeof(int), cudaMemcpyHostToDevice));
+  auto run = [&](const cqf_contraction* l, const cqf_opts& o, bool capture) {
+    return split ? cqf::split_core(B, l, nMat, o, nullptr, G->ws, capture, G->d_flags)
+                 : cqf::contract_core(B, l, nMat, o, nullptr, G->ws, capture, G->d_flags);
+  };
   // warm-up into throw-away outputs, so every kernel of the graph is loaded
   // before capture starts
   const size_t matN = (size_t)B->nbasis * B->nbasis * (opts.is_complex ? 2 : 1);
@@ -54,13 +64,13 @@ cqf_status create(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf
   for (int m = 0; m < nMat; m++) warm[m].AX = tmp + m * matN;
   cqf_opts wo = opts;
   wo.stream = B->stream;
-  cqf_status s = cqf::contract_core(B, warm.data(), nMat, wo, nullptr, G->ws, false, G->d_flags);
+  cqf_status s = run(warm.data(), wo, false);
   cudaStreamSynchronize(B->stream);
   cudaFree(tmp);
   if (s != CQF_OK) return s;
   // capture on the basis' private stream
   CQF_GCUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
-  s = cqf::contract_core(B, list, nMat, wo, nullptr, G->ws, true, G->d_flags);
+  s = run(list, wo, true);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(B->stream, &g);
   if (s != CQF_OK) {

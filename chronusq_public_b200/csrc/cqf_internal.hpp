@@ -100,6 +100,17 @@ inline int contraction_flags(const cqf_contraction& c, bool cplx) {
          (c.hermitian < 0 ? 4 : 0);
 }
 
+// Complex Hermitian contractions on the real fast kernels (cqf_api.cu):
+// eligibility, real-entry count and flags, workspace, and the pipeline on
+// device pointers and a caller-provided workspace (capture-able).
+bool split_eligible(const cqf_basis* B, const cqf_contraction* list, int nMat,
+                    const cqf_opts& opts);
+int split_real_count(const cqf_contraction* list, int nMat);
+void split_flags(const cqf_contraction* list, int nMat, int* fl);
+size_t split_ws_doubles(const cqf_basis* B, int nReal, const cqf_opts& opts);
+cqf_status split_core(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf_opts& opts,
+                      cqf_stats* stats, double* ws, bool capture, const int* d_flags_pre);
+
 // normSrc (optional, device pointers): per entry, the complex matrix whose
 // shell-block norms screen it in place of its own X (the split of a complex
 // Hermitian density keeps the reference's complex screen).

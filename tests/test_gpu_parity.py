@@ -300,3 +300,33 @@ def test_complex_hermitian_f_shells_generic():
     GTODirectTPIContraction(tpi).twoBodyContract([TwoBodyContraction(X, K, True, EXCHANGE)])
     Ko, = ob.contract([X], [1], [1])
     assert np.abs(K - Ko).max() < FP64_TOL
+
+
+def test_complex_hermitian_graph_split():
+    """Complex Hermitian J/K (the density of an RT-TDDFT step) captured as a
+    CUDA graph on the real split: the first replay matches the oracle, the
+    second accumulates the same again."""
+    import torch
+    from chronusq_public_b200.contraction import ContractionGraph
+    basis, tpi, ob, _D = _oracle_and_device("h2o_ccpvdz")
+    N = tpi.nbasis
+    Xs = [_herm_complex(N, 40 + k) for k in range(3)]
+    Xd = [torch.from_numpy(np.ascontiguousarray(x.T)).cuda().t() for x in Xs]
+    outs = [torch.zeros((N, N), dtype=torch.complex128, device="cuda").t() for _ in range(6)]
+    cont = []
+    for k, X in enumerate(Xd):
+        cont.append(TwoBodyContraction(X, outs[2 * k], True, COULOMB))
+        cont.append(TwoBodyContraction(X, outs[2 * k + 1], True, EXCHANGE))
+    g = ContractionGraph(tpi, cont)
+    g.launch()
+    torch.cuda.synchronize()
+    first = [o.cpu().numpy() for o in outs]
+    g.launch()
+    torch.cuda.synchronize()
+    for o, f in zip(outs, first):
+        assert np.abs(o.cpu().numpy() - 2 * f).max() < 1e-12
+    for k, X in enumerate(Xs):
+        Jo, Ko = ob.contract([X, X], [1, 1], [COULOMB, EXCHANGE])
+        assert np.abs(first[2 * k] - Jo).max() < FP64_TOL
+        assert np.abs(first[2 * k + 1] - Ko).max() < FP64_TOL
+    g.close()
