@@ -16,6 +16,8 @@ e2e     = the same build through the public Python API with host (numpy)
 fp64    = the same, all quartets in FP64 (the reference precision).
 cutoff_sweep = the mixed build at the configuration's cutoffs 1e-6 .. 1e-10
           (builds/s, FP32 quartets, Fock and energy error).
+complex_build = the FP64 build of a complex Hermitian density (an RT-TDDFT
+          step's), same workload.
 batched_dD_graph = (H2O)8 / cc-pVDZ, 64 dD densities per CUDA-graph launch,
           FP64 and mixed, beside the same work one density per call in FP64
           (mixed_batched_over_fp64_single: the batched mixed rate over it).
@@ -570,6 +572,31 @@ def main():
         sweep.append({"fp32_cutoff": cut, "builds_per_s": 1e3 * len(msc) / sum(msc),
                       "quartets_fp32": stc["fp32"], "G": Gc})
 
+    # complex Hermitian density (an RT-TDDFT step's): J and K of D + i A, A a
+    # seeded antisymmetric perturbation, FP64, device pointers
+    rngc = np.random.default_rng(6)
+    Ac = rngc.standard_normal((N, N))
+    Xcx = torch.from_numpy(np.ascontiguousarray((D + 0.01j * (Ac - Ac.T)).T)).to(dev).t()
+    Jcx = torch.zeros((N, N), dtype=torch.complex128, device=dev).t()
+    Kcx = torch.zeros((N, N), dtype=torch.complex128, device=dev).t()
+    cxl = [TwoBodyContraction(Xcx, Jcx, True, COULOMB), TwoBodyContraction(Xcx, Kcx, True, EXCHANGE)]
+    for _ in range(args.warmup):
+        con.twoBodyContract(cxl, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    mscx = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        con.twoBodyContract(cxl, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        mscx.append(e0.elapsed_time(e1))
+    complex_build = {"what": "complex Hermitian J+K (D + i A), FP64, device pointers",
+                     "ms_per_build": float(np.median(mscx)),
+                     "builds_per_s": 1e3 / float(np.median(mscx))}
+
     # end-to-end through the public API with host buffers
     fb = FockBuilder(tpi)
     for _ in range(args.warmup):
@@ -654,6 +681,7 @@ def main():
                  "roofline_frac": frac64},
         "mixed_over_fp64": vmx / v64,
         "cutoff_sweep": sweep,
+        "complex_build": complex_build,
         "latency_ms": {"p50": float(np.percentile(msmx, 50)),
                        "p99": float(np.percentile(msmx, 99))},
         "errors_vs_oracle": err,
