@@ -28,7 +28,7 @@ Errors  = max |G - G_oracle| and |E2 - E2_oracle| against the CPU oracle
 C++/OpenMP restatement of directScaffoldNew in oracle/ (the reference
 itself needs libint2/libcint and cannot be built here).
 
-Multi-GPU: the north-star path runs on one GPU; with --gpus N each rank runs
+Multi-GPU: the build runs on one GPU; with --gpus N each rank runs
 an independent replica of the same build (replicas only, no collective) and
 value sums the builds of all ranks over the slowest rank's time.
 """
