@@ -21,7 +21,7 @@ EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_basis_info", "cqf_basis_schwarz", "cqf_basis_one_electron",
            "cqf_basis_nuclear", "cqf_basis_nuclear_pvp",
            "cqf_four_comp_core_hamiltonian",
-           "cqf_two_body_contract", "cqf_two_body_contract_noalloc",
+           "cqf_two_body_contract", "cqf_two_body_contract_noalloc", "cqf_autotune",
            "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
            "cqf_rel_two_body_contract", "cqf_dc_opts_default",
            "cqf_four_comp_gd", "cqf_server_opts_default", "cqf_fock_footprint",
@@ -138,6 +138,9 @@ def lib():
                                         C.c_int, C.POINTER(CqfOpts),
                                         C.POINTER(CqfStats)]
     L.cqf_two_body_contract.restype = C.c_int
+    L.cqf_autotune.argtypes = [C.c_void_p, C.POINTER(CqfContraction), C.c_int,
+                               C.POINTER(CqfOpts), C.c_char_p, C.POINTER(C.c_int)]
+    L.cqf_autotune.restype = C.c_int
     L.cqf_two_body_contract_noalloc.argtypes = L.cqf_two_body_contract.argtypes
     L.cqf_two_body_contract_noalloc.restype = C.c_int
     L.cqf_graph_create.argtypes = [C.c_void_p, C.POINTER(CqfContraction), C.c_int,

@@ -93,6 +93,30 @@ class DirectTPI:
             self.handle, S.ctypes.data_as(dp), T.ctypes.data_as(dp)))
         return S, T
 
+    def autotune(self, D, precision: str = "fp64", fp32_cutoff: float = 0.0,
+                 cache_path: Optional[str] = None) -> bool:
+        """``cqf_autotune`` on the closed-shell J and K of the real symmetric
+        density D (host array): sets this basis' launch shapes; returns True
+        when every class pair came from ``cache_path``."""
+        N = self.nbasis
+        X = np.asfortranarray(D, dtype=np.float64)
+        out = np.zeros((N, N), order="F")
+        arr = (_cabi.CqfContraction * 2)()
+        for i, t in enumerate((COULOMB, EXCHANGE)):
+            arr[i].X = C.c_void_p(X.ctypes.data)
+            arr[i].AX = C.c_void_p(out.ctypes.data)
+            arr[i].hermitian = 1
+            arr[i].type = t
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
+        opts.fp32_cutoff = float(fp32_cutoff)
+        hit = C.c_int(0)
+        _cabi.check(_cabi.lib().cqf_autotune(
+            self.handle, arr, 2, C.byref(opts),
+            cache_path.encode() if cache_path else None, C.byref(hit)))
+        return bool(hit.value)
+
     def nuclear(self, nuclei) -> np.ndarray:
         """V: nuclear-attraction matrix in the field of ``nuclei``
         ((natom, 5) rows {Z, x, y, z, zeta}; ``Molecule.nuclei``), computed

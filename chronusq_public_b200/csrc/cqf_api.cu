@@ -3,6 +3,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdio>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -738,6 +740,8 @@ void free_basis(cqf_basis* B) {
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->evFork) cudaEventDestroy(B->evFork);
+  for (cudaEvent_t e : B->tune_ev)
+    if (e) cudaEventDestroy(e);
   for (int i = 0; i < NAUX; i++) {
     if (B->evJoin[i]) cudaEventDestroy(B->evJoin[i]);
     aux_release(B->device, B->aux[i]);
@@ -845,6 +849,8 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     return fail(CQF_ENODEV, "no CUDA device");
   if (device < 0 || device >= ndev) return fail(CQF_EINVAL, "bad device ordinal");
   B->device = device;
+  for (int i = 0; i < NCLS; i++)
+    for (int j = 0; j < NCLS; j++) B->blocks_per_sm[i][j] = 8;
   CQF_CUDA(cudaSetDevice(device));
   CQF_CUDA(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
   CQF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
@@ -1590,9 +1596,14 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.ketNGroups = B->cls_group_cnt[ck];
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
       unsigned int* w = work + 2 * (cb * NCLS + ck);
-      const cudaStream_t ls = lanes[nlaunch++ % (NAUX + 1)];
-      if (!(fastOK && lm <= 2 && launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, ls)))
+      // autotuning times each class alone, on st, between two events
+      const bool tune = B->tuning && !capture;
+      const cudaStream_t ls = tune ? st : lanes[nlaunch++ % (NAUX + 1)];
+      if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck)], st));
+      if (!(fastOK && lm <= 2 &&
+            launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, ls, B->blocks_per_sm[cb][ck])))
         launch_jk_generic(a, la, lb, lc, ld, ls);
+      if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck) + 1], st));
     }
   for (int i = 0; i < NAUX; i++) {
     CQF_CUDA(cudaEventRecord(B->evJoin[i], B->aux[i]));
@@ -1632,6 +1643,129 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
 }  // namespace cqf
 
 extern "C" {
+
+cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
+                        const cqf_opts* optsIn, const char* cache_path, int* from_cache) {
+  g_err.clear();
+  CQF_TRY(check_contract_args(B, list, nMat));
+  cqf_opts opts;
+  cqf_opts_default(&opts);
+  if (optsIn) opts = *optsIn;
+  if (from_cache) *from_cache = 0;
+  std::lock_guard<std::mutex> lk(B->mu);
+  CQF_CUDA(cudaSetDevice(B->device));
+  cudaDeviceProp prop;
+  CQF_CUDA(cudaGetDeviceProperties(&prop, B->device));
+  std::string gpu = prop.name;
+  for (char& c : gpu)
+    if (c == ' ') c = '_';
+  // key of a class pair: GPU, angular momenta, size bucket log2(nBra nKet),
+  // precision
+  auto key = [&](int cb, int ck) {
+    int la, lb, lc, ld;
+    class_ls(cb, la, lb);
+    class_ls(ck, lc, ld);
+    const double n = std::max(1.0, (double)B->cls_cnt[cb] * B->cls_cnt[ck]);
+    return gpu + " " + std::to_string(la) + std::to_string(lb) + std::to_string(lc) +
+           std::to_string(ld) + " " + std::to_string((int)std::log2(n)) + " " +
+           (opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 ? "mixed" : "fp64");
+  };
+  std::vector<std::pair<int, int>> pairs;
+  for (int cb = 0; cb < NCLS; cb++)
+    for (int ck = 0; ck <= cb; ck++)
+      if (B->cls_cnt[cb] && B->cls_cnt[ck]) pairs.push_back({cb, ck});
+  // cached choices
+  std::map<std::string, int> cache;
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "r")) {
+      char k1[256], k2[64], k3[64], k4[64];
+      int v;
+      while (std::fscanf(f, "%255s %63s %63s %63s %d", k1, k2, k3, k4, &v) == 5)
+        cache[std::string(k1) + " " + k2 + " " + k3 + " " + k4] = v;
+      std::fclose(f);
+    }
+  }
+  bool all = !pairs.empty();
+  for (auto& p : pairs) all = all && cache.count(key(p.first, p.second));
+  if (all) {
+    for (auto& p : pairs) B->blocks_per_sm[p.first][p.second] = cache[key(p.first, p.second)];
+    if (from_cache) *from_cache = 1;
+    return CQF_OK;
+  }
+  // measure: every candidate on the real contraction, each class timed alone
+  const int cw = opts.is_complex ? 2 : 1;
+  const size_t matN = (size_t)B->nbasis * B->nbasis * cw;
+  std::vector<double*> buf(2 * nMat, nullptr);
+  std::vector<cqf_contraction> tl(list, list + nMat);
+  auto release = [&] {
+    for (double* p : buf) cudaFree(p);
+    B->tuning = false;
+  };
+  for (int m = 0; m < nMat; m++) {
+    if (cudaMalloc(&buf[2 * m], matN * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&buf[2 * m + 1], matN * sizeof(double)) != cudaSuccess) {
+      release();
+      return fail(CQF_ENOMEM, "cqf_autotune: scratch allocation");
+    }
+    cudaMemcpy(buf[2 * m], list[m].X, matN * sizeof(double), cudaMemcpyDefault);
+    tl[m].X = buf[2 * m];
+    tl[m].AX = buf[2 * m + 1];
+  }
+  cqf_opts to = opts;
+  to.device_pointers = 1;
+  to.stream = nullptr;
+  if (B->tune_ev.empty()) {
+    B->tune_ev.assign(2 * NCLS * NCLS, nullptr);
+    for (auto& e : B->tune_ev)
+      if (cudaEventCreate(&e) != cudaSuccess) {
+        release();
+        return fail(CQF_ECUDA, "cqf_autotune: event creation");
+      }
+  }
+  if (ensure_ws(B, ws_layout(B, nMat, to).total * sizeof(double)) != CQF_OK) {
+    release();
+    return CQF_ENOMEM;
+  }
+  const int cand[4] = {2, 4, 8, 16};
+  std::vector<float> best(NCLS * NCLS, 1e30f);
+  std::vector<int> choice(NCLS * NCLS, 8);
+  B->tuning = true;
+  for (int c : cand) {
+    for (auto& p : pairs) B->blocks_per_sm[p.first][p.second] = c;
+    for (int rep = 0; rep < 2; rep++) {  // the first run loads and warms
+      cqf_status st = contract_core(B, tl.data(), nMat, to, nullptr,
+                                    static_cast<double*>(B->d_ws), false, nullptr);
+      if (st != CQF_OK) {
+        release();
+        return st;
+      }
+    }
+    for (auto& p : pairs) {
+      const int k = p.first * NCLS + p.second;
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, B->tune_ev[2 * k], B->tune_ev[2 * k + 1]) == cudaSuccess &&
+          ms < best[k]) {
+        best[k] = ms;
+        choice[k] = c;
+      }
+    }
+  }
+  release();
+  for (auto& p : pairs) B->blocks_per_sm[p.first][p.second] = choice[p.first * NCLS + p.second];
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "a")) {
+      for (auto& p : pairs) {
+        const std::string k = key(p.first, p.second);
+        if (!cache.count(k))
+          std::fprintf(f, "%s %d\n", k.c_str(), choice[p.first * NCLS + p.second]);
+      }
+      std::fclose(f);
+    } else {
+      return fail(CQF_EINVAL, std::string("cqf_autotune: cannot write ") + cache_path);
+    }
+  }
+  return CQF_OK;
+}
 
 cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* listIn, int nMat,
                                  const cqf_opts* optsIn, cqf_stats* stats) {

@@ -142,6 +142,13 @@ struct cqf_basis {
   std::vector<cqf::ShellDev> h_shells;
   std::vector<cqf::PairDev> h_pairs;     // final (class, Q-sorted) order
   int cls_beg[cqf::NCLS] = {0}, cls_cnt[cqf::NCLS] = {0};
+  // launch shape of each class pair's persistent kernel: resident blocks per
+  // SM requested (8 by default; cqf_autotune measures and sets it)
+  int blocks_per_sm[cqf::NCLS][cqf::NCLS];
+  // autotuning: when set, contract_core launches the class kernels on one
+  // stream with an event pair around each (tune_ev[2 (cb NCLS + ck) + 0/1])
+  bool tuning = false;
+  std::vector<cudaEvent_t> tune_ev;
   int cls_tile_beg[cqf::NCLS] = {0};    // first ket tile of each class
   int cls_group_beg[cqf::NCLS] = {0}, cls_group_cnt[cqf::NCLS] = {0};
   std::vector<double> h_schwarz;         // nshell^2

@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
 // orientation); returns false when the class has no generated kernel.
 // work: two zeroed device counters for this class (FP64, FP32 launch).
 inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned int* work,
-                           int nsm, cudaStream_t st) {
+                           int nsm, cudaStream_t st, int blocksPerSm = 8) {
   if (a.nBra == 0 || a.nKet == 0) return true;
   bool done = false;
   auto go = [&](auto tag64, auto tag32, bool swap) {
@@ -430,7 +430,8 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
     // persistent blocks: enough for full residency on every SM (extra blocks
     // queue and find the counter exhausted); one work item per warp at a time
     constexpr int WPB = JK_THREADS / 32;
-    const unsigned g = (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * 8);
+    const unsigned g =
+        (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * blocksPerSm);
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
     if constexpr (G64::GROUPED) {
       if (useGroups) {

@@ -140,6 +140,19 @@ cqf_status cqf_four_comp_core_hamiltonian(cqf_basis* basis, int natom, const dou
 cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, int n,
                                  const cqf_opts* opts, cqf_stats* stats);
 
+/* Launch-shape autotuner (no counterpart in the reference, whose CPU loop has
+ * no launch shapes).  Times the contraction `list` (as cqf_two_body_contract
+ * would run it; X is read, AX is not touched) with each candidate launch
+ * shape of the persistent class-quartet kernels -- 2, 4, 8 or 16 resident
+ * blocks per SM requested -- every class timed alone between CUDA events,
+ * and keeps the fastest per class pair in the basis for its later
+ * contractions.  With cache_path, choices are looked up first and new ones
+ * appended, one line per (GPU name, class pair, size bucket log2(nBra nKet),
+ * precision); *from_cache = 1 when every class pair was found there.  It
+ * allocates scratch (cudaMalloc) and synchronises the device while timing. */
+cqf_status cqf_autotune(cqf_basis* basis, const cqf_contraction* list, int n,
+                        const cqf_opts* opts, const char* cache_path, int* from_cache);
+
 /* CUDA-graph form of cqf_two_body_contract for builds repeated on the same
  * device buffers (many densities per launch, RT-TDDFT steps, response
  * right-hand sides).  cqf_graph_create captures the whole contraction once

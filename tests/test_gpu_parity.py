@@ -330,3 +330,23 @@ def test_complex_hermitian_graph_split():
         assert np.abs(first[2 * k] - Jo).max() < FP64_TOL
         assert np.abs(first[2 * k + 1] - Ko).max() < FP64_TOL
     g.close()
+
+
+def test_autotune_sets_shapes_and_caches(tmp_path):
+    """cqf_autotune times the candidate launch shapes per class pair, keeps
+    the fastest, leaves the results unchanged, and a second basis of the same
+    system takes every choice from the cache file without timing."""
+    basis, tpi, ob, D = _oracle_and_device("h2o8_ccpvdz")
+    cache = str(tmp_path / "launch_shapes.txt")
+    assert tpi.autotune(D, cache_path=cache) is False
+    lines = open(cache).read().splitlines()
+    assert lines and all(int(l.split()[-1]) in (2, 4, 8, 16) for l in lines)
+    _G, J, K = FockBuilder(tpi).formRawGD(D)
+    Jo, Ko = ob.contract([D, D], [1, 1], [0, 1])
+    assert np.abs(J - Jo).max() < FP64_TOL
+    assert np.abs(K - Ko).max() < FP64_TOL
+    tpi2 = DirectTPI(basis)
+    assert tpi2.autotune(D, cache_path=cache) is True
+    assert open(cache).read().splitlines() == lines
+    _G2, J2, K2 = FockBuilder(tpi2).formRawGD(D)
+    assert np.abs(J2 - Jo).max() < FP64_TOL and np.abs(K2 - Ko).max() < FP64_TOL
