@@ -63,6 +63,11 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=300,
                     help="requests of the Poisson serving stream (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=10.0)
+    ap.add_argument("--profile-case", default=None,
+                    help="one untimed build of a named case for profiler captures "
+                         "(h2o16_def2svp, h2o8_ccpvdz, ag4_dc, ag1_ssss) and exit")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="precision of --profile-case")
     return ap.parse_args()
 
 
@@ -485,8 +490,52 @@ def run_four_component(args, ws, rank, local, pg):
     print(json.dumps(line), flush=True)
 
 
+def profile_case(args):
+    """One untimed build of a named case on cuda:0 (the command ncu captures
+    wrap; throughput numbers come from the timed runs, never from this)."""
+    import numpy as np
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet, Molecule
+    from chronusq_public_b200.contraction import DirectTPI
+    from chronusq_public_b200.fockbuilder import FockBuilder, FourCompFock
+    name = args.profile_case
+    cut = args.cutoff if args.precision == "mixed" else 0.0
+    if name == "ag1_ssss":
+        # one SSSS contraction of a single Ag atom (uncontracted basis) on a
+        # seeded Hermitian 17-entry input
+        from chronusq_public_b200.contraction import (SSSS, GTODirectRelERIContraction,
+                                                      TwoBodyContraction)
+        basis = BasisSet.build(Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)]),
+                               "sapporo-dkh3-dzp-2012_no", uncontract=True)
+        tpi = DirectTPI(basis)
+        N = basis.nbasis
+        rng = np.random.default_rng(3)
+        X = []
+        for _ in range(17):
+            A = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+            X.append(np.asfortranarray(0.05 * (A + A.conj().T)))
+        lst = [TwoBodyContraction(x, np.zeros((N, N), complex)) for x in X]
+        t0 = time.perf_counter()
+        GTODirectRelERIContraction(tpi).twoBodyContract(lst, SSSS, precision=args.precision,
+                                                        fp32_cutoff=cut)
+    elif name == "ag4_dc":
+        _basis, tpi, D = workloads.build_ag4_dc(lambda b: DirectTPI(b))
+        t0 = time.perf_counter()
+        FourCompFock(tpi).formGD(D, precision=args.precision, fp32_cutoff=cut)
+    else:
+        _mol, _basis, tpi, D = workloads.build_config(name, lambda b: DirectTPI(b))
+        t0 = time.perf_counter()
+        FockBuilder(tpi).formRawGD(D, precision=args.precision, fp32_cutoff=cut)
+    print("%s (%s): one untimed build %.3f s" % (name, args.precision,
+                                                  time.perf_counter() - t0), flush=True)
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     ws, rank, local, pg = dist_init(args)
     if args.impl == "ours" and args.workload == "ag4_dc":
         run_four_component(args, ws, rank, local, pg)

@@ -852,6 +852,7 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   for (int i = 0; i < NCLS; i++)
     for (int j = 0; j < NCLS; j++) B->blocks_per_sm[i][j] = 8;
   CQF_CUDA(cudaSetDevice(device));
+  noalloc_prepare(device);
   CQF_CUDA(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
   CQF_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
   CQF_CUDA(cudaEventCreate(&B->ev0));
@@ -1428,18 +1429,37 @@ cqf_status split_core(cqf_basis* B, const cqf_contraction* list, int nMat, const
   return CQF_OK;
 }
 
-// cqf_two_body_contract's split: host pointers are staged on the device.
-// Caller holds B->mu, device current.
-cqf_status contract_complex_split(cqf_basis* B, const cqf_contraction* list, int nMat,
-                                  const cqf_opts& opts, cqf_stats* stats) {
+std::vector<cqf_contraction> normalized_list(const cqf_contraction* list, int nMat,
+                                             bool* allHer) {
+  std::vector<cqf_contraction> out(list, list + nMat);
+  bool all = true;
+  for (auto& c : out) {
+    c.hermitian = c.hermitian ? 1 : 0;
+    all = all && c.hermitian;
+  }
+  if (allHer) *allHer = all;
+  return out;
+}
+
+// Workspace of contract_complex_split_on: [split workspace | complex X, AX
+// staging (host pointers only)].
+size_t complex_split_ws_doubles(const cqf_basis* B, const cqf_contraction* list, int nMat,
+                                const cqf_opts& opts) {
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  const size_t blk = (NN + 31) / 32 * 32;
+  const size_t inner = split_ws_doubles(B, split_real_count(list, nMat), opts);
+  return inner + (opts.device_pointers ? 0 : 4 * blk * nMat);
+}
+
+// The split with host pointers staged on the device.  Caller holds B->mu,
+// device current.
+cqf_status contract_complex_split_on(cqf_basis* B, const cqf_contraction* list, int nMat,
+                                     const cqf_opts& opts, cqf_stats* stats, double* ws) {
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const size_t NN = (size_t)B->nbasis * B->nbasis;
   const size_t blk = (NN + 31) / 32 * 32;
   const bool host = !opts.device_pointers;
   const size_t inner = split_ws_doubles(B, split_real_count(list, nMat), opts);
-  // [split workspace | complex X, AX staging (host pointers)]
-  CQF_TRY(ensure_ws(B, (inner + (host ? 4 * blk * nMat : 0)) * sizeof(double)));
-  double* ws = static_cast<double*>(B->d_ws);
   std::vector<cqf_contraction> dl(list, list + nMat);
   if (host) {
     for (int m = 0; m < nMat; m++) {
@@ -1644,14 +1664,23 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
 
 extern "C" {
 
-cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
+cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* listIn, int nMat,
                         const cqf_opts* optsIn, const char* cache_path, int* from_cache) {
   g_err.clear();
-  CQF_TRY(check_contract_args(B, list, nMat));
+  CQF_TRY(check_contract_args(B, listIn, nMat));
   cqf_opts opts;
   cqf_opts_default(&opts);
   if (optsIn) opts = *optsIn;
   if (from_cache) *from_cache = 0;
+  bool allHer = true;
+  std::vector<cqf_contraction> list = normalized_list(listIn, nMat, &allHer);
+  // which kernels the contraction runs: only the persistent fast kernels
+  // (real Hermitian-effective matrices, l <= 2; complex Hermitian densities
+  // through their real split) have launch shapes to tune
+  const bool csplit = opts.is_complex && allHer && split_eligible(B, list.data(), nMat, opts);
+  bool fast = !opts.is_complex;
+  for (int m = 0; m < nMat && fast; m++) fast = hermitian_eff(list[m], false);
+  if (!(fast || csplit)) return CQF_OK;  // generic kernels only: nothing to tune
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_CUDA(cudaSetDevice(B->device));
   cudaDeviceProp prop;
@@ -1659,29 +1688,33 @@ cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
   std::string gpu = prop.name;
   for (char& c : gpu)
     if (c == ' ') c = '_';
-  // key of a class pair: GPU, angular momenta, size bucket log2(nBra nKet),
-  // precision
+  const char* kind = csplit ? "csplit" : "real";
+  // key of a class pair: GPU, contraction kind, angular momenta, size bucket
+  // log2(nBra nKet), precision
   auto key = [&](int cb, int ck) {
     int la, lb, lc, ld;
     class_ls(cb, la, lb);
     class_ls(ck, lc, ld);
     const double n = std::max(1.0, (double)B->cls_cnt[cb] * B->cls_cnt[ck]);
-    return gpu + " " + std::to_string(la) + std::to_string(lb) + std::to_string(lc) +
-           std::to_string(ld) + " " + std::to_string((int)std::log2(n)) + " " +
-           (opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 ? "mixed" : "fp64");
+    return gpu + " " + kind + " " + std::to_string(la) + std::to_string(lb) +
+           std::to_string(lc) + std::to_string(ld) + " " + std::to_string((int)std::log2(n)) +
+           " " + (opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 ? "mixed" : "fp64");
   };
+  auto valid_shape = [](int v) { return v == 2 || v == 4 || v == 8 || v == 16; };
   std::vector<std::pair<int, int>> pairs;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck <= cb; ck++)
       if (B->cls_cnt[cb] && B->cls_cnt[ck]) pairs.push_back({cb, ck});
-  // cached choices
+  // cached choices (values other than the candidates are ignored: the class
+  // pair is measured again)
   std::map<std::string, int> cache;
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "r")) {
-      char k1[256], k2[64], k3[64], k4[64];
+      char k1[256], k2[64], k3[64], k4[64], k5[64];
       int v;
-      while (std::fscanf(f, "%255s %63s %63s %63s %d", k1, k2, k3, k4, &v) == 5)
-        cache[std::string(k1) + " " + k2 + " " + k3 + " " + k4] = v;
+      while (std::fscanf(f, "%255s %63s %63s %63s %63s %d", k1, k2, k3, k4, k5, &v) == 6)
+        if (valid_shape(v))
+          cache[std::string(k1) + " " + k2 + " " + k3 + " " + k4 + " " + k5] = v;
       std::fclose(f);
     }
   }
@@ -1692,38 +1725,75 @@ cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
     if (from_cache) *from_cache = 1;
     return CQF_OK;
   }
-  // measure: every candidate on the real contraction, each class timed alone
-  const int cw = opts.is_complex ? 2 : 1;
-  const size_t matN = (size_t)B->nbasis * B->nbasis * cw;
-  std::vector<double*> buf(2 * nMat, nullptr);
-  std::vector<cqf_contraction> tl(list, list + nMat);
-  auto release = [&] {
+  // measure: every candidate on the real contraction that runs, each class
+  // timed alone; the shapes in use are restored if anything fails
+  int saved[NCLS][NCLS];
+  std::memcpy(saved, B->blocks_per_sm, sizeof saved);
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  std::vector<double*> buf;
+  std::vector<cqf_contraction> tl;
+  auto release = [&](bool restore) {
     for (double* p : buf) cudaFree(p);
     B->tuning = false;
+    if (restore) std::memcpy(B->blocks_per_sm, saved, sizeof saved);
+  };
+  auto dev_alloc = [&](size_t doubles) -> double* {
+    double* p = nullptr;
+    if (cudaMalloc(&p, doubles * sizeof(double)) != cudaSuccess) return nullptr;
+    buf.push_back(p);
+    return p;
   };
   for (int m = 0; m < nMat; m++) {
-    if (cudaMalloc(&buf[2 * m], matN * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&buf[2 * m + 1], matN * sizeof(double)) != cudaSuccess) {
-      release();
+    const size_t cw = opts.is_complex ? 2 : 1;
+    double* x = dev_alloc(cw * NN);
+    if (!x || cudaMemcpy(x, list[m].X, cw * NN * sizeof(double), cudaMemcpyDefault) !=
+                  cudaSuccess) {
+      release(true);
+      return fail(CQF_ENOMEM, "cqf_autotune: scratch allocation / copy");
+    }
+    if (!csplit) {
+      double* ax = dev_alloc(NN);
+      if (!ax) {
+        release(true);
+        return fail(CQF_ENOMEM, "cqf_autotune: scratch allocation");
+      }
+      tl.push_back({x, ax, list[m].hermitian, list[m].type});
+      continue;
+    }
+    // the split of a complex Hermitian density: its real part, and for
+    // exchange its imaginary part (antisymmetric) as a second real entry
+    const bool k = list[m].type == CQF_EXCHANGE;
+    double* re = dev_alloc(NN);
+    double* im = k ? dev_alloc(NN) : nullptr;
+    double* ax = dev_alloc(NN);
+    double* ax2 = k ? dev_alloc(NN) : nullptr;
+    if (!re || !ax || (k && (!im || !ax2))) {
+      release(true);
       return fail(CQF_ENOMEM, "cqf_autotune: scratch allocation");
     }
-    cudaMemcpy(buf[2 * m], list[m].X, matN * sizeof(double), cudaMemcpyDefault);
-    tl[m].X = buf[2 * m];
-    tl[m].AX = buf[2 * m + 1];
+    split_complex_kernel<<<grid1(NN, 256), 256, 0, B->stream>>>(x, NN, re, im);
+    tl.push_back({re, ax, 1, list[m].type});
+    if (k) tl.push_back({im, ax2, -1, CQF_EXCHANGE});
   }
+  if (cudaStreamSynchronize(B->stream) != cudaSuccess || (int)tl.size() > MAXMAT) {
+    release(true);
+    return fail(CQF_ECUDA, "cqf_autotune: preparing the real contraction");
+  }
+  const int nT = (int)tl.size();
   cqf_opts to = opts;
   to.device_pointers = 1;
+  to.is_complex = 0;
   to.stream = nullptr;
   if (B->tune_ev.empty()) {
     B->tune_ev.assign(2 * NCLS * NCLS, nullptr);
     for (auto& e : B->tune_ev)
       if (cudaEventCreate(&e) != cudaSuccess) {
-        release();
+        release(true);
         return fail(CQF_ECUDA, "cqf_autotune: event creation");
       }
   }
-  if (ensure_ws(B, ws_layout(B, nMat, to).total * sizeof(double)) != CQF_OK) {
-    release();
+  if (ensure_ws(B, ws_layout(B, nT, to).total * sizeof(double)) != CQF_OK) {
+    release(true);
     return CQF_ENOMEM;
   }
   const int cand[4] = {2, 4, 8, 16};
@@ -1733,10 +1803,10 @@ cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
   for (int c : cand) {
     for (auto& p : pairs) B->blocks_per_sm[p.first][p.second] = c;
     for (int rep = 0; rep < 2; rep++) {  // the first run loads and warms
-      cqf_status st = contract_core(B, tl.data(), nMat, to, nullptr,
+      cqf_status st = contract_core(B, tl.data(), nT, to, nullptr,
                                     static_cast<double*>(B->d_ws), false, nullptr);
       if (st != CQF_OK) {
-        release();
+        release(true);
         return st;
       }
     }
@@ -1750,7 +1820,7 @@ cqf_status cqf_autotune(cqf_basis* B, const cqf_contraction* list, int nMat,
       }
     }
   }
-  release();
+  release(false);
   for (auto& p : pairs) B->blocks_per_sm[p.first][p.second] = choice[p.first * NCLS + p.second];
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "a")) {
@@ -1774,17 +1844,15 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* listIn, in
   cqf_opts opts;
   cqf_opts_default(&opts);
   if (optsIn) opts = *optsIn;
-  // TwoBodyContraction::HER is a bool: any nonzero value is Hermitian
-  std::vector<cqf_contraction> list(listIn, listIn + nMat);
   bool allHer = true;
-  for (auto& c : list) {
-    c.hermitian = c.hermitian ? 1 : 0;
-    allHer = allHer && c.hermitian;
-  }
+  std::vector<cqf_contraction> list = normalized_list(listIn, nMat, &allHer);
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_CUDA(cudaSetDevice(B->device));
-  if (allHer && split_eligible(B, list.data(), nMat, opts))
-    return contract_complex_split(B, list.data(), nMat, opts, stats);
+  if (allHer && split_eligible(B, list.data(), nMat, opts)) {
+    CQF_TRY(ensure_ws(B, complex_split_ws_doubles(B, list.data(), nMat, opts) * sizeof(double)));
+    return contract_complex_split_on(B, list.data(), nMat, opts, stats,
+                                     static_cast<double*>(B->d_ws));
+  }
   CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
   return contract_core(B, list.data(), nMat, opts, stats, static_cast<double*>(B->d_ws), false,
                        nullptr);

@@ -100,6 +100,13 @@ inline int contraction_flags(const cqf_contraction& c, bool cplx) {
          (c.hermitian < 0 ? 4 : 0);
 }
 
+// The caller's contraction list with TwoBodyContraction::HER as the bool it
+// is in the reference (twopints.hpp:59-75): any nonzero value becomes 1, so
+// a caller's "true" never reaches the library's internal -1 flag (the
+// antisymmetric part of a complex split).  *allHer: every entry Hermitian.
+std::vector<cqf_contraction> normalized_list(const cqf_contraction* list, int nMat,
+                                             bool* allHer);
+
 // Complex Hermitian contractions on the real fast kernels (cqf_api.cu):
 // eligibility, real-entry count and flags, workspace, and the pipeline on
 // device pointers and a caller-provided workspace (capture-able).
@@ -111,12 +118,24 @@ size_t split_ws_doubles(const cqf_basis* B, int nReal, const cqf_opts& opts);
 cqf_status split_core(cqf_basis* B, const cqf_contraction* list, int nMat, const cqf_opts& opts,
                       cqf_stats* stats, double* ws, bool capture, const int* d_flags_pre);
 
+// The split for device or host pointers on a caller-provided workspace of
+// complex_split_ws_doubles() doubles (host pointers are staged in it);
+// synchronises before returning.  Caller holds B->mu, device current.
+size_t complex_split_ws_doubles(const cqf_basis* B, const cqf_contraction* list, int nMat,
+                                const cqf_opts& opts);
+cqf_status contract_complex_split_on(cqf_basis* B, const cqf_contraction* list, int nMat,
+                                     const cqf_opts& opts, cqf_stats* stats, double* ws);
+
 // normSrc (optional, device pointers): per entry, the complex matrix whose
 // shell-block norms screen it in place of its own X (the split of a complex
 // Hermitian density keeps the reference's complex screen).
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
                          const int* d_flags_pre, const double* const* normSrc = nullptr);
+
+// Resolves the no-alloc scratch array's device address on `device` (current)
+// during basis creation (cqf_noalloc.cu).
+void noalloc_prepare(int device);
 
 // Launch helpers shared with the four-component path (cqf_api.cu).
 // Shell-block infinity norms of one N x N matrix (complex: |z|).

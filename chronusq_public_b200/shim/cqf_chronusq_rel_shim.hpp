@@ -23,39 +23,20 @@
 #include <cerr.hpp>
 #include <particleintegrals/twopints/gtodirectreleri.hpp>
 
+#include "cqf_chronusq_basis.hpp"
 #include "cqfock.h"
 
 namespace ChronusQ {
 
 template <typename MatsT, typename IntsT>
 class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, IntsT> {
-  mutable cqf_basis* basis_ = nullptr;
-  mutable std::vector<double> alpha_, coef_;
+  // the device basis of the DirectTPI's BasisSet, rebuilt whenever its
+  // shells change (a geometry step moves them)
+  mutable CqfBasisCache cache_;
 
-  void ensure_basis() const {
-    if (basis_) return;
+  cqf_basis* basis() const {
     auto& tpi = *std::dynamic_pointer_cast<DirectTPI<IntsT>>(this->ints_);
-    BasisSet& bs = tpi.basisSet();
-    std::vector<cqf_shell> sh(bs.nShell);
-    alpha_.clear();
-    coef_.clear();
-    for (auto& s : bs.shells) {
-      alpha_.insert(alpha_.end(), s.alpha.begin(), s.alpha.end());
-      coef_.insert(coef_.end(), s.contr[0].coeff.begin(), s.contr[0].coeff.end());
-    }
-    size_t off = 0;
-    for (size_t i = 0; i < bs.nShell; i++) {
-      const libint2::Shell& s = bs.shells[i];
-      sh[i].l = s.contr[0].l;
-      sh[i].pure = s.contr[0].pure ? 1 : 0;
-      sh[i].nprim = (int)s.alpha.size();
-      sh[i].alpha = alpha_.data() + off;
-      sh[i].coeff = coef_.data() + off;
-      for (int x = 0; x < 3; x++) sh[i].origin[x] = s.O[x];
-      off += s.alpha.size();
-    }
-    cqf_status st = cqf_basis_create(sh.data(), (int)sh.size(), tpi.threshSchwarz(), 0, &basis_);
-    if (st != CQF_OK) CErr(std::string("cqf_basis_create: ") + cqf_last_error());
+    return cache_.get(tpi.basisSet(), tpi.threshSchwarz());
   }
 
  public:
@@ -76,7 +57,7 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
                                                                 computeExchange, type4C, approx);
       return;
     }
-    ensure_basis();
+    cqf_basis* b = basis();
     const void* X[CQF_REL_NMAT];
     void* AX[CQF_REL_NMAT];
     for (int m = 0; m < CQF_REL_NMAT; m++) {
@@ -90,13 +71,9 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
     const int type = t == BARE_COULOMB ? CQF_REL_BARE_COULOMB
                      : t == LLSS       ? CQF_REL_LLSS
                                        : CQF_REL_SSSS;
-    cqf_status st = cqf_rel_two_body_contract(basis_, X, AX, type, computeExchange ? 1 : 0, &o,
+    cqf_status st = cqf_rel_two_body_contract(b, X, AX, type, computeExchange ? 1 : 0, &o,
                                               nullptr);
     if (st != CQF_OK) CErr(std::string("cqf_rel_two_body_contract: ") + cqf_last_error());
-  }
-
-  ~B200DirectRelERIContraction() override {
-    if (basis_) cqf_basis_destroy(basis_);
   }
 };
 

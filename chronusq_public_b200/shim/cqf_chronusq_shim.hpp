@@ -17,44 +17,27 @@
 #include <cerr.hpp>
 #include <particleintegrals/twopints/gtodirecttpi.hpp>
 
+#include "cqf_chronusq_basis.hpp"
 #include "cqfock.h"
 
 namespace ChronusQ {
 
 template <typename MatsT, typename IntsT>
 class B200DirectTPIContraction : public GTODirectTPIContraction<MatsT, IntsT> {
-  // one device basis per contraction object; rebuilt when the geometry moves
-  mutable cqf_basis* basis_ = nullptr;
-  mutable std::vector<double> alpha_, coef_;
+  // the device basis of the DirectTPI's BasisSet, rebuilt whenever its
+  // shells change (a geometry step moves them)
+  mutable CqfBasisCache cache_;
 
-  void ensure_basis() const {
-    if (basis_) return;
+  cqf_basis* basis() const {
     auto& tpi = *std::dynamic_pointer_cast<DirectTPI<IntsT>>(this->ints_);
-    BasisSet& bs = tpi.basisSet();
-    std::vector<cqf_shell> sh(bs.nShell);
-    alpha_.clear();
-    coef_.clear();
-    for (auto& s : bs.shells) {
-      alpha_.insert(alpha_.end(), s.alpha.begin(), s.alpha.end());
-      coef_.insert(coef_.end(), s.contr[0].coeff.begin(), s.contr[0].coeff.end());
-    }
-    size_t off = 0;
-    for (size_t i = 0; i < bs.nShell; i++) {
-      const libint2::Shell& s = bs.shells[i];
-      sh[i].l = s.contr[0].l;
-      sh[i].pure = s.contr[0].pure ? 1 : 0;
-      sh[i].nprim = (int)s.alpha.size();
-      sh[i].alpha = alpha_.data() + off;
-      sh[i].coeff = coef_.data() + off;
-      for (int x = 0; x < 3; x++) sh[i].origin[x] = s.O[x];
-      off += s.alpha.size();
-    }
-    cqf_status st = cqf_basis_create(sh.data(), (int)sh.size(), tpi.threshSchwarz(), 0, &basis_);
-    if (st != CQF_OK) CErr(std::string("cqf_basis_create: ") + cqf_last_error());
+    return cache_.get(tpi.basisSet(), tpi.threshSchwarz());
   }
 
  public:
   using GTODirectTPIContraction<MatsT, IntsT>::GTODirectTPIContraction;
+  // keep the convenience overloads of TPIContractions (screen = true, no
+  // EMPerturbation; twopints.hpp:225-244) callable on this type
+  using GTODirectTPIContraction<MatsT, IntsT>::twoBodyContract;
 
   // GTODirectTPIContraction::twoBodyContract (gtodirecttpi.hpp:199-206)
   void twoBodyContract(MPI_Comm comm, const bool screen,
@@ -64,7 +47,7 @@ class B200DirectTPIContraction : public GTODirectTPIContraction<MatsT, IntsT> {
       GTODirectTPIContraction<MatsT, IntsT>::twoBodyContract(comm, screen, list, pert);
       return;
     }
-    ensure_basis();
+    cqf_basis* b = basis();
     std::vector<cqf_contraction> c(list.size());
     for (size_t i = 0; i < list.size(); i++) {
       if (list[i].contType != COULOMB && list[i].contType != EXCHANGE)
@@ -78,12 +61,8 @@ class B200DirectTPIContraction : public GTODirectTPIContraction<MatsT, IntsT> {
     cqf_opts_default(&o);
     o.is_complex = std::is_same<MatsT, std::complex<double>>::value ? 1 : 0;
     o.screen = screen ? 1 : 0;
-    cqf_status st = cqf_two_body_contract(basis_, c.data(), (int)c.size(), &o, nullptr);
+    cqf_status st = cqf_two_body_contract(b, c.data(), (int)c.size(), &o, nullptr);
     if (st != CQF_OK) CErr(std::string("cqf_two_body_contract: ") + cqf_last_error());
-  }
-
-  ~B200DirectTPIContraction() override {
-    if (basis_) cqf_basis_destroy(basis_);
   }
 };
 

@@ -153,54 +153,3 @@ def build_config(name: str, tpi_factory):
     D = occupied_density(S, nocc, seed)
     return mol, basis, tpi, D
 
-
-def main(argv=None):
-    """One FP64 build of a named workload on cuda:0, with its time:
-
-        python -m chronusq_public_b200.workloads ag4_dc
-
-    (a single, unwarmed build -- the command profiling captures use; timed
-    throughput comes from bench.py)."""
-    import argparse
-    import time
-
-    from .contraction import DirectTPI
-    from .fockbuilder import FockBuilder, FourCompFock
-    ap = argparse.ArgumentParser()
-    ap.add_argument("workload")
-    args = ap.parse_args(argv)
-    if args.workload == "ag1_ssss":
-        # one SSSS contraction of a single Ag atom (uncontracted basis) on a
-        # seeded Hermitian 17-entry input: the block kernels' profiling case
-        from .contraction import SSSS, GTODirectRelERIContraction, TwoBodyContraction
-        basis = BasisSet.build(Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)]),
-                               "sapporo-dkh3-dzp-2012_no", uncontract=True)
-        tpi = DirectTPI(basis)
-        N = basis.nbasis
-        rng = np.random.default_rng(3)
-        X = []
-        for _ in range(17):
-            A = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
-            X.append(np.asfortranarray(0.05 * (A + A.conj().T)))
-        lst = [TwoBodyContraction(x, np.zeros((N, N), complex)) for x in X]
-        t0 = time.perf_counter()
-        GTODirectRelERIContraction(tpi).twoBodyContract(lst, SSSS)
-        print("%s: one contraction %.3f s" % (args.workload, time.perf_counter() - t0),
-              flush=True)
-        return
-    if args.workload == "ag4_dc":
-        _basis, tpi, D = build_ag4_dc(lambda b: DirectTPI(b))
-        fb = FourCompFock(tpi)
-        t0 = time.perf_counter()
-        fb.formGD(D)
-    else:
-        _mol, _basis, tpi, D = build_config(args.workload, lambda b: DirectTPI(b))
-        fb = FockBuilder(tpi)
-        t0 = time.perf_counter()
-        fb.formRawGD(D)
-    dt = time.perf_counter() - t0
-    print("%s: one build %.3f s" % (args.workload, dt), flush=True)
-
-
-if __name__ == "__main__":
-    main()

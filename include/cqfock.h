@@ -146,10 +146,15 @@ cqf_status cqf_two_body_contract(cqf_basis* basis, const cqf_contraction* list, 
  * shape of the persistent class-quartet kernels -- 2, 4, 8 or 16 resident
  * blocks per SM requested -- every class timed alone between CUDA events,
  * and keeps the fastest per class pair in the basis for its later
- * contractions.  With cache_path, choices are looked up first and new ones
- * appended, one line per (GPU name, class pair, size bucket log2(nBra nKet),
- * precision); *from_cache = 1 when every class pair was found there.  It
- * allocates scratch (cudaMalloc) and synchronises the device while timing. */
+ * contractions.  Complex Hermitian densities are tuned on the real split
+ * they run as; contractions that run only on the generic kernels (which
+ * have no launch shapes) return CQF_OK without timing anything.  With
+ * cache_path, choices are looked up first and new ones appended, one line
+ * per (GPU name, real / complex-split, class pair, size bucket
+ * log2(nBra nKet), precision); cached values other than 2, 4, 8, 16 are
+ * ignored, and *from_cache = 1 when every class pair was found there.  On
+ * failure the basis keeps the shapes it had.  It allocates scratch
+ * (cudaMalloc) and synchronises the device while timing. */
 cqf_status cqf_autotune(cqf_basis* basis, const cqf_contraction* list, int n,
                         const cqf_opts* opts, const char* cache_path, int* from_cache);
 
@@ -170,17 +175,21 @@ cqf_status cqf_graph_destroy(cqf_graph* graph);
 /* Size of the fixed scratch array of cqf_two_body_contract_noalloc. */
 #define CQF_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 
-/* Same contraction as cqf_two_body_contract, but it allocates no device
+/* Same contraction as cqf_two_body_contract (the same HER normalisation and
+ * kernels, complex Hermitian densities included), but it allocates no device
  * memory: its scratch is one fixed CQF_NOALLOC_SCRATCH_BYTES array compiled
  * into the library (held by every GPU that loads the library until exit).
  * No counterpart in the reference (ChronusQ takes scratch from its memory
  * manager); it is for callers that cannot call cudaMalloc during the call,
- * e.g. inside a framework that owns all device memory.  The basis must already exist (cqf_basis_create allocates).
- * Calls needing more scratch than the array holds return CQF_EINVAL.  The
- * first call on a device resolves the array's device address; make that
- * first call before any stream capture.  All calls share the array and it
- * keeps the last call's contents (each call clears what must start at zero);
- * calls that overlap on the GPU race on it and must be serialised. */
+ * e.g. inside a framework that owns all device memory.  The basis must
+ * already exist: cqf_basis_create, which allocates, also resolves the
+ * array's device address on its device.  CUDA loads kernel code lazily on a
+ * kernel's first launch; a caller that must see no device allocation at all
+ * in these calls runs one contraction of the same kind beforehand (or sets
+ * CUDA_MODULE_LOADING=EAGER).  Calls needing more scratch than the array
+ * holds return CQF_EINVAL.  All calls share the array and it keeps the last
+ * call's contents (each call clears what must start at zero); calls that
+ * overlap on the GPU race on it and must be serialised. */
 cqf_status cqf_two_body_contract_noalloc(cqf_basis* basis, const cqf_contraction* list, int n,
                                          const cqf_opts* opts, cqf_stats* stats);
 

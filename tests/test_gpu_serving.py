@@ -46,6 +46,9 @@ def test_alone_equals_mix_and_oracle():
     st = srv.stats()
     srv.close()
     assert st["completed"] == len(reqs)
+    # the mix really overlapped on the GPU (a server that serialised every
+    # request would have peak_inflight == 1)
+    assert st["peak_inflight"] > 1
     for a, m in zip(alone, mix):
         assert np.abs(a - m).max() < 1e-10
     # one request against the FP64 oracle at the mixed-path tolerance
