@@ -36,7 +36,8 @@ def _contract(entry, tpi, D, outs, types, device_pointers=False, her=1):
     opts = _cabi.CqfOpts()
     _cabi.lib().cqf_opts_default(C.byref(opts))
     opts.device_pointers = 1 if device_pointers else 0
-    opts.is_complex = 1 if np.iscomplexobj(D) else 0
+    cplx = D.is_complex() if device_pointers else np.iscomplexobj(D)
+    opts.is_complex = 1 if cplx else 0
     st = _cabi.CqfStats()
     return entry(tpi.handle, arr, n, C.byref(opts), C.byref(st))
 
