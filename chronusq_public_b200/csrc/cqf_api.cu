@@ -674,6 +674,12 @@ __global__ void from_cart_kernel(const double* __restrict__ Ac, int cplx, int he
 unsigned grid1(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // Real and imaginary parts of an interleaved complex matrix (n entries).
+__global__ void to_float_kernel(const double* __restrict__ x, size_t n, float* y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
 __global__ void split_complex_kernel(const double* __restrict__ Xc, size_t n, double* re,
                                      double* im) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -729,8 +735,7 @@ void free_basis(cqf_basis* B) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
                     (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_pairRange,
-                    (void*)B->d_braPerm,
-                    (void*)B->d_groups, (void*)B->d_schwarz,
+                    (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
                     (void*)B->d_cart2shell, (void*)B->d_ws, (void*)B->d_counters,
                     (void*)B->d_flags, (void*)B->d_qLL, (void*)B->d_qSS, (void*)B->d_relws})
@@ -1070,45 +1075,6 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     pair_range_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_pp, B->d_pairs,
                                                                    B->npair, B->d_pairRange);
     CQF_CUDA(cudaGetLastError());
-    // bra groups: per class, pairs ordered by first shell (stable: Schwarz
-    // order inside a shell), runs of one shell cut into groups of at most
-    // BRA_GROUP_MAX
-    std::vector<int> perm(std::max(1, B->npair));
-    std::vector<int2> grp;
-    for (int c = 0; c < NCLS; c++) {
-      const int beg = B->cls_beg[c], cnt = B->cls_cnt[c];
-      std::vector<int> ord(cnt);
-      for (int i = 0; i < cnt; i++) ord[i] = i;
-      std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
-        return B->h_pairs[beg + x].shA < B->h_pairs[beg + y].shA;
-      });
-      for (int i = 0; i < cnt; i++) perm[beg + i] = ord[i];
-      B->cls_group_beg[c] = (int)grp.size();
-      // a group's primitive pairs are capped (one warp runs its members in
-      // sequence: heavily contracted pairs stay alone), and the groups are
-      // queued heaviest first so the work counter hands them out early
-      std::vector<std::pair<int, int2>> cg;
-      for (int i = 0; i < cnt;) {
-        int j = i, work = 0;
-        const int sh = B->h_pairs[beg + ord[i]].shA;
-        while (j < cnt && j - i < BRA_GROUP_MAX && B->h_pairs[beg + ord[j]].shA == sh &&
-               (j == i || work + B->h_pairs[beg + ord[j]].npp <= BRA_GROUP_NPP)) {
-          work += B->h_pairs[beg + ord[j]].npp;
-          j++;
-        }
-        cg.push_back({work, make_int2(i, j - i)});
-        i = j;
-      }
-      std::stable_sort(cg.begin(), cg.end(),
-                       [](const std::pair<int, int2>& x, const std::pair<int, int2>& y) {
-                         return x.first > y.first;
-                       });
-      for (auto& e : cg) grp.push_back(e.second);
-      B->cls_group_cnt[c] = (int)grp.size() - B->cls_group_beg[c];
-    }
-    if (grp.empty()) grp.push_back(make_int2(0, 0));
-    CQF_TRY(upload(&B->d_braPerm, perm, B->stream));
-    CQF_TRY(upload(&B->d_groups, grp, B->stream));
   }
   B->h_schwarz.resize((size_t)nshell * nshell);
   CQF_CUDA(cudaMemcpyAsync(B->h_schwarz.data(), B->d_schwarz,
@@ -1320,9 +1286,24 @@ WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   L.oNm = take(ns2);
   L.oNmM = take(ns2 * nMat);
   L.oG = take(4);
-  L.oWork = take((NWORK + 1) / 2);
   L.oNmT = take(ns2);
   L.oPN = take((size_t)std::max(1, B->npair));
+  L.oWork = take((NWORK + 1) / 2);
+  // FP32 copy of the Cartesian densities (mixed real builds)
+  const bool mixed = opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 && !opts.is_complex;
+  L.oXc32 = take(mixed ? (matC * nMat + 1) / 2 : 0);
+  // quartet masks of the fast class kernels: for each class pair, room for
+  // either orientation (which class is the bra is the generated kernel's)
+  size_t words = 0;
+  for (int cb = 0; cb < NCLS; cb++)
+    for (int ck = 0; ck < NCLS; ck++) {
+      L.oMaskCls[cb][ck] = words;
+      if (ck > cb || opts.is_complex || !B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
+      const size_t nb = B->cls_cnt[cb], nk = B->cls_cnt[ck];
+      // mask words (uint2) + two word lists (int each) = 2 words per word
+      words += 2 * std::max(nb * ((nk + 31) / 32), nk * ((nb + 31) / 32));
+    }
+  L.oMask = take(std::max<size_t>(words, 1));
   L.total = off;
   return L;
 }
@@ -1499,7 +1480,6 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   const bool host = !opts.device_pointers;
   const size_t oX = Lw.oX, oAX = Lw.oAX, oXc = Lw.oXc, oAc = Lw.oAc, oNm = Lw.oNm,
                oNmM = Lw.oNmM, oG = Lw.oG;
-  unsigned int* work = reinterpret_cast<unsigned int*>(ws + Lw.oWork);
   if (!capture) CQF_CUDA(cudaEventRecord(B->ev0, st));
   std::vector<const double*> Xd(nMat);
   std::vector<double*> AXd(nMat);
@@ -1527,6 +1507,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   }
   CQF_CUDA(cudaMemsetAsync(B->d_counters, 0, 8 * sizeof(unsigned long long), st));
   CQF_CUDA(cudaMemsetAsync(ws + oG, 0, 4 * sizeof(double), st));
+  unsigned int* work = reinterpret_cast<unsigned int*>(ws + Lw.oWork);
   CQF_CUDA(cudaMemsetAsync(work, 0, NWORK * sizeof(unsigned int), st));
 
   // shell-block norms (per matrix, symmetrised when non-Hermitian), max
@@ -1549,6 +1530,12 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       symmetrize_kernel<<<grid1((size_t)nc * nc, 256), 256, 0, st>>>(ws + oXc + m * matC, nc);
   }
   CQF_CUDA(cudaMemsetAsync(ws + oAc, 0, matC * nMat * sizeof(double), st));
+  float* Xc32 = reinterpret_cast<float*>(ws + Lw.oXc32);
+  const bool mixedReal =
+      opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 && !opts.is_complex;
+  if (mixedReal)
+    to_float_kernel<<<(unsigned)std::min<size_t>(grid1(matC * nMat, 256), 4096), 256, 0, st>>>(
+        ws + oXc, matC * nMat, Xc32);
   CQF_CUDA(cudaGetLastError());
 
   JKLaunch a{};
@@ -1570,21 +1557,13 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.ncart = nc;
   a.flags = d_flags;
   a.Xc = ws + oXc;
+  a.Xc32 = mixedReal ? Xc32 : nullptr;
   a.Ac = ws + oAc;
   a.precision = opts.precision;
   a.fp32_cut = opts.fp32_cutoff;
   a.counters = B->d_counters;
   a.ketT = B->d_ketT;
   a.tileOff = B->d_tileOff;
-  a.braPerm = B->d_braPerm;
-  a.groups = B->d_groups;
-  // one J and one K matrix: the grouped kernels sum their per-lane J_cd,
-  // K_ac, K_ad over a bra group before flushing
-  a.jmat = a.kmat = -1;
-  if (nMat == 2 && list[0].type != list[1].type) {
-    a.jmat = list[0].type == CQF_COULOMB ? 0 : 1;
-    a.kmat = 1 - a.jmat;
-  }
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;
   for (int m = 0; m < nMat; m++) fastOK = fastOK && hermitian_eff(list[m], false);
@@ -1610,18 +1589,15 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       a.same = (cb == ck);
       a.braTileBeg = B->cls_tile_beg[cb];
       a.ketTileBeg = B->cls_tile_beg[ck];
-      a.braGroupBeg = B->cls_group_beg[cb];
-      a.braNGroups = B->cls_group_cnt[cb];
-      a.ketGroupBeg = B->cls_group_beg[ck];
-      a.ketNGroups = B->cls_group_cnt[ck];
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
-      unsigned int* w = work + 2 * (cb * NCLS + ck);
       // autotuning times each class alone, on st, between two events
       const bool tune = B->tuning && !capture;
       const cudaStream_t ls = tune ? st : lanes[nlaunch++ % (NAUX + 1)];
       if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck)], st));
+      uint2* masks = reinterpret_cast<uint2*>(ws + Lw.oMask) + Lw.oMaskCls[cb][ck];
       if (!(fastOK && lm <= 2 &&
-            launch_jk_fast(a, la, lb, lc, ld, w, B->nsm, ls, B->blocks_per_sm[cb][ck])))
+            launch_jk_fast(a, la, lb, lc, ld, masks, work + 4 * (cb * NCLS + ck), B->nsm, ls,
+                           B->blocks_per_sm[cb][ck])))
         launch_jk_generic(a, la, lb, lc, ld, ls);
       if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck) + 1], st));
     }

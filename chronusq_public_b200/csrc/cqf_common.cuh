@@ -120,7 +120,8 @@ __device__ __forceinline__ bool fp32_range_ok(float2 rP, float2 rQ, int L, int d
 // ----------------------------------------------------------------- Boys
 // F_0..F_L at T.  Taylor expansion of F_L about the nearest grid point
 // (F_m' = -F_{m+1}), downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1);
-// for T >= TMAX, F_0 = sqrt(pi/T)/2 and upward recursion keeping e^-T.
+// for T >= TMAX, F_0 = sqrt(pi/T)/2 and upward recursion keeping e^-T --
+// evaluated in FP64 by both precisions (boys_f32 rounds the result).
 // `rows` points at the rows of this L (global or shared memory).
 template <int L>
 __device__ __forceinline__ void boys_f64(double T, double* F, const double* __restrict__ rows) {
@@ -183,12 +184,21 @@ __device__ __forceinline__ void boys_f32(float T, float* F, const float* __restr
       for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
     }
   } else {
-    float rT = rsqrtf(T);
-    F[0] = 0.886226925f * rT;
+    // large arguments in FP64 (the asymptotic form and its upward recursion
+    // lose accuracy in FP32 as (2m+1)/(2T) factors accumulate), then rounded;
+    // e^-T <= 2.3e-16 enters the recursion only as a correction, so its FP32
+    // value (relative error ~1e-7) is exact enough
+    const double Td = (double)T;
+    const double rT = rsqrt(Td);
+    double f = 0.88622692545275801365 * rT;  // sqrt(pi)/2
+    F[0] = (float)f;
     if (L > 0) {
-      float e = __expf(-T), h = 0.5f * rT * rT;
+      const double e = (double)__expf(-T), h = 0.5 * rT * rT;
 #pragma unroll
-      for (int m = 0; m < L; m++) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+      for (int m = 0; m < L; m++) {
+        f = ((2 * m + 1) * f - e) * h;
+        F[m + 1] = (float)f;
+      }
     }
   }
 }

@@ -28,8 +28,6 @@ constexpr int MAXMAT = 512;
 constexpr int NAUX = 2;           // auxiliary streams of the class-quartet launches
 constexpr int KETT_NF = 12;
 constexpr int KETT_TILE = 128;
-constexpr int BRA_GROUP_MAX = 8;  // bra pairs per group (same first shell)
-constexpr int BRA_GROUP_NPP = 32; // primitive pairs per group (a single pair may exceed)
 
 // Arguments of one class-quartet J/K launch.
 struct JKLaunch {
@@ -57,13 +55,8 @@ struct JKLaunch {
   const double* ketT;
   const long long* tileOff;
   int braTileBeg, ketTileBeg;
-  // bra groups (grouped light classes): bra pairs of a class reordered so
-  // that pairs with the same first shell are adjacent (braPerm: position in
-  // the class list), cut into groups {first index into braPerm, count}
-  const int* braPerm;
-  const int2* groups;
-  int braGroupBeg, braNGroups, ketGroupBeg, ketNGroups;
-  int jmat, kmat;           // the J and the K matrix when nMat == 2 (else -1)
+  const float* Xc32;        // FP32 copy of Xc (mixed builds, FP32 class kernels)
+  int lsum;                 // la + lb + lc + ld of the launch's class
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
@@ -73,11 +66,16 @@ struct JKLaunch {
 cqf_status fail(cqf_status s, const std::string& msg);
 
 // Workspace layout of one contraction (in doubles, each part 256-B aligned):
-// [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat | gmax
+// [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat |
+// gmax | norms^T | pair norms | work counters | Xc in FP32 (mixed real
+// builds) | quartet masks of the fast class kernels (per class pair one uint2
+// per bra pair and ket tile, then the two lists of non-empty words;
+// oMaskCls[cb][ck]: first uint2 of a class pair, relative to oMask)
+constexpr int NWORK = 4 * NCLS * NCLS;  // class-kernel work counters / list lengths per call
 struct WsLayout {
-  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oWork, oNmT, oPN, total;
+  size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oNmT, oPN, oWork, oXc32, oMask, total;
+  size_t oMaskCls[NCLS][NCLS];
 };
-constexpr int NWORK = 2 * NCLS * NCLS;  // persistent-kernel work counters per call
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
 cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat);
 // The contraction on a caller-provided device workspace of ws_layout().total
@@ -169,7 +167,6 @@ struct cqf_basis {
   bool tuning = false;
   std::vector<cudaEvent_t> tune_ev;
   int cls_tile_beg[cqf::NCLS] = {0};    // first ket tile of each class
-  int cls_group_beg[cqf::NCLS] = {0}, cls_group_cnt[cqf::NCLS] = {0};
   std::vector<double> h_schwarz;         // nshell^2
   // device-resident basis data
   cqf::ShellDev* d_shells = nullptr;
@@ -179,8 +176,6 @@ struct cqf_basis {
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
   float2* d_pairRange = nullptr;         // per pair: FP32 range data
-  int* d_braPerm = nullptr;              // npair: class-relative bra order
-  int2* d_groups = nullptr;              // bra groups of all classes
   double* d_boys64 = nullptr;
   float* d_boys32 = nullptr;
   double* d_schwarz = nullptr;

@@ -1,7 +1,9 @@
 // Closed-shell fast path: real densities flagged Hermitian (symmetric), every
 // shell l <= 2.  One thread per unique quartet, generated straight-line
-// McMurchie-Davidson code per class (gen/cqf_gen_jk.cuh), FP64 or FP32
-// primitive arithmetic chosen per launch, FP64 accumulation.
+// McMurchie-Davidson code per class and precision (gen/cqf_gen_jk.cuh): a
+// planning pass names each quartet's precision, then an FP64 and (mixed
+// builds) an FP32 kernel per class compute their quartets; FP64
+// accumulation.
 //
 // Screening, unique-quartet set and degeneracy are those of the generic
 // kernel (cqf_jk_kernels.cuh); the digestion uses the canonical quartet order
@@ -18,8 +20,8 @@ namespace cqf {
 
 static_assert(JK_THREADS == KETT_TILE, "a ket tile is one block of kets");
 
-template <int N>
-__device__ __forceinline__ void warp_sum(double (&v)[N]) {
+template <typename T, int N>
+__device__ __forceinline__ void warp_sum(T (&v)[N]) {
 #pragma unroll
   for (int i = 0; i < N; i++) {
 #pragma unroll
@@ -65,15 +67,7 @@ __device__ __forceinline__ const float* boys_rows<float>(const JKLaunch& a, int 
   return a.boys32 + (size_t)L * BOYS_NPTS * BOYS_ROW32;
 }
 
-// Persistent class kernel.  Every warp independently takes work items (bra
-// pair, chunk, ket tile of 32) from a device counter until none are left --
-// no block barriers.  The Boys rows of the class's angular sum (29 KB FP64,
-// 12 KB FP32) are read from global memory through L1: staging them in shared
-// memory capped residency at 6 blocks per SM and measured slower.  On the mixed path a warp computes its
-// quartets in FP32 when every surviving quartet's bound is below the cut
-// and in FP64 otherwise (kets are sorted by Schwarz bound, so the warps of
-// a bra row switch from FP64 to FP32 once), in one traversal.
-constexpr int WTILE = 32;  // kets per work item (one warp)
+constexpr int WTILE = 32;  // kets per mask word (one warp's worth)
 
 // Shell-block norm maximum of a quartet in the reference's roles
 // (direct.hpp:1693-1736), with the warp-uniform bra pair P: the pair norms
@@ -97,128 +91,82 @@ __device__ __forceinline__ double sh_max_bra(const JKLaunch& a, const PairDev& P
   return fmax(m, fmax(nP, nQ));
 }
 
-template <class G64, class G32, bool MIXED>
-__global__ void __launch_bounds__(JK_THREADS, G64::MINB)
-    jk_fast_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
-  static_assert(G64::NCHUNK == G32::NCHUNK && G64::NI == G32::NI, "shared chunking");
-  constexpr int NA = ncart(G64::LA), NB = ncart(G64::LB);
-  constexpr int NCH = G64::NCHUNK;
-  constexpr int LSUM = G64::LA + G64::LB + G64::LC + G64::LD;
-  const double cut = MIXED ? a.fp32_cut : 0.0;
-  constexpr bool mixed = MIXED;
-  const double* boys64 = boys_rows<double>(a, LSUM);
-  const float* boys32 = boys_rows<float>(a, LSUM);
+// Planning pass of one class pair: for every (bra pair, tile of 32 kets) the
+// quartets that survive the Schwarz x density screen, split by precision --
+// mask.x: lanes computed in FP64, mask.y: lanes computed in FP32 (mixed
+// builds: screening bound below the cut and inside the FP32 range guard).
+// Quartet set, screens and counts are those of the reference's loop
+// (direct.hpp:1642-1805); in the same class a ket sits at or before its bra
+// (each unordered pair of pairs once).  The masks form one row-major
+// sequence of words (bra pair, ket tile); a warp takes runs of 32
+// consecutive words and appends the indices of its non-empty words to one
+// list per precision (lengths in lcount[0 / 1]), so the class kernels visit
+// only words that name quartets of their precision.
+constexpr int PLAN_RUN = 32;
+template <bool MIXED>
+__global__ void __launch_bounds__(256)
+    jk_plan_kernel(const JKLaunch a, uint2* __restrict__ masks, int* __restrict__ list64,
+                   int* __restrict__ list32, unsigned int* __restrict__ lcount) {
   const int lane = threadIdx.x & 31;
-  const int ketTiles = (a.nKet + WTILE - 1) / WTILE;
-  const long long perBra = (long long)ketTiles * NCH;
-  const long long total = (long long)a.nBra * perBra;
-  const size_t nc = a.ncart;
-  const size_t matStride = (size_t)a.ncart * a.ncart;
-  // quartet counts of this warp, flushed once at exit
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  const int nTiles = (a.nKet + WTILE - 1) / WTILE;
+  const int nWords = a.nBra * nTiles;
+  const int nRuns = (nWords + PLAN_RUN - 1) / PLAN_RUN;
+  const double cut = MIXED ? a.fp32_cut : 0.0;
   unsigned long long cVis = 0, cScr = 0, c32 = 0, c64 = 0;
-
-  for (;;) {
-    unsigned int itemU = 0;
-    if (lane == 0) itemU = atomicAdd(work, 1u);
-    const long long item = (long long)__shfl_sync(0xffffffffu, itemU, 0);
-    if (item >= total) break;
-    const int ib = (int)(item / perBra);
-    const int rem = (int)(item % perBra);
-    const int ch = rem / ketTiles, tile = rem % ketTiles;
-    // same class: each unordered pair {P, Q} once, as ket position <= bra
-    // position (roles still follow the lex order)
-    if (a.same && tile * WTILE > ib) continue;
-    const int jk = tile * WTILE + lane;
-    const PairDev P = a.pairs[a.braBeg + ib];
-    bool visited = false, screened = false, w64 = false, w32 = false;
-    PairDev Q;
-    if (jk < a.nKet && !(a.same && jk > ib)) {
-      Q = a.pairs[a.ketBeg + jk];
-      visited = true;
-    }
-    const bool counter = ch == 0;  // one count per quartet
-    const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * WTILE].Q;
-    if (a.screen && tileMax < a.thresh) {
-      if (counter) {
+  for (int run = gw; run < nRuns; run += nw) {
+    int my64 = -1, my32 = -1, n64 = 0, n32 = 0;
+    const int wEnd = min((run + 1) * PLAN_RUN, nWords);
+    for (int word = run * PLAN_RUN; word < wEnd; word++) {
+      const int ib = word / nTiles, tile = word - ib * nTiles;
+      unsigned b64 = 0u, b32 = 0u;
+      if (!(a.same && tile * WTILE > ib)) {  // else: no quartet in this word
+        const int jk = tile * WTILE + lane;
+        const PairDev P = a.pairs[a.braBeg + ib];
+        const bool visited = jk < a.nKet && !(a.same && jk > ib);
+        const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * WTILE].Q;
+        bool screened = false, w32 = false;
+        if (a.screen && tileMax < a.thresh) {
+          screened = true;
+        } else if (visited && a.screen) {
+          const PairDev Q = a.pairs[a.ketBeg + jk];
+          const bool pRef = P.lex >= Q.lex;
+          const double bound = sh_max_bra(a, P, Q, __ldg(a.pairNorm + a.braBeg + ib),
+                                          __ldg(a.pairNorm + a.ketBeg + jk), pRef) * P.Q * Q.Q;
+          screened = bound < a.thresh;
+          w32 = MIXED && !screened && bound < cut &&
+                fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                              __ldg(a.pairRange + a.ketBeg + jk), a.lsum, 0, 0);
+        }  // without the screen every quartet runs in FP64
         const unsigned bv = __ballot_sync(0xffffffffu, visited);
+        const unsigned bs = __ballot_sync(0xffffffffu, visited && screened);
+        b32 = __ballot_sync(0xffffffffu, visited && !screened && w32);
+        b64 = bv & ~bs & ~b32;
         cVis += __popc(bv);
-        cScr += __popc(bv);
+        cScr += __popc(bs);
+        c32 += __popc(b32);
+        c64 += __popc(b64);
       }
-      continue;
-    }
-    int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
-    if (visited) {
-      const bool pRef = P.lex >= Q.lex;
-      const PairDev& R12 = pRef ? P : Q;
-      const PairDev& R34 = pRef ? Q : P;
-      s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
-      double bound = 1e300;
-      if (a.screen) {
-        bound = sh_max_bra(a, P, Q, __ldg(a.pairNorm + a.braBeg + ib),
-                           __ldg(a.pairNorm + a.ketBeg + jk), pRef) * P.Q * Q.Q;
-        screened = bound < a.thresh;
+      if (lane == 0) masks[word] = make_uint2(b64, b32);
+      if (b64) {
+        if (lane == n64) my64 = word;
+        n64++;
       }
-      w64 = !screened;
-      w32 = w64 && mixed && bound < cut &&
-            fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib), __ldg(a.pairRange + a.ketBeg + jk),
-                          LSUM, 0, 0);
-    }
-    // one precision per warp: FP32 only when every surviving quartet of the
-    // warp is below the cut (no divergent FP64 / FP32 code in a warp)
-    if (__any_sync(0xffffffffu, w64 && !w32)) {
-      w32 = false;
-    } else {
-      w64 = w64 && !w32;
-    }
-    const unsigned b64 = __ballot_sync(0xffffffffu, w64);
-    const unsigned b32 = __ballot_sync(0xffffffffu, w32);
-    if (counter) {
-      cVis += __popc(__ballot_sync(0xffffffffu, visited));
-      cScr += __popc(__ballot_sync(0xffffffffu, screened));
-      c64 += __popc(b64);
-      c32 += __popc(b32);
-    }
-    if (!(b64 | b32)) continue;
-    const bool work_ = w64 || w32;
-
-    const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
-                       ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
-    const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
-    double I[G64::NI];
-    const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
-    if (w64) {
-      G64::template eri<double>(P, Q, a.pp, kq, boys64, ch, I);
-    } else if (MIXED && w32) {
-      G32::template eri<float>(P, Q, a.pp, kq, boys32, ch, I);
-    } else {
-#pragma unroll
-      for (int i = 0; i < G64::NI; i++) I[i] = 0.0;
-    }
-#pragma unroll 1
-    for (int m = 0; m < a.nMat; m++) {
-      const int fl = __ldg(a.flags + m);
-      const bool doJ = !(fl & 2), doK = (fl & 2);
-      double jab[NA * NB];
-#pragma unroll
-      for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
-      const double* X = a.Xc + m * matStride;
-      double* A = a.Ac + m * matStride;
-      G64::digest(I, ch, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, (fl & 4) ? -sK : sK,
-                  doJ && work_, doK && work_,
-                  jab);
-      if (doJ) {
-        // every lane of the warp shares the bra pair: reduce, one atomic each
-#pragma unroll
-        for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
-        warp_sum(jab);
-        if (lane == 0) {
-#pragma unroll
-          for (int i = 0; i < NA * NB; i++)
-            if (jab[i] != 0.0)
-              atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
-        }
+      if (b32) {
+        if (lane == n32) my32 = word;
+        n32++;
       }
     }
+    unsigned int base64 = 0, base32 = 0;
+    if (lane == 0) {
+      if (n64) base64 = atomicAdd(lcount + 0, (unsigned)n64);
+      if (n32) base32 = atomicAdd(lcount + 1, (unsigned)n32);
+    }
+    base64 = __shfl_sync(0xffffffffu, base64, 0);
+    base32 = __shfl_sync(0xffffffffu, base32, 0);
+    if (lane < n64) list64[base64 + lane] = my64;
+    if (lane < n32) list32[base32 + lane] = my32;
   }
   if (lane == 0) {
     if (cVis) atomicAdd(a.counters + 0, cVis);
@@ -228,186 +176,162 @@ __global__ void __launch_bounds__(JK_THREADS, G64::MINB)
   }
 }
 
-// Grouped variant for the light single-chunk classes (G64::GROUPED): a work
-// item is (bra group, ket tile of 32); the group's bra pairs share their
-// first shell A, so each lane's updates J_cd, K_ac and K_ad (targets fixed by
-// its ket pair and by A) are summed in registers over the whole group and
-// flushed once -- fewer atomics than one flush per quartet.  Launched when
-// the call has one J and one K matrix (else jk_fast_kernel runs; the
-// per-matrix flush below keeps the kernel correct for any matrix list).
-// Quartet set, screens, roles, degeneracy and precision choice are those of
-// jk_fast_kernel.
-template <class G64, class G32, bool MIXED>
-__global__ void __launch_bounds__(JK_THREADS, G64::MINB)
-    jk_group_kernel(const JKLaunch a, unsigned int* __restrict__ work) {
-  static_assert(G64::NCHUNK == 1 && G32::NCHUNK == 1, "single-chunk classes");
-  constexpr int NA = ncart(G64::LA), NB = ncart(G64::LB);
-  constexpr int NC = ncart(G64::LC), ND = ncart(G64::LD);
-  constexpr int LSUM = G64::LA + G64::LB + G64::LC + G64::LD;
-  const double cut = MIXED ? a.fp32_cut : 0.0;
-  const double* boys64 = boys_rows<double>(a, LSUM);
-  const float* boys32 = boys_rows<float>(a, LSUM);
+// Position of the n-th (0-based) set bit of m (n < popc(m)).
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const unsigned lo = m & ((1u << w) - 1u);
+    const int c = __popc(lo);
+    if (n >= c) {
+      n -= c;
+      m >>= w;
+      pos += w;
+    } else {
+      m = lo;
+    }
+  }
+  return pos;
+}
+
+// Class kernel of one shell-quartet class in one precision (G = GenJK64_x
+// or GenJK32_x; FP32 = which mask half and word list it uses).  A work item
+// is (run of entriesPerItem consecutive entries of the precision's word
+// list, ket component chunk), handed out by a device counter.  A warp walks
+// its run's words and packs the quartets they name into batches of 32 lanes
+// (nth_set_bit), so every lane of a batch computes a surviving quartet; a
+// batch may span two bra pairs.  The batch's integrals of the chunk come
+// from generated straight-line McMurchie-Davidson code and are digested per
+// density: J_ab warp-reduced when the batch has one bra pair (per lane
+// otherwise), J_cd and the four exchange blocks with FP64 atomics.  The FP32
+// kernel forms integrals and products in FP32 from the FP32 copy of the
+// Cartesian densities; accumulation is FP64 in both.
+template <class G, bool FP32>
+__global__ void __launch_bounds__(JK_THREADS, G::MINB)
+    jk_class_kernel(const JKLaunch a, const uint2* __restrict__ masks,
+                    const int* __restrict__ list, const unsigned int* __restrict__ lcount,
+                    int entriesPerItem, unsigned int* __restrict__ counter) {
+  using T = typename G::T;
+  constexpr int NA = ncart(G::LA), NB = ncart(G::LB);
+  constexpr int NCH = G::NCHUNK;
+  constexpr int LSUM = G::LA + G::LB + G::LC + G::LD;
+  const T* boys = boys_rows<T>(a, LSUM);
+  const T* Xbase = FP32 ? reinterpret_cast<const T*>(a.Xc32) : reinterpret_cast<const T*>(a.Xc);
   const int lane = threadIdx.x & 31;
-  const int ketTiles = (a.nKet + WTILE - 1) / WTILE;
-  const long long total = (long long)a.braNGroups * ketTiles;
+  const int nTiles = (a.nKet + WTILE - 1) / WTILE;
+  const int nEntries = (int)*lcount;  // written by the planning pass
+  const int nItems = (nEntries + entriesPerItem - 1) / entriesPerItem * NCH;
   const size_t nc = a.ncart;
   const size_t matStride = (size_t)a.ncart * a.ncart;
-  const bool grouped = a.jmat >= 0;
-  unsigned long long cVis = 0, cScr = 0, c32 = 0, c64 = 0;
+  // entry e of the list: (word index, this precision's mask of it)
+  auto entry = [&](int e) {
+    const int w = __ldg(list + e);
+    return make_int2(w, (int)(FP32 ? __ldg(&masks[w].y) : __ldg(&masks[w].x)));
+  };
 
   for (;;) {
     unsigned int itemU = 0;
-    if (lane == 0) itemU = atomicAdd(work, 1u);
-    const long long item = (long long)__shfl_sync(0xffffffffu, itemU, 0);
-    if (item >= total) break;
-    const int g = (int)(item / ketTiles), tile = (int)(item % ketTiles);
-    const int2 gr = __ldg(a.groups + a.braGroupBeg + g);
-    const int jk = tile * WTILE + lane;
-    const bool qvalid = jk < a.nKet;
-    PairDev Q;
-    if (qvalid) Q = a.pairs[a.ketBeg + jk];
-    const double tileQ = a.pairs[a.ketBeg + tile * WTILE].Q;
-    double jcd[G64::NJCD], kac[G64::NKAC], kad[G64::NKAD];
-#pragma unroll
-    for (int i = 0; i < G64::NJCD; i++) jcd[i] = 0.0;
-#pragma unroll
-    for (int i = 0; i < G64::NKAC; i++) kac[i] = 0.0;
-#pragma unroll
-    for (int i = 0; i < G64::NKAD; i++) kad[i] = 0.0;
-    int cAgrp = 0;
-    bool any = false;
-
-#pragma unroll 1
-    for (int mm = 0; mm < gr.y; mm++) {
-      const int ib = __ldg(a.braPerm + a.braBeg + gr.x + mm);  // position in the class
-      if (a.same && tile * WTILE > ib) continue;  // warp-uniform
+    if (lane == 0) itemU = atomicAdd(counter, 1u);
+    const int item = (int)__shfl_sync(0xffffffffu, itemU, 0);
+    if (item >= nItems) break;
+    const int run = item / NCH, ch = item - run * NCH;
+    int e = run * entriesPerItem;
+    const int eEnd = min(e + entriesPerItem, nEntries);
+    int2 wm = entry(e);
+    unsigned m = (unsigned)wm.y;
+    for (;;) {
+      // pack the next (up to) 32 named quartets of the run into the lanes
+      int fill = 0, myW = -1, myBit = 0;
+      while (fill < 32 && e < eEnd) {
+        const int c = __popc(m);
+        const int take = min(c, 32 - fill);
+        const int r = lane - fill;
+        if (r >= 0 && r < take) {
+          myW = wm.x;
+          myBit = nth_set_bit(m, r);
+        }
+        fill += take;
+        if (take == c) {
+          if (++e < eEnd) {
+            wm = entry(e);
+            m = (unsigned)wm.y;
+          }
+        } else {
+          m &= ~((2u << nth_set_bit(m, take - 1)) - 1u);  // drop the bits taken
+        }
+      }
+      if (fill == 0) break;
+      const bool work_ = myW >= 0;
+      // lane 0 always holds a quartet; idle lanes take its bra pair
+      const int w0 = __shfl_sync(0xffffffffu, myW, 0);
+      const int wl = work_ ? myW : w0;
+      const int ib = wl / nTiles;
+      const int jk = (wl - ib * nTiles) * WTILE + myBit;
+      const bool oneBra = __all_sync(0xffffffffu, ib == w0 / nTiles);
       const PairDev P = a.pairs[a.braBeg + ib];
-      const bool visited = qvalid && !(a.same && jk > ib);
-      if (a.screen && __ldg(a.maxNorm) * P.Q * tileQ < a.thresh) {
-        const unsigned bv = __ballot_sync(0xffffffffu, visited);
-        cVis += __popc(bv);
-        cScr += __popc(bv);
-        continue;
-      }
-      bool screened = false, w64 = false, w32 = false;
-      int s1 = 0, s2 = 0, s3 = 0, s4 = 0;
-      if (visited) {
-        const bool pRef = P.lex >= Q.lex;
-        const PairDev& R12 = pRef ? P : Q;
-        const PairDev& R34 = pRef ? Q : P;
-        s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
-        double bound = 1e300;
-        if (a.screen) {
-          bound = sh_max_bra(a, P, Q, __ldg(a.pairNorm + a.braBeg + ib),
-                             __ldg(a.pairNorm + a.ketBeg + jk), pRef) * P.Q * Q.Q;
-          screened = bound < a.thresh;
-        }
-        w64 = !screened;
-        w32 = w64 && MIXED && bound < cut &&
-              fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
-                            __ldg(a.pairRange + a.ketBeg + jk), LSUM, 0, 0);
-      }
-      if (__any_sync(0xffffffffu, w64 && !w32)) w32 = false;
-      else w64 = w64 && !w32;
-      const unsigned b64 = __ballot_sync(0xffffffffu, w64);
-      const unsigned b32 = __ballot_sync(0xffffffffu, w32);
-      cVis += __popc(__ballot_sync(0xffffffffu, visited));
-      cScr += __popc(__ballot_sync(0xffffffffu, screened));
-      c64 += __popc(b64);
-      c32 += __popc(b32);
-      if (!(b64 | b32)) continue;
-      const bool work_ = w64 || w32;
-      cAgrp = P.cA;
-      any = any || work_;
-      const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
-                         ((s1 == s3 && s2 == s4) ? 1.0 : 2.0);
-      const double sJ = work_ ? 0.5 * deg : 0.0, sK = work_ ? 0.25 * deg : 0.0;
-      double I[G64::NI];
-      if (w64) {
-        const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
-        G64::template eri<double>(P, Q, a.pp, kq, boys64, 0, I);
-      } else if (MIXED && w32) {
-        const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jk / KETT_TILE) + jk % KETT_TILE};
-        G32::template eri<float>(P, Q, a.pp, kq, boys32, 0, I);
-      } else {
-#pragma unroll
-        for (int i = 0; i < G64::NI; i++) I[i] = 0.0;
-      }
+      PairDev Q{};  // idle lanes: npp = 0, no primitive loop
+      if (work_) Q = a.pairs[a.ketBeg + jk];
+      const bool pRef = P.lex >= Q.lex;
+      const int s1 = pRef ? P.s1 : Q.s1, s2 = pRef ? P.s2 : Q.s2;
+      const int s3 = pRef ? Q.s1 : P.s1, s4 = pRef ? Q.s2 : P.s2;
+      const T deg = T(((s1 == s2) ? 1 : 2) * ((s3 == s4) ? 1 : 2) *
+                      ((s1 == s3 && s2 == s4) ? 1 : 2));
+      const T sJ = work_ ? T(0.5) * deg : T(0), sK = work_ ? T(0.25) * deg : T(0);
+      const int jkc = work_ ? jk : 0;
+      const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jkc / KETT_TILE) + jkc % KETT_TILE};
+      T I[G::NI];
+      G::eri(P, Q, a.pp, kq, boys, ch, I);
 #pragma unroll 1
-      for (int m = 0; m < a.nMat; m++) {
-        const int fl = __ldg(a.flags + m);
+      for (int mt = 0; mt < a.nMat; mt++) {
+        const int fl = __ldg(a.flags + mt);
         const bool doJ = !(fl & 2), doK = (fl & 2);
-        double jab[NA * NB];
+        T jab[NA * NB];
 #pragma unroll
-        for (int i = 0; i < NA * NB; i++) jab[i] = 0.0;
-        const double* X = a.Xc + m * matStride;
-        double* A = a.Ac + m * matStride;
-        G64::digest_g(I, X, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK, (fl & 4) ? -sK : sK,
-                      doJ && work_, doK && work_,
-                      jab, jcd, kac, kad);
-        if (!grouped && work_) {  // flush this matrix's sums now
-#pragma unroll
-          for (int k = 0; k < G64::NJCD; k++) {
-            if (jcd[k] != 0.0)
-              atomicAdd(A + (size_t)(Q.cA + k / ND) + (size_t)(Q.cB + k % ND) * nc, jcd[k]);
-            jcd[k] = 0.0;
-          }
-#pragma unroll
-          for (int k = 0; k < G64::NKAC; k++) {
-            if (kac[k] != 0.0)
-              atomicAdd(A + (size_t)(Q.cA + k % NC) + (size_t)(P.cA + k / NC) * nc, kac[k]);
-            kac[k] = 0.0;
-          }
-#pragma unroll
-          for (int k = 0; k < G64::NKAD; k++) {
-            if (kad[k] != 0.0)
-              atomicAdd(A + (size_t)(Q.cB + k % ND) + (size_t)(P.cA + k / ND) * nc, kad[k]);
-            kad[k] = 0.0;
-          }
-        }
+        for (int i = 0; i < NA * NB; i++) jab[i] = T(0);
+        double* A = a.Ac + mt * matStride;
+        G::digest(I, ch, Xbase + mt * matStride, A, nc, P.cA, P.cB, Q.cA, Q.cB, sJ, sK,
+                  (fl & 4) ? -sK : sK, doJ && work_, doK && work_, jab);
         if (doJ) {
 #pragma unroll
           for (int i = 0; i < NA * NB; i++) jab[i] *= sJ;
-          warp_sum(jab);
-          if (lane == 0) {
+          if (oneBra) {  // the lanes share the bra pair: reduce, one atomic each
+            warp_sum(jab);
+            if (lane == 0) {
+#pragma unroll
+              for (int i = 0; i < NA * NB; i++)
+                if (jab[i] != T(0))
+                  atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc,
+                            double(jab[i]));
+            }
+          } else if (work_) {
 #pragma unroll
             for (int i = 0; i < NA * NB; i++)
-              if (jab[i] != 0.0)
-                atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc, jab[i]);
+              if (jab[i] != T(0))
+                atomicAdd(A + (size_t)(P.cA + i / NB) + (size_t)(P.cB + i % NB) * nc,
+                          double(jab[i]));
           }
         }
       }
     }
-    if (grouped && any) {
-      double* AJ = a.Ac + a.jmat * matStride;
-      double* AK = a.Ac + a.kmat * matStride;
-#pragma unroll
-      for (int k = 0; k < G64::NJCD; k++)
-        if (jcd[k] != 0.0)
-          atomicAdd(AJ + (size_t)(Q.cA + k / ND) + (size_t)(Q.cB + k % ND) * nc, jcd[k]);
-#pragma unroll
-      for (int k = 0; k < G64::NKAC; k++)
-        if (kac[k] != 0.0)
-          atomicAdd(AK + (size_t)(Q.cA + k % NC) + (size_t)(cAgrp + k / NC) * nc, kac[k]);
-#pragma unroll
-      for (int k = 0; k < G64::NKAD; k++)
-        if (kad[k] != 0.0)
-          atomicAdd(AK + (size_t)(Q.cB + k % ND) + (size_t)(cAgrp + k / ND) * nc, kad[k]);
-    }
-  }
-  if (lane == 0) {
-    if (cVis) atomicAdd(a.counters + 0, cVis);
-    if (cScr) atomicAdd(a.counters + 1, cScr);
-    if (c32) atomicAdd(a.counters + 2, c32);
-    if (c64) atomicAdd(a.counters + 3, c64);
   }
 }
 
-// Launches the generated kernels of the class (la lb | lc ld) (either
-// orientation); returns false when the class has no generated kernel.
-// work: two zeroed device counters for this class (FP64, FP32 launch).
-inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned int* work,
-                           int nsm, cudaStream_t st, int blocksPerSm = 8) {
+// Word-list entries per work item of a class kernel: about 256 items per SM
+// over the class pair's words (an upper bound of the non-empty ones) and
+// its chunks, at most 64 entries.
+inline int entries_per_item(long long nWords, int nchunk, int nsm) {
+  const long long per = nWords * nchunk / ((long long)nsm * 256);
+  return (int)std::min<long long>(64, std::max<long long>(1, per));
+}
+
+// Launches the planning pass and the generated class kernels of the class
+// (la lb | lc ld) (either orientation); false when the class has no
+// generated kernel.  masks: the class pair's mask words (nBra x ceil(nKet /
+// 32) uint2) followed by its two word lists (nWords ints each); work: four
+// zeroed device counters (FP64 / FP32 class kernel items, FP64 / FP32 list
+// lengths).
+inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, uint2* masks,
+                           unsigned int* work, int nsm, cudaStream_t st, int blocksPerSm = 8) {
   if (a.nBra == 0 || a.nKet == 0) return true;
   bool done = false;
   auto go = [&](auto tag64, auto tag32, bool swap) {
@@ -418,38 +342,32 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, unsigned 
       b.braBeg = a.ketBeg; b.nBra = a.nKet;
       b.ketBeg = a.braBeg; b.nKet = a.nBra;
       b.braTileBeg = a.ketTileBeg; b.ketTileBeg = a.braTileBeg;
-      b.braGroupBeg = a.ketGroupBeg; b.braNGroups = a.ketNGroups;
-      b.ketGroupBeg = a.braGroupBeg; b.ketNGroups = a.braNGroups;
     }
-    const long long tiles = (long long)((b.nKet + WTILE - 1) / WTILE);
-    // bra groups pay off when one J and one K matrix share the sums;
-    // many-density launches use the per-quartet kernel
-    const bool useGroups = G64::GROUPED && b.jmat >= 0;
-    const long long items = useGroups ? (long long)b.braNGroups * tiles
-                                      : (long long)b.nBra * tiles * G64::NCHUNK;
-    // persistent blocks: enough for full residency on every SM (extra blocks
-    // queue and find the counter exhausted); one work item per warp at a time
-    constexpr int WPB = JK_THREADS / 32;
-    const unsigned g =
-        (unsigned)std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * blocksPerSm);
+    b.lsum = la + lb + lc + ld;
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
-    if constexpr (G64::GROUPED) {
-      if (useGroups) {
-        if (mixed)
-          jk_group_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
-        else
-          jk_group_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
-      } else {
-        if (mixed)
-          jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
-        else
-          jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
-      }
-    } else {
-      if (mixed)
-        jk_fast_kernel<G64, G32, true><<<g, JK_THREADS, 0, st>>>(b, work);
-      else
-        jk_fast_kernel<G64, G32, false><<<g, JK_THREADS, 0, st>>>(b, work);
+    const int nTiles = (b.nKet + WTILE - 1) / WTILE;
+    const long long nWords = (long long)b.nBra * nTiles;
+    const long long nRuns = (nWords + PLAN_RUN - 1) / PLAN_RUN;
+    const unsigned gp = (unsigned)std::min<long long>((nRuns + 7) / 8, (long long)nsm * 8);
+    // word lists: FP64 then FP32, nWords entries each; counts in work[2..3]
+    int* list64 = reinterpret_cast<int*>(masks + nWords);
+    int* list32 = list64 + nWords;
+    if (mixed)
+      jk_plan_kernel<true><<<gp, 256, 0, st>>>(b, masks, list64, list32, work + 2);
+    else
+      jk_plan_kernel<false><<<gp, 256, 0, st>>>(b, masks, list64, list32, work + 2);
+    constexpr int WPB = JK_THREADS / 32;
+    auto grid = [&](long long items) {
+      return (unsigned)std::max<long long>(
+          1, std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * blocksPerSm));
+    };
+    const int e64 = entries_per_item(nWords, G64::NCHUNK, nsm);
+    jk_class_kernel<G64, false><<<grid((nWords + e64 - 1) / e64 * G64::NCHUNK), JK_THREADS, 0,
+                                  st>>>(b, masks, list64, work + 2, e64, work);
+    if (mixed) {
+      const int e32 = entries_per_item(nWords, G32::NCHUNK, nsm);
+      jk_class_kernel<G32, true><<<grid((nWords + e32 - 1) / e32 * G32::NCHUNK), JK_THREADS, 0,
+                                   st>>>(b, masks, list32, work + 3, e32, work + 1);
     }
     done = true;
   };
@@ -484,7 +402,7 @@ __global__ void __launch_bounds__(JK_THREADS)
   auto ta = [&](int c, int mu) { return A.pure ? TA[c * nsph(GC::LA) + mu] : (c == mu ? 1.0 : 0.0); };
   auto tb = [&](int c, int nu) { return B.pure ? TB[c * nsph(GC::LB) + nu] : (c == nu ? 1.0 : 0.0); };
   double I[GC::NI];
-  GC::template eri<double>(P, P, pp, KetAoS{pp + P.pp_off},
+  GC::eri(P, P, pp, KetAoS{pp + P.pp_off},
                            boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I);
   for (int mu = 0; mu < na; mu++)
     for (int nu = 0; nu < nb; nu++) {

@@ -7,7 +7,10 @@ csrc/gen/ (not tracked).  For each class the generator
 * picks the orientation (which pair class is the block's bra) that keeps the
   Hermite intermediate G[cd][tuv] smallest,
 * splits the ket Cartesian components c into chunks so that the live set
-  (integral block + G + R) stays inside the register file,
+  (integral block + G + R) stays inside the register file -- separately for
+  each precision: an FP32 kernel keeps its integrals, Hermite intermediates
+  and digestion products in FP32 (half the registers of FP64), so its chunks
+  are larger,
 * emits E coefficients, Boys/R recursion, the G and integral contractions as
   scalar code with Hermite coefficients constant-folded (E^{00}_0 = 1,
   E^{ij}_t = 0 for t > i + j),
@@ -17,7 +20,9 @@ csrc/gen/ (not tracked).  For each class the generator
   (a warp's atomics then land in one column: the bra is warp-uniform); with a
   symmetric density and the final 1/2 (A + A^T) these equal the reference's
   updates
-  (include/particleintegrals/contract/direct.hpp:1858-1918).
+  (include/particleintegrals/contract/direct.hpp:1858-1918).  Products are
+  formed in the kernel's precision; every update is accumulated with an FP64
+  atomic.
 """
 import itertools
 import os
@@ -119,8 +124,8 @@ def orientation(c1, c2):
 
 def chunk_size(la, lb, lc, ld, prec):
     """ket component pairs (flattened cd index) per chunk, so that the live
-    set (integral chunk + G chunk + R, in 4-byte register units) stays under
-    the budget of the precision; the integral chunk is always FP64."""
+    set (integral chunk + G chunk + R, in 4-byte register units: 2 per FP64
+    value, 1 per FP32 value) stays under the budget."""
     nab = ncart(la) * ncart(lb)
     ncd = ncart(lc) * ncart(ld)
     hab = nherm(la + lb)
@@ -128,13 +133,13 @@ def chunk_size(la, lb, lc, ld, prec):
     w = 2 if prec == 64 else 1
     best = 1
     for cs in range(1, ncd + 1):
-        live = 2 * nab * cs + w * (cs * hab + hl)
+        live = w * (nab * cs + cs * hab + hl)
         if live <= 176:
             best = cs
     return best
 
 
-def use_mirror(la, lb, lc, ld, nchunk):
+def use_mirror(la, lb, lc, ld, nchunk, prec):
     """Ket-outer primitive loops (emit_eri_mirror) for single-chunk classes
     whose live set -- integral block, bra-side Hermite accumulators
     G'[ab][tau nu phi] and R, in 4-byte register units -- fits the budget."""
@@ -142,7 +147,8 @@ def use_mirror(la, lb, lc, ld, nchunk):
         return False
     nab = ncart(la) * ncart(lb)
     ncd = ncart(lc) * ncart(ld)
-    live = 2 * nab * ncd + 2 * (nab * nherm(lc + ld) + nherm(la + lb + lc + ld))
+    w = 2 if prec == 64 else 1
+    live = w * (nab * ncd + nab * nherm(lc + ld) + nherm(la + lb + lc + ld))
     return live <= 176
 
 
@@ -179,7 +185,7 @@ def emit_R(w, L, hall):
     return R
 
 
-def emit_eri_mirror(w, la, lb, lc, ld, CS):
+def emit_eri_mirror(w, la, lb, lc, ld, CS, prec):
     """eri() body with the ket primitives (per lane) in the outer loop and the
     bra primitives (shared by the warp) in the inner one:
         G'[ab][tnp] = sum_ip pref sum_tuv E^ab_tuv R_{t+tau,u+nu,v+phi}
@@ -220,17 +226,7 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS):
     if lab > 0:
         for x in range(3):
             w.line("const T PA%s = T(pa.PA[%d]), PB%s = T(pa.PB[%d]);" % (axes[x], x, axes[x], x))
-    w.line("const T pq = p + q;")
-    w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
-    w.line("const T alpha = p * q * (rpq * rpq);")
-    w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
-    w.line("T F[%d];" % (L + 1))
-    w.open("if constexpr (sizeof(T) == 8) {")
-    w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
-    w.close("} else {")
-    w.ind += 1
-    w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
-    w.close()
+    emit_boys(w, L, prec)
     w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
     R = emit_R(w, L, hall)
     eb = [E1D(w, la, lb, "ea" + axes[x], "o2p", "PA" + axes[x], "PB" + axes[x])
@@ -279,123 +275,64 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS):
             for ib in range(NB):
                 sm = " + ".join(("-" if sg else "") + " * ".join(fac + ["h_%d_%d_%d_%d_%d" % (ia, ib, ta, nu, ph)])
                                 for (ta, nu, ph, fac, sg) in terms)
-                w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+                w.line("I[%d] += %s;" % ((ia * NB + ib) * CS + k, sm))
     w.close("}")  # iq
     w.close("}")  # eri
 
 
-def emit_digest_g(w, A, B, Cc, Dd):
-    """digest_g(): the digestion of a single-chunk class with the updates
-    whose target is fixed by the ket and the bra's first shell -- J_cd, K_ac,
-    K_ad -- added into per-lane arrays (jcd, kac, kad), which the grouped
-    kernel sums over all bra pairs of a group that share that shell before
-    one flush; J_ab into jab (warp-reduced by the caller); K_bd, K_bc with
-    atomics as in digest()."""
-    NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
-    NAB, NCD = NA * NB, NC * ND
-    w.line("static constexpr int NJCD = %d, NKAC = %d, NKAD = %d;" % (NCD, NA * NC, NA * ND))
-    w.open("static __device__ __forceinline__ void digest_g(const double (&I)[%d], "
-           "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
-           "int cC, int cD, double sJ, double sK, double sKac, bool doJ, bool doK, double (&jab)[%d], "
-           "double (&jcd)[%d], double (&kac)[%d], double (&kad)[%d]) {"
-           % (NAB * NCD, NAB, NCD, NA * NC, NA * ND))
-    w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
-    w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
-    els = [(k,) + divmod(k, ND) for k in range(NCD)]  # (k, c, d)
-
-    def Iv(a, b, k):
-        return "I[%d]" % ((a * NB + b) * NCD + k)
-    w.open("if (doJ) {")
-    for (k, c, d) in els:
-        w.line("const double dcd_%d = ld(cD + %d, cC + %d);" % (k, d, c))
-    for a_ in range(NA):
-        for b_ in range(NB):
-            sm = " + ".join("%s * dcd_%d" % (Iv(a_, b_, k), k) for (k, c, d) in els)
-            w.line("jab[%d] += %s;" % (a_ * NB + b_, sm))
-    for a_ in range(NA):
-        for b_ in range(NB):
-            w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a_, b_, a_, b_))
-    for (k, c, d) in els:
-        sm = " + ".join("%s * dab_%d_%d" % (Iv(a_, b_, k), a_, b_)
-                        for a_ in range(NA) for b_ in range(NB))
-        w.line("jcd[%d] += sJ * (%s);" % (k, sm))
-    w.close()
-    w.open("if (doK) {")
-    for b_ in range(NB):
-        for d in range(ND):
-            w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b_, d, b_))
-    for a_ in range(NA):
-        for c in range(NC):
-            sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
-                            for b_ in range(NB) for (k, cc, d) in els if cc == c)
-            w.line("kac[%d] += sKac * (%s);" % (a_ * NC + c, sm))
-    for a_ in range(NA):
-        for c in range(NC):
-            w.line("const double dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
-    for b_ in range(NB):
-        for d in range(ND):
-            sm = " + ".join("%s * dac_%d_%d" % (Iv(a_, b_, k), a_, c)
-                            for a_ in range(NA) for (k, c, dd) in els if dd == d)
-            w.line("add(cD + %d, cB + %d, sK * (%s));" % (d, b_, sm))
-    for b_ in range(NB):
-        for c in range(NC):
-            w.line("const double dbc_%d_%d = ld(cB + %d, cC + %d);" % (b_, c, b_, c))
-    for a_ in range(NA):
-        for d in range(ND):
-            sm = " + ".join("%s * dbc_%d_%d" % (Iv(a_, b_, k), b_, c)
-                            for b_ in range(NB) for (k, c, dd) in els if dd == d)
-            w.line("kad[%d] += sK * (%s);" % (a_ * ND + d, sm))
-    for a_ in range(NA):
-        for d in range(ND):
-            w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a_, d, a_, d))
-    for b_ in range(NB):
-        for c in range(NC):
-            sm = " + ".join("%s * dad_%d_%d" % (Iv(a_, b_, k), a_, d)
-                            for a_ in range(NA) for (k, cc, d) in els if cc == c)
-            w.line("add(cC + %d, cB + %d, sK * (%s));" % (c, b_, sm))
-    w.close()
-    w.close("}")  # digest_g
+def emit_boys(w, L, prec):
+    """1/sqrt(p + q), alpha, T and F_0..F_L in the kernel's precision (the
+    FP32 kernels evaluate T >= 36 in FP64, boys_f32)."""
+    w.line("const T pq = p + q;")
+    w.line("const T rpq = %s;" % ("rsqrt(pq)" if prec == 64 else "rsqrtf(pq)"))
+    w.line("const T alpha = p * q * (rpq * rpq);")
+    w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
+    w.line("T F[%d];" % (L + 1))
+    w.line("boys_f%d<%d>(Targ, F, boys);  // rows of L" % (prec, L))
 
 
 def gen_class(la, lb, lc, ld, prec):
-    """Struct GenJK<prec>_<class>: eri<T>() computes chunk ch (a contiguous
-    range of the flattened ket component index cd) of the contracted Cartesian
-    block; digest() adds that chunk's J/K contributions of one density."""
+    """Struct GenJK<prec>_<class>: eri() computes chunk ch (a contiguous range
+    of the flattened ket component index cd) of the contracted Cartesian
+    block in the struct's precision T; digest() adds that chunk's J/K
+    contributions of one density (products in T, FP64 atomics)."""
     w = W()
     A, B, Cc, Dd = carts(la), carts(lb), carts(lc), carts(ld)
     NA, NB, NC, ND = len(A), len(B), len(Cc), len(Dd)
     NAB, NCD = NA * NB, NC * ND
     lab, lcd = la + lb, lc + ld
     L = lab + lcd
-    # both precisions use the FP64 chunking: one launch computes FP64 and
-    # FP32 quartets side by side with the same chunk index and digestion
-    CS = chunk_size(la, lb, lc, ld, 64)
+    CS = chunk_size(la, lb, lc, ld, prec)
     nchunk = (NCD + CS - 1) // CS
-    mirror = use_mirror(la, lb, lc, ld, nchunk)
+    mirror = use_mirror(la, lb, lc, ld, nchunk, prec)
     chunks = [list(range(k * CS, min(NCD, (k + 1) * CS))) for k in range(nchunk)]
     hab = herm_list(lab)
     hall = herm_list(L)
+    T = "double" if prec == 64 else "float"
     name = "%d_%d%d%d%d" % (prec, la, lb, lc, ld)
-    w.line("// (%s%s|%s%s), FP%d build: NAB=%d NCD=%d L=%d, %d chunk(s) of <= %d cd pairs"
-           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], prec, NAB, NCD, L, nchunk, CS))
+    w.line("// (%s%s|%s%s), FP%d: NAB=%d NCD=%d L=%d, %d chunk(s) of <= %d cd pairs%s"
+           % ("spdf"[la], "spdf"[lb], "spdf"[lc], "spdf"[ld], prec, NAB, NCD, L, nchunk, CS,
+              ", ket-outer primitive loops" if mirror else ""))
     w.open("struct GenJK%s {" % name)
+    w.line("using T = %s;" % T)
     w.line("static constexpr int LA = %d, LB = %d, LC = %d, LD = %d;" % (la, lb, lc, ld))
     w.line("static constexpr int NCHUNK = %d;" % nchunk)
     w.line("static constexpr int NI = %d;  // integrals per chunk" % (NAB * CS))
     # resident blocks per SM the register allocator should target: small
     # low-L classes are latency bound and gain from occupancy
-    minb = 6 if L <= 1 else (4 if (L == 2 and NAB * CS <= 9) else 1)
+    live = (2 if prec == 64 else 1) * (NAB * CS + CS * len(hab) + len(hall))
+    minb = 6 if L <= 1 else (4 if live <= 96 else (2 if live <= 150 else 1))
     w.line("static constexpr int MINB = %d;" % minb)
     # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
-    w.line("template <typename T, class KA>")
+    w.line("template <class KA>")
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
            "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
-           "const int ch, double (&I)[%d]) {" % (NAB * CS))
+           "const int ch, T (&I)[%d]) {" % (NAB * CS))
     if mirror:
-        emit_eri_mirror(w, la, lb, lc, ld, CS)
+        emit_eri_mirror(w, la, lb, lc, ld, CS, prec)
     else:
         w.line("#pragma unroll")
-        w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NAB * CS))
+        w.line("for (int i = 0; i < %d; i++) I[i] = T(0);" % (NAB * CS))
         w.line("const T PI52x2 = T(34.986836655249725693);")
         w.line("#pragma unroll 1")
         w.open("for (int ip = 0; ip < P.npp; ip++) {")
@@ -413,17 +350,7 @@ def gen_class(la, lb, lc, ld, prec):
         w.open("for (int iq = 0; iq < Q.npp; iq++) {")
         w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
         w.line("const T X = Px - T(kq.P(iq, 0)), Y = Py - T(kq.P(iq, 1)), Z = Pz - T(kq.P(iq, 2));")
-        w.line("const T pq = p + q;")
-        w.line("const T rpq = sizeof(T) == 8 ? T(rsqrt(double(pq))) : T(rsqrtf(float(pq)));")
-        w.line("const T alpha = p * q * (rpq * rpq);")
-        w.line("const T Targ = alpha * (X * X + Y * Y + Z * Z);")
-        w.line("T F[%d];" % (L + 1))
-        w.open("if constexpr (sizeof(T) == 8) {")
-        w.line("boys_f64<%d>(Targ, F, reinterpret_cast<const double*>(boys));  // rows of L" % L)
-        w.close("} else {")
-        w.ind += 1
-        w.line("boys_f32<%d>(Targ, F, reinterpret_cast<const float*>(boys));" % L)
-        w.close()
+        emit_boys(w, L, prec)
         w.line("const T pref = PI52x2 * rpq * Kab * Kcd;")
         if lcd > 0:
             for x in range(3):
@@ -431,33 +358,7 @@ def gen_class(la, lb, lc, ld, prec):
                        % (axes[x], x, axes[x], x))
         ek = [E1D(w, lc, ld, "ec" + axes[x], "o2q", "QC" + axes[x], "QD" + axes[x])
               for x in range(3)] if lcd > 0 else None
-        R = {}
-        w.line("const T m2a = T(-2) * alpha;")
-        pw = ["T(1)"]
-        for n in range(1, L + 1):
-            w.line("const T a%d = %s;" % (n, "m2a" if n == 1 else "a%d * m2a" % (n - 1)))
-            pw.append("a%d" % n)
-        for n in range(L, -1, -1):
-            w.line("const T r%d_0_0_0 = %s;" % (n, "F[0]" if n == 0 else "%s * F[%d]" % (pw[n], n)))
-            R[(n, 0, 0, 0)] = "r%d_0_0_0" % n
-        for tot in range(1, L + 1):
-            for n in range(L - tot, -1, -1):
-                for (t, u, v) in [h for h in hall if sum(h) == tot]:
-                    if t > 0:
-                        e = "X * %s" % R[(n + 1, t - 1, u, v)]
-                        if t > 1:
-                            e += " + T(%d) * %s" % (t - 1, R[(n + 1, t - 2, u, v)])
-                    elif u > 0:
-                        e = "Y * %s" % R[(n + 1, t, u - 1, v)]
-                        if u > 1:
-                            e += " + T(%d) * %s" % (u - 1, R[(n + 1, t, u - 2, v)])
-                    else:
-                        e = "Z * %s" % R[(n + 1, t, u, v - 1)]
-                        if v > 1:
-                            e += " + T(%d) * %s" % (v - 1, R[(n + 1, t, u, v - 2)])
-                    nm = "r%d_%d_%d_%d" % (n, t, u, v)
-                    w.line("const T %s = %s;" % (nm, e))
-                    R[(n, t, u, v)] = nm
+        R = emit_R(w, L, hall)
         if nchunk > 1:
             w.open("switch (ch) {")
         for chv, cdl in enumerate(chunks):
@@ -519,19 +420,20 @@ def gen_class(la, lb, lc, ld, prec):
                 for k in range(CS):
                     sm = " + ".join(("%s * " % nm if nm else "") + "g_%d_%d_%d_%d" % (k, t, u, v)
                                     for (t, u, v, nm) in names)
-                    w.line("I[%d] += double(%s);" % ((ia * NB + ib) * CS + k, sm))
+                    w.line("I[%d] += %s;" % ((ia * NB + ib) * CS + k, sm))
         w.close("}")  # ip
         w.close("}")  # eri
     # ---- digestion
-    w.line("// J/K contributions of chunk ch for one density (symmetric X).  The")
-    w.line("// K_ac update reads X(d, b) (the other three read X in bra-row order): sKac")
-    w.line("// = sK for a symmetric X, -sK for an antisymmetric one")
-    w.open("static __device__ __forceinline__ void digest(const double (&I)[%d], const int ch, "
-           "const double* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
-           "int cC, int cD, double sJ, double sK, double sKac, bool doJ, bool doK, double (&jab)[%d]) {"
+    w.line("// J/K contributions of chunk ch for one density (symmetric X, in the")
+    w.line("// kernel's precision).  The K_ac update reads X(d, b) (the other three read")
+    w.line("// X in bra-row order): sKac = sK for a symmetric X, -sK for an antisymmetric")
+    w.line("// one.  Every update is one FP64 atomic.")
+    w.open("static __device__ __forceinline__ void digest(const T (&I)[%d], const int ch, "
+           "const T* __restrict__ X, double* __restrict__ Acc, size_t nc, int cA, int cB, "
+           "int cC, int cD, T sJ, T sK, T sKac, bool doJ, bool doK, T (&jab)[%d]) {"
            % (NAB * CS, NAB))
     w.line("auto ld = [&](int r, int c) { return __ldg(X + (size_t)r + (size_t)c * nc); };")
-    w.line("auto add = [&](int r, int c, double v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, v); };")
+    w.line("auto add = [&](int r, int c, T v) { atomicAdd(Acc + (size_t)r + (size_t)c * nc, double(v)); };")
     if nchunk > 1:
         w.open("switch (ch) {")
     for chv, cdl in enumerate(chunks):
@@ -545,14 +447,14 @@ def gen_class(la, lb, lc, ld, prec):
             return "I[%d]" % ((a * NB + b) * CS + k)
         w.open("if (doJ) {")
         for (k, c, d) in els:
-            w.line("const double dcd_%d = ld(cD + %d, cC + %d);" % (k, d, c))
+            w.line("const T dcd_%d = ld(cD + %d, cC + %d);" % (k, d, c))
         for a_ in range(NA):
             for b_ in range(NB):
                 sm = " + ".join("%s * dcd_%d" % (Iv(a_, b_, k), k) for (k, c, d) in els)
                 w.line("jab[%d] += %s;" % (a_ * NB + b_, sm))
         for a_ in range(NA):
             for b_ in range(NB):
-                w.line("const double dab_%d_%d = ld(cA + %d, cB + %d);" % (a_, b_, a_, b_))
+                w.line("const T dab_%d_%d = ld(cA + %d, cB + %d);" % (a_, b_, a_, b_))
         for (k, c, d) in els:
             sm = " + ".join("%s * dab_%d_%d" % (Iv(a_, b_, k), a_, b_)
                             for a_ in range(NA) for b_ in range(NB))
@@ -562,7 +464,7 @@ def gen_class(la, lb, lc, ld, prec):
         # K_ac += sum_bd I D[d,b]
         for b_ in range(NB):
             for d in ds_:
-                w.line("const double ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b_, d, b_))
+                w.line("const T ddb_%d_%d = ld(cD + %d, cB + %d);" % (d, b_, d, b_))
         for a_ in range(NA):
             for c in cs_:
                 sm = " + ".join("%s * ddb_%d_%d" % (Iv(a_, b_, k), d, b_)
@@ -571,7 +473,7 @@ def gen_class(la, lb, lc, ld, prec):
         # K_bd += sum_ac I D[a,c]
         for a_ in range(NA):
             for c in cs_:
-                w.line("const double dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
+                w.line("const T dac_%d_%d = ld(cA + %d, cC + %d);" % (a_, c, a_, c))
         for b_ in range(NB):
             for d in ds_:
                 sm = " + ".join("%s * dac_%d_%d" % (Iv(a_, b_, k), a_, c)
@@ -580,7 +482,7 @@ def gen_class(la, lb, lc, ld, prec):
         # K_ad += sum_bc I D[b,c]
         for b_ in range(NB):
             for c in cs_:
-                w.line("const double dbc_%d_%d = ld(cB + %d, cC + %d);" % (b_, c, b_, c))
+                w.line("const T dbc_%d_%d = ld(cB + %d, cC + %d);" % (b_, c, b_, c))
         for a_ in range(NA):
             for d in ds_:
                 sm = " + ".join("%s * dbc_%d_%d" % (Iv(a_, b_, k), b_, c)
@@ -589,7 +491,7 @@ def gen_class(la, lb, lc, ld, prec):
         # K_bc += sum_ad I D[a,d]
         for a_ in range(NA):
             for d in ds_:
-                w.line("const double dad_%d_%d = ld(cA + %d, cD + %d);" % (a_, d, a_, d))
+                w.line("const T dad_%d_%d = ld(cA + %d, cD + %d);" % (a_, d, a_, d))
         for b_ in range(NB):
             for c in cs_:
                 sm = " + ".join("%s * dad_%d_%d" % (Iv(a_, b_, k), a_, d)
@@ -602,13 +504,6 @@ def gen_class(la, lb, lc, ld, prec):
     if nchunk > 1:
         w.close("}")
     w.close("}")  # digest
-    # bra groups for the light classes whose bra starts with an s shell: their
-    # per-lane sums (J_cd, K_ac, K_ad) stay small; for p/d first shells the
-    # extra registers spill and measured slower
-    grouped = mirror and la == 0
-    w.line("static constexpr bool GROUPED = %s;" % ("true" if grouped else "false"))
-    if grouped:
-        emit_digest_g(w, A, B, Cc, Dd)
     w.close("};")
     return "\n".join(w.lines), name
 
