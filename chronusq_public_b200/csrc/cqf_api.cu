@@ -428,6 +428,8 @@ __global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double*
         r.PB[x] = r.P[x] - B.O[x];
       }
       r.o2p = 0.5 / r.p;
+      r.ia = ia;
+      r.ib = jb;
       pp[idx] = r;
     }
 }
@@ -456,6 +458,36 @@ __global__ void reorder_pp_kernel(const PrimPairDev* __restrict__ in, const Pair
   for (int k = 0; k < P.npp; k++) out[P.pp_off + k] = in[src[i] + k];
 }
 
+__global__ void fill_kernel(double* __restrict__ x, long long n, double v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+// Each pair's primitive pairs in descending order of their primitive
+// Schwarz bound (insertion sort, one thread per pair), so that the class
+// kernels' primitive loops can stop at the first pair below the screen.
+__global__ void sort_pp_kernel(const PairDev* __restrict__ pairs, int n, PrimPairDev* pp,
+                               double* ppQ) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const PairDev P = pairs[i];
+  PrimPairDev* r = pp + P.pp_off;
+  double* q = ppQ + P.pp_off;
+  for (int k = 1; k < P.npp; k++) {
+    const PrimPairDev rk = r[k];
+    const double qk = q[k];
+    int j = k - 1;
+    while (j >= 0 && q[j] < qk) {
+      r[j + 1] = r[j];
+      q[j + 1] = q[j];
+      j--;
+    }
+    r[j + 1] = rk;
+    q[j + 1] = qk;
+  }
+}
+
 // FP32 range data of each pair: log2 of 2 max p and of max |Kp| over its
 // primitive pairs (fp32_range_ok).
 __global__ void pair_range_kernel(const PrimPairDev* __restrict__ pp, const PairDev* pairs,
@@ -476,7 +508,8 @@ __global__ void pair_range_kernel(const PrimPairDev* __restrict__ pp, const Pair
 // l = thread; field f of primitive iq of lane l at
 // out[tileOff[t] + (iq * KETT_NF + f) * KETT_TILE + l], zero past the pair's
 // primitives, for iq below the tile's largest primitive count.
-__global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp, const PairDev* pairs,
+__global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp,
+                                 const double* __restrict__ ppQ, const PairDev* pairs,
                                  const int* __restrict__ tileFirst,
                                  const int* __restrict__ tileCnt,
                                  const long long* __restrict__ tileOff, double* out) {
@@ -500,6 +533,7 @@ __global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp, const PairD
         f[6 + x] = r.PA[x];
         f[9 + x] = r.PB[x];
       }
+      f[12] = ppQ[off + iq];
     } else {
       for (int k = 0; k < KETT_NF; k++) f[k] = 0.0;
     }
@@ -734,6 +768,7 @@ void free_basis(cqf_basis* B) {
   if (B->stream) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
+                    (void*)B->d_ppQ,
                     (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_pairRange,
                     (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
@@ -1037,6 +1072,22 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     cudaFreeAsync(B->d_pp, B->stream);
     cudaFreeAsync(d_src, B->stream);
     B->d_pp = d_pp2;
+    // primitive Schwarz bounds (the generated classes; others keep an
+    // unscreened bound), then each pair's primitive pairs sorted by them
+    CQF_CUDA(cudaMallocAsync(&B->d_ppQ, std::max<long long>(1, ppoff) * sizeof(double),
+                             B->stream));
+    fill_kernel<<<(unsigned)std::min<long long>(grid1(std::max<long long>(1, ppoff), 256), 4096),
+                  256, 0, B->stream>>>(B->d_ppQ, std::max<long long>(1, ppoff), 1e300);
+    for (int c = 0; c < NCLS; c++) {
+      int la, lb;
+      class_ls(c, la, lb);
+      if (la <= 2)
+        launch_prim_schwarz(la, lb, B->d_pairs, B->d_pp, B->d_boys64, B->cls_beg[c],
+                            B->cls_cnt[c], B->d_ppQ, B->stream);
+    }
+    sort_pp_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_pairs, B->npair, B->d_pp,
+                                                                B->d_ppQ);
+    CQF_CUDA(cudaGetLastError());
     // the same data tile-interleaved for the class kernels' kets: per ket
     // tile (KETT_TILE consecutive pairs of a class), field-major runs of
     // KETT_TILE values for each primitive (zero past a pair's npp)
@@ -1065,8 +1116,8 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
       int *d_tf = nullptr, *d_tc = nullptr;
       CQF_TRY(upload(&d_tf, tfirst, B->stream));
       CQF_TRY(upload(&d_tc, tcnt, B->stream));
-      ket_tiles_kernel<<<ntile, KETT_TILE, 0, B->stream>>>(B->d_pp, B->d_pairs, d_tf, d_tc,
-                                                           B->d_tileOff, B->d_ketT);
+      ket_tiles_kernel<<<ntile, KETT_TILE, 0, B->stream>>>(B->d_pp, B->d_ppQ, B->d_pairs, d_tf,
+                                                           d_tc, B->d_tileOff, B->d_ketT);
       cudaFreeAsync(d_tf, B->stream);
       cudaFreeAsync(d_tc, B->stream);
     }
@@ -1541,6 +1592,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   JKLaunch a{};
   a.pairs = B->d_pairs;
   a.pp = B->d_pp;
+  a.ppQ = B->d_ppQ;
+  a.primK4 = std::pow((double)B->maxPrim, 4);
   a.boys64 = B->d_boys64;
   a.boys32 = B->d_boys32;
   a.screen = opts.screen;

@@ -6,8 +6,10 @@
 //                          src/basisset/basisset.cxx:652-706), grouped into
 //                          angular-momentum classes (lA >= lB) and sorted by
 //                          Schwarz bound (descending) inside each class
-//   PrimPairDev[nprimpair] primitive-pair data (p, K/p, 1/2p, P, PA, PB),
-//                          96 B each, contiguous per shell pair; the same
+//   PrimPairDev[nprimpair] primitive-pair data (p, K/p, 1/2p, P, PA, PB,
+//                          primitive indices), 112 B each, contiguous per
+//                          shell pair in descending order of the primitive
+//                          Schwarz bound (ppQ[nprimpair]); the same
 //                          data tile-interleaved (field-major runs of 128
 //                          kets) for the class kernels' per-lane ket loads
 //   bra groups             per class a bra order by first shell, cut into
@@ -98,6 +100,7 @@ struct __align__(16) PrimPairDev {
   double p, Kp;      // exponent sum; c_a c_b exp(-mu |AB|^2) / p
   double P[3], PA[3], PB[3];
   double o2p;        // 1 / (2p)
+  int ia, ib;        // primitive indices within shells shA and shB
 };
 
 // FP32 range guard of the mixed path.  The Hermite recursion starts from

@@ -23,10 +23,10 @@ inline void class_ls(int c, int& la, int& lb) {
 // Per-matrix flags packed for the kernels: bit0 HER, bit1 EXCHANGE.
 constexpr int MAXMAT = 512;
 
-// Tile-interleaved ket primitive data: fields p, Kp, o2p, P[3], PA[3], PB[3]
-// of KETT_TILE consecutive kets of a class (one persistent-kernel ket tile).
+// Tile-interleaved ket primitive data: fields p, Kp, o2p, P[3], PA[3], PB[3],
+// Qp (primitive Schwarz bound) of KETT_TILE consecutive kets of a class.
 constexpr int NAUX = 2;           // auxiliary streams of the class-quartet launches
-constexpr int KETT_NF = 12;
+constexpr int KETT_NF = 13;
 constexpr int KETT_TILE = 128;
 
 // Arguments of one class-quartet J/K launch.
@@ -56,6 +56,8 @@ struct JKLaunch {
   const long long* tileOff;
   int braTileBeg, ketTileBeg;
   const float* Xc32;        // FP32 copy of Xc (mixed builds, FP32 class kernels)
+  const double* ppQ;        // primitive Schwarz bound of each primitive pair
+  double primK4;            // (largest contraction length)^4 of the basis
   int lsum;                 // la + lb + lc + ld of the launch's class
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
@@ -173,6 +175,7 @@ struct cqf_basis {
   double* d_prim = nullptr;              // alpha | coeff
   cqf::PairDev* d_pairs = nullptr;
   cqf::PrimPairDev* d_pp = nullptr;
+  double* d_ppQ = nullptr;               // primitive Schwarz bounds (pp order)
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
   float2* d_pairRange = nullptr;         // per pair: FP32 range data

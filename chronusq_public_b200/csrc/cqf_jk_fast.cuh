@@ -35,6 +35,8 @@ __device__ __forceinline__ void warp_sum(T (&v)[N]) {
 // each field of primitive iq contiguous (a warp's load is one coalesced run).
 struct KetAoS {
   const PrimPairDev* b;
+  const double* q;  // primitive Schwarz bounds of the same pairs (read only when screening)
+  __device__ __forceinline__ double Qp(int iq) const { return q[iq]; }
   __device__ __forceinline__ double p(int iq) const { return b[iq].p; }
   __device__ __forceinline__ double Kp(int iq) const { return b[iq].Kp; }
   __device__ __forceinline__ double o2p(int iq) const { return b[iq].o2p; }
@@ -53,6 +55,7 @@ struct KetSoA {
   __device__ __forceinline__ double P(int iq, int x) const { return f(iq, 3 + x); }
   __device__ __forceinline__ double PA(int iq, int x) const { return f(iq, 6 + x); }
   __device__ __forceinline__ double PB(int iq, int x) const { return f(iq, 9 + x); }
+  __device__ __forceinline__ double Qp(int iq) const { return f(iq, 12); }
 };
 
 // Rows of the Boys tables for angular sum L (global memory).
@@ -223,6 +226,11 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
   const int nItems = (nEntries + entriesPerItem - 1) / entriesPerItem * NCH;
   const size_t nc = a.ncart;
   const size_t matStride = (size_t)a.ncart * a.ncart;
+  // primitive screen threshold: libint's engine precision as the reference
+  // sets it, max(eps_double, tau / (max shell-block norm x K^4)), K the
+  // largest contraction length (direct.hpp:1563-1589)
+  const double peps =
+      a.screen ? fmax(2.220446049250313e-16, a.thresh / (__ldg(a.maxNorm) * a.primK4)) : 0.0;
   // entry e of the list: (word index, this precision's mask of it)
   auto entry = [&](int e) {
     const int w = __ldg(list + e);
@@ -280,7 +288,7 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
       const int jkc = work_ ? jk : 0;
       const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jkc / KETT_TILE) + jkc % KETT_TILE};
       T I[G::NI];
-      G::eri(P, Q, a.pp, kq, boys, ch, I);
+      G::eri(P, Q, a.pp, kq, boys, ch, I, a.ppQ, peps);
 #pragma unroll 1
       for (int mt = 0; mt < a.nMat; mt++) {
         const int fl = __ldg(a.flags + mt);
@@ -402,8 +410,8 @@ __global__ void __launch_bounds__(JK_THREADS)
   auto ta = [&](int c, int mu) { return A.pure ? TA[c * nsph(GC::LA) + mu] : (c == mu ? 1.0 : 0.0); };
   auto tb = [&](int c, int nu) { return B.pure ? TB[c * nsph(GC::LB) + nu] : (c == nu ? 1.0 : 0.0); };
   double I[GC::NI];
-  GC::eri(P, P, pp, KetAoS{pp + P.pp_off},
-                           boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I);
+  GC::eri(P, P, pp, KetAoS{pp + P.pp_off, nullptr},
+                           boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I, nullptr, 0.0);
   for (int mu = 0; mu < na; mu++)
     for (int nu = 0; nu < nb; nu++) {
       double s = 0.0;
@@ -479,6 +487,59 @@ inline bool launch_schwarz_fast(int la, int lb, const PairDev* pairs, const Prim
   if (!done && A_ == la && B_ == lb && C_ == la && D_ == lb) go(N64{});
   CQF_GEN_JK_CLASSES(CQF_TRY_SCHWARZ)
 #undef CQF_TRY_SCHWARZ
+  return done;
+}
+
+// Primitive Schwarz bounds of the pairs of one class (LA, LB <= 2):
+// Qp = sqrt(max over Cartesian components |(ab|ab)|) of each primitive pair
+// alone (contraction coefficients included; the integrals the class kernels
+// form), one thread per pair.  They bound each primitive quartet's integrals
+// by Qp_ab Qp_cd (Cauchy-Schwarz), the primitive screen's estimate.
+template <class GC>
+__global__ void prim_schwarz_kernel(const PairDev* __restrict__ pairs,
+                                    const PrimPairDev* __restrict__ pp,
+                                    const double* __restrict__ boys, int beg, int n,
+                                    double* __restrict__ ppQ) {
+  constexpr int NA = ncart(GC::LA), NB = ncart(GC::LB), NCH = GC::NCHUNK;
+  constexpr int CS = GC::NI / (NA * NB);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const PairDev P = pairs[beg + k];
+  for (int ip = 0; ip < P.npp; ip++) {
+    PairDev P1 = P;
+    P1.npp = 1;
+    P1.pp_off = P.pp_off + ip;
+    double mx = 0.0;
+    for (int ch = 0; ch < NCH; ch++) {
+      double I[GC::NI];
+      GC::eri(P1, P1, pp, KetAoS{pp + P1.pp_off, nullptr},
+              boys + (size_t)(2 * (GC::LA + GC::LB)) * BOYS_NPTS * BOYS_ROW64, ch, I, nullptr,
+              0.0);
+      for (int kk = 0; kk < CS; kk++) {
+        const int cd = ch * CS + kk;  // the diagonal element (ab | ab), ab = cd
+        if (cd < NA * NB) mx = fmax(mx, fabs(I[cd * CS + kk]));
+      }
+    }
+    ppQ[P.pp_off + ip] = sqrt(mx);
+  }
+}
+
+// Primitive Schwarz bounds of one class with the generated code; false if
+// the class has none.
+inline bool launch_prim_schwarz(int la, int lb, const PairDev* pairs, const PrimPairDev* pp,
+                                const double* boys, int beg, int n, double* ppQ,
+                                cudaStream_t st) {
+  if (n <= 0) return true;
+  bool done = false;
+  auto go = [&](auto tag64) {
+    using G = decltype(tag64);
+    prim_schwarz_kernel<G><<<(n + 63) / 64, 64, 0, st>>>(pairs, pp, boys, beg, n, ppQ);
+    done = true;
+  };
+#define CQF_TRY_PRIM(A_, B_, C_, D_, N64, N32) \
+  if (!done && A_ == la && B_ == lb && C_ == la && D_ == lb) go(N64{});
+  CQF_GEN_JK_CLASSES(CQF_TRY_PRIM)
+#undef CQF_TRY_PRIM
   return done;
 }
 

@@ -187,13 +187,13 @@ __device__ __forceinline__ void op_of(int mu, int nu, int& op, double& sg) {
   }
 }
 
-// exponents of primitive pair ip of pair P (prim_pairs_kernel order: first
-// shell's primitive outer)
+// exponents of the two primitives of primitive pair r (its primitive
+// indices within shells SA and SB)
 __device__ __forceinline__ void pair_exps(const ShellDev& SA, const ShellDev& SB,
-                                          const double* __restrict__ prim, int ip, double& ea,
-                                          double& eb) {
-  ea = __ldg(prim + SA.prim_off + ip / SB.nprim);
-  eb = __ldg(prim + SB.prim_off + ip % SB.nprim);
+                                          const double* __restrict__ prim,
+                                          const PrimPairDev& r, double& ea, double& eb) {
+  ea = __ldg(prim + SA.prim_off + r.ia);
+  eb = __ldg(prim + SB.prim_off + r.ib);
 }
 
 constexpr double PI52X2 = 34.986836655249725693;  // 2 pi^(5/2)
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(REL_THREADS)
       for (int ip = 0; ip < P.npp; ip++) {
         const PrimPairDev& A = a.pp[P.pp_off + ip];
         double ea, eb;
-        pair_exps(SA, SB, a.prim, ip, ea, eb);
+        pair_exps(SA, SB, a.prim, A, ea, eb);
 #pragma unroll 1
         for (int x = 0; x < 3; x++)
           hermite_E_rt<T, LM + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[x]), T(A.PB[x]), Ea[x]);
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(REL_THREADS)
         for (int iq = 0; iq < Q.npp; iq++) {
           const PrimPairDev& B = a.pp[Q.pp_off + iq];
           double ec, ed;
-          pair_exps(SC, SD, a.prim, iq, ec, ed);
+          pair_exps(SC, SD, a.prim, B, ec, ed);
           const T q = T(B.p);
 #pragma unroll 1
           for (int x = 0; x < 3; x++)
@@ -708,8 +708,8 @@ __global__ void __launch_bounds__(RB_THREADS)
     const PrimPairDev& A = a.pp[P.pp_off + ip];
     const PrimPairDev& B = a.pp[Q.pp_off + iq];
     double ea, eb;
-    pair_exps(SA, SB, a.prim, ip, ea, eb);
-    pair_exps(SC, SD, a.prim, iq, ec, ed);
+    pair_exps(SA, SB, a.prim, A, ea, eb);
+    pair_exps(SC, SD, a.prim, B, ec, ed);
     if (tid < 3)
       hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
                                 Eb + tid * E1b);
@@ -976,8 +976,8 @@ __global__ void __launch_bounds__(RB_THREADS)
       const PrimPairDev& A = a.pp[P.pp_off + ip];
       const PrimPairDev& B = a.pp[Q.pp_off + iq];
       double ea, eb, ec, ed;
-      pair_exps(SA, SB, a.prim, ip, ea, eb);
-      pair_exps(SC, SD, a.prim, iq, ec, ed);
+      pair_exps(SA, SB, a.prim, A, ea, eb);
+      pair_exps(SC, SD, a.prim, B, ec, ed);
       __syncthreads();  // the previous primitive quartet's readers are done
       if (tid < 3)
         hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
@@ -1196,14 +1196,14 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
   for (int ip = 0; ip < P.npp; ip++) {
     const PrimPairDev& A = pp[P.pp_off + ip];
     double ea, eb;
-    pair_exps(SA, SB, prim, ip, ea, eb);
+    pair_exps(SA, SB, prim, A, ea, eb);
     for (int x = 0; x < 3; x++)
       hermite_E_rt<double, LM + 1>(la + rb, lb + rb, A.o2p, A.PA[x], A.PB[x], Ea[x]);
     for (int h = 0; h < nherm(Lb); h++) G[h] = 0.0;
     for (int iq = 0; iq < Q.npp; iq++) {
       const PrimPairDev& B = pp[Q.pp_off + iq];
       double ec, ed;
-      pair_exps(SC, SD, prim, iq, ec, ed);
+      pair_exps(SC, SD, prim, B, ec, ed);
       for (int x = 0; x < 3; x++)
         hermite_E_rt<double, LM + 1>(lc + rk, ld + rk, B.o2p, B.PA[x], B.PB[x], Ec[x]);
       const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];

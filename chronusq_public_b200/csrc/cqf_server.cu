@@ -228,8 +228,17 @@ unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell) {
     maxp = std::max<unsigned long long>(maxp, (unsigned long long)std::max(0, shells[s].nprim));
   }
   const unsigned long long ns = nshell, npair = ns * (ns + 1) / 2, nmat = 2;
-  const unsigned long long pairs = npair * (64 + 96 * maxp * maxp) + ns * ns * 8 + 300000;
-  const unsigned long long ws = 8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns);
+  // per pair: its record; per primitive pair: the record (112 B), its
+  // Schwarz bound and the tile-interleaved ket copy (13 doubles)
+  const unsigned long long pairs =
+      npair * (64 + (112 + 8 + 104) * maxp * maxp) + ns * ns * 8 + 300000;
+  // workspace: densities and accumulators (spherical, Cartesian, FP32
+  // copy), norms, and the class kernels' quartet masks and word lists
+  // (16 B per 32 unique quartets of pairs, plus one word per pair and class)
+  const unsigned long long masks = 16 * (npair * ((npair + 31) / 32) / 2 + 28 * npair);
+  const unsigned long long ws =
+      8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns) + 4 * nmat * nc * nc +
+      masks;
   return pairs + ws;
 }
 

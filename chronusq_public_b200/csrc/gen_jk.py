@@ -204,8 +204,11 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS, prec):
     w.line("#pragma unroll")
     w.line("for (int i = 0; i < %d; i++) I[i] = 0.0;" % (NA * NB * CS))
     w.line("const T PI52x2 = T(34.986836655249725693);")
+    w.line("const double qbMax = eps > 0.0 ? __ldg(ppQ + P.pp_off) : 0.0;")
     w.line("#pragma unroll 1")
     w.open("for (int iq = 0; iq < Q.npp; iq++) {")
+    w.line("const double qk = eps > 0.0 ? kq.Qp(iq) : 0.0;")
+    w.line("if (qk * qbMax < eps) break;")
     w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
     w.line("const T Qx = T(kq.P(iq, 0)), Qy = T(kq.P(iq, 1)), Qz = T(kq.P(iq, 2));")
     if lcd > 0:
@@ -220,6 +223,7 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS, prec):
                 w.line("T h_%d_%d_%d_%d_%d = T(0);" % (ia, ib, t, u, v))
     w.line("#pragma unroll 1")
     w.open("for (int ip = 0; ip < P.npp; ip++) {")
+    w.line("if (eps > 0.0 && __ldg(ppQ + P.pp_off + ip) * qk < eps) break;")
     w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
     w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
     w.line("const T X = T(pa.P[0]) - Qx, Y = T(pa.P[1]) - Qy, Z = T(pa.P[2]) - Qz;")
@@ -325,17 +329,25 @@ def gen_class(la, lb, lc, ld, prec):
     w.line("static constexpr int MINB = %d;" % minb)
     # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
     w.line("template <class KA>")
+    # primitive screen (the reference's engine precision, direct.hpp:1563-1589):
+    # primitive quartets with Qp_ab Qp_cd < eps are skipped; a pair's
+    # primitive pairs are sorted by Qp (descending), so a loop stops at the
+    # first one below the bound.  eps = 0 computes every primitive quartet.
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
            "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
-           "const int ch, T (&I)[%d]) {" % (NAB * CS))
+           "const int ch, T (&I)[%d], const double* __restrict__ ppQ, const double eps) {"
+           % (NAB * CS))
     if mirror:
         emit_eri_mirror(w, la, lb, lc, ld, CS, prec)
     else:
         w.line("#pragma unroll")
         w.line("for (int i = 0; i < %d; i++) I[i] = T(0);" % (NAB * CS))
         w.line("const T PI52x2 = T(34.986836655249725693);")
+        w.line("const double qkMax = eps > 0.0 && Q.npp > 0 ? kq.Qp(0) : 0.0;")
         w.line("#pragma unroll 1")
         w.open("for (int ip = 0; ip < P.npp; ip++) {")
+        w.line("const double qb = eps > 0.0 ? __ldg(ppQ + P.pp_off + ip) : 0.0;")
+        w.line("if (qb * qkMax < eps) break;")
         w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
         w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
         w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
@@ -348,6 +360,7 @@ def gen_class(la, lb, lc, ld, prec):
                 w.line("T g_%d_%d_%d_%d = T(0);" % (k, t, u, v))
         w.line("#pragma unroll 1")
         w.open("for (int iq = 0; iq < Q.npp; iq++) {")
+        w.line("if (eps > 0.0 && qb * kq.Qp(iq) < eps) break;")
         w.line("const T q = T(kq.p(iq)), Kcd = T(kq.Kp(iq)), o2q = T(kq.o2p(iq));")
         w.line("const T X = Px - T(kq.P(iq, 0)), Y = Py - T(kq.P(iq, 1)), Z = Pz - T(kq.P(iq, 2));")
         emit_boys(w, L, prec)

@@ -310,7 +310,9 @@ typedef struct {
 
 /* Device bytes a request of this basis is charged for: shell-pair data
  * (upper bound: every pair significant, every pair with the largest
- * primitive count) plus the contraction workspace of one J and one K. */
+ * primitive count) plus the contraction workspace of one J and one K
+ * (densities and accumulators, norms, and the class kernels' quartet masks
+ * and word lists, 16 B per 32 unique quartets of pairs). */
 unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell);
 
 cqf_status cqf_server_create(const cqf_server_opts* opts, cqf_server** out);
