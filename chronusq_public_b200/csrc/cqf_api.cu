@@ -434,11 +434,16 @@ __global__ void prim_pairs_kernel(const ShellDev* __restrict__ sh, const double*
     }
 }
 
+// Sort key of a pair: class, then primitive-pair count (descending: pairs
+// of one contraction length sit together, so a warp's lanes run primitive
+// loops of one length), then Schwarz bound (descending).
 __global__ void sort_keys_kernel(const PairDev* pairs, int n, unsigned long long* keys, int* vals) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   unsigned long long qb = (unsigned long long)__double_as_longlong(pairs[k].Q);  // Q >= 0
-  keys[k] = ((unsigned long long)pairs[k].cls << 56) | ((~qb >> 8) & ((1ull << 56) - 1));
+  const unsigned long long np = 255u - (unsigned)min(pairs[k].npp, 255);
+  keys[k] = ((unsigned long long)pairs[k].cls << 56) | (np << 48) |
+            ((~qb >> 16) & ((1ull << 48) - 1));
   vals[k] = k;
 }
 
@@ -448,7 +453,7 @@ __global__ void gather_pairs_kernel(const PairDev* in, const int* idx, int n, Pa
 }
 
 // Primitive pairs of pair i moved from src[i] to pairs[i].pp_off (the order
-// of the Schwarz-sorted pair list); one thread per pair.
+// of the sorted pair list); one thread per pair.
 __global__ void reorder_pp_kernel(const PrimPairDev* __restrict__ in, const PairDev* pairs,
                                   const long long* __restrict__ src, int n,
                                   PrimPairDev* __restrict__ out) {
@@ -768,7 +773,7 @@ void free_basis(cqf_basis* B) {
   if (B->stream) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
-                    (void*)B->d_ppQ,
+                    (void*)B->d_ppQ, (void*)B->d_qWin,
                     (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_pairRange,
                     (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
@@ -1049,6 +1054,19 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   CQF_CUDA(cudaMemcpyAsync(B->h_pairs.data(), B->d_pairs, B->npair * sizeof(PairDev),
                            cudaMemcpyDeviceToHost, B->stream));
   CQF_CUDA(cudaStreamSynchronize(B->stream));
+  {
+    // largest Schwarz bound over each window of WTILE pairs starting at a
+    // pair, inside its class: the tile-level screens' bound (pairs are not
+    // in Schwarz order across contraction lengths)
+    std::vector<double> qw(std::max(1, B->npair));
+    for (int i = B->npair - 1; i >= 0; i--) {
+      double m = B->h_pairs[i].Q;
+      for (int j = i + 1; j < std::min(B->npair, i + WTILE); j++)
+        if (B->h_pairs[j].cls == B->h_pairs[i].cls) m = std::max(m, B->h_pairs[j].Q);
+      qw[i] = m;
+    }
+    CQF_TRY(upload(&B->d_qWin, qw, B->stream));
+  }
   // primitive pairs in the same order as the sorted pairs: the primitives of
   // consecutive kets of a tile are one contiguous run (moved on the device;
   // only the per-pair offsets cross to the host and back)
@@ -1593,6 +1611,7 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.pairs = B->d_pairs;
   a.pp = B->d_pp;
   a.ppQ = B->d_ppQ;
+  a.qWin = B->d_qWin;
   a.primK4 = std::pow((double)B->maxPrim, 4);
   a.boys64 = B->d_boys64;
   a.boys32 = B->d_boys32;

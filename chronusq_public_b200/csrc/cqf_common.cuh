@@ -4,8 +4,9 @@
 //   ShellDev[nshell]       shell metadata (l, pure, primitive/AO offsets, centre)
 //   PairDev[npair]         significant shell pairs (ShellPairData semantics,
 //                          src/basisset/basisset.cxx:652-706), grouped into
-//                          angular-momentum classes (lA >= lB) and sorted by
-//                          Schwarz bound (descending) inside each class
+//                          angular-momentum classes (lA >= lB), inside each
+//                          class sorted by primitive-pair count, then by
+//                          Schwarz bound (both descending)
 //   PrimPairDev[nprimpair] primitive-pair data (p, K/p, 1/2p, P, PA, PB,
 //                          primitive indices), 112 B each, contiguous per
 //                          shell pair in descending order of the primitive

@@ -28,6 +28,7 @@ constexpr int MAXMAT = 512;
 constexpr int NAUX = 2;           // auxiliary streams of the class-quartet launches
 constexpr int KETT_NF = 13;
 constexpr int KETT_TILE = 128;
+constexpr int WTILE = 32;         // kets per mask word of the class kernels
 
 // Arguments of one class-quartet J/K launch.
 struct JKLaunch {
@@ -57,6 +58,7 @@ struct JKLaunch {
   int braTileBeg, ketTileBeg;
   const float* Xc32;        // FP32 copy of Xc (mixed builds, FP32 class kernels)
   const double* ppQ;        // primitive Schwarz bound of each primitive pair
+  const double* qWin;       // per pair: largest Q of the WTILE pairs from it (same class)
   double primK4;            // (largest contraction length)^4 of the basis
   int lsum;                 // la + lb + lc + ld of the launch's class
   int precision;            // 0 FP64, 1 mixed
@@ -159,7 +161,7 @@ struct cqf_basis {
   long long nprimpair = 0;
   double thresh = 1e-12;
   std::vector<cqf::ShellDev> h_shells;
-  std::vector<cqf::PairDev> h_pairs;     // final (class, Q-sorted) order
+  std::vector<cqf::PairDev> h_pairs;     // final (class, npp, Q) order
   int cls_beg[cqf::NCLS] = {0}, cls_cnt[cqf::NCLS] = {0};
   // launch shape of each class pair's persistent kernel: resident blocks per
   // SM requested (8 by default; cqf_autotune measures and sets it)
@@ -176,6 +178,7 @@ struct cqf_basis {
   cqf::PairDev* d_pairs = nullptr;
   cqf::PrimPairDev* d_pp = nullptr;
   double* d_ppQ = nullptr;               // primitive Schwarz bounds (pp order)
+  double* d_qWin = nullptr;              // per pair: window maximum of Q (tile screens)
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
   float2* d_pairRange = nullptr;         // per pair: FP32 range data

@@ -70,7 +70,6 @@ __device__ __forceinline__ const float* boys_rows<float>(const JKLaunch& a, int 
   return a.boys32 + (size_t)L * BOYS_NPTS * BOYS_ROW32;
 }
 
-constexpr int WTILE = 32;  // kets per mask word (one warp's worth)
 
 // Shell-block norm maximum of a quartet in the reference's roles
 // (direct.hpp:1693-1736), with the warp-uniform bra pair P: the pair norms
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(256)
         const int jk = tile * WTILE + lane;
         const PairDev P = a.pairs[a.braBeg + ib];
         const bool visited = jk < a.nKet && !(a.same && jk > ib);
-        const double tileMax = __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + tile * WTILE].Q;
+        const double tileMax = __ldg(a.maxNorm) * P.Q * __ldg(a.qWin + a.ketBeg + tile * WTILE);
         bool screened = false, w32 = false;
         if (a.screen && tileMax < a.thresh) {
           screened = true;
@@ -199,8 +198,9 @@ __device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
 
 // Class kernel of one shell-quartet class in one precision (G = GenJK64_x
 // or GenJK32_x; FP32 = which mask half and word list it uses).  A work item
-// is (run of entriesPerItem consecutive entries of the precision's word
-// list, ket component chunk), handed out by a device counter.  A warp walks
+// is (run of consecutive entries of the precision's word list -- sized from
+// the list's length, at most entriesPerItem -- ket component chunk), handed
+// out by a device counter.  A warp walks
 // its run's words and packs the quartets they name into batches of 32 lanes
 // (nth_set_bit), so every lane of a batch computes a surviving quartet; a
 // batch may span two bra pairs.  The batch's integrals of the chunk come
@@ -223,7 +223,12 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
   const int lane = threadIdx.x & 31;
   const int nTiles = (a.nKet + WTILE - 1) / WTILE;
   const int nEntries = (int)*lcount;  // written by the planning pass
-  const int nItems = (nEntries + entriesPerItem - 1) / entriesPerItem * NCH;
+  // entries per item from the list's actual length: about four items per
+  // warp of the grid, at most entriesPerItem entries
+  const int gridWarps = (int)(gridDim.x * (blockDim.x / 32));
+  const int epi = max(1, min(entriesPerItem, (int)((long long)nEntries * NCH /
+                                                   (4LL * gridWarps))));
+  const int nItems = (nEntries + epi - 1) / epi * NCH;
   const size_t nc = a.ncart;
   const size_t matStride = (size_t)a.ncart * a.ncart;
   // primitive screen threshold: libint's engine precision as the reference
@@ -243,8 +248,8 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
     const int item = (int)__shfl_sync(0xffffffffu, itemU, 0);
     if (item >= nItems) break;
     const int run = item / NCH, ch = item - run * NCH;
-    int e = run * entriesPerItem;
-    const int eEnd = min(e + entriesPerItem, nEntries);
+    int e = run * epi;
+    const int eEnd = min(e + epi, nEntries);
     int2 wm = entry(e);
     unsigned m = (unsigned)wm.y;
     for (;;) {
@@ -324,12 +329,11 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
   }
 }
 
-// Word-list entries per work item of a class kernel: about 256 items per SM
-// over the class pair's words (an upper bound of the non-empty ones) and
-// its chunks, at most 64 entries.
+// Upper limit of word-list entries per work item of a class kernel (the
+// kernel sizes its items from the list's actual length).
 inline int entries_per_item(long long nWords, int nchunk, int nsm) {
   const long long per = nWords * nchunk / ((long long)nsm * 256);
-  return (int)std::min<long long>(64, std::max<long long>(1, per));
+  return (int)std::min<long long>(64, std::max<long long>(4, per));
 }
 
 // Launches the planning pass and the generated class kernels of the class

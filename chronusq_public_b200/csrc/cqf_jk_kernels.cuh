@@ -163,9 +163,12 @@ __global__ void __launch_bounds__(JK_THREADS)
     Q = a.pairs[a.ketBeg + jk];
     visited = true;
   }
-  // tile-level screen: kets are sorted by Q (descending) inside the class
-  const bool tileDead = a.screen &&
-      __ldg(a.maxNorm) * P.Q * a.pairs[a.ketBeg + blockIdx.y * JK_THREADS].Q < a.thresh;
+  // tile-level screen: the largest Q of the block's kets (window maxima)
+  double tq = 0.0;
+  for (int k = blockIdx.y * JK_THREADS; k < min((int)(blockIdx.y + 1) * JK_THREADS, a.nKet);
+       k += WTILE)
+    tq = fmax(tq, __ldg(a.qWin + a.ketBeg + k));
+  const bool tileDead = a.screen && __ldg(a.maxNorm) * P.Q * tq < a.thresh;
   if (tileDead) {
     count_block(a.counters, visited, visited, false, false);
     return;
