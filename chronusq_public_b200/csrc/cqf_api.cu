@@ -469,6 +469,24 @@ __global__ void fill_kernel(double* __restrict__ x, long long n, double v) {
     x[i] = v;
 }
 
+// FP32 copy of the primitive-pair records.
+__global__ void pp32_kernel(const PrimPairDev* __restrict__ pp, long long n, PrimPair32* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const PrimPairDev r = pp[i];
+    PrimPair32 o;
+    o.p = (float)r.p;
+    o.Kp = (float)r.Kp;
+    o.o2p = (float)r.o2p;
+    for (int x = 0; x < 3; x++) {
+      o.P[x] = (float)r.P[x];
+      o.PA[x] = (float)r.PA[x];
+      o.PB[x] = (float)r.PB[x];
+    }
+    out[i] = o;
+  }
+}
+
 // Each pair's primitive pairs in descending order of their primitive
 // Schwarz bound (insertion sort, one thread per pair), so that the class
 // kernels' primitive loops can stop at the first pair below the screen.
@@ -517,7 +535,8 @@ __global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp,
                                  const double* __restrict__ ppQ, const PairDev* pairs,
                                  const int* __restrict__ tileFirst,
                                  const int* __restrict__ tileCnt,
-                                 const long long* __restrict__ tileOff, double* out) {
+                                 const long long* __restrict__ tileOff, double* out,
+                                 float* out32) {
   const int t = blockIdx.x, l = threadIdx.x;
   const long long base = tileOff[t];
   const int mx = (int)((tileOff[t + 1] - base) / (KETT_NF * KETT_TILE));
@@ -542,7 +561,11 @@ __global__ void ket_tiles_kernel(const PrimPairDev* __restrict__ pp,
     } else {
       for (int k = 0; k < KETT_NF; k++) f[k] = 0.0;
     }
-    for (int k = 0; k < KETT_NF; k++) out[base + ((long long)iq * KETT_NF + k) * KETT_TILE + l] = f[k];
+    for (int k = 0; k < KETT_NF; k++) {
+      const long long o = base + ((long long)iq * KETT_NF + k) * KETT_TILE + l;
+      out[o] = f[k];
+      out32[o] = (float)f[k];
+    }
   }
 }
 
@@ -773,7 +796,7 @@ void free_basis(cqf_basis* B) {
   if (B->stream) {
     cudaStream_t st = B->stream;
     for (void* p : {(void*)B->d_shells, (void*)B->d_prim, (void*)B->d_pairs, (void*)B->d_pp,
-                    (void*)B->d_ppQ, (void*)B->d_qWin,
+                    (void*)B->d_ppQ, (void*)B->d_qWin, (void*)B->d_pp32, (void*)B->d_ketT32,
                     (void*)B->d_ketT, (void*)B->d_tileOff, (void*)B->d_pairRange,
                     (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
@@ -1105,6 +1128,10 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     }
     sort_pp_kernel<<<grid1(B->npair, 128), 128, 0, B->stream>>>(B->d_pairs, B->npair, B->d_pp,
                                                                 B->d_ppQ);
+    CQF_CUDA(cudaMallocAsync(&B->d_pp32, std::max<long long>(1, ppoff) * sizeof(PrimPair32),
+                             B->stream));
+    pp32_kernel<<<(unsigned)std::min<long long>(grid1(std::max<long long>(1, ppoff), 256), 4096),
+                  256, 0, B->stream>>>(B->d_pp, ppoff, B->d_pp32);
     CQF_CUDA(cudaGetLastError());
     // the same data tile-interleaved for the class kernels' kets: per ket
     // tile (KETT_TILE consecutive pairs of a class), field-major runs of
@@ -1129,13 +1156,16 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
     toff.push_back(ktn);
     CQF_CUDA(cudaMallocAsync(&B->d_ketT, (size_t)(ktn + 1) * sizeof(double), B->stream));
     CQF_CUDA(cudaMemsetAsync(B->d_ketT + ktn, 0, sizeof(double), B->stream));
+    CQF_CUDA(cudaMallocAsync(&B->d_ketT32, (size_t)(ktn + 1) * sizeof(float), B->stream));
+    CQF_CUDA(cudaMemsetAsync(B->d_ketT32 + ktn, 0, sizeof(float), B->stream));
     CQF_TRY(upload(&B->d_tileOff, toff, B->stream));
     if (ntile > 0) {
       int *d_tf = nullptr, *d_tc = nullptr;
       CQF_TRY(upload(&d_tf, tfirst, B->stream));
       CQF_TRY(upload(&d_tc, tcnt, B->stream));
       ket_tiles_kernel<<<ntile, KETT_TILE, 0, B->stream>>>(B->d_pp, B->d_ppQ, B->d_pairs, d_tf,
-                                                           d_tc, B->d_tileOff, B->d_ketT);
+                                                           d_tc, B->d_tileOff, B->d_ketT,
+                                                           B->d_ketT32);
       cudaFreeAsync(d_tf, B->stream);
       cudaFreeAsync(d_tc, B->stream);
     }
@@ -1635,6 +1665,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   a.fp32_cut = opts.fp32_cutoff;
   a.counters = B->d_counters;
   a.ketT = B->d_ketT;
+  a.ketT32 = B->d_ketT32;
+  a.pp32 = B->d_pp32;
   a.tileOff = B->d_tileOff;
   // closed-shell fast path: real matrices flagged Hermitian (symmetric)
   bool fastOK = !opts.is_complex;

@@ -104,6 +104,13 @@ struct __align__(16) PrimPairDev {
   int ia, ib;        // primitive indices within shells shA and shB
 };
 
+// FP32 copy of a primitive pair's data for the FP32 class kernels.
+struct __align__(16) PrimPair32 {
+  float p, Kp;
+  float P[3], PA[3], PB[3];
+  float o2p;
+};
+
 // FP32 range guard of the mixed path.  The Hermite recursion starts from
 // R^(n)_000 = (-2 alpha)^n F_n(T), n <= L, so its intermediates reach
 // (2 alpha)^L; alpha = pq / (p + q) <= min(p, q).  Tight primitives (core

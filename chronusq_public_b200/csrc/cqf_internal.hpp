@@ -54,6 +54,8 @@ struct JKLaunch {
   // primitive iq of the ket at tile position l is
   // ketT[tileOff[ketTileBeg + tile] + (iq * KETT_NF + f) * KETT_TILE + l]
   const double* ketT;
+  const float* ketT32;      // FP32 copy of ketT (same offsets)
+  const PrimPair32* pp32;   // FP32 copy of pp
   const long long* tileOff;
   int braTileBeg, ketTileBeg;
   const float* Xc32;        // FP32 copy of Xc (mixed builds, FP32 class kernels)
@@ -180,6 +182,8 @@ struct cqf_basis {
   double* d_ppQ = nullptr;               // primitive Schwarz bounds (pp order)
   double* d_qWin = nullptr;              // per pair: window maximum of Q (tile screens)
   double* d_ketT = nullptr;              // tile-interleaved ket primitive data
+  float* d_ketT32 = nullptr;             // its FP32 copy (FP32 class kernels)
+  cqf::PrimPair32* d_pp32 = nullptr;     // FP32 copy of d_pp
   long long* d_tileOff = nullptr;        // per tile: offset into d_ketT
   float2* d_pairRange = nullptr;         // per pair: FP32 range data
   double* d_boys64 = nullptr;

@@ -44,19 +44,21 @@ struct KetAoS {
   __device__ __forceinline__ double PA(int iq, int x) const { return b[iq].PA[x]; }
   __device__ __forceinline__ double PB(int iq, int x) const { return b[iq].PB[x]; }
 };
-struct KetSoA {
-  const double* q;  // tile base + lane
-  __device__ __forceinline__ double f(int iq, int k) const {
+template <typename E>  // element type: double, or float for the FP32 copy
+struct KetSoAT {
+  const E* q;  // tile base + lane
+  __device__ __forceinline__ E f(int iq, int k) const {
     return __ldg(q + (iq * KETT_NF + k) * KETT_TILE);
   }
-  __device__ __forceinline__ double p(int iq) const { return f(iq, 0); }
-  __device__ __forceinline__ double Kp(int iq) const { return f(iq, 1); }
-  __device__ __forceinline__ double o2p(int iq) const { return f(iq, 2); }
-  __device__ __forceinline__ double P(int iq, int x) const { return f(iq, 3 + x); }
-  __device__ __forceinline__ double PA(int iq, int x) const { return f(iq, 6 + x); }
-  __device__ __forceinline__ double PB(int iq, int x) const { return f(iq, 9 + x); }
-  __device__ __forceinline__ double Qp(int iq) const { return f(iq, 12); }
+  __device__ __forceinline__ E p(int iq) const { return f(iq, 0); }
+  __device__ __forceinline__ E Kp(int iq) const { return f(iq, 1); }
+  __device__ __forceinline__ E o2p(int iq) const { return f(iq, 2); }
+  __device__ __forceinline__ E P(int iq, int x) const { return f(iq, 3 + x); }
+  __device__ __forceinline__ E PA(int iq, int x) const { return f(iq, 6 + x); }
+  __device__ __forceinline__ E PB(int iq, int x) const { return f(iq, 9 + x); }
+  __device__ __forceinline__ double Qp(int iq) const { return (double)f(iq, 12); }
 };
+using KetSoA = KetSoAT<double>;
 
 // Rows of the Boys tables for angular sum L (global memory).
 template <typename T>
@@ -291,9 +293,12 @@ __global__ void __launch_bounds__(JK_THREADS, G::MINB)
                       ((s1 == s3 && s2 == s4) ? 1 : 2));
       const T sJ = work_ ? T(0.5) * deg : T(0), sK = work_ ? T(0.25) * deg : T(0);
       const int jkc = work_ ? jk : 0;
-      const KetSoA kq{a.ketT + __ldg(a.tileOff + a.ketTileBeg + jkc / KETT_TILE) + jkc % KETT_TILE};
+      const long long ko = __ldg(a.tileOff + a.ketTileBeg + jkc / KETT_TILE) + jkc % KETT_TILE;
       T I[G::NI];
-      G::eri(P, Q, a.pp, kq, boys, ch, I, a.ppQ, peps);
+      if constexpr (FP32)  // FP32 copies of the pair data: half the load bytes
+        G::eri(P, Q, a.pp32, KetSoAT<float>{a.ketT32 + ko}, boys, ch, I, a.ppQ, peps);
+      else
+        G::eri(P, Q, a.pp, KetSoA{a.ketT + ko}, boys, ch, I, a.ppQ, peps);
 #pragma unroll 1
       for (int mt = 0; mt < a.nMat; mt++) {
         const int fl = __ldg(a.flags + mt);

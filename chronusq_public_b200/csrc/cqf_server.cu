@@ -228,10 +228,11 @@ unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell) {
     maxp = std::max<unsigned long long>(maxp, (unsigned long long)std::max(0, shells[s].nprim));
   }
   const unsigned long long ns = nshell, npair = ns * (ns + 1) / 2, nmat = 2;
-  // per pair: its record; per primitive pair: the record (112 B), its
-  // Schwarz bound and the tile-interleaved ket copy (13 doubles)
+  // per pair: its record and window bound; per primitive pair: the record
+  // (112 B) and its FP32 copy (48 B), its Schwarz bound and the
+  // tile-interleaved ket copy (13 doubles + 13 floats)
   const unsigned long long pairs =
-      npair * (64 + (112 + 8 + 104) * maxp * maxp) + ns * ns * 8 + 300000;
+      npair * (72 + (112 + 48 + 8 + 104 + 52) * maxp * maxp) + ns * ns * 8 + 300000;
   // workspace: densities and accumulators (spherical, Cartesian, FP32
   // copy), norms, and the class kernels' quartet masks and word lists
   // (16 B per 32 unique quartets of pairs, plus one word per pair and class)

@@ -224,7 +224,7 @@ def emit_eri_mirror(w, la, lb, lc, ld, CS, prec):
     w.line("#pragma unroll 1")
     w.open("for (int ip = 0; ip < P.npp; ip++) {")
     w.line("if (eps > 0.0 && __ldg(ppQ + P.pp_off + ip) * qk < eps) break;")
-    w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
+    w.line("const auto& pa = pp[P.pp_off + ip];")
     w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
     w.line("const T X = T(pa.P[0]) - Qx, Y = T(pa.P[1]) - Qy, Z = T(pa.P[2]) - Qz;")
     if lab > 0:
@@ -328,13 +328,14 @@ def gen_class(la, lb, lc, ld, prec):
     minb = 6 if L <= 1 else (4 if live <= 96 else (2 if live <= 150 else 1))
     w.line("static constexpr int MINB = %d;" % minb)
     # ket primitive data through an accessor (KetAoS / KetSoA, cqf_jk_fast.cuh)
-    w.line("template <class KA>")
+    # bra primitive records through PP: PrimPairDev (FP64) or its FP32 copy
+    w.line("template <class KA, class PP>")
     # primitive screen (the reference's engine precision, direct.hpp:1563-1589):
     # primitive quartets with Qp_ab Qp_cd < eps are skipped; a pair's
     # primitive pairs are sorted by Qp (descending), so a loop stops at the
     # first one below the bound.  eps = 0 computes every primitive quartet.
     w.open("static __device__ __forceinline__ void eri(const PairDev& P, const PairDev& Q, "
-           "const PrimPairDev* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
+           "const PP* __restrict__ pp, const KA& kq, const T* __restrict__ boys, "
            "const int ch, T (&I)[%d], const double* __restrict__ ppQ, const double eps) {"
            % (NAB * CS))
     if mirror:
@@ -348,7 +349,7 @@ def gen_class(la, lb, lc, ld, prec):
         w.open("for (int ip = 0; ip < P.npp; ip++) {")
         w.line("const double qb = eps > 0.0 ? __ldg(ppQ + P.pp_off + ip) : 0.0;")
         w.line("if (qb * qkMax < eps) break;")
-        w.line("const PrimPairDev& pa = pp[P.pp_off + ip];")
+        w.line("const auto& pa = pp[P.pp_off + ip];")
         w.line("const T p = T(pa.p), Kab = T(pa.Kp), o2p = T(pa.o2p);")
         w.line("const T Px = T(pa.P[0]), Py = T(pa.P[1]), Pz = T(pa.P[2]);")
         axes = "xyz"

@@ -125,7 +125,7 @@ def _footprint_model(basis, nmat=2):
     ns, N, nc = basis.nshell, basis.nbasis, basis.ncart
     npair = ns * (ns + 1) // 2
     kprim = basis.max_prim ** 2
-    pairs = npair * (64 + (112 + 8 + 104) * kprim) + ns * ns * 8 + 300_000
+    pairs = npair * (72 + (112 + 48 + 8 + 104 + 52) * kprim) + ns * ns * 8 + 300_000
     masks = 16 * (npair * ((npair + 31) // 32) // 2 + 28 * npair)
     ws = (8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns)
           + 4 * nmat * nc * nc + masks)
