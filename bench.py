@@ -17,12 +17,20 @@ fp64    = the same, all quartets in FP64 (the reference precision).
 cutoff_sweep = the mixed build at the configuration's cutoffs 1e-6 .. 1e-10
           (builds/s, FP32 quartets, Fock and energy error).
 complex_build = the FP64 build of a complex Hermitian density (an RT-TDDFT
-          step's), same workload.
-batched_dD_graph = (H2O)8 / cc-pVDZ, 64 dD densities per CUDA-graph launch,
-          FP64 and mixed, beside the same work one density per call in FP64
-          (mixed_batched_over_fp64_single: the batched mixed rate over it).
+          step's), same workload, with its error against the oracle.
+batched_dD_graph = config 4: (H2O)8 / cc-pVDZ, 64 dD densities per CUDA-graph
+          launch, FP64 (incremental builds stay FP64) and mixed, each with
+          its error against the oracle on two of the densities, beside the
+          same work one density per call in FP64.
+four_component_ag4 = config 3: the Ag4 four-component Dirac-Coulomb build
+          (FP64 and mixed, one timed build each, the mixed build's deviation,
+          a bounded CPU sample with the GPU's deviation from the oracle).
+serving = config 5: 2,000 Poisson-arrival requests replayed at each of
+          --serving-rates (the last above saturation), p50/p99 latency,
+          per-phase times, sampled errors against the oracle.
 Errors  = max |G - G_oracle| and |E2 - E2_oracle| against the CPU oracle
-          (FP64), computed once outside the timed region.
+          (FP64), computed once outside the timed region.  The extra
+          workloads run only with one rank.
 
 --impl reference times the reference's algorithm on the host cores: the
 C++/OpenMP restatement of directScaffoldNew in oracle/ (the reference
@@ -47,6 +55,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("Fock builds/s (mixed vs FP64, same B200) at <=1e-6 Eh Fock err; "
           "p50/p99 latency")
+# DRAM bytes of one mixed build from an ncu capture (profiles/), by workload
+TRAFFIC_BYTES = {}
 
 
 def parse():
@@ -58,11 +68,14 @@ def parse():
     ap.add_argument("--workload", default="h2o16_def2svp")
     ap.add_argument("--cutoff", type=float, default=1e-2)
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--four-comp", type=int, default=1,
+                    help="also time the Ag4 four-component build (config 3)")
     ap.add_argument("--batched", type=int, default=1,
                     help="also time the 64-density dD build as a CUDA graph")
-    ap.add_argument("--serving-requests", type=int, default=300,
+    ap.add_argument("--serving-requests", type=int, default=2000,
                     help="requests of the Poisson serving stream (0: skip)")
-    ap.add_argument("--serving-rate", type=float, default=10.0)
+    ap.add_argument("--serving-rates", type=float, nargs="+", default=[20.0, 80.0, 160.0],
+                    help="arrival rates (Hz) the stream is replayed at")
     ap.add_argument("--profile-case", default=None,
                     help="one untimed build of a named case for profiler captures "
                          "(h2o16_def2svp, h2o8_ccpvdz, ag4_dc, ag1_ssss) and exit")
@@ -150,6 +163,12 @@ def fma_peaks():
     return L.cqf_fma_peak_tflops(1, 4096), L.cqf_fma_peak_tflops(0, 16384)
 
 
+def oracle_module():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
 def cpu_baseline(basis, D, budget_s=25.0):
     """Times the oracle (C++/OpenMP restatement of directScaffoldNew) on all
     host cores: one warm-up build then as many builds as fit the budget."""
@@ -170,7 +189,7 @@ def cpu_baseline(basis, D, budget_s=25.0):
                 cores=os.cpu_count(), G=2 * J - K)
 
 
-def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64):
+def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64, check=True):
     """(H2O)8 / cc-pVDZ (N = 192): 64 symmetric perturbations
     dD_k = 1e-3 (X_k + X_k^T) contracted (J and K) against one pass of
     screened ERIs, incremental (AX += G[dD]), captured once as a CUDA graph
@@ -230,61 +249,101 @@ def run_batched(dev, steps, warmup, precision="fp64", cutoff=0.0, ndens=64):
         e1.record(stream)
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
+    # error of one launch against the oracle on two of the densities (the
+    # graph accumulates, so the outputs are zeroed and it is replayed once)
+    for o in out:
+        o.zero_()
+    g.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
     g.close()
+    err = None
+    if check:
+        O = oracle_module()
+        ob = O.OracleBasis(basis)
+        errs = []
+        for k in (0, 1):
+            Jo, Ko = ob.contract([dDs[k], dDs[k]], [1, 1], [0, 1])
+            J = out[2 * k].t().contiguous().t().cpu().numpy()
+            K = out[2 * k + 1].t().contiguous().t().cpu().numpy()
+            errs.append(float(np.abs((2 * J - K) - (2 * Jo - Ko)).max()))
+        err = {"fock_maxabs_vs_oracle": max(errs), "densities_checked": 2,
+               "what": "max |G_k - G_k(oracle)|, G = 2J - K of dD_0 and dD_1 (one launch)"}
     t = float(np.median(ms)) / 1e3
     res = {"workload": "h2o8_ccpvdz x 64 dD (J+K), CUDA graph", "nbasis": N,
            "densities_per_launch": ndens, "ms_per_launch": t * 1e3,
-           "builds_per_s": ndens / t, "precision": precision, "fp32_cutoff": cutoff}
+           "builds_per_s": ndens / t, "precision": precision, "fp32_cutoff": cutoff,
+           "errors": err}
     if single:
         res["fp64_single_density"] = single
     return res
 
 
-def run_serving(dev, nreq, rate, cutoff):
-    """The serving stream: nreq requests with Poisson arrivals at `rate` Hz,
-    each a seeded (H2O)_n, n ~ U{1..32}, cc-pVDZ or def2-SVP (50/50), its own
-    seeded density, mixed precision; continuous batching with memory
-    admission.  Latency = completion - arrival."""
-    import numpy as np
-
+def prepare_serving(dev, nreq):
+    """The requests of the serving stream (config 5): nreq seeded (H2O)_n,
+    n ~ U{1..32}, cc-pVDZ or def2-SVP (50/50), each with its own seeded
+    S-orthonormalised occupied-orbital density (5 per water); arrival offsets
+    of a unit-rate Poisson process (divided by the rate when replayed).  S
+    comes from the device, before any timed stream starts."""
     from chronusq_public_b200 import workloads
     from chronusq_public_b200.basis import BasisSet
     from chronusq_public_b200.contraction import DirectTPI
-    from chronusq_public_b200.serving import FockRequest, FockServer, poisson_stream
-    reqs = poisson_stream(nreq, rate, seed=5)
+    from chronusq_public_b200.serving import poisson_stream
     prepared = []
-    for r in reqs:
+    for r in poisson_stream(nreq, 1.0, seed=5):
         mol = workloads.water_cluster(r["nwater"], seed=r["geom_seed"],
                                       box=max(6.0, 10.0 * (r["nwater"] / 16.0) ** (1 / 3)))
         basis = BasisSet.build(mol, r["basis"])
-        # seeded S-orthonormalised occupied-orbital density (5 per water);
-        # S from the device, before the timed stream starts
         tpi = DirectTPI(basis, device=dev.index or 0)
         S, _ = tpi.one_electron()
         tpi.close()
         D = workloads.occupied_density(S, 5 * r["nwater"], r["dens_seed"])
-        prepared.append((r, mol, D))
+        prepared.append((r, mol, D, basis))
+    return prepared
+
+
+def run_serving(dev, prepared, rate, cutoff, check=0):
+    """Replays the prepared requests with Poisson arrivals at `rate` Hz into
+    the native server (continuous batching, memory admission), mixed
+    precision.  Latency = completion - arrival.  With check > 0 that many
+    requests of at most 8 waters (every k-th of them) are compared with the
+    oracle's G = 2J - K."""
+    import numpy as np
+
+    from chronusq_public_b200.serving import FockRequest, FockServer
     srv = FockServer(device=dev.index or 0, slots=8, mem_budget=16 << 30)
     futs = []
     t0 = time.perf_counter()
-    for (r, mol, D) in prepared:
+    for (r, mol, D, _b) in prepared:
+        ta = r["t"] / rate
         now = time.perf_counter() - t0
-        if r["t"] > now:
-            time.sleep(r["t"] - now)
+        if ta > now:
+            time.sleep(ta - now)
         futs.append(srv.submit(FockRequest(mol, r["basis"], D, precision="mixed",
                                            fp32_cutoff=cutoff, rid=r["rid"],
-                                           arrival=t0 + r["t"])))
-    for f in futs:
-        f.result(timeout=600)
+                                           arrival=t0 + ta)))
+    results = [f.result(timeout=900) for f in futs]
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    return {"requests": nreq, "arrival_rate_hz": rate, "wall_s": wall,
-            "builds_per_s": nreq / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "mean_ms": st["mean_ms"], "fp32_cutoff": cutoff,
-            "phases_ms": {k: st[k] for k in ("prep_ms", "queue_ms", "setup_ms", "build_ms")
-                          if k in st},
-            "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
+    out = {"requests": len(prepared), "arrival_rate_hz": rate, "wall_s": wall,
+           "builds_per_s": len(prepared) / wall, "p50_ms": st["p50_ms"],
+           "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "fp32_cutoff": cutoff,
+           "peak_inflight": st.get("peak_inflight"),
+           "phases_ms": {k: st[k] for k in ("prep_ms", "queue_ms", "setup_ms", "build_ms")
+                         if k in st},
+           "mix": "U{1..32} waters, cc-pVDZ/def2-SVP 50/50"}
+    if check > 0:
+        O = oracle_module()
+        small = [i for i, p in enumerate(prepared) if p[0]["nwater"] <= 8]
+        pick = small[::max(1, len(small) // check)][:check]
+        errs = []
+        for i in pick:
+            D, basis = prepared[i][2], prepared[i][3]
+            Jo, Ko = O.OracleBasis(basis).contract([D, D], [1, 1], [0, 1])
+            errs.append(float(np.abs(results[i] - (2 * Jo - Ko)).max()))
+        out["errors"] = {"fock_maxabs_vs_oracle": max(errs), "requests_checked": len(pick),
+                         "what": "max |G - G(oracle)| over sampled requests of <= 8 waters"}
+    return out
 
 
 def reference_arm_4c(args, ws):
@@ -367,6 +426,85 @@ def reference_arm(args, ws, rank):
             "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_four_component_sub(args, local):
+    """Config 3 inside the default run: the Ag4 four-component build
+    (BareCoulomb + DiracCoulomb + SSSS, libcint branch; N = 608, 4C dimension
+    2432), one FP64 and one mixed build timed with CUDA events after a
+    warm-up on a zero density (which computes the 4C Schwarz tables with
+    every quartet screened); the mixed build's largest deviation from the
+    FP64 one; the bounded CPU sample (one Ag atom, bare Coulomb + LLSS) timed
+    on the oracle and on the GPU, with the GPU's deviation from the oracle."""
+    import numpy as np
+    import torch
+
+    from chronusq_public_b200 import workloads
+    from chronusq_public_b200.basis import BasisSet, Molecule
+    from chronusq_public_b200.contraction import DirectTPI
+    from chronusq_public_b200.fockbuilder import FourCompFock
+
+    dev = torch.device("cuda", local)
+    basis, tpi, D = workloads.build_ag4_dc(lambda b: DirectTPI(b, device=local))
+    N2 = 2 * basis.nbasis
+    Dd = [torch.from_numpy(np.ascontiguousarray(d.T)).to(dev).t() for d in D]
+    fb = FourCompFock(tpi)
+    stream = torch.cuda.Stream(dev)
+    fb.formGD([torch.zeros_like(d) for d in Dd], stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+
+    def timed(**kw):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        G = fb.formGD(Dd, stream=stream.cuda_stream, **kw)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, G, dict(fb.last_stats)
+
+    with ClockSampler(local) as clk:
+        t64, G, s64 = timed()
+        t32, Gm, s32 = timed(precision="mixed", fp32_cutoff=args.cutoff)
+    herm = max(float((g - g.conj().t()).abs().max()) for g in G)
+    mixed_err = max(float((a - b).abs().max()) for a, b in zip(Gm, G))
+    del Gm
+    out = {"workload": "ag4_dc", "nbasis_1c": basis.nbasis, "dim_4c": 2 * N2,
+           "hamiltonian": "BareCoulomb + DiracCoulomb + SSSS (libcint)",
+           "fp64": {"s_per_build": t64, "builds_per_s": 1.0 / t64,
+                    "quartets_computed": s64["fp64"], "quartets_screened": s64["screened"]},
+           "mixed": {"s_per_build": t32, "builds_per_s": 1.0 / t32,
+                     "fp32_cutoff": args.cutoff, "quartets_fp32": s32["fp32"],
+                     "quartets_fp64": s32["fp64"], "speedup_vs_fp64": t64 / t32,
+                     "G_maxabs_vs_fp64": mixed_err},
+           "checks": {"G_hermiticity_maxabs": herm},
+           "clocks": clk.summary()}
+    if not args.no_oracle:
+        O = oracle_module()
+        b1 = BasisSet.build(Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)]),
+                            "sapporo-dkh3-dzp-2012_no", uncontract=True)
+        tpi1 = DirectTPI(b1, device=local)
+        S1, T1 = tpi1.one_electron()
+        D1 = workloads.spinor_density_4c(S1, T1, 47, 3)
+        ob = O.OracleBasis(b1)
+        t0 = time.perf_counter()
+        Go = ob.dirac_coulomb(D1, bare=True, dc=True, ssss=False)
+        tcpu = time.perf_counter() - t0
+        fb1 = FourCompFock(tpi1, DiracCoulombSSSS=False)
+        fb1.formGD(D1)
+        t0 = time.perf_counter()
+        Gg = fb1.formGD(D1)
+        tg = time.perf_counter() - t0
+        out["cpu_baseline"] = {
+            "value": 1.0 / tcpu, "unit": "builds/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "one Ag atom (N = 152), bare Coulomb + LLSS, C++/OpenMP restatement "
+                      "of directScaffoldLibcint + formGDDirect",
+            "gpu_same_sample_builds_per_s": 1.0 / tg,
+            "fock_maxabs_gpu_vs_oracle": max(float(np.abs(a - b).max())
+                                             for a, b in zip(Gg, Go)),
+            "G_maxabs_of_sample": max(float(np.abs(b).max()) for b in Go)}
+        tpi1.close()
+    tpi.close()
+    return out
 
 
 def run_four_component(args, ws, rank, local, pg):
@@ -645,6 +783,16 @@ def main():
     complex_build = {"what": "complex Hermitian J+K (D + i A), FP64, device pointers",
                      "ms_per_build": float(np.median(mscx)),
                      "builds_per_s": 1e3 / float(np.median(mscx))}
+    Zcx = D + 0.01j * (Ac - Ac.T)
+    if not args.no_oracle and ws == 1:
+        Jcx.zero_(); Kcx.zero_()
+        con.twoBodyContract(cxl, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        Jo, Ko = oracle_module().OracleBasis(basis).contract([Zcx, Zcx], [1, 1], [0, 1])
+        Gc = (2 * Jcx - Kcx).t().contiguous().t().cpu().numpy()
+        complex_build["errors"] = {
+            "fock_maxabs_vs_oracle": float(np.abs(Gc - (2 * Jo - Ko)).max()),
+            "what": "max |G - G(oracle)|, G = 2J - K of the complex Hermitian density"}
 
     # end-to-end through the public API with host buffers
     fb = FockBuilder(tpi)
@@ -652,10 +800,11 @@ def main():
         fb.formRawGD(D, precision="mixed", fp32_cutoff=args.cutoff)
     torch.cuda.synchronize()
     te = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        fb.formRawGD(D, precision="mixed", fp32_cutoff=args.cutoff)
-        te.append(time.perf_counter() - t0)
+    with ClockSampler(local) as clk_e2e:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fb.formRawGD(D, precision="mixed", fp32_cutoff=args.cutoff)
+            te.append(time.perf_counter() - t0)
 
     def agg(x):
         t = torch.tensor([sum(x)], dtype=torch.float64, device=dev)
@@ -686,15 +835,26 @@ def main():
     frac64 = (fl64["f64"] / (p64 * 1e12)) / (t64 / K)
 
     batched = None
-    if args.batched:
-        batched = {"fp64": run_batched(dev, args.steps, args.warmup),
-                   "mixed": run_batched(dev, args.steps, args.warmup, "mixed", args.cutoff)}
-        batched["mixed_batched_over_fp64_single"] = (
-            batched["mixed"]["builds_per_s"]
+    if args.batched and ws == 1:
+        # config 4's incremental dD build runs in FP64 (FockBuilder keeps
+        # increments in FP64); the mixed graph is reported beside it with its
+        # error
+        chk = not args.no_oracle
+        batched = {"fp64": run_batched(dev, args.steps, args.warmup, check=chk),
+                   "mixed": run_batched(dev, args.steps, args.warmup, "mixed", args.cutoff,
+                                        check=chk)}
+        batched["fp64_graph_over_fp64_single"] = (
+            batched["fp64"]["builds_per_s"]
             / batched["fp64"]["fp64_single_density"]["builds_per_s"])
+    four_comp = None
+    if args.four_comp and ws == 1:
+        four_comp = run_four_component_sub(args, local)
     serving = None
-    if args.serving_requests > 0:
-        serving = run_serving(dev, args.serving_requests, args.serving_rate, args.cutoff)
+    if args.serving_requests > 0 and ws == 1:
+        prepared = prepare_serving(dev, args.serving_requests)
+        serving = {"rates": [run_serving(dev, prepared, r, args.cutoff,
+                                         check=3 if k == 0 else 0)
+                             for k, r in enumerate(args.serving_rates)]}
 
     cpu = None
     err = {}
@@ -713,10 +873,11 @@ def main():
         sw["fock_maxabs"] = float(np.abs(Gc - Gref).max())
         sw["energy_err"] = abs(two_electron_energy(Gc, D) - two_electron_energy(Gref, D))
         sw["errors_against"] = "oracle" if cpu else "FP64 GPU build"
-    # kernels per build: block norms x2, max, norms_aux, to_cart x2, one per
-    # class pair, back transform x2
+    # kernels per mixed build: block norms x2, max, norms_aux, to_cart x2,
+    # the FP32 density copy, per class pair the planning pass and the FP64
+    # and FP32 class kernels, back transform x2
     ncls = len({(max(a.l, b.l), min(a.l, b.l)) for a in basis.shells for b in basis.shells})
-    launches_per_step = 2 + 1 + 1 + 2 + ncls * (ncls + 1) // 2 + 2
+    launches_per_step = 2 + 1 + 1 + 2 + 1 + 3 * (ncls * (ncls + 1) // 2) + 2
     line = {
         "metric": METRIC, "value": vmx, "unit": "builds/s", "n_gpus": ws,
         "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / K,
@@ -741,17 +902,23 @@ def main():
                               "source": "measured in this run (FMA microbenchmark)"},
                      "unit": "TFLOP/s", "frac": frac,
                      "gflop_per_build": {"f64": fl["f64"] / 1e9, "f32": fl["f32"] / 1e9},
-                     # DRAM bytes of one FP64 build (all its launches) from an
-                     # ncu capture with per-launch cache flush (an upper bound)
-                     "traffic": 1.02e8 if args.workload == "h2o16_def2svp" else None},
+                     "traffic": TRAFFIC_BYTES.get(args.workload),
+                     "traffic_source": "constant: DRAM read+write bytes of one mixed build "
+                                       "(all its launches) from the ncu capture in "
+                                       "profiles/launches_jk_h2o16_def2svp.md, per-launch "
+                                       "cache flush (an upper bound); not measured in "
+                                       "this run"},
         "e2e": {"value": ve2e, "unit": "builds/s",
                 "h2d_bytes_per_step": 8 * N * N,
-                "d2h_bytes_per_step": 2 * 8 * N * N},
+                "d2h_bytes_per_step": 2 * 8 * N * N,
+                "clocks": clk_e2e.summary()},
         "gpu_launches": launches_per_step * K,
         "clocks": clocks,
     }
     if batched:
         line["batched_dD_graph"] = batched
+    if four_comp:
+        line["four_component_ag4"] = four_comp
     if serving:
         line["serving"] = serving
     if cpu:

@@ -1391,18 +1391,23 @@ WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts) {
   // FP32 copy of the Cartesian densities (mixed real builds)
   const bool mixed = opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0 && !opts.is_complex;
   L.oXc32 = take(mixed ? (matC * nMat + 1) / 2 : 0);
-  // quartet masks of the fast class kernels: for each class pair, room for
-  // either orientation (which class is the bra is the generated kernel's)
-  size_t words = 0;
-  for (int cb = 0; cb < NCLS; cb++)
-    for (int ck = 0; ck < NCLS; ck++) {
-      L.oMaskCls[cb][ck] = words;
-      if (ck > cb || opts.is_complex || !B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
+  // quartet masks of the fast class kernels: one region per launch stream,
+  // as many mask words as the largest class pair needs (either orientation)
+  // up to MASK_CAP_WORDS, and at least one bra row of the widest class;
+  // larger class pairs run in slabs of bra pairs
+  size_t need = 0, row = 1;
+  for (int cb = 0; cb < NCLS; cb++) {
+    row = std::max<size_t>(row, ((size_t)B->cls_cnt[cb] + WTILE - 1) / WTILE);
+    for (int ck = 0; ck <= cb; ck++) {
+      if (opts.is_complex || !B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
       const size_t nb = B->cls_cnt[cb], nk = B->cls_cnt[ck];
-      // mask words (uint2) + two word lists (int each) = 2 words per word
-      words += 2 * std::max(nb * ((nk + 31) / 32), nk * ((nb + 31) / 32));
+      need = std::max(need, std::max(nb * ((nk + WTILE - 1) / WTILE),
+                                     nk * ((nb + WTILE - 1) / WTILE)));
     }
-  L.oMask = take(std::max<size_t>(words, 1));
+  }
+  L.maskWords = need == 0 ? 0 : std::max(row, std::min(need, MASK_CAP_WORDS));
+  // per word: the uint2 mask and one entry in each of the two word lists
+  L.oMask = take(std::max<size_t>(2 * L.maskWords * (NAUX + 1), 1));
   L.total = off;
   return L;
 }
@@ -1420,7 +1425,41 @@ cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, 
 
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
-                         const int* d_flags_pre, const double* const* normSrc);
+                         const int* d_flags_pre, const double* const* normSrc,
+                         double* pinned);
+
+struct PinnedBuf {
+  double* p;
+  size_t bytes;
+  bool busy;
+};
+static std::mutex g_pinned_mu;
+static std::vector<PinnedBuf> g_pinned;
+
+cqf_status pinned_acquire(size_t bytes, double** out) {
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  PinnedBuf* best = nullptr;
+  for (auto& b : g_pinned)
+    if (!b.busy && b.bytes >= bytes && (!best || b.bytes < best->bytes)) best = &b;
+  if (!best) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CQF_ENOMEM, "page-locked host staging allocation failed");
+    }
+    g_pinned.push_back({static_cast<double*>(p), bytes, false});
+    best = &g_pinned.back();
+  }
+  best->busy = true;
+  *out = best->p;
+  return CQF_OK;
+}
+
+void pinned_release(double* p) {
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  for (auto& b : g_pinned)
+    if (b.p == p) b.busy = false;
+}
 
 // Complex Hermitian densities on the real fast kernels: with X = S + iA (S
 // real symmetric, A real antisymmetric), J[X] = J[S] and K[X] = K[S] + i K[A],
@@ -1569,7 +1608,8 @@ cqf_status contract_complex_split_on(cqf_basis* B, const cqf_contraction* list, 
 // made B's device current.
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
-                         const int* d_flags_pre, const double* const* normSrc) {
+                         const int* d_flags_pre, const double* const* normSrc,
+                         double* pinned) {
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const int cw = opts.is_complex ? 2 : 1;
@@ -1583,7 +1623,14 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   std::vector<const double*> Xd(nMat);
   std::vector<double*> AXd(nMat);
   for (int m = 0; m < nMat; m++) {
-    if (host) {
+    if (host && pinned && !capture) {
+      Xd[m] = ws + oX + m * matN;
+      AXd[m] = ws + oAX + m * matN;
+      std::memcpy(pinned + m * matN, list[m].X, matN * sizeof(double));
+      CQF_CUDA(cudaMemcpyAsync((void*)Xd[m], pinned + m * matN, matN * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+      CQF_CUDA(cudaMemsetAsync(AXd[m], 0, matN * sizeof(double), st));
+    } else if (host) {
       Xd[m] = ws + oX + m * matN;
       AXd[m] = ws + oAX + m * matN;
       CQF_CUDA(cudaMemcpyAsync((void*)Xd[m], list[m].X, matN * sizeof(double),
@@ -1696,12 +1743,14 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
       const int lm = std::max(std::max(la, lb), std::max(lc, ld));
       // autotuning times each class alone, on st, between two events
       const bool tune = B->tuning && !capture;
-      const cudaStream_t ls = tune ? st : lanes[nlaunch++ % (NAUX + 1)];
+      const int li = tune ? 0 : nlaunch++ % (NAUX + 1);
+      const cudaStream_t ls = lanes[li];
       if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck)], st));
-      uint2* masks = reinterpret_cast<uint2*>(ws + Lw.oMask) + Lw.oMaskCls[cb][ck];
+      uint2* masks = reinterpret_cast<uint2*>(ws + Lw.oMask) + 2 * Lw.maskWords * li;
+      a.braOff = 0;
       if (!(fastOK && lm <= 2 &&
-            launch_jk_fast(a, la, lb, lc, ld, masks, work + 4 * (cb * NCLS + ck), B->nsm, ls,
-                           B->blocks_per_sm[cb][ck])))
+            launch_jk_fast(a, la, lb, lc, ld, masks, (long long)Lw.maskWords, work + 4 * li,
+                           B->nsm, ls, B->blocks_per_sm[cb][ck])))
         launch_jk_generic(a, la, lb, lc, ld, ls);
       if (tune) CQF_CUDA(cudaEventRecord(B->tune_ev[2 * (cb * NCLS + ck) + 1], st));
     }
@@ -1717,16 +1766,23 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
         N, nc, B->d_shells,
         B->d_ao2shell, B->d_sph, B->d_sphOff, AXd[m]);
   CQF_CUDA(cudaGetLastError());
+  const bool staged = host && pinned && !capture;
   if (host)
     for (int m = 0; m < nMat; m++)
-      CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXd[m], matN * sizeof(double), cudaMemcpyDeviceToHost,
-                               st));
+      CQF_CUDA(cudaMemcpyAsync(staged ? pinned + (size_t)(nMat + m) * matN : list[m].AX, AXd[m],
+                               matN * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (capture) return CQF_OK;
   CQF_CUDA(cudaEventRecord(B->ev1, st));
   unsigned long long cnt[4] = {0, 0, 0, 0};
   CQF_CUDA(cudaMemcpyAsync(cnt, B->d_counters, 4 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
   CQF_CUDA(cudaStreamSynchronize(st));
+  if (staged)  // AX += G[X] on the host
+    for (int m = 0; m < nMat; m++) {
+      double* ax = static_cast<double*>(list[m].AX);
+      const double* g = pinned + (size_t)(nMat + m) * matN;
+      for (size_t i = 0; i < matN; i++) ax[i] += g[i];
+    }
   if (stats) {
     stats->quartets_total = (long long)cnt[0];
     stats->quartets_screened = (long long)cnt[1];
@@ -1934,8 +1990,19 @@ cqf_status cqf_two_body_contract(cqf_basis* B, const cqf_contraction* listIn, in
                                      static_cast<double*>(B->d_ws));
   }
   CQF_TRY(ensure_ws(B, ws_layout(B, nMat, opts).total * sizeof(double)));
-  return contract_core(B, list.data(), nMat, opts, stats, static_cast<double*>(B->d_ws), false,
-                       nullptr);
+  if (opts.device_pointers)
+    return contract_core(B, list.data(), nMat, opts, stats, static_cast<double*>(B->d_ws),
+                         false, nullptr);
+  // host pointers: X up and the result down through a pooled page-locked
+  // buffer (contract_core synchronises before returning)
+  const size_t matN = (size_t)B->nbasis * B->nbasis * (opts.is_complex ? 2 : 1);
+  double* pinned = nullptr;
+  CQF_TRY(pinned_acquire(2 * nMat * matN * sizeof(double), &pinned));
+  const cqf_status s = contract_core(B, list.data(), nMat, opts, stats,
+                                     static_cast<double*>(B->d_ws), false, nullptr, nullptr,
+                                     pinned);
+  pinned_release(pinned);
+  return s;
 }
 
 }  // extern "C"

@@ -63,6 +63,7 @@ struct JKLaunch {
   const double* qWin;       // per pair: largest Q of the WTILE pairs from it (same class)
   double primK4;            // (largest contraction length)^4 of the basis
   int lsum;                 // la + lb + lc + ld of the launch's class
+  int braOff;               // position of the launch's first bra pair in its class (slabs)
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
@@ -74,13 +75,17 @@ cqf_status fail(cqf_status s, const std::string& msg);
 // Workspace layout of one contraction (in doubles, each part 256-B aligned):
 // [X copies | AX copies] (host pointers only) | Xc | Ac | norms | normsMat |
 // gmax | norms^T | pair norms | work counters | Xc in FP32 (mixed real
-// builds) | quartet masks of the fast class kernels (per class pair one uint2
-// per bra pair and ket tile, then the two lists of non-empty words;
-// oMaskCls[cb][ck]: first uint2 of a class pair, relative to oMask)
-constexpr int NWORK = 4 * NCLS * NCLS;  // class-kernel work counters / list lengths per call
+// builds) | quartet masks of the fast class kernels (per launch stream a
+// region of maskWords uint2 masks, one per bra pair and ket tile, then the
+// two lists of non-empty words)
+// class-kernel work counters / list lengths: four per launch stream
+constexpr int NWORK = 4 * (NAUX + 1);
+// mask words a launch stream's region holds at most (16 B per word: the
+// uint2 mask and two list entries); class pairs with more run in slabs
+constexpr size_t MASK_CAP_WORDS = size_t(1) << 18;
 struct WsLayout {
   size_t oX, oAX, oXc, oAc, oNm, oNmM, oG, oNmT, oPN, oWork, oXc32, oMask, total;
-  size_t oMaskCls[NCLS][NCLS];
+  size_t maskWords;  // mask words of each launch stream's region
 };
 WsLayout ws_layout(const cqf_basis* B, int nMat, const cqf_opts& opts);
 cqf_status check_contract_args(const cqf_basis* B, const cqf_contraction* list, int nMat);
@@ -133,9 +138,22 @@ cqf_status contract_complex_split_on(cqf_basis* B, const cqf_contraction* list, 
 // normSrc (optional, device pointers): per entry, the complex matrix whose
 // shell-block norms screen it in place of its own X (the split of a complex
 // Hermitian density keeps the reference's complex screen).
+// pinned (host pointers, optional): page-locked host buffer of 2 nMat
+// matrices; X goes to the device through it and the contraction's result
+// comes back through it and is added to the caller's AX on the host (no
+// upload of AX).  Without it the host matrices are copied directly.
 cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
-                         const int* d_flags_pre, const double* const* normSrc = nullptr);
+                         const int* d_flags_pre, const double* const* normSrc = nullptr,
+                         double* pinned = nullptr);
+// Page-locked host staging buffers of host-pointer contractions, shared by
+// every basis of the process: acquire returns a buffer of at least `bytes`
+// that no other call holds (allocating one only when none fits), release
+// returns it.  They are kept until the process exits -- freeing page-locked
+// memory synchronises the whole device, which would stall the concurrent
+// requests of a server.
+cqf_status pinned_acquire(size_t bytes, double** out);
+void pinned_release(double* p);
 
 // Resolves the no-alloc scratch array's device address on `device` (current)
 // during basis creation (cqf_noalloc.cu).

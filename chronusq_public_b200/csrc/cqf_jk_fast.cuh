@@ -125,10 +125,11 @@ __global__ void __launch_bounds__(256)
     for (int word = run * PLAN_RUN; word < wEnd; word++) {
       const int ib = word / nTiles, tile = word - ib * nTiles;
       unsigned b64 = 0u, b32 = 0u;
-      if (!(a.same && tile * WTILE > ib)) {  // else: no quartet in this word
+      const int ibc = ib + a.braOff;  // the bra's position in its class
+      if (!(a.same && tile * WTILE > ibc)) {  // else: no quartet in this word
         const int jk = tile * WTILE + lane;
         const PairDev P = a.pairs[a.braBeg + ib];
-        const bool visited = jk < a.nKet && !(a.same && jk > ib);
+        const bool visited = jk < a.nKet && !(a.same && jk > ibc);
         const double tileMax = __ldg(a.maxNorm) * P.Q * __ldg(a.qWin + a.ketBeg + tile * WTILE);
         bool screened = false, w32 = false;
         if (a.screen && tileMax < a.thresh) {
@@ -343,12 +344,13 @@ inline int entries_per_item(long long nWords, int nchunk, int nsm) {
 
 // Launches the planning pass and the generated class kernels of the class
 // (la lb | lc ld) (either orientation); false when the class has no
-// generated kernel.  masks: the class pair's mask words (nBra x ceil(nKet /
-// 32) uint2) followed by its two word lists (nWords ints each); work: four
-// zeroed device counters (FP64 / FP32 class kernel items, FP64 / FP32 list
-// lengths).
+// generated kernel.  masks: the launch stream's region of maskWords uint2
+// (mask words of a slab of bra pairs x ceil(nKet / 32) ket tiles, then its
+// two word lists); work: the stream's four counters (FP64 / FP32 class
+// kernel items, FP64 / FP32 list lengths), zeroed here before each slab.
 inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, uint2* masks,
-                           unsigned int* work, int nsm, cudaStream_t st, int blocksPerSm = 8) {
+                           long long maskWords, unsigned int* work, int nsm, cudaStream_t st,
+                           int blocksPerSm = 8) {
   if (a.nBra == 0 || a.nKet == 0) return true;
   bool done = false;
   auto go = [&](auto tag64, auto tag32, bool swap) {
@@ -363,28 +365,39 @@ inline bool launch_jk_fast(JKLaunch a, int la, int lb, int lc, int ld, uint2* ma
     b.lsum = la + lb + lc + ld;
     const bool mixed = b.precision == 1 && b.fp32_cut > 0.0;
     const int nTiles = (b.nKet + WTILE - 1) / WTILE;
-    const long long nWords = (long long)b.nBra * nTiles;
-    const long long nRuns = (nWords + PLAN_RUN - 1) / PLAN_RUN;
-    const unsigned gp = (unsigned)std::min<long long>((nRuns + 7) / 8, (long long)nsm * 8);
-    // word lists: FP64 then FP32, nWords entries each; counts in work[2..3]
-    int* list64 = reinterpret_cast<int*>(masks + nWords);
-    int* list32 = list64 + nWords;
-    if (mixed)
-      jk_plan_kernel<true><<<gp, 256, 0, st>>>(b, masks, list64, list32, work + 2);
-    else
-      jk_plan_kernel<false><<<gp, 256, 0, st>>>(b, masks, list64, list32, work + 2);
-    constexpr int WPB = JK_THREADS / 32;
-    auto grid = [&](long long items) {
-      return (unsigned)std::max<long long>(
-          1, std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * blocksPerSm));
-    };
-    const int e64 = entries_per_item(nWords, G64::NCHUNK, nsm);
-    jk_class_kernel<G64, false><<<grid((nWords + e64 - 1) / e64 * G64::NCHUNK), JK_THREADS, 0,
-                                  st>>>(b, masks, list64, work + 2, e64, work);
-    if (mixed) {
-      const int e32 = entries_per_item(nWords, G32::NCHUNK, nsm);
-      jk_class_kernel<G32, true><<<grid((nWords + e32 - 1) / e32 * G32::NCHUNK), JK_THREADS, 0,
-                                   st>>>(b, masks, list32, work + 3, e32, work + 1);
+    // slabs of bra pairs whose mask words fit the stream's region; each
+    // reuses the region and the stream's counters after the last one's
+    // kernels (stream order)
+    const int slab = (int)std::max<long long>(1, maskWords / nTiles);
+    for (int ib0 = 0; ib0 < b.nBra; ib0 += slab) {
+      JKLaunch c = b;
+      c.braBeg = b.braBeg + ib0;
+      c.nBra = std::min(slab, b.nBra - ib0);
+      c.braOff = b.braOff + ib0;
+      cudaMemsetAsync(work, 0, 4 * sizeof(unsigned int), st);
+      const long long nWords = (long long)c.nBra * nTiles;
+      const long long nRuns = (nWords + PLAN_RUN - 1) / PLAN_RUN;
+      const unsigned gp = (unsigned)std::min<long long>((nRuns + 7) / 8, (long long)nsm * 8);
+      // word lists: FP64 then FP32, nWords entries each; counts in work[2..3]
+      int* list64 = reinterpret_cast<int*>(masks + nWords);
+      int* list32 = list64 + nWords;
+      if (mixed)
+        jk_plan_kernel<true><<<gp, 256, 0, st>>>(c, masks, list64, list32, work + 2);
+      else
+        jk_plan_kernel<false><<<gp, 256, 0, st>>>(c, masks, list64, list32, work + 2);
+      constexpr int WPB = JK_THREADS / 32;
+      auto grid = [&](long long items) {
+        return (unsigned)std::max<long long>(
+            1, std::min<long long>((items + WPB - 1) / WPB, (long long)nsm * blocksPerSm));
+      };
+      const int e64 = entries_per_item(nWords, G64::NCHUNK, nsm);
+      jk_class_kernel<G64, false><<<grid((nWords + e64 - 1) / e64 * G64::NCHUNK), JK_THREADS,
+                                    0, st>>>(c, masks, list64, work + 2, e64, work);
+      if (mixed) {
+        const int e32 = entries_per_item(nWords, G32::NCHUNK, nsm);
+        jk_class_kernel<G32, true><<<grid((nWords + e32 - 1) / e32 * G32::NCHUNK), JK_THREADS,
+                                     0, st>>>(c, masks, list32, work + 3, e32, work + 1);
+      }
     }
     done = true;
   };

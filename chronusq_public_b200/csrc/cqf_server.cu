@@ -235,8 +235,11 @@ unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell) {
       npair * (72 + (112 + 48 + 8 + 104 + 52) * maxp * maxp) + ns * ns * 8 + 300000;
   // workspace: densities and accumulators (spherical, Cartesian, FP32
   // copy), norms, and the class kernels' quartet masks and word lists
-  // (16 B per 32 unique quartets of pairs, plus one word per pair and class)
-  const unsigned long long masks = 16 * (npair * ((npair + 31) / 32) / 2 + 28 * npair);
+  // (16 B per mask word -- 32 quartets of a bra pair and a ket tile -- in
+  // each of the three launch streams' regions, at most 2^18 words each)
+  const unsigned long long maskw = std::min<unsigned long long>(
+      npair * ((npair + 31) / 32), 1ull << 18);
+  const unsigned long long masks = 3 * 16 * maskw;
   const unsigned long long ws =
       8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns) + 4 * nmat * nc * nc +
       masks;

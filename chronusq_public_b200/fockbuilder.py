@@ -24,7 +24,12 @@ class FockBuilder:
                   fp32_cutoff: float = 0.0, increment: bool = False,
                   J=None, K=None):
         """Returns (G, J, K).  With ``increment`` the J/K passed in are
-        accumulated (the incremental dD build of formGD, impl.hpp:80-88)."""
+        accumulated (the incremental dD build of formGD, impl.hpp:80-88);
+        that build always runs in FP64 -- mixed precision applies to builds
+        from the full density, whose FP32 errors do not accumulate over SCF
+        iterations the way the increments' would."""
+        if increment:
+            precision = "fp64"
         N = self.tpi.nbasis
         if J is None or not increment:
             J = np.zeros((N, N), order="F")

@@ -312,7 +312,8 @@ typedef struct {
  * (upper bound: every pair significant, every pair with the largest
  * primitive count) plus the contraction workspace of one J and one K
  * (densities and accumulators, norms, and the class kernels' quartet masks
- * and word lists, 16 B per 32 unique quartets of pairs). */
+ * and word lists: 16 B per 32 quartets of a bra pair and a ket tile in each
+ * of three launch streams' regions, at most 4 MiB each). */
 unsigned long long cqf_fock_footprint(const cqf_shell* shells, int nshell);
 
 cqf_status cqf_server_create(const cqf_server_opts* opts, cqf_server** out);

@@ -126,7 +126,7 @@ def _footprint_model(basis, nmat=2):
     npair = ns * (ns + 1) // 2
     kprim = basis.max_prim ** 2
     pairs = npair * (72 + (112 + 48 + 8 + 104 + 52) * kprim) + ns * ns * 8 + 300_000
-    masks = 16 * (npair * ((npair + 31) // 32) // 2 + 28 * npair)
+    masks = 3 * 16 * min(npair * ((npair + 31) // 32), 1 << 18)
     ws = (8 * (2 * nmat * N * N + 2 * nmat * nc * nc + (nmat + 1) * ns * ns)
           + 4 * nmat * nc * nc + masks)
     return pairs + ws
