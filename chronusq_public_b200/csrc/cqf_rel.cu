@@ -1166,18 +1166,19 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
 // ------------------------------------------------------------ 4C Schwarz
 // Q^LL(a,b) = sqrt(max |(ab|ab)|) and Q^SS(a,b) = C2 sqrt(max over the 81
 // components of |(dA dB ab|dA dB ab)|), both over every element of the
-// spherical quartet block (direct4C_libcint.hpp:341-481).  One block per
-// pair: each component's Cartesian quartet block is built in shared memory
-// one ket column per thread, transformed to the spherical basis index by
-// index, and reduced.
+// spherical quartet block (direct4C_libcint.hpp:341-481).  Every (pair,
+// component) is one unit of work for a group of threads, one Cartesian ket
+// column per thread (rel_schwarz_kernel).
 
-// Cartesian column out[(a*nb + b) * stride] = (d ab | d cd) of the ket
-// component pair (c, d) with derivative directions dir[0..3] (-1: none).
+// Cartesian column out[(a*nb + b) * stride] += (d ab | d cd) of the ket
+// component pair (c, d) with derivative directions dir[0..3] (-1: none),
+// summed over the bra primitive pairs ip = ip0, ip0 + ipStep, ... (shared
+// memory, added atomically: several threads may share a column).
 template <int LM>
 __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const int* dir,
                              const PairDev& P, const PairDev& Q, const PrimPairDev* pp,
                              const ShellDev* shells, const double* prim, const double* boys,
-                             double* out, int stride) {
+                             double* out, int stride, int ip0, int ipStep) {
   constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
   constexpr int HB = nherm(2 * LM + 2);
   constexpr int HL = nherm(4 * LM + 4);
@@ -1192,8 +1193,7 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
   const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
   double Ea[3][E1], Ec[3][E1], G[HB], Rv[HL], F[4 * LM + 5], f[3][FL], g[3][FL];
   int nf[3], ng[3];
-  for (int k = 0; k < na * nb; k++) out[k * stride] = 0.0;
-  for (int ip = 0; ip < P.npp; ip++) {
+  for (int ip = ip0; ip < P.npp; ip += ipStep) {
     const PrimPairDev& A = pp[P.pp_off + ip];
     double ea, eb;
     pair_exps(SA, SB, prim, A, ea, eb);
@@ -1228,19 +1228,21 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
           ng[x] = axis_factor(Ea[x], lb + rb, la + lb + 2 * rb + 1, ax[x], bx[x], ty, 2.0 * ea,
                               2.0 * eb, g[x]);
         }
-        out[(ai * nb + bi) * stride] += bra_dot(g[0], ng[0], g[1], ng[1], g[2], ng[2], G);
+        atomicAdd(out + (ai * nb + bi) * stride,
+                  bra_dot(g[0], ng[0], g[1], ng[1], g[2], ng[2], G));
       }
   }
 }
 
 // one index of a 4-index block (row-major, index 3 fastest) from Cartesian
-// to spherical: out[.. mu ..] = sum_c T[c][mu] in[.. c ..]
+// to spherical: out[.. mu ..] = sum_c T[c][mu] in[.. c ..]; the gs threads
+// of a group (g0 = this thread's index in it) share the work
 __device__ void sph_index(const double* in, double* out, int* dims, int k, const double* T,
-                          int nsk) {
+                          int nsk, int g0, int gs) {
   int od[4] = {dims[0], dims[1], dims[2], dims[3]};
   od[k] = nsk;
   const int tot = od[0] * od[1] * od[2] * od[3];
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+  for (int e = g0; e < tot; e += gs) {
     int i[4], r = e;
     for (int q = 3; q >= 0; q--) {
       i[q] = r % od[q];
@@ -1259,76 +1261,89 @@ __device__ void sph_index(const double* in, double* out, int* dims, int k, const
   dims[k] = nsk;
 }
 
-__device__ double block_absmax(const double* buf, int n) {
-  __shared__ double red[32];
-  double m = 0.0;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) m = fmax(m, fabs(buf[e]));
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    m = (threadIdx.x < (blockDim.x + 31) / 32) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) red[0] = m;
-  }
-  __syncthreads();
-  m = red[0];
-  __syncthreads();
-  return m;
-}
-
 constexpr int SCH_THREADS = 128;
 
+// One (pair, component) per group of gsize threads, SCH_THREADS / gsize
+// groups per block, units enumerated pair-major over ncomp components per
+// pair: component 0 is the plain (ab|ab) block when lowLL, the others the
+// 81 derivative blocks (dA_i dB_j ab | dA_k dB_l ab).  A group builds the
+// Cartesian block in shared memory -- thread g0 takes ket column g0 % cpow
+// (cpow: the column count rounded up to a power of two) and every
+// (gsize / cpow)-th bra primitive pair from g0 / cpow -- transforms it to
+// the spherical basis index by index, and folds its largest |element| into
+// the pair's maximum (mx[2 pair + 0 / 1]: plain / derivative) with an atomic
+// max on the bit pattern (non-negative doubles order as integers).
 template <int LM>
 __global__ void __launch_bounds__(SCH_THREADS)
     rel_schwarz_kernel(const PairDev* __restrict__ pairs, const PrimPairDev* __restrict__ pp,
                        const ShellDev* __restrict__ shells, const double* __restrict__ prim,
                        const double* __restrict__ boys, const double* __restrict__ sph,
-                       const int* __restrict__ sphOff, int beg, int la, int lb, int needLL,
-                       int needSS, int nshell, double* qLL, double* qSS) {
+                       const int* __restrict__ sphOff, int beg, int npair, int la, int lb,
+                       int ncomp, int lowLL, int gsize, int cpow, unsigned long long* mx) {
   extern __shared__ double sm[];
-  const PairDev P = pairs[beg + blockIdx.x];
-  const ShellDev SA = shells[P.shA], SB = shells[P.shB];
   const int na = ncart(la), nb = ncart(lb);
   const int n4 = na * nb * na * nb;
-  double mxLL = 0.0, mxSS = 0.0;
-  for (int comp = needLL ? -1 : 0; comp < (needSS ? 81 : 0); comp++) {
-    int dir[4] = {-1, -1, -1, -1};
-    if (comp >= 0) {
-      dir[0] = comp / 27;
-      dir[1] = (comp / 9) % 3;
-      dir[2] = (comp / 3) % 3;
-      dir[3] = comp % 3;
-    }
-    double* cur = sm;
-    double* nxt = sm + n4;
-    for (int col = threadIdx.x; col < na * nb; col += blockDim.x)
-      deriv_column<LM>(la, lb, la, lb, col / nb, col % nb, dir, P, P, pp, shells, prim, boys,
-                       cur + col, na * nb);
-    __syncthreads();
-    int dims[4] = {na, nb, na, nb};
-    const ShellDev* S4[4] = {&SA, &SB, &SA, &SB};
-    for (int k = 0; k < 4; k++) {
-      const ShellDev& S = *S4[k];
-      if (!S.pure) continue;
-      sph_index(cur, nxt, dims, k, sph + sphOff[S.l], nsph(S.l));
-      __syncthreads();
+  const int groups = SCH_THREADS / gsize;
+  const int g = threadIdx.x / gsize, g0 = threadIdx.x % gsize;
+  const long long unit = (long long)blockIdx.x * groups + g;
+  const bool live = unit < (long long)npair * ncomp;
+  const int ip = live ? (int)(unit / ncomp) : 0;
+  const int comp = live ? (int)(unit % ncomp) : 0;
+  const PairDev P = pairs[beg + ip];
+  const ShellDev SA = shells[P.shA], SB = shells[P.shB];
+  int dir[4] = {-1, -1, -1, -1};
+  const int dc = comp - lowLL;  // derivative component 0..80, or -1: plain
+  if (dc >= 0) {
+    dir[0] = dc / 27;
+    dir[1] = (dc / 9) % 3;
+    dir[2] = (dc / 3) % 3;
+    dir[3] = dc % 3;
+  }
+  double* cur = sm + (size_t)g * 2 * n4;
+  double* nxt = cur + n4;
+  for (int e = g0; e < n4; e += gsize) cur[e] = 0.0;
+  __syncthreads();
+  const int col = g0 % cpow, slice = g0 / cpow, nslice = gsize / cpow;
+  if (live && col < na * nb)
+    deriv_column<LM>(la, lb, la, lb, col / nb, col % nb, dir, P, P, pp, shells, prim, boys,
+                     cur + col, na * nb, slice, nslice);
+  __syncthreads();
+  int dims[4] = {na, nb, na, nb};
+  const ShellDev* S4[4] = {&SA, &SB, &SA, &SB};
+  for (int k = 0; k < 4; k++) {  // every thread reaches each barrier
+    const ShellDev& S = *S4[k];
+    if (live && S.pure) {
+      sph_index(cur, nxt, dims, k, sph + sphOff[S.l], nsph(S.l), g0, gsize);
       double* t = cur;
       cur = nxt;
       nxt = t;
     }
-    const double m = block_absmax(cur, dims[0] * dims[1] * dims[2] * dims[3]);
-    if (comp < 0) mxLL = m;
-    else mxSS = fmax(mxSS, m);
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const size_t e1 = P.s1 + (size_t)P.s2 * nshell, e2 = P.s2 + (size_t)P.s1 * nshell;
-    if (needLL) qLL[e1] = qLL[e2] = sqrt(mxLL);
-    if (needSS) {
-      const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
-      qSS[e1] = qSS[e2] = C2 * sqrt(mxSS);
-    }
+  if (!live) return;
+  double m = 0.0;
+  const int tot = dims[0] * dims[1] * dims[2] * dims[3];
+  for (int e = g0; e < tot; e += gsize) m = fmax(m, fabs(cur[e]));
+  if (m > 0.0)
+    atomicMax(mx + 2 * (size_t)ip + (dc >= 0 ? 1 : 0),
+              (unsigned long long)__double_as_longlong(m));
+}
+
+// Q^LL = sqrt(max), Q^SS = C2 sqrt(max) of each pair of a class into both
+// triangles of the nshell x nshell tables (direct4C_libcint.hpp:388-394,
+// :464-470).
+__global__ void rel_schwarz_finish_kernel(const PairDev* __restrict__ pairs, int beg, int npair,
+                                          const unsigned long long* __restrict__ mx,
+                                          int needLL, int needSS, int nshell, double* qLL,
+                                          double* qSS) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= npair) return;
+  const PairDev P = pairs[beg + ip];
+  const size_t e1 = P.s1 + (size_t)P.s2 * nshell, e2 = P.s2 + (size_t)P.s1 * nshell;
+  if (needLL) qLL[e1] = qLL[e2] = sqrt(__longlong_as_double((long long)mx[2 * ip]));
+  if (needSS) {
+    const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
+    qSS[e1] = qSS[e2] = C2 * sqrt(__longlong_as_double((long long)mx[2 * ip + 1]));
   }
 }
 
@@ -1347,27 +1362,47 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream
     CQF_RCUDA(cudaMemsetAsync(B->d_qSS, 0, ns2 * sizeof(double), B->stream));
   }
   CQF_RCUDA(cudaStreamSynchronize(B->stream));
+  unsigned long long* mx = nullptr;
+  CQF_RCUDA(cudaMallocAsync(&mx, 2 * (size_t)std::max(1, B->npair) * sizeof(unsigned long long),
+                            st));
+  CQF_RCUDA(cudaMemsetAsync(mx, 0, 2 * (size_t)std::max(1, B->npair) * sizeof(unsigned long long),
+                            st));
+  const int ncomp = (needLL ? 1 : 0) + (needSS ? 81 : 0);
   for (int c = 0; c < NCLS; c++) {
     if (B->cls_cnt[c] <= 0) continue;
     int la, lb;
     class_ls(c, la, lb);
     const int n4 = ncart(la) * ncart(lb) * ncart(la) * ncart(lb);
-    const size_t smem = 2 * (size_t)n4 * sizeof(double);
+    // threads per (pair, component): at least a warp, and the Cartesian
+    // column count rounded up to a power of two (the spare threads split the
+    // bra primitive pairs)
+    int cpow = 1;
+    while (cpow < ncart(la) * ncart(lb)) cpow *= 2;
+    const int gsize = std::min(SCH_THREADS, std::max(32, cpow));
+    const int groups = SCH_THREADS / gsize;
+    const size_t smem = (size_t)groups * 2 * n4 * sizeof(double);
+    const long long units = (long long)B->cls_cnt[c] * ncomp;
+    const unsigned nblk = (unsigned)((units + groups - 1) / groups);
+    unsigned long long* mxc = mx + 2 * (size_t)B->cls_beg[c];
     const int lm = std::max(la, 1);
-#define CQF_SCH(LMV)                                                                         \
-  if (lm == LMV) {                                                                           \
-    CQF_RCUDA(cudaFuncSetAttribute(rel_schwarz_kernel<LMV>,                                  \
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    rel_schwarz_kernel<LMV><<<B->cls_cnt[c], SCH_THREADS, smem, st>>>(                       \
-        B->d_pairs, B->d_pp, B->d_shells, B->d_prim, B->d_boys64, B->d_sph, B->d_sphOff,     \
-        B->cls_beg[c], la, lb, needLL, needSS, B->nshell, B->d_qLL, B->d_qSS);               \
+#define CQF_SCH(LMV)                                                                          \
+  if (lm == LMV) {                                                                            \
+    CQF_RCUDA(cudaFuncSetAttribute(rel_schwarz_kernel<LMV>,                                   \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
+    rel_schwarz_kernel<LMV><<<nblk, SCH_THREADS, smem, st>>>(                                 \
+        B->d_pairs, B->d_pp, B->d_shells, B->d_prim, B->d_boys64, B->d_sph, B->d_sphOff,      \
+        B->cls_beg[c], B->cls_cnt[c], la, lb, ncomp, needLL ? 1 : 0, gsize, cpow, mxc);       \
   }
     CQF_SCH(1)
     CQF_SCH(2)
     CQF_SCH(3)
 #undef CQF_SCH
+    rel_schwarz_finish_kernel<<<(B->cls_cnt[c] + 127) / 128, 128, 0, st>>>(
+        B->d_pairs, B->cls_beg[c], B->cls_cnt[c], mxc, needLL, needSS, B->nshell, B->d_qLL,
+        B->d_qSS);
     CQF_RCUDA(cudaGetLastError());
   }
+  cudaFreeAsync(mx, st);
   if (needLL) {
     B->h_qLL.resize(ns2);
     CQF_RCUDA(cudaMemcpyAsync(B->h_qLL.data(), B->d_qLL, ns2 * sizeof(double),
