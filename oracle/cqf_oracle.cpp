@@ -1805,6 +1805,18 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
 // GTODirectRelERIContraction::twoBodyContract on the 17 N x N complex
 // (X, AX) entries in DIRAC_PAULI_SPINOR_COMP order; AX is zeroed first
 // (direct4C_libcint.hpp:313-314).
+// Derivative ERIs of one contracted shell quartet (eri_deriv_quartet):
+// comp-major blocks over the AO functions of s1..s4, derivatives (d/dr of
+// the orbital) on the centres in dmask (bit 0..3 = s1..s4); returns the
+// number of values written.
+int orc_eri_deriv_quartet(void* b, int s1, int s2, int s3, int s4, int dmask, double* out) {
+  const auto* bs = static_cast<const Basis*>(b);
+  std::vector<double> buf;
+  eri_deriv_quartet(*bs, s1, s2, s3, s4, dmask, buf);
+  std::copy(buf.begin(), buf.end(), out);
+  return (int)buf.size();
+}
+
 int orc_rel_contract(void* b, int type, const void* const* Xv, void* const* AXv, double thresh,
                      int exchange) {
   auto* bs = static_cast<Basis*>(b);

@@ -65,6 +65,9 @@ def lib():
         L.orc_rel_contract.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                        C.POINTER(C.c_void_p), C.c_double, C.c_int]
         L.orc_rel_contract.restype = C.c_int
+        L.orc_eri_deriv_quartet.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, dp]
+        L.orc_eri_deriv_quartet.restype = C.c_int
         _lib = L
     return _lib
 
@@ -143,6 +146,16 @@ class OracleBasis:
         out = np.zeros(int(np.prod(n)) * 16)
         k = lib().orc_eri_quartet(self.h, s1, s2, s3, s4, _dp(out))
         return out[:k].reshape(n)
+
+    def eri_deriv_quartet(self, s1, s2, s3, s4, dmask):
+        """(ncomp, n1, n2, n3, n4) derivative ERIs, derivatives (d/dr of the
+        orbital) on the centres in dmask (bit 0..3 = s1..s4); component index
+        over the differentiated centres in order, the last fastest."""
+        n = [int(self.sizes[s]) for s in (s1, s2, s3, s4)]
+        nd = bin(dmask & 15).count("1")
+        out = np.zeros(3 ** nd * int(np.prod(n)))
+        k = lib().orc_eri_deriv_quartet(self.h, s1, s2, s3, s4, dmask, _dp(out))
+        return out[:k].reshape([3 ** nd] + n)
 
     def schwarz(self):
         Q = np.zeros((self.nshell, self.nshell), order="F")
