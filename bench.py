@@ -56,7 +56,7 @@ sys.path.insert(0, ROOT)
 METRIC = ("Fock builds/s (mixed vs FP64, same B200) at <=1e-6 Eh Fock err; "
           "p50/p99 latency")
 # DRAM bytes of one mixed build from an ncu capture (profiles/), by workload
-TRAFFIC_BYTES = {}
+TRAFFIC_BYTES = {"h2o16_def2svp": 1.32e8}
 
 
 def parse():
@@ -161,6 +161,36 @@ def fma_peaks():
     L.cqf_fma_peak_tflops.restype = ctypes.c_double
     L.cqf_fma_peak_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
     return L.cqf_fma_peak_tflops(1, 4096), L.cqf_fma_peak_tflops(0, 16384)
+
+
+def build_launches(basis, Q, mixed):
+    """Kernels one closed-shell J+K build launches (l <= 2 bases): block
+    norms x2, max, norms_aux, Cartesian transforms x2, the FP32 density copy
+    (mixed), per class pair and bra slab the planning pass and the FP64 (and
+    FP32) class kernel, back transforms x2.  Class sizes are the significant
+    pairs (nonzero Schwarz bound) per angular-momentum class; the slab size
+    is the library's mask region (2^18 words per stream)."""
+    sys.path.insert(0, os.path.join(ROOT, "chronusq_public_b200", "csrc"))
+    from gen_jk import orientation
+    ls = [s.l for s in basis.shells]
+    cnt = {}
+    for i in range(basis.nshell):
+        for j in range(i + 1):
+            if Q[i, j] > 0.0:
+                c = (max(ls[i], ls[j]), min(ls[i], ls[j]))
+                cnt[c] = cnt.get(c, 0) + 1
+    cls = sorted(cnt)
+    tiles = lambda n: (n + 31) // 32
+    need = max([max(cnt[a] * tiles(cnt[b]), cnt[b] * tiles(cnt[a]))
+                for i, a in enumerate(cls) for b in cls[:i + 1]] + [0])
+    words = max(max(tiles(n) for n in cnt.values()), min(need, 1 << 18))
+    n = 2 + 1 + 1 + 2 + (1 if mixed else 0) + 2
+    for i, a in enumerate(cls):
+        for b in cls[:i + 1]:
+            bra, ket = orientation(a, b)
+            slab = max(1, words // tiles(cnt[ket]))
+            n += (-(-cnt[bra] // slab)) * (3 if mixed else 2)
+    return n
 
 
 def oracle_module():
@@ -873,11 +903,7 @@ def main():
         sw["fock_maxabs"] = float(np.abs(Gc - Gref).max())
         sw["energy_err"] = abs(two_electron_energy(Gc, D) - two_electron_energy(Gref, D))
         sw["errors_against"] = "oracle" if cpu else "FP64 GPU build"
-    # kernels per mixed build: block norms x2, max, norms_aux, to_cart x2,
-    # the FP32 density copy, per class pair the planning pass and the FP64
-    # and FP32 class kernels, back transform x2
-    ncls = len({(max(a.l, b.l), min(a.l, b.l)) for a in basis.shells for b in basis.shells})
-    launches_per_step = 2 + 1 + 1 + 2 + 1 + 3 * (ncls * (ncls + 1) // 2) + 2
+    launches_per_step = build_launches(basis, Q, mixed=True)
     line = {
         "metric": METRIC, "value": vmx, "unit": "builds/s", "n_gpus": ws,
         "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / K,
