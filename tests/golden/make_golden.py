@@ -16,6 +16,9 @@ Sources (paths within xsligroup/chronusq_public):
   tests/scf/serial/rhf/water_cc-pVDZ_RHF_READDEN.inp.
 * tests/scf/reference/water_cc-pVDZ_DC-HF_RHFGuess_READDEN.bin.ref -- one 4C
   Dirac-Coulomb build (tests/scf/fourcomphf.cxx:143-150).
+* tests/scf/reference/UPu_184+_P_DCG_finitenuc.bin.ref and CuH3_321g_DCG.bin.ref
+  -- converged 4C Dirac-Coulomb-Gaunt SCFs (inputs under
+  tests/scf/serial/fourcomp/): D and G = F - H of the final build.
 
 HDF5 datasets written from column-major buffers read back transposed; the
 fixtures store them in natural (row = first index) orientation.
@@ -41,6 +44,27 @@ CONTRACT_CASES = [
 def _inline_basis(inp_path):
     txt = open(inp_path).read()
     return txt.split("BasisDef:")[1].split("[MISC]")[0]
+
+
+def _geometry(text):
+    """The [Molecule] geom: lines as 'Sym x y z' strings (Angstrom)."""
+    lines = text.splitlines()
+    i = [k for k, l in enumerate(lines) if l.strip().lower().startswith("geom")][0]
+    out = []
+    for l in lines[i + 1:]:
+        t = l.split()
+        if len(t) != 4 or not t[0].isalpha():
+            break
+        out.append(" ".join(t))
+    return "\n".join(out)
+
+
+def _basis_name(text):
+    for l in text.splitlines():
+        t = l.replace("=", " ").split()
+        if len(t) == 2 and t[0].lower() == "basis":
+            return t[1].lower()
+    raise ValueError("no basis name")
 
 
 def main(ref_root):
@@ -105,6 +129,29 @@ def main(ref_root):
         out["D_" + comp] = np.where(np.abs(D) < 1e-200, 0, D).copy()
         out["G_" + comp] = np.where(np.abs(G) < 1e-200, 0, G).copy()
     np.savez_compressed(os.path.join(HERE, "qn_4chf_dc.npz"), **out)
+
+    # converged four-component Dirac-Coulomb-Gaunt SCF references (bare
+    # Coulomb + Dirac-Coulomb LLSS + Gaunt, SSSS off, libcint, in-core
+    # integrals): D and G = F - H of the final build, with the molecule and
+    # basis of each input
+    for name, inp, key in [
+            ("UPu_184+_P_DCG_finitenuc", "tests/scf/serial/fourcomp/UPu_184+_P_DCG_finitenuc.inp",
+             "gaunt_upu"),
+            ("CuH3_321g_DCG", "tests/scf/serial/fourcomp/CuH3_321g_DCG.inp", "gaunt_cuh3")]:
+        f = H5File(os.path.join(rd, name + ".bin.ref"))
+        out = {}
+        for comp in ("SCALAR", "MX", "MY", "MZ"):
+            D = f.read("/SCF/1PDM_" + comp).T
+            G = f.read("/SCF/FOCK_" + comp).T - f.read("/INTS/CORE_HAMILTONIAN_" + comp).T
+            out["D_" + comp] = np.where(np.abs(D) < 1e-200, 0, D).copy()
+            out["G_" + comp] = np.where(np.abs(G) < 1e-200, 0, G).copy()
+        text = open(os.path.join(ref_root, inp)).read()
+        out["geometry"] = np.array(_geometry(text))
+        if "DefineBasis" in text:
+            out["basisdef"] = np.array(_inline_basis(os.path.join(ref_root, inp)))
+        else:
+            out["basisname"] = np.array(_basis_name(text))
+        np.savez_compressed(os.path.join(HERE, key + ".npz"), **out)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,49 @@
+"""The Gaunt term restated from two-spinor physics (tests/twospinor.py),
+pinned to the reference's converged Dirac-Coulomb-Gaunt SCF builds
+(tests/scf/reference/UPu_184+_P_DCG_finitenuc.bin.ref and
+CuH3_321g_DCG.bin.ref; bare Coulomb + LLSS + Gaunt, SSSS off, libcint):
+G_golden = F - H must equal the oracle's bare Coulomb + LLSS build plus the
+restated Gaunt matrix on the stored density, every block and Pauli
+component.  CPU only."""
+import numpy as np
+import pytest
+
+import oracle as O
+import twospinor as TS
+from chronusq_public_b200.basis import BasisSet, Molecule, parse_gbs
+from helpers import golden
+
+COMPS = ("SCALAR", "MX", "MY", "MZ")
+
+
+def _system(name):
+    g = golden(name)
+    atoms = []
+    for line in str(g["geometry"]).splitlines():
+        s, x, y, z = line.split()
+        atoms.append((s, float(x), float(y), float(z)))
+    mol = Molecule.from_angstrom(atoms)
+    if "basisdef" in g:
+        basis = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
+    else:
+        basis = BasisSet.build(mol, str(g["basisname"]))
+    D = [np.asarray(g["D_" + c]) for c in COMPS]
+    G = [np.asarray(g["G_" + c]) for c in COMPS]
+    return basis, D, G
+
+
+@pytest.mark.parametrize("name", ["gaunt_upu.npz", "gaunt_cuh3.npz"])
+def test_gaunt_reproduces_reference_dcg_build(name):
+    basis, D, Gref = _system(name)
+    assert 2 * basis.nbasis == D[0].shape[0]
+    ob = O.OracleBasis(basis)
+    Gdc = ob.dirac_coulomb(D, bare=True, dc=True, ssss=False, libcint=True)
+    Gg = TS.gaunt(basis, D)
+    scale = max(np.abs(g).max() for g in Gref)
+    gaunt_size = max(np.abs(g).max() for g in Gg)
+    for c in range(4):
+        err = np.abs(Gdc[c] + Gg[c] - Gref[c]).max()
+        assert err < 1e-8 * max(1.0, scale), (COMPS[c], err, scale)
+    # the Gaunt term is visible at this tolerance (the check is not vacuous)
+    miss = max(np.abs(Gdc[c] - Gref[c]).max() for c in range(4))
+    assert miss > 1e3 * 1e-8 * max(1.0, scale), (miss, gaunt_size)

@@ -24,12 +24,8 @@ import pytest
 
 import oracle as O
 from chronusq_public_b200.basis import BasisSet
-from chronusq_public_b200.workloads import SPEED_OF_LIGHT
 from helpers import water_ref
-
-SIG = np.array([[[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]]], dtype=complex)
-# sigma_i sigma_j, (3, 3, 2, 2)
-SS = np.einsum("iab,jbc->ijac", SIG, SIG)
+from twospinor import C2, SS, deriv_tensor as _tensor, pauli as _pauli, spin_blocks as _spin_blocks
 
 
 @pytest.fixture(scope="module")
@@ -92,46 +88,6 @@ def test_four_centre_derivative_eris_match_finite_differences(water):
         assert np.abs(der[comp] - fd).max() < 2e-3 * np.abs(fd).max(), (i, j, k, l)
 
 
-def _tensor(basis, dmask):
-    """Full (ncomp, N, N, N, N) derivative ERI tensor of the basis."""
-    ob = O.OracleBasis(basis)
-    N = basis.nbasis
-    nd = bin(dmask).count("1")
-    out = np.zeros((3 ** nd, N, N, N, N))
-    off, sz = basis.offsets, basis.sizes
-    ns = basis.nshell
-    for a in range(ns):
-        for b in range(ns):
-            for c in range(ns):
-                for d in range(ns):
-                    blk = ob.eri_deriv_quartet(a, b, c, d, dmask)
-                    out[:, off[a]:off[a] + sz[a], off[b]:off[b] + sz[b],
-                        off[c]:off[c] + sz[c], off[d]:off[d] + sz[d]] = blk
-    return out.reshape((3,) * nd + (N, N, N, N))
-
-
-def _spin_blocks(M, N):
-    """Pauli components [S, X, Y, Z] (2N x 2N, LL first) -> the four spatial
-    blocks LL, LS, SL, SS as spin-orbital arrays [mu, s, nu, s']."""
-    S, X, Y, Z = M
-    out = {}
-    for name, (r, c) in {"LL": (0, 0), "LS": (0, 1), "SL": (1, 0), "SS": (1, 1)}.items():
-        sl = (slice(r * N, (r + 1) * N), slice(c * N, (c + 1) * N))
-        b = np.zeros((N, 2, N, 2), dtype=complex)
-        b[:, 0, :, 0] = (S[sl] + Z[sl]) / 2
-        b[:, 1, :, 1] = (S[sl] - Z[sl]) / 2
-        b[:, 0, :, 1] = (X[sl] - 1j * Y[sl]) / 2
-        b[:, 1, :, 0] = (X[sl] + 1j * Y[sl]) / 2
-        out[name] = b
-    return out
-
-
-def _pauli(b):
-    """Spin-orbital block [mu, s, nu, s'] -> Pauli components [S, X, Y, Z]."""
-    aa, bb, ab, ba = b[:, 0, :, 0], b[:, 1, :, 1], b[:, 0, :, 1], b[:, 1, :, 0]
-    return [aa + bb, ab + ba, 1j * (ab - ba), aa - bb]
-
-
 @pytest.fixture(scope="module")
 def four_comp(water):
     N = water.nbasis
@@ -152,7 +108,6 @@ def _block(G, N, r, c):
 
 def test_llss_and_ssss_from_two_spinors(water, four_comp):
     N, D, g_llss, g_ssss = four_comp
-    C2 = 1.0 / (4.0 * SPEED_OF_LIGHT ** 2)
     Db = _spin_blocks(D, N)
     I3 = _tensor(water, 3)     # (d_i mu d_j nu | ka la)
     I12 = _tensor(water, 12)   # (mu nu | d_k ka d_l la)
