@@ -1718,6 +1718,193 @@ void direct_4c(const Basis& bs, int type, const cdbl* const* X, cdbl* const* AX,
       for (int j = 0; j < i; j++) AX[m][j + (size_t)i * N] = std::conj(AX[m][i + (size_t)j * N]);
 }
 
+// ---------------------------------------------------------------- Gaunt
+// The Gaunt term -alpha_1.alpha_2 / r12 (direct4C_libcint.hpp:2833-3907).
+// Its 29-entry list continues DIRAC_PAULI_SPINOR_COMP with the LS Coulomb,
+// SL Coulomb and SL exchange entries (:279-310).
+enum { CLSMS = NREL, CLSMX, CLSMY, CLSMZ, CSLMS, CSLMX, CSLMY, CSLMZ, XSLMS, XSLMX, XSLMY, XSLMZ,
+       NGAUNT };
+
+// The 3 x 3 derivative block T[j][l] = (m d_j n | d_l k l) of one element,
+// d/dr of the orbital on the second and third function, as the invariants
+// the spin algebra needs: t = tr T, the cross vector tau = (T_yz - T_zy,
+// T_zx - T_xz, T_xy - T_yx) and S' = T + T^T - t I.  The transposed block
+// T^T has the same t and S' and -tau.
+struct GT {
+  double T[3][3], t, tau[3], Sp[3][3];
+};
+GT gt_of(const double* v, bool transpose) {
+  GT g;
+  for (int j = 0; j < 3; j++)
+    for (int l = 0; l < 3; l++) g.T[j][l] = transpose ? v[3 * l + j] : v[3 * j + l];
+  g.t = g.T[0][0] + g.T[1][1] + g.T[2][2];
+  g.tau[0] = g.T[1][2] - g.T[2][1];
+  g.tau[1] = g.T[2][0] - g.T[0][2];
+  g.tau[2] = g.T[0][1] - g.T[1][0];
+  for (int j = 0; j < 3; j++)
+    for (int l = 0; l < 3; l++) g.Sp[j][l] = g.T[j][l] + g.T[l][j] - (j == l ? g.t : 0.0);
+  return g;
+}
+
+// Spin algebra of the four update kinds.  With two-spinor charge densities
+// rho^k_LS = (-i/2c) sum_j (s_k s_j) chi d_j chi, rho^k_SL its adjoint, and
+// the identities sum_k s_k X s_k = 2 tr(X) - X and
+// sum_jl T_jl s_j (d0 + d.s) s_l = d0 t - i d.tau + (i d0 tau + S' d).s,
+// every update is a fixed 4 x 4 complex map of Pauli components (storage
+// scale S = 2 d0 etc. carries through, the maps being linear):
+//   LL exchange from the SS density  (:3436-3480):  3 (d0 t - i d.tau), -(i d0 tau + S' d)
+//   SS exchange from the LL density  (:3487-3535):  3 d0 t - i d.tau, -3 i d0 tau - S' d
+//   LS Coulomb from SL (1) and LS (2) (:3541-3610): (d1_0 - d2_0) t + i (d1 + d2).tau,
+//                                       i (d2_0 - d1_0) tau + (T^T - t)(d1 + d2)
+//   LS exchange from the SL density  (:3613-3680):  d0 t - i d.tau, i d0 tau + S' d - 4 T^T d
+Q4 g_ll(const GT& g, const Q4& d) {
+  Q4 r;
+  cdbl dt = d.v[0] * g.tau[0] + d.v[1] * g.tau[1] + d.v[2] * g.tau[2];
+  r.s = 3.0 * (d.s * g.t - I1 * dt);
+  for (int x = 0; x < 3; x++)
+    r.v[x] = -(I1 * d.s * g.tau[x] + g.Sp[x][0] * d.v[0] + g.Sp[x][1] * d.v[1] + g.Sp[x][2] * d.v[2]);
+  return r;
+}
+Q4 g_ss(const GT& g, const Q4& d) {
+  Q4 r;
+  cdbl dt = d.v[0] * g.tau[0] + d.v[1] * g.tau[1] + d.v[2] * g.tau[2];
+  r.s = 3.0 * d.s * g.t - I1 * dt;
+  for (int x = 0; x < 3; x++)
+    r.v[x] = -3.0 * I1 * d.s * g.tau[x] -
+             (g.Sp[x][0] * d.v[0] + g.Sp[x][1] * d.v[1] + g.Sp[x][2] * d.v[2]);
+  return r;
+}
+Q4 g_cls(const GT& g, const Q4& d1, const Q4& d2) {
+  Q4 r;
+  cdbl e[3];
+  for (int x = 0; x < 3; x++) e[x] = d1.v[x] + d2.v[x];
+  r.s = (d1.s - d2.s) * g.t + I1 * (e[0] * g.tau[0] + e[1] * g.tau[1] + e[2] * g.tau[2]);
+  for (int x = 0; x < 3; x++)
+    r.v[x] = I1 * (d2.s - d1.s) * g.tau[x] + g.T[0][x] * e[0] + g.T[1][x] * e[1] +
+             g.T[2][x] * e[2] - g.t * e[x];
+  return r;
+}
+Q4 g_xls(const GT& g, const Q4& d) {
+  Q4 r;
+  cdbl dt = d.v[0] * g.tau[0] + d.v[1] * g.tau[1] + d.v[2] * g.tau[2];
+  r.s = d.s * g.t - I1 * dt;
+  for (int x = 0; x < 3; x++) {
+    r.v[x] = I1 * d.s * g.tau[x];
+    for (int y = 0; y < 3; y++) r.v[x] += (g.Sp[x][y] - 4.0 * g.T[y][x]) * d.v[y];
+  }
+  return r;
+}
+
+// SchwarzGaunt (:2910-2955): Q^G(s1, s2) = C1 sqrt(max |(d s1 s2 | d s1 s2)|)
+// over the 9 components and the block, derivatives on the first function of
+// each pair, C1 = 1 / 2c; not symmetric in (s1, s2).
+void schwarz_gaunt(const Basis& bs, std::vector<double>& QG) {
+  const int ns = (int)bs.shells.size();
+  const double C1 = 1.0 / (2.0 * 137.035999074);
+  QG.assign((size_t)ns * ns, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int s1 = 0; s1 < ns; s1++) {
+    std::vector<double> buf;
+    for (int s2 = 0; s2 < ns; s2++) {
+      eri_deriv_quartet(bs, s1, s2, s1, s2, 5, buf);
+      double mx = 0;
+      for (double v : buf) mx = std::max(mx, std::abs(v));
+      QG[s1 + (size_t)s2 * ns] = C1 * std::sqrt(mx);
+    }
+  }
+}
+
+// The Gaunt contraction on the 29 (X, AX) entries; AX is zeroed first.
+// Quartets (:2996-3160): s1, s2 over all shells, s3 <= s2, s4 <= (s2 == s3 ?
+// s1 : last) -- every unordered pair of (differentiated, other) shell pairs
+// (s2, s1), (s3, s4) once -- screened by max shell-block norm of the 16
+// exchange densities times Q^G(s3, s4) Q^G(s2, s1).  Per element (m n | k l)
+// the reference's update sites and conditions (:3436-3680), with T and, for
+// the image (l k | n m), T^T; then LL and SS exchange get their upper
+// triangles from the lower ones (:3833-3858).
+void direct_gaunt(const Basis& bs, const cdbl* const* X, cdbl* const* AX, double thresh,
+                  const std::vector<double>& QG, bool exchange) {
+  const int ns = (int)bs.shells.size(), N = bs.nbasis;
+  const size_t NN = (size_t)N * N;
+  for (int m = 0; m < NGAUNT; m++) std::fill(AX[m], AX[m] + NN, cdbl(0.0));
+  std::vector<double> nrm((size_t)ns * ns, 0.0), tmp;
+  for (int base : {(int)XLSMS, (int)XSLMS, (int)XLLMS, (int)XSSMS})
+    for (int c = 0; c < 4; c++) {
+      norms_c(bs, X[base + c], tmp);
+      for (size_t i = 0; i < nrm.size(); i++) nrm[i] = std::max(nrm[i], std::abs(tmp[i]));
+    }
+  auto B = [&](int a, int b) { return nrm[a + (size_t)b * ns]; };
+  const int nth = omp_get_max_threads();
+  std::vector<cdbl> loc((size_t)nth * NGAUNT * NN, cdbl(0.0));
+#pragma omp parallel
+  {
+    const int tid = omp_get_thread_num();
+    cdbl* A[NGAUNT];
+    for (int m = 0; m < NGAUNT; m++) A[m] = &loc[((size_t)tid * NGAUNT + m) * NN];
+    auto ix = [N](int r, int c) { return (size_t)r + (size_t)c * N; };
+    auto put = [&](int base, size_t e, const Q4& q) {
+      A[base][e] += q.s;
+      for (int x = 0; x < 3; x++) A[base + 1 + x][e] += q.v[x];
+    };
+    std::vector<double> buf;
+    size_t s1234 = 0;
+    for (int s1 = 0; s1 < ns; s1++)
+      for (int s2 = 0; s2 < ns; s2++) {
+        const double shMax12 = B(s2, s1);
+        for (int s3 = 0; s3 <= s2; s3++) {
+          const double shMax123 = std::max(std::max(B(s1, s3), B(s2, s3)), shMax12);
+          const int s4max = (s2 == s3) ? s1 : ns - 1;
+          for (int s4 = 0; s4 <= s4max; s4++, s1234++) {
+            if (s1234 % nth != (size_t)tid) continue;
+            double shMax = std::max(B(s1, s4), std::max(B(s2, s4), B(s3, s4)));
+            shMax = std::max(shMax, shMax123);
+            if (shMax * QG[s3 + (size_t)s4 * ns] * QG[s2 + (size_t)s1 * ns] < thresh) continue;
+            eri_deriv_quartet(bs, s1, s2, s3, s4, 6, buf);
+            const int n1 = bs.shells[s1].size(), n2 = bs.shells[s2].size();
+            const int n3 = bs.shells[s3].size(), n4 = bs.shells[s4].size();
+            const size_t nq = (size_t)n1 * n2 * n3 * n4;
+            const bool img = (s1 != s4) || (s2 != s3);
+            for (int i = 0; i < n1; i++)
+              for (int j = 0; j < n2; j++)
+                for (int k = 0; k < n3; k++)
+                  for (int l = 0; l < n4; l++) {
+                    const int m1 = bs.off[s1] + i, m2 = bs.off[s2] + j;
+                    const int m3 = bs.off[s3] + k, m4 = bs.off[s4] + l;
+                    const size_t q = (((size_t)i * n2 + j) * n3 + k) * n4 + l;
+                    double v[9];
+                    for (int c = 0; c < 9; c++) v[c] = buf[(size_t)c * nq + q];
+                    const GT T = gt_of(v, false), Tt = gt_of(v, true);
+                    if (exchange) {
+                      if (s1 >= s4) put(XLLMS, ix(m1, m4), g_ll(T, dens(X, XSSMS, ix(m2, m3))));
+                      if (s1 < s4 || (s1 == s4 && s2 != s3))
+                        put(XLLMS, ix(m4, m1), g_ll(Tt, dens(X, XSSMS, ix(m3, m2))));
+                      put(XSSMS, ix(m2, m3), g_ss(Tt, dens(X, XLLMS, ix(m1, m4))));
+                      if (s1 != s4 && s2 == s3)
+                        put(XSSMS, ix(m3, m2), g_ss(T, dens(X, XLLMS, ix(m4, m1))));
+                    }
+                    put(CLSMS, ix(m1, m2),
+                        g_cls(T, dens(X, CSLMS, ix(m3, m4)), dens(X, CLSMS, ix(m4, m3))));
+                    if (img)
+                      put(CLSMS, ix(m4, m3),
+                          g_cls(Tt, dens(X, CSLMS, ix(m2, m1)), dens(X, CLSMS, ix(m1, m2))));
+                    if (exchange) {
+                      put(XLSMS, ix(m1, m3), g_xls(T, dens(X, XSLMS, ix(m2, m4))));
+                      if (img) put(XLSMS, ix(m4, m2), g_xls(Tt, dens(X, XSLMS, ix(m3, m1))));
+                    }
+                  }
+          }
+        }
+      }
+  }
+  for (int t = 0; t < nth; t++)
+    for (int m = 0; m < NGAUNT; m++)
+      for (size_t e = 0; e < NN; e++) AX[m][e] += loc[((size_t)t * NGAUNT + m) * NN + e];
+  if (!exchange) return;
+  for (int m : {XLLMS, XLLMX, XLLMY, XLLMZ, XSSMS, XSSMX, XSSMY, XSSMZ})
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < i; j++) AX[m][j + (size_t)i * N] = std::conj(AX[m][i + (size_t)j * N]);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1731,7 +1918,7 @@ extern "C" {
 // (fourcompfock/impl.hpp:3901-3933), without it the 1C J/K contraction and
 // twoeH_LL = J (:3934-3969).
 int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare, int dc,
-                      int ssss, double xHFX, double thresh, int libcint) {
+                      int ssss, double xHFX, double thresh, int libcint, int gaunt) {
   auto* bs = static_cast<Basis*>(b);
   const int N = bs->nbasis, N2 = 2 * N;
   const cdbl* const* D = reinterpret_cast<const cdbl* const*>(Dv);
@@ -1739,26 +1926,29 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
   const double c = 137.035999074, C2 = 1.0 / (4 * c * c), C4 = 1.0 / (16 * c * c * c * c);
   const bool exch = std::abs(xHFX) >= 1e-12;
   const size_t NN = (size_t)N * N, NN2 = (size_t)N2 * N2;
-  // blocks LL, SS, LS of each Pauli component
-  std::vector<cdbl> blk[3][4];
+  // blocks LL, SS, LS, SL of each Pauli component
+  std::vector<cdbl> blk[4][4];
+  const int bro[4] = {0, N, 0, N}, bco[4] = {0, N, N, 0};
   for (int cmp = 0; cmp < 4; cmp++)
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < 4; k++) {
       blk[k][cmp].assign(NN, 0.0);
-      const int ro = (k == 1) ? N : 0, co = (k == 0) ? 0 : N;  // LL (0,0) SS (N,N) LS (0,N)
       for (int j = 0; j < N; j++)
         for (int i = 0; i < N; i++)
-          blk[k][cmp][i + (size_t)j * N] = D[cmp][(ro + i) + (size_t)(co + j) * N2];
+          blk[k][cmp][i + (size_t)j * N] = D[cmp][(bro[k] + i) + (size_t)(bco[k] + j) * N2];
     }
-  std::vector<cdbl> ax((size_t)NREL * NN);
-  const cdbl* X[NREL];
-  cdbl* AX[NREL];
-  for (int m = 0; m < NREL; m++) AX[m] = &ax[(size_t)m * NN];
+  std::vector<cdbl> ax((size_t)NGAUNT * NN);
+  const cdbl* X[NGAUNT];
+  cdbl* AX[NGAUNT];
+  for (int m = 0; m < NGAUNT; m++) AX[m] = &ax[(size_t)m * NN];
   X[CLLMS] = blk[0][0].data();
   for (int c4 = 0; c4 < 4; c4++) {
     X[XLLMS + c4] = blk[0][c4].data();
     X[CSSMS + c4] = blk[1][c4].data();
     X[XSSMS + c4] = blk[1][c4].data();
     X[XLSMS + c4] = blk[2][c4].data();
+    X[CLSMS + c4] = blk[2][c4].data();
+    X[CSLMS + c4] = blk[3][c4].data();
+    X[XSLMS + c4] = blk[3][c4].data();
   }
   std::vector<cdbl> twoeH[4], K[4];
   for (int c4 = 0; c4 < 4; c4++) {
@@ -1790,6 +1980,18 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
     if (exch)
       for (int c4 = 0; c4 < 4; c4++) add(K[c4], N, N, AX[XSSMS + c4], -C4);
   }
+  if (gaunt) {  // impl.hpp:4235-4376
+    std::vector<double> QG;
+    schwarz_gaunt(*bs, QG);
+    direct_gaunt(*bs, X, AX, thresh, QG, exch);
+    for (int c4 = 0; c4 < 4; c4++) add(twoeH[c4], 0, N, AX[CLSMS + c4], 2.0 * C2);
+    if (exch)
+      for (int c4 = 0; c4 < 4; c4++) {
+        add(K[c4], 0, 0, AX[XLLMS + c4], -C2);
+        add(K[c4], N, N, AX[XSSMS + c4], -C2);
+        add(K[c4], 0, N, AX[XLSMS + c4], -C2);
+      }
+  }
   // LS -> SL as the conjugate transpose, then G = twoeH - xHFX K
   for (int c4 = 0; c4 < 4; c4++) {
     for (auto* M : {&twoeH[c4], &K[c4]})
@@ -1801,10 +2003,10 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
   return 0;
 }
 
-// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS) of
-// GTODirectRelERIContraction::twoBodyContract on the 17 N x N complex
-// (X, AX) entries in DIRAC_PAULI_SPINOR_COMP order; AX is zeroed first
-// (direct4C_libcint.hpp:313-314).
+// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS, 3 GAUNT) of
+// GTODirectRelERIContraction::twoBodyContract on the N x N complex (X, AX)
+// entries in DIRAC_PAULI_SPINOR_COMP order (17, or 29 for GAUNT); AX is
+// zeroed first (direct4C_libcint.hpp:313-314).
 // Derivative ERIs of one contracted shell quartet (eri_deriv_quartet):
 // comp-major blocks over the AO functions of s1..s4, derivatives (d/dr of
 // the orbital) on the centres in dmask (bit 0..3 = s1..s4); returns the
@@ -1822,6 +2024,12 @@ int orc_rel_contract(void* b, int type, const void* const* Xv, void* const* AXv,
   auto* bs = static_cast<Basis*>(b);
   const cdbl* const* X = reinterpret_cast<const cdbl* const*>(Xv);
   cdbl* const* AX = reinterpret_cast<cdbl* const*>(AXv);
+  if (type == 3) {
+    std::vector<double> QG;
+    schwarz_gaunt(*bs, QG);
+    direct_gaunt(*bs, X, AX, thresh, QG, exchange != 0);
+    return 0;
+  }
   Schwarz4C Qs;
   schwarz_4c(*bs, type <= 1, type >= 1, Qs);
   direct_4c(*bs, type, X, AX, thresh, Qs, exchange != 0);

@@ -60,7 +60,7 @@ def lib():
                                 C.c_double, C.c_double, dp]
         L.orc_dirac_coulomb.argtypes = [C.c_void_p, C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p), C.c_int, C.c_int,
-                                        C.c_int, C.c_double, C.c_double, C.c_int]
+                                        C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
         L.orc_dirac_coulomb.restype = C.c_int
         L.orc_rel_contract.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                        C.POINTER(C.c_void_p), C.c_double, C.c_int]
@@ -192,7 +192,7 @@ class OracleBasis:
         return AX
 
     def dirac_coulomb(self, D, bare=True, dc=True, ssss=True, xHFX=1.0,
-                      thresh=1e-12, libcint=True):
+                      thresh=1e-12, libcint=True, gaunt=False):
         """FourCompFock::formGDDirect: D = [S, X, Y, Z] Pauli components of
         the 2N x 2N density; returns G = twoeH - xHFX K (same layout)."""
         Ds = [np.asfortranarray(d, dtype=np.complex128) for d in D]
@@ -200,16 +200,19 @@ class OracleBasis:
         dp_ = (C.c_void_p * 4)(*[d.ctypes.data for d in Ds])
         gp_ = (C.c_void_p * 4)(*[g.ctypes.data for g in Gs])
         lib().orc_dirac_coulomb(self.h, dp_, gp_, int(bare), int(dc), int(ssss),
-                                xHFX, thresh, int(libcint))
+                                xHFX, thresh, int(libcint), int(gaunt))
         return Gs
 
     def rel_contract(self, X, contType, exchange=True, thresh=1e-12):
         """GTODirectRelERIContraction::twoBodyContract: X = the 17 N x N
-        complex matrices (DIRAC_PAULI_SPINOR_COMP order); returns the 17 AX."""
+        complex matrices (29 for GAUNT, contType 3; DIRAC_PAULI_SPINOR_COMP
+        order); returns as many AX."""
+        n = 29 if contType == 3 else 17
+        assert len(X) == n
         Xs = [np.asfortranarray(x, dtype=np.complex128) for x in X]
         AX = [np.zeros_like(x, order="F") for x in Xs]
-        xp = (C.c_void_p * 17)(*[x.ctypes.data for x in Xs])
-        ap = (C.c_void_p * 17)(*[a.ctypes.data for a in AX])
+        xp = (C.c_void_p * n)(*[x.ctypes.data for x in Xs])
+        ap = (C.c_void_p * n)(*[a.ctypes.data for a in AX])
         lib().orc_rel_contract(self.h, int(contType), xp, ap, thresh,
                                1 if exchange else 0)
         return AX
