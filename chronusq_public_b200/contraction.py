@@ -300,19 +300,36 @@ class GTODirectTPIContraction:
 
 
 # ---------------------------------------------------------------- 4C
-BARE_COULOMB, LLSS, SSSS = (_cabi.CQF_REL_BARE_COULOMB, _cabi.CQF_REL_LLSS,
-                            _cabi.CQF_REL_SSSS)
-# DIRAC_PAULI_SPINOR_COMP order of the 17 (X, AX) entries
-# (include/particleintegrals/contract/direct4C_libcint.hpp:279-310)
+BARE_COULOMB, LLSS, SSSS, GAUNT = (_cabi.CQF_REL_BARE_COULOMB, _cabi.CQF_REL_LLSS,
+                                   _cabi.CQF_REL_SSSS, _cabi.CQF_REL_GAUNT)
+# DIRAC_PAULI_SPINOR_COMP order of the 17 (X, AX) entries, and the 12 the
+# GAUNT list adds (include/particleintegrals/contract/direct4C_libcint.hpp:
+# 279-310)
 REL_COMPS = ("CLLMS", "XLLMS", "XLLMX", "XLLMY", "XLLMZ", "CSSMS", "CSSMX",
              "CSSMY", "CSSMZ", "XSSMS", "XSSMX", "XSSMY", "XSSMZ", "XLSMS",
              "XLSMX", "XLSMY", "XLSMZ")
+GAUNT_COMPS = REL_COMPS + ("CLSMS", "CLSMX", "CLSMY", "CLSMZ", "CSLMS", "CSLMX",
+                           "CSLMY", "CSLMZ", "XSLMS", "XSLMX", "XSLMY", "XSLMZ")
 
 
 def _stats(st):
     return dict(total=st.quartets_total, screened=st.quartets_screened,
                 fp32=st.quartets_fp32, fp64=st.quartets_fp64,
                 device_ms=st.device_ms)
+
+
+def _rel_outputs(contType: int, exchange: bool) -> List[int]:
+    """Entries a 4C contraction type writes."""
+    four = lambda b: list(range(b, b + 4))  # noqa: E731
+    if contType == BARE_COULOMB:
+        return [_cabi.CQF_CLLMS] + (four(_cabi.CQF_XLLMS) if exchange else [])
+    if contType == LLSS:
+        return ([_cabi.CQF_CLLMS] + four(_cabi.CQF_CSSMS)
+                + (four(_cabi.CQF_XLSMS) if exchange else []))
+    if contType == SSSS:
+        return four(_cabi.CQF_CSSMS) + (four(_cabi.CQF_XSSMS) if exchange else [])
+    return four(_cabi.CQF_CLSMS) + ((four(_cabi.CQF_XLLMS) + four(_cabi.CQF_XSSMS)
+                                     + four(_cabi.CQF_XLSMS)) if exchange else [])
 
 
 class GTODirectRelERIContraction:
@@ -327,18 +344,20 @@ class GTODirectRelERIContraction:
                         contType: int, computeExchange: bool = True,
                         screen: bool = True, precision: str = "fp64",
                         fp32_cutoff: float = 0.0, stream=None) -> None:
-        """17 entries in REL_COMPS order (None for entries the type does not
-        use).  Every given AX is overwritten (the reference zeroes AX on
-        entry); X and AX are N x N complex (numpy, or column-major CUDA
-        complex128 tensors).  precision="mixed" runs the quartets whose
-        screening bound is below fp32_cutoff in FP32 arithmetic (the
-        reference is FP64 throughout)."""
-        if len(matList) != _cabi.CQF_REL_NMAT:
-            raise ValueError("a 4C contraction list has 17 entries")
+        """17 entries in REL_COMPS order (29 in GAUNT_COMPS order for
+        GAUNT; None for entries the type does not use).  The AX the type
+        writes are overwritten (the reference zeroes AX on entry); X and AX
+        are N x N complex (numpy, or column-major CUDA complex128 tensors).
+        precision="mixed" runs the quartets whose screening bound is below
+        fp32_cutoff in FP32 arithmetic (the reference is FP64 throughout;
+        GAUNT always runs in FP64)."""
+        n = _cabi.CQF_REL_NMAT_GAUNT if contType == GAUNT else _cabi.CQF_REL_NMAT
+        if len(matList) != n:
+            raise ValueError("a 4C contraction list has %d entries" % n)
         N = self.tpi.nbasis
         present = [c for c in matList if c is not None]
         dev = bool(present) and _is_torch(present[0].X)
-        n = _cabi.CQF_REL_NMAT
+        outs = set(_rel_outputs(contType, computeExchange))
         xs = (C.c_void_p * n)()
         axs = (C.c_void_p * n)()
         keep, writeback = [], []
@@ -355,11 +374,13 @@ class GTODirectRelERIContraction:
                 X = np.asfortranarray(c.X, dtype=np.complex128)
                 if X.shape != (N, N):
                     raise ValueError("matrix shape must be (N, N)")
-                AX = np.zeros((N, N), dtype=np.complex128, order="F")
-                keep += [X, AX]
-                writeback.append((c, AX))
+                keep.append(X)
                 xs[i] = X.ctypes.data
-                axs[i] = AX.ctypes.data
+                if i in outs:
+                    AX = np.zeros((N, N), dtype=np.complex128, order="F")
+                    keep.append(AX)
+                    writeback.append((c, AX))
+                    axs[i] = AX.ctypes.data
         opts = _cabi.CqfOpts()
         _cabi.lib().cqf_opts_default(C.byref(opts))
         opts.is_complex = 1

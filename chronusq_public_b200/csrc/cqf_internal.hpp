@@ -227,8 +227,8 @@ struct cqf_basis {
   // each, zero for pairs outside the significant-pair list) and workspace
   double* d_qLL = nullptr;
   double* d_qSS = nullptr;
-  bool rel_qLL = false, rel_qSS = false;
-  std::vector<double> h_qLL, h_qSS;
+  double* d_qG = nullptr;  // Gaunt: qG[d + o * nshell], derivative on shell d
+  bool rel_qLL = false, rel_qSS = false, rel_qG = false;
   void* d_relws = nullptr;
   size_t relws_bytes = 0;
   std::mutex mu;

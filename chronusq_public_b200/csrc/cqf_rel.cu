@@ -1163,6 +1163,370 @@ void launch_rel(const RelLaunch& a, int la, int lb, int lc, int ld, cudaStream_t
   if (a.mixed) launch_rel_prec<TYPE, float>(a, la, lb, lc, ld, st);
 }
 
+// ------------------------------------------------------------------ Gaunt
+// The Gaunt term -alpha_1.alpha_2 / r12 (direct4C_libcint.hpp:2833-3907).
+// The reference runs over unordered pairs of (differentiated, other) shell
+// pairs X = (s2, s1), Y = (s3, s4) with the integrals (m d_j n | d_l k l).
+// Here a thread takes an unordered quartet of unordered significant pairs
+// {P, Q} (P = (A, B), Q = (C, D)) and computes, per Cartesian element, the
+// 36 blocks (A B with d_j on A or B | C D with d_l on C or D) at once: the
+// four (or, for P = Q, three) reference quartets {X, Y} the placements
+// make, each screened on its own by shMax Q^G(X) Q^G(Y).  Per element and
+// surviving quartet, in the reference's orientation (X >= Y as (deriv,
+// other) shell indices), its update sites and conditions with T and, for
+// the image, T^T -- the four update kinds as Pauli-algebra maps of the
+// invariants t = tr T, tau (cross vector) and S' = T + T^T - t:
+//   LL exchange from SS:  3 (d0 t - i d.tau),   -(i d0 tau + S' d)
+//   SS exchange from LL:  3 d0 t - i d.tau,     -3 i d0 tau - S' d
+//   LS Coulomb from SL (1), LS (2):  (d1_0 - d2_0) t + i (d1 + d2).tau,
+//                                     i (d2_0 - d1_0) tau + (T^T - t)(d1 + d2)
+//   LS exchange from SL:  d0 t - i d.tau,       i d0 tau + S' d - 4 T^T d
+// LL and SS exchange are accumulated in the lower shell triangle (half
+// weight on diagonal shell blocks) and completed as B + B^H by the back
+// transform, the reference's "upper = conj(lower)" (:3833-3858).  FP64.
+struct GauntLaunch {
+  const PairDev* pairs;
+  const PrimPairDev* pp;
+  const ShellDev* shells;
+  const double* prim;
+  const double* boys;
+  int braBeg, nBra, ketBeg, nKet, same;
+  int screen;
+  double thresh;
+  const double* norms;  // max shell-block norms of the 16 exchange densities
+  const double* qG;     // Gaunt Schwarz, qG[deriv + other * nshell]
+  int nShell, ncart, exchange;
+  const double* Xll[4];  // Cartesian complex densities: XLLM*, XSSM*, CLSM*, CSLM*, XSLM*
+  const double* Xss[4];
+  const double* Cls[4];
+  const double* Csl[4];
+  const double* Xsl[4];
+  double* Kll[4];  // complex accumulators: LL / SS exchange, LS Coulomb, LS exchange
+  double* Kss[4];
+  double* Jls[4];
+  double* Kls[4];
+  unsigned long long* counters;
+};
+
+// bra component pairs per unit of work (the accumulator holds 36 blocks
+// of each): a whole (pp) or (dd) pair, a fifth of an (ff) one
+__host__ __device__ constexpr int gaunt_abch(int lm) { return lm <= 1 ? 9 : (lm == 2 ? 36 : 20); }
+
+struct GInv {
+  double T[3][3], t, tau[3], S[3][3];
+};
+__device__ __forceinline__ void gaunt_inv(const double* v, bool tr, GInv& g) {
+#pragma unroll
+  for (int j = 0; j < 3; j++)
+#pragma unroll
+    for (int l = 0; l < 3; l++) g.T[j][l] = tr ? v[3 * l + j] : v[3 * j + l];
+  g.t = g.T[0][0] + g.T[1][1] + g.T[2][2];
+  g.tau[0] = g.T[1][2] - g.T[2][1];
+  g.tau[1] = g.T[2][0] - g.T[0][2];
+  g.tau[2] = g.T[0][1] - g.T[1][0];
+#pragma unroll
+  for (int j = 0; j < 3; j++)
+#pragma unroll
+    for (int l = 0; l < 3; l++) g.S[j][l] = g.T[j][l] + g.T[l][j] - (j == l ? g.t : 0.0);
+}
+
+struct Z4 {  // Pauli components (s, x, y, z), complex
+  double2 c[4];
+};
+__device__ __forceinline__ Z4 ld4(const double* const* X, size_t e) {
+  return Z4{{ldz(X[0], e), ldz(X[1], e), ldz(X[2], e), ldz(X[3], e)}};
+}
+__device__ __forceinline__ void add4(double* const* A, size_t e, const Z4& v, double w) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) addz(A[k], e, v.c[k], w);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double f) {
+  return make_double2(a.x * f, a.y * f);
+}
+// sum_x w[x] d_x over the vector part
+__device__ __forceinline__ double2 vdot(const Z4& d, const double* w) {
+  return make_double2(d.c[1].x * w[0] + d.c[2].x * w[1] + d.c[3].x * w[2],
+                      d.c[1].y * w[0] + d.c[2].y * w[1] + d.c[3].y * w[2]);
+}
+// sum_y M[x][y] d_y (trans: M[y][x])
+__device__ __forceinline__ double2 vmat(const Z4& d, const double (*M)[3], int x, bool trans) {
+  double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int y = 0; y < 3; y++) {
+    const double m = trans ? M[y][x] : M[x][y];
+    r.x += m * d.c[1 + y].x;
+    r.y += m * d.c[1 + y].y;
+  }
+  return r;
+}
+
+__device__ __forceinline__ Z4 gaunt_ll(const GInv& g, const Z4& d) {
+  Z4 r;
+  r.c[0] = cscale(csub(cscale(d.c[0], g.t), ctimes_i(vdot(d, g.tau))), 3.0);
+#pragma unroll
+  for (int x = 0; x < 3; x++)
+    r.c[1 + x] = cscale(cadd(ctimes_i(cscale(d.c[0], g.tau[x])), vmat(d, g.S, x, false)), -1.0);
+  return r;
+}
+__device__ __forceinline__ Z4 gaunt_ss(const GInv& g, const Z4& d) {
+  Z4 r;
+  r.c[0] = csub(cscale(d.c[0], 3.0 * g.t), ctimes_i(vdot(d, g.tau)));
+#pragma unroll
+  for (int x = 0; x < 3; x++)
+    r.c[1 + x] = csub(ctimes_i(cscale(d.c[0], -3.0 * g.tau[x])), vmat(d, g.S, x, false));
+  return r;
+}
+__device__ __forceinline__ Z4 gaunt_cls(const GInv& g, const Z4& d1, const Z4& d2) {
+  Z4 e;
+  e.c[0] = csub(d1.c[0], d2.c[0]);
+#pragma unroll
+  for (int x = 1; x < 4; x++) e.c[x] = cadd(d1.c[x], d2.c[x]);
+  Z4 r;
+  r.c[0] = cadd(cscale(e.c[0], g.t), ctimes_i(vdot(e, g.tau)));
+#pragma unroll
+  for (int x = 0; x < 3; x++)
+    r.c[1 + x] = cadd(ctimes_i(cscale(e.c[0], -g.tau[x])),
+                      csub(vmat(e, g.T, x, true), cscale(e.c[1 + x], g.t)));
+  return r;
+}
+__device__ __forceinline__ Z4 gaunt_xls(const GInv& g, const Z4& d) {
+  Z4 r;
+  r.c[0] = csub(cscale(d.c[0], g.t), ctimes_i(vdot(d, g.tau)));
+#pragma unroll
+  for (int x = 0; x < 3; x++)
+    r.c[1 + x] = cadd(ctimes_i(cscale(d.c[0], g.tau[x])),
+                      csub(vmat(d, g.S, x, false), cscale(vmat(d, g.T, x, true), 4.0)));
+  return r;
+}
+
+// The update sites of one reference quartet (s1 s2 | s3 s4) at element
+// (m1 m2 | m3 m4) (Cartesian AO indices), T = v (row: the s2 direction).
+__device__ __forceinline__ void gaunt_sites(const GauntLaunch& a, const double* v, int s1, int s2,
+                                            int s3, int s4, int m1, int m2, int m3, int m4) {
+  const size_t nc = a.ncart;
+  auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
+  GInv T, Tt;
+  gaunt_inv(v, false, T);
+  gaunt_inv(v, true, Tt);
+  const bool img = (s1 != s4) || (s2 != s3);
+  if (a.exchange) {
+    const double w14 = (s1 == s4) ? 0.5 : 1.0, w23 = (s2 == s3) ? 0.5 : 1.0;
+    if (s1 >= s4) add4(a.Kll, ix(m1, m4), gaunt_ll(T, ld4(a.Xss, ix(m2, m3))), w14);
+    if (s1 < s4 || (s1 == s4 && s2 != s3))
+      add4(a.Kll, ix(m4, m1), gaunt_ll(Tt, ld4(a.Xss, ix(m3, m2))), w14);
+    add4(a.Kss, ix(m2, m3), gaunt_ss(Tt, ld4(a.Xll, ix(m1, m4))), w23);
+    if (s1 != s4 && s2 == s3) add4(a.Kss, ix(m3, m2), gaunt_ss(T, ld4(a.Xll, ix(m4, m1))), 0.5);
+  }
+  add4(a.Jls, ix(m1, m2), gaunt_cls(T, ld4(a.Csl, ix(m3, m4)), ld4(a.Cls, ix(m4, m3))), 1.0);
+  if (img)
+    add4(a.Jls, ix(m4, m3), gaunt_cls(Tt, ld4(a.Csl, ix(m2, m1)), ld4(a.Cls, ix(m1, m2))), 1.0);
+  if (a.exchange) {
+    add4(a.Kls, ix(m1, m3), gaunt_xls(T, ld4(a.Xsl, ix(m2, m4))), 1.0);
+    if (img) add4(a.Kls, ix(m4, m2), gaunt_xls(Tt, ld4(a.Xsl, ix(m3, m1))), 1.0);
+  }
+}
+
+// One thread per (quartet {P, Q}, unit); units = ket component pairs (c, d)
+// x slices of gaunt_abch(LM) bra component pairs, split over nsplit threads.
+template <int LM>
+__global__ void __launch_bounds__(REL_THREADS)
+    gaunt_kernel(const GauntLaunch a, int la, int lb, int lc, int ld, int nsplit, int nslice) {
+  const int ib = blockIdx.x;
+  const int split = blockIdx.y % nsplit;
+  const int jk = (blockIdx.y / nsplit) * REL_THREADS + threadIdx.x;
+  const int ns = a.nShell;
+  const bool visited = jk < a.nKet && !(a.same && jk > ib);
+  const PairDev P = a.pairs[a.braBeg + ib];
+  PairDev Q = P;
+  unsigned alive = 0;  // bit 2 pb + pk: derivative on B (pb) / D (pk)
+  if (visited) {
+    Q = a.pairs[a.ketBeg + jk];
+    const double shMax = sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns);
+    const bool samePQ = P.lex == Q.lex;
+#pragma unroll
+    for (int pb = 0; pb < 2; pb++)
+#pragma unroll
+      for (int pk = 0; pk < 2; pk++) {
+        if ((pb && P.shA == P.shB) || (pk && Q.shA == Q.shB) || (samePQ && pb > pk)) continue;
+        const int xd = pb ? P.shB : P.shA, xo = pb ? P.shA : P.shB;
+        const int yd = pk ? Q.shB : Q.shA, yo = pk ? Q.shA : Q.shB;
+        const double bound = shMax * __ldg(a.qG + xd + (size_t)xo * ns) *
+                             __ldg(a.qG + yd + (size_t)yo * ns);
+        if (!a.screen || bound >= a.thresh) alive |= 1u << (2 * pb + pk);
+      }
+  }
+  if (split == 0) {
+    const unsigned mask = __activemask();
+    const unsigned bv = __ballot_sync(mask, visited), bw = __ballot_sync(mask, alive != 0);
+    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
+      if (bv) atomicAdd(a.counters + 0, (unsigned long long)__popc(bv));
+      if (bv & ~bw) atomicAdd(a.counters + 1, (unsigned long long)__popc(bv & ~bw));
+      if (bw) atomicAdd(a.counters + 3, (unsigned long long)__popc(bw));
+    }
+  }
+  if (!alive) return;
+
+  constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
+  constexpr int HB = nherm(2 * LM + 1);
+  constexpr int HL = nherm(4 * LM + 2);
+  constexpr int FL = 2 * LM + 3;
+  constexpr int ABCH = gaunt_abch(LM);
+  const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb, ncd = ncc * nd;
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+  const int Lb = la + lb + 1, Lk = lc + ld + 1, L = Lb + Lk;
+  // which placements some surviving quartet needs
+  const bool needB[2] = {(alive & 3u) != 0, (alive & 12u) != 0};
+  const bool needK[2] = {(alive & 5u) != 0, (alive & 10u) != 0};
+
+  double Ea[3][E1], Ec[3][E1];
+  double G[6][HB];  // [pk * 3 + l]
+  double Rv[HL];
+  double F[4 * LM + 3];
+  double acc[ABCH * 36];
+  double fa[3][3][FL], fc[3][3][FL];
+  int nfa[3][3], nfc[3][3];
+
+#pragma unroll 1
+  for (int u = split; u < ncd * nslice; u += nsplit) {
+    const int cd = u / nslice, sl = u % nslice;
+    const int ab0 = sl * ABCH, ab1 = min(nab, ab0 + ABCH);
+    if (ab0 >= ab1) continue;
+    const int c = cd / nd, d = cd % nd;
+    const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
+    const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+#pragma unroll 1
+    for (int k = 0; k < (ab1 - ab0) * 36; k++) acc[k] = 0.0;
+#pragma unroll 1
+    for (int ip = 0; ip < P.npp; ip++) {
+      const PrimPairDev& A = a.pp[P.pp_off + ip];
+      double ea, eb;
+      pair_exps(SA, SB, a.prim, A, ea, eb);
+#pragma unroll 1
+      for (int x = 0; x < 3; x++)
+        hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
+#pragma unroll 1
+      for (int k = 0; k < 6; k++)
+#pragma unroll 1
+        for (int h = 0; h < nherm(Lb); h++) G[k][h] = 0.0;
+#pragma unroll 1
+      for (int iq = 0; iq < Q.npp; iq++) {
+        const PrimPairDev& Bq = a.pp[Q.pp_off + iq];
+        double ec, ed;
+        pair_exps(SC, SD, a.prim, Bq, ec, ed);
+#pragma unroll 1
+        for (int x = 0; x < 3; x++)
+          hermite_E_rt<double, LM + 1>(lc + 1, ld + 1, Bq.o2p, Bq.PA[x], Bq.PB[x], Ec[x]);
+        const double X = A.P[0] - Bq.P[0], Y = A.P[1] - Bq.P[1], Z = A.P[2] - Bq.P[2];
+        const double pq = A.p + Bq.p, alpha = A.p * Bq.p / pq;
+        const double pref = PI52X2 / sqrt(pq) * A.Kp * Bq.Kp;
+        boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), F, a.boys);
+        hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
+#pragma unroll 1
+        for (int x = 0; x < 3; x++)
+#pragma unroll 1
+          for (int ty = 0; ty < 3; ty++) {
+            if (ty > 0 && !needK[ty - 1]) continue;
+            nfc[x][ty] = axis_factor<double>(Ec[x], ld + 1, lc + ld + 3, ci[x], di[x], ty,
+                                             2.0 * ec, 2.0 * ed, fc[x][ty]);
+#pragma unroll 1
+            for (int t = 1; t < nfc[x][ty]; t += 2) fc[x][ty][t] = -fc[x][ty][t];
+          }
+#pragma unroll 1
+        for (int pk = 0; pk < 2; pk++) {
+          if (!needK[pk]) continue;
+#pragma unroll 1
+          for (int l = 0; l < 3; l++) {
+            const int tx = (l == 0) ? 1 + pk : 0, ty = (l == 1) ? 1 + pk : 0,
+                      tz = (l == 2) ? 1 + pk : 0;
+            ket_add<double>(G[pk * 3 + l], pref, fc[0][tx], nfc[0][tx], fc[1][ty], nfc[1][ty],
+                            fc[2][tz], nfc[2][tz], Lb, Rv);
+          }
+        }
+      }
+#pragma unroll 1
+      for (int ab = ab0; ab < ab1; ab++) {
+        const int ai = ab / nb, bi = ab % nb;
+        const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+        const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+#pragma unroll 1
+        for (int x = 0; x < 3; x++)
+#pragma unroll 1
+          for (int ty = 0; ty < 3; ty++) {
+            if (ty > 0 && !needB[ty - 1]) continue;
+            nfa[x][ty] = axis_factor<double>(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty,
+                                             2.0 * ea, 2.0 * eb, fa[x][ty]);
+          }
+        double* m = acc + (ab - ab0) * 36;
+#pragma unroll 1
+        for (int pb = 0; pb < 2; pb++) {
+          if (!needB[pb]) continue;
+#pragma unroll 1
+          for (int j = 0; j < 3; j++) {
+            const int tx = (j == 0) ? 1 + pb : 0, ty = (j == 1) ? 1 + pb : 0,
+                      tz = (j == 2) ? 1 + pb : 0;
+#pragma unroll 1
+            for (int pk = 0; pk < 2; pk++) {
+              if (!(alive & (1u << (2 * pb + pk)))) continue;
+#pragma unroll 1
+              for (int l = 0; l < 3; l++)
+                m[((pb * 3 + j) * 2 + pk) * 3 + l] +=
+                    bra_dot<double>(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty], fa[2][tz],
+                                    nfa[2][tz], G[pk * 3 + l]);
+            }
+          }
+        }
+      }
+    }
+    // digestion: every surviving reference quartet of every element
+    const int gC = Q.cA + c, gD = Q.cB + d;
+#pragma unroll 1
+    for (int ab = ab0; ab < ab1; ab++) {
+      const int gA = P.cA + ab / nb, gB = P.cB + ab % nb;
+      const double* m = acc + (ab - ab0) * 36;
+#pragma unroll 1
+      for (int pb = 0; pb < 2; pb++)
+#pragma unroll 1
+        for (int pk = 0; pk < 2; pk++) {
+          if (!(alive & (1u << (2 * pb + pk)))) continue;
+          const int xd = pb ? P.shB : P.shA, xo = pb ? P.shA : P.shB;
+          const int yd = pk ? Q.shB : Q.shA, yo = pk ? Q.shA : Q.shB;
+          const int xdA = pb ? gB : gA, xoA = pb ? gA : gB;
+          const int ydA = pk ? gD : gC, yoA = pk ? gC : gD;
+          const bool xb = xd > yd || (xd == yd && xo >= yo);
+          double v[9];
+#pragma unroll
+          for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int l = 0; l < 3; l++) {
+              const double t = m[((pb * 3 + j) * 2 + pk) * 3 + l];
+              if (xb) v[3 * j + l] = t;
+              else v[3 * l + j] = t;
+            }
+          if (xb) gaunt_sites(a, v, xo, xd, yd, yo, xoA, xdA, ydA, yoA);
+          else gaunt_sites(a, v, yo, yd, xd, xo, yoA, ydA, xdA, xoA);
+        }
+    }
+  }
+}
+
+void launch_gaunt(const GauntLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
+  if (a.nBra == 0 || a.nKet == 0) return;
+  const int tiles = (a.nKet + REL_THREADS - 1) / REL_THREADS;
+  const int lm = std::max(std::max(la, lb), std::max(lc, ld));
+  const int nab = ncart(la) * ncart(lb), abch = gaunt_abch(std::max(lm, 1));
+  const int nslice = (nab + abch - 1) / abch;
+  const long long quartets = (long long)a.nBra * a.nKet;
+  const int units = ncart(lc) * ncart(ld) * nslice;
+  int nsplit = (int)std::min<long long>(units, std::max<long long>(1, (1 << 18) / quartets));
+  nsplit = std::max(1, std::min(nsplit, 65535 / tiles));
+  dim3 grid(a.nBra, tiles * nsplit);
+  if (lm <= 1) gaunt_kernel<1><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+  else if (lm == 2) gaunt_kernel<2><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+  else gaunt_kernel<3><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+}
+
 // ------------------------------------------------------------ 4C Schwarz
 // Q^LL(a,b) = sqrt(max |(ab|ab)|) and Q^SS(a,b) = C2 sqrt(max over the 81
 // components of |(dA dB ab|dA dB ab)|), both over every element of the
@@ -1264,26 +1628,29 @@ __device__ void sph_index(const double* in, double* out, int* dims, int k, const
 constexpr int SCH_THREADS = 128;
 
 // One (pair, component) per group of gsize threads, SCH_THREADS / gsize
-// groups per block, units enumerated pair-major over ncomp components per
-// pair: component 0 is the plain (ab|ab) block when lowLL, the others the
-// 81 derivative blocks (dA_i dB_j ab | dA_k dB_l ab).  A group builds the
+// groups per block, units enumerated pair-major over the components of a
+// pair: the plain (ab|ab) block (when lowLL), the 81 blocks
+// (dA_i dB_j ab | dA_k dB_l ab) (nSS = 81) and the 18 Gaunt blocks
+// (dA_i b | dA_k b), (a dB_i | a dB_k) (nG = 18).  A group builds the
 // Cartesian block in shared memory -- thread g0 takes ket column g0 % cpow
 // (cpow: the column count rounded up to a power of two) and every
 // (gsize / cpow)-th bra primitive pair from g0 / cpow -- transforms it to
 // the spherical basis index by index, and folds its largest |element| into
-// the pair's maximum (mx[2 pair + 0 / 1]: plain / derivative) with an atomic
-// max on the bit pattern (non-negative doubles order as integers).
+// the pair's maximum (mx[4 pair + 0..3]: plain, SS, Gaunt on A, Gaunt on B)
+// with an atomic max on the bit pattern (non-negative doubles order as
+// integers).
 template <int LM>
 __global__ void __launch_bounds__(SCH_THREADS)
     rel_schwarz_kernel(const PairDev* __restrict__ pairs, const PrimPairDev* __restrict__ pp,
                        const ShellDev* __restrict__ shells, const double* __restrict__ prim,
                        const double* __restrict__ boys, const double* __restrict__ sph,
                        const int* __restrict__ sphOff, int beg, int npair, int la, int lb,
-                       int ncomp, int lowLL, int gsize, int cpow, unsigned long long* mx) {
+                       int lowLL, int nSS, int nG, int gsize, int cpow, unsigned long long* mx) {
   extern __shared__ double sm[];
   const int na = ncart(la), nb = ncart(lb);
   const int n4 = na * nb * na * nb;
   const int groups = SCH_THREADS / gsize;
+  const int ncomp = lowLL + nSS + nG;
   const int g = threadIdx.x / gsize, g0 = threadIdx.x % gsize;
   const long long unit = (long long)blockIdx.x * groups + g;
   const bool live = unit < (long long)npair * ncomp;
@@ -1292,12 +1659,20 @@ __global__ void __launch_bounds__(SCH_THREADS)
   const PairDev P = pairs[beg + ip];
   const ShellDev SA = shells[P.shA], SB = shells[P.shB];
   int dir[4] = {-1, -1, -1, -1};
-  const int dc = comp - lowLL;  // derivative component 0..80, or -1: plain
-  if (dc >= 0) {
+  int slot = 0;
+  if (comp >= lowLL + nSS) {  // Gaunt: one derivative in each pair
+    const int gc = comp - lowLL - nSS;
+    const int side = gc / 9;  // 0: on A, 1: on B
+    dir[side] = (gc % 9) / 3;
+    dir[2 + side] = gc % 3;
+    slot = 2 + side;
+  } else if (comp >= lowLL) {
+    const int dc = comp - lowLL;  // derivative component 0..80
     dir[0] = dc / 27;
     dir[1] = (dc / 9) % 3;
     dir[2] = (dc / 3) % 3;
     dir[3] = dc % 3;
+    slot = 1;
   }
   double* cur = sm + (size_t)g * 2 * n4;
   double* nxt = cur + n4;
@@ -1325,49 +1700,54 @@ __global__ void __launch_bounds__(SCH_THREADS)
   const int tot = dims[0] * dims[1] * dims[2] * dims[3];
   for (int e = g0; e < tot; e += gsize) m = fmax(m, fabs(cur[e]));
   if (m > 0.0)
-    atomicMax(mx + 2 * (size_t)ip + (dc >= 0 ? 1 : 0),
-              (unsigned long long)__double_as_longlong(m));
+    atomicMax(mx + 4 * (size_t)ip + slot, (unsigned long long)__double_as_longlong(m));
 }
 
 // Q^LL = sqrt(max), Q^SS = C2 sqrt(max) of each pair of a class into both
 // triangles of the nshell x nshell tables (direct4C_libcint.hpp:388-394,
-// :464-470).
+// :464-470); Q^G(d, o) = C1 sqrt(max) with the derivative on shell d
+// (SchwarzGaunt, :2910-2955, C1 = 1 / 2c), not symmetric.
 __global__ void rel_schwarz_finish_kernel(const PairDev* __restrict__ pairs, int beg, int npair,
                                           const unsigned long long* __restrict__ mx,
-                                          int needLL, int needSS, int nshell, double* qLL,
-                                          double* qSS) {
+                                          int needLL, int needSS, int needG, int nshell,
+                                          double* qLL, double* qSS, double* qG) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= npair) return;
   const PairDev P = pairs[beg + ip];
   const size_t e1 = P.s1 + (size_t)P.s2 * nshell, e2 = P.s2 + (size_t)P.s1 * nshell;
-  if (needLL) qLL[e1] = qLL[e2] = sqrt(__longlong_as_double((long long)mx[2 * ip]));
+  auto v = [&](int k) { return sqrt(__longlong_as_double((long long)mx[4 * ip + k])); };
+  if (needLL) qLL[e1] = qLL[e2] = v(0);
   if (needSS) {
     const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
-    qSS[e1] = qSS[e2] = C2 * sqrt(__longlong_as_double((long long)mx[2 * ip + 1]));
+    qSS[e1] = qSS[e2] = C2 * v(1);
+  }
+  if (needG) {
+    const double C1 = 1.0 / (2.0 * SPEED_OF_LIGHT);
+    qG[P.shA + (size_t)P.shB * nshell] = C1 * v(2);
+    qG[P.shB + (size_t)P.shA * nshell] = C1 * v(3);
   }
 }
 
-cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream_t st) {
+cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, bool needG,
+                              cudaStream_t st) {
   needLL = needLL && !B->rel_qLL;
   needSS = needSS && !B->rel_qSS;
-  if (!needLL && !needSS) return CQF_OK;
+  needG = needG && !B->rel_qG;
+  if (!needLL && !needSS && !needG) return CQF_OK;
   const size_t ns2 = (size_t)B->nshell * B->nshell;
   // basis-owned, stream-ordered on the basis' stream (freed by free_basis)
-  if (!B->d_qLL) {
-    CQF_RCUDA(cudaMallocAsync(&B->d_qLL, ns2 * sizeof(double), B->stream));
-    CQF_RCUDA(cudaMemsetAsync(B->d_qLL, 0, ns2 * sizeof(double), B->stream));
-  }
-  if (!B->d_qSS) {
-    CQF_RCUDA(cudaMallocAsync(&B->d_qSS, ns2 * sizeof(double), B->stream));
-    CQF_RCUDA(cudaMemsetAsync(B->d_qSS, 0, ns2 * sizeof(double), B->stream));
-  }
+  for (double** q : {&B->d_qLL, &B->d_qSS, &B->d_qG})
+    if (!*q) {
+      CQF_RCUDA(cudaMallocAsync(q, ns2 * sizeof(double), B->stream));
+      CQF_RCUDA(cudaMemsetAsync(*q, 0, ns2 * sizeof(double), B->stream));
+    }
   CQF_RCUDA(cudaStreamSynchronize(B->stream));
   unsigned long long* mx = nullptr;
-  CQF_RCUDA(cudaMallocAsync(&mx, 2 * (size_t)std::max(1, B->npair) * sizeof(unsigned long long),
-                            st));
-  CQF_RCUDA(cudaMemsetAsync(mx, 0, 2 * (size_t)std::max(1, B->npair) * sizeof(unsigned long long),
-                            st));
-  const int ncomp = (needLL ? 1 : 0) + (needSS ? 81 : 0);
+  const size_t mxn = 4 * (size_t)std::max(1, B->npair);
+  CQF_RCUDA(cudaMallocAsync(&mx, mxn * sizeof(unsigned long long), st));
+  CQF_RCUDA(cudaMemsetAsync(mx, 0, mxn * sizeof(unsigned long long), st));
+  const int nSS = needSS ? 81 : 0, nG = needG ? 18 : 0;
+  const int ncomp = (needLL ? 1 : 0) + nSS + nG;
   for (int c = 0; c < NCLS; c++) {
     if (B->cls_cnt[c] <= 0) continue;
     int la, lb;
@@ -1383,7 +1763,7 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream
     const size_t smem = (size_t)groups * 2 * n4 * sizeof(double);
     const long long units = (long long)B->cls_cnt[c] * ncomp;
     const unsigned nblk = (unsigned)((units + groups - 1) / groups);
-    unsigned long long* mxc = mx + 2 * (size_t)B->cls_beg[c];
+    unsigned long long* mxc = mx + 4 * (size_t)B->cls_beg[c];
     const int lm = std::max(la, 1);
 #define CQF_SCH(LMV)                                                                          \
   if (lm == LMV) {                                                                            \
@@ -1391,31 +1771,22 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, cudaStream
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
     rel_schwarz_kernel<LMV><<<nblk, SCH_THREADS, smem, st>>>(                                 \
         B->d_pairs, B->d_pp, B->d_shells, B->d_prim, B->d_boys64, B->d_sph, B->d_sphOff,      \
-        B->cls_beg[c], B->cls_cnt[c], la, lb, ncomp, needLL ? 1 : 0, gsize, cpow, mxc);       \
+        B->cls_beg[c], B->cls_cnt[c], la, lb, needLL ? 1 : 0, nSS, nG, gsize, cpow, mxc);     \
   }
     CQF_SCH(1)
     CQF_SCH(2)
     CQF_SCH(3)
 #undef CQF_SCH
     rel_schwarz_finish_kernel<<<(B->cls_cnt[c] + 127) / 128, 128, 0, st>>>(
-        B->d_pairs, B->cls_beg[c], B->cls_cnt[c], mxc, needLL, needSS, B->nshell, B->d_qLL,
-        B->d_qSS);
+        B->d_pairs, B->cls_beg[c], B->cls_cnt[c], mxc, needLL, needSS, needG, B->nshell,
+        B->d_qLL, B->d_qSS, B->d_qG);
     CQF_RCUDA(cudaGetLastError());
   }
   cudaFreeAsync(mx, st);
-  if (needLL) {
-    B->h_qLL.resize(ns2);
-    CQF_RCUDA(cudaMemcpyAsync(B->h_qLL.data(), B->d_qLL, ns2 * sizeof(double),
-                              cudaMemcpyDeviceToHost, st));
-  }
-  if (needSS) {
-    B->h_qSS.resize(ns2);
-    CQF_RCUDA(cudaMemcpyAsync(B->h_qSS.data(), B->d_qSS, ns2 * sizeof(double),
-                              cudaMemcpyDeviceToHost, st));
-  }
   CQF_RCUDA(cudaStreamSynchronize(st));
   B->rel_qLL = B->rel_qLL || needLL;
   B->rel_qSS = B->rel_qSS || needSS;
+  B->rel_qG = B->rel_qG || needG;
   return CQF_OK;
 }
 
@@ -1542,8 +1913,44 @@ size_t align32(size_t n) { return (n + 31) / 32 * 32; }
 // screened, FP32, FP64 quartet counts, added to.
 size_t rel_ws_doubles(const cqf_basis* B) {
   const size_t nc2 = (size_t)B->ncart * B->ncart, ns2 = (size_t)B->nshell * B->nshell;
-  return align32(9 * 2 * nc2) + align32(13 * nc2) + align32(10 * ns2) + 64;
+  const size_t dc = align32(9 * 2 * nc2) + align32(13 * nc2) + align32(10 * ns2);
+  // Gaunt: 20 Cartesian complex densities | 16 complex accumulators | norms
+  const size_t ga = align32(20 * 2 * nc2) + align32(16 * 2 * nc2) + align32(18 * ns2);
+  return std::max(dc, ga) + 64;
 }
+
+// The entries a contraction type writes (the others are neither zeroed nor
+// written: the reference's GAUNT list points its CSLM* / XSLM* entries at
+// the CLSM* / XLSM* outputs).
+std::vector<int> rel_outputs(int type, bool exch) {
+  std::vector<int> o;
+  auto four = [&](int base) {
+    for (int c = 0; c < 4; c++) o.push_back(base + c);
+  };
+  if (type == CQF_REL_BARE_COULOMB) {
+    o.push_back(CQF_CLLMS);
+    if (exch) four(CQF_XLLMS);
+  } else if (type == CQF_REL_LLSS) {
+    o.push_back(CQF_CLLMS);
+    four(CQF_CSSMS);
+    if (exch) four(CQF_XLSMS);
+  } else if (type == CQF_REL_SSSS) {
+    four(CQF_CSSMS);
+    if (exch) four(CQF_XSSMS);
+  } else {
+    four(CQF_CLSMS);
+    if (exch) {
+      four(CQF_XLLMS);
+      four(CQF_XSSMS);
+      four(CQF_XLSMS);
+    }
+  }
+  return o;
+}
+
+cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int exch,
+                              const cqf_opts& opts, cudaStream_t st, double* ws,
+                              unsigned long long* cnt);
 
 cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int type,
                             int exch, const cqf_opts& opts, cudaStream_t st, double* ws,
@@ -1552,8 +1959,9 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   const bool mixed = opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
-  for (int m = 0; m < CQF_REL_NMAT; m++)
+  for (int m : rel_outputs(type, exch))
     if (AX[m]) CQF_RCUDA(cudaMemsetAsync(AX[m], 0, 2 * NN * sizeof(double), st));
+  if (type == CQF_REL_GAUNT) return gaunt_contract_dev(B, X, AX, exch, opts, st, ws, cnt);
 
   if (type == CQF_REL_BARE_COULOMB) {
     // (LL|LL): the 1C engine on J[Re X] and K[X] (the same quartets, screen
@@ -1590,7 +1998,7 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   }
 
   const bool llss = (type == CQF_REL_LLSS);
-  CQF_RTRY(ensure_rel_schwarz(B, llss, true, st));
+  CQF_RTRY(ensure_rel_schwarz(B, llss, true, false, st));
   // required entries
   std::vector<int> need = {CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ};
   if (llss) need.push_back(CQF_CLLMS);
@@ -1702,6 +2110,126 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   return CQF_OK;
 }
 
+
+// The GAUNT contraction on device pointers (X, AX: 29 entries).  Needs
+// X[CLSM*], X[CSLM*] and, with exchange, X[XLLM*], X[XSSM*], X[XSLM*];
+// writes AX[CLSM*] and, with exchange, AX[XLLM*], AX[XSSM*], AX[XLSM*].
+// The screening norms are the max over the 16 exchange densities the
+// reference uses (:2957-3020), of those given.  FP64 (opts.precision is
+// not applied to this term).
+cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int exch,
+                              const cqf_opts& opts, cudaStream_t st, double* ws,
+                              unsigned long long* cnt) {
+  const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
+  const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
+  (void)NN;
+  std::vector<int> need;
+  for (int c = 0; c < 4; c++) {
+    need.push_back(CQF_CLSMS + c);
+    need.push_back(CQF_CSLMS + c);
+    if (exch) {
+      need.push_back(CQF_XLLMS + c);
+      need.push_back(CQF_XSSMS + c);
+      need.push_back(CQF_XSLMS + c);
+    }
+  }
+  for (int m : need)
+    if (!X[m]) return fail(CQF_EINVAL, "missing X entry for the GAUNT contraction");
+  for (int m : rel_outputs(CQF_REL_GAUNT, exch))
+    if (!AX[m]) return fail(CQF_EINVAL, "missing AX entry for the GAUNT contraction");
+  CQF_RTRY(ensure_rel_schwarz(B, false, false, true, st));
+
+  double* xc = ws;
+  double* accb = ws + align32(20 * 2 * nc2);
+  double* nrm = accb + align32(16 * 2 * nc2);
+  auto XC = [&](int slot) { return xc + (size_t)slot * 2 * nc2; };
+  auto AC = [&](int slot) { return accb + (size_t)slot * 2 * nc2; };
+  // density slots: 0 XLLM*, 4 XSSM*, 8 CLSM*, 12 CSLM*, 16 XSLM*
+  const int src[5] = {CQF_XLLMS, CQF_XSSMS, CQF_CLSMS, CQF_CSLMS, CQF_XSLMS};
+  for (int k = 0; k < 5; k++)
+    for (int c = 0; c < 4; c++)
+      if (X[src[k] + c]) launch_to_cart(B, X[src[k] + c], 1, XC(4 * k + c), st);
+  // screening norms: max over XLSM*, XSLM*, XLLM*, XSSM*
+  // (without exchange, the LS / SL Coulomb entries stand for the same
+  // LS / SL blocks)
+  std::vector<int> smats;
+  for (int base : {(int)CQF_XLSMS, (int)CQF_XSLMS, (int)CQF_XLLMS, (int)CQF_XSSMS})
+    for (int c = 0; c < 4; c++) {
+      int m = base + c;
+      if (!X[m] && base == CQF_XLSMS) m = CQF_CLSMS + c;
+      if (!X[m] && base == CQF_XSLMS) m = CQF_CSLMS + c;
+      if (X[m]) smats.push_back(m);
+    }
+  double* nmAll = nrm + ns2;
+  for (size_t i = 0; i < smats.size(); i++)
+    launch_block_norms(B, X[smats[i]], 1, nmAll + i * ns2, st);
+  launch_max_norms(nmAll, (int)smats.size(), ns2, nrm,
+                   reinterpret_cast<unsigned long long*>(nmAll + 16 * ns2), st);
+  CQF_RCUDA(cudaMemsetAsync(accb, 0, 16 * 2 * nc2 * sizeof(double), st));
+  unsigned long long* dcnt = B->d_counters;
+  CQF_RCUDA(cudaMemsetAsync(dcnt, 0, 4 * sizeof(unsigned long long), st));
+  CQF_RCUDA(cudaGetLastError());
+
+  GauntLaunch a{};
+  a.pairs = B->d_pairs;
+  a.pp = B->d_pp;
+  a.shells = B->d_shells;
+  a.prim = B->d_prim;
+  a.boys = B->d_boys64;
+  a.screen = opts.screen;
+  a.thresh = B->thresh;
+  a.norms = nrm;
+  a.qG = B->d_qG;
+  a.nShell = ns;
+  a.ncart = nc;
+  a.exchange = exch;
+  for (int c = 0; c < 4; c++) {
+    a.Xll[c] = XC(0 + c);
+    a.Xss[c] = XC(4 + c);
+    a.Cls[c] = XC(8 + c);
+    a.Csl[c] = XC(12 + c);
+    a.Xsl[c] = XC(16 + c);
+    a.Kll[c] = AC(0 + c);
+    a.Kss[c] = AC(4 + c);
+    a.Jls[c] = AC(8 + c);
+    a.Kls[c] = AC(12 + c);
+  }
+  a.counters = dcnt;
+  for (int cb = 0; cb < NCLS; cb++)
+    for (int ck = 0; ck <= cb; ck++) {
+      if (!B->cls_cnt[cb] || !B->cls_cnt[ck]) continue;
+      int la, lb, lc, ld;
+      class_ls(cb, la, lb);
+      class_ls(ck, lc, ld);
+      a.braBeg = B->cls_beg[cb];
+      a.nBra = B->cls_cnt[cb];
+      a.ketBeg = B->cls_beg[ck];
+      a.nKet = B->cls_cnt[ck];
+      a.same = (cb == ck);
+      launch_gaunt(a, la, lb, lc, ld, st);
+    }
+  CQF_RCUDA(cudaGetLastError());
+  auto back = [&](const double* srcAcc, int mode, double* dst) {
+    rel_from_cart_kernel<<<rgrid(NN, 256), 256, 0, st>>>(srcAcc, mode, N, nc, B->d_shells,
+                                                         B->d_ao2shell, B->d_sph, B->d_sphOff,
+                                                         dst);
+  };
+  for (int c = 0; c < 4; c++) {
+    back(AC(8 + c), 0, AX[CQF_CLSMS + c]);
+    if (exch) {
+      back(AC(0 + c), 3, AX[CQF_XLLMS + c]);
+      back(AC(4 + c), 3, AX[CQF_XSSMS + c]);
+      back(AC(12 + c), 0, AX[CQF_XLSMS + c]);
+    }
+  }
+  CQF_RCUDA(cudaGetLastError());
+  unsigned long long h[4];
+  CQF_RCUDA(cudaMemcpyAsync(h, dcnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CQF_RCUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < 4; k++) cnt[k] += h[k];
+  return CQF_OK;
+}
+
 }  // namespace
 }  // namespace cqf
 
@@ -1713,7 +2241,7 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
                                      int type, int compute_exchange, const cqf_opts* optsIn,
                                      cqf_stats* stats) {
   if (!B || !X || !AX) return fail(CQF_EINVAL, "cqf_rel_two_body_contract: null argument");
-  if (type < CQF_REL_BARE_COULOMB || type > CQF_REL_SSSS)
+  if (type < CQF_REL_BARE_COULOMB || type > CQF_REL_GAUNT)
     return fail(CQF_EINVAL, "cqf_rel_two_body_contract: unknown contraction type");
   cqf_opts o;
   cqf_opts_default(&o);
@@ -1721,21 +2249,23 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_RCUDA(cudaSetDevice(B->device));
   cudaStream_t st = o.stream ? (cudaStream_t)o.stream : B->stream;
+  const int nmat = (type == CQF_REL_GAUNT) ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
+  const std::vector<int> outs = rel_outputs(type, compute_exchange != 0);
   const size_t NN = (size_t)B->nbasis * B->nbasis;
   const size_t wsd = rel_ws_doubles(B);
-  const size_t hostd = o.device_pointers ? 0 : align32(2 * NN) * 2 * CQF_REL_NMAT;
+  const size_t hostd = o.device_pointers ? 0 : align32(2 * NN) * 2 * nmat;
   CQF_RTRY(ensure_relws(B, (wsd + hostd) * sizeof(double)));
   double* ws = static_cast<double*>(B->d_relws);
   double* hbuf = ws + wsd;
-  const double* Xd[CQF_REL_NMAT];
-  double* AXd[CQF_REL_NMAT];
-  for (int m = 0; m < CQF_REL_NMAT; m++) {
+  const double* Xd[CQF_REL_NMAT_GAUNT] = {};
+  double* AXd[CQF_REL_NMAT_GAUNT] = {};
+  for (int m = 0; m < nmat; m++) {
     if (o.device_pointers) {
       Xd[m] = static_cast<const double*>(X[m]);
       AXd[m] = static_cast<double*>(AX[m]);
     } else {
       double* xd = hbuf + (size_t)m * align32(2 * NN);
-      double* ad = hbuf + (size_t)(CQF_REL_NMAT + m) * align32(2 * NN);
+      double* ad = hbuf + (size_t)(nmat + m) * align32(2 * NN);
       Xd[m] = X[m] ? xd : nullptr;
       AXd[m] = AX[m] ? ad : nullptr;
       if (X[m])
@@ -1746,8 +2276,9 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
   unsigned long long cnt[4] = {0, 0, 0, 0};
   CQF_RTRY(rel_contract_dev(B, Xd, AXd, type, compute_exchange, o, st, ws, cnt));
   CQF_RCUDA(cudaEventRecord(B->ev1, st));
+  // only the entries the type writes come back (a list may alias the others)
   if (!o.device_pointers)
-    for (int m = 0; m < CQF_REL_NMAT; m++)
+    for (int m : outs)
       if (AX[m])
         CQF_RCUDA(cudaMemcpyAsync(AX[m], AXd[m], 2 * NN * sizeof(double), cudaMemcpyDeviceToHost,
                                   st));
@@ -1771,6 +2302,7 @@ void cqf_dc_opts_default(cqf_dc_opts* o) {
   o->dirac_coulomb_ssss = 1;
   o->libcint = 1;
   o->xHFX = 1.0;
+  o->gaunt = 0;
 }
 
 cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
@@ -1792,17 +2324,17 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
   const double c2 = SPEED_OF_LIGHT * SPEED_OF_LIGHT;
   const double C2 = 1.0 / (4.0 * c2), C4 = 1.0 / (16.0 * c2 * c2);
   const bool exch = std::fabs(dc.xHFX) >= 1e-12;
-  // workspace: rel scratch | blocks 12 x N^2 | AX 17 x N^2 | twoeH 4 x 4N^2 |
+  // workspace: rel scratch | blocks 16 x N^2 | AX 29 x N^2 | twoeH 4 x 4N^2 |
   // K 4 x 4N^2 | D/G staging (host pointers) 8 x 4N^2, all complex
   const size_t wsd = rel_ws_doubles(B);
   const size_t blkd = align32(2 * NN), bigd = align32(2 * NN2);
-  const size_t total = wsd + 12 * blkd + CQF_REL_NMAT * blkd + 8 * bigd +
+  const size_t total = wsd + 16 * blkd + CQF_REL_NMAT_GAUNT * blkd + 8 * bigd +
                        (o.device_pointers ? 0 : 8 * bigd);
   CQF_RTRY(ensure_relws(B, total * sizeof(double)));
   double* ws = static_cast<double*>(B->d_relws);
   double* blk = ws + wsd;
-  double* axb = blk + 12 * blkd;
-  double* twoeH = axb + CQF_REL_NMAT * blkd;
+  double* axb = blk + 16 * blkd;
+  double* twoeH = axb + CQF_REL_NMAT_GAUNT * blkd;
   double* Kb = twoeH + 4 * bigd;
   double* stage = Kb + 4 * bigd;
   const double* Dd[4];
@@ -1819,24 +2351,28 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
     }
   }
   CQF_RCUDA(cudaEventRecord(B->ev0, st));
-  // LL / SS / LS blocks of each Pauli component (impl.hpp:3847-3857)
+  // LL / SS / LS (/ SL, for Gaunt) blocks of each Pauli component
+  // (impl.hpp:3847-3857)
   auto B3 = [&](int k, int c) { return blk + (size_t)(k * 4 + c) * blkd; };
-  const int ro[3] = {0, N, 0}, co[3] = {0, N, N};
-  for (int k = 0; k < 3; k++)
+  const int ro[4] = {0, N, 0, N}, co[4] = {0, N, N, 0};
+  for (int k = 0; k < (dc.gaunt ? 4 : 3); k++)
     for (int c = 0; c < 4; c++)
       get_block_kernel<<<rgrid(NN, 256), 256, 0, st>>>(Dd[c], N, ro[k], co[k], B3(k, c));
   CQF_RCUDA(cudaMemsetAsync(twoeH, 0, 8 * bigd * sizeof(double), st));
   CQF_RCUDA(cudaGetLastError());
-  const double* X[CQF_REL_NMAT];
-  double* AX[CQF_REL_NMAT];
+  const double* X[CQF_REL_NMAT_GAUNT];
+  double* AX[CQF_REL_NMAT_GAUNT];
   X[CQF_CLLMS] = B3(0, 0);
   for (int c = 0; c < 4; c++) {
     X[CQF_XLLMS + c] = B3(0, c);
     X[CQF_CSSMS + c] = B3(1, c);
     X[CQF_XSSMS + c] = B3(1, c);
     X[CQF_XLSMS + c] = B3(2, c);
+    X[CQF_CLSMS + c] = B3(2, c);
+    X[CQF_CSLMS + c] = B3(3, c);
+    X[CQF_XSLMS + c] = B3(3, c);
   }
-  for (int m = 0; m < CQF_REL_NMAT; m++) AX[m] = axb + (size_t)m * blkd;
+  for (int m = 0; m < CQF_REL_NMAT_GAUNT; m++) AX[m] = axb + (size_t)m * blkd;
   auto H = [&](int c) { return twoeH + (size_t)c * bigd; };
   auto Kk = [&](int c) { return Kb + (size_t)c * bigd; };
   auto add = [&](double* M, int r0, int c0, const double* src, double f) {
@@ -1861,6 +2397,16 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
     for (int c = 0; c < 4; c++) add(H(c), N, N, AX[CQF_CSSMS + c], 2.0 * C4);
     if (exch)
       for (int c = 0; c < 4; c++) add(Kk(c), N, N, AX[CQF_XSSMS + c], -C4);
+  }
+  if (dc.gaunt) {  // impl.hpp:4235-4376 (C2, the Gauge term being absent)
+    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_GAUNT, exch, o, st, ws, cnt));
+    for (int c = 0; c < 4; c++) add(H(c), 0, N, AX[CQF_CLSMS + c], 2.0 * C2);
+    if (exch)
+      for (int c = 0; c < 4; c++) {
+        add(Kk(c), 0, 0, AX[CQF_XLLMS + c], -C2);
+        add(Kk(c), N, N, AX[CQF_XSSMS + c], -C2);
+        add(Kk(c), 0, N, AX[CQF_XLSMS + c], -C2);
+      }
   }
   for (int c = 0; c < 4; c++)
     finish_gd_kernel<<<rgrid(NN2, 256), 256, 0, st>>>(H(c), Kk(c), N, dc.xHFX, exch ? 1 : 0,

@@ -75,7 +75,8 @@ class FourCompFock:
     (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) on the GPU.
 
     Hamiltonian switches as the reference's HamiltonianOptions (BareCoulomb,
-    DiracCoulomb, DiracCoulombSSSS, Libcint); the density is the four Pauli
+    DiracCoulomb, DiracCoulombSSSS, Libcint, Gaunt; the Gauge term is not
+    built); the density is the four Pauli
     components (scalar, MX, MY, MZ) of the 2N x 2N complex 4C one-particle
     density (LL block first).  ``formGD`` returns the same four components of
     G = twoeH - xHFX K.
@@ -83,12 +84,13 @@ class FourCompFock:
 
     def __init__(self, tpi: DirectTPI, BareCoulomb: bool = True,
                  DiracCoulomb: bool = True, DiracCoulombSSSS: bool = True,
-                 Libcint: bool = True):
+                 Libcint: bool = True, Gaunt: bool = False):
         self.tpi = tpi
         self.BareCoulomb = BareCoulomb
         self.DiracCoulomb = DiracCoulomb
         self.DiracCoulombSSSS = DiracCoulombSSSS
         self.Libcint = Libcint
+        self.Gaunt = Gaunt
         self.last_stats = None
 
     def formGD(self, D: List, xHFX: float = 1.0, screen: bool = True,
@@ -129,6 +131,7 @@ class FourCompFock:
         dco.dirac_coulomb = int(self.DiracCoulomb)
         dco.dirac_coulomb_ssss = int(self.DiracCoulombSSSS)
         dco.libcint = int(self.Libcint)
+        dco.gaunt = int(self.Gaunt)
         dco.xHFX = float(xHFX)
         opts = _cabi.CqfOpts()
         _cabi.lib().cqf_opts_default(C.byref(opts))

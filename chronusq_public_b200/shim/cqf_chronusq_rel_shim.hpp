@@ -6,14 +6,15 @@
 // twoBodyContract overload of the reference class
 // (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94), which
 // FourCompFock::formGDDirect calls on the concrete type for BARE_COULOMB,
-// LLSS and SSSS (include/fockbuilder/fourcompfock/impl.hpp:3923, :4030,
-// :4177): the 17 (X, AX) entries in DIRAC_PAULI_SPINOR_COMP order go to
-// cqf_rel_two_body_contract, which zeroes AX like directScaffoldLibcint
+// LLSS, SSSS and GAUNT (include/fockbuilder/fourcompfock/impl.hpp:3923,
+// :4030, :4177, :4279): the 17 (X, AX) entries in DIRAC_PAULI_SPINOR_COMP
+// order (29 for GAUNT) go to cqf_rel_two_body_contract, which zeroes the AX
+// it writes like directScaffoldLibcint
 // (include/particleintegrals/contract/direct4C_libcint.hpp:313-314).  Other
-// contraction types (LLLL, GAUNT, GAUGE), the spin-free / spin-dependent
-// variants, approximations and MPI runs stay on the reference
-// implementation.  A nonzero cqf_status becomes CErr.  Compiles only inside
-// the ChronusQ tree (it includes ChronusQ headers).
+// contraction types (LLLL, GAUGE), the spin-free / spin-dependent variants,
+// approximations and MPI runs stay on the reference implementation.  A
+// nonzero cqf_status becomes CErr.  Compiles only inside the ChronusQ tree
+// (it includes ChronusQ headers).
 #pragma once
 
 #include <complex>
@@ -50,17 +51,18 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
       const override {
     const auto t = list.empty() ? COULOMB : list[0].contType;
     const bool ours = MPISize(comm) == 1 && type4C == TYPE_4C::All &&
-                      approx == APPROXIMATION_TYPE_4C::None && list.size() == 17 &&
-                      (t == BARE_COULOMB || t == LLSS || t == SSSS);
+                      approx == APPROXIMATION_TYPE_4C::None &&
+                      ((list.size() == 17 && (t == BARE_COULOMB || t == LLSS || t == SSSS)) ||
+                       (list.size() == 29 && t == GAUNT));
     if (!ours) {
       GTODirectRelERIContraction<MatsT, IntsT>::twoBodyContract(comm, screen, list, pert,
                                                                 computeExchange, type4C, approx);
       return;
     }
     cqf_basis* b = basis();
-    const void* X[CQF_REL_NMAT];
-    void* AX[CQF_REL_NMAT];
-    for (int m = 0; m < CQF_REL_NMAT; m++) {
+    const void* X[CQF_REL_NMAT_GAUNT] = {};
+    void* AX[CQF_REL_NMAT_GAUNT] = {};
+    for (int m = 0; m < (int)list.size(); m++) {
       X[m] = list[m].X;
       AX[m] = list[m].AX;
     }
@@ -70,7 +72,8 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
     o.screen = screen ? 1 : 0;
     const int type = t == BARE_COULOMB ? CQF_REL_BARE_COULOMB
                      : t == LLSS       ? CQF_REL_LLSS
-                                       : CQF_REL_SSSS;
+                     : t == SSSS       ? CQF_REL_SSSS
+                                       : CQF_REL_GAUNT;
     cqf_status st = cqf_rel_two_body_contract(b, X, AX, type, computeExchange ? 1 : 0, &o,
                                               nullptr);
     if (st != CQF_OK) CErr(std::string("cqf_rel_two_body_contract: ") + cqf_last_error());

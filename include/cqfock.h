@@ -194,24 +194,32 @@ cqf_status cqf_two_body_contract_noalloc(cqf_basis* basis, const cqf_contraction
                                          const cqf_opts* opts, cqf_stats* stats);
 
 /* ---------------------------------------------------------------------
- * Four-component Dirac-Coulomb contraction.
+ * Four-component Dirac-Coulomb(-Gaunt) contraction.
  *
- * The 17 (X, AX) entries of one relativistic contraction, in the order of
+ * The (X, AX) entries of one relativistic contraction, in the order of
  * DIRAC_PAULI_SPINOR_COMP (include/particleintegrals/contract/
  * direct4C_libcint.hpp:279-310): Coulomb LL (MS), exchange LL (MS, MX, MY,
- * MZ), Coulomb SS (4), exchange SS (4), exchange LS (4).  Every X and AX is
- * an N x N complex (interleaved re, im) column-major matrix, N = nbasis.
+ * MZ), Coulomb SS (4), exchange SS (4), exchange LS (4) -- 17 entries --
+ * and, for GAUNT only, Coulomb LS (4), Coulomb SL (4), exchange SL (4) --
+ * 29 entries.  Every X and AX is an N x N complex (interleaved re, im)
+ * column-major matrix, N = nbasis.
  * --------------------------------------------------------------------- */
 typedef enum {
   CQF_CLLMS = 0, CQF_XLLMS, CQF_XLLMX, CQF_XLLMY, CQF_XLLMZ,
   CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ,
   CQF_XSSMS, CQF_XSSMX, CQF_XSSMY, CQF_XSSMZ,
   CQF_XLSMS, CQF_XLSMX, CQF_XLSMY, CQF_XLSMZ,
-  CQF_REL_NMAT
+  CQF_REL_NMAT,
+  CQF_CLSMS = CQF_REL_NMAT, CQF_CLSMX, CQF_CLSMY, CQF_CLSMZ,
+  CQF_CSLMS, CQF_CSLMX, CQF_CSLMY, CQF_CSLMZ,
+  CQF_XSLMS, CQF_XSLMX, CQF_XSLMY, CQF_XSLMZ,
+  CQF_REL_NMAT_GAUNT
 } cqf_rel_comp;
 
 /* TYPE of the 4C contraction (entry 0's contType in the reference). */
-typedef enum { CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2 } cqf_rel_type;
+typedef enum {
+  CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2, CQF_REL_GAUNT = 3
+} cqf_rel_type;
 
 /* GTODirectRelERIContraction::twoBodyContract (include/particleintegrals/
  * twopints/gtodirectreleri.hpp:75-94) -> directScaffoldLibcint
@@ -221,7 +229,15 @@ typedef enum { CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2 } cq
  *   LLSS: AX[CLLMS], AX[CSSM*] (Coulomb, order c^-2) and, with
  *         compute_exchange, AX[XLSM*] (:810-1441)
  *   SSSS: AX[CSSM*] and, with compute_exchange, AX[XSSM*] (:1841-2832).
- * Entries a type does not read or write may be NULL.  The densities must be
+ *   GAUNT (29 entries, :2833-3907): AX[CLSM*] (Coulomb, LS block, from the
+ *         LS and SL densities X[CLSM*], X[CSLM*]) and, with
+ *         compute_exchange, AX[XLLM*] (from the SS density X[XSSM*]),
+ *         AX[XSSM*] (from the LL density X[XLLM*]) and AX[XLSM*] (from the
+ *         SL density X[XSLM*]); always FP64.  AX[CSLM*] and AX[XSLM*] are
+ *         neither read nor written (the reference's list points them at the
+ *         CLSM* / XLSM* outputs; such aliasing is allowed).
+ * Entries a type does not read or write may be NULL; only the entries a
+ * type writes are zeroed.  The densities must be
  * Hermitian, as the reference requires (:144-145).  opts->is_complex is
  * ignored (always complex); opts->device_pointers, opts->stream, opts->screen
  * apply, and opts->precision = CQF_MIXED runs the quartets whose screening
@@ -232,23 +248,26 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* basis, const void* const* X, voi
                                      cqf_stats* stats);
 
 /* Hamiltonian switches of the 4C two-electron build (the reference's
- * HamiltonianOptions: BareCoulomb, DiracCoulomb, DiracCoulombSSSS, Libcint)
- * and the exchange scaling xHFX. */
+ * HamiltonianOptions: BareCoulomb, DiracCoulomb, DiracCoulombSSSS, Libcint,
+ * Gaunt) and the exchange scaling xHFX.  The Gauge term is not built. */
 typedef struct {
   int bare_coulomb, dirac_coulomb, dirac_coulomb_ssss, libcint;
   double xHFX;
+  int gaunt;
 } cqf_dc_opts;
-/* Defaults of the reference: all three on, libcint on, xHFX = 1. */
+/* Defaults of the reference: bare Coulomb, Dirac-Coulomb and SSSS on,
+ * libcint on, Gaunt off, xHFX = 1. */
 void cqf_dc_opts_default(cqf_dc_opts* o);
 
 /* FourCompFock::formGDDirect (include/fockbuilder/fourcompfock/impl.hpp:
  * 3752-4636): D[4] = Pauli components (scalar, MX, MY, MZ) of the
  * 2N x 2N complex 4C density (column-major, LL block first); G[4] receives
  * twoeH - xHFX K with the 2C^2 / -C^2 / 2C^4 / -C^4 weights of the LLSS and
- * SSSS terms, twoeH_LL = 2 J (libcint) or J, and the SL blocks set to the
- * conjugate transpose of the LS blocks.  opts as for
+ * SSSS terms, the Gaunt term's 2C^2 (LS Coulomb) and -C^2 (LL, SS, LS
+ * exchange) (impl.hpp:4235-4376), twoeH_LL = 2 J (libcint) or J, and the SL
+ * blocks set to the conjugate transpose of the LS blocks.  opts as for
  * cqf_rel_two_body_contract (CQF_MIXED applies to every contraction type of
- * the build, the bare-Coulomb one included). */
+ * the build but the Gaunt one, the bare-Coulomb one included). */
 cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const* G,
                             const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 

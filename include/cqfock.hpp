@@ -136,8 +136,9 @@ class GTODirectTPIContraction {
 
 // GTODirectRelERIContraction<dcomplex,double>::twoBodyContract
 // (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94): 17 entries
-// in DIRAC_PAULI_SPINOR_COMP order, contType of entry 0 = BARE_COULOMB, LLSS
-// or SSSS; every AX is overwritten (zeroed, then the contraction).
+// in DIRAC_PAULI_SPINOR_COMP order (29 for GAUNT), contType of entry 0 =
+// BARE_COULOMB, LLSS, SSSS or GAUNT; the AX the type writes are overwritten
+// (zeroed, then the contraction).
 class GTODirectRelERIContraction {
  public:
   explicit GTODirectRelERIContraction(std::shared_ptr<DirectTPI> tpi) : tpi_(std::move(tpi)) {}
@@ -145,18 +146,22 @@ class GTODirectRelERIContraction {
   void twoBodyContract(const bool screen,
                        std::vector<TwoBodyContraction<std::complex<double>>>& list,
                        const bool computeExchange = true, cqf_stats* stats = nullptr) const {
-    if (list.size() != CQF_REL_NMAT)
-      throw std::runtime_error("GTODirectRelERIContraction: the 4C list has 17 entries");
+    if (list.empty()) throw std::runtime_error("GTODirectRelERIContraction: empty list");
     int type;
     switch (list[0].contType) {
       case BARE_COULOMB: type = CQF_REL_BARE_COULOMB; break;
       case LLSS: type = CQF_REL_LLSS; break;
       case SSSS: type = CQF_REL_SSSS; break;
+      case GAUNT: type = CQF_REL_GAUNT; break;
       default: throw std::runtime_error("GTODirectRelERIContraction: unsupported contraction type");
     }
-    const void* X[CQF_REL_NMAT];
-    void* AX[CQF_REL_NMAT];
-    for (int m = 0; m < CQF_REL_NMAT; m++) {
+    const int n = type == CQF_REL_GAUNT ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
+    if ((int)list.size() != n)
+      throw std::runtime_error("GTODirectRelERIContraction: the 4C list has 17 entries (29 for "
+                               "GAUNT)");
+    const void* X[CQF_REL_NMAT_GAUNT] = {};
+    void* AX[CQF_REL_NMAT_GAUNT] = {};
+    for (int m = 0; m < n; m++) {
       X[m] = list[m].X;
       AX[m] = list[m].AX;
     }
@@ -175,20 +180,21 @@ class GTODirectRelERIContraction {
 
 // FourCompFock<dcomplex,double>::formGDDirect
 // (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) with the
-// HamiltonianOptions switches BareCoulomb, DiracCoulomb, DiracCoulombSSSS and
-// Libcint.  D and G: the four Pauli components (scalar, MX, MY, MZ) of the
-// 2N x 2N complex 4C matrices, column-major, LL block first.
+// HamiltonianOptions switches BareCoulomb, DiracCoulomb, DiracCoulombSSSS,
+// Libcint and Gaunt.  D and G: the four Pauli components (scalar, MX, MY,
+// MZ) of the 2N x 2N complex 4C matrices, column-major, LL block first.
 class FourCompFock {
  public:
   explicit FourCompFock(std::shared_ptr<DirectTPI> tpi, bool BareCoulomb = true,
                         bool DiracCoulomb = true, bool DiracCoulombSSSS = true,
-                        bool Libcint = true)
+                        bool Libcint = true, bool Gaunt = false)
       : tpi_(std::move(tpi)) {
     cqf_dc_opts_default(&dc_);
     dc_.bare_coulomb = BareCoulomb;
     dc_.dirac_coulomb = DiracCoulomb;
     dc_.dirac_coulomb_ssss = DiracCoulombSSSS;
     dc_.libcint = Libcint;
+    dc_.gaunt = Gaunt;
   }
 
   void formGD(const std::complex<double>* const D[4], std::complex<double>* const G[4],

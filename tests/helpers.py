@@ -76,3 +76,22 @@ def tight_ao_scale(basis, damp=1e-5):
         if sh.alpha.max() > 1e4:
             f[basis.offsets[s]:basis.offsets[s] + sh.size] = damp
     return f
+
+
+def gaunt_system(name):
+    """(basis, D, G) of a Dirac-Coulomb-Gaunt golden build (gaunt_*.npz):
+    the molecule and basis of the reference input, and the four Pauli
+    components of its density and of G = F - H."""
+    g = golden(name)
+    atoms = []
+    for line in str(g["geometry"]).splitlines():
+        s, x, y, z = line.split()
+        atoms.append((s, float(x), float(y), float(z)))
+    mol = Molecule.from_angstrom(atoms)
+    if "basisdef" in g:
+        basis = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
+    else:
+        basis = BasisSet.build(mol, str(g["basisname"]))
+    comps = ("SCALAR", "MX", "MY", "MZ")
+    return (basis, [np.asarray(g["D_" + c]) for c in comps],
+            [np.asarray(g["G_" + c]) for c in comps])

@@ -10,26 +10,9 @@ import pytest
 
 import oracle as O
 import twospinor as TS
-from chronusq_public_b200.basis import BasisSet, Molecule, parse_gbs
-from helpers import golden
+from helpers import gaunt_system as _system
 
 COMPS = ("SCALAR", "MX", "MY", "MZ")
-
-
-def _system(name):
-    g = golden(name)
-    atoms = []
-    for line in str(g["geometry"]).splitlines():
-        s, x, y, z = line.split()
-        atoms.append((s, float(x), float(y), float(z)))
-    mol = Molecule.from_angstrom(atoms)
-    if "basisdef" in g:
-        basis = BasisSet.build(mol, parse_gbs(str(g["basisdef"])))
-    else:
-        basis = BasisSet.build(mol, str(g["basisname"]))
-    D = [np.asarray(g["D_" + c]) for c in COMPS]
-    G = [np.asarray(g["G_" + c]) for c in COMPS]
-    return basis, D, G
 
 
 @pytest.mark.parametrize("name", ["gaunt_upu.npz", "gaunt_cuh3.npz"])

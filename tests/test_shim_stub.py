@@ -101,3 +101,39 @@ def test_rel_shim_rebuilds_basis_after_geometry_step(tmp_path):
         for k in range(5):
             AX = out[k * N * N:(k + 1) * N * N].reshape(N, N, order="F")
             assert np.abs(AX - ref[k]).max() < 1e-9, (g, k)
+
+
+@pytest.mark.gpu
+def test_rel_shim_gaunt_list_with_aliased_outputs(tmp_path):
+    """The reference's 29-entry GAUNT list through the shim, its CSLM* /
+    XSLM* AX pointing at the CLSM* / XLSM* outputs as in
+    fourcompfock/impl.hpp:4237-4274, against the oracle."""
+    import oracle as O
+    exe = _build(str(tmp_path))
+    b0, _ = _geometries()
+    _write_shells(tmp_path / "shells0.txt", b0)
+    N = b0.nbasis
+    rng = np.random.default_rng(13)
+    # a Hermitian 4C density: Pauli components of a Hermitian 2N x 2N matrix
+    blocks = []
+    for _ in range(4):
+        A = rng.standard_normal((2 * N, 2 * N)) + 1j * rng.standard_normal((2 * N, 2 * N))
+        blocks.append(0.05 * (A + A.conj().T))
+    ro, co = (0, N, 0, N), (0, N, N, 0)  # LL, SS, LS, SL
+    G = []
+    for k in range(4):
+        for c in range(4):
+            G.append(np.asfortranarray(blocks[c][ro[k]:ro[k] + N, co[k]:co[k] + N]))
+    for i, g in enumerate(G):
+        g.T.tofile(str(tmp_path / ("G%d.bin" % i)))
+    subprocess.check_call([exe, str(tmp_path), "gaunt"])
+    X = [G[0]] + G[0:4] + G[4:8] + G[4:8] + G[8:12] + G[8:12] + G[12:16] + G[12:16]
+    ref = O.OracleBasis(b0).rel_contract(X, 3, True)
+    out = np.fromfile(str(tmp_path / "GAUNT.bin"), dtype=np.complex128)
+    k = 0
+    for base in (1, 9, 13, 17):
+        for c in range(4):
+            AX = out[k * N * N:(k + 1) * N * N].reshape(N, N, order="F")
+            scale = max(1.0, np.abs(ref[base + c]).max())
+            assert np.abs(AX - ref[base + c]).max() < 1e-9 * scale, (base, c)
+            k += 1
