@@ -1247,10 +1247,24 @@ void build_tuples(RaisedTable& T, int c, int lmax) {
 }
 
 // Uncontracted primitive table for exponents (a,b,c,d) on centres (A..D).
+// Kernel: 1 / r12 (op == nullptr), or d_i d_j r12 (op = {i, j}, each 0..2 or
+// -1 for none; derivatives in r = r1 - r2).  For r12 the Hermite integrals
+// are the derivatives in R = P - Q of the s-type integral, which is the
+// Coulomb prefactor / (2 alpha) times f(T) = e^-T + (1 + 2T) F_0(T) (the
+// mean of |r| under the Gaussian of width 1 / (2 alpha) centred at R, with
+// T = alpha R^2); its T-derivatives are f' = F_0 - F_1 and
+// f^(n) = (-1)^(n-1) (F_(n-1) - F_n), so the McMurchie-Davidson recursion
+// runs unchanged on Ft_0 = f, Ft_n = F_n - F_(n-1), and the operator
+// derivatives d_i d_j shift the Hermite index by e_i + e_j.
 void prim_table(double a, const double* A, double b, const double* B, double c, const double* C,
-                double d, const double* D, RaisedTable& T) {
+                double d, const double* D, RaisedTable& T, const int* op = nullptr) {
   int l1 = T.lm[0], l2 = T.lm[1], l3 = T.lm[2], l4 = T.lm[3];
-  int lab = l1 + l2, lcd = l3 + l4, L = lab + lcd;
+  int lab = l1 + l2, lcd = l3 + l4;
+  int sh[3] = {0, 0, 0};
+  if (op)
+    for (int k = 0; k < 2; k++)
+      if (op[k] >= 0) sh[op[k]]++;
+  const int L = lab + lcd + sh[0] + sh[1] + sh[2];
   double p = a + b, q = c + d, alpha = p * q / (p + q);
   double P[3], Q[3], PQ[3];
   for (int x = 0; x < 3; x++) {
@@ -1265,6 +1279,7 @@ void prim_table(double a, const double* A, double b, const double* B, double c, 
   }
   double Kab = std::exp(-a * b / p * AB2), Kcd = std::exp(-c * d / q * CD2);
   double pref = 2.0 * std::pow(M_PI, 2.5) / (p * q * std::sqrt(p + q)) * Kab * Kcd;
+  if (op) pref /= 2.0 * alpha;
   std::vector<double> Eb[3], Ek[3];
   for (int x = 0; x < 3; x++) {
     hermite_E(l1, l2, p, P[x] - A[x], P[x] - B[x], Eb[x]);
@@ -1276,7 +1291,12 @@ void prim_table(double a, const double* A, double b, const double* B, double c, 
     return (((size_t)nn * L1 + t) * L1 + u) * L1 + v;
   };
   double F[96];
-  boys().eval(L, alpha * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]), F);
+  const double Targ = alpha * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+  boys().eval(L, Targ, F);
+  if (op) {
+    for (int nn = L; nn >= 1; nn--) F[nn] -= F[nn - 1];
+    F[0] = std::exp(-Targ) + (1.0 + 2.0 * Targ) * F[0];
+  }
   double f = 1.0;
   for (int nn = 0; nn <= L; nn++) { R[Ridx(nn, 0, 0, 0)] = f * F[nn]; f *= -2.0 * alpha; }
   for (int nn = L - 1; nn >= 0; nn--)
@@ -1317,7 +1337,7 @@ void prim_table(double a, const double* A, double b, const double* B, double c, 
                 for (int ph = 0; ph <= tc[2] + td[2]; ph++) {
                   double e = ex[ta] * ey[nu] * ez[ph];
                   if ((ta + nu + ph) & 1) e = -e;
-                  s += e * R[Ridx(0, t + ta, u + nu, v + ph)];
+                  s += e * R[Ridx(0, t + ta + sh[0], u + nu + sh[1], v + ph + sh[2])];
                 }
             g[(t * Lb1 + u) * Lb1 + v] = pref * s;
           }
@@ -1347,7 +1367,7 @@ void prim_table(double a, const double* A, double b, const double* B, double c, 
 // (bit 0..3 = s1..s4); comp = sum over differentiated centres, in order,
 // of 3-digit indices (x, y, z), the last centre varying fastest.
 void eri_deriv_quartet(const Basis& bs, int s1, int s2, int s3, int s4, int dmask,
-                       std::vector<double>& out) {
+                       std::vector<double>& out, const int* op = nullptr) {
   const int sh[4] = {s1, s2, s3, s4};
   const Shell* S[4] = {&bs.shells[s1], &bs.shells[s2], &bs.shells[s3], &bs.shells[s4]};
   int nd = 0;
@@ -1366,7 +1386,7 @@ void eri_deriv_quartet(const Basis& bs, int s1, int s2, int s3, int s4, int dmas
         for (size_t l = 0; l < S[3]->alpha.size(); l++) {
           const double ex[4] = {S[0]->alpha[i], S[1]->alpha[j], S[2]->alpha[k], S[3]->alpha[l]};
           const double cf = S[0]->coef[i] * S[1]->coef[j] * S[2]->coef[k] * S[3]->coef[l];
-          prim_table(ex[0], S[0]->O, ex[1], S[1]->O, ex[2], S[2]->O, ex[3], S[3]->O, T);
+          prim_table(ex[0], S[0]->O, ex[1], S[1]->O, ex[2], S[2]->O, ex[3], S[3]->O, T, op);
           const int nT2 = T.n[2] * T.n[3], nT1 = T.n[1];
           for (int a = 0; a < nc[0]; a++)
             for (int b = 0; b < nc[1]; b++)
@@ -1905,6 +1925,229 @@ void direct_gaunt(const Basis& bs, const cdbl* const* X, cdbl* const* AX, double
       for (int j = 0; j < i; j++) AX[m][j + (size_t)i * N] = std::conj(AX[m][i + (size_t)j * N]);
 }
 
+
+// ---------------------------------------------------------------- Gauge
+// The gauge part of the Breit interaction (direct4C_libcint.hpp:3908-5160):
+// the GAUNT list and update sites with the kernel -r_i r_i' / r12^3 of
+// (alpha_1 . r12)(alpha_2 . r12) / r12^3 in place of Gaunt's
+// -delta_ii' / r12 (the build then halves the Gaunt weight, so that the sum
+// is the Breit term).  Per element the integrals are
+//   V[i][i'][j][l] = (m d_j n | -r_i r_i' / r^3 | d_l k l)
+//                  = -delta_ii' T[j][l] + (m d_j n | d_i d_i' r12 | d_l k l),
+// using r_i r_i' / r^3 = delta_ii' / r - d_i d_i' r (derivatives in
+// r = r1 - r2).  With sigma_i sigma_j = Q_ij and general V the four update
+// kinds are
+//   LL exchange from SS:  -sum V^{ii'}_{jl} Q_ij D Q_li'
+//   SS exchange from LL:  -sum V^{ii'}_{jl} Q_ji D Q_i'l
+//   LS Coulomb from SL (1), LS (2):
+//                  1/2 sum V^{ii'}_{jl} Q_ij (tr[Q_li' D2] - tr[Q_i'l D1])
+//   LS exchange from SL:   sum V^{ii'}_{jl} Q_ij D Q_i'l
+// (for V = -delta T they reduce to the Gaunt maps); the image (l k | n m)
+// takes V with j and l exchanged (the kernel is even in r12).
+struct GV {
+  double v[3][3][3][3];  // [i][i'][j][l]
+};
+Q4 qij(int i, int j) {  // sigma_i sigma_j = delta_ij + i eps_ijm sigma_m
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  if (i == j) r.s = 1.0;
+  else {
+    const int m = 3 - i - j;
+    r.v[m] = (j == (i + 1) % 3) ? I1 : -I1;
+  }
+  return r;
+}
+cdbl qtr(const Q4& q) { return 2.0 * q.s; }  // trace of the 2 x 2 matrix
+Q4 qscale(const Q4& q, cdbl f) {
+  Q4 r{q.s * f, {q.v[0] * f, q.v[1] * f, q.v[2] * f}};
+  return r;
+}
+void qacc(Q4& a, const Q4& b) {
+  a.s += b.s;
+  for (int x = 0; x < 3; x++) a.v[x] += b.v[x];
+}
+GV gv_of(const double* T, const double* const* U, size_t q, size_t nq, bool img) {
+  // T: 9 Coulomb components [j][l]; U[6]: d_i d_i' r12 for (i, i') = xx, xy,
+  // xz, yy, yz, zz, each 9 components [j][l]
+  static const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  GV g;
+  for (int i = 0; i < 3; i++)
+    for (int ip = 0; ip < 3; ip++)
+      for (int j = 0; j < 3; j++)
+        for (int l = 0; l < 3; l++) {
+          const int jj = img ? l : j, ll = img ? j : l;
+          double v = U[sym[i][ip]][(size_t)(3 * jj + ll) * nq + q];
+          if (i == ip) v -= T[(size_t)(3 * jj + ll) * nq + q];
+          g.v[i][ip][j][l] = v;
+        }
+  return g;
+}
+Q4 gg_ll(const GV& g, const Q4& d) {
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  for (int i = 0; i < 3; i++)
+    for (int ip = 0; ip < 3; ip++)
+      for (int j = 0; j < 3; j++)
+        for (int l = 0; l < 3; l++)
+          if (g.v[i][ip][j][l] != 0.0)
+            qacc(r, qscale(qmul(qmul(qij(i, j), d), qij(l, ip)), -g.v[i][ip][j][l]));
+  return r;
+}
+Q4 gg_ss(const GV& g, const Q4& d) {
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  for (int i = 0; i < 3; i++)
+    for (int ip = 0; ip < 3; ip++)
+      for (int j = 0; j < 3; j++)
+        for (int l = 0; l < 3; l++)
+          if (g.v[i][ip][j][l] != 0.0)
+            qacc(r, qscale(qmul(qmul(qij(j, i), d), qij(ip, l)), -g.v[i][ip][j][l]));
+  return r;
+}
+Q4 gg_cls(const GV& g, const Q4& d1, const Q4& d2) {
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  for (int i = 0; i < 3; i++)
+    for (int ip = 0; ip < 3; ip++)
+      for (int j = 0; j < 3; j++)
+        for (int l = 0; l < 3; l++)
+          if (g.v[i][ip][j][l] != 0.0) {
+            const cdbl w = 0.5 * g.v[i][ip][j][l] *
+                           (qtr(qmul(qij(l, ip), d2)) - qtr(qmul(qij(ip, l), d1)));
+            qacc(r, qscale(qij(i, j), w));
+          }
+  return r;
+}
+Q4 gg_xls(const GV& g, const Q4& d) {
+  Q4 r{0.0, {0.0, 0.0, 0.0}};
+  for (int i = 0; i < 3; i++)
+    for (int ip = 0; ip < 3; ip++)
+      for (int j = 0; j < 3; j++)
+        for (int l = 0; l < 3; l++)
+          if (g.v[i][ip][j][l] != 0.0)
+            qacc(r, qscale(qmul(qmul(qij(i, j), d), qij(ip, l)), g.v[i][ip][j][l]));
+  return r;
+}
+
+// The V blocks of one contracted quartet: T (Coulomb, 9 components) and the
+// six d_i d_i' r12 blocks, derivatives on the centres in dmask.
+void gauge_blocks(const Basis& bs, int s1, int s2, int s3, int s4, int dmask,
+                  std::vector<double>& T, std::vector<double> (&U)[6]) {
+  static const int ops[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  eri_deriv_quartet(bs, s1, s2, s3, s4, dmask, T);
+  for (int k = 0; k < 6; k++) eri_deriv_quartet(bs, s1, s2, s3, s4, dmask, U[k], ops[k]);
+}
+
+// SchwarzGauge (:3960-4005): Q(o, d) = C1 sqrt(max |V|) over the block
+// (o d_j d | o d_l d) and its components, derivatives on the second
+// function of each pair, indexed [o + d * nshell].  The reference maxes over
+// libcint's 16 spin components of the same operator; here over the 81
+// spatial components of V.
+void schwarz_gauge(const Basis& bs, std::vector<double>& QB) {
+  const int ns = (int)bs.shells.size();
+  const double C1 = 1.0 / (2.0 * 137.035999074);
+  QB.assign((size_t)ns * ns, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int o = 0; o < ns; o++) {
+    std::vector<double> T, U[6];
+    for (int d = 0; d < ns; d++) {
+      gauge_blocks(bs, o, d, o, d, 10, T, U);
+      const size_t nq = T.size() / 9;
+      const double* Up[6];
+      for (int k = 0; k < 6; k++) Up[k] = U[k].data();
+      double mx = 0.0;
+      for (size_t q = 0; q < nq; q++) {
+        const GV g = gv_of(T.data(), Up, q, nq, false);
+        for (int a = 0; a < 81; a++) mx = std::max(mx, std::abs((&g.v[0][0][0][0])[a]));
+      }
+      QB[o + (size_t)d * ns] = C1 * std::sqrt(mx);
+    }
+  }
+}
+
+// The GAUGE contraction on the 29 (X, AX) entries; AX is zeroed first.
+// Quartets and sites as direct_gaunt (:4170-4215, :4400-5100), screened by
+// shMax Q(s1, s2) Q(s4, s3) (:4213).
+void direct_gauge(const Basis& bs, const cdbl* const* X, cdbl* const* AX, double thresh,
+                  const std::vector<double>& QB, bool exchange) {
+  const int ns = (int)bs.shells.size(), N = bs.nbasis;
+  const size_t NN = (size_t)N * N;
+  for (int m = 0; m < NGAUNT; m++) std::fill(AX[m], AX[m] + NN, cdbl(0.0));
+  std::vector<double> nrm((size_t)ns * ns, 0.0), tmp;
+  for (int base : {(int)XLSMS, (int)XSLMS, (int)XLLMS, (int)XSSMS})
+    for (int c = 0; c < 4; c++) {
+      norms_c(bs, X[base + c], tmp);
+      for (size_t i = 0; i < nrm.size(); i++) nrm[i] = std::max(nrm[i], std::abs(tmp[i]));
+    }
+  auto B = [&](int a, int b) { return nrm[a + (size_t)b * ns]; };
+  const int nth = omp_get_max_threads();
+  std::vector<cdbl> loc((size_t)nth * NGAUNT * NN, cdbl(0.0));
+#pragma omp parallel
+  {
+    const int tid = omp_get_thread_num();
+    cdbl* A[NGAUNT];
+    for (int m = 0; m < NGAUNT; m++) A[m] = &loc[((size_t)tid * NGAUNT + m) * NN];
+    auto ix = [N](int r, int c) { return (size_t)r + (size_t)c * N; };
+    auto put = [&](int base, size_t e, const Q4& q) {
+      A[base][e] += q.s;
+      for (int x = 0; x < 3; x++) A[base + 1 + x][e] += q.v[x];
+    };
+    std::vector<double> T, U[6];
+    size_t s1234 = 0;
+    for (int s1 = 0; s1 < ns; s1++)
+      for (int s2 = 0; s2 < ns; s2++) {
+        const double shMax12 = B(s2, s1);
+        for (int s3 = 0; s3 <= s2; s3++) {
+          const double shMax123 = std::max(std::max(B(s1, s3), B(s2, s3)), shMax12);
+          const int s4max = (s2 == s3) ? s1 : ns - 1;
+          for (int s4 = 0; s4 <= s4max; s4++, s1234++) {
+            if (s1234 % nth != (size_t)tid) continue;
+            double shMax = std::max(B(s1, s4), std::max(B(s2, s4), B(s3, s4)));
+            shMax = std::max(shMax, shMax123);
+            if (shMax * QB[s1 + (size_t)s2 * ns] * QB[s4 + (size_t)s3 * ns] < thresh) continue;
+            gauge_blocks(bs, s1, s2, s3, s4, 6, T, U);
+            const double* Up[6];
+            for (int k = 0; k < 6; k++) Up[k] = U[k].data();
+            const int n1 = bs.shells[s1].size(), n2 = bs.shells[s2].size();
+            const int n3 = bs.shells[s3].size(), n4 = bs.shells[s4].size();
+            const size_t nq = (size_t)n1 * n2 * n3 * n4;
+            const bool img = (s1 != s4) || (s2 != s3);
+            for (int i = 0; i < n1; i++)
+              for (int j = 0; j < n2; j++)
+                for (int k = 0; k < n3; k++)
+                  for (int l = 0; l < n4; l++) {
+                    const int m1 = bs.off[s1] + i, m2 = bs.off[s2] + j;
+                    const int m3 = bs.off[s3] + k, m4 = bs.off[s4] + l;
+                    const size_t q = (((size_t)i * n2 + j) * n3 + k) * n4 + l;
+                    const GV V = gv_of(T.data(), Up, q, nq, false);
+                    const GV Vt = gv_of(T.data(), Up, q, nq, true);
+                    if (exchange) {
+                      if (s1 >= s4) put(XLLMS, ix(m1, m4), gg_ll(V, dens(X, XSSMS, ix(m2, m3))));
+                      if (s1 < s4 || (s1 == s4 && s2 != s3))
+                        put(XLLMS, ix(m4, m1), gg_ll(Vt, dens(X, XSSMS, ix(m3, m2))));
+                      put(XSSMS, ix(m2, m3), gg_ss(V, dens(X, XLLMS, ix(m1, m4))));
+                      if (s1 != s4 && s2 == s3)
+                        put(XSSMS, ix(m3, m2), gg_ss(Vt, dens(X, XLLMS, ix(m4, m1))));
+                    }
+                    put(CLSMS, ix(m1, m2),
+                        gg_cls(V, dens(X, CSLMS, ix(m3, m4)), dens(X, CLSMS, ix(m4, m3))));
+                    if (img)
+                      put(CLSMS, ix(m4, m3),
+                          gg_cls(Vt, dens(X, CSLMS, ix(m2, m1)), dens(X, CLSMS, ix(m1, m2))));
+                    if (exchange) {
+                      put(XLSMS, ix(m1, m3), gg_xls(V, dens(X, XSLMS, ix(m2, m4))));
+                      if (img) put(XLSMS, ix(m4, m2), gg_xls(Vt, dens(X, XSLMS, ix(m3, m1))));
+                    }
+                  }
+          }
+        }
+      }
+  }
+  for (int t = 0; t < nth; t++)
+    for (int m = 0; m < NGAUNT; m++)
+      for (size_t e = 0; e < NN; e++) AX[m][e] += loc[((size_t)t * NGAUNT + m) * NN + e];
+  if (!exchange) return;
+  for (int m : {XLLMS, XLLMX, XLLMY, XLLMZ, XSSMS, XSSMX, XSSMY, XSSMZ})
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < i; j++) AX[m][j + (size_t)i * N] = std::conj(AX[m][i + (size_t)j * N]);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1918,7 +2161,7 @@ extern "C" {
 // (fourcompfock/impl.hpp:3901-3933), without it the 1C J/K contraction and
 // twoeH_LL = J (:3934-3969).
 int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare, int dc,
-                      int ssss, double xHFX, double thresh, int libcint, int gaunt) {
+                      int ssss, double xHFX, double thresh, int libcint, int gaunt, int gauge) {
   auto* bs = static_cast<Basis*>(b);
   const int N = bs->nbasis, N2 = 2 * N;
   const cdbl* const* D = reinterpret_cast<const cdbl* const*>(Dv);
@@ -1980,17 +2223,29 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
     if (exch)
       for (int c4 = 0; c4 < 4; c4++) add(K[c4], N, N, AX[XSSMS + c4], -C4);
   }
-  if (gaunt) {  // impl.hpp:4235-4376
+  // Gaunt and Gauge (impl.hpp:4228-4540): with the gauge term both are
+  // weighted C2 / 2 (their sum is the Breit term)
+  const double C2b = gauge ? 0.5 * C2 : C2;
+  auto breit_add = [&]() {
+    for (int c4 = 0; c4 < 4; c4++) add(twoeH[c4], 0, N, AX[CLSMS + c4], 2.0 * C2b);
+    if (exch)
+      for (int c4 = 0; c4 < 4; c4++) {
+        add(K[c4], 0, 0, AX[XLLMS + c4], -C2b);
+        add(K[c4], N, N, AX[XSSMS + c4], -C2b);
+        add(K[c4], 0, N, AX[XLSMS + c4], -C2b);
+      }
+  };
+  if (gaunt) {
     std::vector<double> QG;
     schwarz_gaunt(*bs, QG);
     direct_gaunt(*bs, X, AX, thresh, QG, exch);
-    for (int c4 = 0; c4 < 4; c4++) add(twoeH[c4], 0, N, AX[CLSMS + c4], 2.0 * C2);
-    if (exch)
-      for (int c4 = 0; c4 < 4; c4++) {
-        add(K[c4], 0, 0, AX[XLLMS + c4], -C2);
-        add(K[c4], N, N, AX[XSSMS + c4], -C2);
-        add(K[c4], 0, N, AX[XLSMS + c4], -C2);
-      }
+    breit_add();
+  }
+  if (gauge) {
+    std::vector<double> QB;
+    schwarz_gauge(*bs, QB);
+    direct_gauge(*bs, X, AX, thresh, QB, exch);
+    breit_add();
   }
   // LS -> SL as the conjugate transpose, then G = twoeH - xHFX K
   for (int c4 = 0; c4 < 4; c4++) {
@@ -2003,10 +2258,10 @@ int orc_dirac_coulomb(void* b, const void* const* Dv, void* const* Gv, int bare,
   return 0;
 }
 
-// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS, 3 GAUNT) of
+// One contraction type (0 BARE_COULOMB, 1 LLSS, 2 SSSS, 3 GAUNT, 4 GAUGE) of
 // GTODirectRelERIContraction::twoBodyContract on the N x N complex (X, AX)
-// entries in DIRAC_PAULI_SPINOR_COMP order (17, or 29 for GAUNT); AX is
-// zeroed first (direct4C_libcint.hpp:313-314).
+// entries in DIRAC_PAULI_SPINOR_COMP order (17, or 29 for GAUNT and GAUGE);
+// AX is zeroed first (direct4C_libcint.hpp:313-314).
 // Derivative ERIs of one contracted shell quartet (eri_deriv_quartet):
 // comp-major blocks over the AO functions of s1..s4, derivatives (d/dr of
 // the orbital) on the centres in dmask (bit 0..3 = s1..s4); returns the
@@ -2015,6 +2270,18 @@ int orc_eri_deriv_quartet(void* b, int s1, int s2, int s3, int s4, int dmask, do
   const auto* bs = static_cast<const Basis*>(b);
   std::vector<double> buf;
   eri_deriv_quartet(*bs, s1, s2, s3, s4, dmask, buf);
+  std::copy(buf.begin(), buf.end(), out);
+  return (int)buf.size();
+}
+
+// As orc_eri_deriv_quartet with the kernel d_i d_j r12 (i, j = 0..2, -1 for
+// none; derivatives in r = r1 - r2) in place of 1 / r12.
+int orc_r12_deriv_quartet(void* b, int s1, int s2, int s3, int s4, int dmask, int i, int j,
+                          double* out) {
+  const auto* bs = static_cast<const Basis*>(b);
+  const int op[2] = {i, j};
+  std::vector<double> buf;
+  eri_deriv_quartet(*bs, s1, s2, s3, s4, dmask, buf, op);
   std::copy(buf.begin(), buf.end(), out);
   return (int)buf.size();
 }
@@ -2028,6 +2295,12 @@ int orc_rel_contract(void* b, int type, const void* const* Xv, void* const* AXv,
     std::vector<double> QG;
     schwarz_gaunt(*bs, QG);
     direct_gaunt(*bs, X, AX, thresh, QG, exchange != 0);
+    return 0;
+  }
+  if (type == 4) {
+    std::vector<double> QB;
+    schwarz_gauge(*bs, QB);
+    direct_gauge(*bs, X, AX, thresh, QB, exchange != 0);
     return 0;
   }
   Schwarz4C Qs;

@@ -60,7 +60,8 @@ def lib():
                                 C.c_double, C.c_double, dp]
         L.orc_dirac_coulomb.argtypes = [C.c_void_p, C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p), C.c_int, C.c_int,
-                                        C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
+                                        C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                        C.c_int]
         L.orc_dirac_coulomb.restype = C.c_int
         L.orc_rel_contract.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                        C.POINTER(C.c_void_p), C.c_double, C.c_int]
@@ -68,6 +69,8 @@ def lib():
         L.orc_eri_deriv_quartet.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                             C.c_int, C.c_int, dp]
         L.orc_eri_deriv_quartet.restype = C.c_int
+        L.orc_r12_deriv_quartet.argtypes = [C.c_void_p] + [C.c_int] * 7 + [dp]
+        L.orc_r12_deriv_quartet.restype = C.c_int
         _lib = L
     return _lib
 
@@ -157,6 +160,15 @@ class OracleBasis:
         k = lib().orc_eri_deriv_quartet(self.h, s1, s2, s3, s4, dmask, _dp(out))
         return out[:k].reshape([3 ** nd] + n)
 
+    def r12_deriv_quartet(self, s1, s2, s3, s4, dmask, i=-1, j=-1):
+        """As eri_deriv_quartet with the kernel d_i d_j r12 (i, j = 0..2,
+        -1 for none; derivatives in r = r1 - r2) in place of 1 / r12."""
+        n = [int(self.sizes[s]) for s in (s1, s2, s3, s4)]
+        nd = bin(dmask & 15).count("1")
+        out = np.zeros(3 ** nd * int(np.prod(n)))
+        k = lib().orc_r12_deriv_quartet(self.h, s1, s2, s3, s4, dmask, i, j, _dp(out))
+        return out[:k].reshape([3 ** nd] + n)
+
     def schwarz(self):
         Q = np.zeros((self.nshell, self.nshell), order="F")
         lib().orc_schwarz(self.h, _dp(Q))
@@ -192,7 +204,7 @@ class OracleBasis:
         return AX
 
     def dirac_coulomb(self, D, bare=True, dc=True, ssss=True, xHFX=1.0,
-                      thresh=1e-12, libcint=True, gaunt=False):
+                      thresh=1e-12, libcint=True, gaunt=False, gauge=False):
         """FourCompFock::formGDDirect: D = [S, X, Y, Z] Pauli components of
         the 2N x 2N density; returns G = twoeH - xHFX K (same layout)."""
         Ds = [np.asfortranarray(d, dtype=np.complex128) for d in D]
@@ -200,14 +212,14 @@ class OracleBasis:
         dp_ = (C.c_void_p * 4)(*[d.ctypes.data for d in Ds])
         gp_ = (C.c_void_p * 4)(*[g.ctypes.data for g in Gs])
         lib().orc_dirac_coulomb(self.h, dp_, gp_, int(bare), int(dc), int(ssss),
-                                xHFX, thresh, int(libcint), int(gaunt))
+                                xHFX, thresh, int(libcint), int(gaunt), int(gauge))
         return Gs
 
     def rel_contract(self, X, contType, exchange=True, thresh=1e-12):
         """GTODirectRelERIContraction::twoBodyContract: X = the 17 N x N
-        complex matrices (29 for GAUNT, contType 3; DIRAC_PAULI_SPINOR_COMP
-        order); returns as many AX."""
-        n = 29 if contType == 3 else 17
+        complex matrices (29 for GAUNT and GAUGE, contType 3 and 4;
+        DIRAC_PAULI_SPINOR_COMP order); returns as many AX."""
+        n = 29 if contType in (3, 4) else 17
         assert len(X) == n
         Xs = [np.asfortranarray(x, dtype=np.complex128) for x in X]
         AX = [np.zeros_like(x, order="F") for x in Xs]

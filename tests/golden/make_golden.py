@@ -19,6 +19,8 @@ Sources (paths within xsligroup/chronusq_public):
 * tests/scf/reference/UPu_184+_P_DCG_finitenuc.bin.ref and CuH3_321g_DCG.bin.ref
   -- converged 4C Dirac-Coulomb-Gaunt SCFs (inputs under
   tests/scf/serial/fourcomp/): D and G = F - H of the final build.
+* tests/scf/reference/UPu_184+_P_DCGGS_finitenuc.bin.ref -- the same with
+  SSSS, Gaunt and Gauge on (Dirac-Coulomb-Breit).
 
 HDF5 datasets written from column-major buffers read back transposed; the
 fixtures store them in natural (row = first index) orientation.
@@ -137,7 +139,10 @@ def main(ref_root):
     for name, inp, key in [
             ("UPu_184+_P_DCG_finitenuc", "tests/scf/serial/fourcomp/UPu_184+_P_DCG_finitenuc.inp",
              "gaunt_upu"),
-            ("CuH3_321g_DCG", "tests/scf/serial/fourcomp/CuH3_321g_DCG.inp", "gaunt_cuh3")]:
+            ("CuH3_321g_DCG", "tests/scf/serial/fourcomp/CuH3_321g_DCG.inp", "gaunt_cuh3"),
+            # bare + Dirac-Coulomb + SSSS + Gaunt + Gauge (Breit)
+            ("UPu_184+_P_DCGGS_finitenuc",
+             "tests/scf/serial/fourcomp/UPu_184+_P_DCGGS_finitenuc.inp", "breit_upu")]:
         f = H5File(os.path.join(rd, name + ".bin.ref"))
         out = {}
         for comp in ("SCALAR", "MX", "MY", "MZ"):

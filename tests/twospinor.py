@@ -18,6 +18,14 @@ X = ab + ba, Y = i (ab - ba), Z = aa - bb (the same convention for D and G).
   SL: (i / 2c) sum_j (sigma_j sigma_k)_ss' d_j chi_mu chi_nu --
   and (PQ|RS)_Gaunt = -sum_k (rho^k_PQ | rho^k_RS).
 
+* Breit gauge part, -(alpha_1 . r)(alpha_2 . r) / r^3 (r = r1 - r2): the
+  same densities with the kernel K_ii' = -r_i r_i' / r^3 between rho^i and
+  rho^i' in place of Gaunt's -delta_ii' / r.  Since
+  r_i r_i' / r^3 = delta_ii' / r - d_i d_i' r, it is Gaunt plus the kernel
+  d_i d_i' r12, whose integrals are the oracle's r12 integrals with the
+  Hermite index shifted (checked against the Coulomb ones through
+  sum_i d_i d_i r = 2 / r in test_gaunt_golden.py).
+
 Derivative ERIs (d/dr of the orbitals) come from the oracle's
 eri_deriv_quartet, checked against finite differences in
 test_oracle_deriv.py.
@@ -110,3 +118,57 @@ def gaunt(basis, D):
     KLS = np.einsum("jlxuty,jlabcd,buct->axdy", M_LSLS, T, Db["SL"], **o)
     KSL = np.einsum("jlxuty,jlabcd,audt->bxcy", M_SLSL, T, Db["LS"], **o)
     return assemble({"LL": -KLL, "SS": -KSS, "LS": JLS - KLS, "SL": JSL - KSL}, N)
+
+
+def r12_tensor(basis):
+    """U[i, i', j, l, a, b, c, d] = (a d_j b | d_i d_i' r12 | c d_l d)."""
+    ob = O.OracleBasis(basis)
+    N = basis.nbasis
+    off, sz = basis.offsets, basis.sizes
+    ns = basis.nshell
+    U = np.zeros((3, 3, 3, 3, N, N, N, N))
+    for i in range(3):
+        for ip in range(i, 3):
+            for a in range(ns):
+                for b in range(ns):
+                    for c in range(ns):
+                        for d in range(ns):
+                            blk = ob.r12_deriv_quartet(a, b, c, d, 10, i, ip)
+                            U[i, ip, :, :, off[a]:off[a] + sz[a], off[b]:off[b] + sz[b],
+                              off[c]:off[c] + sz[c], off[d]:off[d] + sz[d]] = \
+                                blk.reshape(3, 3, sz[a], sz[b], sz[c], sz[d])
+            U[ip, i] = U[i, ip]
+    return U
+
+
+def kernel_term(basis, D, V):
+    """G = J - K of the two-electron operator sum_ii' alpha_1i K_ii' alpha_2i'
+    with V[i, i', j, l, a, b, c, d] = (a d_j b | K_ii' | c d_l d) (4 Pauli
+    components); V = -delta_ii' T is the Gaunt term."""
+    N = basis.nbasis
+    Db = spin_blocks(D, N)
+    k4 = C2
+    o = dict(optimize=True)
+    A = {"LSLS": -k4 * np.einsum("ijxy,kltu,ikjlabcd->xytuabcd", SS, SS, V, **o),
+         "LSSL": k4 * np.einsum("ijxy,lktu,ikjlabcd->xytuabcd", SS, SS, V, **o),
+         "SLLS": k4 * np.einsum("jixy,kltu,ikjlabcd->xytuabcd", SS, SS, V, **o),
+         "SLSL": -k4 * np.einsum("jixy,lktu,ikjlabcd->xytuabcd", SS, SS, V, **o)}
+    JLS = (np.einsum("xytuabcd,duct->axby", A["LSLS"], Db["SL"], **o)
+           + np.einsum("xytuabcd,cudt->axby", A["LSSL"], Db["LS"], **o))
+    JSL = (np.einsum("xytuabcd,duct->bxay", A["SLLS"], Db["SL"], **o)
+           + np.einsum("xytuabcd,cudt->bxay", A["SLSL"], Db["LS"], **o))
+    KLL = np.einsum("xutyabcd,budt->axcy", A["LSSL"], Db["SS"], **o)
+    KSS = np.einsum("xutyabcd,auct->bxdy", A["SLLS"], Db["LL"], **o)
+    KLS = np.einsum("xutyabcd,buct->axdy", A["LSLS"], Db["SL"], **o)
+    KSL = np.einsum("xutyabcd,audt->bxcy", A["SLSL"], Db["LS"], **o)
+    return assemble({"LL": -KLL, "SS": -KSS, "LS": JLS - KLS, "SL": JSL - KSL}, N)
+
+
+def gauge(basis, D):
+    """The gauge term -(alpha_1 . r)(alpha_2 . r) / r^3 at the Gaunt term's
+    weight (the Breit build takes half of each)."""
+    T = deriv_tensor(basis, 10)
+    V = r12_tensor(basis)
+    for i in range(3):
+        V[i, i] -= T
+    return kernel_term(basis, D, V)
