@@ -35,7 +35,7 @@ EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
 (CQF_CLSMS, CQF_CLSMX, CQF_CLSMY, CQF_CLSMZ, CQF_CSLMS, CQF_CSLMX, CQF_CSLMY,
  CQF_CSLMZ, CQF_XSLMS, CQF_XSLMX, CQF_XSLMY, CQF_XSLMZ,
  CQF_REL_NMAT_GAUNT) = range(17, 30)
-CQF_REL_BARE_COULOMB, CQF_REL_LLSS, CQF_REL_SSSS, CQF_REL_GAUNT = range(4)
+CQF_REL_BARE_COULOMB, CQF_REL_LLSS, CQF_REL_SSSS, CQF_REL_GAUNT, CQF_REL_GAUGE = range(5)
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 
@@ -68,7 +68,7 @@ class CqfStats(C.Structure):
 class CqfDcOpts(C.Structure):
     _fields_ = [("bare_coulomb", C.c_int), ("dirac_coulomb", C.c_int),
                 ("dirac_coulomb_ssss", C.c_int), ("libcint", C.c_int),
-                ("xHFX", C.c_double), ("gaunt", C.c_int)]
+                ("xHFX", C.c_double), ("gaunt", C.c_int), ("gauge", C.c_int)]
 
 
 class CqfServerOpts(C.Structure):

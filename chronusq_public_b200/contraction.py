@@ -300,10 +300,11 @@ class GTODirectTPIContraction:
 
 
 # ---------------------------------------------------------------- 4C
-BARE_COULOMB, LLSS, SSSS, GAUNT = (_cabi.CQF_REL_BARE_COULOMB, _cabi.CQF_REL_LLSS,
-                                   _cabi.CQF_REL_SSSS, _cabi.CQF_REL_GAUNT)
+BARE_COULOMB, LLSS, SSSS, GAUNT, GAUGE = (
+    _cabi.CQF_REL_BARE_COULOMB, _cabi.CQF_REL_LLSS, _cabi.CQF_REL_SSSS, _cabi.CQF_REL_GAUNT,
+    _cabi.CQF_REL_GAUGE)
 # DIRAC_PAULI_SPINOR_COMP order of the 17 (X, AX) entries, and the 12 the
-# GAUNT list adds (include/particleintegrals/contract/direct4C_libcint.hpp:
+# GAUNT and GAUGE lists add (include/particleintegrals/contract/direct4C_libcint.hpp:
 # 279-310)
 REL_COMPS = ("CLLMS", "XLLMS", "XLLMX", "XLLMY", "XLLMZ", "CSSMS", "CSSMX",
              "CSSMY", "CSSMZ", "XSSMS", "XSSMX", "XSSMY", "XSSMZ", "XLSMS",
@@ -345,13 +346,14 @@ class GTODirectRelERIContraction:
                         screen: bool = True, precision: str = "fp64",
                         fp32_cutoff: float = 0.0, stream=None) -> None:
         """17 entries in REL_COMPS order (29 in GAUNT_COMPS order for
-        GAUNT; None for entries the type does not use).  The AX the type
-        writes are overwritten (the reference zeroes AX on entry); X and AX
-        are N x N complex (numpy, or column-major CUDA complex128 tensors).
+        GAUNT and GAUGE; None for entries the type does not use).  The AX the
+        type writes are overwritten (the reference zeroes AX on entry); X and
+        AX are N x N complex (numpy, or column-major CUDA complex128 tensors).
         precision="mixed" runs the quartets whose screening bound is below
         fp32_cutoff in FP32 arithmetic (the reference is FP64 throughout;
-        GAUNT always runs in FP64)."""
-        n = _cabi.CQF_REL_NMAT_GAUNT if contType == GAUNT else _cabi.CQF_REL_NMAT
+        GAUNT and GAUGE always run in FP64)."""
+        n = (_cabi.CQF_REL_NMAT_GAUNT if contType in (GAUNT, GAUGE)
+             else _cabi.CQF_REL_NMAT)
         if len(matList) != n:
             raise ValueError("a 4C contraction list has %d entries" % n)
         N = self.tpi.nbasis

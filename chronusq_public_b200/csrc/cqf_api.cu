@@ -801,7 +801,7 @@ void free_basis(cqf_basis* B) {
                     (void*)B->d_schwarz,
                     (void*)B->d_sph, (void*)B->d_sphOff, (void*)B->d_ao2shell,
                     (void*)B->d_cart2shell, (void*)B->d_ws, (void*)B->d_counters,
-                    (void*)B->d_flags, (void*)B->d_qLL, (void*)B->d_qSS, (void*)B->d_qG,
+                    (void*)B->d_flags, (void*)B->d_qLL, (void*)B->d_qSS, (void*)B->d_qG, (void*)B->d_qB,
                     (void*)B->d_relws})
       if (p) cudaFreeAsync(p, st);
     cudaStreamSynchronize(st);

@@ -228,7 +228,8 @@ struct cqf_basis {
   double* d_qLL = nullptr;
   double* d_qSS = nullptr;
   double* d_qG = nullptr;  // Gaunt: qG[d + o * nshell], derivative on shell d
-  bool rel_qLL = false, rel_qSS = false, rel_qG = false;
+  double* d_qB = nullptr;  // gauge, the same layout
+  bool rel_qLL = false, rel_qSS = false, rel_qG = false, rel_qB = false;
   void* d_relws = nullptr;
   size_t relws_bytes = 0;
   std::mutex mu;

@@ -129,11 +129,13 @@ __device__ __forceinline__ int axis_factor(const T* E, int l2r, int Lr, int i, i
   return n;
 }
 
-// G[tuv] += s * sum f_x[tau] f_y[nu] f_z[phi] R_{t+tau,u+nu,v+phi} for
-// t+u+v <= Lb; the ket factors carry the (-1)^(tau+nu+phi) sign already.
+// G[tuv] += s * sum f_x[tau] f_y[nu] f_z[phi] R_{t+tau+sx,u+nu+sy,v+phi+sz}
+// for t+u+v <= Lb; the ket factors carry the (-1)^(tau+nu+phi) sign
+// already; (sx, sy, sz): the Hermite shift of an operator derivative.
 template <typename T>
 __device__ __forceinline__ void ket_add(T* G, T s, const T* fx, int nx, const T* fy, int ny,
-                                        const T* fz, int nz, int Lb, const T* Rv) {
+                                        const T* fz, int nz, int Lb, const T* Rv, int sx = 0,
+                                        int sy = 0, int sz = 0) {
 #pragma unroll 1
   for (int t = 0; t <= Lb; t++)
 #pragma unroll 1
@@ -150,7 +152,8 @@ __device__ __forceinline__ void ket_add(T* G, T s, const T* fx, int nx, const T*
             const T fab = fa * fy[b];
             if (fab == T(0)) continue;
 #pragma unroll 1
-            for (int c = 0; c < nz; c++) acc += fab * fz[c] * Rv[hidx(t + a, u + b, v + c)];
+            for (int c = 0; c < nz; c++)
+              acc += fab * fz[c] * Rv[hidx(t + a + sx, u + b + sy, v + c + sz)];
           }
         }
         G[hidx(t, u, v)] += s * acc;
@@ -197,6 +200,26 @@ __device__ __forceinline__ void pair_exps(const ShellDev& SA, const ShellDev& SB
 }
 
 constexpr double PI52X2 = 34.986836655249725693;  // 2 pi^(5/2)
+
+// The kernel r12 in place of 1 / r12: the Hermite integrals are the
+// R = P - Q derivatives of the Coulomb prefactor / (2 alpha) times
+// f(T) = e^-T + (1 + 2T) F_0(T) (the mean of |r| under the Gaussian of the
+// pair product), f' = F_0 - F_1, f^(n) = (-1)^(n-1) (F_(n-1) - F_n); the
+// McMurchie-Davidson recursion then runs on Ft_0 = f, Ft_n = F_n - F_(n-1)
+// (replaces F_0..F_L in place).  An operator derivative d_i d_j r12
+// (derivatives in r = r1 - r2) shifts the Hermite index by e_i + e_j.
+// the symmetric operator-derivative pairs (i, i'), i <= i': xx, xy, xz, yy,
+// yz, zz
+__host__ __device__ __forceinline__ void op_pair(int k, int& i, int& ip) {
+  i = (k >= 3) + (k >= 5);
+  ip = k - (i == 0 ? 0 : (i == 1 ? 2 : 3));
+}
+
+__device__ __forceinline__ void r12_aux(int L, double T, double* F) {
+#pragma unroll 1
+  for (int n = L; n >= 1; n--) F[n] -= F[n - 1];
+  F[0] = exp(-T) + (1.0 + 2.0 * T) * F[0];
+}
 
 struct RelLaunch {
   const PairDev* pairs;
@@ -1326,9 +1349,167 @@ __device__ __forceinline__ void gaunt_sites(const GauntLaunch& a, const double* 
   }
 }
 
+// ------------------------------------------------ gauge (Breit) term
+// The gauge part of the Breit interaction (direct4C_libcint.hpp:3908-5160):
+// the GAUNT list, quartets and update sites with the kernel
+// K_ii' = -r_i r_i' / r12^3 between the densities rho^i, rho^i' in place of
+// Gaunt's -delta_ii' / r12.  Per element
+//   V[i][i'][j][l] = (m d_j n | K_ii' | d_l k l)
+//                  = -delta_ii' T[j][l] + (m d_j n | d_i d_i' r12 | d_l k l)
+// (r_i r_i' / r^3 = delta_ii' / r - d_i d_i' r), and with
+// W(M, D) = sum_jl M_jl s_j D s_l (the closed form above) the update kinds
+// are, Q_ij = s_i s_j:
+//   LL exchange from SS:  -sum_ii' s_i W(V^{ii'}, D) s_i'
+//   SS exchange from LL:  -sum_jl  s_j W(V_{jl}, D) s_l     (M_ii' = V^{ii'}_jl)
+//   LS Coulomb from SL (1), LS (2):  1/2 sum_ij Q_ij sum_i'l V^{ii'}_jl
+//                                     (tr[Q_li' D2] - tr[Q_i'l D1])
+//   LS exchange from SL:  sum_il s_i W(N_il, D) s_l         (N_ji' = V^{ii'}_jl)
+// (for V = -delta T they are the Gaunt maps).  The image takes V with j
+// and l exchanged (the kernel is even in r12 and symmetric in i, i').
+struct GVd {
+  double v[3][3][3][3];  // [i][i'][j][l]
+};
+__device__ __forceinline__ Q4 qunit(int a) {  // sigma_a
+  Q4 r{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  if (a == 0) r.x = make_double2(1, 0);
+  else if (a == 1) r.y = make_double2(1, 0);
+  else r.z = make_double2(1, 0);
+  return r;
+}
+__device__ __forceinline__ Q4 q_of(const Z4& z) { return Q4{z.c[0], z.c[1], z.c[2], z.c[3]}; }
+__device__ __forceinline__ Z4 z_of(const Q4& q) { return Z4{{q.s, q.x, q.y, q.z}}; }
+__device__ __forceinline__ void zacc(Z4& a, const Q4& b, double f) {
+  a.c[0] = cadd(a.c[0], cscale(b.s, f));
+  a.c[1] = cadd(a.c[1], cscale(b.x, f));
+  a.c[2] = cadd(a.c[2], cscale(b.y, f));
+  a.c[3] = cadd(a.c[3], cscale(b.z, f));
+}
+// W(M, D) = sum_jl M_jl s_j D s_l = d0 t - i d.tau + (i d0 tau + S' d).s
+__device__ __forceinline__ Q4 w_map(const double (*M)[3], const Z4& d) {
+  GInv g;
+  double v[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) v[k] = M[k / 3][k % 3];
+  gaunt_inv(v, false, g);
+  Q4 r;
+  r.s = csub(cscale(d.c[0], g.t), ctimes_i(vdot(d, g.tau)));
+  double2 w[3];
+#pragma unroll
+  for (int x = 0; x < 3; x++) w[x] = cadd(ctimes_i(cscale(d.c[0], g.tau[x])), vmat(d, g.S, x, false));
+  r.x = w[0];
+  r.y = w[1];
+  r.z = w[2];
+  return r;
+}
+__device__ Z4 gauge_ll(const GVd& V, const Z4& d) {
+  Z4 r{{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)}};
+#pragma unroll 1
+  for (int i = 0; i < 3; i++)
+#pragma unroll 1
+    for (int ip = 0; ip < 3; ip++)
+      zacc(r, qmul(qmul(qunit(i), w_map(V.v[i][ip], d)), qunit(ip)), -1.0);
+  return r;
+}
+__device__ Z4 gauge_ss(const GVd& V, const Z4& d) {
+  Z4 r{{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)}};
+#pragma unroll 1
+  for (int j = 0; j < 3; j++)
+#pragma unroll 1
+    for (int l = 0; l < 3; l++) {
+      double M[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int ip = 0; ip < 3; ip++) M[i][ip] = V.v[i][ip][j][l];
+      zacc(r, qmul(qmul(qunit(j), w_map(M, d)), qunit(l)), -1.0);
+    }
+  return r;
+}
+__device__ Z4 gauge_xls(const GVd& V, const Z4& d) {
+  Z4 r{{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)}};
+#pragma unroll 1
+  for (int i = 0; i < 3; i++)
+#pragma unroll 1
+    for (int l = 0; l < 3; l++) {
+      double M[3][3];
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int ip = 0; ip < 3; ip++) M[j][ip] = V.v[i][ip][j][l];
+      zacc(r, qmul(qmul(qunit(i), w_map(M, d)), qunit(l)), 1.0);
+    }
+  return r;
+}
+// tr[s_a s_b D] = 2 (delta_ab d0 + i eps_abm d_m)
+__device__ __forceinline__ double2 tr_qq(int a, int b, const Z4& d) {
+  if (a == b) return cscale(d.c[0], 2.0);
+  const int m = 3 - a - b;
+  const double e = (b == (a + 1) % 3) ? 2.0 : -2.0;
+  return ctimes_i(cscale(d.c[1 + m], e));
+}
+__device__ Z4 gauge_cls(const GVd& V, const Z4& d1, const Z4& d2) {
+  double2 sv[3][3];  // [l][i']
+#pragma unroll 1
+  for (int l = 0; l < 3; l++)
+#pragma unroll 1
+    for (int ip = 0; ip < 3; ip++) sv[l][ip] = csub(tr_qq(l, ip, d2), tr_qq(ip, l, d1));
+  Z4 r{{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)}};
+#pragma unroll 1
+  for (int i = 0; i < 3; i++)
+#pragma unroll 1
+    for (int j = 0; j < 3; j++) {
+      double2 c = make_double2(0, 0);
+#pragma unroll
+      for (int ip = 0; ip < 3; ip++)
+#pragma unroll
+        for (int l = 0; l < 3; l++) c = cadd(c, cscale(sv[l][ip], V.v[i][ip][j][l]));
+      c = cscale(c, 0.5);
+      // Q_ij = delta_ij + i eps_ijm s_m
+      if (i == j) r.c[0] = cadd(r.c[0], c);
+      else {
+        const int m = 3 - i - j;
+        const double e = (j == (i + 1) % 3) ? 1.0 : -1.0;
+        r.c[1 + m] = cadd(r.c[1 + m], ctimes_i(cscale(c, e)));
+      }
+    }
+  return r;
+}
+
+// The gauge update sites of one reference quartet at one element (as
+// gaunt_sites), V and its image Vt.
+__device__ void gauge_sites(const GauntLaunch& a, const GVd& V, const GVd& Vt, int s1, int s2,
+                            int s3, int s4, int m1, int m2, int m3, int m4) {
+  const size_t nc = a.ncart;
+  auto ix = [nc](int r, int c) -> size_t { return (size_t)r + (size_t)c * nc; };
+  const bool img = (s1 != s4) || (s2 != s3);
+  if (a.exchange) {
+    const double w14 = (s1 == s4) ? 0.5 : 1.0, w23 = (s2 == s3) ? 0.5 : 1.0;
+    if (s1 >= s4) add4(a.Kll, ix(m1, m4), gauge_ll(V, ld4(a.Xss, ix(m2, m3))), w14);
+    if (s1 < s4 || (s1 == s4 && s2 != s3))
+      add4(a.Kll, ix(m4, m1), gauge_ll(Vt, ld4(a.Xss, ix(m3, m2))), w14);
+    add4(a.Kss, ix(m2, m3), gauge_ss(V, ld4(a.Xll, ix(m1, m4))), w23);
+    if (s1 != s4 && s2 == s3) add4(a.Kss, ix(m3, m2), gauge_ss(Vt, ld4(a.Xll, ix(m4, m1))), 0.5);
+  }
+  add4(a.Jls, ix(m1, m2), gauge_cls(V, ld4(a.Csl, ix(m3, m4)), ld4(a.Cls, ix(m4, m3))), 1.0);
+  if (img)
+    add4(a.Jls, ix(m4, m3), gauge_cls(Vt, ld4(a.Csl, ix(m2, m1)), ld4(a.Cls, ix(m1, m2))), 1.0);
+  if (a.exchange) {
+    add4(a.Kls, ix(m1, m3), gauge_xls(V, ld4(a.Xsl, ix(m2, m4))), 1.0);
+    if (img) add4(a.Kls, ix(m4, m2), gauge_xls(Vt, ld4(a.Xsl, ix(m3, m1))), 1.0);
+  }
+}
+
+// bra component pairs per unit of work of the gauge kernel (its
+// accumulator holds 7 x 36 blocks of each)
+__host__ __device__ constexpr int gauge_abch(int lm) { return lm <= 2 ? 9 : 4; }
+
 // One thread per (quartet {P, Q}, unit); units = ket component pairs (c, d)
-// x slices of gaunt_abch(LM) bra component pairs, split over nsplit threads.
-template <int LM>
+// x slices of bra component pairs, split over nsplit threads.  GAUNT: one
+// operator, 1 / r12.  GAUGE: seven -- 1 / r12 and d_i d_i' r12 for the six
+// pairs i <= i' -- each a pass over the primitive pairs (the r12 passes on
+// the auxiliary functions of r12_aux, the Hermite index shifted by
+// e_i + e_i').
+template <int LM, bool GAUGE>
 __global__ void __launch_bounds__(REL_THREADS)
     gaunt_kernel(const GauntLaunch a, int la, int lb, int lc, int ld, int nsplit, int nslice) {
   const int ib = blockIdx.x;
@@ -1366,16 +1547,17 @@ __global__ void __launch_bounds__(REL_THREADS)
   }
   if (!alive) return;
 
+  constexpr int NOP = GAUGE ? 7 : 1;
   constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
   constexpr int HB = nherm(2 * LM + 1);
-  constexpr int HL = nherm(4 * LM + 2);
+  constexpr int HL = nherm(4 * LM + 2 + (GAUGE ? 2 : 0));
   constexpr int FL = 2 * LM + 3;
-  constexpr int ABCH = gaunt_abch(LM);
+  constexpr int ABCH = GAUGE ? gauge_abch(LM) : gaunt_abch(LM);
   const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
   const int nab = na * nb, ncd = ncc * nd;
   const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
   const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
-  const int Lb = la + lb + 1, Lk = lc + ld + 1, L = Lb + Lk;
+  const int Lb = la + lb + 1, Lk = lc + ld + 1;
   // which placements some surviving quartet needs
   const bool needB[2] = {(alive & 3u) != 0, (alive & 12u) != 0};
   const bool needK[2] = {(alive & 5u) != 0, (alive & 10u) != 0};
@@ -1383,8 +1565,8 @@ __global__ void __launch_bounds__(REL_THREADS)
   double Ea[3][E1], Ec[3][E1];
   double G[6][HB];  // [pk * 3 + l]
   double Rv[HL];
-  double F[4 * LM + 3];
-  double acc[ABCH * 36];
+  double F[4 * LM + 5];
+  double acc[ABCH * NOP * 36];
   double fa[3][3][FL], fc[3][3][FL];
   int nfa[3][3], nfc[3][3];
 
@@ -1397,83 +1579,95 @@ __global__ void __launch_bounds__(REL_THREADS)
     const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
     const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
 #pragma unroll 1
-    for (int k = 0; k < (ab1 - ab0) * 36; k++) acc[k] = 0.0;
+    for (int k = 0; k < (ab1 - ab0) * NOP * 36; k++) acc[k] = 0.0;
 #pragma unroll 1
-    for (int ip = 0; ip < P.npp; ip++) {
-      const PrimPairDev& A = a.pp[P.pp_off + ip];
-      double ea, eb;
-      pair_exps(SA, SB, a.prim, A, ea, eb);
+    for (int op = 0; op < NOP; op++) {
+      int oi = -1, oj = -1;
+      if (op > 0) op_pair(op - 1, oi, oj);
+      const int sx = (oi == 0) + (oj == 0), sy = (oi == 1) + (oj == 1), sz = (oi == 2) + (oj == 2);
+      const int L = Lb + Lk + (op > 0 ? 2 : 0);
 #pragma unroll 1
-      for (int x = 0; x < 3; x++)
-        hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
-#pragma unroll 1
-      for (int k = 0; k < 6; k++)
-#pragma unroll 1
-        for (int h = 0; h < nherm(Lb); h++) G[k][h] = 0.0;
-#pragma unroll 1
-      for (int iq = 0; iq < Q.npp; iq++) {
-        const PrimPairDev& Bq = a.pp[Q.pp_off + iq];
-        double ec, ed;
-        pair_exps(SC, SD, a.prim, Bq, ec, ed);
+      for (int ip = 0; ip < P.npp; ip++) {
+        const PrimPairDev& A = a.pp[P.pp_off + ip];
+        double ea, eb;
+        pair_exps(SA, SB, a.prim, A, ea, eb);
 #pragma unroll 1
         for (int x = 0; x < 3; x++)
-          hermite_E_rt<double, LM + 1>(lc + 1, ld + 1, Bq.o2p, Bq.PA[x], Bq.PB[x], Ec[x]);
-        const double X = A.P[0] - Bq.P[0], Y = A.P[1] - Bq.P[1], Z = A.P[2] - Bq.P[2];
-        const double pq = A.p + Bq.p, alpha = A.p * Bq.p / pq;
-        const double pref = PI52X2 / sqrt(pq) * A.Kp * Bq.Kp;
-        boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), F, a.boys);
-        hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
+          hermite_E_rt<double, LM + 1>(la + 1, lb + 1, A.o2p, A.PA[x], A.PB[x], Ea[x]);
 #pragma unroll 1
-        for (int x = 0; x < 3; x++)
+        for (int k = 0; k < 6; k++)
 #pragma unroll 1
-          for (int ty = 0; ty < 3; ty++) {
-            if (ty > 0 && !needK[ty - 1]) continue;
-            nfc[x][ty] = axis_factor<double>(Ec[x], ld + 1, lc + ld + 3, ci[x], di[x], ty,
-                                             2.0 * ec, 2.0 * ed, fc[x][ty]);
+          for (int h = 0; h < nherm(Lb); h++) G[k][h] = 0.0;
 #pragma unroll 1
-            for (int t = 1; t < nfc[x][ty]; t += 2) fc[x][ty][t] = -fc[x][ty][t];
+        for (int iq = 0; iq < Q.npp; iq++) {
+          const PrimPairDev& Bq = a.pp[Q.pp_off + iq];
+          double ec, ed;
+          pair_exps(SC, SD, a.prim, Bq, ec, ed);
+#pragma unroll 1
+          for (int x = 0; x < 3; x++)
+            hermite_E_rt<double, LM + 1>(lc + 1, ld + 1, Bq.o2p, Bq.PA[x], Bq.PB[x], Ec[x]);
+          const double X = A.P[0] - Bq.P[0], Y = A.P[1] - Bq.P[1], Z = A.P[2] - Bq.P[2];
+          const double pq = A.p + Bq.p, alpha = A.p * Bq.p / pq;
+          double pref = PI52X2 / sqrt(pq) * A.Kp * Bq.Kp;
+          const double Targ = alpha * (X * X + Y * Y + Z * Z);
+          boys_rt<double>(L, Targ, F, a.boys);
+          if (op > 0) {
+            r12_aux(L, Targ, F);
+            pref /= 2.0 * alpha;
           }
+          hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
 #pragma unroll 1
-        for (int pk = 0; pk < 2; pk++) {
-          if (!needK[pk]) continue;
+          for (int x = 0; x < 3; x++)
 #pragma unroll 1
-          for (int l = 0; l < 3; l++) {
-            const int tx = (l == 0) ? 1 + pk : 0, ty = (l == 1) ? 1 + pk : 0,
-                      tz = (l == 2) ? 1 + pk : 0;
-            ket_add<double>(G[pk * 3 + l], pref, fc[0][tx], nfc[0][tx], fc[1][ty], nfc[1][ty],
-                            fc[2][tz], nfc[2][tz], Lb, Rv);
+            for (int ty = 0; ty < 3; ty++) {
+              if (ty > 0 && !needK[ty - 1]) continue;
+              nfc[x][ty] = axis_factor<double>(Ec[x], ld + 1, lc + ld + 3, ci[x], di[x], ty,
+                                               2.0 * ec, 2.0 * ed, fc[x][ty]);
+#pragma unroll 1
+              for (int t = 1; t < nfc[x][ty]; t += 2) fc[x][ty][t] = -fc[x][ty][t];
+            }
+#pragma unroll 1
+          for (int pk = 0; pk < 2; pk++) {
+            if (!needK[pk]) continue;
+#pragma unroll 1
+            for (int l = 0; l < 3; l++) {
+              const int tx = (l == 0) ? 1 + pk : 0, ty = (l == 1) ? 1 + pk : 0,
+                        tz = (l == 2) ? 1 + pk : 0;
+              ket_add<double>(G[pk * 3 + l], pref, fc[0][tx], nfc[0][tx], fc[1][ty],
+                              nfc[1][ty], fc[2][tz], nfc[2][tz], Lb, Rv, sx, sy, sz);
+            }
           }
         }
-      }
 #pragma unroll 1
-      for (int ab = ab0; ab < ab1; ab++) {
-        const int ai = ab / nb, bi = ab % nb;
-        const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
-        const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+        for (int ab = ab0; ab < ab1; ab++) {
+          const int ai = ab / nb, bi = ab % nb;
+          const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+          const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
 #pragma unroll 1
-        for (int x = 0; x < 3; x++)
+          for (int x = 0; x < 3; x++)
 #pragma unroll 1
-          for (int ty = 0; ty < 3; ty++) {
-            if (ty > 0 && !needB[ty - 1]) continue;
-            nfa[x][ty] = axis_factor<double>(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty,
-                                             2.0 * ea, 2.0 * eb, fa[x][ty]);
-          }
-        double* m = acc + (ab - ab0) * 36;
+            for (int ty = 0; ty < 3; ty++) {
+              if (ty > 0 && !needB[ty - 1]) continue;
+              nfa[x][ty] = axis_factor<double>(Ea[x], lb + 1, la + lb + 3, ax[x], bx[x], ty,
+                                               2.0 * ea, 2.0 * eb, fa[x][ty]);
+            }
+          double* m = acc + ((ab - ab0) * NOP + op) * 36;
 #pragma unroll 1
-        for (int pb = 0; pb < 2; pb++) {
-          if (!needB[pb]) continue;
+          for (int pb = 0; pb < 2; pb++) {
+            if (!needB[pb]) continue;
 #pragma unroll 1
-          for (int j = 0; j < 3; j++) {
-            const int tx = (j == 0) ? 1 + pb : 0, ty = (j == 1) ? 1 + pb : 0,
-                      tz = (j == 2) ? 1 + pb : 0;
+            for (int j = 0; j < 3; j++) {
+              const int tx = (j == 0) ? 1 + pb : 0, ty = (j == 1) ? 1 + pb : 0,
+                        tz = (j == 2) ? 1 + pb : 0;
 #pragma unroll 1
-            for (int pk = 0; pk < 2; pk++) {
-              if (!(alive & (1u << (2 * pb + pk)))) continue;
+              for (int pk = 0; pk < 2; pk++) {
+                if (!(alive & (1u << (2 * pb + pk)))) continue;
 #pragma unroll 1
-              for (int l = 0; l < 3; l++)
-                m[((pb * 3 + j) * 2 + pk) * 3 + l] +=
-                    bra_dot<double>(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty], fa[2][tz],
-                                    nfa[2][tz], G[pk * 3 + l]);
+                for (int l = 0; l < 3; l++)
+                  m[((pb * 3 + j) * 2 + pk) * 3 + l] +=
+                      bra_dot<double>(fa[0][tx], nfa[0][tx], fa[1][ty], nfa[1][ty], fa[2][tz],
+                                      nfa[2][tz], G[pk * 3 + l]);
+              }
             }
           }
         }
@@ -1484,7 +1678,7 @@ __global__ void __launch_bounds__(REL_THREADS)
 #pragma unroll 1
     for (int ab = ab0; ab < ab1; ab++) {
       const int gA = P.cA + ab / nb, gB = P.cB + ab % nb;
-      const double* m = acc + (ab - ab0) * 36;
+      const double* m = acc + (ab - ab0) * NOP * 36;
 #pragma unroll 1
       for (int pb = 0; pb < 2; pb++)
 #pragma unroll 1
@@ -1495,36 +1689,65 @@ __global__ void __launch_bounds__(REL_THREADS)
           const int xdA = pb ? gB : gA, xoA = pb ? gA : gB;
           const int ydA = pk ? gD : gC, yoA = pk ? gC : gD;
           const bool xb = xd > yd || (xd == yd && xo >= yo);
-          double v[9];
+          // the reference's orientation: bra X (j on X) or Y (j on Y)
+          auto comp = [&](int o, int j, int l) -> double {
+            return xb ? m[o * 36 + ((pb * 3 + j) * 2 + pk) * 3 + l]
+                      : m[o * 36 + ((pb * 3 + l) * 2 + pk) * 3 + j];
+          };
+          if (!GAUGE) {
+            double v[9];
 #pragma unroll
-          for (int j = 0; j < 3; j++)
+            for (int j = 0; j < 3; j++)
 #pragma unroll
-            for (int l = 0; l < 3; l++) {
-              const double t = m[((pb * 3 + j) * 2 + pk) * 3 + l];
-              if (xb) v[3 * j + l] = t;
-              else v[3 * l + j] = t;
+              for (int l = 0; l < 3; l++) v[3 * j + l] = comp(0, j, l);
+            if (xb) gaunt_sites(a, v, xo, xd, yd, yo, xoA, xdA, ydA, yoA);
+            else gaunt_sites(a, v, yo, yd, xd, xo, yoA, ydA, xdA, xoA);
+          } else {
+            GVd V, Vt;
+#pragma unroll 1
+            for (int k = 0; k < 6; k++) {
+              int i, ip;
+              op_pair(k, i, ip);
+#pragma unroll 1
+              for (int j = 0; j < 3; j++)
+#pragma unroll 1
+                for (int l = 0; l < 3; l++) {
+                  double v = comp(1 + k, j, l), vt = comp(1 + k, l, j);
+                  if (i == ip) {
+                    v -= comp(0, j, l);
+                    vt -= comp(0, l, j);
+                  }
+                  V.v[i][ip][j][l] = V.v[ip][i][j][l] = v;
+                  Vt.v[i][ip][j][l] = Vt.v[ip][i][j][l] = vt;
+                }
             }
-          if (xb) gaunt_sites(a, v, xo, xd, yd, yo, xoA, xdA, ydA, yoA);
-          else gaunt_sites(a, v, yo, yd, xd, xo, yoA, ydA, xdA, xoA);
+            if (xb) gauge_sites(a, V, Vt, xo, xd, yd, yo, xoA, xdA, ydA, yoA);
+            else gauge_sites(a, V, Vt, yo, yd, xd, xo, yoA, ydA, xdA, xoA);
+          }
         }
     }
   }
 }
 
+template <bool GAUGE>
 void launch_gaunt(const GauntLaunch& a, int la, int lb, int lc, int ld, cudaStream_t st) {
   if (a.nBra == 0 || a.nKet == 0) return;
   const int tiles = (a.nKet + REL_THREADS - 1) / REL_THREADS;
   const int lm = std::max(std::max(la, lb), std::max(lc, ld));
-  const int nab = ncart(la) * ncart(lb), abch = gaunt_abch(std::max(lm, 1));
+  const int nab = ncart(la) * ncart(lb);
+  const int abch = GAUGE ? gauge_abch(std::max(lm, 1)) : gaunt_abch(std::max(lm, 1));
   const int nslice = (nab + abch - 1) / abch;
   const long long quartets = (long long)a.nBra * a.nKet;
   const int units = ncart(lc) * ncart(ld) * nslice;
   int nsplit = (int)std::min<long long>(units, std::max<long long>(1, (1 << 18) / quartets));
   nsplit = std::max(1, std::min(nsplit, 65535 / tiles));
   dim3 grid(a.nBra, tiles * nsplit);
-  if (lm <= 1) gaunt_kernel<1><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
-  else if (lm == 2) gaunt_kernel<2><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
-  else gaunt_kernel<3><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+  if (lm <= 1)
+    gaunt_kernel<1, GAUGE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+  else if (lm == 2)
+    gaunt_kernel<2, GAUGE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
+  else
+    gaunt_kernel<3, GAUGE><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit, nslice);
 }
 
 // ------------------------------------------------------------ 4C Schwarz
@@ -1534,15 +1757,17 @@ void launch_gaunt(const GauntLaunch& a, int la, int lb, int lc, int ld, cudaStre
 // component) is one unit of work for a group of threads, one Cartesian ket
 // column per thread (rel_schwarz_kernel).
 
-// Cartesian column out[(a*nb + b) * stride] += (d ab | d cd) of the ket
-// component pair (c, d) with derivative directions dir[0..3] (-1: none),
-// summed over the bra primitive pairs ip = ip0, ip0 + ipStep, ... (shared
-// memory, added atomically: several threads may share a column).
+// Cartesian column out[(a*nb + b) * stride] += w (d ab | K | d cd) of the
+// ket component pair (c, d) with derivative directions dir[0..3] (-1:
+// none), summed over the bra primitive pairs ip = ip0, ip0 + ipStep, ...
+// (shared memory, added atomically: several threads may share a column).
+// K = 1 / r12, or d_opi d_opj r12 when opi >= 0.
 template <int LM>
 __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const int* dir,
                              const PairDev& P, const PairDev& Q, const PrimPairDev* pp,
                              const ShellDev* shells, const double* prim, const double* boys,
-                             double* out, int stride, int ip0, int ipStep) {
+                             double* out, int stride, int ip0, int ipStep, int opi = -1,
+                             int opj = -1, double w = 1.0) {
   constexpr int E1 = (LM + 2) * (LM + 2) * (2 * LM + 3);
   constexpr int HB = nherm(2 * LM + 2);
   constexpr int HL = nherm(4 * LM + 4);
@@ -1551,7 +1776,8 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
   const int rb = (dir[0] >= 0 || dir[1] >= 0) ? 1 : 0, rk = (dir[2] >= 0 || dir[3] >= 0) ? 1 : 0;
   const int Lb = la + lb + (dir[0] >= 0) + (dir[1] >= 0);
   const int Lk = lc + ld + (dir[2] >= 0) + (dir[3] >= 0);
-  const int L = Lb + Lk;
+  const int sh[3] = {(opi == 0) + (opj == 0), (opi == 1) + (opj == 1), (opi == 2) + (opj == 2)};
+  const int L = Lb + Lk + (opi >= 0 ? 2 : 0);
   const ShellDev SA = shells[P.shA], SB = shells[P.shB], SC = shells[Q.shA], SD = shells[Q.shB];
   const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
   const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
@@ -1572,8 +1798,13 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
         hermite_E_rt<double, LM + 1>(lc + rk, ld + rk, B.o2p, B.PA[x], B.PB[x], Ec[x]);
       const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
       const double pq = A.p + B.p, alpha = A.p * B.p / pq;
-      const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
-      boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), F, boys);
+      double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+      const double Targ = alpha * (X * X + Y * Y + Z * Z);
+      boys_rt<double>(L, Targ, F, boys);
+      if (opi >= 0) {
+        r12_aux(L, Targ, F);
+        pref /= 2.0 * alpha;
+      }
       hermite_R_rt<double>(L, alpha, X, Y, Z, F, Rv);
       for (int x = 0; x < 3; x++) {
         const int ty = (dir[2] == x) | ((dir[3] == x) << 1);
@@ -1581,7 +1812,7 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
                             2.0 * ed, f[x]);
         for (int t = 1; t < nf[x]; t += 2) f[x][t] = -f[x][t];
       }
-      ket_add(G, pref, f[0], nf[0], f[1], nf[1], f[2], nf[2], Lb, Rv);
+      ket_add(G, pref, f[0], nf[0], f[1], nf[1], f[2], nf[2], Lb, Rv, sh[0], sh[1], sh[2]);
     }
     for (int ai = 0; ai < na; ai++)
       for (int bi = 0; bi < nb; bi++) {
@@ -1593,7 +1824,7 @@ __device__ void deriv_column(int la, int lb, int lc, int ld, int c, int d, const
                               2.0 * eb, g[x]);
         }
         atomicAdd(out + (ai * nb + bi) * stride,
-                  bra_dot(g[0], ng[0], g[1], ng[1], g[2], ng[2], G));
+                  w * bra_dot(g[0], ng[0], g[1], ng[1], g[2], ng[2], G));
       }
   }
 }
@@ -1630,27 +1861,31 @@ constexpr int SCH_THREADS = 128;
 // One (pair, component) per group of gsize threads, SCH_THREADS / gsize
 // groups per block, units enumerated pair-major over the components of a
 // pair: the plain (ab|ab) block (when lowLL), the 81 blocks
-// (dA_i dB_j ab | dA_k dB_l ab) (nSS = 81) and the 18 Gaunt blocks
-// (dA_i b | dA_k b), (a dB_i | a dB_k) (nG = 18).  A group builds the
+// (dA_i dB_j ab | dA_k dB_l ab) (nSS = 81), the 18 Gaunt blocks
+// (dA_i b | dA_k b), (a dB_i | a dB_k) (nG = 18) and the 108 gauge blocks
+// (dA_j b | -r_i r_i' / r^3 | dA_l b) and the same on B (nB = 108; i <= i',
+// the kernel -delta_ii' / r12 + d_i d_i' r12).  A group builds the
 // Cartesian block in shared memory -- thread g0 takes ket column g0 % cpow
 // (cpow: the column count rounded up to a power of two) and every
 // (gsize / cpow)-th bra primitive pair from g0 / cpow -- transforms it to
 // the spherical basis index by index, and folds its largest |element| into
-// the pair's maximum (mx[4 pair + 0..3]: plain, SS, Gaunt on A, Gaunt on B)
-// with an atomic max on the bit pattern (non-negative doubles order as
-// integers).
+// the pair's maximum (mx[6 pair + 0..5]: plain, SS, Gaunt on A, Gaunt on B,
+// gauge on A, gauge on B) with an atomic max on the bit pattern
+// (non-negative doubles order as integers).
+constexpr int SCH_SLOTS = 6;
 template <int LM>
 __global__ void __launch_bounds__(SCH_THREADS)
     rel_schwarz_kernel(const PairDev* __restrict__ pairs, const PrimPairDev* __restrict__ pp,
                        const ShellDev* __restrict__ shells, const double* __restrict__ prim,
                        const double* __restrict__ boys, const double* __restrict__ sph,
                        const int* __restrict__ sphOff, int beg, int npair, int la, int lb,
-                       int lowLL, int nSS, int nG, int gsize, int cpow, unsigned long long* mx) {
+                       int lowLL, int nSS, int nG, int nB, int gsize, int cpow,
+                       unsigned long long* mx) {
   extern __shared__ double sm[];
   const int na = ncart(la), nb = ncart(lb);
   const int n4 = na * nb * na * nb;
   const int groups = SCH_THREADS / gsize;
-  const int ncomp = lowLL + nSS + nG;
+  const int ncomp = lowLL + nSS + nG + nB;
   const int g = threadIdx.x / gsize, g0 = threadIdx.x % gsize;
   const long long unit = (long long)blockIdx.x * groups + g;
   const bool live = unit < (long long)npair * ncomp;
@@ -1659,8 +1894,15 @@ __global__ void __launch_bounds__(SCH_THREADS)
   const PairDev P = pairs[beg + ip];
   const ShellDev SA = shells[P.shA], SB = shells[P.shB];
   int dir[4] = {-1, -1, -1, -1};
-  int slot = 0;
-  if (comp >= lowLL + nSS) {  // Gaunt: one derivative in each pair
+  int slot = 0, opi = -1, opj = -1;
+  if (comp >= lowLL + nSS + nG) {  // gauge: one derivative in each pair
+    const int gc = comp - lowLL - nSS - nG;
+    const int side = gc / 54, r = gc % 54;
+    op_pair(r / 9, opi, opj);
+    dir[side] = (r % 9) / 3;
+    dir[2 + side] = r % 3;
+    slot = 4 + side;
+  } else if (comp >= lowLL + nSS) {  // Gaunt: one derivative in each pair
     const int gc = comp - lowLL - nSS;
     const int side = gc / 9;  // 0: on A, 1: on B
     dir[side] = (gc % 9) / 3;
@@ -1679,9 +1921,13 @@ __global__ void __launch_bounds__(SCH_THREADS)
   for (int e = g0; e < n4; e += gsize) cur[e] = 0.0;
   __syncthreads();
   const int col = g0 % cpow, slice = g0 / cpow, nslice = gsize / cpow;
-  if (live && col < na * nb)
+  if (live && col < na * nb) {
     deriv_column<LM>(la, lb, la, lb, col / nb, col % nb, dir, P, P, pp, shells, prim, boys,
-                     cur + col, na * nb, slice, nslice);
+                     cur + col, na * nb, slice, nslice, opi, opj);
+    if (opi >= 0 && opi == opj)  // the -delta_ii' / r12 part of the gauge kernel
+      deriv_column<LM>(la, lb, la, lb, col / nb, col % nb, dir, P, P, pp, shells, prim, boys,
+                       cur + col, na * nb, slice, nslice, -1, -1, -1.0);
+  }
   __syncthreads();
   int dims[4] = {na, nb, na, nb};
   const ShellDev* S4[4] = {&SA, &SB, &SA, &SB};
@@ -1700,22 +1946,28 @@ __global__ void __launch_bounds__(SCH_THREADS)
   const int tot = dims[0] * dims[1] * dims[2] * dims[3];
   for (int e = g0; e < tot; e += gsize) m = fmax(m, fabs(cur[e]));
   if (m > 0.0)
-    atomicMax(mx + 4 * (size_t)ip + slot, (unsigned long long)__double_as_longlong(m));
+    atomicMax(mx + SCH_SLOTS * (size_t)ip + slot, (unsigned long long)__double_as_longlong(m));
 }
 
 // Q^LL = sqrt(max), Q^SS = C2 sqrt(max) of each pair of a class into both
 // triangles of the nshell x nshell tables (direct4C_libcint.hpp:388-394,
 // :464-470); Q^G(d, o) = C1 sqrt(max) with the derivative on shell d
-// (SchwarzGaunt, :2910-2955, C1 = 1 / 2c), not symmetric.
+// (SchwarzGaunt, :2910-2955, C1 = 1 / 2c), not symmetric; the same for the
+// gauge kernel, Q^B(d, o) (SchwarzGauge, :3960-4005, which maxes over
+// libcint's 16 spin components of the operator where this maxes over its
+// 81 spatial components).
 __global__ void rel_schwarz_finish_kernel(const PairDev* __restrict__ pairs, int beg, int npair,
                                           const unsigned long long* __restrict__ mx,
-                                          int needLL, int needSS, int needG, int nshell,
-                                          double* qLL, double* qSS, double* qG) {
+                                          int needLL, int needSS, int needG, int needB,
+                                          int nshell, double* qLL, double* qSS, double* qG,
+                                          double* qB) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= npair) return;
   const PairDev P = pairs[beg + ip];
   const size_t e1 = P.s1 + (size_t)P.s2 * nshell, e2 = P.s2 + (size_t)P.s1 * nshell;
-  auto v = [&](int k) { return sqrt(__longlong_as_double((long long)mx[4 * ip + k])); };
+  auto v = [&](int k) {
+    return sqrt(__longlong_as_double((long long)mx[SCH_SLOTS * ip + k]));
+  };
   if (needLL) qLL[e1] = qLL[e2] = v(0);
   if (needSS) {
     const double C2 = 1.0 / (4.0 * SPEED_OF_LIGHT * SPEED_OF_LIGHT);
@@ -1726,28 +1978,34 @@ __global__ void rel_schwarz_finish_kernel(const PairDev* __restrict__ pairs, int
     qG[P.shA + (size_t)P.shB * nshell] = C1 * v(2);
     qG[P.shB + (size_t)P.shA * nshell] = C1 * v(3);
   }
+  if (needB) {
+    const double C1 = 1.0 / (2.0 * SPEED_OF_LIGHT);
+    qB[P.shA + (size_t)P.shB * nshell] = C1 * v(4);
+    qB[P.shB + (size_t)P.shA * nshell] = C1 * v(5);
+  }
 }
 
 cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, bool needG,
-                              cudaStream_t st) {
+                              bool needB, cudaStream_t st) {
   needLL = needLL && !B->rel_qLL;
   needSS = needSS && !B->rel_qSS;
   needG = needG && !B->rel_qG;
-  if (!needLL && !needSS && !needG) return CQF_OK;
+  needB = needB && !B->rel_qB;
+  if (!needLL && !needSS && !needG && !needB) return CQF_OK;
   const size_t ns2 = (size_t)B->nshell * B->nshell;
   // basis-owned, stream-ordered on the basis' stream (freed by free_basis)
-  for (double** q : {&B->d_qLL, &B->d_qSS, &B->d_qG})
+  for (double** q : {&B->d_qLL, &B->d_qSS, &B->d_qG, &B->d_qB})
     if (!*q) {
       CQF_RCUDA(cudaMallocAsync(q, ns2 * sizeof(double), B->stream));
       CQF_RCUDA(cudaMemsetAsync(*q, 0, ns2 * sizeof(double), B->stream));
     }
   CQF_RCUDA(cudaStreamSynchronize(B->stream));
   unsigned long long* mx = nullptr;
-  const size_t mxn = 4 * (size_t)std::max(1, B->npair);
+  const size_t mxn = SCH_SLOTS * (size_t)std::max(1, B->npair);
   CQF_RCUDA(cudaMallocAsync(&mx, mxn * sizeof(unsigned long long), st));
   CQF_RCUDA(cudaMemsetAsync(mx, 0, mxn * sizeof(unsigned long long), st));
-  const int nSS = needSS ? 81 : 0, nG = needG ? 18 : 0;
-  const int ncomp = (needLL ? 1 : 0) + nSS + nG;
+  const int nSS = needSS ? 81 : 0, nG = needG ? 18 : 0, nB = needB ? 108 : 0;
+  const int ncomp = (needLL ? 1 : 0) + nSS + nG + nB;
   for (int c = 0; c < NCLS; c++) {
     if (B->cls_cnt[c] <= 0) continue;
     int la, lb;
@@ -1763,7 +2021,7 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, bool needG
     const size_t smem = (size_t)groups * 2 * n4 * sizeof(double);
     const long long units = (long long)B->cls_cnt[c] * ncomp;
     const unsigned nblk = (unsigned)((units + groups - 1) / groups);
-    unsigned long long* mxc = mx + 4 * (size_t)B->cls_beg[c];
+    unsigned long long* mxc = mx + SCH_SLOTS * (size_t)B->cls_beg[c];
     const int lm = std::max(la, 1);
 #define CQF_SCH(LMV)                                                                          \
   if (lm == LMV) {                                                                            \
@@ -1771,15 +2029,15 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, bool needG
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));  \
     rel_schwarz_kernel<LMV><<<nblk, SCH_THREADS, smem, st>>>(                                 \
         B->d_pairs, B->d_pp, B->d_shells, B->d_prim, B->d_boys64, B->d_sph, B->d_sphOff,      \
-        B->cls_beg[c], B->cls_cnt[c], la, lb, needLL ? 1 : 0, nSS, nG, gsize, cpow, mxc);     \
+        B->cls_beg[c], B->cls_cnt[c], la, lb, needLL ? 1 : 0, nSS, nG, nB, gsize, cpow, mxc); \
   }
     CQF_SCH(1)
     CQF_SCH(2)
     CQF_SCH(3)
 #undef CQF_SCH
     rel_schwarz_finish_kernel<<<(B->cls_cnt[c] + 127) / 128, 128, 0, st>>>(
-        B->d_pairs, B->cls_beg[c], B->cls_cnt[c], mxc, needLL, needSS, needG, B->nshell,
-        B->d_qLL, B->d_qSS, B->d_qG);
+        B->d_pairs, B->cls_beg[c], B->cls_cnt[c], mxc, needLL, needSS, needG, needB,
+        B->nshell, B->d_qLL, B->d_qSS, B->d_qG, B->d_qB);
     CQF_RCUDA(cudaGetLastError());
   }
   cudaFreeAsync(mx, st);
@@ -1787,6 +2045,7 @@ cqf_status ensure_rel_schwarz(cqf_basis* B, bool needLL, bool needSS, bool needG
   B->rel_qLL = B->rel_qLL || needLL;
   B->rel_qSS = B->rel_qSS || needSS;
   B->rel_qG = B->rel_qG || needG;
+  B->rel_qB = B->rel_qB || needB;
   return CQF_OK;
 }
 
@@ -1949,7 +2208,7 @@ std::vector<int> rel_outputs(int type, bool exch) {
 }
 
 cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int exch,
-                              const cqf_opts& opts, cudaStream_t st, double* ws,
+                              bool gauge, const cqf_opts& opts, cudaStream_t st, double* ws,
                               unsigned long long* cnt);
 
 cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int type,
@@ -1961,7 +2220,8 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
   for (int m : rel_outputs(type, exch))
     if (AX[m]) CQF_RCUDA(cudaMemsetAsync(AX[m], 0, 2 * NN * sizeof(double), st));
-  if (type == CQF_REL_GAUNT) return gaunt_contract_dev(B, X, AX, exch, opts, st, ws, cnt);
+  if (type == CQF_REL_GAUNT || type == CQF_REL_GAUGE)
+    return gaunt_contract_dev(B, X, AX, exch, type == CQF_REL_GAUGE, opts, st, ws, cnt);
 
   if (type == CQF_REL_BARE_COULOMB) {
     // (LL|LL): the 1C engine on J[Re X] and K[X] (the same quartets, screen
@@ -1998,7 +2258,7 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   }
 
   const bool llss = (type == CQF_REL_LLSS);
-  CQF_RTRY(ensure_rel_schwarz(B, llss, true, false, st));
+  CQF_RTRY(ensure_rel_schwarz(B, llss, true, false, false, st));
   // required entries
   std::vector<int> need = {CQF_CSSMS, CQF_CSSMX, CQF_CSSMY, CQF_CSSMZ};
   if (llss) need.push_back(CQF_CLLMS);
@@ -2111,14 +2371,14 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
 }
 
 
-// The GAUNT contraction on device pointers (X, AX: 29 entries).  Needs
-// X[CLSM*], X[CSLM*] and, with exchange, X[XLLM*], X[XSSM*], X[XSLM*];
-// writes AX[CLSM*] and, with exchange, AX[XLLM*], AX[XSSM*], AX[XLSM*].
-// The screening norms are the max over the 16 exchange densities the
-// reference uses (:2957-3020), of those given.  FP64 (opts.precision is
-// not applied to this term).
+// The GAUNT (or GAUGE) contraction on device pointers (X, AX: 29
+// entries).  Needs X[CLSM*], X[CSLM*] and, with exchange, X[XLLM*],
+// X[XSSM*], X[XSLM*]; writes AX[CLSM*] and, with exchange, AX[XLLM*],
+// AX[XSSM*], AX[XLSM*].  The screening norms are the max over the 16
+// exchange densities the reference uses (:2957-3020, :4060-4130), of those
+// given.  FP64 (opts.precision is not applied to these terms).
 cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int exch,
-                              const cqf_opts& opts, cudaStream_t st, double* ws,
+                              bool gauge, const cqf_opts& opts, cudaStream_t st, double* ws,
                               unsigned long long* cnt) {
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const size_t NN = (size_t)N * N, nc2 = (size_t)nc * nc, ns2 = (size_t)ns * ns;
@@ -2134,10 +2394,10 @@ cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* cons
     }
   }
   for (int m : need)
-    if (!X[m]) return fail(CQF_EINVAL, "missing X entry for the GAUNT contraction");
+    if (!X[m]) return fail(CQF_EINVAL, "missing X entry for the GAUNT / GAUGE contraction");
   for (int m : rel_outputs(CQF_REL_GAUNT, exch))
-    if (!AX[m]) return fail(CQF_EINVAL, "missing AX entry for the GAUNT contraction");
-  CQF_RTRY(ensure_rel_schwarz(B, false, false, true, st));
+    if (!AX[m]) return fail(CQF_EINVAL, "missing AX entry for the GAUNT / GAUGE contraction");
+  CQF_RTRY(ensure_rel_schwarz(B, false, false, !gauge, gauge, st));
 
   double* xc = ws;
   double* accb = ws + align32(20 * 2 * nc2);
@@ -2179,7 +2439,7 @@ cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* cons
   a.screen = opts.screen;
   a.thresh = B->thresh;
   a.norms = nrm;
-  a.qG = B->d_qG;
+  a.qG = gauge ? B->d_qB : B->d_qG;
   a.nShell = ns;
   a.ncart = nc;
   a.exchange = exch;
@@ -2206,7 +2466,8 @@ cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* cons
       a.ketBeg = B->cls_beg[ck];
       a.nKet = B->cls_cnt[ck];
       a.same = (cb == ck);
-      launch_gaunt(a, la, lb, lc, ld, st);
+      if (gauge) launch_gaunt<true>(a, la, lb, lc, ld, st);
+      else launch_gaunt<false>(a, la, lb, lc, ld, st);
     }
   CQF_RCUDA(cudaGetLastError());
   auto back = [&](const double* srcAcc, int mode, double* dst) {
@@ -2241,7 +2502,7 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
                                      int type, int compute_exchange, const cqf_opts* optsIn,
                                      cqf_stats* stats) {
   if (!B || !X || !AX) return fail(CQF_EINVAL, "cqf_rel_two_body_contract: null argument");
-  if (type < CQF_REL_BARE_COULOMB || type > CQF_REL_GAUNT)
+  if (type < CQF_REL_BARE_COULOMB || type > CQF_REL_GAUGE)
     return fail(CQF_EINVAL, "cqf_rel_two_body_contract: unknown contraction type");
   cqf_opts o;
   cqf_opts_default(&o);
@@ -2249,7 +2510,7 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* B, const void* const* X, void* c
   std::lock_guard<std::mutex> lk(B->mu);
   CQF_RCUDA(cudaSetDevice(B->device));
   cudaStream_t st = o.stream ? (cudaStream_t)o.stream : B->stream;
-  const int nmat = (type == CQF_REL_GAUNT) ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
+  const int nmat = (type >= CQF_REL_GAUNT) ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
   const std::vector<int> outs = rel_outputs(type, compute_exchange != 0);
   const size_t NN = (size_t)B->nbasis * B->nbasis;
   const size_t wsd = rel_ws_doubles(B);
@@ -2303,6 +2564,7 @@ void cqf_dc_opts_default(cqf_dc_opts* o) {
   o->libcint = 1;
   o->xHFX = 1.0;
   o->gaunt = 0;
+  o->gauge = 0;
 }
 
 cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
@@ -2355,7 +2617,7 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
   // (impl.hpp:3847-3857)
   auto B3 = [&](int k, int c) { return blk + (size_t)(k * 4 + c) * blkd; };
   const int ro[4] = {0, N, 0, N}, co[4] = {0, N, N, 0};
-  for (int k = 0; k < (dc.gaunt ? 4 : 3); k++)
+  for (int k = 0; k < (dc.gaunt || dc.gauge ? 4 : 3); k++)
     for (int c = 0; c < 4; c++)
       get_block_kernel<<<rgrid(NN, 256), 256, 0, st>>>(Dd[c], N, ro[k], co[k], B3(k, c));
   CQF_RCUDA(cudaMemsetAsync(twoeH, 0, 8 * bigd * sizeof(double), st));
@@ -2398,14 +2660,18 @@ cqf_status cqf_four_comp_gd(cqf_basis* B, const void* const* D, void* const* G,
     if (exch)
       for (int c = 0; c < 4; c++) add(Kk(c), N, N, AX[CQF_XSSMS + c], -C4);
   }
-  if (dc.gaunt) {  // impl.hpp:4235-4376 (C2, the Gauge term being absent)
-    CQF_RTRY(rel_contract_dev(B, X, AX, CQF_REL_GAUNT, exch, o, st, ws, cnt));
-    for (int c = 0; c < 4; c++) add(H(c), 0, N, AX[CQF_CLSMS + c], 2.0 * C2);
+  // Gaunt and Gauge (impl.hpp:4228-4540): with the gauge term both are
+  // weighted C2 / 2 (their sum is the Breit term)
+  const double C2b = dc.gauge ? 0.5 * C2 : C2;
+  for (int t : {(int)CQF_REL_GAUNT, (int)CQF_REL_GAUGE}) {
+    if (!(t == CQF_REL_GAUNT ? dc.gaunt : dc.gauge)) continue;
+    CQF_RTRY(rel_contract_dev(B, X, AX, t, exch, o, st, ws, cnt));
+    for (int c = 0; c < 4; c++) add(H(c), 0, N, AX[CQF_CLSMS + c], 2.0 * C2b);
     if (exch)
       for (int c = 0; c < 4; c++) {
-        add(Kk(c), 0, 0, AX[CQF_XLLMS + c], -C2);
-        add(Kk(c), N, N, AX[CQF_XSSMS + c], -C2);
-        add(Kk(c), 0, N, AX[CQF_XLSMS + c], -C2);
+        add(Kk(c), 0, 0, AX[CQF_XLLMS + c], -C2b);
+        add(Kk(c), N, N, AX[CQF_XSSMS + c], -C2b);
+        add(Kk(c), 0, N, AX[CQF_XLSMS + c], -C2b);
       }
   }
   for (int c = 0; c < 4; c++)

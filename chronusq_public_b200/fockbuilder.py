@@ -75,8 +75,9 @@ class FourCompFock:
     (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) on the GPU.
 
     Hamiltonian switches as the reference's HamiltonianOptions (BareCoulomb,
-    DiracCoulomb, DiracCoulombSSSS, Libcint, Gaunt; the Gauge term is not
-    built); the density is the four Pauli
+    DiracCoulomb, DiracCoulombSSSS, Libcint, Gaunt, Gauge; with Gauge the
+    Gaunt and gauge terms are weighted C^2 / 2, the Breit interaction); the
+    density is the four Pauli
     components (scalar, MX, MY, MZ) of the 2N x 2N complex 4C one-particle
     density (LL block first).  ``formGD`` returns the same four components of
     G = twoeH - xHFX K.
@@ -84,13 +85,14 @@ class FourCompFock:
 
     def __init__(self, tpi: DirectTPI, BareCoulomb: bool = True,
                  DiracCoulomb: bool = True, DiracCoulombSSSS: bool = True,
-                 Libcint: bool = True, Gaunt: bool = False):
+                 Libcint: bool = True, Gaunt: bool = False, Gauge: bool = False):
         self.tpi = tpi
         self.BareCoulomb = BareCoulomb
         self.DiracCoulomb = DiracCoulomb
         self.DiracCoulombSSSS = DiracCoulombSSSS
         self.Libcint = Libcint
         self.Gaunt = Gaunt
+        self.Gauge = Gauge
         self.last_stats = None
 
     def formGD(self, D: List, xHFX: float = 1.0, screen: bool = True,
@@ -132,6 +134,7 @@ class FourCompFock:
         dco.dirac_coulomb_ssss = int(self.DiracCoulombSSSS)
         dco.libcint = int(self.Libcint)
         dco.gaunt = int(self.Gaunt)
+        dco.gauge = int(self.Gauge)
         dco.xHFX = float(xHFX)
         opts = _cabi.CqfOpts()
         _cabi.lib().cqf_opts_default(C.byref(opts))

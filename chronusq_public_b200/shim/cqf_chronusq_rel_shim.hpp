@@ -6,12 +6,13 @@
 // twoBodyContract overload of the reference class
 // (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94), which
 // FourCompFock::formGDDirect calls on the concrete type for BARE_COULOMB,
-// LLSS, SSSS and GAUNT (include/fockbuilder/fourcompfock/impl.hpp:3923,
-// :4030, :4177, :4279): the 17 (X, AX) entries in DIRAC_PAULI_SPINOR_COMP
-// order (29 for GAUNT) go to cqf_rel_two_body_contract, which zeroes the AX
-// it writes like directScaffoldLibcint
-// (include/particleintegrals/contract/direct4C_libcint.hpp:313-314).  Other
-// contraction types (LLLL, GAUGE), the spin-free / spin-dependent variants,
+// LLSS, SSSS, GAUNT and GAUGE (include/fockbuilder/fourcompfock/impl.hpp:
+// 3923, :4030, :4177, :4279, :4441): the 17 (X, AX) entries in
+// DIRAC_PAULI_SPINOR_COMP order (29 for GAUNT and GAUGE) go to
+// cqf_rel_two_body_contract, which zeroes the AX it writes like
+// directScaffoldLibcint (include/particleintegrals/contract/
+// direct4C_libcint.hpp:313-314).  The other contraction type (LLLL), the
+// spin-free / spin-dependent variants,
 // approximations and MPI runs stay on the reference implementation.  A
 // nonzero cqf_status becomes CErr.  Compiles only inside the ChronusQ tree
 // (it includes ChronusQ headers).
@@ -53,7 +54,7 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
     const bool ours = MPISize(comm) == 1 && type4C == TYPE_4C::All &&
                       approx == APPROXIMATION_TYPE_4C::None &&
                       ((list.size() == 17 && (t == BARE_COULOMB || t == LLSS || t == SSSS)) ||
-                       (list.size() == 29 && t == GAUNT));
+                       (list.size() == 29 && (t == GAUNT || t == GAUGE)));
     if (!ours) {
       GTODirectRelERIContraction<MatsT, IntsT>::twoBodyContract(comm, screen, list, pert,
                                                                 computeExchange, type4C, approx);
@@ -73,7 +74,8 @@ class B200DirectRelERIContraction : public GTODirectRelERIContraction<MatsT, Int
     const int type = t == BARE_COULOMB ? CQF_REL_BARE_COULOMB
                      : t == LLSS       ? CQF_REL_LLSS
                      : t == SSSS       ? CQF_REL_SSSS
-                                       : CQF_REL_GAUNT;
+                     : t == GAUNT      ? CQF_REL_GAUNT
+                                       : CQF_REL_GAUGE;
     cqf_status st = cqf_rel_two_body_contract(b, X, AX, type, computeExchange ? 1 : 0, &o,
                                               nullptr);
     if (st != CQF_OK) CErr(std::string("cqf_rel_two_body_contract: ") + cqf_last_error());

@@ -200,8 +200,8 @@ cqf_status cqf_two_body_contract_noalloc(cqf_basis* basis, const cqf_contraction
  * DIRAC_PAULI_SPINOR_COMP (include/particleintegrals/contract/
  * direct4C_libcint.hpp:279-310): Coulomb LL (MS), exchange LL (MS, MX, MY,
  * MZ), Coulomb SS (4), exchange SS (4), exchange LS (4) -- 17 entries --
- * and, for GAUNT only, Coulomb LS (4), Coulomb SL (4), exchange SL (4) --
- * 29 entries.  Every X and AX is an N x N complex (interleaved re, im)
+ * and, for GAUNT and GAUGE only, Coulomb LS (4), Coulomb SL (4), exchange
+ * SL (4) -- 29 entries.  Every X and AX is an N x N complex (interleaved re, im)
  * column-major matrix, N = nbasis.
  * --------------------------------------------------------------------- */
 typedef enum {
@@ -218,7 +218,8 @@ typedef enum {
 
 /* TYPE of the 4C contraction (entry 0's contType in the reference). */
 typedef enum {
-  CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2, CQF_REL_GAUNT = 3
+  CQF_REL_BARE_COULOMB = 0, CQF_REL_LLSS = 1, CQF_REL_SSSS = 2, CQF_REL_GAUNT = 3,
+  CQF_REL_GAUGE = 4
 } cqf_rel_type;
 
 /* GTODirectRelERIContraction::twoBodyContract (include/particleintegrals/
@@ -236,6 +237,9 @@ typedef enum {
  *         SL density X[XSLM*]); always FP64.  AX[CSLM*] and AX[XSLM*] are
  *         neither read nor written (the reference's list points them at the
  *         CLSM* / XLSM* outputs; such aliasing is allowed).
+ *   GAUGE (29 entries, :3908-5160): the same entries and sites with the
+ *         gauge kernel -(alpha_1 . r12)(alpha_2 . r12) / r12^3 of the Breit
+ *         interaction in place of Gaunt's -alpha_1 . alpha_2 / r12.
  * Entries a type does not read or write may be NULL; only the entries a
  * type writes are zeroed.  The densities must be
  * Hermitian, as the reference requires (:144-145).  opts->is_complex is
@@ -249,25 +253,26 @@ cqf_status cqf_rel_two_body_contract(cqf_basis* basis, const void* const* X, voi
 
 /* Hamiltonian switches of the 4C two-electron build (the reference's
  * HamiltonianOptions: BareCoulomb, DiracCoulomb, DiracCoulombSSSS, Libcint,
- * Gaunt) and the exchange scaling xHFX.  The Gauge term is not built. */
+ * Gaunt, Gauge) and the exchange scaling xHFX. */
 typedef struct {
   int bare_coulomb, dirac_coulomb, dirac_coulomb_ssss, libcint;
   double xHFX;
-  int gaunt;
+  int gaunt, gauge;
 } cqf_dc_opts;
 /* Defaults of the reference: bare Coulomb, Dirac-Coulomb and SSSS on,
- * libcint on, Gaunt off, xHFX = 1. */
+ * libcint on, Gaunt and Gauge off, xHFX = 1. */
 void cqf_dc_opts_default(cqf_dc_opts* o);
 
 /* FourCompFock::formGDDirect (include/fockbuilder/fourcompfock/impl.hpp:
  * 3752-4636): D[4] = Pauli components (scalar, MX, MY, MZ) of the
  * 2N x 2N complex 4C density (column-major, LL block first); G[4] receives
  * twoeH - xHFX K with the 2C^2 / -C^2 / 2C^4 / -C^4 weights of the LLSS and
- * SSSS terms, the Gaunt term's 2C^2 (LS Coulomb) and -C^2 (LL, SS, LS
- * exchange) (impl.hpp:4235-4376), twoeH_LL = 2 J (libcint) or J, and the SL
- * blocks set to the conjugate transpose of the LS blocks.  opts as for
+ * SSSS terms, the Gaunt and Gauge terms' 2C'^2 (LS Coulomb) and -C'^2 (LL,
+ * SS, LS exchange), C'^2 = C^2, or C^2 / 2 with the gauge term on (the
+ * Breit interaction; impl.hpp:4228-4540), twoeH_LL = 2 J (libcint) or J,
+ * and the SL blocks set to the conjugate transpose of the LS blocks.  opts as for
  * cqf_rel_two_body_contract (CQF_MIXED applies to every contraction type of
- * the build but the Gaunt one, the bare-Coulomb one included). */
+ * the build but Gaunt and Gauge, the bare-Coulomb one included). */
 cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const* G,
                             const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 

@@ -136,9 +136,9 @@ class GTODirectTPIContraction {
 
 // GTODirectRelERIContraction<dcomplex,double>::twoBodyContract
 // (include/particleintegrals/twopints/gtodirectreleri.hpp:75-94): 17 entries
-// in DIRAC_PAULI_SPINOR_COMP order (29 for GAUNT), contType of entry 0 =
-// BARE_COULOMB, LLSS, SSSS or GAUNT; the AX the type writes are overwritten
-// (zeroed, then the contraction).
+// in DIRAC_PAULI_SPINOR_COMP order (29 for GAUNT and GAUGE), contType of
+// entry 0 = BARE_COULOMB, LLSS, SSSS, GAUNT or GAUGE; the AX the type writes
+// are overwritten (zeroed, then the contraction).
 class GTODirectRelERIContraction {
  public:
   explicit GTODirectRelERIContraction(std::shared_ptr<DirectTPI> tpi) : tpi_(std::move(tpi)) {}
@@ -153,12 +153,13 @@ class GTODirectRelERIContraction {
       case LLSS: type = CQF_REL_LLSS; break;
       case SSSS: type = CQF_REL_SSSS; break;
       case GAUNT: type = CQF_REL_GAUNT; break;
+      case GAUGE: type = CQF_REL_GAUGE; break;
       default: throw std::runtime_error("GTODirectRelERIContraction: unsupported contraction type");
     }
-    const int n = type == CQF_REL_GAUNT ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
+    const int n = type >= CQF_REL_GAUNT ? CQF_REL_NMAT_GAUNT : CQF_REL_NMAT;
     if ((int)list.size() != n)
       throw std::runtime_error("GTODirectRelERIContraction: the 4C list has 17 entries (29 for "
-                               "GAUNT)");
+                               "GAUNT and GAUGE)");
     const void* X[CQF_REL_NMAT_GAUNT] = {};
     void* AX[CQF_REL_NMAT_GAUNT] = {};
     for (int m = 0; m < n; m++) {
@@ -181,13 +182,13 @@ class GTODirectRelERIContraction {
 // FourCompFock<dcomplex,double>::formGDDirect
 // (include/fockbuilder/fourcompfock/impl.hpp:3752-4636) with the
 // HamiltonianOptions switches BareCoulomb, DiracCoulomb, DiracCoulombSSSS,
-// Libcint and Gaunt.  D and G: the four Pauli components (scalar, MX, MY,
+// Libcint, Gaunt and Gauge.  D and G: the four Pauli components (scalar, MX, MY,
 // MZ) of the 2N x 2N complex 4C matrices, column-major, LL block first.
 class FourCompFock {
  public:
   explicit FourCompFock(std::shared_ptr<DirectTPI> tpi, bool BareCoulomb = true,
                         bool DiracCoulomb = true, bool DiracCoulombSSSS = true,
-                        bool Libcint = true, bool Gaunt = false)
+                        bool Libcint = true, bool Gaunt = false, bool Gauge = false)
       : tpi_(std::move(tpi)) {
     cqf_dc_opts_default(&dc_);
     dc_.bare_coulomb = BareCoulomb;
@@ -195,6 +196,7 @@ class FourCompFock {
     dc_.dirac_coulomb_ssss = DiracCoulombSSSS;
     dc_.libcint = Libcint;
     dc_.gaunt = Gaunt;
+    dc_.gauge = Gauge;
   }
 
   void formGD(const std::complex<double>* const D[4], std::complex<double>* const G[4],

@@ -10,10 +10,10 @@
 //                          R0..R4.bin (N x N each: CLLMS, XLLMS, XLLMX, XLLMY,
 //                          XLLMZ) at the same three geometries -> REL0..2.bin
 //                          (the five outputs)
-//   shim_driver <dir> gaunt : GAUNT on the 4C density blocks G0..G15.bin (LL,
-//                          SS, LS, SL x scalar, MX, MY, MZ) at the geometry
-//                          of shells0.txt -> GAUNT.bin (XLLM*, XSSM*, XLSM*,
-//                          CLSM*)
+//   shim_driver <dir> gaunt|gauge : GAUNT / GAUGE on the 4C density blocks
+//                          G0..G15.bin (LL, SS, LS, SL x scalar, MX, MY, MZ)
+//                          at the geometry of shells0.txt -> gaunt.bin /
+//                          gauge.bin (XLLM*, XSSM*, XLSM*, CLSM*)
 // shells<k>.txt: nshell, then per shell "l pure nprim x y z" + alpha + coeff
 #include <complex>
 #include <fstream>
@@ -68,7 +68,7 @@ static void write_bin(const std::string& path, const std::vector<T>& v) {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::cerr << "usage: shim_driver <dir> 1c|4c|gaunt" << std::endl;
+    std::cerr << "usage: shim_driver <dir> 1c|4c|gaunt|gauge" << std::endl;
     return 2;
   }
   const std::string dir = argv[1], mode = argv[2];
@@ -109,7 +109,7 @@ int main(int argc, char** argv) {
         for (int k = 0; k < 5; k++) o.insert(o.end(), out[k].begin(), out[k].end());
         write_bin(dir + "/REL" + std::to_string(g) + ".bin", o);
       }
-    } else if (mode == "gaunt") {
+    } else if (mode == "gaunt" || mode == "gauge") {
       // the reference's GAUNT list (fourcompfock/impl.hpp:4237-4274): 29
       // entries, the CSLM* / XSLM* AX pointed at the CLSM* / XLSM* outputs
       using Z = std::complex<double>;
@@ -127,13 +127,13 @@ int main(int argc, char** argv) {
         list[21 + c] = {G[12 + c].data(), out[17 + c].data(), true, EXCHANGE};  // CSLM*
         list[25 + c] = {G[12 + c].data(), out[13 + c].data(), true, EXCHANGE};  // XSLM*
       }
-      list[0] = {G[0].data(), out[0].data(), true, GAUNT};
+      list[0] = {G[0].data(), out[0].data(), true, mode == "gaunt" ? GAUNT : GAUGE};
       EMPerturbation pert;
       con.twoBodyContract(MPI_COMM_WORLD, true, list, pert);
       std::vector<Z> o;
       for (int base : {1, 9, 13, 17})
         for (int c = 0; c < 4; c++) o.insert(o.end(), out[base + c].begin(), out[base + c].end());
-      write_bin(dir + "/GAUNT.bin", o);
+      write_bin(dir + "/" + mode + ".bin", o);
     } else {
       std::cerr << "unknown mode " << mode << std::endl;
       return 2;

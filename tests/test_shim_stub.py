@@ -104,10 +104,11 @@ def test_rel_shim_rebuilds_basis_after_geometry_step(tmp_path):
 
 
 @pytest.mark.gpu
-def test_rel_shim_gaunt_list_with_aliased_outputs(tmp_path):
-    """The reference's 29-entry GAUNT list through the shim, its CSLM* /
-    XSLM* AX pointing at the CLSM* / XLSM* outputs as in
-    fourcompfock/impl.hpp:4237-4274, against the oracle."""
+@pytest.mark.parametrize("mode", ["gaunt", "gauge"])
+def test_rel_shim_gaunt_list_with_aliased_outputs(tmp_path, mode):
+    """The reference's 29-entry GAUNT / GAUGE list through the shim, its
+    CSLM* / XSLM* AX pointing at the CLSM* / XLSM* outputs as in
+    fourcompfock/impl.hpp:4237-4274, :4399-4436, against the oracle."""
     import oracle as O
     exe = _build(str(tmp_path))
     b0, _ = _geometries()
@@ -126,10 +127,10 @@ def test_rel_shim_gaunt_list_with_aliased_outputs(tmp_path):
             G.append(np.asfortranarray(blocks[c][ro[k]:ro[k] + N, co[k]:co[k] + N]))
     for i, g in enumerate(G):
         g.T.tofile(str(tmp_path / ("G%d.bin" % i)))
-    subprocess.check_call([exe, str(tmp_path), "gaunt"])
+    subprocess.check_call([exe, str(tmp_path), mode])
     X = [G[0]] + G[0:4] + G[4:8] + G[4:8] + G[8:12] + G[8:12] + G[12:16] + G[12:16]
-    ref = O.OracleBasis(b0).rel_contract(X, 3, True)
-    out = np.fromfile(str(tmp_path / "GAUNT.bin"), dtype=np.complex128)
+    ref = O.OracleBasis(b0).rel_contract(X, 3 if mode == "gaunt" else 4, True)
+    out = np.fromfile(str(tmp_path / (mode + ".bin")), dtype=np.complex128)
     k = 0
     for base in (1, 9, 13, 17):
         for c in range(4):
