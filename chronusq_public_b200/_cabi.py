@@ -54,7 +54,8 @@ class CqfContraction(C.Structure):
 class CqfOpts(C.Structure):
     _fields_ = [("is_complex", C.c_int), ("screen", C.c_int),
                 ("device_pointers", C.c_int), ("precision", C.c_int),
-                ("fp32_cutoff", C.c_double), ("stream", C.c_void_p)]
+                ("fp32_cutoff", C.c_double), ("stream", C.c_void_p),
+                ("shard_index", C.c_int), ("shard_count", C.c_int)]
 
 
 class CqfStats(C.Structure):

@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import List, Optional
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -237,8 +237,12 @@ class GTODirectTPIContraction:
 
     def twoBodyContract(self, matList: List[TwoBodyContraction],
                         screen: bool = True, precision: str = "fp64",
-                        fp32_cutoff: float = 0.0, stream=None) -> None:
-        """AX += G[X] for every entry (directScaffoldNew semantics)."""
+                        fp32_cutoff: float = 0.0, stream=None,
+                        shard: Tuple[int, int] = (0, 1)) -> None:
+        """AX += G[X] for every entry (directScaffoldNew semantics).
+        ``shard = (index, count)``: only this process's share of the
+        shell-pair work (cqf_opts::shard_index / shard_count); the shares sum
+        to the whole contraction."""
         if not matList:
             return
         N = self.tpi.nbasis
@@ -285,6 +289,7 @@ class GTODirectTPIContraction:
         opts.precision = _cabi.CQF_MIXED if precision == "mixed" else _cabi.CQF_FP64
         opts.fp32_cutoff = float(fp32_cutoff)
         opts.stream = _stream_arg(stream)
+        opts.shard_index, opts.shard_count = int(shard[0]), int(shard[1])
         st = _cabi.CqfStats()
         _cabi.check(_cabi.lib().cqf_two_body_contract(
             self.tpi.handle, arr, n, C.byref(opts), C.byref(st)))
@@ -344,7 +349,8 @@ class GTODirectRelERIContraction:
     def twoBodyContract(self, matList: List[TwoBodyContraction],
                         contType: int, computeExchange: bool = True,
                         screen: bool = True, precision: str = "fp64",
-                        fp32_cutoff: float = 0.0, stream=None) -> None:
+                        fp32_cutoff: float = 0.0, stream=None,
+                        shard: Tuple[int, int] = (0, 1)) -> None:
         """17 entries in REL_COMPS order (29 in GAUNT_COMPS order for
         GAUNT and GAUGE; None for entries the type does not use).  The AX the
         type writes are overwritten (the reference zeroes AX on entry); X and
@@ -391,6 +397,7 @@ class GTODirectRelERIContraction:
         opts.fp32_cutoff = float(fp32_cutoff)
         opts.device_pointers = 1 if dev else 0
         opts.stream = _stream_arg(stream)
+        opts.shard_index, opts.shard_count = int(shard[0]), int(shard[1])
         st = _cabi.CqfStats()
         _cabi.check(_cabi.lib().cqf_rel_two_body_contract(
             self.tpi.handle, xs, axs, int(contType), 1 if computeExchange else 0,

@@ -1207,6 +1207,8 @@ void cqf_opts_default(cqf_opts* o) {
   o->precision = CQF_FP64;
   o->fp32_cutoff = 0.0;
   o->stream = nullptr;
+  o->shard_index = 0;
+  o->shard_count = 1;
 }
 
 const char* cqf_last_error(void) { return g_err.c_str(); }
@@ -1611,6 +1613,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
                          const cqf_opts& opts, cqf_stats* stats, double* ws, bool capture,
                          const int* d_flags_pre, const double* const* normSrc,
                          double* pinned) {
+  if (opts.shard_count < 1 || opts.shard_index < 0 || opts.shard_index >= opts.shard_count)
+    return fail(CQF_EINVAL, "shard_index must lie in [0, shard_count)");
   cudaStream_t st = opts.stream ? (cudaStream_t)opts.stream : B->stream;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
   const int cw = opts.is_complex ? 2 : 1;
@@ -1686,6 +1690,8 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
   CQF_CUDA(cudaGetLastError());
 
   JKLaunch a{};
+  a.shardIdx = opts.shard_index;
+  a.shardCnt = std::max(1, opts.shard_count);
   a.pairs = B->d_pairs;
   a.pp = B->d_pp;
   a.ppQ = B->d_ppQ;

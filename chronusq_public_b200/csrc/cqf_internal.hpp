@@ -66,8 +66,15 @@ struct JKLaunch {
   int braOff;               // position of the launch's first bra pair in its class (slabs)
   int precision;            // 0 FP64, 1 mixed
   double fp32_cut;          // mixed: bound < cut -> FP32 ERIs
+  int shardIdx, shardCnt;   // bra pairs p with p % shardCnt == shardIdx only
   unsigned long long* counters;  // [0] visited, [1] screened, [2] fp32, [3] fp64
 };
+
+// Whether bra pair p (position in the pair list) belongs to this call's
+// shard of the work (cqf_opts::shard_index / shard_count).
+__host__ __device__ inline bool in_shard(int p, int idx, int cnt) {
+  return cnt <= 1 || p % cnt == idx;
+}
 
 // Sets the thread's last-error text and returns s (cqf_api.cu).
 cqf_status fail(cqf_status s, const std::string& msg);

@@ -126,7 +126,8 @@ __global__ void __launch_bounds__(256)
       const int ib = word / nTiles, tile = word - ib * nTiles;
       unsigned b64 = 0u, b32 = 0u;
       const int ibc = ib + a.braOff;  // the bra's position in its class
-      if (!(a.same && tile * WTILE > ibc)) {  // else: no quartet in this word
+      // else: no quartet in this word (above the diagonal, or another shard's bra)
+      if (!(a.same && tile * WTILE > ibc) && in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) {
         const int jk = tile * WTILE + lane;
         const PairDev P = a.pairs[a.braBeg + ib];
         const bool visited = jk < a.nKet && !(a.same && jk > ibc);

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(JK_THREADS)
     jk_generic_kernel(const JKLaunch a, int la, int lb, int lc, int ld) {
   const int ib = blockIdx.x;
   const int jk = blockIdx.y * JK_THREADS + threadIdx.x;
+  if (!in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;  // another shard's bra
   const PairDev P = a.pairs[a.braBeg + ib];
   const int ns = a.nShell;
 

@@ -244,6 +244,7 @@ struct RelLaunch {
   double* Jll;           // real
   double* Jss[4];        // real
   double* K[4];          // complex
+  int shardIdx, shardCnt;  // bra pairs p with p % shardCnt == shardIdx only
   unsigned long long* counters;
 };
 
@@ -382,6 +383,7 @@ __global__ void __launch_bounds__(REL_THREADS)
     rel_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int nsplit) {
   constexpr bool IS32 = sizeof(T) == 4;
   const int ib = blockIdx.x;
+  if (!in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;  // another shard's bra
   const int split = blockIdx.y % nsplit;
   const int jk = (blockIdx.y / nsplit) * REL_THREADS + threadIdx.x;
   const int ns = a.nShell;
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(RB_THREADS)
     ib = (int)(q / a.nKet);
     jk = (int)(q % a.nKet);
   }
-  if (ib >= a.nBra) return;
+  if (ib >= a.nBra || !in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
@@ -944,7 +946,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   extern __shared__ double sm[];
   const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   const int ib = (int)(q / a.nKet), jk = (int)(q % a.nKet);
-  if (ib >= a.nBra) return;
+  if (ib >= a.nBra || !in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
@@ -1228,6 +1230,7 @@ struct GauntLaunch {
   double* Kss[4];
   double* Jls[4];
   double* Kls[4];
+  int shardIdx, shardCnt;  // bra pairs p with p % shardCnt == shardIdx only
   unsigned long long* counters;
 };
 
@@ -1513,6 +1516,7 @@ template <int LM, bool GAUGE>
 __global__ void __launch_bounds__(REL_THREADS)
     gaunt_kernel(const GauntLaunch a, int la, int lb, int lc, int ld, int nsplit, int nslice) {
   const int ib = blockIdx.x;
+  if (!in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;  // another shard's bra
   const int split = blockIdx.y % nsplit;
   const int jk = (blockIdx.y / nsplit) * REL_THREADS + threadIdx.x;
   const int ns = a.nShell;
@@ -2214,6 +2218,8 @@ cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* cons
 cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const* AX, int type,
                             int exch, const cqf_opts& opts, cudaStream_t st, double* ws,
                             unsigned long long* cnt) {
+  if (opts.shard_count < 1 || opts.shard_index < 0 || opts.shard_index >= opts.shard_count)
+    return fail(CQF_EINVAL, "shard_index must lie in [0, shard_count)");
   const int screen = opts.screen;
   const bool mixed = opts.precision == CQF_MIXED && opts.fp32_cutoff > 0.0;
   const int N = B->nbasis, nc = B->ncart, ns = B->nshell;
@@ -2246,6 +2252,8 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
     o.precision = opts.precision;
     o.fp32_cutoff = opts.fp32_cutoff;
     o.stream = st;
+    o.shard_index = opts.shard_index;
+    o.shard_count = opts.shard_count;
     CQF_RTRY(basis_workspace(B, ws_layout(B, (int)list.size(), o).total * sizeof(double)));
     cqf_stats s1{};
     CQF_RTRY(contract_core(B, list.data(), (int)list.size(), o, &s1,
@@ -2331,6 +2339,8 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
     a.K[c] = Kc[c];
   }
   a.Jll = Jll;
+  a.shardIdx = opts.shard_index;
+  a.shardCnt = std::max(1, opts.shard_count);
   a.counters = dcnt;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck < NCLS; ck++) {
@@ -2454,6 +2464,8 @@ cqf_status gaunt_contract_dev(cqf_basis* B, const double* const* X, double* cons
     a.Jls[c] = AC(8 + c);
     a.Kls[c] = AC(12 + c);
   }
+  a.shardIdx = opts.shard_index;
+  a.shardCnt = std::max(1, opts.shard_count);
   a.counters = dcnt;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck <= cb; ck++) {

@@ -4,6 +4,13 @@ Restates ``include/fockbuilder/impl.hpp``: ``formRawGDInBatches`` (:109-244)
 zeroes J/K, contracts {D, J, HER, COULOMB} and {D, K, HER, EXCHANGE} in one
 ``twoBodyContract`` call (:139-212) and assembles G = 2J - xHFX K (:223-237);
 ``formFock`` adds the core Hamiltonian (:280-319).  D is ``onePDM.S``.
+
+With a ``torch.distributed`` process group the builders split the work the
+way the reference splits its shell-pair loop over MPI ranks
+(direct.hpp:1600-1604; 4C direct4C_libcint.hpp:933-936): each rank computes
+its shard of the bra shell pairs and the shards are summed over the group
+(the reference's MPIReduce, direct.hpp:2085-2107), NCCL for device matrices
+and host matrices on an NCCL group, the group's own backend otherwise.
 """
 from __future__ import annotations
 
@@ -12,12 +19,55 @@ from typing import List, Optional
 import numpy as np
 
 from .contraction import (COULOMB, EXCHANGE, DirectTPI,
-                          GTODirectTPIContraction, TwoBodyContraction)
+                          GTODirectTPIContraction, TwoBodyContraction, _is_torch)
+
+
+def _shard_of(group):
+    if group is None:
+        return (0, 1)
+    import torch.distributed as dist
+    return (dist.get_rank(group), dist.get_world_size(group))
+
+
+def allreduce_sum(arrays, group, device: int = 0) -> None:
+    """Sums each array (numpy, or torch) over the process group, in place."""
+    if group is None:
+        return
+    import torch
+    import torch.distributed as dist
+    nccl = dist.get_backend(group) == "nccl"
+    for a in arrays:
+        if _is_torch(a):
+            if not a.is_contiguous() and a.T.is_contiguous():
+                a = a.T  # column-major matrices: the same storage
+            if a.is_complex():
+                a = torch.view_as_real(a)
+            if not a.is_contiguous():
+                raise ValueError("allreduce_sum: tensors must be contiguous")
+            dist.all_reduce(a, group=group)
+            continue
+        flat = np.ravel(a, order="K")
+        if not np.shares_memory(flat, a):
+            raise ValueError("allreduce_sum: arrays must be contiguous")
+        if np.iscomplexobj(flat):
+            flat = flat.view(np.float64)
+        t = torch.from_numpy(flat)
+        if nccl:
+            d = t.to("cuda:%d" % device)
+            dist.all_reduce(d, group=group)
+            t.copy_(d.cpu())
+        else:
+            dist.all_reduce(t, group=group)
 
 
 class FockBuilder:
-    def __init__(self, tpi: DirectTPI):
+    """``group``: a torch.distributed process group whose ranks share the
+    build (each its shard of the shell-pair work, then a sum); None: the
+    whole build on this process."""
+
+    def __init__(self, tpi: DirectTPI, group=None):
         self.tpi = tpi
+        self.group = group
         self.contraction = GTODirectTPIContraction(tpi)
 
     def formRawGD(self, D, xHFX: float = 1.0, precision: str = "fp64",
@@ -35,11 +85,22 @@ class FockBuilder:
             J = np.zeros((N, N), order="F")
         if K is None or not increment:
             K = np.zeros((N, N), order="F")
+        shard = _shard_of(self.group)
+        if increment and shard[1] > 1:
+            # the increments of every shard go into zeroed buffers; the sum
+            # is added once
+            J0, K0 = J, K
+            J, K = np.zeros((N, N), order="F"), np.zeros((N, N), order="F")
         cont = [TwoBodyContraction(D, J, True, COULOMB)]
         if xHFX != 0.0:
             cont.append(TwoBodyContraction(D, K, True, EXCHANGE))
         self.contraction.twoBodyContract(cont, precision=precision,
-                                         fp32_cutoff=fp32_cutoff)
+                                         fp32_cutoff=fp32_cutoff, shard=shard)
+        allreduce_sum([J, K], self.group, self.tpi.device)
+        if increment and shard[1] > 1:
+            J0 += J
+            K0 += K
+            J, K = J0, K0
         G = 2.0 * J - xHFX * K
         return G, J, K
 
@@ -56,7 +117,9 @@ class FockBuilder:
             if xHFX != 0.0:
                 cont.append(TwoBodyContraction(D, K, True, EXCHANGE))
         self.contraction.twoBodyContract(cont, precision=precision,
-                                         fp32_cutoff=fp32_cutoff)
+                                         fp32_cutoff=fp32_cutoff,
+                                         shard=_shard_of(self.group))
+        allreduce_sum(Js + Ks, self.group, self.tpi.device)
         return [2.0 * J - xHFX * K for J, K in zip(Js, Ks)]
 
     def formFock(self, H, D, **kw):
@@ -85,8 +148,10 @@ class FourCompFock:
 
     def __init__(self, tpi: DirectTPI, BareCoulomb: bool = True,
                  DiracCoulomb: bool = True, DiracCoulombSSSS: bool = True,
-                 Libcint: bool = True, Gaunt: bool = False, Gauge: bool = False):
+                 Libcint: bool = True, Gaunt: bool = False, Gauge: bool = False,
+                 group=None):
         self.tpi = tpi
+        self.group = group
         self.BareCoulomb = BareCoulomb
         self.DiracCoulomb = DiracCoulomb
         self.DiracCoulombSSSS = DiracCoulombSSSS
@@ -144,8 +209,13 @@ class FourCompFock:
         opts.fp32_cutoff = float(fp32_cutoff)
         opts.device_pointers = 1 if dev else 0
         opts.stream = _stream_arg(stream)
+        opts.shard_index, opts.shard_count = _shard_of(self.group)
         st = _cabi.CqfStats()
         _cabi.check(_cabi.lib().cqf_four_comp_gd(
             self.tpi.handle, dp, gp, C.byref(dco), C.byref(opts), C.byref(st)))
+        if dev and self.group is not None:
+            import torch
+            torch.cuda.synchronize(D[0].device)
+        allreduce_sum(G, self.group, self.tpi.device)
         self.last_stats = _stats(st)
         return G

@@ -77,6 +77,16 @@ typedef struct {
   int precision;        /* cqf_precision */
   double fp32_cutoff;   /* mixed: quartets with bound < cutoff run in FP32 */
   void* stream;         /* cudaStream_t to run on; NULL = the basis' stream */
+  /* Work split over processes (the reference's MPI split of the shell-pair
+   * loop, direct.hpp:1600-1604, 4C direct4C_libcint.hpp:933-936): with
+   * shard_count > 1 a call computes only the quartets whose bra shell pair
+   * (number p in the library's pair order) has p % shard_count ==
+   * shard_index; the shards' results sum to the whole contraction (or 4C
+   * build), and the caller sums them (the reference's MPIReduce,
+   * direct.hpp:2085-2107).  AX is accumulated into, so give a prior value on
+   * one shard only.  Defaults 0 / 1. */
+  int shard_index;
+  int shard_count;
 } cqf_opts;
 
 typedef struct {

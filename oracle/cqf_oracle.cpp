@@ -564,10 +564,14 @@ struct Stats {
 // GTODirectTPIContraction::directScaffoldNew, one basis (basisSet_ ==
 // basisSet2_), screen = true.  AX is accumulated as with >1 thread
 // (direct.hpp:2047-2058): AX += 1/2 (A + A^H) (HER) or AX += 1/2 A.
+// mpiRank / mpiSize: the reference's MPI split, contiguous chunks of the
+// significant-pair counter s12 of (nshell (nshell + 1) / 2) / mpiSize pairs,
+// the last rank taking the rest (direct.hpp:1600-1604, :1655-1656); the
+// ranks' AX sum to the whole contraction (MPIReduce, :2085-2107).
 template <typename T>
 void direct_scaffold(Basis& bs, int nMat, const int* her, const int* type,
                      const T* const* X, T* const* AX, double thresh, int nThreads,
-                     bool screen, Stats* stats) {
+                     bool screen, Stats* stats, int mpiRank = 0, int mpiSize = 1) {
   int ns = (int)bs.shells.size();
   int N = bs.nbasis;
   if (!bs.have_schwarz) compute_schwarz(bs);
@@ -599,6 +603,10 @@ void direct_scaffold(Basis& bs, int nMat, const int* her, const int* type,
 
   std::vector<T> AXraw((size_t)nThreads * nMat * N * N, T(0.0));
   std::vector<int64_t> nTot(nThreads, 0), nSkip(nThreads, 0);
+  const size_t npairMax = (size_t)ns * (ns + 1) / 2;
+  const size_t mpiChunks = npairMax / (size_t)mpiSize;
+  const size_t mpiS12St = (size_t)mpiRank * mpiChunks;
+  const size_t mpiS12End = (mpiRank == mpiSize - 1) ? npairMax : (size_t)(mpiRank + 1) * mpiChunks;
 
 #pragma omp parallel num_threads(nThreads)
   {
@@ -612,6 +620,10 @@ void direct_scaffold(Basis& bs, int nMat, const int* her, const int* type,
       int n1 = bs.shells[s1].size(), bf1s = bs.off[s1];
       for (int s2 : bs.sig[s1]) {
         int n2 = bs.shells[s2].size(), bf2s = bs.off[s2];
+        if (s12 < mpiS12St || s12 >= mpiS12End) {
+          s12++;
+          continue;
+        }
         if ((s12++) % nThreads != (size_t)tid) continue;
         double s12deg = (s1 == s2) ? 1.0 : 2.0;
         double shz12 = 0, shMax12 = 0;
@@ -1126,25 +1138,33 @@ int orc_sig_pairs(void* b, int* s1out, int* s2out) {
 
 // directScaffoldNew restated.  X/AX: arrays of nMat pointers to column-major
 // N x N buffers (double or interleaved complex).  AX is accumulated.
-int orc_contract(void* b, int nMat, int is_complex, const int* her, const int* type,
-                 const void* const* X, void* const* AX, double thresh, int nthreads,
-                 int screen, long long* stats_out) {
+int orc_contract_part(void* b, int nMat, int is_complex, const int* her, const int* type,
+                      const void* const* X, void* const* AX, double thresh, int nthreads,
+                      int screen, long long* stats_out, int mpi_rank, int mpi_size) {
   auto* bs = static_cast<Basis*>(b);
   Stats st;
+  if (mpi_size < 1 || mpi_rank < 0 || mpi_rank >= mpi_size) return 1;
   if (is_complex)
     direct_scaffold<dcomplex>(*bs, nMat, her, type, reinterpret_cast<const dcomplex* const*>(X),
                               reinterpret_cast<dcomplex* const*>(AX), thresh, nthreads,
-                              screen != 0, &st);
+                              screen != 0, &st, mpi_rank, mpi_size);
   else
     direct_scaffold<double>(*bs, nMat, her, type, reinterpret_cast<const double* const*>(X),
                             reinterpret_cast<double* const*>(AX), thresh, nthreads, screen != 0,
-                            &st);
+                            &st, mpi_rank, mpi_size);
   if (stats_out) {
     stats_out[0] = st.quartets_total;
     stats_out[1] = st.quartets_screened;
     stats_out[2] = st.quartets_computed;
   }
   return 0;
+}
+
+int orc_contract(void* b, int nMat, int is_complex, const int* her, const int* type,
+                 const void* const* X, void* const* AX, double thresh, int nthreads,
+                 int screen, long long* stats_out) {
+  return orc_contract_part(b, nMat, is_complex, her, type, X, AX, thresh, nthreads, screen,
+                           stats_out, 0, 1);
 }
 
 // Algorithmic FLOP count of one build under the frozen count model, over the

@@ -56,6 +56,8 @@ def lib():
                                    C.POINTER(C.c_void_p),
                                    C.POINTER(C.c_void_p), C.c_double, C.c_int,
                                    C.c_int, C.POINTER(C.c_longlong)]
+        L.orc_contract_part.argtypes = L.orc_contract.argtypes + [C.c_int, C.c_int]
+        L.orc_contract_part.restype = C.c_int
         L.orc_flops.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                 C.c_double, C.c_double, dp]
         L.orc_dirac_coulomb.argtypes = [C.c_void_p, C.POINTER(C.c_void_p),
@@ -182,9 +184,11 @@ class OracleBasis:
         return a, b
 
     def contract(self, mats, her, types, thresh=1e-12, nthreads=0,
-                 screen=True, AX=None):
+                 screen=True, AX=None, mpi=(0, 1)):
         """Restated ``twoBodyContract``: returns the list of AX (accumulated
-        into ``AX`` when given).  ``mats``: N x N arrays (real or complex)."""
+        into ``AX`` when given).  ``mats``: N x N arrays (real or complex).
+        ``mpi = (rank, size)``: this rank's part under the reference's MPI
+        split of the shell-pair loop."""
         is_c = any(np.iscomplexobj(m) for m in mats)
         dt = np.complex128 if is_c else np.float64
         Xs = [np.asfortranarray(m, dtype=dt) for m in mats]
@@ -198,8 +202,11 @@ class OracleBasis:
         h = np.array(her, dtype=np.int32)
         t = np.array(types, dtype=np.int32)
         st = (C.c_longlong * 3)()
-        lib().orc_contract(self.h, n, 1 if is_c else 0, _ip(h), _ip(t), xp, ap,
-                           thresh, nthreads, 1 if screen else 0, st)
+        rc = lib().orc_contract_part(self.h, n, 1 if is_c else 0, _ip(h), _ip(t), xp, ap,
+                                     thresh, nthreads, 1 if screen else 0, st,
+                                     int(mpi[0]), int(mpi[1]))
+        if rc:
+            raise ValueError("mpi rank outside [0, size)")
         self.last_stats = dict(total=st[0], screened=st[1], computed=st[2])
         return AX
 
