@@ -24,7 +24,8 @@ EXPORTS = ("cqf_opts_default", "cqf_basis_create", "cqf_basis_destroy",
            "cqf_two_body_contract", "cqf_two_body_contract_noalloc", "cqf_autotune",
            "cqf_graph_create", "cqf_graph_launch", "cqf_graph_destroy",
            "cqf_rel_two_body_contract", "cqf_dc_opts_default",
-           "cqf_four_comp_gd", "cqf_server_opts_default", "cqf_fock_footprint",
+           "cqf_four_comp_gd", "cqf_grad_two_body_contract",
+           "cqf_server_opts_default", "cqf_fock_footprint",
            "cqf_server_create", "cqf_server_submit", "cqf_server_wait",
            "cqf_server_get_stats", "cqf_server_destroy", "cqf_last_error")
 # cqf_rel_comp / cqf_rel_type (DIRAC_PAULI_SPINOR_COMP order)
@@ -165,6 +166,10 @@ def lib():
         C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
         C.POINTER(CqfDcOpts), C.POINTER(CqfOpts), C.POINTER(CqfStats)]
     L.cqf_four_comp_gd.restype = C.c_int
+    L.cqf_grad_two_body_contract.argtypes = [
+        C.c_void_p, C.POINTER(C.c_int), C.c_int, C.POINTER(CqfContraction), C.c_int,
+        C.POINTER(C.c_void_p), C.POINTER(CqfOpts), C.POINTER(CqfStats)]
+    L.cqf_grad_two_body_contract.restype = C.c_int
     L.cqf_server_opts_default.argtypes = [C.POINTER(CqfServerOpts)]
     L.cqf_server_opts_default.restype = None
     L.cqf_fock_footprint.argtypes = [C.POINTER(CqfShell), C.c_int]

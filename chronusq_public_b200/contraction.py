@@ -408,3 +408,81 @@ class GTODirectRelERIContraction:
             else:
                 c.AX = AX
         self.last_stats = _stats(st)
+
+
+class DirectGradContraction:
+    """``DirectGradContraction<double,double>::gradTwoBodyContract``
+    (include/particleintegrals/gradints.hpp:278-283 -> directScaffoldGrad,
+    contract/direct.hpp:2198-2571) on the GPU."""
+
+    def __init__(self, tpi: DirectTPI):
+        self.tpi = tpi
+        self.last_stats: Optional[dict] = None
+
+    def gradTwoBodyContract(self, cList: List[List[TwoBodyContraction]],
+                            shell_atom, stream=None,
+                            shard: Tuple[int, int] = (0, 1)) -> None:
+        """``cList[3 atom + xyz][m]``: the contraction of matrix m for that
+        nuclear coordinate (all components share X, HER and contType; each
+        its own AX, added into as 1/2 (A + A^T)).  X real symmetric N x N
+        (numpy, or column-major CUDA float64 tensors); ``shell_atom[s]``:
+        the atom of shell s.  Non-Hermitian and complex X are not built."""
+        nGrad = len(cList)
+        if nGrad == 0 or nGrad % 3:
+            raise ValueError("cList has 3 entries per atom")
+        nMat = len(cList[0])
+        N = self.tpi.nbasis
+        first = cList[0]
+        dev = _is_torch(first[0].X)
+        arr = (_cabi.CqfContraction * nMat)()
+        keep, writeback = [], []
+        for m, c in enumerate(first):
+            if dev:
+                X = c.X
+                if tuple(X.shape) != (N, N) or not X.is_cuda or X.stride() != (1, N):
+                    raise ValueError("device matrices must be (N, N) column-major")
+                arr[m].X = C.c_void_p(X.data_ptr())
+            else:
+                X = np.asfortranarray(c.X, dtype=np.float64)
+                if X.shape != (N, N):
+                    raise ValueError("matrix shape must be (N, N)")
+                keep.append(X)
+                arr[m].X = C.c_void_p(X.ctypes.data)
+            arr[m].hermitian = 1 if c.HER else 0
+            arr[m].type = int(c.contType)
+        axs = (C.c_void_p * (nGrad * nMat))()
+        for g, comp in enumerate(cList):
+            if len(comp) != nMat:
+                raise ValueError("every component has the same matrices")
+            for m, c in enumerate(comp):
+                if dev:
+                    if tuple(c.AX.shape) != (N, N) or c.AX.stride() != (1, N):
+                        raise ValueError("device matrices must be (N, N) column-major")
+                    axs[g * nMat + m] = c.AX.data_ptr()
+                else:
+                    if isinstance(c.AX, np.ndarray) and c.AX.dtype == np.float64 \
+                            and c.AX.flags.f_contiguous and c.AX.shape == (N, N):
+                        AX = c.AX
+                    else:
+                        AX = np.asfortranarray(c.AX, dtype=np.float64)
+                        writeback.append((c, AX))
+                    keep.append(AX)
+                    axs[g * nMat + m] = AX.ctypes.data
+        sa = np.ascontiguousarray(shell_atom, dtype=np.int32)
+        if sa.shape != (self.tpi.nshell,):
+            raise ValueError("shell_atom has one entry per shell")
+        opts = _cabi.CqfOpts()
+        _cabi.lib().cqf_opts_default(C.byref(opts))
+        opts.device_pointers = 1 if dev else 0
+        opts.stream = _stream_arg(stream)
+        opts.shard_index, opts.shard_count = int(shard[0]), int(shard[1])
+        st = _cabi.CqfStats()
+        _cabi.check(_cabi.lib().cqf_grad_two_body_contract(
+            self.tpi.handle, sa.ctypes.data_as(C.POINTER(C.c_int)), nGrad // 3, arr, nMat,
+            axs, C.byref(opts), C.byref(st)))
+        for c, AX in writeback:
+            if isinstance(c.AX, np.ndarray) and c.AX.shape == (N, N):
+                c.AX[...] = AX
+            else:
+                c.AX = AX
+        self.last_stats = _stats(st)

@@ -1360,6 +1360,14 @@ void launch_max_norms(const double* nm, int nMat, size_t ns2, double* out,
   max_norms_kernel<<<grid1(ns2, 256), 256, 0, st>>>(nm, nMat, ns2, out, gmax);
 }
 
+void launch_from_cart(const cqf_basis* B, const double* Ac, int cplx, int her, double* AX,
+                      cudaStream_t st) {
+  const size_t NN = (size_t)B->nbasis * B->nbasis;
+  from_cart_kernel<<<grid1(NN, 256), 256, 0, st>>>(Ac, cplx, her, B->nbasis, B->ncart,
+                                                   B->d_shells, B->d_ao2shell, B->d_sph,
+                                                   B->d_sphOff, AX);
+}
+
 void launch_to_cart(const cqf_basis* B, const double* X, int cplx, double* Xc, cudaStream_t st) {
   const size_t nc2 = (size_t)B->ncart * B->ncart;
   to_cart_kernel<<<grid1(nc2, 256), 256, 0, st>>>(X, cplx, B->nbasis, B->ncart, B->d_shells,

@@ -175,6 +175,10 @@ void launch_max_norms(const double* nm, int nMat, size_t ns2, double* out,
                       unsigned long long* gmax, cudaStream_t st);
 // Xc = T X T^T (spherical -> Cartesian AO), real or complex interleaved.
 void launch_to_cart(const cqf_basis* B, const double* X, int cplx, double* Xc, cudaStream_t st);
+// AX (N x N) += the back transform of the Cartesian accumulator Ac:
+// 1/2 (B + B^H) with her = 1, 1/2 B with her = 0 (B = T^T Ac T).
+void launch_from_cart(const cqf_basis* B, const double* Ac, int cplx, int her, double* AX,
+                      cudaStream_t st);
 // Grows the basis' contraction workspace (B->d_ws) to at least `bytes`.
 cqf_status basis_workspace(cqf_basis* B, size_t bytes);
 

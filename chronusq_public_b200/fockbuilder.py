@@ -18,7 +18,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from .contraction import (COULOMB, EXCHANGE, DirectTPI,
+from .contraction import (COULOMB, EXCHANGE, DirectGradContraction, DirectTPI,
                           GTODirectTPIContraction, TwoBodyContraction, _is_torch)
 
 
@@ -125,6 +125,32 @@ class FockBuilder:
     def formFock(self, H, D, **kw):
         G, _J, _K = self.formRawGD(D, **kw)
         return H + G
+
+    def getGDGrad(self, D, shell_atom, natom: int, xHFX: float = 1.0) -> np.ndarray:
+        """``FockBuilder::getGDGrad`` (include/fockbuilder/impl.hpp:400-497)
+        for a closed-shell real density: the two-electron energy gradient
+        1/4 Tr[D (2 J^x - xHFX K^x)] for every nuclear coordinate, (natom, 3),
+        with J^x / K^x from the gradient contraction."""
+        N = self.tpi.nbasis
+        cList, JL, KL = [], [], []
+        for _ in range(3 * natom):
+            J = np.zeros((N, N), order="F")
+            comp = [TwoBodyContraction(D, J, True, COULOMB)]
+            JL.append(J)
+            if abs(xHFX) > 1e-12:
+                K = np.zeros((N, N), order="F")
+                comp.append(TwoBodyContraction(D, K, True, EXCHANGE))
+                KL.append(K)
+            cList.append(comp)
+        DirectGradContraction(self.tpi).gradTwoBodyContract(
+            cList, shell_atom, shard=_shard_of(self.group))
+        allreduce_sum(JL + KL, self.group, self.tpi.device)
+        Dt = np.asarray(D).T
+        out = np.zeros(3 * natom)
+        for g in range(3 * natom):
+            G = 2.0 * JL[g] - (xHFX * KL[g] if KL else 0.0)
+            out[g] = 0.25 * float(np.sum(G * Dt))
+        return out.reshape(natom, 3)
 
 
 def two_electron_energy(G, D) -> float:

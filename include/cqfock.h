@@ -287,6 +287,24 @@ cqf_status cqf_four_comp_gd(cqf_basis* basis, const void* const* D, void* const*
                             const cqf_dc_opts* dc, const cqf_opts* opts, cqf_stats* stats);
 
 /* ---------------------------------------------------------------------
+ * Nuclear-gradient contraction.
+ *
+ * DirectGradContraction::gradTwoBodyContract (include/particleintegrals/
+ * gradints.hpp:278-283) -> directScaffoldGrad (include/particleintegrals/
+ * contract/direct.hpp:2198-2571): for each of the nMat Hermitian real
+ * matrices list[m].X (COULOMB or EXCHANGE; list[m].AX is not used) and each
+ * nuclear coordinate (atom, xyz), the J- or K-type contraction of
+ * d(mu nu|la si)/dR_{atom,xyz}, added into AX[(3 atom + xyz) * nMat + m]
+ * (3 natom nMat N x N arrays) as 1/2 (A + A^T).  shell_atom[s] is the atom
+ * of shell s (ChronusQ's mapSh2Cen).  Every quartet of significant pairs is
+ * computed (the reference does not screen here); FP64; at most 8 matrices;
+ * complex and non-Hermitian X are not built (the reference stops on the
+ * latter).  opts: device_pointers, stream, shard_index / shard_count. */
+cqf_status cqf_grad_two_body_contract(cqf_basis* basis, const int* shell_atom, int natom,
+                                      const cqf_contraction* list, int nMat, void* const* AX,
+                                      const cqf_opts* opts, cqf_stats* stats);
+
+/* ---------------------------------------------------------------------
  * Fock-build server: requests of any basis size arrive at any time and
  * share one GPU (continuous batching).  No counterpart in the reference
  * (ChronusQ runs one build at a time); each request is the closed-shell

@@ -216,4 +216,37 @@ class FourCompFock {
   cqf_dc_opts dc_;
 };
 
+// DirectGradContraction<double,double>::gradTwoBodyContract
+// (include/particleintegrals/gradints.hpp:278-283): cList[3 atom + xyz][m],
+// every component with the same X / HER / contType and its own AX (added
+// into); shellAtom: ChronusQ's mapSh2Cen.
+class DirectGradContraction {
+ public:
+  explicit DirectGradContraction(std::shared_ptr<DirectTPI> tpi) : tpi_(std::move(tpi)) {}
+
+  void gradTwoBodyContract(std::vector<std::vector<TwoBodyContraction<double>>>& cList,
+                           const std::vector<int>& shellAtom, cqf_stats* stats = nullptr) const {
+    if (cList.empty() || cList.size() % 3)
+      throw std::runtime_error("DirectGradContraction: 3 components per atom");
+    const int nMat = (int)cList[0].size();
+    std::vector<cqf_contraction> list(nMat);
+    for (int m = 0; m < nMat; m++)
+      list[m] = {cList[0][m].X, nullptr, cList[0][m].HER ? 1 : 0, (int)cList[0][m].contType};
+    std::vector<void*> AX;
+    for (auto& comp : cList) {
+      if ((int)comp.size() != nMat)
+        throw std::runtime_error("DirectGradContraction: ragged contraction list");
+      for (auto& c : comp) AX.push_back(c.AX);
+    }
+    cqf_opts o;
+    cqf_opts_default(&o);
+    check(cqf_grad_two_body_contract(tpi_->handle(), shellAtom.data(), (int)cList.size() / 3,
+                                     list.data(), nMat, AX.data(), &o, stats),
+          "cqf_grad_two_body_contract");
+  }
+
+ private:
+  std::shared_ptr<DirectTPI> tpi_;
+};
+
 }  // namespace cqfock

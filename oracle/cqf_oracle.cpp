@@ -1472,6 +1472,89 @@ void eri_deriv_quartet(const Basis& bs, int s1, int s2, int s3, int s4, int dmas
   (void)sh;
 }
 
+// DirectGradContraction::directScaffoldGrad (direct.hpp:2198-2571): for
+// Hermitian real X, the contractions of the first derivatives of the ERIs
+// with respect to the nuclear coordinates -- over the 8-fold quartet loop of
+// significant pairs without screening (:2343-2398), the 12 derivatives of
+// each quartet (3 per centre; d/dA = -d/dr of the orbital) scaled by
+// 0.5 * degeneracy, each added into the matrices of gradient component
+// atom(shell) * 3 + xyz with the COULOMB / EXCHANGE update sites
+// (:2470-2520) -- then AX += 1/2 (A + A^T) per component and matrix
+// (:2550-2560).  AX: [component][matrix], 3 * nAtom * nMat N x N arrays.
+void grad_scaffold(const Basis& bs, const int* shellAtom, int nAtom, int nMat, const int* type,
+                   const double* const* X, double* const* AX, int nThreads) {
+  const int ns = (int)bs.shells.size(), N = bs.nbasis;
+  const size_t NN = (size_t)N * N;
+  const int nGrad = 3 * nAtom;
+  if (nThreads <= 0) nThreads = omp_get_max_threads();
+  std::vector<double> loc((size_t)nThreads * nGrad * nMat * NN, 0.0);
+#pragma omp parallel num_threads(nThreads)
+  {
+    const int tid = omp_get_thread_num();
+    double* A = &loc[(size_t)tid * nGrad * nMat * NN];
+    auto at = [&](int g, int m, int r, int c) -> double& {
+      return A[((size_t)g * nMat + m) * NN + r + (size_t)c * N];
+    };
+    std::vector<double> buf[4];
+    size_t s12 = 0;
+    for (int s1 = 0; s1 < ns; s1++)
+      for (int s2 : bs.sig[s1]) {
+        if ((s12++) % nThreads != (size_t)tid) continue;
+        const double s12deg = (s1 == s2) ? 1.0 : 2.0;
+        for (int s3 = 0; s3 <= s1; s3++) {
+          const int s4max = (s1 == s3) ? s2 : s3;
+          for (int s4 : bs.sig[s3]) {
+            if (s4 > s4max) break;
+            const double s34deg = (s3 == s4) ? 1.0 : 2.0;
+            const double s1234deg = (s1 == s3) ? (s2 == s4 ? 1.0 : 2.0) : 2.0;
+            const double f = -0.5 * s12deg * s34deg * s1234deg;  // d/dA = -d/dr
+            const int sh[4] = {s1, s2, s3, s4};
+            for (int c = 0; c < 4; c++) eri_deriv_quartet(bs, s1, s2, s3, s4, 1 << c, buf[c]);
+            const int n1 = bs.shells[s1].size(), n2 = bs.shells[s2].size();
+            const int n3 = bs.shells[s3].size(), n4 = bs.shells[s4].size();
+            const size_t nq = (size_t)n1 * n2 * n3 * n4;
+            for (int c = 0; c < 4; c++)
+              for (int xyz = 0; xyz < 3; xyz++) {
+                const int g = shellAtom[sh[c]] * 3 + xyz;
+                const double* I = buf[c].data() + (size_t)xyz * nq;
+                for (int i = 0; i < n1; i++)
+                  for (int j = 0; j < n2; j++)
+                    for (int k = 0; k < n3; k++)
+                      for (int l = 0; l < n4; l++) {
+                        const double v = f * I[(((size_t)i * n2 + j) * n3 + k) * n4 + l];
+                        const int b1 = bs.off[s1] + i, b2 = bs.off[s2] + j;
+                        const int b3 = bs.off[s3] + k, b4 = bs.off[s4] + l;
+                        for (int m = 0; m < nMat; m++) {
+                          const double* Xm = X[m];
+                          auto x = [&](int r, int cc) { return Xm[r + (size_t)cc * N]; };
+                          if (type[m] == 0) {  // COULOMB
+                            at(g, m, b1, b2) += x(b4, b3) * v;
+                            at(g, m, b4, b3) += x(b1, b2) * v;
+                          } else {  // EXCHANGE
+                            at(g, m, b1, b3) += 0.5 * x(b4, b2) * v;
+                            at(g, m, b4, b2) += 0.5 * x(b3, b1) * v;
+                            at(g, m, b4, b1) += 0.5 * x(b3, b2) * v;
+                            at(g, m, b2, b3) += 0.5 * x(b4, b1) * v;
+                          }
+                        }
+                      }
+              }
+          }
+        }
+      }
+  }
+  for (int g = 0; g < nGrad; g++)
+    for (int m = 0; m < nMat; m++) {
+      double* out = AX[(size_t)g * nMat + m];
+      for (int t = 0; t < nThreads; t++) {
+        const double* a = &loc[(((size_t)t * nGrad + g) * nMat + m) * NN];
+        for (int c = 0; c < N; c++)
+          for (int r = 0; r < N; r++)
+            out[r + (size_t)c * N] += 0.5 * (a[r + (size_t)c * N] + a[c + (size_t)r * N]);
+      }
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -2328,5 +2411,14 @@ int orc_rel_contract(void* b, int type, const void* const* Xv, void* const* AXv,
   direct_4c(*bs, type, X, AX, thresh, Qs, exchange != 0);
   return 0;
 }
+
+// DirectGradContraction::directScaffoldGrad on real Hermitian X
+// (grad_scaffold); AX: 3 * natom * nMat arrays, component-major.
+int orc_grad_contract(void* b, const int* shell_atom, int natom, int nMat, const int* type,
+                      const double* const* X, double* const* AX, int nthreads) {
+  grad_scaffold(*static_cast<Basis*>(b), shell_atom, natom, nMat, type, X, AX, nthreads);
+  return 0;
+}
+
 
 }  // extern "C"

@@ -58,6 +58,9 @@ def lib():
                                    C.c_int, C.POINTER(C.c_longlong)]
         L.orc_contract_part.argtypes = L.orc_contract.argtypes + [C.c_int, C.c_int]
         L.orc_contract_part.restype = C.c_int
+        L.orc_grad_contract.argtypes = [C.c_void_p, ip, C.c_int, C.c_int, ip,
+                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]
+        L.orc_grad_contract.restype = C.c_int
         L.orc_flops.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
                                 C.c_double, C.c_double, dp]
         L.orc_dirac_coulomb.argtypes = [C.c_void_p, C.POINTER(C.c_void_p),
@@ -209,6 +212,22 @@ class OracleBasis:
             raise ValueError("mpi rank outside [0, size)")
         self.last_stats = dict(total=st[0], screened=st[1], computed=st[2])
         return AX
+
+    def grad_contract(self, mats, types, shell_atom, natom, nthreads=0):
+        """Restated ``DirectGradContraction::directScaffoldGrad`` on real
+        symmetric ``mats``: returns [3 * natom][len(mats)] N x N arrays, the
+        contractions of d(mu nu|la si)/dR for every atom and x, y, z."""
+        N = self.nbasis
+        Xs = [np.asfortranarray(m, dtype=np.float64) for m in mats]
+        n = len(Xs)
+        out = [[np.zeros((N, N), order="F") for _ in range(n)] for _ in range(3 * natom)]
+        flat = [a for comp in out for a in comp]
+        xp = (C.c_void_p * n)(*[x.ctypes.data for x in Xs])
+        ap = (C.c_void_p * len(flat))(*[a.ctypes.data for a in flat])
+        sa = np.ascontiguousarray(shell_atom, dtype=np.int32)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        lib().orc_grad_contract(self.h, _ip(sa), int(natom), n, _ip(t), xp, ap, nthreads)
+        return out
 
     def dirac_coulomb(self, D, bare=True, dc=True, ssss=True, xHFX=1.0,
                       thresh=1e-12, libcint=True, gaunt=False, gauge=False):
