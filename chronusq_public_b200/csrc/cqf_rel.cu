@@ -1026,17 +1026,22 @@ __global__ void __launch_bounds__(RB_THREADS)
 // run as register-tiled loops over shared memory, every lane busy: a thread
 // owns a 4 x 4 tile, for the second product (one bra pair's 4 operator
 // components) x (one ket pair's 4 components; LLSS: 4 ket pairs), which is
-// then digested from registers at the reference's update sites.  Same
-// quartet set, screens and digestion as the block kernels, which keep the
-// contracted quartets (and the classes whose layout does not fit).
+// then digested from registers at the reference's update sites.  A block
+// takes one bra pair and a tile of up to KT ket pairs: the bra's E tables,
+// axis factors and H are built once and stay in shared memory while the
+// block walks its kets; per ket the R recursion runs in one warp (warp
+// syncs only) from a table of Hermite indices.  Same quartet set, screens
+// and digestion as the block kernels, which keep the contracted quartets
+// (and the classes whose layout does not fit).
 constexpr int RG_THREADS = 256;
 constexpr size_t RG_SMEM_MAX = 224 * 1024;
 
 struct RelGemmLayout {
   int HB, HBp, HK, HR, CH, CR, CRp, NT;
   int oH, oRm, oFk, oJs, oTuv, oScr;
-  int oEb, oEk, oR0, oR1, oFa, oF;  // phase 1, in the scratch area
-  int oK, oG;                       // per ket chunk, in the scratch area
+  int oEb, oFa;                 // bra phase, in the scratch area
+  int oEk, oR0, oR1, oF;        // per-ket phase, in the scratch area
+  int oK, oG;                   // per ket chunk, in the scratch area
   int total;
 };
 __host__ __device__ inline int rg_round(int n, int m) { return (n + m - 1) / m * m; }
@@ -1054,7 +1059,7 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   Lo.CH = CH;
   Lo.CR = CH * NB;
   Lo.CRp = rg_round(Lo.CR, 4);
-  Lo.NT = nherm(Lb > Lk ? Lb : Lk);
+  Lo.NT = nherm(L);
   int o = 0;
   auto take = [&](int n) { int r = o; o += rg_round(n, 2); return r; };
   Lo.oH = take(Lo.HB * Lo.HR);
@@ -1064,18 +1069,21 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   Lo.oTuv = take((Lo.NT + 1) / 2);  // packed (t, u, v) of each Hermite index, as int
   Lo.oScr = o;
   int p = o;
-  auto take1 = [&](int n) { int r = p; p += rg_round(n, 2); return r; };
-  Lo.oEb = take1(3 * (la + 2) * (lb + 2) * (la + lb + 3));
-  Lo.oEk = take1(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
-  Lo.oR0 = take1(nherm(L));
-  Lo.oR1 = take1(nherm(L));
-  Lo.oFa = take1(nab * 12 * FL);
-  Lo.oF = take1(L + 1);
+  auto takeB = [&](int n) { int r = p; p += rg_round(n, 2); return r; };
+  Lo.oEb = takeB(3 * (la + 2) * (lb + 2) * (la + lb + 3));
+  Lo.oFa = takeB(nab * 12 * FL);
+  int k = o;
+  auto takeK = [&](int n) { int r = k; k += rg_round(n, 2); return r; };
+  Lo.oEk = takeK(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
+  Lo.oR0 = takeK(nherm(L));
+  Lo.oR1 = takeK(nherm(L));
+  Lo.oF = takeK(L + 1);
   int q = o;
-  auto take2 = [&](int n) { int r = q; q += rg_round(n, 2); return r; };
-  Lo.oK = take2(Lo.HK * Lo.CRp);
-  Lo.oG = take2(Lo.HBp * Lo.CRp);
-  Lo.total = p > q ? p : q;
+  auto takeC = [&](int n) { int r = q; q += rg_round(n, 2); return r; };
+  Lo.oK = takeC(Lo.HK * Lo.CRp);
+  Lo.oG = takeC(Lo.HBp * Lo.CRp);
+  Lo.total = p > k ? p : k;
+  if (q > Lo.total) Lo.total = q;
   return Lo;
 }
 // the largest ket chunk whose layout fits (0: the class does not fit)
@@ -1086,58 +1094,23 @@ inline int rel_gemm_chunk(int la, int lb, int lc, int ld, int type) {
       return ch;
   return 0;
 }
+// ket pairs per block
+constexpr int RG_KT = 8;
 
 template <int TYPE>
-__global__ void __launch_bounds__(RG_THREADS)
+__global__ void __launch_bounds__(RG_THREADS, 2)
     rel_gemm_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int CH) {
   extern __shared__ double sm[];
+  const int nTiles = (a.nKet + RG_KT - 1) / RG_KT;
   const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
-  int ib, jk;
-  if (TYPE == 2 && a.same) {  // SSSS, one class: unordered pairs jk <= ib
-    long long r = (long long)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
-    while (r * (r + 1) / 2 > q) r--;
-    while ((r + 1) * (r + 2) / 2 <= q) r++;
-    ib = (int)r;
-    jk = (int)(q - r * (r + 1) / 2);
-  } else {
-    ib = (int)(q / a.nKet);
-    jk = (int)(q % a.nKet);
-  }
+  const int ib = (int)(q / nTiles), tile = (int)(q % nTiles);
   if (ib >= a.nBra || !in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;
-  const int ns = a.nShell;
+  const bool tri = (TYPE == 2 && a.same);  // SSSS, one class: kets jk <= ib
+  if (tri && tile * RG_KT > ib) return;
   const PairDev P = a.pairs[a.braBeg + ib];
-  const PairDev Q = a.pairs[a.ketBeg + jk];
-  if (P.npp != 1 || Q.npp != 1) return;  // contracted: the block kernels
-  bool work, mine;
-  {
-    int s1, s2, s3, s4;
-    double q12, q34;
-    if (TYPE == 1) {
-      s1 = P.s1; s2 = P.s2; s3 = Q.s1; s4 = Q.s2;
-      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
-      q34 = __ldg(a.qLL + s3 + (size_t)s4 * ns);
-    } else {
-      const bool pRef = P.lex >= Q.lex;
-      const PairDev& R12 = pRef ? P : Q;
-      const PairDev& R34 = pRef ? Q : P;
-      s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
-      q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
-      q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
-    }
-    const double bound = sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34;
-    work = !a.screen || bound >= a.thresh;
-    const bool lo = a.mixed && bound < a.cut &&
-                    fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
-                                  __ldg(a.pairRange + a.ketBeg + jk),
-                                  la + lb + lc + ld + 2 + 2 * (TYPE == 2), 1, TYPE == 2);
-    mine = work && !lo;
-  }
-  if (threadIdx.x == 0) {
-    atomicAdd(a.counters + 0, 1ull);
-    if (!work) atomicAdd(a.counters + 1, 1ull);
-    if (mine) atomicAdd(a.counters + 3, 1ull);
-  }
-  if (!mine) return;  // block-uniform
+  if (P.npp != 1) return;  // contracted: the block kernels
+  const int jkEnd = min(tile * RG_KT + RG_KT, tri ? ib + 1 : a.nKet);
+  const int ns = a.nShell;
 
   constexpr int NB = (TYPE == 2) ? 4 : 1;
   const int tid = threadIdx.x;
@@ -1154,19 +1127,18 @@ __global__ void __launch_bounds__(RG_THREADS)
   double* Js = sm + Lo.oJs;
   int* tuv = reinterpret_cast<int*>(sm + Lo.oTuv);
   double* Eb = sm + Lo.oEb;
+  double* fa = sm + Lo.oFa;
   double* Ek = sm + Lo.oEk;
   double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
-  double* fa = sm + Lo.oFa;
   double* Fs = sm + Lo.oF;
   double* Ks = sm + Lo.oK;
   double* Gs = sm + Lo.oG;
   const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
   const int E1k = (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK);
   const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
-  const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
-  const bool dAB = P.shA == P.shB, dCD = Q.shA == Q.shB, samePQ = P.lex == Q.lex;
+  const bool dAB = P.shA == P.shB;
   const double s12d = dAB ? 1.0 : 2.0;
-  const double w12 = dAB ? 0.5 : 1.0, w34 = dCD ? 0.5 : 1.0;
+  const double w12 = dAB ? 0.5 : 1.0;
   const size_t nc = a.ncart;
   auto unpack = [&](int h, int& t, int& u, int& v) {
     const int w = tuv[h];
@@ -1175,21 +1147,12 @@ __global__ void __launch_bounds__(RG_THREADS)
     v = w >> 16;
   };
 
-  // ---- phase 1: E tables, R, the axis factors of every component pair
+  // ---- bra phase, once per block: E tables, axis factors, H
   const PrimPairDev& A = a.pp[P.pp_off];
-  const PrimPairDev& B = a.pp[Q.pp_off];
-  double ea, eb, ec, ed;
+  double ea, eb;
   pair_exps(SA, SB, a.prim, A, ea, eb);
-  pair_exps(SC, SD, a.prim, B, ec, ed);
   if (tid < 3)
     hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid], Eb + tid * E1b);
-  else if (tid < 6)
-    hermite_E_rt<double, LMAX + 1>(lc + dK, ld + dK, B.o2p, B.PA[tid - 3], B.PB[tid - 3],
-                                   Ek + (tid - 3) * E1k);
-  const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
-  const double pq = A.p + B.p, alpha = A.p * B.p / pq;
-  const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
-  if (tid == 6) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
   for (int h = tid; h < Lo.NT; h += RG_THREADS) {
     int t, u, v;
     hinv(h, t, u, v);
@@ -1197,36 +1160,6 @@ __global__ void __launch_bounds__(RG_THREADS)
   }
   for (int e = tid; e < 4 * CH; e += RG_THREADS) Js[e] = 0.0;
   __syncthreads();
-  {
-    const double m2a = -2.0 * alpha;
-    for (int n = L; n >= 0; n--) {
-      double* cur = Rb[n & 1];
-      const double* prv = Rb[(n + 1) & 1];
-      const int cnt = nherm(L - n);
-      for (int e = tid; e < cnt; e += RG_THREADS) {
-        int t, u, v;
-        hinv(e, t, u, v);
-        double val;
-        if (e == 0) {
-          double f = 1.0;
-          for (int k = 0; k < n; k++) f *= m2a;
-          val = f * Fs[n];
-        } else if (t > 0) {
-          val = X * prv[hidx(t - 1, u, v)];
-          if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
-        } else if (u > 0) {
-          val = Y * prv[hidx(0, u - 1, v)];
-          if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
-        } else {
-          val = Z * prv[hidx(0, 0, v - 1)];
-          if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
-        }
-        cur[e] = val;
-      }
-      __syncthreads();
-    }
-  }
-  const double* R = Rb[0];
   for (int it = tid; it < nab * 12; it += RG_THREADS) {
     const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
     const int ai = ab / nb, bi = ab % nb;
@@ -1235,19 +1168,7 @@ __global__ void __launch_bounds__(RG_THREADS)
     axis_factor<double>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
                         fa + (size_t)it * FL);
   }
-  for (int it = tid; it < ncd * 12; it += RG_THREADS) {
-    const int cd = it / 12, x = (it % 12) / 4, ty = it % 4;
-    if (TYPE == 1 && ty) continue;
-    const int c = cd / nd, d = cd % nd;
-    const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
-    const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
-    double* f = fk + (size_t)it * FLk;
-    const int n = axis_factor<double>(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
-                                      2.0 * ec, 2.0 * ed, f);
-    for (int t = 1; t < n; t += 2) f[t] = -f[t];
-  }
   __syncthreads();
-  // H[h][(ab, op)] and Rm[h'][h] (pref folded in)
   for (int e = tid; e < HB * HR; e += RG_THREADS) {
     const int h = e / HR, row = e % HR, ab = row / 4, op = row % 4;
     const int ai = ab / nb, bi = ab % nb;
@@ -1274,170 +1195,265 @@ __global__ void __launch_bounds__(RG_THREADS)
       }
     Hs[e] = val;
   }
-  for (int e = tid; e < HK * HBp; e += RG_THREADS) {
-    const int hp = e / HBp, h = e % HBp;
-    double val = 0.0;
-    if (h < HB) {
-      int t, u, v, t2, u2, v2;
-      unpack(h, t, u, v);
-      unpack(hp, t2, u2, v2);
-      val = pref * R[hidx(t + t2, u + u2, v + v2)];
-    }
-    Rm[e] = val;
-  }
-  __syncthreads();
+  __syncthreads();  // H is complete; the bra scratch (Eb, fa) is free
 
-  // ---- ket chunks
+  // ---- the block's kets, one at a time
 #pragma unroll 1
-  for (int cd0 = 0; cd0 < ncd; cd0 += CH) {
-    const int nch = min(CH, ncd - cd0);
-    // K[h'][(cdl, b)]
-    for (int e = tid; e < HK * CRp; e += RG_THREADS) {
-      const int hp = e / CRp, r = e % CRp, cdl = r / NB, b = r % NB;
-      double val = 0.0;
-      if (cdl < nch) {
-        const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
-        const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
-        const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
-        int t, u, v;
-        unpack(hp, t, u, v);
-        const double* f0 = fk + (size_t)cd * 12 * FLk;
-        if (TYPE == 1) {
-          if (t <= ci[0] + di[0] && u <= ci[1] + di[1] && v <= ci[2] + di[2])
-            val = f0[(0 * 4) * FLk + t] * f0[(1 * 4) * FLk + u] * f0[(2 * 4) * FLk + v];
-        } else {
-          for (int kk = 0; kk < 3; kk++)
-            for (int ll = 0; ll < 3; ll++) {
-              int o2;
-              double sg;
-              op_of(kk, ll, o2, sg);
-              if (o2 != b) continue;
-              const int tx = (kk == 0) | ((ll == 0) << 1), ty = (kk == 1) | ((ll == 1) << 1),
-                        tz = (kk == 2) | ((ll == 2) << 1);
-              if (t >= ci[0] + di[0] + (tx & 1) + (tx >> 1) + 1 ||
-                  u >= ci[1] + di[1] + (ty & 1) + (ty >> 1) + 1 ||
-                  v >= ci[2] + di[2] + (tz & 1) + (tz >> 1) + 1)
-                continue;
-              val += sg * f0[(0 * 4 + tx) * FLk + t] * f0[(1 * 4 + ty) * FLk + u] *
-                     f0[(2 * 4 + tz) * FLk + v];
-            }
-        }
-      }
-      Ks[e] = val;
-    }
-    __syncthreads();
-    // G = K^T Rm, 4 x 4 tiles (rows of K, columns h)
+  for (int jk = tile * RG_KT; jk < jkEnd; jk++) {
+    const PairDev Q = a.pairs[a.ketBeg + jk];
+    if (Q.npp != 1) continue;  // contracted: the block kernels (block-uniform)
+    bool work, mine;
     {
-      const int tr = CRp / 4, th = HBp / 4;
-      for (int unit = tid; unit < tr * th; unit += RG_THREADS) {
-        const int r0 = (unit % tr) * 4, h0 = (unit / tr) * 4;
-        double acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-#pragma unroll 2
-        for (int hp = 0; hp < HK; hp++) {
-          const double2 k01 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0);
-          const double2 k23 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0 + 2);
-          const double2 m01 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0);
-          const double2 m23 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0 + 2);
-          const double kv[4] = {k01.x, k01.y, k23.x, k23.y};
-          const double mv[4] = {m01.x, m01.y, m23.x, m23.y};
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = fma(kv[i], mv[j], acc[i][j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          double2* g = reinterpret_cast<double2*>(Gs + (size_t)(h0 + j) * CRp + r0);
-          g[0] = make_double2(acc[0][j], acc[1][j]);
-          g[1] = make_double2(acc[2][j], acc[3][j]);
-        }
-      }
-    }
-    __syncthreads();
-    // M = H^T G, one 4 x 4 tile per unit, digested from registers
-    {
-      const int ngrp = (TYPE == 2) ? nch : (nch + 3) / 4;
-      for (int unit = tid; unit < nab * ngrp; unit += RG_THREADS) {
-        const int ab = unit % nab, grp = unit / nab;
-        const int col0 = (TYPE == 2) ? grp * 4 : grp * 4;  // first column of the tile
-        double acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-#pragma unroll 2
-        for (int h = 0; h < HB; h++) {
-          const double2 h01 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4);
-          const double2 h23 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4 + 2);
-          const double2 g01 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0);
-          const double2 g23 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0 + 2);
-          const double hv[4] = {h01.x, h01.y, h23.x, h23.y};
-          const double gv[4] = {g01.x, g01.y, g23.x, g23.y};
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = fma(hv[i], gv[j], acc[i][j]);
-        }
-        const int ai = ab / nb, bi = ab % nb;
-        auto column = [&](int cdl) {
-          const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
-          const int gC = Q.cA + c, gD = Q.cB + d;
-          RelCol col{gC, gD, dAB, dCD, samePQ, dCD ? 1.0 : 2.0, w12, samePQ ? 0.5 : 1.0, 0.0,
-                     {0, 0, 0, 0}};
-          if (TYPE == 1) {
-            col.rhoLL = __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc));
-          } else {
-            const size_t eDC = (size_t)gD + (size_t)gC * nc;
-            col.rvDC[0] = __ldg(a.Xss[0] + 2 * eDC);
-            col.rvDC[1] = -__ldg(a.Xss[1] + 2 * eDC + 1);
-            col.rvDC[2] = -__ldg(a.Xss[2] + 2 * eDC + 1);
-            col.rvDC[3] = -__ldg(a.Xss[3] + 2 * eDC + 1);
-          }
-          return col;
-        };
-        if (TYPE == 2) {
-          double m[16];
-#pragma unroll
-          for (int op = 0; op < 4; op++)
-#pragma unroll
-            for (int b = 0; b < 4; b++) m[op * 4 + b] = acc[op][b];
-          double jl[4] = {0.0, 0.0, 0.0, 0.0};
-          rel_digest<TYPE>(a, P, column(grp), ai, bi, m, jl);
-#pragma unroll
-          for (int b = 0; b < 4; b++)
-            if (jl[b] != 0.0) atomicAdd(Js + grp * 4 + b, jl[b]);
-        } else {
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const int cdl = grp * 4 + k;
-            if (cdl >= nch) break;
-            double m[4] = {acc[0][k], acc[1][k], acc[2][k], acc[3][k]};
-            double jl[4] = {0.0, 0.0, 0.0, 0.0};
-            rel_digest<TYPE>(a, P, column(cdl), ai, bi, m, jl);
-            if (jl[0] != 0.0) atomicAdd(Js + cdl * 4, jl[0]);
-          }
-        }
-      }
-    }
-    __syncthreads();
-    // per-column Coulomb flush (as the block kernels)
-    for (int cdl = tid; cdl < nch; cdl += RG_THREADS) {
-      const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
-      const size_t eCD = (size_t)(Q.cA + c) + (size_t)(Q.cB + d) * nc;
+      int s1, s2, s3, s4;
+      double q12, q34;
       if (TYPE == 1) {
-        if (Js[cdl * 4] != 0.0) atomicAdd(a.Jll + eCD, w34 * s12d * Js[cdl * 4]);
-      } else if (!samePQ) {
-        for (int b = 0; b < 4; b++)
-          if (Js[cdl * 4 + b] != 0.0) atomicAdd(a.Jss[b] + eCD, w34 * s12d * Js[cdl * 4 + b]);
+        s1 = P.s1; s2 = P.s2; s3 = Q.s1; s4 = Q.s2;
+        q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+        q34 = __ldg(a.qLL + s3 + (size_t)s4 * ns);
+      } else {
+        const bool pRef = P.lex >= Q.lex;
+        const PairDev& R12 = pRef ? P : Q;
+        const PairDev& R34 = pRef ? Q : P;
+        s1 = R12.s1; s2 = R12.s2; s3 = R34.s1; s4 = R34.s2;
+        q12 = __ldg(a.qSS + s1 + (size_t)s2 * ns);
+        q34 = __ldg(a.qSS + s3 + (size_t)s4 * ns);
       }
-      for (int b = 0; b < 4; b++) Js[cdl * 4 + b] = 0.0;
+      const double bound = sh_max(a.norms, s1, s2, s3, s4, ns) * q12 * q34;
+      work = !a.screen || bound >= a.thresh;
+      const bool lo = a.mixed && bound < a.cut &&
+                      fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                                    __ldg(a.pairRange + a.ketBeg + jk),
+                                    la + lb + lc + ld + 2 + 2 * (TYPE == 2), 1, TYPE == 2);
+      mine = work && !lo;
+    }
+    if (tid == 0) {
+      atomicAdd(a.counters + 0, 1ull);
+      if (!work) atomicAdd(a.counters + 1, 1ull);
+      if (mine) atomicAdd(a.counters + 3, 1ull);
+    }
+    if (!mine) continue;  // block-uniform
+    const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+    const bool dCD = Q.shA == Q.shB, samePQ = P.lex == Q.lex;
+    const double w34 = dCD ? 0.5 : 1.0;
+    const PrimPairDev& B = a.pp[Q.pp_off];
+    double ec, ed;
+    pair_exps(SC, SD, a.prim, B, ec, ed);
+    const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
+    const double pq = A.p + B.p, alpha = A.p * B.p / pq;
+    const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+    // R in warp 0 (warp syncs only); the ket E tables beside it
+    if (tid < 32) {
+      if (tid == 0) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+      __syncwarp();
+      const double m2a = -2.0 * alpha;
+      for (int n = L; n >= 0; n--) {
+        double* cur = Rb[n & 1];
+        const double* prv = Rb[(n + 1) & 1];
+        const int cnt = nherm(L - n);
+        for (int e = tid; e < cnt; e += 32) {
+          int t, u, v;
+          unpack(e, t, u, v);
+          double val;
+          if (e == 0) {
+            double f = 1.0;
+            for (int k = 0; k < n; k++) f *= m2a;
+            val = f * Fs[n];
+          } else if (t > 0) {
+            val = X * prv[hidx(t - 1, u, v)];
+            if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+          } else if (u > 0) {
+            val = Y * prv[hidx(0, u - 1, v)];
+            if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+          } else {
+            val = Z * prv[hidx(0, 0, v - 1)];
+            if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+          }
+          cur[e] = val;
+        }
+        __syncwarp();
+      }
+    } else if (tid < 35) {
+      hermite_E_rt<double, LMAX + 1>(lc + dK, ld + dK, B.o2p, B.PA[tid - 32], B.PB[tid - 32],
+                                     Ek + (tid - 32) * E1k);
     }
     __syncthreads();
-  }
+    const double* R = Rb[0];
+    for (int it = tid; it < ncd * 12; it += RG_THREADS) {
+      const int cd = it / 12, x = (it % 12) / 4, ty = it % 4;
+      if (TYPE == 1 && ty) continue;
+      const int c = cd / nd, d = cd % nd;
+      const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
+      const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
+      double* f = fk + (size_t)it * FLk;
+      const int n = axis_factor<double>(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
+                                        2.0 * ec, 2.0 * ed, f);
+      for (int t = 1; t < n; t += 2) f[t] = -f[t];
+    }
+    for (int e = tid; e < HK * HBp; e += RG_THREADS) {
+      const int hp = e / HBp, h = e % HBp;
+      double val = 0.0;
+      if (h < HB) {
+        int t, u, v, t2, u2, v2;
+        unpack(h, t, u, v);
+        unpack(hp, t2, u2, v2);
+        val = pref * R[hidx(t + t2, u + u2, v + v2)];
+      }
+      Rm[e] = val;
+    }
+    __syncthreads();  // fk and Rm are complete; the per-ket scratch is free
+
+    // ---- ket chunks
+  #pragma unroll 1
+    for (int cd0 = 0; cd0 < ncd; cd0 += CH) {
+      const int nch = min(CH, ncd - cd0);
+      // K[h'][(cdl, b)]
+      for (int e = tid; e < HK * CRp; e += RG_THREADS) {
+        const int hp = e / CRp, r = e % CRp, cdl = r / NB, b = r % NB;
+        double val = 0.0;
+        if (cdl < nch) {
+          const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
+          const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
+          const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
+          int t, u, v;
+          unpack(hp, t, u, v);
+          const double* f0 = fk + (size_t)cd * 12 * FLk;
+          if (TYPE == 1) {
+            if (t <= ci[0] + di[0] && u <= ci[1] + di[1] && v <= ci[2] + di[2])
+              val = f0[(0 * 4) * FLk + t] * f0[(1 * 4) * FLk + u] * f0[(2 * 4) * FLk + v];
+          } else {
+            for (int kk = 0; kk < 3; kk++)
+              for (int ll = 0; ll < 3; ll++) {
+                int o2;
+                double sg;
+                op_of(kk, ll, o2, sg);
+                if (o2 != b) continue;
+                const int tx = (kk == 0) | ((ll == 0) << 1), ty = (kk == 1) | ((ll == 1) << 1),
+                          tz = (kk == 2) | ((ll == 2) << 1);
+                if (t >= ci[0] + di[0] + (tx & 1) + (tx >> 1) + 1 ||
+                    u >= ci[1] + di[1] + (ty & 1) + (ty >> 1) + 1 ||
+                    v >= ci[2] + di[2] + (tz & 1) + (tz >> 1) + 1)
+                  continue;
+                val += sg * f0[(0 * 4 + tx) * FLk + t] * f0[(1 * 4 + ty) * FLk + u] *
+                       f0[(2 * 4 + tz) * FLk + v];
+              }
+          }
+        }
+        Ks[e] = val;
+      }
+      __syncthreads();
+      // G = K^T Rm, 4 x 4 tiles (rows of K, columns h)
+      {
+        const int tr = CRp / 4, th = HBp / 4;
+        for (int unit = tid; unit < tr * th; unit += RG_THREADS) {
+          const int r0 = (unit % tr) * 4, h0 = (unit / tr) * 4;
+          double acc[4][4];
+  #pragma unroll
+          for (int i = 0; i < 4; i++)
+  #pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  #pragma unroll 2
+          for (int hp = 0; hp < HK; hp++) {
+            const double2 k01 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0);
+            const double2 k23 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0 + 2);
+            const double2 m01 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0);
+            const double2 m23 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0 + 2);
+            const double kv[4] = {k01.x, k01.y, k23.x, k23.y};
+            const double mv[4] = {m01.x, m01.y, m23.x, m23.y};
+  #pragma unroll
+            for (int i = 0; i < 4; i++)
+  #pragma unroll
+              for (int j = 0; j < 4; j++) acc[i][j] = fma(kv[i], mv[j], acc[i][j]);
+          }
+  #pragma unroll
+          for (int j = 0; j < 4; j++) {
+            double2* g = reinterpret_cast<double2*>(Gs + (size_t)(h0 + j) * CRp + r0);
+            g[0] = make_double2(acc[0][j], acc[1][j]);
+            g[1] = make_double2(acc[2][j], acc[3][j]);
+          }
+        }
+      }
+      __syncthreads();
+      // M = H^T G, one 4 x 4 tile per unit, digested from registers
+      {
+        const int ngrp = (TYPE == 2) ? nch : (nch + 3) / 4;
+        for (int unit = tid; unit < nab * ngrp; unit += RG_THREADS) {
+          const int ab = unit % nab, grp = unit / nab;
+          const int col0 = (TYPE == 2) ? grp * 4 : grp * 4;  // first column of the tile
+          double acc[4][4];
+  #pragma unroll
+          for (int i = 0; i < 4; i++)
+  #pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  #pragma unroll 2
+          for (int h = 0; h < HB; h++) {
+            const double2 h01 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4);
+            const double2 h23 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4 + 2);
+            const double2 g01 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0);
+            const double2 g23 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0 + 2);
+            const double hv[4] = {h01.x, h01.y, h23.x, h23.y};
+            const double gv[4] = {g01.x, g01.y, g23.x, g23.y};
+  #pragma unroll
+            for (int i = 0; i < 4; i++)
+  #pragma unroll
+              for (int j = 0; j < 4; j++) acc[i][j] = fma(hv[i], gv[j], acc[i][j]);
+          }
+          const int ai = ab / nb, bi = ab % nb;
+          auto column = [&](int cdl) {
+            const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
+            const int gC = Q.cA + c, gD = Q.cB + d;
+            RelCol col{gC, gD, dAB, dCD, samePQ, dCD ? 1.0 : 2.0, w12, samePQ ? 0.5 : 1.0, 0.0,
+                       {0, 0, 0, 0}};
+            if (TYPE == 1) {
+              col.rhoLL = __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc));
+            } else {
+              const size_t eDC = (size_t)gD + (size_t)gC * nc;
+              col.rvDC[0] = __ldg(a.Xss[0] + 2 * eDC);
+              col.rvDC[1] = -__ldg(a.Xss[1] + 2 * eDC + 1);
+              col.rvDC[2] = -__ldg(a.Xss[2] + 2 * eDC + 1);
+              col.rvDC[3] = -__ldg(a.Xss[3] + 2 * eDC + 1);
+            }
+            return col;
+          };
+          if (TYPE == 2) {
+            double m[16];
+  #pragma unroll
+            for (int op = 0; op < 4; op++)
+  #pragma unroll
+              for (int b = 0; b < 4; b++) m[op * 4 + b] = acc[op][b];
+            double jl[4] = {0.0, 0.0, 0.0, 0.0};
+            rel_digest<TYPE>(a, P, column(grp), ai, bi, m, jl);
+  #pragma unroll
+            for (int b = 0; b < 4; b++)
+              if (jl[b] != 0.0) atomicAdd(Js + grp * 4 + b, jl[b]);
+          } else {
+  #pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const int cdl = grp * 4 + k;
+              if (cdl >= nch) break;
+              double m[4] = {acc[0][k], acc[1][k], acc[2][k], acc[3][k]};
+              double jl[4] = {0.0, 0.0, 0.0, 0.0};
+              rel_digest<TYPE>(a, P, column(cdl), ai, bi, m, jl);
+              if (jl[0] != 0.0) atomicAdd(Js + cdl * 4, jl[0]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      // per-column Coulomb flush (as the block kernels)
+      for (int cdl = tid; cdl < nch; cdl += RG_THREADS) {
+        const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
+        const size_t eCD = (size_t)(Q.cA + c) + (size_t)(Q.cB + d) * nc;
+        if (TYPE == 1) {
+          if (Js[cdl * 4] != 0.0) atomicAdd(a.Jll + eCD, w34 * s12d * Js[cdl * 4]);
+        } else if (!samePQ) {
+          for (int b = 0; b < 4; b++)
+            if (Js[cdl * 4 + b] != 0.0) atomicAdd(a.Jss[b] + eCD, w34 * s12d * Js[cdl * 4 + b]);
+        }
+        for (int b = 0; b < 4; b++) Js[cdl * 4 + b] = 0.0;
+      }
+      __syncthreads();
+    }
+  }  // kets
 }
 
 // Dynamic shared-memory limit of the block kernels (the largest layout, SSSS
@@ -1456,17 +1472,16 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
     // single-primitive SSSS quartets of the d and f classes: the GEMM form,
     // when its layout fits; the other kernels skip them.  (LLSS quartets are
     // lighter -- one ket operator -- and the LLSS block kernel, with every
-    // ket component pair's Hermite sums built at once, measured faster:
-    // one Ag atom 0.68 s in the GEMM form against 0.43 s.)
+    // ket component pair's Hermite sums built at once, measured faster: one
+    // Ag atom 0.40 s in the GEMM form against 0.27 s.)
     const int CH = rel_gemm_chunk(la, lb, lc, ld, TYPE);
     if (CH > 0) {
       const size_t smem = (size_t)rel_gemm_layout(la, lb, lc, ld, TYPE, CH).total * sizeof(double);
       cudaFuncSetAttribute(rel_gemm_kernel<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)RG_SMEM_MAX);
-      const long long nq = (TYPE == 2 && a.same) ? (long long)a.nBra * (a.nBra + 1) / 2
-                                                 : (long long)a.nBra * a.nKet;
-      const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
-      const unsigned gy = (unsigned)((nq + gx - 1) / gx);
+      const long long nb = (long long)a.nBra * ((a.nKet + RG_KT - 1) / RG_KT);
+      const unsigned gx = (unsigned)std::min<long long>(nb, 65535);
+      const unsigned gy = (unsigned)((nb + gx - 1) / gx);
       rel_gemm_kernel<TYPE><<<dim3(gx, gy), RG_THREADS, smem, st>>>(a, la, lb, lc, ld, CH);
       a.skipSingle = 1;
     }
