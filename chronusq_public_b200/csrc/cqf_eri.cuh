@@ -122,11 +122,17 @@ __device__ __forceinline__ void boys_rt<float>(int L, float T, float* F, const f
 #pragma unroll 1
     for (int m = L - 1; m >= 0; m--) F[m] = (t2 * F[m + 1] + e) / (2 * m + 1);
   } else {
-    float rT = rsqrtf(T);
-    F[0] = 0.886226925f * rT;
-    float e = __expf(-T), h = 0.5f * rT * rT;
+    // large arguments in FP64, as boys_f32 does: sqrt(pi / T) / 2 and the
+    // upward recursion, with e^-T from the FP32 exponential (below 2e-16 here)
+    const double Td = (double)T, rT = rsqrt(Td), h = 0.5 * rT * rT;
+    const double e = (double)__expf(-T);
+    double f = 0.88622692545275801365 * rT;
+    F[0] = (float)f;
 #pragma unroll 1
-    for (int m = 0; m < L; m++) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    for (int m = 0; m < L; m++) {
+      f = ((2 * m + 1) * f - e) * h;
+      F[m + 1] = (float)f;
+    }
   }
 }
 

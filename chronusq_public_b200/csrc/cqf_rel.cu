@@ -1045,8 +1045,9 @@ struct RelGemmLayout {
   int total;
 };
 __host__ __device__ inline int rg_round(int n, int m) { return (n + m - 1) / m * m; }
+// offsets and total in elements of esz bytes (8: FP64, 4: FP32 arithmetic)
 __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc, int ld, int type,
-                                                         int CH) {
+                                                         int CH, int esz) {
   const int dK = type == 2 ? 1 : 0, NB = type == 2 ? 4 : 1;
   const int Lb = la + lb + 2, Lk = lc + ld + 2 * dK, L = Lb + Lk;
   const int nab = ncart(la) * ncart(lb), ncd = ncart(lc) * ncart(ld);
@@ -1061,25 +1062,25 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   Lo.CRp = rg_round(Lo.CR, 4);
   Lo.NT = nherm(L);
   int o = 0;
-  auto take = [&](int n) { int r = o; o += rg_round(n, 2); return r; };
+  auto take = [&](int n) { int r = o; o += rg_round(n, 4); return r; };
   Lo.oH = take(Lo.HB * Lo.HR);
   Lo.oRm = take(Lo.HK * Lo.HBp);
   Lo.oFk = take(ncd * 12 * FLk);
-  Lo.oJs = take(CH * 4);
-  Lo.oTuv = take((Lo.NT + 1) / 2);  // packed (t, u, v) of each Hermite index, as int
+  Lo.oJs = take(CH * 4 * 8 / esz);           // per-column Coulomb sums, double
+  Lo.oTuv = take((Lo.NT * 4 + esz - 1) / esz);  // packed (t, u, v) of each Hermite index, int
   Lo.oScr = o;
   int p = o;
-  auto takeB = [&](int n) { int r = p; p += rg_round(n, 2); return r; };
+  auto takeB = [&](int n) { int r = p; p += rg_round(n, 4); return r; };
   Lo.oEb = takeB(3 * (la + 2) * (lb + 2) * (la + lb + 3));
   Lo.oFa = takeB(nab * 12 * FL);
   int k = o;
-  auto takeK = [&](int n) { int r = k; k += rg_round(n, 2); return r; };
+  auto takeK = [&](int n) { int r = k; k += rg_round(n, 4); return r; };
   Lo.oEk = takeK(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
   Lo.oR0 = takeK(nherm(L));
   Lo.oR1 = takeK(nherm(L));
   Lo.oF = takeK(L + 1);
   int q = o;
-  auto takeC = [&](int n) { int r = q; q += rg_round(n, 2); return r; };
+  auto takeC = [&](int n) { int r = q; q += rg_round(n, 4); return r; };
   Lo.oK = takeC(Lo.HK * Lo.CRp);
   Lo.oG = takeC(Lo.HBp * Lo.CRp);
   Lo.total = p > k ? p : k;
@@ -1087,20 +1088,41 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   return Lo;
 }
 // the largest ket chunk whose layout fits (0: the class does not fit)
-inline int rel_gemm_chunk(int la, int lb, int lc, int ld, int type) {
+inline int rel_gemm_chunk(int la, int lb, int lc, int ld, int type, int esz) {
   const int ncd = ncart(lc) * ncart(ld);
   for (int ch = ncd; ch >= 1; ch--)
-    if ((size_t)rel_gemm_layout(la, lb, lc, ld, type, ch).total * sizeof(double) <= RG_SMEM_MAX)
+    if ((size_t)rel_gemm_layout(la, lb, lc, ld, type, ch, esz).total * esz <= RG_SMEM_MAX)
       return ch;
   return 0;
+}
+// four consecutive elements (16-byte aligned)
+__device__ __forceinline__ void rg_ld4(const double* p, double (&v)[4]) {
+  const double2 a = *reinterpret_cast<const double2*>(p);
+  const double2 b = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void rg_ld4(const float* p, float (&v)[4]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void rg_st4(double* p, double a, double b, double c, double d) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+  reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+}
+__device__ __forceinline__ void rg_st4(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
 }
 // ket pairs per block
 constexpr int RG_KT = 8;
 
-template <int TYPE>
+// T: primitive arithmetic (double; float for the small-bound quartets of a
+// mixed launch); the operator components are digested in FP64.
+template <int TYPE, typename T>
 __global__ void __launch_bounds__(RG_THREADS, 2)
     rel_gemm_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int CH) {
+  constexpr bool IS32 = sizeof(T) == 4;
   extern __shared__ double sm[];
+  T* smT = reinterpret_cast<T*>(sm);
   const int nTiles = (a.nKet + RG_KT - 1) / RG_KT;
   const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   const int ib = (int)(q / nTiles), tile = (int)(q % nTiles);
@@ -1119,20 +1141,21 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
   const int dK = (TYPE == 2) ? 1 : 0;
   const int Lb = la + lb + 2, Lk = lc + ld + 2 * dK, L = Lb + Lk;
   const int FL = 2 * max(la, lb) + 3, FLk = 2 * max(lc, ld) + 3;
-  const RelGemmLayout Lo = rel_gemm_layout(la, lb, lc, ld, TYPE, CH);
+  const RelGemmLayout Lo = rel_gemm_layout(la, lb, lc, ld, TYPE, CH, (int)sizeof(T));
   const int HB = Lo.HB, HBp = Lo.HBp, HK = Lo.HK, HR = Lo.HR, CRp = Lo.CRp;
-  double* Hs = sm + Lo.oH;
-  double* Rm = sm + Lo.oRm;
-  double* fk = sm + Lo.oFk;
-  double* Js = sm + Lo.oJs;
-  int* tuv = reinterpret_cast<int*>(sm + Lo.oTuv);
-  double* Eb = sm + Lo.oEb;
-  double* fa = sm + Lo.oFa;
-  double* Ek = sm + Lo.oEk;
-  double* Rb[2] = {sm + Lo.oR0, sm + Lo.oR1};
-  double* Fs = sm + Lo.oF;
-  double* Ks = sm + Lo.oK;
-  double* Gs = sm + Lo.oG;
+  T* Hs = smT + Lo.oH;
+  T* Rm = smT + Lo.oRm;
+  T* fk = smT + Lo.oFk;
+  double* Js = reinterpret_cast<double*>(smT + Lo.oJs);
+  int* tuv = reinterpret_cast<int*>(smT + Lo.oTuv);
+  T* Eb = smT + Lo.oEb;
+  T* fa = smT + Lo.oFa;
+  T* Ek = smT + Lo.oEk;
+  T* Rb[2] = {smT + Lo.oR0, smT + Lo.oR1};
+  T* Fs = smT + Lo.oF;
+  T* Ks = smT + Lo.oK;
+  T* Gs = smT + Lo.oG;
+  const T* boysT = reinterpret_cast<const T*>(IS32 ? (const void*)a.boys32 : (const void*)a.boys);
   const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
   const int E1k = (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK);
   const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
@@ -1152,7 +1175,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
   double ea, eb;
   pair_exps(SA, SB, a.prim, A, ea, eb);
   if (tid < 3)
-    hermite_E_rt<double, LMAX + 1>(la + 1, lb + 1, A.o2p, A.PA[tid], A.PB[tid], Eb + tid * E1b);
+    hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
+                              Eb + tid * E1b);
   for (int h = tid; h < Lo.NT; h += RG_THREADS) {
     int t, u, v;
     hinv(h, t, u, v);
@@ -1165,8 +1189,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     const int ai = ab / nb, bi = ab % nb;
     const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
     const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
-    axis_factor<double>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, 2.0 * ea, 2.0 * eb,
-                        fa + (size_t)it * FL);
+    axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
+                   fa + (size_t)it * FL);
   }
   __syncthreads();
   for (int e = tid; e < HB * HR; e += RG_THREADS) {
@@ -1176,7 +1200,7 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     unpack(h, t, u, v);
     const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
     const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
-    double val = 0.0;
+    T val = T(0);
     for (int mu = 0; mu < 3; mu++)
       for (int nu = 0; nu < 3; nu++) {
         int o2;
@@ -1189,7 +1213,7 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
             u >= ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1 ||
             v >= ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1)
           continue;
-        val += sg * fa[((size_t)ab * 12 + 0 * 4 + tx) * FL + t] *
+        val += T(sg) * fa[((size_t)ab * 12 + 0 * 4 + tx) * FL + t] *
                fa[((size_t)ab * 12 + 1 * 4 + ty) * FL + u] *
                fa[((size_t)ab * 12 + 2 * 4 + tz) * FL + v];
       }
@@ -1224,12 +1248,12 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
                       fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
                                     __ldg(a.pairRange + a.ketBeg + jk),
                                     la + lb + lc + ld + 2 + 2 * (TYPE == 2), 1, TYPE == 2);
-      mine = work && !lo;
+      mine = work && (IS32 ? lo : !lo);
     }
     if (tid == 0) {
-      atomicAdd(a.counters + 0, 1ull);
-      if (!work) atomicAdd(a.counters + 1, 1ull);
-      if (mine) atomicAdd(a.counters + 3, 1ull);
+      if (!IS32) atomicAdd(a.counters + 0, 1ull);
+      if (!IS32 && !work) atomicAdd(a.counters + 1, 1ull);
+      if (mine) atomicAdd(a.counters + (IS32 ? 2 : 3), 1ull);
     }
     if (!mine) continue;  // block-uniform
     const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
@@ -1238,60 +1262,60 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     const PrimPairDev& B = a.pp[Q.pp_off];
     double ec, ed;
     pair_exps(SC, SD, a.prim, B, ec, ed);
-    const double X = A.P[0] - B.P[0], Y = A.P[1] - B.P[1], Z = A.P[2] - B.P[2];
-    const double pq = A.p + B.p, alpha = A.p * B.p / pq;
-    const double pref = PI52X2 / sqrt(pq) * A.Kp * B.Kp;
+    const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
+    const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
+    const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
     // R in warp 0 (warp syncs only); the ket E tables beside it
     if (tid < 32) {
-      if (tid == 0) boys_rt<double>(L, alpha * (X * X + Y * Y + Z * Z), Fs, a.boys);
+      if (tid == 0) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
       __syncwarp();
-      const double m2a = -2.0 * alpha;
+      const T m2a = T(-2) * alpha;
       for (int n = L; n >= 0; n--) {
-        double* cur = Rb[n & 1];
-        const double* prv = Rb[(n + 1) & 1];
+        T* cur = Rb[n & 1];
+        const T* prv = Rb[(n + 1) & 1];
         const int cnt = nherm(L - n);
         for (int e = tid; e < cnt; e += 32) {
           int t, u, v;
           unpack(e, t, u, v);
-          double val;
+          T val;
           if (e == 0) {
-            double f = 1.0;
+            T f = T(1);
             for (int k = 0; k < n; k++) f *= m2a;
             val = f * Fs[n];
           } else if (t > 0) {
             val = X * prv[hidx(t - 1, u, v)];
-            if (t > 1) val += (t - 1) * prv[hidx(t - 2, u, v)];
+            if (t > 1) val += T(t - 1) * prv[hidx(t - 2, u, v)];
           } else if (u > 0) {
             val = Y * prv[hidx(0, u - 1, v)];
-            if (u > 1) val += (u - 1) * prv[hidx(0, u - 2, v)];
+            if (u > 1) val += T(u - 1) * prv[hidx(0, u - 2, v)];
           } else {
             val = Z * prv[hidx(0, 0, v - 1)];
-            if (v > 1) val += (v - 1) * prv[hidx(0, 0, v - 2)];
+            if (v > 1) val += T(v - 1) * prv[hidx(0, 0, v - 2)];
           }
           cur[e] = val;
         }
         __syncwarp();
       }
     } else if (tid < 35) {
-      hermite_E_rt<double, LMAX + 1>(lc + dK, ld + dK, B.o2p, B.PA[tid - 32], B.PB[tid - 32],
-                                     Ek + (tid - 32) * E1k);
+      hermite_E_rt<T, LMAX + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[tid - 32]),
+                                T(B.PB[tid - 32]), Ek + (tid - 32) * E1k);
     }
     __syncthreads();
-    const double* R = Rb[0];
+    const T* R = Rb[0];
     for (int it = tid; it < ncd * 12; it += RG_THREADS) {
       const int cd = it / 12, x = (it % 12) / 4, ty = it % 4;
       if (TYPE == 1 && ty) continue;
       const int c = cd / nd, d = cd % nd;
       const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
       const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
-      double* f = fk + (size_t)it * FLk;
-      const int n = axis_factor<double>(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
-                                        2.0 * ec, 2.0 * ed, f);
+      T* f = fk + (size_t)it * FLk;
+      const int n = axis_factor<T>(Ek + x * E1k, ld + dK, lc + ld + 2 * dK + 1, ci, di, ty,
+                                   T(2.0 * ec), T(2.0 * ed), f);
       for (int t = 1; t < n; t += 2) f[t] = -f[t];
     }
     for (int e = tid; e < HK * HBp; e += RG_THREADS) {
       const int hp = e / HBp, h = e % HBp;
-      double val = 0.0;
+      T val = T(0);
       if (h < HB) {
         int t, u, v, t2, u2, v2;
         unpack(h, t, u, v);
@@ -1303,20 +1327,20 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     __syncthreads();  // fk and Rm are complete; the per-ket scratch is free
 
     // ---- ket chunks
-  #pragma unroll 1
+#pragma unroll 1
     for (int cd0 = 0; cd0 < ncd; cd0 += CH) {
       const int nch = min(CH, ncd - cd0);
       // K[h'][(cdl, b)]
       for (int e = tid; e < HK * CRp; e += RG_THREADS) {
         const int hp = e / CRp, r = e % CRp, cdl = r / NB, b = r % NB;
-        double val = 0.0;
+        T val = T(0);
         if (cdl < nch) {
           const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
           const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
           const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
           int t, u, v;
           unpack(hp, t, u, v);
-          const double* f0 = fk + (size_t)cd * 12 * FLk;
+          const T* f0 = fk + (size_t)cd * 12 * FLk;
           if (TYPE == 1) {
             if (t <= ci[0] + di[0] && u <= ci[1] + di[1] && v <= ci[2] + di[2])
               val = f0[(0 * 4) * FLk + t] * f0[(1 * 4) * FLk + u] * f0[(2 * 4) * FLk + v];
@@ -1333,7 +1357,7 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
                     u >= ci[1] + di[1] + (ty & 1) + (ty >> 1) + 1 ||
                     v >= ci[2] + di[2] + (tz & 1) + (tz >> 1) + 1)
                   continue;
-                val += sg * f0[(0 * 4 + tx) * FLk + t] * f0[(1 * 4 + ty) * FLk + u] *
+                val += T(sg) * f0[(0 * 4 + tx) * FLk + t] * f0[(1 * 4 + ty) * FLk + u] *
                        f0[(2 * 4 + tz) * FLk + v];
               }
           }
@@ -1346,29 +1370,24 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
         const int tr = CRp / 4, th = HBp / 4;
         for (int unit = tid; unit < tr * th; unit += RG_THREADS) {
           const int r0 = (unit % tr) * 4, h0 = (unit / tr) * 4;
-          double acc[4][4];
-  #pragma unroll
+          T acc[4][4];
+#pragma unroll
           for (int i = 0; i < 4; i++)
-  #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-  #pragma unroll 2
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+#pragma unroll 2
           for (int hp = 0; hp < HK; hp++) {
-            const double2 k01 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0);
-            const double2 k23 = *reinterpret_cast<const double2*>(Ks + (size_t)hp * CRp + r0 + 2);
-            const double2 m01 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0);
-            const double2 m23 = *reinterpret_cast<const double2*>(Rm + (size_t)hp * HBp + h0 + 2);
-            const double kv[4] = {k01.x, k01.y, k23.x, k23.y};
-            const double mv[4] = {m01.x, m01.y, m23.x, m23.y};
-  #pragma unroll
+            T kv[4], mv[4];
+            rg_ld4(Ks + (size_t)hp * CRp + r0, kv);
+            rg_ld4(Rm + (size_t)hp * HBp + h0, mv);
+#pragma unroll
             for (int i = 0; i < 4; i++)
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 4; j++) acc[i][j] = fma(kv[i], mv[j], acc[i][j]);
           }
-  #pragma unroll
+#pragma unroll
           for (int j = 0; j < 4; j++) {
-            double2* g = reinterpret_cast<double2*>(Gs + (size_t)(h0 + j) * CRp + r0);
-            g[0] = make_double2(acc[0][j], acc[1][j]);
-            g[1] = make_double2(acc[2][j], acc[3][j]);
+            rg_st4(Gs + (size_t)(h0 + j) * CRp + r0, acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
           }
         }
       }
@@ -1379,22 +1398,19 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
         for (int unit = tid; unit < nab * ngrp; unit += RG_THREADS) {
           const int ab = unit % nab, grp = unit / nab;
           const int col0 = (TYPE == 2) ? grp * 4 : grp * 4;  // first column of the tile
-          double acc[4][4];
-  #pragma unroll
+          T acc[4][4];
+#pragma unroll
           for (int i = 0; i < 4; i++)
-  #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-  #pragma unroll 2
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = T(0);
+#pragma unroll 2
           for (int h = 0; h < HB; h++) {
-            const double2 h01 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4);
-            const double2 h23 = *reinterpret_cast<const double2*>(Hs + (size_t)h * HR + ab * 4 + 2);
-            const double2 g01 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0);
-            const double2 g23 = *reinterpret_cast<const double2*>(Gs + (size_t)h * CRp + col0 + 2);
-            const double hv[4] = {h01.x, h01.y, h23.x, h23.y};
-            const double gv[4] = {g01.x, g01.y, g23.x, g23.y};
-  #pragma unroll
+            T hv[4], gv[4];
+            rg_ld4(Hs + (size_t)h * HR + ab * 4, hv);
+            rg_ld4(Gs + (size_t)h * CRp + col0, gv);
+#pragma unroll
             for (int i = 0; i < 4; i++)
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 4; j++) acc[i][j] = fma(hv[i], gv[j], acc[i][j]);
           }
           const int ai = ab / nb, bi = ab % nb;
@@ -1416,21 +1432,22 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
           };
           if (TYPE == 2) {
             double m[16];
-  #pragma unroll
+#pragma unroll
             for (int op = 0; op < 4; op++)
-  #pragma unroll
-              for (int b = 0; b < 4; b++) m[op * 4 + b] = acc[op][b];
+#pragma unroll
+              for (int b = 0; b < 4; b++) m[op * 4 + b] = (double)acc[op][b];
             double jl[4] = {0.0, 0.0, 0.0, 0.0};
             rel_digest<TYPE>(a, P, column(grp), ai, bi, m, jl);
-  #pragma unroll
+#pragma unroll
             for (int b = 0; b < 4; b++)
               if (jl[b] != 0.0) atomicAdd(Js + grp * 4 + b, jl[b]);
           } else {
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < 4; k++) {
               const int cdl = grp * 4 + k;
               if (cdl >= nch) break;
-              double m[4] = {acc[0][k], acc[1][k], acc[2][k], acc[3][k]};
+              double m[4] = {(double)acc[0][k], (double)acc[1][k], (double)acc[2][k],
+                             (double)acc[3][k]};
               double jl[4] = {0.0, 0.0, 0.0, 0.0};
               rel_digest<TYPE>(a, P, column(cdl), ai, bi, m, jl);
               if (jl[0] != 0.0) atomicAdd(Js + cdl * 4, jl[0]);
@@ -1468,21 +1485,22 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
   RelLaunch a = aIn;
   a.skipSingle = 0;
   const int lmax = std::max(std::max(la, lb), std::max(lc, ld));
-  if (TYPE == 2 && sizeof(T) == 8 && lmax >= 2) {
+  if (TYPE == 2 && lmax >= 2) {
     // single-primitive SSSS quartets of the d and f classes: the GEMM form,
     // when its layout fits; the other kernels skip them.  (LLSS quartets are
     // lighter -- one ket operator -- and the LLSS block kernel, with every
     // ket component pair's Hermite sums built at once, measured faster: one
     // Ag atom 0.40 s in the GEMM form against 0.27 s.)
-    const int CH = rel_gemm_chunk(la, lb, lc, ld, TYPE);
+    const int esz = (int)sizeof(T);
+    const int CH = rel_gemm_chunk(la, lb, lc, ld, TYPE, esz);
     if (CH > 0) {
-      const size_t smem = (size_t)rel_gemm_layout(la, lb, lc, ld, TYPE, CH).total * sizeof(double);
-      cudaFuncSetAttribute(rel_gemm_kernel<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      const size_t smem = (size_t)rel_gemm_layout(la, lb, lc, ld, TYPE, CH, esz).total * esz;
+      cudaFuncSetAttribute(rel_gemm_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)RG_SMEM_MAX);
       const long long nb = (long long)a.nBra * ((a.nKet + RG_KT - 1) / RG_KT);
       const unsigned gx = (unsigned)std::min<long long>(nb, 65535);
       const unsigned gy = (unsigned)((nb + gx - 1) / gx);
-      rel_gemm_kernel<TYPE><<<dim3(gx, gy), RG_THREADS, smem, st>>>(a, la, lb, lc, ld, CH);
+      rel_gemm_kernel<TYPE, T><<<dim3(gx, gy), RG_THREADS, smem, st>>>(a, la, lb, lc, ld, CH);
       a.skipSingle = 1;
     }
   }
