@@ -1490,7 +1490,7 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
     // when its layout fits; the other kernels skip them.  (LLSS quartets are
     // lighter -- one ket operator -- and the LLSS block kernel, with every
     // ket component pair's Hermite sums built at once, measured faster: one
-    // Ag atom 0.40 s in the GEMM form against 0.27 s.)
+    // Ag atom 0.31 s in the GEMM form against 0.27 s.)
     const int esz = (int)sizeof(T);
     const int CH = rel_gemm_chunk(la, lb, lc, ld, TYPE, esz);
     if (CH > 0) {
