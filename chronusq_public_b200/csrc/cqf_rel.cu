@@ -1029,8 +1029,8 @@ __global__ void __launch_bounds__(RB_THREADS)
 // then digested from registers at the reference's update sites.  A block
 // takes one bra pair and a tile of up to KT ket pairs: the bra's E tables,
 // axis factors and H are built once and stay in shared memory while the
-// block walks its kets; per ket the R recursion runs in one warp (warp
-// syncs only) from a table of Hermite indices.  Same quartet set, screens
+// block walks its kets; per ket the R recursion runs over the block from a
+// table of Hermite indices.  Same quartet set, screens
 // and digestion as the block kernels, which keep the contracted quartets
 // (and the classes whose layout does not fit).
 constexpr int RG_THREADS = 256;
@@ -1265,16 +1265,20 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
     const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
     const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
-    // R in warp 0 (warp syncs only); the ket E tables beside it
-    if (tid < 32) {
-      if (tid == 0) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
-      __syncwarp();
+    // Boys (one thread) and the ket E tables, then R level by level over the
+    // block, indices from the table
+    if (tid == 0) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+    else if (tid >= 32 && tid < 35)
+      hermite_E_rt<T, LMAX + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[tid - 32]),
+                                T(B.PB[tid - 32]), Ek + (tid - 32) * E1k);
+    __syncthreads();
+    {
       const T m2a = T(-2) * alpha;
       for (int n = L; n >= 0; n--) {
         T* cur = Rb[n & 1];
         const T* prv = Rb[(n + 1) & 1];
         const int cnt = nherm(L - n);
-        for (int e = tid; e < cnt; e += 32) {
+        for (int e = tid; e < cnt; e += RG_THREADS) {
           int t, u, v;
           unpack(e, t, u, v);
           T val;
@@ -1294,13 +1298,9 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
           }
           cur[e] = val;
         }
-        __syncwarp();
+        __syncthreads();
       }
-    } else if (tid < 35) {
-      hermite_E_rt<T, LMAX + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[tid - 32]),
-                                T(B.PB[tid - 32]), Ek + (tid - 32) * E1k);
     }
-    __syncthreads();
     const T* R = Rb[0];
     for (int it = tid; it < ncd * 12; it += RG_THREADS) {
       const int cd = it / 12, x = (it % 12) / 4, ty = it % 4;
