@@ -253,6 +253,7 @@ class GTODirectTPIContraction:
         arr = (_cabi.CqfContraction * n)()
         keep = []
         writeback = []
+        conv = {}  # one column-major copy per source X (J and K share D)
         for i, c in enumerate(matList):
             if dev:
                 for t in (c.X, c.AX):
@@ -267,7 +268,9 @@ class GTODirectTPIContraction:
                 arr[i].AX = C.c_void_p(c.AX.data_ptr())
             else:
                 dt = np.complex128 if is_c else np.float64
-                X = np.asfortranarray(c.X, dtype=dt)
+                X = conv.get(id(c.X))
+                if X is None:
+                    X = conv[id(c.X)] = np.asfortranarray(c.X, dtype=dt)
                 if X.shape != (N, N):
                     raise ValueError("matrix shape must be (N, N)")
                 if not (isinstance(c.AX, np.ndarray) and c.AX.dtype == dt

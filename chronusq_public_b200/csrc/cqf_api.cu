@@ -809,6 +809,8 @@ void free_basis(cqf_basis* B) {
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->evFork) cudaEventDestroy(B->evFork);
+  for (cudaEvent_t e : B->evStage)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : B->tune_ev)
     if (e) cudaEventDestroy(e);
   for (int i = 0; i < NAUX; i++) {
@@ -927,6 +929,7 @@ cqf_status basis_create(const cqf_shell* shells, int nshell, double thresh, int 
   CQF_CUDA(cudaEventCreate(&B->ev0));
   CQF_CUDA(cudaEventCreate(&B->ev1));
   CQF_CUDA(cudaEventCreateWithFlags(&B->evFork, cudaEventDisableTiming));
+  for (cudaEvent_t& e : B->evStage) CQF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (int i = 0; i < NAUX; i++) {
     CQF_TRY(aux_stream(device, &B->aux[i]));
     CQF_CUDA(cudaEventCreateWithFlags(&B->evJoin[i], cudaEventDisableTiming));
@@ -1639,10 +1642,25 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
     if (host && pinned && !capture) {
       Xd[m] = ws + oX + m * matN;
       AXd[m] = ws + oAX + m * matN;
-      std::memcpy(pinned + m * matN, list[m].X, matN * sizeof(double));
-      CQF_CUDA(cudaMemcpyAsync((void*)Xd[m], pinned + m * matN, matN * sizeof(double),
-                               cudaMemcpyHostToDevice, st));
       CQF_CUDA(cudaMemsetAsync(AXd[m], 0, matN * sizeof(double), st));
+      // J and K of one density share X (formRawGDInBatches passes the same
+      // onePDM to both): one upload serves every entry with that pointer
+      int same = -1;
+      for (int k = 0; k < m && same < 0; k++)
+        if (list[k].X == list[m].X) same = k;
+      if (same >= 0) {
+        Xd[m] = Xd[same];
+        continue;
+      }
+      // in pieces: the host copy of one piece overlaps the upload of the last
+      const size_t piece = (matN + NSTAGE - 1) / NSTAGE;
+      for (size_t o = 0; o < matN; o += piece) {
+        const size_t n = std::min(piece, matN - o);
+        std::memcpy(pinned + m * matN + o, static_cast<const double*>(list[m].X) + o,
+                    n * sizeof(double));
+        CQF_CUDA(cudaMemcpyAsync((void*)(Xd[m] + o), pinned + m * matN + o, n * sizeof(double),
+                                 cudaMemcpyHostToDevice, st));
+      }
     } else if (host) {
       Xd[m] = ws + oX + m * matN;
       AXd[m] = ws + oAX + m * matN;
@@ -1782,22 +1800,42 @@ cqf_status contract_core(cqf_basis* B, const cqf_contraction* list, int nMat,
         B->d_ao2shell, B->d_sph, B->d_sphOff, AXd[m]);
   CQF_CUDA(cudaGetLastError());
   const bool staged = host && pinned && !capture;
-  if (host)
+  // staged downloads go in NSTAGE pieces over all matrices, an event after
+  // each, so that AX += G[X] on the host runs behind the transfer
+  const size_t allN = (size_t)nMat * matN, piece = (allN + NSTAGE - 1) / NSTAGE;
+  if (staged) {  // AXd[m] = ws + oAX + m matN: one contiguous range
+    int i = 0;
+    for (size_t o = 0; o < allN; o += piece, i++) {
+      CQF_CUDA(cudaMemcpyAsync(pinned + allN + o, ws + oAX + o,
+                               std::min(piece, allN - o) * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+      CQF_CUDA(cudaEventRecord(B->evStage[i], st));
+    }
+  } else if (host) {
     for (int m = 0; m < nMat; m++)
-      CQF_CUDA(cudaMemcpyAsync(staged ? pinned + (size_t)(nMat + m) * matN : list[m].AX, AXd[m],
-                               matN * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CQF_CUDA(cudaMemcpyAsync(list[m].AX, AXd[m], matN * sizeof(double), cudaMemcpyDeviceToHost,
+                               st));
+  }
   if (capture) return CQF_OK;
   CQF_CUDA(cudaEventRecord(B->ev1, st));
   unsigned long long cnt[4] = {0, 0, 0, 0};
   CQF_CUDA(cudaMemcpyAsync(cnt, B->d_counters, 4 * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, st));
-  CQF_CUDA(cudaStreamSynchronize(st));
-  if (staged)  // AX += G[X] on the host
-    for (int m = 0; m < nMat; m++) {
-      double* ax = static_cast<double*>(list[m].AX);
-      const double* g = pinned + (size_t)(nMat + m) * matN;
-      for (size_t i = 0; i < matN; i++) ax[i] += g[i];
+  if (staged) {  // AX += G[X] on the host, each piece once it has landed
+    int i = 0;
+    for (size_t o = 0; o < allN; o += piece, i++) {
+      CQF_CUDA(cudaEventSynchronize(B->evStage[i]));
+      const size_t end = std::min(o + piece, allN);
+      for (size_t e = o; e < end;) {
+        const size_t m = e / matN, off = e % matN, n = std::min(end - e, matN - off);
+        double* ax = static_cast<double*>(list[m].AX) + off;
+        const double* g = pinned + allN + e;
+        for (size_t k = 0; k < n; k++) ax[k] += g[k];
+        e += n;
+      }
     }
+  }
+  CQF_CUDA(cudaStreamSynchronize(st));
   if (stats) {
     stats->quartets_total = (long long)cnt[0];
     stats->quartets_screened = (long long)cnt[1];

@@ -26,6 +26,7 @@ constexpr int MAXMAT = 512;
 // Tile-interleaved ket primitive data: fields p, Kp, o2p, P[3], PA[3], PB[3],
 // Qp (primitive Schwarz bound) of KETT_TILE consecutive kets of a class.
 constexpr int NAUX = 2;           // auxiliary streams of the class-quartet launches
+constexpr int NSTAGE = 8;         // pieces of a host-pointer download (one event each)
 constexpr int KETT_NF = 13;
 constexpr int KETT_TILE = 128;
 constexpr int WTILE = 32;         // kets per mask word of the class kernels
@@ -229,6 +230,7 @@ struct cqf_basis {
   int* d_flags = nullptr;                // MAXMAT per-matrix flags
   std::vector<int> h_flags;              // host staging of the flags
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evStage[cqf::NSTAGE] = {};  // host-pointer downloads, piece by piece
   // class-quartet kernels are spread over the call's stream and these NAUX
   // (fork / join by events) so that each persistent launch's tail overlaps
   // the next one's start; the streams come from a per-device pool

@@ -72,19 +72,37 @@ class FockBuilder:
 
     def formRawGD(self, D, xHFX: float = 1.0, precision: str = "fp64",
                   fp32_cutoff: float = 0.0, increment: bool = False,
-                  J=None, K=None):
+                  J=None, K=None, G=None):
         """Returns (G, J, K).  With ``increment`` the J/K passed in are
         accumulated (the incremental dD build of formGD, impl.hpp:80-88);
         that build always runs in FP64 -- mixed precision applies to builds
         from the full density, whose FP32 errors do not accumulate over SCF
-        iterations the way the increments' would."""
+        iterations the way the increments' would.
+
+        J, K and G given as column-major N x N float64 arrays are the output
+        storage, as the reference writes into the SingleSlater's own
+        coulombMatrix / exchangeMatrix / twoeH (impl.hpp:131-137, :223-237):
+        outside ``increment`` they are zeroed in place, so an SCF loop that
+        passes the same arrays every iteration allocates nothing."""
         if increment:
             precision = "fp64"
         N = self.tpi.nbasis
-        if J is None or not increment:
-            J = np.zeros((N, N), order="F")
-        if K is None or not increment:
-            K = np.zeros((N, N), order="F")
+
+        def _out(A, keep):
+            if A is None:
+                return np.zeros((N, N), order="F")
+            if (not isinstance(A, np.ndarray) or A.shape != (N, N)
+                    or A.dtype != np.float64 or not A.flags.f_contiguous):
+                raise ValueError("formRawGD: outputs must be column-major "
+                                 "(N, N) float64 arrays")
+            if not keep:
+                A.fill(0.0)
+            return A
+
+        if increment and (J is None or K is None):
+            raise ValueError("formRawGD: increment accumulates into J and K")
+        J = _out(J, increment)
+        K = _out(K, increment)
         shard = _shard_of(self.group)
         if increment and shard[1] > 1:
             # the increments of every shard go into zeroed buffers; the sum
@@ -101,7 +119,15 @@ class FockBuilder:
             J0 += J
             K0 += K
             J, K = J0, K0
-        G = 2.0 * J - xHFX * K
+        if G is None:
+            G = 2.0 * J - xHFX * K
+        else:
+            G = _out(G, True)
+            np.multiply(J, 2.0, out=G)
+            if xHFX == 1.0:
+                np.subtract(G, K, out=G)
+            elif xHFX != 0.0:
+                G -= xHFX * K
         return G, J, K
 
     def formRawGDBatch(self, Ds: List[np.ndarray], xHFX: float = 1.0,

@@ -106,6 +106,32 @@ def test_accumulate_semantics():
     assert np.abs(J2 - 2 * J1).max() < 1e-12
 
 
+def test_output_buffers_and_increment():
+    """Caller-owned J/K/G are zeroed and reused (the reference writes into
+    the SingleSlater's matrices); an incremental build from dD accumulates
+    into them, FP64 even when mixed is asked for (formGD, impl.hpp:80-88)."""
+    basis, tpi, ob, D = _oracle_and_device("h2o_ccpvdz")
+    N = tpi.nbasis
+    fb = FockBuilder(tpi)
+    J, K, G = (np.full((N, N), 7.0, order="F") for _ in range(3))
+    G1, J1, K1 = fb.formRawGD(D, J=J, K=K, G=G)
+    assert G1 is G and J1 is J and K1 is K
+    Jo, Ko = ob.contract([D, D], [1, 1], [COULOMB, EXCHANGE])
+    assert np.abs(J - Jo).max() < FP64_TOL
+    assert np.abs(G - (2 * Jo - Ko)).max() < FP64_TOL
+    rng = np.random.default_rng(11)
+    X = rng.standard_normal((N, N))
+    dD = np.asfortranarray(1e-3 * (X + X.T))
+    fb.formRawGD(dD, J=J, K=K, G=G, increment=True, precision="mixed",
+                 fp32_cutoff=1.0)
+    Jo2, Ko2 = ob.contract([D + dD, D + dD], [1, 1], [COULOMB, EXCHANGE])
+    assert np.abs(J - Jo2).max() < FP64_TOL
+    assert np.abs(K - Ko2).max() < FP64_TOL
+    assert fb.contraction.last_stats["fp32"] == 0
+    with pytest.raises(ValueError):
+        fb.formRawGD(D, J=np.zeros((N, N)), K=K)  # row-major output
+
+
 def test_mixed_precision_within_1e6():
     basis, tpi, ob, D = _oracle_and_device("h2o8_ccpvdz")
     fb = FockBuilder(tpi)
