@@ -78,7 +78,7 @@ def parse():
                     help="arrival rates (Hz) the stream is replayed at")
     ap.add_argument("--profile-case", default=None,
                     help="one untimed build of a named case for profiler captures "
-                         "(h2o16_def2svp, h2o8_ccpvdz, ag4_dc, ag1_ssss) and exit")
+                         "(h2o16_def2svp, h2o8_ccpvdz, ag4_dc, ag1_ssss, ag1_llss) and exit")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of --profile-case")
     return ap.parse_args()
@@ -669,10 +669,10 @@ def profile_case(args):
     from chronusq_public_b200.fockbuilder import FockBuilder, FourCompFock
     name = args.profile_case
     cut = args.cutoff if args.precision == "mixed" else 0.0
-    if name == "ag1_ssss":
-        # one SSSS contraction of a single Ag atom (uncontracted basis) on a
-        # seeded Hermitian 17-entry input
-        from chronusq_public_b200.contraction import (SSSS, GTODirectRelERIContraction,
+    if name in ("ag1_ssss", "ag1_llss"):
+        # one SSSS (or LLSS) contraction of a single Ag atom (uncontracted
+        # basis) on a seeded Hermitian 17-entry input
+        from chronusq_public_b200.contraction import (LLSS, SSSS, GTODirectRelERIContraction,
                                                       TwoBodyContraction)
         basis = BasisSet.build(Molecule.from_angstrom([("Ag", 0.0, 0.0, 0.0)]),
                                "sapporo-dkh3-dzp-2012_no", uncontract=True)
@@ -685,8 +685,9 @@ def profile_case(args):
             X.append(np.asfortranarray(0.05 * (A + A.conj().T)))
         lst = [TwoBodyContraction(x, np.zeros((N, N), complex)) for x in X]
         t0 = time.perf_counter()
-        GTODirectRelERIContraction(tpi).twoBodyContract(lst, SSSS, precision=args.precision,
-                                                        fp32_cutoff=cut)
+        GTODirectRelERIContraction(tpi).twoBodyContract(
+            lst, SSSS if name == "ag1_ssss" else LLSS, precision=args.precision,
+            fp32_cutoff=cut)
     elif name == "ag4_dc":
         _basis, tpi, D = workloads.build_ag4_dc(lambda b: DirectTPI(b))
         t0 = time.perf_counter()

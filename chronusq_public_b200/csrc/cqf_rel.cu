@@ -128,6 +128,7 @@ struct RelLaunch {
   double* K[4];          // complex
   int shardIdx, shardCnt;  // bra pairs p with p % shardCnt == shardIdx only
   int skipSingle;          // single-primitive quartets go to rel_gemm_kernel
+  int contracted;          // some bra or ket pair has more than one primitive pair
   unsigned long long* counters;
 };
 
@@ -796,11 +797,15 @@ __global__ void __launch_bounds__(RB_THREADS)
   }
 }
 
-// Shared-memory layout of rel_llss_block_kernel (doubles).
+// Shared-memory layout of rel_llss_block_kernel (doubles).  The axis
+// factors depend on a component pair only through its two exponents on the
+// axis, so they are kept per (axis, i, j[, derivative type]); single-primitive
+// launches digest each element as it is made and keep no accumulator Mc.
 struct LlssBlockLayout {
   int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, total;
 };
-__host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int lc, int ld) {
+__host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int lc, int ld,
+                                                             bool single) {
   const int Lb = la + lb + 2, L = Lb + lc + ld;
   const int nab = ncart(la) * ncart(lb), ncd = ncart(lc) * ncart(ld);
   const int FL = 2 * (la > lb ? la : lb) + 3, FLk = lc + ld + 1;
@@ -811,10 +816,10 @@ __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int
   Lo.oR1 = take(nherm(L));
   Lo.oEb = take(3 * (la + 2) * (lb + 2) * (la + lb + 3));
   Lo.oEk = take(3 * (lc + 1) * (ld + 1) * (lc + ld + 1));
-  Lo.oFa = take(nab * 12 * FL);
-  Lo.oFc = take(ncd * 3 * FLk);
+  Lo.oFa = take(3 * (la + 1) * (lb + 1) * 4 * FL);
+  Lo.oFc = take(3 * (lc + 1) * (ld + 1) * FLk);
   Lo.oG = take(ncd * nherm(Lb));
-  Lo.oM = take(nab * ncd * 4);
+  Lo.oM = take(single ? 0 : nab * ncd * 4);
   Lo.oF = take(L + 1);
   Lo.oJ = take(ncd);
   Lo.total = o;
@@ -826,7 +831,10 @@ __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int
 // built at once, and the operator components of every (bra, ket) component
 // element are one work unit per thread (nab x ncd units); digestion per
 // element, the per-column Coulomb sums J_LL(C,D) reduced in shared memory.
-template <typename T>
+// SINGLE: the instance for quartets of two single-primitive pairs (every
+// quartet of an uncontracted basis), which digests each element at once;
+// the other instance then takes the rest.
+template <typename T, bool SINGLE>
 __global__ void __launch_bounds__(RB_THREADS)
     rel_llss_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
   constexpr bool IS32 = sizeof(T) == 4;
@@ -837,7 +845,8 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
-  if (a.skipSingle && P.npp == 1 && Q.npp == 1) return;  // rel_gemm_kernel's
+  if (SINGLE ? (P.npp != 1 || Q.npp != 1) : (a.skipSingle && P.npp == 1 && Q.npp == 1))
+    return;  // the other instance's
   const double bound = sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) *
                        __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
                        __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns);
@@ -860,7 +869,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int Lb = la + lb + 2, L = Lb + lc + ld;
   const int hb = nherm(Lb);
   const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
-  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
+  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, SINGLE);
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -880,8 +889,17 @@ __global__ void __launch_bounds__(RB_THREADS)
   const size_t nc = a.ncart;
   const T* R = Rb[0];
 
-  for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
+  if (!SINGLE)
+    for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
   for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
+  // the axis factor vectors of (axis x, bra exponents i, j, type ty) and
+  // (axis x, ket exponents i, j)
+  auto faOf = [&](int x, int i, int j, int ty) {
+    return fa + (size_t)(((x * (la + 1) + i) * (lb + 1) + j) * 4 + ty) * FL;
+  };
+  auto fcOf = [&](int x, int i, int j) {
+    return fc + (size_t)((x * (lc + 1) + i) * (ld + 1) + j) * FLk;
+  };
 #pragma unroll 1
   for (int ip = 0; ip < P.npp; ip++)
 #pragma unroll 1
@@ -930,20 +948,17 @@ __global__ void __launch_bounds__(RB_THREADS)
         }
         __syncthreads();
       }
-      // bra factors (every pair, axis, derivative type); ket factors of every
-      // ket component pair (undifferentiated, sign (-1)^t folded in)
-      for (int it = tid; it < nab * 12; it += RB_THREADS) {
-        const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
-        const int ai = ab / nb, bi = ab % nb;
-        const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
-        const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
+      // bra factors (every axis, exponent pair, derivative type); ket factors
+      // (undifferentiated, sign (-1)^t folded in)
+      for (int it = tid; it < 3 * (la + 1) * (lb + 1) * 4; it += RB_THREADS) {
+        const int ty = it % 4, jb = (it / 4) % (lb + 1), ia = (it / 4 / (lb + 1)) % (la + 1),
+                  x = it / 4 / (lb + 1) / (la + 1);
         axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
                        fa + (size_t)it * FL);
       }
-      for (int it = tid; it < ncd * 3; it += RB_THREADS) {
-        const int cd = it / 3, x = it % 3, c = cd / nd, d = cd % nd;
-        const int ci = x == 0 ? cart_lx(lc, c) : (x == 1 ? cart_ly(lc, c) : cart_lz(lc, c));
-        const int di = x == 0 ? cart_lx(ld, d) : (x == 1 ? cart_ly(ld, d) : cart_lz(ld, d));
+      for (int it = tid; it < 3 * (lc + 1) * (ld + 1); it += RB_THREADS) {
+        const int di = it % (ld + 1), ci = (it / (ld + 1)) % (lc + 1),
+                  x = it / (ld + 1) / (lc + 1);
         T* f = fc + (size_t)it * FLk;
         const int n = axis_factor<T>(Ek + x * E1k, ld, lc + ld + 1, ci, di, 0, T(0), T(0), f);
         for (int t = 1; t < n; t += 2) f[t] = -f[t];
@@ -954,9 +969,9 @@ __global__ void __launch_bounds__(RB_THREADS)
         const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
         int t, u, v;
         hinv(h, t, u, v);
-        const T* fx = fc + (size_t)(cd * 3 + 0) * FLk;
-        const T* fy = fc + (size_t)(cd * 3 + 1) * FLk;
-        const T* fz = fc + (size_t)(cd * 3 + 2) * FLk;
+        const T* fx = fcOf(0, cart_lx(lc, c), cart_lx(ld, d));
+        const T* fy = fcOf(1, cart_ly(lc, c), cart_ly(ld, d));
+        const T* fz = fcOf(2, cart_lz(lc, c), cart_lz(ld, d));
         const int nx = cart_lx(lc, c) + cart_lx(ld, d) + 1;
         const int ny = cart_ly(lc, c) + cart_ly(ld, d) + 1;
         const int nz = cart_lz(lc, c) + cart_lz(ld, d) + 1;
@@ -986,19 +1001,28 @@ __global__ void __launch_bounds__(RB_THREADS)
             op_of(mu, nu, op, sg);
             const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
                       tz = (mu == 2) | ((nu == 2) << 1);
-            m4[op] += sg * (double)bra_dot<T>(fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL,
+            m4[op] += sg * (double)bra_dot<T>(faOf(0, ax[0], bx[0], tx),
                                    ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1,
-                                   fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL,
+                                   faOf(1, ax[1], bx[1], ty),
                                    ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1,
-                                   fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL,
+                                   faOf(2, ax[2], bx[2], tz),
                                    ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + (size_t)cd * hb);
           }
-        for (int op = 0; op < 4; op++) Mc[(size_t)e * 4 + op] += m4[op];
+        if (SINGLE) {  // one primitive quartet: digest the element now
+          const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
+          RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
+                     __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc)), {0, 0, 0, 0}};
+          double jl[4] = {0.0, 0.0, 0.0, 0.0};
+          rel_digest<1>(a, P, col, ai, bi, m4, jl);
+          if (jl[0] != 0.0) atomicAdd(Js + cd, jl[0]);
+        } else {
+          for (int op = 0; op < 4; op++) Mc[(size_t)e * 4 + op] += m4[op];
+        }
       }
     }
   __syncthreads();
   // digestion, one (bra, ket) component element per thread
-  for (int e = tid; e < nab * ncd; e += RB_THREADS) {
+  for (int e = tid; e < (SINGLE ? 0 : nab * ncd); e += RB_THREADS) {
     const int ab = e / ncd, cd = e % ncd;
     const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
     RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
@@ -1519,18 +1543,26 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
   }
   if (TYPE == 1) {
     // LLSS d/f classes: one block per quartet with every ket component at
-    // once, when it fits in shared memory; else per thread
-    const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld);
-    const size_t smem = (size_t)Lo.total * sizeof(double);
-    if (smem <= REL_SMEM_MAX) {
+    // once, when it fits in shared memory (single-primitive quartets in
+    // their own instance); else per thread
+    const long long nq = (long long)a.nBra * a.nKet;
+    const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
+    const unsigned gy = (unsigned)((nq + gx - 1) / gx);
+    const size_t smem1 = (size_t)llss_block_layout(la, lb, lc, ld, true).total * sizeof(double);
+    if (smem1 <= REL_SMEM_MAX) {
       // always the same limit (on the current device), never one below a
       // launch still queued
-      cudaFuncSetAttribute(rel_llss_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)REL_SMEM_MAX);
-      const long long nq = (long long)a.nBra * a.nKet;
-      const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
-      const unsigned gy = (unsigned)((nq + gx - 1) / gx);
-      rel_llss_block_kernel<T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+      cudaFuncSetAttribute(rel_llss_block_kernel<T, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REL_SMEM_MAX);
+      rel_llss_block_kernel<T, true><<<dim3(gx, gy), RB_THREADS, smem1, st>>>(a, la, lb, lc, ld);
+      a.skipSingle = 1;
+      if (!a.contracted) return;
+    }
+    const size_t smem = (size_t)llss_block_layout(la, lb, lc, ld, false).total * sizeof(double);
+    if (smem <= REL_SMEM_MAX) {
+      cudaFuncSetAttribute(rel_llss_block_kernel<T, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REL_SMEM_MAX);
+      rel_llss_block_kernel<T, false><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
     } else if (lm == 2) {
       rel_kernel<2, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     } else {
@@ -2723,6 +2755,11 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
       a.ketBeg = B->cls_beg[ck];
       a.nKet = B->cls_cnt[ck];
       a.same = (cb == ck);
+      a.contracted = 0;
+      for (int i = 0; i < a.nBra && !a.contracted; i++)
+        a.contracted = B->h_pairs[a.braBeg + i].npp > 1;
+      for (int i = 0; i < a.nKet && !a.contracted; i++)
+        a.contracted = B->h_pairs[a.ketBeg + i].npp > 1;
       if (llss) launch_rel<1>(a, la, lb, lc, ld, st);
       else launch_rel<2>(a, la, lb, lc, ld, st);
     }
