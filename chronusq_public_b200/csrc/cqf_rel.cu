@@ -514,7 +514,7 @@ __host__ __device__ inline RelBlockLayout rel_block_layout(int la, int lb, int l
   Lo.oR1 = take(nherm(L));
   Lo.oEb = take(3 * (la + 2) * (lb + 2) * (la + lb + 3));
   Lo.oEk = take(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
-  Lo.oFa = take(nab * 12 * FL);
+  Lo.oFa = take(3 * (la + 1) * (lb + 1) * 4 * FL);  // per (axis, exponent pair, type)
   Lo.oFc = take(12 * FLk);
   Lo.oG = take(NB * nherm(Lb));
   Lo.oM = take(nab * 4 * NB);
@@ -662,16 +662,17 @@ __global__ void __launch_bounds__(RB_THREADS)
       }
       __syncthreads();
     }
-    // bra factors of every component pair, axis and derivative type
-    for (int it = tid; it < nab * 12; it += RB_THREADS) {
-      const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
-      const int ai = ab / nb, bi = ab % nb;
-      const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
-      const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
+    // bra factors of every axis, exponent pair and derivative type
+    for (int it = tid; it < 3 * (la + 1) * (lb + 1) * 4; it += RB_THREADS) {
+      const int ty = it % 4, jb = (it / 4) % (lb + 1), ia = (it / 4 / (lb + 1)) % (la + 1),
+                x = it / 4 / (lb + 1) / (la + 1);
       axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
                      fa + (size_t)it * FL);
     }
     __syncthreads();
+  };
+  auto faOf = [&](int x, int i, int j, int ty) {
+    return fa + (size_t)(((x * (la + 1) + i) * (lb + 1) + j) * 4 + ty) * FL;
   };
 
   const bool single = P.npp == 1 && Q.npp == 1;
@@ -754,9 +755,9 @@ __global__ void __launch_bounds__(RB_THREADS)
               op_of(mu, nu, op, sg);
               const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
                         tz = (mu == 2) | ((nu == 2) << 1);
-              const T* gx = fa + ((size_t)ab * 12 + 0 * 4 + tx) * FL;
-              const T* gy = fa + ((size_t)ab * 12 + 1 * 4 + ty) * FL;
-              const T* gz = fa + ((size_t)ab * 12 + 2 * 4 + tz) * FL;
+              const T* gx = faOf(0, ax[0], bx[0], tx);
+              const T* gy = faOf(1, ax[1], bx[1], ty);
+              const T* gz = faOf(2, ax[2], bx[2], tz);
               m4[op] += sg * (double)bra_dot<T>(gx, ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1, gy,
                                      ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1, gz,
                                      ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + b * hb);
