@@ -129,6 +129,7 @@ struct RelLaunch {
   int shardIdx, shardCnt;  // bra pairs p with p % shardCnt == shardIdx only
   int skipSingle;          // single-primitive quartets go to rel_gemm_kernel
   int contracted;          // some bra or ket pair has more than one primitive pair
+  int nsm;                 // multiprocessors of the device
   unsigned long long* counters;
 };
 
@@ -832,10 +833,9 @@ __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int
 // built at once, and the operator components of every (bra, ket) component
 // element are one work unit per thread (nab x ncd units); digestion per
 // element, the per-column Coulomb sums J_LL(C,D) reduced in shared memory.
-// SINGLE: the instance for quartets of two single-primitive pairs (every
-// quartet of an uncontracted basis), which digests each element at once;
-// the other instance then takes the rest.
-template <typename T, bool SINGLE>
+// With skipSingle set the quartets of two single-primitive pairs are
+// rel_llss_single_kernel's.
+template <typename T>
 __global__ void __launch_bounds__(RB_THREADS)
     rel_llss_block_kernel(const RelLaunch a, int la, int lb, int lc, int ld) {
   constexpr bool IS32 = sizeof(T) == 4;
@@ -846,8 +846,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int ns = a.nShell;
   const PairDev P = a.pairs[a.braBeg + ib];
   const PairDev Q = a.pairs[a.ketBeg + jk];
-  if (SINGLE ? (P.npp != 1 || Q.npp != 1) : (a.skipSingle && P.npp == 1 && Q.npp == 1))
-    return;  // the other instance's
+  if (a.skipSingle && P.npp == 1 && Q.npp == 1) return;  // rel_llss_single_kernel's
   const double bound = sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) *
                        __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
                        __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns);
@@ -870,7 +869,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int Lb = la + lb + 2, L = Lb + lc + ld;
   const int hb = nherm(Lb);
   const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
-  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, SINGLE);
+  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, false);
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -890,8 +889,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const size_t nc = a.ncart;
   const T* R = Rb[0];
 
-  if (!SINGLE)
-    for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
+  for (int e = tid; e < nab * ncd * 4; e += RB_THREADS) Mc[e] = 0.0;
   for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
   // the axis factor vectors of (axis x, bra exponents i, j, type ty) and
   // (axis x, ket exponents i, j)
@@ -1009,21 +1007,12 @@ __global__ void __launch_bounds__(RB_THREADS)
                                    faOf(2, ax[2], bx[2], tz),
                                    ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + (size_t)cd * hb);
           }
-        if (SINGLE) {  // one primitive quartet: digest the element now
-          const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
-          RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
-                     __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc)), {0, 0, 0, 0}};
-          double jl[4] = {0.0, 0.0, 0.0, 0.0};
-          rel_digest<1>(a, P, col, ai, bi, m4, jl);
-          if (jl[0] != 0.0) atomicAdd(Js + cd, jl[0]);
-        } else {
-          for (int op = 0; op < 4; op++) Mc[(size_t)e * 4 + op] += m4[op];
-        }
+        for (int op = 0; op < 4; op++) Mc[(size_t)e * 4 + op] += m4[op];
       }
     }
   __syncthreads();
   // digestion, one (bra, ket) component element per thread
-  for (int e = tid; e < (SINGLE ? 0 : nab * ncd); e += RB_THREADS) {
+  for (int e = tid; e < nab * ncd; e += RB_THREADS) {
     const int ab = e / ncd, cd = e % ncd;
     const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
     RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
@@ -1037,6 +1026,208 @@ __global__ void __launch_bounds__(RB_THREADS)
     if (Js[cd] != 0.0)
       atomicAdd(a.Jll + (size_t)(Q.cA + cd / nd) + (size_t)(Q.cB + cd % nd) * nc,
                 w34 * s12d * Js[cd]);
+}
+
+// LLSS quartets of two single-primitive pairs (every quartet of an
+// uncontracted basis): one block per bra pair and tile of kt ket pairs (kt
+// up to LS_KT; 1 for launches too small to fill the GPU otherwise).
+// The bra pair's E tables and axis factors are made once; per ket its E
+// tables, Boys values and R (level by level over the block), the ket factors,
+// G[cd][tuv] of every ket component pair, then the operator components of
+// every (bra, ket) component element, digested as they are made (one
+// primitive quartet: nothing to accumulate).  Same quartet set, screens and
+// updates as rel_llss_block_kernel.
+constexpr int LS_KT = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(RB_THREADS)
+    rel_llss_single_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int kt) {
+  constexpr bool IS32 = sizeof(T) == 4;
+  extern __shared__ double sm[];
+  const int nTiles = (a.nKet + kt - 1) / kt;
+  const long long q = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  const int ib = (int)(q / nTiles), tile = (int)(q % nTiles);
+  if (ib >= a.nBra || !in_shard(a.braBeg + ib, a.shardIdx, a.shardCnt)) return;
+  const PairDev P = a.pairs[a.braBeg + ib];
+  if (P.npp != 1) return;  // contracted bra: rel_llss_block_kernel
+  const int jkEnd = min(tile * kt + kt, a.nKet);
+  const int ns = a.nShell;
+  const T* boysT = reinterpret_cast<const T*>(IS32 ? (const void*)a.boys32 : (const void*)a.boys);
+
+  const int tid = threadIdx.x;
+  const int na = ncart(la), nb = ncart(lb), ncc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb, ncd = ncc * nd;
+  const int Lb = la + lb + 2, L = Lb + lc + ld;
+  const int hb = nherm(Lb);
+  const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
+  const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, true);
+  T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
+  T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
+  T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
+  T* fa = reinterpret_cast<T*>(sm + Lo.oFa);
+  T* fc = reinterpret_cast<T*>(sm + Lo.oFc);
+  T* G = reinterpret_cast<T*>(sm + Lo.oG);
+  T* Fs = reinterpret_cast<T*>(sm + Lo.oF);
+  double* Js = sm + Lo.oJ;
+  const int E1b = (la + 2) * (lb + 2) * (la + lb + 3);
+  const int E1k = (lc + 1) * (ld + 1) * (lc + ld + 1);
+  const ShellDev SA = a.shells[P.shA], SB = a.shells[P.shB];
+  const bool dAB = P.shA == P.shB;
+  const double s12d = dAB ? 1.0 : 2.0, w12 = dAB ? 0.5 : 1.0;
+  const size_t nc = a.ncart;
+  const T* R = Rb[0];
+  auto faOf = [&](int x, int i, int j, int ty) {
+    return fa + (size_t)(((x * (la + 1) + i) * (lb + 1) + j) * 4 + ty) * FL;
+  };
+  auto fcOf = [&](int x, int i, int j) {
+    return fc + (size_t)((x * (lc + 1) + i) * (ld + 1) + j) * FLk;
+  };
+
+  // ---- bra phase: E tables and axis factors of every axis, exponent pair
+  // and derivative type
+  const PrimPairDev& A = a.pp[P.pp_off];
+  double ea, eb;
+  pair_exps(SA, SB, a.prim, A, ea, eb);
+  if (tid < 3)
+    hermite_E_rt<T, LMAX + 1>(la + 1, lb + 1, T(A.o2p), T(A.PA[tid]), T(A.PB[tid]),
+                              Eb + tid * E1b);
+  __syncthreads();
+  for (int it = tid; it < 3 * (la + 1) * (lb + 1) * 4; it += RB_THREADS) {
+    const int ty = it % 4, jb = (it / 4) % (lb + 1), ia = (it / 4 / (lb + 1)) % (la + 1),
+              x = it / 4 / (lb + 1) / (la + 1);
+    axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
+                   fa + (size_t)it * FL);
+  }
+  // (read after the barriers of the first ket)
+
+  // ---- the tile's kets
+#pragma unroll 1
+  for (int jk = tile * kt; jk < jkEnd; jk++) {
+    const PairDev Q = a.pairs[a.ketBeg + jk];
+    if (Q.npp != 1) continue;  // contracted ket: rel_llss_block_kernel (block-uniform)
+    const double bound = sh_max(a.norms, P.s1, P.s2, Q.s1, Q.s2, ns) *
+                         __ldg(a.qSS + P.s1 + (size_t)P.s2 * ns) *
+                         __ldg(a.qLL + Q.s1 + (size_t)Q.s2 * ns);
+    const bool work = !a.screen || bound >= a.thresh;
+    const bool lo = a.mixed && bound < a.cut &&
+                    fp32_range_ok(__ldg(a.pairRange + a.braBeg + ib),
+                                  __ldg(a.pairRange + a.ketBeg + jk), la + lb + lc + ld + 2, 1,
+                                  0);
+    const bool mine = work && (IS32 ? lo : !lo);
+    if (tid == 0) {
+      if (!IS32) atomicAdd(a.counters + 0, 1ull);
+      if (!IS32 && !work) atomicAdd(a.counters + 1, 1ull);
+      if (mine) atomicAdd(a.counters + (IS32 ? 2 : 3), 1ull);
+    }
+    if (!mine) continue;  // block-uniform
+    const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
+    const bool dCD = Q.shA == Q.shB;
+    const double s34d = dCD ? 1.0 : 2.0, w34 = dCD ? 0.5 : 1.0;
+    const PrimPairDev& B = a.pp[Q.pp_off];
+    const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
+    const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
+    const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
+    // the previous ket's readers are past the barrier that ended its loop
+    if (tid < 3)
+      hermite_E_rt<T, LMAX + 1>(lc, ld, T(B.o2p), T(B.PA[tid]), T(B.PB[tid]), Ek + tid * E1k);
+    else if (tid == 32)
+      boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+    for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
+    __syncthreads();
+    const T m2a = T(-2) * alpha;
+    for (int n = L; n >= 0; n--) {
+      T* cur = Rb[n & 1];
+      const T* prv = Rb[(n + 1) & 1];
+      const int cnt = nherm(L - n);
+      for (int e = tid; e < cnt; e += RB_THREADS) {
+        int t, u, v;
+        hinv(e, t, u, v);
+        T val;
+        if (e == 0) {
+          T f = T(1);
+          for (int k = 0; k < n; k++) f *= m2a;
+          val = f * Fs[n];
+        } else if (t > 0) {
+          val = X * prv[hidx(t - 1, u, v)];
+          if (t > 1) val += T(t - 1) * prv[hidx(t - 2, u, v)];
+        } else if (u > 0) {
+          val = Y * prv[hidx(0, u - 1, v)];
+          if (u > 1) val += T(u - 1) * prv[hidx(0, u - 2, v)];
+        } else {
+          val = Z * prv[hidx(0, 0, v - 1)];
+          if (v > 1) val += T(v - 1) * prv[hidx(0, 0, v - 2)];
+        }
+        cur[e] = val;
+      }
+      if (n == L) {  // the ket factors beside the first level (Ek is complete)
+        for (int it = tid; it < 3 * (lc + 1) * (ld + 1); it += RB_THREADS) {
+          const int di = it % (ld + 1), ci = (it / (ld + 1)) % (lc + 1),
+                    x = it / (ld + 1) / (lc + 1);
+          T* f = fc + (size_t)it * FLk;
+          const int nf = axis_factor<T>(Ek + x * E1k, ld, lc + ld + 1, ci, di, 0, T(0), T(0), f);
+          for (int t = 1; t < nf; t += 2) f[t] = -f[t];
+        }
+      }
+      __syncthreads();
+    }
+    // G[cd][tuv] of every ket component pair
+    for (int e = tid; e < ncd * hb; e += RB_THREADS) {
+      const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
+      int t, u, v;
+      hinv(h, t, u, v);
+      const T* fx = fcOf(0, cart_lx(lc, c), cart_lx(ld, d));
+      const T* fy = fcOf(1, cart_ly(lc, c), cart_ly(ld, d));
+      const T* fz = fcOf(2, cart_lz(lc, c), cart_lz(ld, d));
+      const int nx = cart_lx(lc, c) + cart_lx(ld, d) + 1;
+      const int ny = cart_ly(lc, c) + cart_ly(ld, d) + 1;
+      const int nz = cart_lz(lc, c) + cart_lz(ld, d) + 1;
+      T acc = T(0);
+      for (int i = 0; i < nx; i++) {
+        if (fx[i] == T(0)) continue;
+        for (int j = 0; j < ny; j++) {
+          const T fxy = fx[i] * fy[j];
+          if (fxy == T(0)) continue;
+          for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+        }
+      }
+      G[e] = pref * acc;
+    }
+    __syncthreads();
+    // operator components of every (bra, ket) component element, digested
+    for (int e = tid; e < nab * ncd; e += RB_THREADS) {
+      const int ab = e / ncd, cd = e % ncd;
+      const int ai = ab / nb, bi = ab % nb;
+      const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
+      const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
+      double m4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int mu = 0; mu < 3; mu++)
+        for (int nu = 0; nu < 3; nu++) {
+          int op;
+          double sg;
+          op_of(mu, nu, op, sg);
+          const int tx = (mu == 0) | ((nu == 0) << 1), ty = (mu == 1) | ((nu == 1) << 1),
+                    tz = (mu == 2) | ((nu == 2) << 1);
+          m4[op] += sg * (double)bra_dot<T>(faOf(0, ax[0], bx[0], tx),
+                                 ax[0] + bx[0] + (tx & 1) + (tx >> 1) + 1,
+                                 faOf(1, ax[1], bx[1], ty),
+                                 ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1,
+                                 faOf(2, ax[2], bx[2], tz),
+                                 ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + (size_t)cd * hb);
+        }
+      const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
+      RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
+                 __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc)), {0, 0, 0, 0}};
+      double jl[4] = {0.0, 0.0, 0.0, 0.0};
+      rel_digest<1>(a, P, col, ai, bi, m4, jl);
+      if (jl[0] != 0.0) atomicAdd(Js + cd, jl[0]);
+    }
+    __syncthreads();
+    for (int cd = tid; cd < ncd; cd += RB_THREADS)
+      if (Js[cd] != 0.0)
+        atomicAdd(a.Jll + (size_t)(Q.cA + cd / nd) + (size_t)(Q.cB + cd % nd) * nc,
+                  w34 * s12d * Js[cd]);
+    __syncthreads();  // the ket's shared memory is free for the next one
+  }
 }
 
 // ---------------------------------------- GEMM form of the block kernels
@@ -1553,17 +1744,24 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
     if (smem1 <= REL_SMEM_MAX) {
       // always the same limit (on the current device), never one below a
       // launch still queued
-      cudaFuncSetAttribute(rel_llss_block_kernel<T, true>,
+      cudaFuncSetAttribute(rel_llss_single_kernel<T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REL_SMEM_MAX);
-      rel_llss_block_kernel<T, true><<<dim3(gx, gy), RB_THREADS, smem1, st>>>(a, la, lb, lc, ld);
+      // ket tiles only where the launch keeps ~64 blocks per SM without them
+      const int kt = (int)std::max<long long>(
+          1, std::min<long long>(LS_KT, nq / (64LL * std::max(1, a.nsm))));
+      const long long nb1 = (long long)a.nBra * ((a.nKet + kt - 1) / kt);
+      const unsigned gx1 = (unsigned)std::min<long long>(nb1, 65535);
+      const unsigned gy1 = (unsigned)((nb1 + gx1 - 1) / gx1);
+      rel_llss_single_kernel<T><<<dim3(gx1, gy1), RB_THREADS, smem1, st>>>(a, la, lb, lc, ld,
+                                                                           kt);
       a.skipSingle = 1;
       if (!a.contracted) return;
     }
     const size_t smem = (size_t)llss_block_layout(la, lb, lc, ld, false).total * sizeof(double);
     if (smem <= REL_SMEM_MAX) {
-      cudaFuncSetAttribute(rel_llss_block_kernel<T, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REL_SMEM_MAX);
-      rel_llss_block_kernel<T, false><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
+      cudaFuncSetAttribute(rel_llss_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)REL_SMEM_MAX);
+      rel_llss_block_kernel<T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
     } else if (lm == 2) {
       rel_kernel<2, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     } else {
@@ -2744,6 +2942,7 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
   a.shardIdx = opts.shard_index;
   a.shardCnt = std::max(1, opts.shard_count);
   a.counters = dcnt;
+  a.nsm = B->nsm;
   for (int cb = 0; cb < NCLS; cb++)
     for (int ck = 0; ck < NCLS; ck++) {
       if (!llss && ck > cb) continue;
