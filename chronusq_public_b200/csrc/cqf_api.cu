@@ -1479,12 +1479,12 @@ void pinned_release(double* p) {
 // real symmetric, A real antisymmetric), J[X] = J[S] and K[X] = K[S] + i K[A],
 // so one real contraction -- J on S, K on S and K on A (flagged
 // antisymmetric) -- gives every result; the screen uses the norms of the
-// complex X, as the reference's does.  Used when every class of the basis
-// runs on the fast kernels (l <= 2; split_eligible).
+// complex X, as the reference's does.  The classes with f shells run on the
+// real generic kernel, the others on the fast ones (split_eligible).
 
 bool split_eligible(const cqf_basis* B, const cqf_contraction* list, int nMat,
                     const cqf_opts& opts) {
-  if (!opts.is_complex || B->maxL > 2) return false;
+  if (!opts.is_complex || B->maxL > LMAX) return false;
   int nReal = 0;
   for (int m = 0; m < nMat; m++) {
     if (!list[m].hermitian) return false;

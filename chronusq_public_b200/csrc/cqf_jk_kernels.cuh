@@ -92,6 +92,9 @@ __device__ __forceinline__ void digest_one(int flags, const double* __restrict__
       M::addre(A, ix(i1, i2), M::ldre(X, ix(i4, i3)) * v);
       M::addre(A, ix(i4, i3), M::ldre(X, ix(i1, i2)) * v);
     } else {
+      // (bit 2, the antisymmetric part of a split complex Hermitian density,
+      // needs nothing here: these four updates read X in the orientation
+      // the antisymmetric back transform expects, as the class kernels' do)
       const double h = 0.5 * v;
       M::add(A, ix(i1, i3), M::ldc(X, ix(i4, i2)), h);
       M::add(A, ix(i4, i2), M::ldc(X, ix(i1, i3)), h);

@@ -2854,10 +2854,19 @@ cqf_status rel_contract_dev(cqf_basis* B, const double* const* X, double* const*
     o.stream = st;
     o.shard_index = opts.shard_index;
     o.shard_count = opts.shard_count;
-    CQF_RTRY(basis_workspace(B, ws_layout(B, (int)list.size(), o).total * sizeof(double)));
     cqf_stats s1{};
-    CQF_RTRY(contract_core(B, list.data(), (int)list.size(), o, &s1,
-                           static_cast<double*>(B->d_ws), false, nullptr));
+    const int n = (int)list.size();
+    if (split_eligible(B, list.data(), n, o)) {
+      // Hermitian entries: real and imaginary parts on the real kernels
+      CQF_RTRY(basis_workspace(
+          B, split_ws_doubles(B, split_real_count(list.data(), n), o) * sizeof(double)));
+      CQF_RTRY(split_core(B, list.data(), n, o, &s1, static_cast<double*>(B->d_ws), false,
+                          nullptr));
+    } else {
+      CQF_RTRY(basis_workspace(B, ws_layout(B, n, o).total * sizeof(double)));
+      CQF_RTRY(contract_core(B, list.data(), n, o, &s1, static_cast<double*>(B->d_ws), false,
+                             nullptr));
+    }
     cnt[0] += s1.quartets_total;
     cnt[1] += s1.quartets_screened;
     cnt[2] += s1.quartets_fp32;
