@@ -734,7 +734,7 @@ __global__ void __launch_bounds__(RB_THREADS)
                 for (int j = 0; j < ny; j++) {
                   const T fxy = fx[i] * fy[j];
                   if (fxy == T(0)) continue;
-                  for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+                  acc += fxy * hdot_v(fz, nz, R, t + i, u + j, v);
                 }
               }
               gsum += T(sg) * acc;
@@ -980,7 +980,7 @@ __global__ void __launch_bounds__(RB_THREADS)
           for (int j = 0; j < ny; j++) {
             const T fxy = fx[i] * fy[j];
             if (fxy == T(0)) continue;
-            for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+            acc += fxy * hdot_v(fz, nz, R, t + i, u + j, v);
           }
         }
         G[e] = pref * acc;
@@ -1187,7 +1187,7 @@ __global__ void __launch_bounds__(RB_THREADS)
         for (int j = 0; j < ny; j++) {
           const T fxy = fx[i] * fy[j];
           if (fxy == T(0)) continue;
-          for (int k = 0; k < nz; k++) acc += fxy * fz[k] * R[hidx(t + i, u + j, v + k)];
+          acc += fxy * hdot_v(fz, nz, R, t + i, u + j, v);
         }
       }
       G[e] = pref * acc;
