@@ -136,6 +136,52 @@ __device__ __forceinline__ void boys_rt<float>(int L, float T, float* F, const f
   }
 }
 
+// F_0 .. F_L spread over the lanes of one warp: below TMAX every order from
+// its own table row (the Taylor sum boys_rt uses for F_L), above it lane 0
+// runs boys_rt's upward recursion.  All 32 lanes call it; F is shared memory.
+template <typename T>
+__device__ __forceinline__ void boys_lanes(int L, T Targ, T* F, const T* tab, int lane);
+
+template <>
+__device__ __forceinline__ void boys_lanes<double>(int L, double T, double* F, const double* tab,
+                                                   int lane) {
+  if (T < BOYS_TMAX) {
+    const int j = __double2int_rn(T * (1.0 / BOYS_DT));
+    const double dT = j * BOYS_DT - T;
+#pragma unroll 1
+    for (int m = lane; m <= L; m += 32) {
+      const double* row = tab + ((size_t)m * BOYS_NPTS + j) * BOYS_ROW64;
+      double s = __ldg(row + BOYS_K64);
+#pragma unroll
+      for (int k = BOYS_K64 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0 / (k + 1));
+      F[m] = s;
+    }
+  } else if (lane == 0) {
+    boys_rt<double>(L, T, F, tab);
+  }
+  __syncwarp();
+}
+
+template <>
+__device__ __forceinline__ void boys_lanes<float>(int L, float T, float* F, const float* tab,
+                                                  int lane) {
+  if (T < (float)BOYS_TMAX) {
+    const int j = __float2int_rn(T * (float)(1.0 / BOYS_DT));
+    const float dT = j * (float)BOYS_DT - T;
+#pragma unroll 1
+    for (int m = lane; m <= L; m += 32) {
+      const float* row = tab + ((size_t)m * BOYS_NPTS + j) * BOYS_ROW32;
+      float s = __ldg(row + BOYS_K32);
+#pragma unroll
+      for (int k = BOYS_K32 - 1; k >= 0; k--) s = __ldg(row + k) + s * dT * (1.0f / (k + 1));
+      F[m] = s;
+    }
+  } else if (lane == 0) {
+    boys_rt<float>(L, T, F, tab);
+  }
+  __syncwarp();
+}
+
 // Storage bounds for angular momenta up to LM per shell.
 template <int LM>
 struct RtBounds {

@@ -633,7 +633,8 @@ __global__ void __launch_bounds__(RB_THREADS)
     const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
     const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
     pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
-    if (tid == 6) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+    if (tid >= 32 && tid < 64)
+      boys_lanes<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT, tid - 32);
     __syncthreads();
     // R^(n)_tuv, n = L .. 0, from R^(n+1); level n in Rb[n & 1]
     const T m2a = T(-2) * alpha;
@@ -918,7 +919,8 @@ __global__ void __launch_bounds__(RB_THREADS)
       const T X = T(A.P[0] - B.P[0]), Y = T(A.P[1] - B.P[1]), Z = T(A.P[2] - B.P[2]);
       const T pq = T(A.p) + T(B.p), alpha = T(A.p) * T(B.p) / pq;
       const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
-      if (tid == 6) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+      if (tid >= 32 && tid < 64)
+        boys_lanes<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT, tid - 32);
       __syncthreads();
       const T m2a = T(-2) * alpha;
       for (int n = L; n >= 0; n--) {
@@ -1130,8 +1132,8 @@ __global__ void __launch_bounds__(RB_THREADS)
     // the previous ket's readers are past the barrier that ended its loop
     if (tid < 3)
       hermite_E_rt<T, LMAX + 1>(lc, ld, T(B.o2p), T(B.PA[tid]), T(B.PB[tid]), Ek + tid * E1k);
-    else if (tid == 32)
-      boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+    else if (tid >= 32 && tid < 64)
+      boys_lanes<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT, tid - 32);
     for (int e = tid; e < ncd; e += RB_THREADS) Js[e] = 0.0;
     __syncthreads();
     const T m2a = T(-2) * alpha;
@@ -1483,7 +1485,7 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
     const T pref = T(PI52X2) / sqrt(pq) * T(A.Kp) * T(B.Kp);
     // Boys (one thread) and the ket E tables, then R level by level over the
     // block, indices from the table
-    if (tid == 0) boys_rt<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT);
+    if (tid < 32) boys_lanes<T>(L, alpha * (X * X + Y * Y + Z * Z), Fs, boysT, tid);
     else if (tid >= 32 && tid < 35)
       hermite_E_rt<T, LMAX + 1>(lc + dK, ld + dK, T(B.o2p), T(B.PA[tid - 32]),
                                 T(B.PB[tid - 32]), Ek + (tid - 32) * E1k);
