@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(RB_THREADS)
 constexpr int LS_KT = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(RB_THREADS)
+__global__ void __launch_bounds__(RB_THREADS, 8)
     rel_llss_single_kernel(const RelLaunch a, int la, int lb, int lc, int ld, int kt) {
   constexpr bool IS32 = sizeof(T) == 4;
   extern __shared__ double sm[];
@@ -1122,7 +1122,6 @@ __global__ void __launch_bounds__(RB_THREADS)
       if (mine) atomicAdd(a.counters + (IS32 ? 2 : 3), 1ull);
     }
     if (!mine) continue;  // block-uniform
-    const ShellDev SC = a.shells[Q.shA], SD = a.shells[Q.shB];
     const bool dCD = Q.shA == Q.shB;
     const double s34d = dCD ? 1.0 : 2.0, w34 = dCD ? 0.5 : 1.0;
     const PrimPairDev& B = a.pp[Q.pp_off];
@@ -1703,12 +1702,12 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
   RelLaunch a = aIn;
   a.skipSingle = 0;
   const int lmax = std::max(std::max(la, lb), std::max(lc, ld));
-  if (TYPE == 2 && lmax >= 2) {
+  if constexpr (TYPE == 2) if (lmax >= 2) {
     // single-primitive SSSS quartets of the d and f classes: the GEMM form,
     // when its layout fits; the other kernels skip them.  (LLSS quartets are
-    // lighter -- one ket operator -- and the LLSS block kernel, with every
-    // ket component pair's Hermite sums built at once, measured faster: one
-    // Ag atom 0.31 s in the GEMM form against 0.27 s.)
+    // lighter -- one ket operator -- and the LLSS kernels, with every ket
+    // component pair's Hermite sums built at once, measured faster: one Ag
+    // atom 0.31 s in the GEMM form against 0.27 s for the first of them.)
     const int esz = (int)sizeof(T);
     const int CH = rel_gemm_chunk(la, lb, lc, ld, TYPE, esz);
     if (CH > 0) {
@@ -1735,7 +1734,7 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
     rel_kernel<1, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     return;
   }
-  if (TYPE == 1) {
+  if constexpr (TYPE == 1) {
     // LLSS d/f classes: one block per quartet with every ket component at
     // once, when it fits in shared memory (single-primitive quartets in
     // their own instance); else per thread
@@ -1769,18 +1768,18 @@ void launch_rel_prec(const RelLaunch& aIn, int la, int lb, int lc, int ld, cudaS
     } else {
       rel_kernel<3, TYPE, T><<<grid, REL_THREADS, 0, st>>>(a, la, lb, lc, ld, nsplit);
     }
-    return;
+  } else {
+    // SSSS d and f classes: one block per quartet, intermediates in shared memory
+    const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
+    const size_t smem = (size_t)Lo.total * sizeof(double);
+    cudaFuncSetAttribute(rel_block_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)REL_SMEM_MAX);
+    const long long nq = a.same ? (long long)a.nBra * (a.nBra + 1) / 2
+                                : (long long)a.nBra * a.nKet;
+    const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
+    const unsigned gy = (unsigned)((nq + gx - 1) / gx);
+    rel_block_kernel<TYPE, T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
   }
-  // SSSS d and f classes: one block per quartet, intermediates in shared memory
-  const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
-  const size_t smem = (size_t)Lo.total * sizeof(double);
-  cudaFuncSetAttribute(rel_block_kernel<TYPE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)REL_SMEM_MAX);
-  const long long nq = (TYPE == 2 && a.same) ? (long long)a.nBra * (a.nBra + 1) / 2
-                                             : (long long)a.nBra * a.nKet;
-  const unsigned gx = (unsigned)std::min<long long>(nq, 65535);
-  const unsigned gy = (unsigned)((nq + gx - 1) / gx);
-  rel_block_kernel<TYPE, T><<<dim3(gx, gy), RB_THREADS, smem, st>>>(a, la, lb, lc, ld);
 }
 
 template <int TYPE>
@@ -1981,8 +1980,6 @@ __device__ __forceinline__ Q4 qunit(int a) {  // sigma_a
   else r.z = make_double2(1, 0);
   return r;
 }
-__device__ __forceinline__ Q4 q_of(const Z4& z) { return Q4{z.c[0], z.c[1], z.c[2], z.c[3]}; }
-__device__ __forceinline__ Z4 z_of(const Q4& q) { return Z4{{q.s, q.x, q.y, q.z}}; }
 __device__ __forceinline__ void zacc(Z4& a, const Q4& b, double f) {
   a.c[0] = cadd(a.c[0], cscale(b.s, f));
   a.c[1] = cadd(a.c[1], cscale(b.x, f));
