@@ -1252,6 +1252,7 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
 // (and the classes whose layout does not fit).
 constexpr int RG_THREADS = 256;
 constexpr size_t RG_SMEM_MAX = 224 * 1024;
+constexpr size_t RG_SMEM_HALF = 112 * 1024;  // two blocks per SM (228 KB, 1 KB reserved each)
 
 struct RelGemmLayout {
   int HB, HBp, HK, HR, CH, CR, CRp, NT;
@@ -1289,7 +1290,7 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   int p = o;
   auto takeB = [&](int n) { int r = p; p += rg_round(n, 4); return r; };
   Lo.oEb = takeB(3 * (la + 2) * (lb + 2) * (la + lb + 3));
-  Lo.oFa = takeB(nab * 12 * FL);
+  Lo.oFa = takeB(3 * (la + 1) * (lb + 1) * 4 * FL);  // per (axis, exponent pair, type)
   int k = o;
   auto takeK = [&](int n) { int r = k; k += rg_round(n, 4); return r; };
   Lo.oEk = takeK(3 * (lc + 1 + dK) * (ld + 1 + dK) * (lc + ld + 1 + 2 * dK));
@@ -1304,9 +1305,16 @@ __host__ __device__ inline RelGemmLayout rel_gemm_layout(int la, int lb, int lc,
   if (q > Lo.total) Lo.total = q;
   return Lo;
 }
-// the largest ket chunk whose layout fits (0: the class does not fit)
+// the ket chunk: the largest whose layout leaves two blocks per SM, if that
+// is at least 4 ket pairs (or all of them); else the largest that fits at
+// all (one block per SM); 0: the class does not fit
 inline int rel_gemm_chunk(int la, int lb, int lc, int ld, int type, int esz) {
   const int ncd = ncart(lc) * ncart(ld);
+  for (int ch = ncd; ch >= 1; ch--)
+    if ((size_t)rel_gemm_layout(la, lb, lc, ld, type, ch, esz).total * esz <= RG_SMEM_HALF) {
+      if (ch >= 4 || ch == ncd) return ch;
+      break;
+    }
   for (int ch = ncd; ch >= 1; ch--)
     if ((size_t)rel_gemm_layout(la, lb, lc, ld, type, ch, esz).total * esz <= RG_SMEM_MAX)
       return ch;
@@ -1401,15 +1409,16 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
   }
   for (int e = tid; e < 4 * CH; e += RG_THREADS) Js[e] = 0.0;
   __syncthreads();
-  for (int it = tid; it < nab * 12; it += RG_THREADS) {
-    const int ab = it / 12, x = (it % 12) / 4, ty = it % 4;
-    const int ai = ab / nb, bi = ab % nb;
-    const int ia = x == 0 ? cart_lx(la, ai) : (x == 1 ? cart_ly(la, ai) : cart_lz(la, ai));
-    const int jb = x == 0 ? cart_lx(lb, bi) : (x == 1 ? cart_ly(lb, bi) : cart_lz(lb, bi));
+  for (int it = tid; it < 3 * (la + 1) * (lb + 1) * 4; it += RG_THREADS) {
+    const int ty = it % 4, jb = (it / 4) % (lb + 1), ia = (it / 4 / (lb + 1)) % (la + 1),
+              x = it / 4 / (lb + 1) / (la + 1);
     axis_factor<T>(Eb + x * E1b, lb + 1, la + lb + 3, ia, jb, ty, T(2.0 * ea), T(2.0 * eb),
                    fa + (size_t)it * FL);
   }
   __syncthreads();
+  auto faOf = [&](int x, int i, int j, int ty) {
+    return fa + (size_t)(((x * (la + 1) + i) * (lb + 1) + j) * 4 + ty) * FL;
+  };
   for (int e = tid; e < HB * HR; e += RG_THREADS) {
     const int h = e / HR, row = e % HR, ab = row / 4, op = row % 4;
     const int ai = ab / nb, bi = ab % nb;
@@ -1430,9 +1439,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
             u >= ax[1] + bx[1] + (ty & 1) + (ty >> 1) + 1 ||
             v >= ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1)
           continue;
-        val += T(sg) * fa[((size_t)ab * 12 + 0 * 4 + tx) * FL + t] *
-               fa[((size_t)ab * 12 + 1 * 4 + ty) * FL + u] *
-               fa[((size_t)ab * 12 + 2 * 4 + tz) * FL + v];
+        val += T(sg) * faOf(0, ax[0], bx[0], tx)[t] * faOf(1, ax[1], bx[1], ty)[u] *
+               faOf(2, ax[2], bx[2], tz)[v];
       }
     Hs[e] = val;
   }
