@@ -56,28 +56,19 @@ __host__ __device__ constexpr int nherm(int L) {
 __host__ __device__ constexpr int hidx(int t, int u, int v) {
   return nherm(t + u + v - 1) + (u + v) * (u + v + 1) / 2 + v;
 }
-// Cartesian exponents of component i of an l shell (libint / CCA order)
-__host__ __device__ constexpr int cart_lx(int l, int i) {
-  int k = 0;
-  for (int a = 0; a <= l; a++)
-    for (int b = 0; b <= a; b++) {
-      if (k == i) return l - a;
-      k++;
-    }
-  return 0;
-}
-__host__ __device__ constexpr int cart_ly(int l, int i) {
-  int k = 0;
-  for (int a = 0; a <= l; a++)
-    for (int b = 0; b <= a; b++) {
-      if (k == i) return a - b;
-      k++;
-    }
-  return 0;
+// Cartesian exponents of component i of an l shell (libint / CCA order):
+// i = a (a + 1) / 2 + b runs over a = 0 .. l, b = 0 .. a with
+// (lx, ly, lz) = (l - a, a - b, b).  The row a of i by comparisons with the
+// triangular numbers (components of l <= 8).
+__host__ __device__ constexpr int cart_row(int i) {
+  return (i >= 1) + (i >= 3) + (i >= 6) + (i >= 10) + (i >= 15) + (i >= 21) + (i >= 28) +
+         (i >= 36);
 }
 __host__ __device__ constexpr int cart_lz(int l, int i) {
-  return l - cart_lx(l, i) - cart_ly(l, i);
+  return i - cart_row(i) * (cart_row(i) + 1) / 2;
 }
+__host__ __device__ constexpr int cart_lx(int l, int i) { return l - cart_row(i); }
+__host__ __device__ constexpr int cart_ly(int l, int i) { return cart_row(i) - cart_lz(l, i); }
 
 struct __align__(16) ShellDev {
   int l, pure, nprim, prim_off;
