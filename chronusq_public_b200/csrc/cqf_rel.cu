@@ -496,9 +496,25 @@ __device__ __forceinline__ void hinv(int e, int& t, int& u, int& v) {
 
 constexpr int RB_THREADS = 128;
 
+// The block kernels' table of Hermite indices: tab[h] = t | u << 8 | v << 16
+// for h < n (hinv once per block instead of per use).
+__device__ __forceinline__ void htab_fill(int* tab, int n) {
+  for (int h = threadIdx.x; h < n; h += blockDim.x) {
+    int t, u, v;
+    hinv(h, t, u, v);
+    tab[h] = t | (u << 8) | (v << 16);
+  }
+}
+__device__ __forceinline__ void htab_get(const int* tab, int h, int& t, int& u, int& v) {
+  const int w = tab[h];
+  t = w & 255;
+  u = (w >> 8) & 255;
+  v = w >> 16;
+}
+
 // Shared-memory layout of rel_block_kernel (doubles), per launch.
 struct RelBlockLayout {
-  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, total;
+  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, oT, total;
 };
 __host__ __device__ inline RelBlockLayout rel_block_layout(int la, int lb, int lc, int ld,
                                                            int type) {
@@ -521,6 +537,7 @@ __host__ __device__ inline RelBlockLayout rel_block_layout(int la, int lb, int l
   Lo.oM = take(nab * 4 * NB);
   Lo.oF = take(L + 1);
   Lo.oJ = take(4);
+  Lo.oT = take((nherm(L) + 1) / 2);  // packed (t, u, v) of each Hermite index, int
   Lo.total = o;
   return Lo;
 }
@@ -596,6 +613,8 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int Lb = la + lb + 2, L = Lb + lc + ld + 2 * dK;
   const int FL = 2 * max(la, lb) + 3, FLk = 2 * max(lc, ld) + 3;
   const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
+  int* htab = reinterpret_cast<int*>(sm + Lo.oT);
+  htab_fill(htab, nherm(L));  // read after prep's first barrier
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -644,7 +663,7 @@ __global__ void __launch_bounds__(RB_THREADS)
       const int cnt = nherm(L - n);
       for (int e = tid; e < cnt; e += RB_THREADS) {
         int t, u, v;
-        hinv(e, t, u, v);
+        htab_get(htab, e, t, u, v);
         T val;
         if (e == 0) {
           T f = T(1);
@@ -707,7 +726,7 @@ __global__ void __launch_bounds__(RB_THREADS)
         for (int e = tid; e < NB * hb; e += RB_THREADS) {
           const int b = e / hb, h = e % hb;
           int t, u, v;
-          hinv(h, t, u, v);
+          htab_get(htab, h, t, u, v);
           const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
           const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
           T gsum = T(0);
@@ -805,7 +824,7 @@ __global__ void __launch_bounds__(RB_THREADS)
 // axis, so they are kept per (axis, i, j[, derivative type]); single-primitive
 // launches digest each element as it is made and keep no accumulator Mc.
 struct LlssBlockLayout {
-  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, total;
+  int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, oT, total;
 };
 __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int lc, int ld,
                                                              bool single) {
@@ -825,6 +844,7 @@ __host__ __device__ inline LlssBlockLayout llss_block_layout(int la, int lb, int
   Lo.oM = take(single ? 0 : nab * ncd * 4);
   Lo.oF = take(L + 1);
   Lo.oJ = take(ncd);
+  Lo.oT = take((nherm(L) + 1) / 2);  // packed (t, u, v) of each Hermite index, int
   Lo.total = o;
   return Lo;
 }
@@ -871,6 +891,8 @@ __global__ void __launch_bounds__(RB_THREADS)
   const int hb = nherm(Lb);
   const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
   const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, false);
+  int* htab = reinterpret_cast<int*>(sm + Lo.oT);
+  htab_fill(htab, nherm(L));  // read after the first barrier of the primitive loop
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -929,7 +951,7 @@ __global__ void __launch_bounds__(RB_THREADS)
         const int cnt = nherm(L - n);
         for (int e = tid; e < cnt; e += RB_THREADS) {
           int t, u, v;
-          hinv(e, t, u, v);
+          htab_get(htab, e, t, u, v);
           T val;
           if (e == 0) {
             T f = T(1);
@@ -969,7 +991,7 @@ __global__ void __launch_bounds__(RB_THREADS)
       for (int e = tid; e < ncd * hb; e += RB_THREADS) {
         const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
         int t, u, v;
-        hinv(h, t, u, v);
+        htab_get(htab, h, t, u, v);
         const T* fx = fcOf(0, cart_lx(lc, c), cart_lx(ld, d));
         const T* fy = fcOf(1, cart_ly(lc, c), cart_ly(ld, d));
         const T* fz = fcOf(2, cart_lz(lc, c), cart_lz(ld, d));
@@ -1063,6 +1085,8 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
   const int hb = nherm(Lb);
   const int FL = 2 * max(la, lb) + 3, FLk = lc + ld + 1;
   const LlssBlockLayout Lo = llss_block_layout(la, lb, lc, ld, true);
+  int* htab = reinterpret_cast<int*>(sm + Lo.oT);
+  htab_fill(htab, nherm(L));  // read after the bra phase's barrier
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -1142,7 +1166,7 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
       const int cnt = nherm(L - n);
       for (int e = tid; e < cnt; e += RB_THREADS) {
         int t, u, v;
-        hinv(e, t, u, v);
+        htab_get(htab, e, t, u, v);
         T val;
         if (e == 0) {
           T f = T(1);
@@ -1175,7 +1199,7 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
     for (int e = tid; e < ncd * hb; e += RB_THREADS) {
       const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
       int t, u, v;
-      hinv(h, t, u, v);
+      htab_get(htab, h, t, u, v);
       const T* fx = fcOf(0, cart_lx(lc, c), cart_lx(ld, d));
       const T* fy = fcOf(1, cart_ly(lc, c), cart_ly(ld, d));
       const T* fz = fcOf(2, cart_lz(lc, c), cart_lz(ld, d));
