@@ -512,6 +512,23 @@ __device__ __forceinline__ void htab_get(const int* tab, int h, int& t, int& u, 
   v = w >> 16;
 }
 
+// Division by a runtime divisor d >= 1 as a multiply-high: with
+// m = ceil(2^32 / d), floor(x m / 2^32) = floor(x / d) for 0 <= x < 2^32 / d
+// (the error of m is below d).  The kernels' element indices are < 2^20.
+struct FastDiv {
+  unsigned m;
+  int d;
+  __device__ __forceinline__ explicit FastDiv(int dv)
+      : m(dv == 1 ? 0u : 0xFFFFFFFFu / (unsigned)dv + 1u), d(dv) {}
+  __device__ __forceinline__ int div(int x) const {
+    return d == 1 ? x : (int)__umulhi((unsigned)x, m);
+  }
+  __device__ __forceinline__ void divmod(int x, int& q, int& r) const {
+    q = div(x);
+    r = x - q * d;
+  }
+};
+
 // Shared-memory layout of rel_block_kernel (doubles), per launch.
 struct RelBlockLayout {
   int oR0, oR1, oEb, oEk, oFa, oFc, oG, oM, oF, oJ, oT, total;
@@ -615,6 +632,7 @@ __global__ void __launch_bounds__(RB_THREADS)
   const RelBlockLayout Lo = rel_block_layout(la, lb, lc, ld, TYPE);
   int* htab = reinterpret_cast<int*>(sm + Lo.oT);
   htab_fill(htab, nherm(L));  // read after prep's first barrier
+  const FastDiv fhbB(nherm(Lb)), fnbB(nb);
   T* Rb[2] = {reinterpret_cast<T*>(sm + Lo.oR0), reinterpret_cast<T*>(sm + Lo.oR1)};
   T* Eb = reinterpret_cast<T*>(sm + Lo.oEb);
   T* Ek = reinterpret_cast<T*>(sm + Lo.oEk);
@@ -724,7 +742,8 @@ __global__ void __launch_bounds__(RB_THREADS)
         // G[b][tuv]
         const int hb = nherm(Lb);
         for (int e = tid; e < NB * hb; e += RB_THREADS) {
-          const int b = e / hb, h = e % hb;
+          int b, h;
+          fhbB.divmod(e, b, h);
           int t, u, v;
           htab_get(htab, h, t, u, v);
           const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
@@ -765,7 +784,8 @@ __global__ void __launch_bounds__(RB_THREADS)
         // operator components of every bra component pair: unit (ab, b)
         for (int e = tid; e < nab * NB; e += RB_THREADS) {
           const int ab = e / NB, b = e % NB;
-          const int ai = ab / nb, bi = ab % nb;
+          int ai, bi;
+          fnbB.divmod(ab, ai, bi);
           const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
           const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
           double m4[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1108,6 +1128,7 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
   auto fcOf = [&](int x, int i, int j) {
     return fc + (size_t)((x * (lc + 1) + i) * (ld + 1) + j) * FLk;
   };
+  const FastDiv fncd(ncd), fnb(nb), fnd(nd), fhb(hb);
 
   // ---- bra phase: E tables and axis factors of every axis, exponent pair
   // and derivative type
@@ -1197,7 +1218,9 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
     }
     // G[cd][tuv] of every ket component pair
     for (int e = tid; e < ncd * hb; e += RB_THREADS) {
-      const int cd = e / hb, h = e % hb, c = cd / nd, d = cd % nd;
+      int cd, h, c, d;
+      fhb.divmod(e, cd, h);
+      fnd.divmod(cd, c, d);
       int t, u, v;
       htab_get(htab, h, t, u, v);
       const T* fx = fcOf(0, cart_lx(lc, c), cart_lx(ld, d));
@@ -1220,8 +1243,10 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
     __syncthreads();
     // operator components of every (bra, ket) component element, digested
     for (int e = tid; e < nab * ncd; e += RB_THREADS) {
-      const int ab = e / ncd, cd = e % ncd;
-      const int ai = ab / nb, bi = ab % nb;
+      int ab, cd, ai, bi, c, d;
+      fncd.divmod(e, ab, cd);
+      fnb.divmod(ab, ai, bi);
+      fnd.divmod(cd, c, d);
       const int ax[3] = {cart_lx(la, ai), cart_ly(la, ai), cart_lz(la, ai)};
       const int bx[3] = {cart_lx(lb, bi), cart_ly(lb, bi), cart_lz(lb, bi)};
       double m4[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1239,7 +1264,7 @@ __global__ void __launch_bounds__(RB_THREADS, 8)
                                  faOf(2, ax[2], bx[2], tz),
                                  ax[2] + bx[2] + (tz & 1) + (tz >> 1) + 1, G + (size_t)cd * hb);
         }
-      const int gC = Q.cA + cd / nd, gD = Q.cB + cd % nd;
+      const int gC = Q.cA + c, gD = Q.cB + d;
       RelCol col{gC, gD, dAB, dCD, false, s34d, w12, 1.0,
                  __ldg(a.Xll + 2 * ((size_t)gD + (size_t)gC * nc)), {0, 0, 0, 0}};
       double jl[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1392,6 +1417,7 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
   const int FL = 2 * max(la, lb) + 3, FLk = 2 * max(lc, ld) + 3;
   const RelGemmLayout Lo = rel_gemm_layout(la, lb, lc, ld, TYPE, CH, (int)sizeof(T));
   const int HB = Lo.HB, HBp = Lo.HBp, HK = Lo.HK, HR = Lo.HR, CRp = Lo.CRp;
+  const FastDiv fHBp(HBp), fCRp(CRp), ftr(CRp / 4), fnab(nab), fnb(nb), fnd(nd);
   T* Hs = smT + Lo.oH;
   T* Rm = smT + Lo.oRm;
   T* fk = smT + Lo.oFk;
@@ -1563,7 +1589,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
       for (int t = 1; t < n; t += 2) f[t] = -f[t];
     }
     for (int e = tid; e < HK * HBp; e += RG_THREADS) {
-      const int hp = e / HBp, h = e % HBp;
+      int hp, h;
+      fHBp.divmod(e, hp, h);
       T val = T(0);
       if (h < HB) {
         int t, u, v, t2, u2, v2;
@@ -1581,10 +1608,14 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
       const int nch = min(CH, ncd - cd0);
       // K[h'][(cdl, b)]
       for (int e = tid; e < HK * CRp; e += RG_THREADS) {
-        const int hp = e / CRp, r = e % CRp, cdl = r / NB, b = r % NB;
+        int hp, r;
+        fCRp.divmod(e, hp, r);
+        const int cdl = r / NB, b = r % NB;
         T val = T(0);
         if (cdl < nch) {
-          const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
+          const int cd = cd0 + cdl;
+          int c, d;
+          fnd.divmod(cd, c, d);
           const int ci[3] = {cart_lx(lc, c), cart_ly(lc, c), cart_lz(lc, c)};
           const int di[3] = {cart_lx(ld, d), cart_ly(ld, d), cart_lz(ld, d)};
           int t, u, v;
@@ -1618,7 +1649,9 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
       {
         const int tr = CRp / 4, th = HBp / 4;
         for (int unit = tid; unit < tr * th; unit += RG_THREADS) {
-          const int r0 = (unit % tr) * 4, h0 = (unit / tr) * 4;
+          int hq, rq;
+          ftr.divmod(unit, hq, rq);
+          const int r0 = rq * 4, h0 = hq * 4;
           T acc[4][4];
 #pragma unroll
           for (int i = 0; i < 4; i++)
@@ -1645,7 +1678,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
       {
         const int ngrp = (TYPE == 2) ? nch : (nch + 3) / 4;
         for (int unit = tid; unit < nab * ngrp; unit += RG_THREADS) {
-          const int ab = unit % nab, grp = unit / nab;
+          int grp, ab;
+          fnab.divmod(unit, grp, ab);
           const int col0 = (TYPE == 2) ? grp * 4 : grp * 4;  // first column of the tile
           T acc[4][4];
 #pragma unroll
@@ -1662,9 +1696,11 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
 #pragma unroll
               for (int j = 0; j < 4; j++) acc[i][j] = fma(hv[i], gv[j], acc[i][j]);
           }
-          const int ai = ab / nb, bi = ab % nb;
+          int ai, bi;
+          fnb.divmod(ab, ai, bi);
           auto column = [&](int cdl) {
-            const int cd = cd0 + cdl, c = cd / nd, d = cd % nd;
+            int c, d;
+            fnd.divmod(cd0 + cdl, c, d);
             const int gC = Q.cA + c, gD = Q.cB + d;
             RelCol col{gC, gD, dAB, dCD, samePQ, dCD ? 1.0 : 2.0, w12, samePQ ? 0.5 : 1.0, 0.0,
                        {0, 0, 0, 0}};
