@@ -95,6 +95,35 @@ __device__ __forceinline__ Q4 qmul(const Q4& p, const Q4& q) {
   return r;
 }
 
+// p (m0 + i w . sigma) for real m0 and w: m0 p.s + i p.v.w, and
+// i p.s w + m0 p.v - p.v x w (the general product with the zero parts of the
+// right factor left out)
+__device__ __forceinline__ Q4 qmul_ri(const Q4& p, double m0, double w1, double w2,
+                                      double w3) {
+  const double2 pw = make_double2(p.x.x * w1 + p.y.x * w2 + p.z.x * w3,
+                                  p.x.y * w1 + p.y.y * w2 + p.z.y * w3);
+  Q4 r;
+  r.s = make_double2(m0 * p.s.x - pw.y, m0 * p.s.y + pw.x);
+  // i p.s w_k = (-p.s.y w_k, p.s.x w_k)
+  r.x = make_double2(-p.s.y * w1 + m0 * p.x.x - (p.y.x * w3 - p.z.x * w2),
+                     p.s.x * w1 + m0 * p.x.y - (p.y.y * w3 - p.z.y * w2));
+  r.y = make_double2(-p.s.y * w2 + m0 * p.y.x - (p.z.x * w1 - p.x.x * w3),
+                     p.s.x * w2 + m0 * p.y.y - (p.z.y * w1 - p.x.y * w3));
+  r.z = make_double2(-p.s.y * w3 + m0 * p.z.x - (p.x.x * w2 - p.y.x * w1),
+                     p.s.x * w3 + m0 * p.z.y - (p.x.y * w2 - p.y.y * w1));
+  return r;
+}
+
+// t sigma_k (k = 1, 2, 3): sigma_j sigma_k = delta_jk + i eps_jkl sigma_l, so
+// t sigma_x = (t.x, t.s, i t.z, -i t.y), t sigma_y = (t.y, -i t.z, t.s, i t.x),
+// t sigma_z = (t.z, i t.y, -i t.x, t.s)
+__device__ __forceinline__ Q4 qsig(const Q4& t, int k) {
+  auto mi = [](double2 a) { return make_double2(a.y, -a.x); };  // -i a
+  if (k == 1) return Q4{t.x, t.s, ctimes_i(t.z), mi(t.y)};
+  if (k == 2) return Q4{t.y, mi(t.z), t.s, ctimes_i(t.x)};
+  return Q4{t.z, ctimes_i(t.y), mi(t.x), t.s};
+}
+
 __device__ __forceinline__ double2 ldz(const double* X, size_t e) {
   return __ldg(reinterpret_cast<const double2*>(X) + e);
 }
@@ -172,9 +201,8 @@ __device__ __forceinline__ void rel_digest(const RelLaunch& a, const PairDev& P,
     auto ls = [&](int t1, int t2, int d1, int d2, double flip) {
       const size_t e = ix(d1, d2);
       Q4 dq{ldz(a.Xk[0], e), ldz(a.Xk[1], e), ldz(a.Xk[2], e), ldz(a.Xk[3], e)};
-      Q4 Cq{make_double2(m[0], 0.0), make_double2(0.0, flip * m[1]),
-            make_double2(0.0, flip * m[2]), make_double2(0.0, flip * m[3])};
-      const Q4 r = qmul(dq, Cq);
+      // dq (m0 + i flip m.sigma)
+      const Q4 r = qmul_ri(dq, m[0], flip * m[1], flip * m[2], flip * m[3]);
       const size_t t = ix(t1, t2);
       addz(a.K[0], t, r.s, -1.0);
       addz(a.K[1], t, r.x, -1.0);
@@ -228,13 +256,8 @@ __device__ __forceinline__ void rel_digest(const RelLaunch& a, const PairDev& P,
           cz = make_double2(-f2 * cz.y, f2 * cz.x);
         }
         const Q4 Lq{cs, cx, cy, cz};
-        Q4 sb{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
-              make_double2(0, 0)};
-        if (b == 0) sb.s = make_double2(1, 0);
-        else if (b == 1) sb.x = make_double2(1, 0);
-        else if (b == 2) sb.y = make_double2(1, 0);
-        else sb.z = make_double2(1, 0);
-        const Q4 t = qmul(qmul(Lq, dq), sb);
+        const Q4 ld = qmul(Lq, dq);
+        const Q4 t = b == 0 ? ld : qsig(ld, b);  // (Lq dq) sigma_b
         r.s = cadd(r.s, t.s);
         r.x = cadd(r.x, t.x);
         r.y = cadd(r.y, t.y);
