@@ -156,7 +156,7 @@ struct RelLaunch {
   double* Jss[4];        // real
   double* K[4];          // complex
   int shardIdx, shardCnt;  // bra pairs p with p % shardCnt == shardIdx only
-  int skipSingle;          // single-primitive quartets go to rel_gemm_kernel
+  int skipSingle;          // single-primitive quartets: rel_gemm / rel_llss_single_kernel's
   int contracted;          // some bra or ket pair has more than one primitive pair
   int nsm;                 // multiprocessors of the device
   unsigned long long* counters;
@@ -1781,8 +1781,8 @@ __global__ void __launch_bounds__(RG_THREADS, 2)
   }  // kets
 }
 
-// Dynamic shared-memory limit of the block kernels (the largest layout, SSSS
-// (ff|ff), is 129 KB; LLSS layouts above it run per thread).
+// Dynamic shared-memory limit of the block kernels (SSSS (ff|ff) takes 51 KB;
+// the one LLSS layout above the limit, (ff|ff) at 165 KB, runs per thread).
 constexpr size_t REL_SMEM_MAX = 160 * 1024;
 
 // One class in one arithmetic precision: the instance in T computes the
