@@ -36,24 +36,6 @@ __device__ __forceinline__ int axis_factor(const T* E, int l2r, int Lr, int i, i
   return n;
 }
 
-// sum_k f[k] H[hidx(t, u, v + k)] for k < n, the Hermite index stepped
-// incrementally: hidx(t, u, v + 1) - hidx(t, u, v) = (s + 1)(s + 2) / 2 +
-// (u + v) + 2 with s = t + u + v, and that step grows by s + 3 per k.
-template <typename T>
-__device__ __forceinline__ T hdot_v(const T* f, int n, const T* H, int t, int u, int v) {
-  const int s = t + u + v;
-  int idx = hidx(t, u, v);
-  int inc = (s + 1) * (s + 2) / 2 + (u + v) + 2;
-  T acc = T(0);
-#pragma unroll 1
-  for (int k = 0; k < n; k++) {
-    acc += f[k] * H[idx];
-    idx += inc;
-    inc += s + k + 3;
-  }
-  return acc;
-}
-
 // G[tuv] += s * sum f_x[tau] f_y[nu] f_z[phi] R_{t+tau+sx,u+nu+sy,v+phi+sz}
 // for t+u+v <= Lb; the ket factors carry the (-1)^(tau+nu+phi) sign
 // already; (sx, sy, sz): the Hermite shift of an operator derivative.

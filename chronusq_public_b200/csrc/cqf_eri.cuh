@@ -182,6 +182,24 @@ __device__ __forceinline__ void boys_lanes<float>(int L, float T, float* F, cons
   __syncwarp();
 }
 
+// sum_k f[k] H[hidx(t, u, v + k)] for k < n, the Hermite index stepped
+// incrementally: hidx(t, u, v + 1) - hidx(t, u, v) = (s + 1)(s + 2) / 2 +
+// (u + v) + 2 with s = t + u + v, and that step grows by s + 3 per k.
+template <typename T>
+__device__ __forceinline__ T hdot_v(const T* f, int n, const T* H, int t, int u, int v) {
+  const int s = t + u + v;
+  int idx = hidx(t, u, v);
+  int inc = (s + 1) * (s + 2) / 2 + (u + v) + 2;
+  T acc = T(0);
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    acc += f[k] * H[idx];
+    idx += inc;
+    inc += s + k + 3;
+  }
+  return acc;
+}
+
 // Storage bounds for angular momenta up to LM per shell.
 template <int LM>
 struct RtBounds {
@@ -236,6 +254,10 @@ __device__ void eri_column_rt(int la, int lb, int lc, int ld, int c, int d, cons
       const T* ex = Ec[0] + (cx * (ld + 1) + dx) * Lcd1;
       const T* ey = Ec[1] + (cy * (ld + 1) + dy) * Lcd1;
       const T* ez = Ec[2] + (cz * (ld + 1) + dz) * Lcd1;
+      // the ket's (-1)^(tau + nu + phi): phi's in ezs, tau's and nu's in exy
+      T ezs[2 * LM + 1];
+#pragma unroll 1
+      for (int ph = 0; ph <= cz + dz; ph++) ezs[ph] = (ph & 1) ? -ez[ph] : ez[ph];
 #pragma unroll 1
       for (int t = 0; t <= lab; t++)
 #pragma unroll 1
@@ -247,13 +269,8 @@ __device__ void eri_column_rt(int la, int lb, int lc, int ld, int c, int d, cons
             for (int ta = 0; ta <= cx + dx; ta++)
 #pragma unroll 1
               for (int nu = 0; nu <= cy + dy; nu++) {
-                const T exy = ex[ta] * ey[nu];
-#pragma unroll 1
-                for (int ph = 0; ph <= cz + dz; ph++) {
-                  const T e = exy * ez[ph];
-                  const T r = Rv[hidx(t + ta, u + nu, v + ph)];
-                  s += ((ta + nu + ph) & 1) ? -e * r : e * r;
-                }
+                const T exy = ((ta + nu) & 1) ? -(ex[ta] * ey[nu]) : ex[ta] * ey[nu];
+                s += exy * hdot_v(ezs, cz + dz + 1, Rv, t + ta, u + nu, v);
               }
             G[hidx(t, u, v)] += pref * s;
           }
@@ -271,11 +288,8 @@ __device__ void eri_column_rt(int la, int lb, int lc, int ld, int c, int d, cons
 #pragma unroll 1
         for (int t = 0; t <= ax + bx; t++)
 #pragma unroll 1
-          for (int u = 0; u <= ay + by; u++) {
-            const T fxy = fx[t] * fy[u];
-#pragma unroll 1
-            for (int v = 0; v <= az + bz; v++) s += fxy * fz[v] * G[hidx(t, u, v)];
-          }
+          for (int u = 0; u <= ay + by; u++)
+            s += fx[t] * fy[u] * hdot_v(fz, az + bz + 1, G, t, u, 0);
         col[a * nb + b] += double(s);
       }
     }
